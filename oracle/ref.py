@@ -1,0 +1,303 @@
+"""ctypes front-end for the oracle libraries built by oracle/Makefile.
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, the smoke check and the CPU
+baseline leg of bench.py.  The libraries wrap the reference FornaxAMR C core
+(compiled unmodified from its own sources) plus oracle/ref_harness.c, so every
+number produced here is the reference's CPU path.
+
+Block arrays are returned as numpy copies in the reference's own per-block
+layout (src/prj_defs.h:383-453 of the reference): W is [var][stage][cell] with
+cell = LIDX, eosvar/flux/v_riemann are AoSoA with 4-wide k lanes, Bf is
+[stage][FACE_IDX], emf is [EDGE_IDX].
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REF_DIR = os.path.join(HERE, "_ref")
+
+BS = 16
+NG = 2
+PBS = BS + 2 * NG
+NCELLS = PBS ** 3
+NFACES = (PBS + 1) * PBS * PBS
+NEDGES = (PBS + 1) * (PBS + 1) * PBS
+NSTAGES = 2
+
+ARR_W, ARR_EOSVAR, ARR_U, ARR_RHS, ARR_FLUX, ARR_VRIEMANN, ARR_GRAV, ARR_BF, ARR_BV1, ARR_BV2, ARR_EMF = range(11)
+
+CFG_SOD, CFG_FOURIER_MHD, CFG_AMR_BLAST, CFG_COLLAPSE = 1, 2, 3, 4
+
+
+class RhParams(C.Structure):
+    _fields_ = [
+        ("config", C.c_int),
+        ("root", C.c_int * 3),
+        ("max_level", C.c_int),
+        ("max_blocks", C.c_int),
+        ("xmin", C.c_double * 3),
+        ("xmax", C.c_double * 3),
+        ("gamma", C.c_double),
+        ("cfl", C.c_double),
+        ("dt_factor", C.c_double),
+        ("t_end", C.c_double),
+        ("nmodes", C.c_int),
+        ("kmax", C.c_int),
+        ("amp_rho", C.c_double),
+        ("amp_v", C.c_double),
+        ("amp_A", C.c_double),
+        ("seed_rho", C.c_ulonglong),
+        ("seed_v", C.c_ulonglong),
+        ("seed_A", C.c_ulonglong),
+        ("center", C.c_double * 3),
+        ("refine_radius", C.c_double * 4),
+        ("p_in", C.c_double),
+        ("p_out", C.c_double),
+        ("r_in", C.c_double),
+        ("B0", C.c_double * 3),
+        ("rho_c", C.c_double),
+        ("r0", C.c_double),
+        ("K", C.c_double),
+        ("beta", C.c_double),
+        ("gm_point", C.c_double),
+    ]
+
+
+def lib_path(mhd: bool) -> str:
+    return os.path.join(REF_DIR, "libprjref_mhd.so" if mhd else "libprjref_hydro.so")
+
+
+def available(mhd: bool = True) -> bool:
+    return os.path.exists(lib_path(mhd))
+
+
+class Reference:
+    """One loaded copy of the reference core (one build variant)."""
+
+    def __init__(self, mhd: bool = True):
+        path = lib_path(mhd)
+        if not os.path.exists(path):
+            raise FileNotFoundError(f"oracle library missing: {path} (run make -C oracle)")
+        self.mhd = mhd
+        self.lib = L = C.CDLL(path, mode=C.RTLD_LOCAL)
+        dp = C.POINTER(C.c_double)
+        ip = C.POINTER(C.c_int)
+        L.rh_setup.argtypes = [C.POINTER(RhParams)]
+        L.rh_setup.restype = C.c_int
+        L.rh_calc_dt.restype = C.c_double
+        L.rh_step.argtypes = [C.c_double, dp]
+        L.rh_stage.argtypes = [C.c_int, C.c_double, dp]
+        L.rh_run.argtypes = [C.c_int, dp]
+        L.rh_run.restype = C.c_int
+        L.rh_time_steps.argtypes = [C.c_int, C.c_double]
+        L.rh_time_steps.restype = C.c_double
+        L.rh_block_geom.argtypes = [C.c_int, ip, dp]
+        L.rh_block_slots.argtypes = [C.c_int, ip]
+        L.rh_block_array.argtypes = [C.c_int, C.c_int, C.c_int]
+        L.rh_block_array.restype = dp
+        L.rh_mc_slope.argtypes = [C.c_double] * 3
+        L.rh_mc_slope.restype = C.c_double
+        L.rh_hllc.argtypes = [dp, dp] + [C.c_double] * 7 + [dp]
+        L.rh_prim2cons.argtypes = [dp, dp]
+        L.rh_cons2prim.argtypes = [dp, dp]
+        L.rh_eos_rey.argtypes = [C.c_double] * 3 + [dp]
+        L.rh_set_gamma.argtypes = [C.c_double]
+        L.rh_flux_update.argtypes = [C.c_int, C.c_int, C.c_int]
+        L.rh_sim_time.restype = C.c_double
+        L.rh_sim_dt.restype = C.c_double
+        if mhd:
+            L.rh_hlld.argtypes = [dp, dp] + [C.c_double] * 5 + [dp]
+            L.rh_emf_upwind.argtypes = [dp, dp, dp]
+            L.rh_emf_upwind.restype = C.c_double
+        self.nhydro = L.rh_nhydro()
+
+    # -- set-up and stepping ------------------------------------------------
+    def setup(self, params: RhParams) -> None:
+        rc = self.lib.rh_setup(C.byref(params))
+        if rc != 0:
+            raise RuntimeError(f"rh_setup failed with {rc}")
+
+    def calc_dt(self) -> float:
+        return self.lib.rh_calc_dt()
+
+    def step(self, dt: float) -> float:
+        out = C.c_double(0.0)
+        self.lib.rh_step(dt, C.byref(out))
+        return out.value
+
+    def stage(self, which: int, dt: float) -> float:
+        out = C.c_double(0.0)
+        self.lib.rh_stage(which, dt, C.byref(out))
+        return out.value
+
+    def run(self, nsteps: int):
+        st = (C.c_double * 3)()
+        n = self.lib.rh_run(nsteps, st)
+        return n, st[0], st[1], int(st[2])
+
+    def time_steps(self, nsteps: int, dt: float) -> float:
+        return self.lib.rh_time_steps(nsteps, dt)
+
+    # -- mesh description -----------------------------------------------------
+    def nblocks(self) -> int:
+        return self.lib.rh_nblocks()
+
+    def block_geom(self, b: int):
+        ints = (C.c_int * 4)()
+        dbl = (C.c_double * 13)()
+        self.lib.rh_block_geom(b, ints, dbl)
+        return list(ints), np.array(dbl[:], dtype=np.float64)
+
+    def block_slots(self, b: int) -> np.ndarray:
+        out = (C.c_int * (56 * 15))()
+        self.lib.rh_block_slots(b, out)
+        return np.array(out[:], dtype=np.int32).reshape(56, 15)
+
+    # -- block arrays ---------------------------------------------------------
+    def _arr(self, b: int, which: int, dir_: int, count: int) -> np.ndarray:
+        p = self.lib.rh_block_array(b, which, dir_)
+        if not p:
+            raise ValueError("array not present in this build")
+        return np.ctypeslib.as_array(p, shape=(count,)).copy()
+
+    def _set(self, b: int, which: int, dir_: int, data: np.ndarray) -> None:
+        p = self.lib.rh_block_array(b, which, dir_)
+        if not p:
+            raise ValueError("array not present in this build")
+        dst = np.ctypeslib.as_array(p, shape=(data.size,))
+        dst[:] = data.ravel()
+
+    def W(self, b: int) -> np.ndarray:
+        return self._arr(b, ARR_W, 0, self.nhydro * NSTAGES * NCELLS)
+
+    def set_W(self, b: int, data: np.ndarray) -> None:
+        self._set(b, ARR_W, 0, data)
+
+    def eosvar(self, b: int) -> np.ndarray:
+        return self._arr(b, ARR_EOSVAR, 0, 3 * NCELLS)
+
+    def flux(self, b: int, d: int) -> np.ndarray:
+        return self._arr(b, ARR_FLUX, d, self.nhydro * NCELLS)
+
+    def vriemann(self, b: int, d: int) -> np.ndarray:
+        return self._arr(b, ARR_VRIEMANN, d, 3 * NCELLS)
+
+    def grav(self, b: int, d: int) -> np.ndarray:
+        return self._arr(b, ARR_GRAV, d, NCELLS)
+
+    def rhs(self, b: int) -> np.ndarray:
+        return self._arr(b, ARR_RHS, 0, self.nhydro * NCELLS)
+
+    def Bf(self, b: int, d: int) -> np.ndarray:
+        return self._arr(b, ARR_BF, d, NSTAGES * NFACES)
+
+    def set_Bf(self, b: int, d: int, data: np.ndarray) -> None:
+        self._set(b, ARR_BF, d, data)
+
+    def Bv(self, b: int, d: int):
+        return self._arr(b, ARR_BV1, d, NCELLS), self._arr(b, ARR_BV2, d, NCELLS)
+
+    def emf(self, b: int, d: int) -> np.ndarray:
+        return self._arr(b, ARR_EMF, d, NEDGES)
+
+    def flux_update(self, b: int, w_slot: int, use_bf1: int) -> None:
+        self.lib.rh_flux_update(b, w_slot, use_bf1)
+
+    # -- single kernels -------------------------------------------------------
+    def mc_slope(self, qm, q0, qp) -> float:
+        return self.lib.rh_mc_slope(qm, q0, qp)
+
+    def hlld(self, WL, WR, pL, pR, gL, gR, bn) -> np.ndarray:
+        wl = np.ascontiguousarray(WL, dtype=np.float64)
+        wr = np.ascontiguousarray(WR, dtype=np.float64)
+        out = np.zeros(14)
+        dp = C.POINTER(C.c_double)
+        self.lib.rh_hlld(wl.ctypes.data_as(dp), wr.ctypes.data_as(dp), pL, pR, gL, gR, bn,
+                         out.ctypes.data_as(dp))
+        return out
+
+    def hllc(self, WL, WR, pL, pR, gL, gR, du, dv, dw) -> np.ndarray:
+        wl = np.ascontiguousarray(WL, dtype=np.float64)
+        wr = np.ascontiguousarray(WR, dtype=np.float64)
+        out = np.zeros(self.nhydro + 3)
+        dp = C.POINTER(C.c_double)
+        self.lib.rh_hllc(wl.ctypes.data_as(dp), wr.ctypes.data_as(dp), pL, pR, gL, gR,
+                         du, dv, dw, out.ctypes.data_as(dp))
+        return out
+
+    def emf_upwind(self, face, cell, vn) -> float:
+        dp = C.POINTER(C.c_double)
+        f = np.ascontiguousarray(face, dtype=np.float64)
+        c = np.ascontiguousarray(cell, dtype=np.float64)
+        v = np.ascontiguousarray(vn, dtype=np.float64)
+        return self.lib.rh_emf_upwind(f.ctypes.data_as(dp), c.ctypes.data_as(dp), v.ctypes.data_as(dp))
+
+    def prim2cons(self, w) -> np.ndarray:
+        dp = C.POINTER(C.c_double)
+        w = np.ascontiguousarray(w, dtype=np.float64)
+        u = np.zeros(self.nhydro)
+        self.lib.rh_prim2cons(w.ctypes.data_as(dp), u.ctypes.data_as(dp))
+        return u
+
+    def cons2prim(self, u) -> np.ndarray:
+        dp = C.POINTER(C.c_double)
+        u = np.ascontiguousarray(u, dtype=np.float64)
+        w = np.zeros(self.nhydro)
+        self.lib.rh_cons2prim(u.ctypes.data_as(dp), w.ctypes.data_as(dp))
+        return w
+
+    def eos_rey(self, rho, eint, ye) -> np.ndarray:
+        dp = C.POINTER(C.c_double)
+        out = np.zeros(3)
+        self.lib.rh_eos_rey(rho, eint, ye, out.ctypes.data_as(dp))
+        return out
+
+    def set_gamma(self, g: float) -> None:
+        self.lib.rh_set_gamma(g)
+
+
+# ---------------------------------------------------------------------------
+# Workload presets (the same recipes the product's own generators implement)
+# ---------------------------------------------------------------------------
+
+def params_sod(nblocks_x: int = 64, gamma: float = 1.4, t_end: float = 0.2) -> RhParams:
+    """1-D Sod tube run as a 3-D pencil of nblocks_x blocks of 16^3 cells on
+    x in [0,1] (transverse extent one block, dx equal on all axes)."""
+    p = RhParams()
+    p.config = CFG_SOD
+    p.root[:] = [nblocks_x, 1, 1]
+    p.max_level = 0
+    p.xmin[:] = [0.0, 0.0, 0.0]
+    p.xmax[:] = [1.0, 1.0 / nblocks_x, 1.0 / nblocks_x]
+    p.gamma = gamma
+    p.cfl = 0.4
+    p.dt_factor = 1.2
+    p.t_end = t_end
+    return p
+
+
+def params_fourier(root: int = 8, nmodes: int = 32, kmax: int = 4, amp_rho: float = 0.1,
+                   amp_v: float = 0.1, amp_A: float = 0.05, gamma: float = 5.0 / 3.0,
+                   seeds=(1, 2, 3)) -> RhParams:
+    """Seeded Fourier-mode ideal MHD on [0,1]^3 with root^3 blocks of 16^3."""
+    p = RhParams()
+    p.config = CFG_FOURIER_MHD
+    p.root[:] = [root, root, root]
+    p.max_level = 0
+    p.xmin[:] = [0.0, 0.0, 0.0]
+    p.xmax[:] = [1.0, 1.0, 1.0]
+    p.gamma = gamma
+    p.cfl = 0.4
+    p.dt_factor = 1.2
+    p.t_end = 1.0e30
+    p.nmodes = nmodes
+    p.kmax = kmax
+    p.amp_rho = amp_rho
+    p.amp_v = amp_v
+    p.amp_A = amp_A
+    p.seed_rho, p.seed_v, p.seed_A = seeds
+    return p
