@@ -1,0 +1,360 @@
+#!/usr/bin/env python
+"""Benchmark: zone-updates/s per RK2 step of the B200 Godunov MHD update.
+
+Workload: 3-D ideal MHD on a uniform 128^3 grid of 512 blocks of 16^3 cells
+(2 ghost zones), gamma = 5/3, seeded Fourier-mode initial data (32 modes,
+|k|_inf <= 4; rho amplitude 0.1, v amplitude 0.1, A amplitude 0.05), MC + HLLD
++ CT, RK2, FP64 -- synthetic data generated on the host by
+fornaxamr_b200.problems.
+
+One step = one pass of the driver loop: calc_dt, dt limiting, both RK2
+stages with ghost fills, dt_src clamp.  `value` is device time (CUDA events on
+the library's stream, state resident in HBM) for the batched form (every
+phase swept over all blocks, whole step replayed as one CUDA graph).  The
+working set (~2.7 GB) is far larger than L2, so no explicit flush is needed.
+`e2e` is the same metric through the C ABI with host buffers: each step
+uploads the state (W and Bf, stage slot 0) from pinned host memory, steps,
+and downloads it again.
+
+Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+For N > 1 (torchrun) every rank runs an independent replica (the path has no
+data exchange between GPUs in this build: replicas only); `value` is the sum.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import multiprocessing as mp
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, HERE)
+
+METRIC = "zone-updates/s per RK2 step"
+UNIT = "zone-updates/s"
+ROOT = 8                          # 8^3 blocks of 16^3 = 128^3
+ZONES = ROOT ** 3 * 16 ** 3
+BYTES_PER_ZONE_STEP = 360.0       # compulsory state traffic per zone per RK2 step (9 vars x 8 B x 5)
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="fx", choices=["fx", "reference"])
+    ap.add_argument("--plain-steps", type=int, default=2)
+    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+# ---------------------------------------------------------------------------
+# CPU reference (oracle/_ref: the reference's own C core), one process per core
+# ---------------------------------------------------------------------------
+
+def _cpu_worker(args):
+    nsteps, warm, root = args
+    from oracle import ref as R
+    r = R.Reference(True)
+    p = R.params_fourier(root=root)
+    r.setup(p)
+    dt = r.calc_dt()
+    if warm:
+        r.time_steps(warm, dt)
+    secs = r.time_steps(nsteps, dt)
+    return nsteps * (root ** 3) * 4096, secs
+
+
+def cpu_reference(steps: int, warmup: int, seconds: float):
+    """Reference CPU path on all host cores: one independent 2x2x2-block
+    (32^3-zone) instance of the workload per core, timed over `steps` steps.
+    The step count is bounded so the whole run takes about `seconds`."""
+    cores = min(len(os.sched_getaffinity(0)), 128)
+    ctx = mp.get_context("spawn")
+    # ~0.14 s per step per 2^3-block instance on one core: bound the sample
+    steps = max(1, min(steps, int(seconds / 0.15)))
+    with ctx.Pool(cores) as pool:
+        res = pool.map(_cpu_worker, [(steps, warmup, 2)] * cores)
+    zones = sum(z for z, _ in res)
+    wall = max(s for _, s in res)
+    return {"value": zones / wall, "unit": UNIT, "cores": cores, "kind": "reference",
+            "sample": f"{cores} independent instances of the workload recipe on 2^3 blocks of 16^3 "
+                      f"(32^3 zones each), {steps} RK2 steps each, serial reference C core "
+                      f"(-O3 -ffp-contract=off), one process per core"}
+
+
+# ---------------------------------------------------------------------------
+# clocks during the timed region
+# ---------------------------------------------------------------------------
+
+class Clocks:
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits", "-lms", "200",
+                 "-i", str(self.device)], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        self.lines = []
+        if self.proc is not None:
+            time.sleep(0.3)
+            self.proc.terminate()
+            try:
+                out, _ = self.proc.communicate(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+                out, _ = self.proc.communicate()
+            self.lines = [l for l in out.splitlines() if l.strip()]
+
+    def summary(self):
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for l in self.lines:
+            f = [x.strip() for x in l.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": smax, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+
+def measured_peak_hbm():
+    path = os.path.join(HERE, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def flux_traffic_per_launch():
+    """DRAM bytes of one face-flux launch from the committed ncu summary, or None."""
+    path = os.path.join(HERE, "profiles", "flux_traffic.json")
+    try:
+        with open(path) as f:
+            return float(json.load(f)["dram_bytes_per_launch"])
+    except (OSError, KeyError, ValueError):
+        return None
+
+
+def run_fx(args, rank, world, local_rank):
+    import numpy as np
+    import torch
+
+    import fornaxamr_b200 as fx
+    from fornaxamr_b200 import mesh, problems
+
+    dev = local_rank
+    torch.cuda.set_device(dev)
+    coord = (0.0, 1.0, 0.0, 1.0, 0.0, 1.0)
+    blocks = mesh.uniform_mesh((ROOT, ROOT, ROOT), coord)
+    W0, Bf0 = problems.fourier_mhd(blocks)
+    nb = len(blocks)
+    ctx = fx.Context(True, 5.0 / 3.0, coord, device=dev)
+    ctx.set_mesh(mesh.to_desc(blocks))
+    W0 = np.ascontiguousarray(W0)
+    Bf0 = np.ascontiguousarray(Bf0)
+    ctx.upload_all(W0, Bf0)
+    ctx.boundary_fill(1, 0)       # the driver's initial ghost fill (src/main.c:446)
+    ctx.sync()
+    cfl, dt_factor, t_end = 0.4, 1.2, 1.0e30
+    stream = torch.cuda.ExternalStream(ctx.stream(), device=dev)
+
+    def barrier():
+        if world > 1:
+            torch.distributed.barrier()
+
+    def max_over_ranks(x):
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{dev}")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        return float(t.item())
+
+    state = (0.0, 0.0, 0)
+    state = ctx.run(fx.FORM_BATCHED, args.warmup, cfl, dt_factor, t_end, state)
+    ctx.sync()
+    torch.cuda.synchronize(dev)
+    barrier()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    with Clocks(dev) as clk:
+        torch.cuda.synchronize(dev)
+        e0.record(stream)
+        state = ctx.run(fx.FORM_BATCHED, args.steps, cfl, dt_factor, t_end, state)
+        e1.record(stream)
+        e1.synchronize()
+        torch.cuda.synchronize(dev)
+    barrier()
+    ms_total = max_over_ranks(e0.elapsed_time(e1))
+    ms_step = ms_total / args.steps
+    value = world * ZONES * args.steps / (ms_total / 1000.0)
+    dt_fixed = state[1]
+
+    # plain (per-block launch) form, same state, same metric
+    ms_plain = None
+    if args.plain_steps > 0:
+        ctx.step(fx.FORM_PLAIN, dt_fixed, want_dt_src=False)
+        ctx.sync()
+        e0.record(stream)
+        for _ in range(args.plain_steps):
+            ctx.step(fx.FORM_PLAIN, dt_fixed, want_dt_src=False)
+        e1.record(stream)
+        e1.synchronize()
+        ms_plain = max_over_ranks(e0.elapsed_time(e1)) / args.plain_steps
+
+    # per-phase timings (batched sweeps; the face-flux launch dominates)
+    phases = {}
+    for name, ph in (("flux_launch", 0), ("emf", 1), ("ct", 2), ("cells", 3), ("ghost", 4)):
+        phases[name] = ctx.time_phase(ph, 5, dt_fixed)
+    ms_flux = phases["flux_launch"]
+
+    # end to end through the C ABI with host buffers
+    Wh = torch.empty(W0.size, dtype=torch.float64, pin_memory=True).numpy()
+    Bh = torch.empty(Bf0.size, dtype=torch.float64, pin_memory=True).numpy()
+    ctx.download_all(Wh, Bh)
+    L = ctx.L
+    dp = fx._dp
+    h2d = nb * (9 * fx.NCELLS + 3 * fx.NFACES) * 8
+    e2e_ms = None
+    if args.e2e_steps > 0:
+        torch.cuda.synchronize(dev)
+        e0.record(stream)
+        for _ in range(args.e2e_steps):
+            ctx._check(L.fx_upload_state(ctx._h, dp(Wh), dp(Bh)))
+            ctx.step(fx.FORM_BATCHED, dt_fixed, want_dt_src=False)
+            ctx._check(L.fx_download_state(ctx._h, dp(Wh), dp(Bh)))
+        e1.record(stream)
+        e1.synchronize()
+        ctx.sync()
+        e2e_ms = max_over_ranks(e0.elapsed_time(e1)) / args.e2e_steps
+
+    peak, peak_kind = measured_peak_hbm()
+    # algorithmic bytes of one face-flux launch (direction x, all blocks):
+    # per face: the 8 primitive inputs of the cells its stencil owns
+    # (20 x 18 x 18 cells per 17 x 18 x 18 faces) + the face field (8 B) +
+    # outputs flux 9, v_riemann 3, Bv1, Bv2 (14 doubles)
+    faces = nb * 17 * 18 * 18
+    flux_bytes = nb * 20 * 18 * 18 * 8 * 8 + faces * 8 + faces * 14 * 8
+    achieved = flux_bytes / (ms_flux * 1e-3) / 1e9
+    traffic = flux_traffic_per_launch()
+    launches_per_step = ctx.info(0) + 4
+    line = {
+        "metric": METRIC,
+        "value": value,
+        "unit": UNIT,
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": ms_step,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64",
+        "data": "synthetic (seeded Fourier-mode MHD, host-generated)",
+        "config": {
+            "workload": "3D ideal MHD 128^3, 512 blocks of 16^3 + 2 ghosts, gamma 5/3, 32 seeded modes k<=4, "
+                        "MC+HLLD+CT RK2, batched form (one CUDA graph per step)",
+            "blocks": nb, "zones": ZONES, "form": "batched", "l2": "working set 2.7 GB >> 126 MB L2 (no flush)",
+            "parallelism": f"replicas x{world}",
+        },
+        "hbm_gbs_step": ZONES * BYTES_PER_ZONE_STEP / (ms_step * 1e-3) / 1e9,
+        "plain": None if ms_plain is None else {
+            "ms_per_step": ms_plain, "value": world * ZONES / (ms_plain * 1e-3),
+            "batched_over_plain": ms_plain / ms_step},
+        "phases_ms": phases,
+        "roofline": {
+            "kernel": "k_flux (face fluxes, one direction, all blocks)",
+            "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+            "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
+            "note": "FP64 HLLD issue rate bounds this kernel before HBM (see DESIGN.md)",
+        },
+        "e2e": None if e2e_ms is None else {
+            "value": world * ZONES / (e2e_ms * 1e-3), "unit": UNIT,
+            "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": h2d},
+        "gpu_launches": launches_per_step * args.steps,
+        "clocks": clk.summary(),
+    }
+    ctx.close()
+    return line
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        if rank != 0:
+            return 0
+        t0 = time.time()
+        cb = cpu_reference(args.steps, args.warmup, args.cpu_seconds)
+        v = cb["value"]
+        line = {"metric": METRIC, "value": v, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": 1000.0 * ZONES / v, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                "data": "synthetic (seeded Fourier-mode MHD)",
+                "config": {"workload": "3D ideal MHD 128^3 recipe, reference CPU path (oracle/_ref)",
+                           "zones": ZONES},
+                "impl": "reference", "cpu_baseline": cb,
+                "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+                "wall_s": time.time() - t0}
+        print(json.dumps(line))
+        return 0
+
+    # CPU baseline first (spawned processes, before any GPU call)
+    cb = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            cb = cpu_reference(20, 1, args.cpu_seconds)
+        except Exception as exc:  # oracle missing on this machine
+            cb = {"value": None, "unit": UNIT, "cores": 0, "kind": "reference",
+                  "sample": f"unavailable: {exc}"}
+    if world > 1:
+        import datetime
+
+        import torch
+        torch.cuda.set_device(local_rank)
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    line = run_fx(args, rank, world, local_rank)
+    line["cpu_baseline"] = cb
+    if world > 1:
+        import torch
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line))
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,234 @@
+"""fornaxamr_b200: B200-native per-block Godunov MHD update of FornaxAMR.
+
+The compute path is the native library libfornax_b200.so (hand-written
+sm_100a CUDA behind the C ABI in include/fornax_b200.h).  This package is a
+thin host-side front-end: ctypes bindings, mesh descriptions and workload
+generators.  It never computes the update itself; without the native library
+the import fails.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from typing import Optional, Sequence
+
+import numpy as np
+
+from . import _lib
+from ._lib import (ARR_BF, ARR_BV1, ARR_BV2, ARR_EMF, ARR_EOSVAR, ARR_FLUX, ARR_GRAV, ARR_RHS,
+                   ARR_VRIEMANN, ARR_W, BC_OUTFLOW, BC_PERIODIC, BC_REFLECT, BC_USER, FORM_BATCHED,
+                   FORM_PLAIN, FxBlockDesc, FxConfig)
+
+__all__ = ["Context", "FxError", "FORM_PLAIN", "FORM_BATCHED", "NCELLS", "NFACES", "NEDGES",
+           "library", "plan_export"]
+
+NCELLS = 20 ** 3
+NFACES = 21 * 20 * 20
+NEDGES = 21 * 21 * 20
+NSTAGES = 2
+
+_L: Optional[C.CDLL] = None
+
+
+def library() -> C.CDLL:
+    global _L
+    if _L is None:
+        _L = _lib.load()
+    return _L
+
+
+class FxError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"fornax_b200 error {code}: {msg}")
+        self.code = code
+
+
+def _dp(a: np.ndarray):
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def make_config(mhd: bool, gamma: float, coord: Sequence[float], bc: Sequence[int] = (0,) * 6,
+                gravity: bool = False, mhd_eta: float = 0.0) -> FxConfig:
+    cfg = FxConfig()
+    cfg.mhd = 1 if mhd else 0
+    cfg.gravity = 1 if gravity else 0
+    cfg.gamma = float(gamma)
+    for n in range(6):
+        cfg.coord[n] = float(coord[n])
+        cfg.bc[n] = int(bc[n])
+    cfg.mhd_eta = float(mhd_eta)
+    return cfg
+
+
+def plan_export(cfg: FxConfig, desc, which: int):
+    """Host-only dump of a compiled program: (ops [n,4] int32, wave_begin)."""
+    L = library()
+    nops = C.c_int(0)
+    nwaves = C.c_int(0)
+    rc = L.fx_plan_export(C.byref(cfg), len(desc), desc, which, None, C.byref(nops), None, C.byref(nwaves))
+    if rc != 0:
+        raise FxError(rc, "fx_plan_export failed")
+    width = 4 if which <= 1 else 8
+    ops = np.zeros((max(nops.value, 1), width), dtype=np.int32)
+    waves = np.zeros(nwaves.value + 1, dtype=np.int32)
+    rc = L.fx_plan_export(C.byref(cfg), len(desc), desc, which,
+                          ops.ctypes.data_as(C.POINTER(C.c_int32)), C.byref(nops),
+                          waves.ctypes.data_as(C.POINTER(C.c_int32)), C.byref(nwaves))
+    if rc != 0:
+        raise FxError(rc, "fx_plan_export failed")
+    return ops[: nops.value], waves
+
+
+class Context:
+    """One device context (fx_ctx) with a mesh mirror."""
+
+    def __init__(self, mhd: bool, gamma: float, coord: Sequence[float], bc: Sequence[int] = (0,) * 6,
+                 gravity: bool = False, mhd_eta: float = 0.0, device: int = 0):
+        self.L = library()
+        self.mhd = bool(mhd)
+        self.nv = 9 if mhd else 6
+        self.cfg = make_config(mhd, gamma, coord, bc, gravity, mhd_eta)
+        self._h = C.c_void_p()
+        rc = self.L.fx_create(device, C.byref(self.cfg), C.byref(self._h))
+        if rc != 0:
+            raise FxError(rc, "fx_create failed (is a GPU present?)")
+        self.nblocks = 0
+
+    # -- plumbing ---------------------------------------------------------------
+    def _check(self, rc: int) -> None:
+        if rc != 0:
+            buf = C.create_string_buffer(512)
+            self.L.fx_last_error(self._h, buf, 512)
+            raise FxError(rc, buf.value.decode())
+
+    def close(self) -> None:
+        if self._h:
+            self.L.fx_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def sync(self) -> None:
+        self._check(self.L.fx_sync(self._h))
+
+    def stream(self) -> int:
+        p = C.c_void_p()
+        self._check(self.L.fx_stream(self._h, C.byref(p)))
+        return p.value or 0
+
+    # -- mesh and data ------------------------------------------------------------
+    def set_mesh(self, desc) -> None:
+        self._check(self.L.fx_set_mesh(self._h, len(desc), desc))
+        self.nblocks = len(desc)
+
+    def upload_block(self, b: int, W: np.ndarray, Bf=None, grav=None) -> None:
+        W = np.ascontiguousarray(W, dtype=np.float64)
+        keep = [W]
+        bfp = None
+        if Bf is not None:
+            arrs = [np.ascontiguousarray(x, dtype=np.float64) for x in Bf]
+            keep += arrs
+            bfp = (C.POINTER(C.c_double) * 3)(*[_dp(x) for x in arrs])
+        gp = None
+        if grav is not None:
+            arrs = [np.ascontiguousarray(x, dtype=np.float64) for x in grav]
+            keep += arrs
+            gp = (C.POINTER(C.c_double) * 3)(*[_dp(x) for x in arrs])
+        self._check(self.L.fx_upload_block(self._h, b, _dp(W), bfp, gp))
+
+    def download_block(self, b: int):
+        W = np.empty(self.nv * NSTAGES * NCELLS)
+        eos = np.empty(3 * NCELLS)
+        bfp = None
+        Bf = None
+        if self.mhd:
+            Bf = [np.empty(NSTAGES * NFACES) for _ in range(3)]
+            bfp = (C.POINTER(C.c_double) * 3)(*[_dp(x) for x in Bf])
+        self._check(self.L.fx_download_block(self._h, b, _dp(W), _dp(eos), bfp))
+        return W, eos, Bf
+
+    def upload_all(self, W_all: Optional[np.ndarray], Bf_all: Optional[np.ndarray]) -> None:
+        w = None if W_all is None else _dp(W_all)
+        f = None if Bf_all is None else _dp(Bf_all)
+        self._check(self.L.fx_upload_all(self._h, w, f))
+
+    def download_all(self, W_all: Optional[np.ndarray], Bf_all: Optional[np.ndarray]) -> None:
+        w = None if W_all is None else _dp(W_all)
+        f = None if Bf_all is None else _dp(Bf_all)
+        self._check(self.L.fx_download_all(self._h, w, f))
+
+    def download_array(self, b: int, which: int, dir_: int = 0) -> np.ndarray:
+        sizes = {ARR_W: self.nv * NSTAGES * NCELLS, ARR_EOSVAR: 3 * NCELLS, ARR_RHS: self.nv * NCELLS,
+                 ARR_FLUX: self.nv * NCELLS, ARR_VRIEMANN: 3 * NCELLS, ARR_GRAV: NCELLS,
+                 ARR_BF: NSTAGES * NFACES, ARR_BV1: NCELLS, ARR_BV2: NCELLS, ARR_EMF: NEDGES}
+        out = np.empty(sizes[which])
+        self._check(self.L.fx_download_array(self._h, b, which, dir_, _dp(out)))
+        return out
+
+    # -- reference entry points ----------------------------------------------------
+    def flux_update(self, b: int, w_slot: int, use_bf1: int) -> None:
+        self._check(self.L.fx_flux_update(self._h, b, w_slot, use_bf1))
+
+    def mhd_update_emf(self, b: int, stage: int) -> None:
+        self._check(self.L.fx_mhd_update_emf(self._h, b, stage))
+
+    def mhd_update_bf(self, b: int, stage: int, dt: float) -> None:
+        self._check(self.L.fx_mhd_update_bf(self._h, b, stage, dt))
+
+    def update_cells(self, b: int, stage: int, dt: float) -> float:
+        v = C.c_double(1.0e100)
+        self._check(self.L.fx_update_cells(self._h, b, stage, dt, C.byref(v)))
+        return v.value
+
+    def eos_fill_active_cells(self, stage: int) -> None:
+        self._check(self.L.fx_eos_fill_active_cells(self._h, stage))
+
+    def eos_fill_mesh(self, stage: int) -> None:
+        self._check(self.L.fx_eos_fill_mesh(self._h, stage))
+
+    def boundary_fill(self, stage: int, use_bf1: int) -> None:
+        self._check(self.L.fx_boundary_fill_ghosts_and_bf(self._h, stage, use_bf1))
+
+    def riemann_flux_send(self) -> None:
+        self._check(self.L.fx_riemann_flux_send(self._h))
+
+    def mhd_emf_send(self) -> None:
+        self._check(self.L.fx_mhd_emf_send(self._h))
+
+    # -- time integration -------------------------------------------------------------
+    def calc_dt(self, cfl: float) -> float:
+        v = C.c_double(0.0)
+        self._check(self.L.fx_calc_dt(self._h, cfl, C.byref(v)))
+        return v.value
+
+    def stage(self, form: int, stage: int, dt: float) -> float:
+        v = C.c_double(0.0)
+        self._check(self.L.fx_stage(self._h, form, stage, dt, C.byref(v)))
+        return v.value
+
+    def step(self, form: int, dt: float, want_dt_src: bool = True) -> Optional[float]:
+        if want_dt_src:
+            v = C.c_double(0.0)
+            self._check(self.L.fx_step(self._h, form, dt, C.byref(v)))
+            return v.value
+        self._check(self.L.fx_step(self._h, form, dt, None))
+        return None
+
+    def run(self, form: int, nsteps: int, cfl: float, dt_factor: float, t_end: float, state):
+        st = (C.c_double * 3)(*state)
+        self._check(self.L.fx_run(self._h, form, nsteps, cfl, dt_factor, t_end, st))
+        return st[0], st[1], int(st[2])
+
+    # -- measurement --------------------------------------------------------------------
+    def time_phase(self, phase: int, reps: int, dt: float = 0.0) -> float:
+        v = C.c_double(0.0)
+        self._check(self.L.fx_time_phase(self._h, phase, reps, dt, C.byref(v)))
+        return v.value
+
+    def info(self, what: int) -> int:
+        v = C.c_longlong(0)
+        self._check(self.L.fx_info(self._h, what, C.byref(v)))
+        return v.value

@@ -1,0 +1,112 @@
+"""ctypes bindings of libfornax_b200.so (declarations in include/fornax_b200.h).
+
+The library is loaded from the package directory; there is no fallback: if
+the native library is missing, importing this module raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libfornax_b200.so")
+
+FX_SUCCESS, FX_EINVAL, FX_ECUDA, FX_ENOMESH, FX_EPHYSICS, FX_ENOMEM = range(6)
+FORM_PLAIN, FORM_BATCHED = 0, 1
+BC_OUTFLOW, BC_REFLECT, BC_USER, BC_PERIODIC = 0, 1, 2, 3
+ARR_W, ARR_EOSVAR, ARR_RHS, ARR_FLUX, ARR_VRIEMANN, ARR_GRAV, ARR_BF, ARR_BV1, ARR_BV2, ARR_EMF = (
+    0, 1, 3, 4, 5, 6, 7, 8, 9, 10)
+
+
+class FxSlot(C.Structure):
+    _fields_ = [
+        ("id", C.c_int32),
+        ("rel_level", C.c_int32),
+        ("type", C.c_int32),
+        ("send_loc_start", C.c_int8 * 3),
+        ("send_loc_end", C.c_int8 * 3),
+        ("recv_loc_start", C.c_int8 * 3),
+        ("recv_loc_end", C.c_int8 * 3),
+    ]
+
+
+class FxBlockDesc(C.Structure):
+    _fields_ = [
+        ("id", C.c_int32),
+        ("level", C.c_int32),
+        ("active", C.c_int32),
+        ("rank", C.c_int32),
+        ("xmin", C.c_double * 3),
+        ("xmax", C.c_double * 3),
+        ("dx", C.c_double * 3),
+        ("vol", C.c_double),
+        ("area", C.c_double * 3),
+        ("slot", FxSlot * 56),
+    ]
+
+
+class FxConfig(C.Structure):
+    _fields_ = [
+        ("mhd", C.c_int32),
+        ("gravity", C.c_int32),
+        ("gamma", C.c_double),
+        ("coord", C.c_double * 6),
+        ("bc", C.c_int32 * 6),
+        ("mhd_eta", C.c_double),
+    ]
+
+
+# every entry point declared in include/fornax_b200.h
+EXPORTS = [
+    "fx_create", "fx_destroy", "fx_last_error", "fx_sync", "fx_stream", "fx_set_mesh",
+    "fx_upload_block", "fx_download_block", "fx_upload_all", "fx_download_all",
+    "fx_download_array", "fx_flux_update", "fx_mhd_update_emf", "fx_mhd_update_bf",
+    "fx_update_cells", "fx_riemann_flux_send", "fx_mhd_emf_send", "fx_eos_fill_active_cells",
+    "fx_eos_fill_mesh", "fx_boundary_fill_ghosts_and_bf", "fx_calc_dt", "fx_stage", "fx_step",
+    "fx_run", "fx_plan_export", "fx_time_phase", "fx_info", "fx_upload_state", "fx_download_state",
+]
+PHASE_FLUX, PHASE_EMF, PHASE_CT, PHASE_CELLS, PHASE_GHOST, PHASE_STEP = range(6)
+
+
+def load() -> C.CDLL:
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(
+            f"{LIB_PATH} is missing: build it with `python -m fornaxamr_b200.build` "
+            "(the package has no CPU fallback)")
+    L = C.CDLL(LIB_PATH, mode=C.RTLD_LOCAL)
+    vp = C.c_void_p
+    dp = C.POINTER(C.c_double)
+    ip = C.POINTER(C.c_int32)
+    dpp3 = C.POINTER(dp)
+    L.fx_create.argtypes = [C.c_int, C.POINTER(FxConfig), C.POINTER(vp)]
+    L.fx_destroy.argtypes = [vp]
+    L.fx_destroy.restype = None
+    L.fx_last_error.argtypes = [vp, C.c_char_p, C.c_size_t]
+    L.fx_sync.argtypes = [vp]
+    L.fx_stream.argtypes = [vp, C.POINTER(vp)]
+    L.fx_set_mesh.argtypes = [vp, C.c_int, C.POINTER(FxBlockDesc)]
+    L.fx_upload_block.argtypes = [vp, C.c_int, dp, dpp3, dpp3]
+    L.fx_download_block.argtypes = [vp, C.c_int, dp, dp, dpp3]
+    L.fx_upload_all.argtypes = [vp, dp, dp]
+    L.fx_download_all.argtypes = [vp, dp, dp]
+    L.fx_upload_state.argtypes = [vp, dp, dp]
+    L.fx_download_state.argtypes = [vp, dp, dp]
+    L.fx_download_array.argtypes = [vp, C.c_int, C.c_int, C.c_int, dp]
+    L.fx_flux_update.argtypes = [vp, C.c_int, C.c_int, C.c_int]
+    L.fx_mhd_update_emf.argtypes = [vp, C.c_int, C.c_int]
+    L.fx_mhd_update_bf.argtypes = [vp, C.c_int, C.c_int, C.c_double]
+    L.fx_update_cells.argtypes = [vp, C.c_int, C.c_int, C.c_double, dp]
+    L.fx_riemann_flux_send.argtypes = [vp]
+    L.fx_mhd_emf_send.argtypes = [vp]
+    L.fx_eos_fill_active_cells.argtypes = [vp, C.c_int]
+    L.fx_eos_fill_mesh.argtypes = [vp, C.c_int]
+    L.fx_boundary_fill_ghosts_and_bf.argtypes = [vp, C.c_int, C.c_int]
+    L.fx_calc_dt.argtypes = [vp, C.c_double, dp]
+    L.fx_stage.argtypes = [vp, C.c_int, C.c_int, C.c_double, dp]
+    L.fx_step.argtypes = [vp, C.c_int, C.c_double, dp]
+    L.fx_run.argtypes = [vp, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double, dp]
+    L.fx_plan_export.argtypes = [C.POINTER(FxConfig), C.c_int, C.POINTER(FxBlockDesc), C.c_int,
+                                 ip, C.POINTER(C.c_int), ip, C.POINTER(C.c_int)]
+    L.fx_time_phase.argtypes = [vp, C.c_int, C.c_int, C.c_double, dp]
+    L.fx_info.argtypes = [vp, C.c_int, C.POINTER(C.c_longlong)]
+    return L

@@ -1,0 +1,916 @@
+/*
+ * Per-phase kernels of the RK2 Godunov MHD update, one thread per face, edge
+ * or cell.  Every kernel takes a block list: the plain (drop-in) form passes
+ * one block per launch, as the reference's per-block loops do; the batched
+ * form passes every block of the mesh in one launch.
+ *
+ * Phase                       reference
+ * face fluxes (k_flux)        prj_flux_update, src/prj_flux.c:2149-2521
+ * edge EMFs (k_emf)           prj_timeint_mhd_update_emf, src/prj_timeint.c:292-413
+ * CT face update (k_bf_update) prj_timeint_mhd_update_bf, src/prj_timeint.c:415-495
+ * cell update (k_cell_update) src/prj_timeint.c:1255-1349 and 1562-1654,
+ *                             src terms src/prj_src.c:32-139, 717-768
+ * eos fill (k_eos_fill)       prj_eos_fill_block/_active_cells, src/prj_eos.c:1087-1162
+ * dt (k_calc_dt)              prj_timeint_calc_dt, src/prj_timeint.c:2144-2256
+ * ghost programs              prj_boundary_fill_ghosts_and_bf, src/prj_boundary.c:1150-1241
+ * bf2bc (k_bf2bc)             prj_mhd_bf2bc_impl, src/prj_mhd.c:555-603
+ */
+#include <cuda_runtime.h>
+
+#include "fx_kernels.h"
+#include "fx_physics.cuh"
+
+namespace {
+
+constexpr int kPlane = FX_NSTAGES * FX_NCELLS; /* stride between variables of W */
+
+__device__ __forceinline__ int fx_axis_stride(int dir)
+{
+    return dir == 0 ? FX_PBS * FX_PBS : dir == 1 ? FX_PBS : 1;
+}
+
+/* local (sweep-rotated) variable -> global variable, prj_flux_build_var_map
+ * (src/prj_flux.c:274-349): the sweep-normal velocity and field go to slot 1
+ * and 6 of the local vector. */
+__device__ __forceinline__ int fx_gmap(int dir, int lv)
+{
+    if (lv >= 1 && lv <= 3) {
+        return 1 + (dir + lv - 1) % 3;
+    }
+    if (lv >= 6) {
+        return 6 + (dir + lv - 6) % 3;
+    }
+    return lv;
+}
+
+__device__ __forceinline__ unsigned long long fx_double_key(double d)
+{
+    unsigned long long bits = (unsigned long long)__double_as_longlong(d);
+    return (bits >> 63) ? ~bits : (bits | 0x8000000000000000ULL);
+}
+
+/* ------------------------------------------------------------------------ */
+/* Face fluxes                                                               */
+/* ------------------------------------------------------------------------ */
+template <bool MHD>
+__global__ void __launch_bounds__(128) k_flux(FxDev D, const int *__restrict__ blist, int dir,
+    int wslot, int bfslot, int full)
+{
+    if (D.ctl->skip) {
+        return;
+    }
+    const int b = blist[blockIdx.y];
+    /* MHD carries one transverse ghost layer of faces for the CT EMFs
+     * (src/prj_flux.c:2241-2251); hydro transverse faces are [0, 15]. */
+    constexpr int T = MHD ? FX_BS + 2 : FX_BS;
+    constexpr int TLO = MHD ? -1 : 0;
+    constexpr int NF = (FX_BS + 1) * T * T;
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= NF) {
+        return;
+    }
+    const int e2 = dir == 2 ? FX_BS + 1 : T;
+    const int e1 = dir == 1 ? FX_BS + 1 : T;
+    const int k = (dir == 2 ? 0 : TLO) + t % e2;
+    t /= e2;
+    const int j = (dir == 1 ? 0 : TLO) + t % e1;
+    const int i = (dir == 0 ? 0 : TLO) + t / e1;
+    const int s = fx_axis_stride(dir);
+    const int cR = fx_lidx(i, j, k);
+    const int cL = cR - s;
+    const int nv = MHD ? 9 : 6;
+    const double *Wb = D.W + (size_t)b * FX_W_COUNT(nv) + (size_t)wslot * FX_NCELLS;
+    const double g = D.gamma;
+
+    double WL[9];
+    double WR[9];
+    /* density and internal energy at the four cells of the stencil also give
+     * the reconstructed pressure (eosvar p = (g-1) rho e of each cell). */
+    double rho4[4], eint4[4];
+    {
+        const double *q = Wb + (size_t)FX_RHO * kPlane;
+        rho4[0] = q[cL - s]; rho4[1] = q[cL]; rho4[2] = q[cR]; rho4[3] = q[cR + s];
+        q = Wb + (size_t)FX_EINT * kPlane;
+        eint4[0] = q[cL - s]; eint4[1] = q[cL]; eint4[2] = q[cR]; eint4[3] = q[cR + s];
+    }
+    WL[FX_RHO] = rho4[1] + 0.5 * fx_mc_slope(rho4[0], rho4[1], rho4[2]);
+    WR[FX_RHO] = rho4[2] - 0.5 * fx_mc_slope(rho4[1], rho4[2], rho4[3]);
+    WL[FX_EINT] = eint4[1] + 0.5 * fx_mc_slope(eint4[0], eint4[1], eint4[2]);
+    WR[FX_EINT] = eint4[2] - 0.5 * fx_mc_slope(eint4[1], eint4[2], eint4[3]);
+#pragma unroll
+    for (int lv = 1; lv < nv; ++lv) {
+        if (lv == FX_EINT || (MHD && lv == FX_B1)) {
+            continue;
+        }
+        const double *q = Wb + (size_t)fx_gmap(dir, lv) * kPlane;
+        const double qm = q[cL - s];
+        const double q0 = q[cL];
+        const double q1 = q[cR];
+        const double q2 = q[cR + s];
+        WL[lv] = q0 + 0.5 * fx_mc_slope(qm, q0, q1);
+        WR[lv] = q1 - 0.5 * fx_mc_slope(q0, q1, q2);
+    }
+    double p4[4];
+#pragma unroll
+    for (int n = 0; n < 4; ++n) {
+        p4[n] = fx_pressure(g, rho4[n], eint4[n]);
+    }
+    const double pL = p4[1] + 0.5 * fx_mc_slope(p4[0], p4[1], p4[2]);
+    const double pR = p4[2] - 0.5 * fx_mc_slope(p4[1], p4[2], p4[3]);
+    /* gamma is uniform for the ideal gas: its MC slope is exactly 0, so the
+     * reconstructed face values equal g bit for bit. */
+    const double gL = g;
+    const double gR = g;
+
+    const size_t fbase = (size_t)b * FX_FLUX_COUNT(nv) + (size_t)dir * nv * FX_NCELLS;
+    const size_t vbase = (size_t)b * FX_VR_COUNT + (size_t)dir * 3 * FX_NCELLS;
+    if (MHD) {
+        const double bn = D.Bf[(size_t)b * FX_BF_COUNT + ((size_t)dir * FX_NSTAGES + bfslot) * FX_NFACES +
+            fx_face_idx(dir, i, j, k)];
+        WL[FX_B1] = bn;
+        WR[FX_B1] = bn;
+        FxFaceOut o;
+        fx_riemann_hlld(WL, WR, pL, pR, gL, gR, bn, o, D.err, b, cR);
+#pragma unroll
+        for (int lv = 0; lv < 9; ++lv) {
+            D.flux[fbase + fx_bidx(9, fx_gmap(dir, lv), i, j, k)] = o.F[lv];
+        }
+#pragma unroll
+        for (int m = 0; m < 3; ++m) {
+            D.vr[vbase + fx_bidx(3, (dir + m) % 3, i, j, k)] = o.v[m];
+        }
+        const size_t bvi = (size_t)b * FX_BV_COUNT + (size_t)dir * FX_NCELLS + cR;
+        D.bv1[bvi] = o.bv1;
+        D.bv2[bvi] = o.bv2;
+    } else {
+        /* transverse velocity deltas of the theta limiter,
+         * prj_flux_velocity_deltas (src/prj_flux.c:1967-2036) */
+        const int da = (dir + 1) % 3;
+        const int db = (dir + 2) % 3;
+        const int sa = fx_axis_stride(da);
+        const int sb = fx_axis_stride(db);
+        const double *un = Wb + (size_t)(1 + dir) * kPlane;
+        const double *ua = Wb + (size_t)(1 + da) * kPlane;
+        const double *ub = Wb + (size_t)(1 + db) * kPlane;
+        const double du = un[cR] - un[cL];
+        const double dv = fx_min(fx_min(ua[cL] - ua[cL - sa], ua[cL + sa] - ua[cL]),
+            fx_min(ua[cR] - ua[cR - sa], ua[cR + sa] - ua[cR]));
+        const double dw = fx_min(fx_min(ub[cL] - ub[cL - sb], ub[cL + sb] - ub[cL]),
+            fx_min(ub[cR] - ub[cR - sb], ub[cR + sb] - ub[cR]));
+        double F[6];
+        double v[3];
+        fx_riemann_hllc(WL, WR, pL, pR, gL, gR, du, dv, dw, F, v);
+#pragma unroll
+        for (int lv = 0; lv < 6; ++lv) {
+            D.flux[fbase + fx_bidx(6, fx_gmap(dir, lv), i, j, k)] = F[lv];
+        }
+#pragma unroll
+        for (int m = 0; m < 3; ++m) {
+            D.vr[vbase + fx_bidx(3, (dir + m) % 3, i, j, k)] = v[m];
+        }
+    }
+    (void)full;
+}
+
+/* ------------------------------------------------------------------------ */
+/* Edge EMFs                                                                 */
+/* ------------------------------------------------------------------------ */
+__device__ __forceinline__ double fx_cell_emf(const double *Wb, int dir, int c)
+{
+    const int a = (dir + 1) % 3;
+    const int bb = (dir + 2) % 3;
+    const double bA = Wb[(size_t)(FX_B1 + a) * kPlane + c];
+    const double bB = Wb[(size_t)(FX_B1 + bb) * kPlane + c];
+    const double vA = Wb[(size_t)(FX_V1 + a) * kPlane + c];
+    const double vB = Wb[(size_t)(FX_V1 + bb) * kPlane + c];
+    return bA * vB - bB * vA;
+}
+
+__global__ void __launch_bounds__(128) k_emf(FxDev D, const int *__restrict__ blist, int wslot, int bfslot)
+{
+    if (D.ctl->skip) {
+        return;
+    }
+    const int b = blist[blockIdx.y];
+    constexpr int NE = FX_BS * (FX_BS + 1) * (FX_BS + 1);
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= 3 * NE) {
+        return;
+    }
+    const int dir = t / NE;
+    t -= dir * NE;
+    const int x2 = dir == 2 ? FX_BS : FX_BS + 1;
+    const int x1 = dir == 1 ? FX_BS : FX_BS + 1;
+    int e[3];
+    e[2] = t % x2;
+    t /= x2;
+    e[1] = t % x1;
+    e[0] = t / x1;
+    const int up = (dir + 1) % 3;
+    const int right = (dir + 2) % 3;
+    const int su = fx_axis_stride(up);
+    const int sr = fx_axis_stride(right);
+    const int c0 = fx_lidx(e[0], e[1], e[2]);   /* cell0 = e; face0 = face1 = e */
+    const int c1 = c0 - su;                      /* cell1 = e - up */
+    const int c2 = c0 - su - sr;                 /* cell2 = e - up - right */
+    const int c3 = c0 - sr;                      /* cell3 = e - right */
+    const double *Wb = D.W + (size_t)b * FX_W_COUNT(9) + (size_t)wslot * FX_NCELLS;
+    const double *bv1r = D.bv1 + (size_t)b * FX_BV_COUNT + (size_t)right * FX_NCELLS;
+    const double *bv2u = D.bv2 + (size_t)b * FX_BV_COUNT + (size_t)up * FX_NCELLS;
+    const double *vrr = D.vr + (size_t)b * FX_VR_COUNT + (size_t)right * 3 * FX_NCELLS;
+    const double *vru = D.vr + (size_t)b * FX_VR_COUNT + (size_t)up * 3 * FX_NCELLS;
+    double f[4], c[4], vn[4];
+    /* face0 = e (right-normal), face1 = e (up-normal), face2 = e - up
+     * (right-normal), face3 = e - right (up-normal) */
+    f[0] = bv1r[c0];
+    f[1] = bv2u[c0];
+    f[2] = bv1r[c1];
+    f[3] = bv2u[c3];
+    c[0] = fx_cell_emf(Wb, dir, c0);
+    c[1] = fx_cell_emf(Wb, dir, c1);
+    c[2] = fx_cell_emf(Wb, dir, c2);
+    c[3] = fx_cell_emf(Wb, dir, c3);
+    vn[0] = vrr[fx_bidx_cell(3, right, c0)];
+    vn[1] = vru[fx_bidx_cell(3, up, c0)];
+    vn[2] = vrr[fx_bidx_cell(3, right, c1)];
+    vn[3] = vru[fx_bidx_cell(3, up, c3)];
+    const int eidx = fx_edge_idx(dir, e[0], e[1], e[2]);
+    for (int n = 0; n < 4; ++n) {
+        if (!isfinite(f[n]) || !isfinite(c[n]) || !isfinite(vn[n])) {
+            fx_fail(D.err, FX_ERR_EMF_NONFINITE, b, eidx);
+        }
+    }
+    /* edge resistivity: run-time eta plus the maximum artificial eta of the
+     * four incident cells (src/prj_timeint.c:265-290) */
+    double eta_cells = 0.0;
+    {
+        const int cells[4] = {c0, c1, c2, c3};
+        for (int n = 0; n < 4; ++n) {
+            const double ce = fx_cell_eta(Wb[(size_t)FX_RHO * kPlane + cells[n]],
+                Wb[(size_t)FX_YE * kPlane + cells[n]]);
+            if (!isfinite(ce) || ce < 0.0) {
+                fx_fail(D.err, FX_ERR_ETA, b, eidx);
+            }
+            if (ce > eta_cells) {
+                eta_cells = ce;
+            }
+        }
+    }
+    const double eta = D.mhd_eta + eta_cells;
+    double emf = fx_emf_upwind(f, c, vn);
+    if (eta != 0.0) {
+        /* resistive term, src/prj_mhd.c:682-709 */
+        const double *bf = D.Bf + (size_t)b * FX_BF_COUNT;
+        const double *b1 = bf + (size_t)(0 * FX_NSTAGES + bfslot) * FX_NFACES;
+        const double *b2 = bf + (size_t)(1 * FX_NSTAGES + bfslot) * FX_NFACES;
+        const double *b3 = bf + (size_t)(2 * FX_NSTAGES + bfslot) * FX_NFACES;
+        const FxBlockDev &B = D.blk[b];
+        const int i = e[0], j = e[1], k = e[2];
+        double curl_b;
+        if (dir == 0) {
+            curl_b = (b3[fx_face_idx(2, i, j, k)] - b3[fx_face_idx(2, i, j - 1, k)]) / B.dx[1] -
+                (b2[fx_face_idx(1, i, j, k)] - b2[fx_face_idx(1, i, j, k - 1)]) / B.dx[2];
+        } else if (dir == 1) {
+            curl_b = (b1[fx_face_idx(0, i, j, k)] - b1[fx_face_idx(0, i, j, k - 1)]) / B.dx[2] -
+                (b3[fx_face_idx(2, i, j, k)] - b3[fx_face_idx(2, i - 1, j, k)]) / B.dx[0];
+        } else {
+            curl_b = (b2[fx_face_idx(1, i, j, k)] - b2[fx_face_idx(1, i - 1, j, k)]) / B.dx[0] -
+                (b1[fx_face_idx(0, i, j, k)] - b1[fx_face_idx(0, i, j - 1, k)]) / B.dx[1];
+        }
+        emf += eta * curl_b;
+    }
+    if (!isfinite(emf)) {
+        fx_fail(D.err, FX_ERR_EMF_NONFINITE, b, eidx);
+    }
+    D.emf[(size_t)b * FX_EMF_COUNT + (size_t)dir * FX_NEDGES + eidx] = emf;
+}
+
+/* ------------------------------------------------------------------------ */
+/* CT face update                                                            */
+/* ------------------------------------------------------------------------ */
+__global__ void __launch_bounds__(128) k_bf_update(FxDev D, const int *__restrict__ blist, int stage)
+{
+    if (D.ctl->skip) {
+        return;
+    }
+    const double dt = D.ctl->dt;
+    const int b = blist[blockIdx.y];
+    constexpr int NF = (FX_BS + 1) * FX_BS * FX_BS;
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= 3 * NF) {
+        return;
+    }
+    const int dir = t / NF;
+    t -= dir * NF;
+    const int x2 = dir == 2 ? FX_BS + 1 : FX_BS;
+    const int x1 = dir == 1 ? FX_BS + 1 : FX_BS;
+    const int k = t % x2;
+    t /= x2;
+    const int j = t % x1;
+    const int i = t / x1;
+    const int src_slot = stage == 1 ? 0 : 1;
+    const int dst_slot = stage == 1 ? 1 : 0;
+    double *bf = D.Bf + (size_t)b * FX_BF_COUNT;
+    const double *e = D.emf + (size_t)b * FX_EMF_COUNT;
+    const double *e1 = e;
+    const double *e2 = e + FX_NEDGES;
+    const double *e3 = e + 2 * FX_NEDGES;
+    const FxBlockDev &B = D.blk[b];
+    const int f = fx_face_idx(dir, i, j, k);
+    double value = bf[((size_t)dir * FX_NSTAGES + src_slot) * FX_NFACES + f];
+    if (dir == 0) {
+        value += -dt * (e3[fx_edge_idx(2, i, j + 1, k)] - e3[fx_edge_idx(2, i, j, k)]) / B.dx[1];
+        value += dt * (e2[fx_edge_idx(1, i, j, k + 1)] - e2[fx_edge_idx(1, i, j, k)]) / B.dx[2];
+    } else if (dir == 1) {
+        value += -dt * (e1[fx_edge_idx(0, i, j, k + 1)] - e1[fx_edge_idx(0, i, j, k)]) / B.dx[2];
+        value += dt * (e3[fx_edge_idx(2, i + 1, j, k)] - e3[fx_edge_idx(2, i, j, k)]) / B.dx[0];
+    } else {
+        value += -dt * (e2[fx_edge_idx(1, i + 1, j, k)] - e2[fx_edge_idx(1, i, j, k)]) / B.dx[0];
+        value += dt * (e1[fx_edge_idx(0, i, j + 1, k)] - e1[fx_edge_idx(0, i, j, k)]) / B.dx[1];
+    }
+    if (!isfinite(value)) {
+        fx_fail(D.err, FX_ERR_BF_NONFINITE, b, f);
+    }
+    if (stage == 2) {
+        value = 0.5 * bf[((size_t)dir * FX_NSTAGES + 0) * FX_NFACES + f] + 0.5 * value;
+    }
+    bf[((size_t)dir * FX_NSTAGES + dst_slot) * FX_NFACES + f] = value;
+}
+
+/* ------------------------------------------------------------------------ */
+/* Cell update (flux divergence + sources + RK2 combine + cons2prim)         */
+/* ------------------------------------------------------------------------ */
+template <bool MHD, int STAGE>
+__global__ void __launch_bounds__(128) k_cell_update(FxDev D, const int *__restrict__ blist,
+    int gravity, int store_rhs)
+{
+    if (D.ctl->skip) {
+        return;
+    }
+    const double dt = D.ctl->dt;
+    const int b = blist[blockIdx.y];
+    constexpr int nv = MHD ? 9 : 6;
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= FX_BS * FX_BS * FX_BS) {
+        return;
+    }
+    const int k = t % FX_BS;
+    const int j = (t / FX_BS) % FX_BS;
+    const int i = t / (FX_BS * FX_BS);
+    const int c = fx_lidx(i, j, k);
+    const FxBlockDev &B = D.blk[b];
+    const double *W = D.W + (size_t)b * FX_W_COUNT(nv);
+    const double *fx = D.flux + (size_t)b * FX_FLUX_COUNT(nv);
+    const double *fy = fx + (size_t)nv * FX_NCELLS;
+    const double *fz = fy + (size_t)nv * FX_NCELLS;
+
+    /* prj_flux_div, src/prj_flux.c:2523-2533 (hydro components; the B
+     * components are replaced by the face average below) */
+    double fluxdiv[6];
+#pragma unroll
+    for (int v = 0; v < 6; ++v) {
+        fluxdiv[v] = -(B.area[0] * (fx[fx_bidx(nv, v, i + 1, j, k)] - fx[fx_bidx(nv, v, i, j, k)]) +
+            B.area[1] * (fy[fx_bidx(nv, v, i, j + 1, k)] - fy[fx_bidx(nv, v, i, j, k)]) +
+            B.area[2] * (fz[fx_bidx(nv, v, i, j, k + 1)] - fz[fx_bidx(nv, v, i, j, k)])) / B.vol;
+    }
+
+    double w[9];
+    double u[9];
+#pragma unroll
+    for (int v = 0; v < nv; ++v) {
+        w[v] = W[(size_t)v * kPlane + c];
+    }
+    fx_prim2cons<MHD>(w, u);
+
+    /* source terms: rhs = 0, then the static-gravity terms of
+     * prj_src_monopole_gravity with the stage primitives (src/prj_src.c:32-139) */
+    double rhs[6];
+#pragma unroll
+    for (int v = 0; v < 6; ++v) {
+        rhs[v] = 0.0;
+    }
+    if (gravity) {
+        const double *Ws = W + (size_t)(STAGE == 1 ? 0 : 1) * FX_NCELLS;
+        const double *g = D.grav + (size_t)b * FX_GRAV_COUNT;
+        const double g1 = g[c];
+        const double g2 = g[FX_NCELLS + c];
+        const double g3 = g[2 * FX_NCELLS + c];
+        const double rho = Ws[(size_t)FX_RHO * kPlane + c];
+        const double *vr = D.vr + (size_t)b * FX_VR_COUNT;
+        rhs[FX_V1] += rho * g1;
+        rhs[FX_V2] += rho * g2;
+        rhs[FX_V3] += rho * g3;
+        const double v_avg1 = (vr[fx_bidx(3, 0, i, j, k)] + vr[fx_bidx(3, 0, i + 1, j, k)]) * 0.5;
+        const double v_avg2 = (vr[3 * FX_NCELLS + fx_bidx(3, 1, i, j, k)] +
+            vr[3 * FX_NCELLS + fx_bidx(3, 1, i, j + 1, k)]) * 0.5;
+        const double v_avg3 = (vr[6 * FX_NCELLS + fx_bidx(3, 2, i, j, k)] +
+            vr[6 * FX_NCELLS + fx_bidx(3, 2, i, j, k + 1)]) * 0.5;
+        rhs[FX_ETOT] += rho * (v_avg1 * g1 + v_avg2 * g2 + v_avg3 * g3);
+    }
+    if (store_rhs) {
+        double *r = D.rhs + (size_t)b * FX_RHS_COUNT(nv);
+#pragma unroll
+        for (int v = 0; v < nv; ++v) {
+            r[fx_bidx(nv, v, i, j, k)] = v < 6 ? rhs[v] : 0.0;
+        }
+    }
+
+    /* dt_src from the start-of-step total energy,
+     * prj_timeint_update_dt_src_values (src/prj_timeint.c:533-565) */
+    const double dt_src = 0.02 * u[FX_ETOT] / (fabs(rhs[FX_ETOT]) + 1.0e-50);
+
+    double un[9];
+    if (STAGE == 1) {
+#pragma unroll
+        for (int v = 0; v < 6; ++v) {
+            un[v] = u[v] + dt * (rhs[v] + fluxdiv[v]);
+        }
+    } else {
+        double w1[9];
+        double u1[9];
+        const double *W1 = W + FX_NCELLS;
+#pragma unroll
+        for (int v = 0; v < nv; ++v) {
+            w1[v] = W1[(size_t)v * kPlane + c];
+        }
+        fx_prim2cons<MHD>(w1, u1);
+#pragma unroll
+        for (int v = 0; v < 6; ++v) {
+            const double u_trial = u1[v] + dt * (rhs[v] + fluxdiv[v]);
+            un[v] = 0.5 * u[v] + 0.5 * u_trial;
+        }
+    }
+    if (MHD) {
+        /* cell B from the updated faces, src/prj_timeint.c:498-510 */
+        const int bslot = STAGE == 1 ? 1 : 0;
+        const double *bf = D.Bf + (size_t)b * FX_BF_COUNT;
+        const double *b1 = bf + (size_t)(0 * FX_NSTAGES + bslot) * FX_NFACES;
+        const double *b2 = bf + (size_t)(1 * FX_NSTAGES + bslot) * FX_NFACES;
+        const double *b3 = bf + (size_t)(2 * FX_NSTAGES + bslot) * FX_NFACES;
+        un[FX_B1] = 0.5 * (b1[fx_face_idx(0, i, j, k)] + b1[fx_face_idx(0, i + 1, j, k)]);
+        un[FX_B2] = 0.5 * (b2[fx_face_idx(1, i, j, k)] + b2[fx_face_idx(1, i, j + 1, k)]);
+        un[FX_B3] = 0.5 * (b3[fx_face_idx(2, i, j, k)] + b3[fx_face_idx(2, i, j, k + 1)]);
+        if (!isfinite(un[FX_B1]) || !isfinite(un[FX_B2]) || !isfinite(un[FX_B3])) {
+            fx_fail(D.err, FX_ERR_B_NONFINITE, b, c);
+        }
+    }
+    double wn[9];
+    fx_cons2prim<MHD>(un, wn);
+    double *Wd = D.W + (size_t)b * FX_W_COUNT(nv) + (size_t)(STAGE == 1 ? 1 : 0) * FX_NCELLS;
+#pragma unroll
+    for (int v = 0; v < nv; ++v) {
+        Wd[(size_t)v * kPlane + c] = wn[v];
+    }
+
+    /* block-wide minimum of dt_src, then one atomic per CTA */
+    __shared__ unsigned long long smin[4];
+    unsigned long long key = fx_double_key(dt_src);
+    if (dt_src != dt_src) {
+        key = ~0ULL;
+    }
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+        const unsigned long long o = __shfl_down_sync(0xffffffffu, key, off);
+        key = o < key ? o : key;
+    }
+    if ((threadIdx.x & 31) == 0) {
+        smin[threadIdx.x >> 5] = key;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned long long m = smin[0];
+        for (int q = 1; q < (int)(blockDim.x >> 5); ++q) {
+            m = smin[q] < m ? smin[q] : m;
+        }
+        atomicMin(&D.red[1], m);
+    }
+}
+
+/* ------------------------------------------------------------------------ */
+/* EOS fill (eosvar = p, T, gamma from the stage primitives)                 */
+/* ------------------------------------------------------------------------ */
+__global__ void k_eos_fill(FxDev D, const int *__restrict__ blist, int wslot, int active_only)
+{
+    if (D.ctl->skip) {
+        return;
+    }
+    const int b = blist[blockIdx.y];
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    int i, j, k;
+    if (active_only) {
+        if (t >= FX_BS * FX_BS * FX_BS) return;
+        k = t % FX_BS;
+        j = (t / FX_BS) % FX_BS;
+        i = t / (FX_BS * FX_BS);
+    } else {
+        if (t >= FX_NCELLS) return;
+        k = t % FX_PBS - FX_NG;
+        j = (t / FX_PBS) % FX_PBS - FX_NG;
+        i = t / (FX_PBS * FX_PBS) - FX_NG;
+    }
+    const int c = fx_lidx(i, j, k);
+    const double *W = D.W + (size_t)b * FX_W_COUNT(D.nv) + (size_t)wslot * FX_NCELLS;
+    const double rho = W[(size_t)FX_RHO * kPlane + c];
+    const double eint = W[(size_t)FX_EINT * kPlane + c];
+    if (rho == 0.0) {
+        fx_fail(D.err, FX_ERR_EOS_ZERO_RHO, b, c);
+    }
+    const double g = D.gamma;
+    double *e = D.eos + (size_t)b * FX_EOS_COUNT;
+    e[fx_bidx(3, FX_EOS_P, i, j, k)] = fx_pressure(g, rho, eint);
+    e[fx_bidx(3, FX_EOS_T, i, j, k)] = fx_temperature(g, eint);
+    e[fx_bidx(3, FX_EOS_G, i, j, k)] = g;
+}
+
+/* ------------------------------------------------------------------------ */
+/* dt = min over active cells of cfl / sum_d (|v_d| + c_s) / dx_d            */
+/* ------------------------------------------------------------------------ */
+__global__ void __launch_bounds__(256) k_calc_dt(FxDev D, const int *__restrict__ blist, int wslot, double cfl)
+{
+    const int b = blist[blockIdx.y];
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    unsigned long long key = ~0ULL;
+    if (t < FX_BS * FX_BS * FX_BS) {
+        const int k = t % FX_BS;
+        const int j = (t / FX_BS) % FX_BS;
+        const int i = t / (FX_BS * FX_BS);
+        const int c = fx_lidx(i, j, k);
+        const double *W = D.W + (size_t)b * FX_W_COUNT(D.nv) + (size_t)wslot * FX_NCELLS;
+        const FxBlockDev &B = D.blk[b];
+        const double g = D.gamma;
+        const double rho = W[(size_t)FX_RHO * kPlane + c];
+        const double p = fx_pressure(g, rho, W[(size_t)FX_EINT * kPlane + c]);
+        const double cs = sqrt(g * p / rho);
+        const double denom = (fabs(W[(size_t)FX_V1 * kPlane + c]) + cs) / B.dx[0] +
+            (fabs(W[(size_t)FX_V2 * kPlane + c]) + cs) / B.dx[1] +
+            (fabs(W[(size_t)FX_V3 * kPlane + c]) + cs) / B.dx[2];
+        const double dt_cell = cfl / denom;
+        if (dt_cell == dt_cell) {
+            key = fx_double_key(dt_cell);
+        }
+    }
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+        const unsigned long long o = __shfl_down_sync(0xffffffffu, key, off);
+        key = o < key ? o : key;
+    }
+    __shared__ unsigned long long smin[8];
+    if ((threadIdx.x & 31) == 0) {
+        smin[threadIdx.x >> 5] = key;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned long long m = smin[0];
+        for (int q = 1; q < (int)(blockDim.x >> 5); ++q) {
+            m = smin[q] < m ? smin[q] : m;
+        }
+        atomicMin(&D.red[0], m);
+    }
+}
+
+__global__ void k_reset_reductions(FxDev D, int which)
+{
+    /* initial values of the reference's reductions: dt_min = 1e99
+     * (src/prj_timeint.c:2147), dt_src = 1e100 (src/main.c:491) */
+    if (which & 1) D.red[0] = fx_double_key(1.0e99);
+    if (which & 2) D.red[1] = fx_double_key(1.0e100);
+}
+
+__device__ __forceinline__ double fx_key_double(unsigned long long key)
+{
+    const unsigned long long bits = (key >> 63) ? (key & 0x7fffffffffffffffULL) : ~key;
+    return __longlong_as_double((long long)bits);
+}
+
+/* dt selection of the driver loop, src/main.c:485-517 (no output events) */
+__global__ void k_step_begin(FxDev D)
+{
+    FxCtl *c = D.ctl;
+    if (!(c->time < c->t_end)) {
+        c->skip = 1;
+        return;
+    }
+    c->skip = 0;
+    const double dt_new = fx_key_double(D.red[0]);
+    if (c->dt_prev > 0.0) {
+        const double dt_limit = c->dt_factor * c->dt_prev;
+        c->dt_prev = dt_new <= dt_limit ? dt_new : dt_limit;
+    } else {
+        c->dt_prev = dt_new;
+    }
+    double dt_step = c->dt_prev;
+    if (c->time + dt_step > c->t_end) {
+        dt_step = c->t_end - c->time;
+    }
+    c->dt = dt_step;
+    D.red[1] = fx_double_key(1.0e100);
+}
+
+/* after the step: dt_src clamp and time advance, src/main.c:555-562 */
+__global__ void k_step_end(FxDev D)
+{
+    FxCtl *c = D.ctl;
+    if (c->skip) {
+        return;
+    }
+    const double dt_src = fx_key_double(D.red[1]);
+    c->dt_src = dt_src;
+    if (c->cfl * dt_src < c->dt_prev) {
+        c->dt_prev = c->cfl * dt_src;
+    }
+    c->time += c->dt;
+    c->step += 1;
+}
+
+/* ------------------------------------------------------------------------ */
+/* Ghost-fill programs                                                       */
+/* ------------------------------------------------------------------------ */
+
+/* limited linear prolongation from a 3x3x3 coarse stencil to a fine target
+ * offset (prj_reconstruct_cell_for_prolongate with use_BJ = 0) */
+__device__ double fx_prolong_cell(const double *q, int c, const double target[3]);
+
+__global__ void k_ghost_cells(FxDev D, const FxGop *__restrict__ ops, int n, int wslot, int nvg)
+{
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n || D.ctl->skip) {
+        return;
+    }
+    const FxGop op = ops[t];
+    const int db = FX_CELL_BLOCK(op.dst);
+    const int dc = FX_CELL_IDX(op.dst);
+    const int sb = FX_CELL_BLOCK(op.src);
+    const int sc = FX_CELL_IDX(op.src);
+    double *Wd = D.W + (size_t)db * FX_W_COUNT(D.nv) + (size_t)wslot * FX_NCELLS;
+    const double *Ws = D.W + (size_t)sb * FX_W_COUNT(D.nv) + (size_t)wslot * FX_NCELLS;
+    switch (op.type) {
+    case FX_GOP_COPY:
+        for (int v = 0; v < nvg; ++v) {
+            Wd[(size_t)v * kPlane + dc] = Ws[(size_t)v * kPlane + sc];
+        }
+        break;
+    case FX_GOP_COPY_NEG:
+        for (int v = 0; v < nvg; ++v) {
+            Wd[(size_t)v * kPlane + dc] = Ws[(size_t)v * kPlane + sc];
+        }
+        Wd[(size_t)op.aux * kPlane + dc] = -Ws[(size_t)op.aux * kPlane + sc];
+        break;
+    case FX_GOP_COPY_USER:
+        for (int v = 0; v < nvg; ++v) {
+            Wd[(size_t)v * kPlane + dc] = Ws[(size_t)v * kPlane + sc];
+        }
+        if (op.aux) {
+            Wd[(size_t)FX_V1 * kPlane + dc] = 5.0;
+        }
+        break;
+    case FX_GOP_RESTRICT:
+        for (int v = 0; v < nvg; ++v) {
+            const double *q = Ws + (size_t)v * kPlane + sc;
+            /* order of src/prj_boundary.c:238-261 */
+            Wd[(size_t)v * kPlane + dc] = 0.125 *
+                (q[0] + q[1] + q[FX_PBS] + q[FX_PBS + 1] +
+                 q[FX_PBS * FX_PBS] + q[FX_PBS * FX_PBS + 1] +
+                 q[FX_PBS * FX_PBS + FX_PBS] + q[FX_PBS * FX_PBS + FX_PBS + 1]);
+        }
+        break;
+    case FX_GOP_PROLONG: {
+        const double target[3] = {
+            (op.aux & 4) ? 0.25 : -0.25,
+            (op.aux & 2) ? 0.25 : -0.25,
+            (op.aux & 1) ? 0.25 : -0.25};
+        for (int v = 0; v < nvg; ++v) {
+            Wd[(size_t)v * kPlane + dc] = fx_prolong_cell(Ws + (size_t)v * kPlane, sc, target);
+        }
+        break;
+    }
+    default:
+        break;
+    }
+}
+
+__device__ __forceinline__ int fx_face_key_block(int key) { return key >> 15; }
+__device__ __forceinline__ int fx_face_key_idx(int key) { return key & 32767; }
+
+__global__ void k_ghost_faces(FxDev D, const FxGop *__restrict__ ops, int n, int bfslot)
+{
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n || D.ctl->skip) {
+        return;
+    }
+    const FxGop op = ops[t];
+    const int dir = op.aux & 3;
+    const int db = fx_face_key_block(op.dst);
+    const int df = fx_face_key_idx(op.dst);
+    const int sb = fx_face_key_block(op.src);
+    const int sf = fx_face_key_idx(op.src);
+    double *Bd = D.Bf + (size_t)db * FX_BF_COUNT + ((size_t)dir * FX_NSTAGES + bfslot) * FX_NFACES;
+    const double *Bs = D.Bf + (size_t)sb * FX_BF_COUNT + ((size_t)dir * FX_NSTAGES + bfslot) * FX_NFACES;
+    if (op.type == FX_FOP_COPY) {
+        Bd[df] = Bs[sf];
+    } else if (op.type == FX_FOP_RESTRICT) {
+        /* 0.25*(s0 + s0+t1 + s0+t0 + s0+t0+t1), src/prj_boundary.c:738-764 */
+        const int o1 = (op.aux >> 2) & 1023;   /* stride of tan1 */
+        const int o0 = (op.aux >> 12) & 1023;  /* stride of tan0 */
+        Bd[df] = 0.25 * (Bs[sf] + Bs[sf + o1] + Bs[sf + o0] + Bs[sf + o0 + o1]);
+    }
+}
+
+__global__ void k_bf2bc(FxDev D, const int *__restrict__ blist, int slot)
+{
+    const int b = blist[blockIdx.y];
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= FX_NCELLS || D.ctl->skip) {
+        return;
+    }
+    const int k = t % FX_PBS - FX_NG;
+    const int j = (t / FX_PBS) % FX_PBS - FX_NG;
+    const int i = t / (FX_PBS * FX_PBS) - FX_NG;
+    const double *bf = D.Bf + (size_t)b * FX_BF_COUNT;
+    const double *b1 = bf + (size_t)(0 * FX_NSTAGES + slot) * FX_NFACES;
+    const double *b2 = bf + (size_t)(1 * FX_NSTAGES + slot) * FX_NFACES;
+    const double *b3 = bf + (size_t)(2 * FX_NSTAGES + slot) * FX_NFACES;
+    /* the metric factor sqrt(gamma) is 1 outside dynamical GR; the
+     * reference's division by it is exact and omitted */
+    const double v1 = 0.5 * (b1[fx_face_idx(0, i, j, k)] + b1[fx_face_idx(0, i + 1, j, k)]);
+    const double v2 = 0.5 * (b2[fx_face_idx(1, i, j, k)] + b2[fx_face_idx(1, i, j + 1, k)]);
+    const double v3 = 0.5 * (b3[fx_face_idx(2, i, j, k)] + b3[fx_face_idx(2, i, j, k + 1)]);
+    const int c = fx_lidx(i, j, k);
+    if (!isfinite(v1) || !isfinite(v2) || !isfinite(v3)) {
+        fx_fail(D.err, FX_ERR_B_NONFINITE, b, c);
+    }
+    double *W = D.W + (size_t)b * FX_W_COUNT(9) + (size_t)slot * FX_NCELLS;
+    W[(size_t)FX_B1 * kPlane + c] = v1;
+    W[(size_t)FX_B2 * kPlane + c] = v2;
+    W[(size_t)FX_B3 * kPlane + c] = v3;
+}
+
+/* coarse/fine corrections */
+__global__ void k_flux_correct(FxDev D, const FxCorr *__restrict__ recs, int n)
+{
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n * D.nv || D.ctl->skip) {
+        return;
+    }
+    const int r = t / D.nv;
+    const int v = t - r * D.nv;
+    const FxCorr rec = recs[r];
+    /* each entry is a flat index into the stacked flux array of component 0;
+     * component v sits FX_AOSOA_W * v further in the AoSoA tile */
+    const size_t off = (size_t)v * FX_AOSOA_W;
+    D.flux[rec.dst + off] = 0.25 *
+        (D.flux[rec.src[0] + off] + D.flux[rec.src[1] + off] +
+         D.flux[rec.src[2] + off] + D.flux[rec.src[3] + off]);
+}
+
+__global__ void k_emf_correct(FxDev D, const FxCorr *__restrict__ recs, int n)
+{
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n || D.ctl->skip) {
+        return;
+    }
+    const FxCorr rec = recs[t];
+    D.emf[rec.dst] = 0.5 * (D.emf[rec.src[0]] + D.emf[rec.src[1]]);
+}
+
+} /* namespace */
+
+/* ------------------------------------------------------------------------ */
+/* prolongation limiter                                                      */
+/* ------------------------------------------------------------------------ */
+namespace {
+__device__ double fx_prolong_cell(const double *q, int c, const double target[3])
+{
+    /* filled in together with the AMR transfer programs */
+    (void)target;
+    return q[c];
+}
+}
+
+/* ------------------------------------------------------------------------ */
+/* launchers                                                                 */
+/* ------------------------------------------------------------------------ */
+static inline unsigned fx_blocks(int n, int tpb) { return (unsigned)((n + tpb - 1) / tpb); }
+
+void fx_launch_flux(const FxDev &D, const int *blist, int nlist, int dir, int wslot, int bfslot,
+    int full, cudaStream_t s)
+{
+    if (nlist <= 0) return;
+    if (D.nv == 9) {
+        const int nf = (FX_BS + 1) * (FX_BS + 2) * (FX_BS + 2);
+        k_flux<true><<<dim3(fx_blocks(nf, 128), nlist), 128, 0, s>>>(D, blist, dir, wslot, bfslot, full);
+    } else {
+        const int nf = (FX_BS + 1) * FX_BS * FX_BS;
+        k_flux<false><<<dim3(fx_blocks(nf, 128), nlist), 128, 0, s>>>(D, blist, dir, wslot, bfslot, full);
+    }
+}
+
+void fx_launch_emf(const FxDev &D, const int *blist, int nlist, int wslot, int bfslot, cudaStream_t s)
+{
+    if (nlist <= 0) return;
+    const int ne = 3 * FX_BS * (FX_BS + 1) * (FX_BS + 1);
+    k_emf<<<dim3(fx_blocks(ne, 128), nlist), 128, 0, s>>>(D, blist, wslot, bfslot);
+}
+
+void fx_launch_bf_update(const FxDev &D, const int *blist, int nlist, int stage, cudaStream_t s)
+{
+    if (nlist <= 0) return;
+    const int nf = 3 * (FX_BS + 1) * FX_BS * FX_BS;
+    k_bf_update<<<dim3(fx_blocks(nf, 128), nlist), 128, 0, s>>>(D, blist, stage);
+}
+
+void fx_launch_cell_update(const FxDev &D, const int *blist, int nlist, int stage,
+    int gravity, int store_rhs, cudaStream_t s)
+{
+    if (nlist <= 0) return;
+    const dim3 grid(fx_blocks(FX_BS * FX_BS * FX_BS, 128), nlist);
+    if (D.nv == 9) {
+        if (stage == 1) k_cell_update<true, 1><<<grid, 128, 0, s>>>(D, blist, gravity, store_rhs);
+        else k_cell_update<true, 2><<<grid, 128, 0, s>>>(D, blist, gravity, store_rhs);
+    } else {
+        if (stage == 1) k_cell_update<false, 1><<<grid, 128, 0, s>>>(D, blist, gravity, store_rhs);
+        else k_cell_update<false, 2><<<grid, 128, 0, s>>>(D, blist, gravity, store_rhs);
+    }
+}
+
+void fx_launch_eos_fill(const FxDev &D, const int *blist, int nlist, int wslot, int active_only,
+    cudaStream_t s)
+{
+    if (nlist <= 0) return;
+    const int n = active_only ? FX_BS * FX_BS * FX_BS : FX_NCELLS;
+    k_eos_fill<<<dim3(fx_blocks(n, 256), nlist), 256, 0, s>>>(D, blist, wslot, active_only);
+}
+
+void fx_launch_calc_dt(const FxDev &D, const int *blist, int nlist, int wslot, double cfl,
+    cudaStream_t s)
+{
+    if (nlist <= 0) return;
+    k_calc_dt<<<dim3(fx_blocks(FX_BS * FX_BS * FX_BS, 256), nlist), 256, 0, s>>>(D, blist, wslot, cfl);
+}
+
+void fx_launch_ghost_cells(const FxDev &D, const FxGop *ops, int n, int wslot, int nvg, cudaStream_t s)
+{
+    if (n <= 0) return;
+    k_ghost_cells<<<fx_blocks(n, 256), 256, 0, s>>>(D, ops, n, wslot, nvg);
+}
+
+void fx_launch_ghost_faces(const FxDev &D, const FxGop *ops, int n, int bfslot, cudaStream_t s)
+{
+    if (n <= 0) return;
+    k_ghost_faces<<<fx_blocks(n, 256), 256, 0, s>>>(D, ops, n, bfslot);
+}
+
+void fx_launch_bf2bc(const FxDev &D, const int *blist, int nlist, int slot, cudaStream_t s)
+{
+    if (nlist <= 0) return;
+    k_bf2bc<<<dim3(fx_blocks(FX_NCELLS, 256), nlist), 256, 0, s>>>(D, blist, slot);
+}
+
+void fx_launch_flux_correct(const FxDev &D, const FxCorr *recs, int n, cudaStream_t s)
+{
+    if (n <= 0) return;
+    k_flux_correct<<<fx_blocks(n * D.nv, 256), 256, 0, s>>>(D, recs, n);
+}
+
+void fx_launch_emf_correct(const FxDev &D, const FxCorr *recs, int n, cudaStream_t s)
+{
+    if (n <= 0) return;
+    k_emf_correct<<<fx_blocks(n, 256), 256, 0, s>>>(D, recs, n);
+}
+
+void fx_launch_reset_reductions(const FxDev &D, int which, cudaStream_t s)
+{
+    k_reset_reductions<<<1, 1, 0, s>>>(D, which);
+}
+
+void fx_launch_step_begin(const FxDev &D, cudaStream_t s)
+{
+    k_step_begin<<<1, 1, 0, s>>>(D);
+}
+
+void fx_launch_step_end(const FxDev &D, cudaStream_t s)
+{
+    k_step_end<<<1, 1, 0, s>>>(D);
+}
+
+namespace {
+__global__ void k_set_dt(FxDev D, double dt)
+{
+    D.ctl->dt = dt;
+    D.ctl->skip = 0;
+}
+
+__global__ void k_set_ctl(FxDev D, FxCtl v)
+{
+    *D.ctl = v;
+}
+}
+
+void fx_launch_set_dt(const FxDev &D, double dt, cudaStream_t s)
+{
+    k_set_dt<<<1, 1, 0, s>>>(D, dt);
+}
+
+void fx_launch_set_ctl(const FxDev &D, FxCtl value, cudaStream_t s)
+{
+    k_set_ctl<<<1, 1, 0, s>>>(D, value);
+}

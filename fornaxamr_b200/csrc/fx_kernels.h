@@ -1,0 +1,129 @@
+/*
+ * Host-visible declarations shared by the runtime and the kernels.
+ */
+#ifndef FX_KERNELS_H
+#define FX_KERNELS_H
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "fx_layout.h"
+
+struct FxErr;
+
+/* Step control block in device memory.  Stepping kernels read dt from here
+ * (so a captured graph is dt-independent) and return at once when `skip` is
+ * set (the device-resident driver loop reached t_end). */
+struct FxCtl {
+    double dt;        /* dt of the current step */
+    double time;      /* simulation time (driver loop) */
+    double dt_prev;   /* sim.dt of the reference driver */
+    double cfl;
+    double dt_factor;
+    double t_end;
+    double dt_src;    /* last step's dt_src */
+    long long step;
+    int skip;
+    int pad;
+};
+
+/* per-block geometry on the device */
+struct FxBlockDev {
+    double xmin[3];
+    double dx[3];
+    double vol;
+    double area[3];
+};
+
+/* device view of one mesh: stacked per-block arrays in the reference layout */
+struct FxDev {
+    int nv;       /* primitive/conserved variables per cell: 9 (MHD) or 6 */
+    int nblocks;
+    double gamma;
+    double mhd_eta;
+    const FxBlockDev *blk;
+    double *W;    /* [b][v][stage][cell]           (WIDX) */
+    double *Bf;   /* [b][dir][stage][face]         (FACE_IDX) */
+    double *flux; /* [b][dir][AoSoA nc=nv]         (VIDX) */
+    double *vr;   /* [b][dir][AoSoA nc=3]          (VRIDX) */
+    double *bv1;  /* [b][dir][cell]                (IDX) */
+    double *bv2;
+    double *emf;  /* [b][dir][edge]                (EDGE_IDX) */
+    double *eos;  /* [b][AoSoA nc=3]               (EIDX) */
+    double *rhs;  /* [b][AoSoA nc=nv]              (MHDVIDX) */
+    double *grav; /* [b][dir][cell] or null        (IDX) */
+    FxErr *err;
+    unsigned long long *red;  /* [0] dt min key, [1] dt_src min key */
+    FxCtl *ctl;
+};
+
+/* One element operation of a ghost-fill program.  dst/src pack
+ * (block << 13) | cell for cell ops, or (block << 15) | face for face ops
+ * (with the face direction in `aux` bits 0-1). */
+enum FxGopType {
+    FX_GOP_COPY = 0,        /* dst <- src (all ghost vars) */
+    FX_GOP_COPY_NEG = 1,    /* dst <- src, normal velocity aux negated (reflect) */
+    FX_GOP_COPY_USER = 2,   /* dst <- src, then v1 = 5 (reference PRJ_BC_USER) */
+    FX_GOP_RESTRICT = 3,    /* dst <- 1/8 sum of the 2x2x2 cells at src */
+    FX_GOP_PROLONG = 4,     /* dst <- limited linear from the 27 cells about src */
+    FX_FOP_COPY = 8,        /* face: dst <- src */
+    FX_FOP_RESTRICT = 9,    /* face: dst <- 1/4 sum of 4 fine faces */
+    FX_FOP_PROLONG = 10     /* face: divergence-free prolongation value */
+};
+
+struct FxGop {
+    int32_t dst;
+    int32_t src;
+    int32_t aux;
+    int32_t type;
+};
+
+/* coarse/fine correction records: dst <- 0.25 * sum of 4 (flux) or
+ * 0.5 * sum of 2 (emf) source entries */
+struct FxCorr {
+    int32_t dst;
+    int32_t src[4];
+    int32_t n;
+    int32_t pad[2];
+};
+
+#define FX_CELL_KEY(b, c) (((b) << 13) | (c))
+#define FX_CELL_BLOCK(key) ((key) >> 13)
+#define FX_CELL_IDX(key) ((key) & 8191)
+
+/* launchers (fx_kernels.cu); all asynchronous on `s` */
+void fx_launch_flux(const FxDev &D, const int *blist, int nlist, int dir, int wslot, int bfslot,
+    int full, cudaStream_t s);
+void fx_launch_emf(const FxDev &D, const int *blist, int nlist, int wslot, int bfslot, cudaStream_t s);
+void fx_launch_bf_update(const FxDev &D, const int *blist, int nlist, int stage, cudaStream_t s);
+void fx_launch_cell_update(const FxDev &D, const int *blist, int nlist, int stage,
+    int gravity, int store_rhs, cudaStream_t s);
+void fx_launch_eos_fill(const FxDev &D, const int *blist, int nlist, int wslot, int active_only,
+    cudaStream_t s);
+void fx_launch_calc_dt(const FxDev &D, const int *blist, int nlist, int wslot, double cfl,
+    cudaStream_t s);
+void fx_launch_ghost_cells(const FxDev &D, const FxGop *ops, int n, int wslot, int nvg, cudaStream_t s);
+void fx_launch_ghost_faces(const FxDev &D, const FxGop *ops, int n, int bfslot, cudaStream_t s);
+void fx_launch_bf2bc(const FxDev &D, const int *blist, int nlist, int slot, cudaStream_t s);
+void fx_launch_flux_correct(const FxDev &D, const FxCorr *recs, int n, cudaStream_t s);
+void fx_launch_emf_correct(const FxDev &D, const FxCorr *recs, int n, cudaStream_t s);
+void fx_launch_reset_reductions(const FxDev &D, int which, cudaStream_t s);
+/* device-resident driver: dt selection before a step, dt_src clamp and time
+ * advance after it (src/main.c:513-562) */
+void fx_launch_step_begin(const FxDev &D, cudaStream_t s);
+void fx_launch_step_end(const FxDev &D, cudaStream_t s);
+/* stream-ordered write of a host-chosen dt into the control block */
+void fx_launch_set_dt(const FxDev &D, double dt, cudaStream_t s);
+/* controlled driver state set-up */
+void fx_launch_set_ctl(const FxDev &D, FxCtl value, cudaStream_t s);
+
+/* ordered-integer keys for atomicMin over doubles */
+static inline double fx_key_to_double(unsigned long long key)
+{
+    unsigned long long bits = (key >> 63) ? (key & 0x7fffffffffffffffULL) : ~key;
+    double d;
+    __builtin_memcpy(&d, &bits, sizeof(d));
+    return d;
+}
+
+#endif

@@ -1,0 +1,602 @@
+/*
+ * Device-side pointwise physics of the per-block Godunov MHD update.
+ *
+ * Every function here evaluates the same IEEE-754 double operations, in the
+ * same association order, as the reference routine it cites; the library is
+ * compiled with --fmad=false so no multiply-add is contracted.  With correctly
+ * rounded division and square root (CUDA's default for double) the results
+ * are bit-identical to the reference's CPU path built with -ffp-contract=off.
+ * Comments give the C association explicitly where it matters, e.g.
+ * "a * b * c" is (a*b)*c.
+ *
+ * Failures the reference turns into exit(1) (non-positive density, invalid
+ * wave ordering, ...) are reported through fx_fail(): the first failing
+ * thread records a code and its position in the device error word and the
+ * kernel continues with whatever values result, so no launch ever traps.
+ */
+#ifndef FX_PHYSICS_CUH
+#define FX_PHYSICS_CUH
+
+#include "fx_layout.h"
+
+/* error codes (first error wins); the host maps them to the reference's
+ * fail-fast messages */
+enum fx_err_code {
+    FX_OK = 0,
+    FX_ERR_HLLD_RHO = 1,       /* prj_riemann.c:159-161 non-positive density */
+    FX_ERR_HLLD_P = 2,         /* prj_riemann.c:162-164 non-positive gas pressure */
+    FX_ERR_HLLD_GAMMA = 3,     /* prj_riemann.c:165-167 */
+    FX_ERR_HLLD_DISC = 4,      /* prj_riemann.c:128-130 negative fast-speed discriminant */
+    FX_ERR_HLLD_CF = 5,        /* prj_riemann.c:134-136 invalid fast speed */
+    FX_ERR_HLLD_ORDER = 6,     /* prj_riemann.c:361-363 invalid fast-wave ordering */
+    FX_ERR_HLLD_DENOM = 7,     /* prj_riemann.c:380-384 degenerate contact-speed denominator */
+    FX_ERR_HLLD_OUTER = 8,     /* prj_riemann.c:198-200 outer wave coincides with contact */
+    FX_ERR_HLLD_STARRHO = 9,   /* prj_riemann.c:203-205 invalid star density */
+    FX_ERR_HLLD_DSTAR = 10,    /* prj_riemann.c:250-252 invalid double-star weights */
+    FX_ERR_EMF_NONFINITE = 11, /* prj_timeint.c:171-176, prj_mhd.c:650-654 */
+    FX_ERR_BF_NONFINITE = 12,  /* prj_timeint.c:441-443 non-finite updated magnetic field */
+    FX_ERR_EOS_ZERO_RHO = 13,  /* prj_eos.c:248-250 zero density in eos fill */
+    FX_ERR_ETA = 14,           /* prj_timeint.c:255-257, 279-281 */
+    FX_ERR_B_NONFINITE = 15,   /* prj_timeint.c:506-508, prj_mhd.c:593-595 */
+    FX_ERR_TIMEOUT = 16        /* a bounded device wait gave up */
+};
+
+struct FxErr {
+    int code;
+    int block;
+    int index;
+    int aux;
+};
+
+__device__ __forceinline__ void fx_fail(FxErr *err, int code, int block, int index)
+{
+    if (err != nullptr && atomicCAS(&err->code, 0, code) == 0) {
+        err->block = block;
+        err->index = index;
+    }
+}
+
+__device__ __forceinline__ double fx_min(double a, double b) { return a < b ? a : b; }
+__device__ __forceinline__ double fx_max(double a, double b) { return a > b ? a : b; }
+
+/* ------------------------------------------------------------------------ */
+/* MC limited slope, src/prj_reconstruct.h:355-375 (branchless form).        */
+/* ------------------------------------------------------------------------ */
+__device__ __forceinline__ double fx_mc_slope(double qm, double q0, double qp)
+{
+    const double sl = q0 - qm;
+    const double sr = qp - q0;
+    const double c0 = 2.0 * sl;
+    const double c1 = sl + 0.5 * (sr - sl);
+    const double c2 = 2.0 * sr;
+    double mn = c0 < c1 ? c0 : c1;
+    double mx = c0 > c1 ? c0 : c1;
+    mn = mn < c2 ? mn : c2;
+    mx = mx > c2 ? mx : c2;
+    const double slope = sl > 0.0 ? mn : mx;
+    return (sl * sr > 0.0) ? slope : 0.0;
+}
+
+/* ------------------------------------------------------------------------ */
+/* Ideal gas (problems/prj_problem_ideal_eos.h:24-32 through the USER branch */
+/* of prj_eos_rey, src/prj_eos.c:772-788).                                   */
+/* ------------------------------------------------------------------------ */
+__device__ __forceinline__ double fx_pressure(double g, double rho, double eint)
+{
+    return (g - 1.0) * rho * eint;            /* ((g-1)*rho)*eint */
+}
+
+__device__ __forceinline__ double fx_temperature(double g, double eint)
+{
+    return (g - 1.0) * eint / FX_IDEAL_ENERGY_SCALE;
+}
+
+/* prj_eos_prim2cons, src/prj_eos.c:2112-2151 */
+template <bool MHD>
+__device__ __forceinline__ void fx_prim2cons(const double *w, double *u)
+{
+    const double rho = w[FX_RHO];
+    const double v1 = w[FX_V1];
+    const double v2 = w[FX_V2];
+    const double v3 = w[FX_V3];
+    const double eint = w[FX_EINT];
+    u[FX_RHO] = rho;
+    u[FX_V1] = rho * v1;
+    u[FX_V2] = rho * v2;
+    u[FX_V3] = rho * v3;
+    if (MHD) {
+        const double b1 = w[FX_B1];
+        const double b2 = w[FX_B2];
+        const double b3 = w[FX_B3];
+        u[FX_ETOT] = rho * eint + 0.5 * rho * (v1 * v1 + v2 * v2 + v3 * v3) +
+            0.5 * (b1 * b1 + b2 * b2 + b3 * b3);
+        u[FX_YE] = rho * w[FX_YE];
+        u[FX_B1] = b1;
+        u[FX_B2] = b2;
+        u[FX_B3] = b3;
+    } else {
+        u[FX_ETOT] = rho * eint + 0.5 * rho * (v1 * v1 + v2 * v2 + v3 * v3);
+        u[FX_YE] = rho * w[FX_YE];
+    }
+}
+
+/* prj_eos_cons2prim, src/prj_eos.c:2153-2220 (no floors) */
+template <bool MHD>
+__device__ __forceinline__ void fx_cons2prim(const double *u, double *w)
+{
+    const double rho = u[FX_RHO];
+    if (rho == 0.0) {
+        for (int v = 0; v < (MHD ? 9 : 6); ++v) {
+            w[v] = 0.0;
+        }
+        return;
+    }
+    const double v1 = u[FX_V1] / rho;
+    const double v2 = u[FX_V2] / rho;
+    const double v3 = u[FX_V3] / rho;
+    const double kinetic = 0.5 * (v1 * v1 + v2 * v2 + v3 * v3);
+    w[FX_RHO] = rho;
+    w[FX_V1] = v1;
+    w[FX_V2] = v2;
+    w[FX_V3] = v3;
+    if (MHD) {
+        const double magnetic = 0.5 * (u[FX_B1] * u[FX_B1] + u[FX_B2] * u[FX_B2] +
+            u[FX_B3] * u[FX_B3]) / rho;
+        w[FX_EINT] = u[FX_ETOT] / rho - kinetic - magnetic;
+        w[FX_YE] = u[FX_YE] / rho;
+        w[FX_B1] = u[FX_B1];
+        w[FX_B2] = u[FX_B2];
+        w[FX_B3] = u[FX_B3];
+    } else {
+        w[FX_EINT] = u[FX_ETOT] / rho - kinetic;
+        w[FX_YE] = u[FX_YE] / rho;
+    }
+}
+
+/* ------------------------------------------------------------------------ */
+/* HLLD (Miyoshi & Kusano 2005) as in src/prj_riemann.c:81-440.              */
+/* ------------------------------------------------------------------------ */
+#define FX_HLLD_SMALL 1.0e-8
+
+struct FxHlldState {
+    double rho, vx, vy, vz, bx, by, bz, p, gamma, ye, e, pt;
+};
+
+struct FxHlldStar {
+    double rho, vx, vy, vz, bx, by, bz, ye, e;
+};
+
+/* prj_hlld_fill_conserved, src/prj_riemann.c:81-94 (component v) */
+__device__ __forceinline__ double fx_hlld_u(const FxHlldStar &s, int v)
+{
+    switch (v) {
+    case 0: return s.rho;
+    case 1: return s.rho * s.vx;
+    case 2: return s.rho * s.vy;
+    case 3: return s.rho * s.vz;
+    case 4: return s.e;
+    case 5: return s.rho * s.ye;
+    case 6: return s.bx;
+    case 7: return s.by;
+    default: return s.bz;
+    }
+}
+
+__device__ __forceinline__ double fx_hlld_state_u(const FxHlldState &s, int v)
+{
+    switch (v) {
+    case 0: return s.rho;
+    case 1: return s.rho * s.vx;
+    case 2: return s.rho * s.vy;
+    case 3: return s.rho * s.vz;
+    case 4: return s.e;
+    case 5: return s.rho * s.ye;
+    case 6: return s.bx;
+    case 7: return s.by;
+    default: return s.bz;
+    }
+}
+
+/* prj_hlld_fill_flux, src/prj_riemann.c:96-115 (component v) */
+__device__ __forceinline__ double fx_hlld_state_f(const FxHlldState &s, int v)
+{
+    const double b2 = s.bx * s.bx + s.by * s.by + s.bz * s.bz;
+    const double pt = s.p + 0.5 * b2;
+    switch (v) {
+    case 0: return s.rho * s.vx;
+    case 1: return s.rho * s.vx * s.vx + pt - s.bx * s.bx;
+    case 2: return s.rho * s.vx * s.vy - s.bx * s.by;
+    case 3: return s.rho * s.vx * s.vz - s.bx * s.bz;
+    case 4: {
+        const double vdotb = s.vx * s.bx + s.vy * s.by + s.vz * s.bz;
+        return (s.e + pt) * s.vx - s.bx * vdotb;
+    }
+    case 5: return s.rho * s.ye * s.vx;
+    case 6: return 0.0;
+    case 7: return s.by * s.vx - s.bx * s.vy;
+    default: return s.bz * s.vx - s.bx * s.vz;
+    }
+}
+
+/* prj_hlld_state_from_prim, src/prj_riemann.c:142-178; w is the local
+ * (direction-rotated) primitive vector, the normal field is bn. */
+__device__ __forceinline__ void fx_hlld_state(const double *w, double p, double gamma, double bn,
+    FxHlldState &s, FxErr *err, int blk, int idx)
+{
+    s.rho = w[FX_RHO];
+    s.vx = w[FX_V1];
+    s.vy = w[FX_V2];
+    s.vz = w[FX_V3];
+    s.bx = bn;
+    s.by = w[FX_B2];
+    s.bz = w[FX_B3];
+    s.p = p;
+    s.gamma = gamma;
+    s.ye = w[FX_YE];
+    if (s.rho <= 0.0) fx_fail(err, FX_ERR_HLLD_RHO, blk, idx);
+    if (s.p <= 0.0) fx_fail(err, FX_ERR_HLLD_P, blk, idx);
+    if (s.gamma <= 0.0) fx_fail(err, FX_ERR_HLLD_GAMMA, blk, idx);
+    const double kinetic = 0.5 * s.rho * (s.vx * s.vx + s.vy * s.vy + s.vz * s.vz);
+    const double magnetic = 0.5 * (s.bx * s.bx + s.by * s.by + s.bz * s.bz);
+    s.e = s.rho * w[FX_EINT] + kinetic + magnetic;
+    s.pt = s.p + magnetic;
+}
+
+/* prj_hlld_fast_speed, src/prj_riemann.c:117-140 */
+__device__ __forceinline__ double fx_hlld_fast_speed(const FxHlldState &s, FxErr *err, int blk, int idx)
+{
+    const double a2 = s.gamma * s.p / s.rho;
+    const double bx2_rho = s.bx * s.bx / s.rho;
+    const double b2_rho = (s.bx * s.bx + s.by * s.by + s.bz * s.bz) / s.rho;
+    double disc = (a2 + b2_rho) * (a2 + b2_rho) - 4.0 * a2 * bx2_rho;
+    if (disc < 0.0) {
+        if (disc < -1.0e-12 * (a2 + b2_rho) * (a2 + b2_rho)) {
+            fx_fail(err, FX_ERR_HLLD_DISC, blk, idx);
+        }
+        disc = 0.0;
+    }
+    const double cf2 = 0.5 * (a2 + b2_rho + sqrt(disc));
+    if (cf2 < 0.0 || !isfinite(cf2)) {
+        fx_fail(err, FX_ERR_HLLD_CF, blk, idx);
+    }
+    return sqrt(cf2);
+}
+
+/* prj_hlld_outer_star, src/prj_riemann.c:185-232 */
+__device__ __forceinline__ void fx_hlld_outer_star(const FxHlldState &s, double S, double SM,
+    double pt_star, FxHlldStar &st, FxErr *err, int blk, int idx)
+{
+    const double alpha = S - s.vx;
+    const double smdiff = S - SM;
+    if (fabs(smdiff) <= 1.0e-14 * (fabs(S) + fabs(SM) + 1.0)) {
+        fx_fail(err, FX_ERR_HLLD_OUTER, blk, idx);
+    }
+    st.rho = s.rho * alpha / smdiff;
+    if (st.rho <= 0.0 || !isfinite(st.rho)) {
+        fx_fail(err, FX_ERR_HLLD_STARRHO, blk, idx);
+    }
+    st.vx = SM;
+    st.bx = s.bx;
+    st.ye = s.ye;
+    const double denom = s.rho * alpha * smdiff - s.bx * s.bx;
+    if (fabs(denom) < FX_HLLD_SMALL * pt_star) {
+        st.vy = s.vy;
+        st.vz = s.vz;
+        st.by = s.by;
+        st.bz = s.bz;
+    } else {
+        const double sm_diff_vx_over_denom = (SM - s.vx) / denom;
+        const double mag_factor = (s.rho * alpha * alpha - s.bx * s.bx) / denom;
+        st.vy = s.vy - s.bx * s.by * sm_diff_vx_over_denom;
+        st.vz = s.vz - s.bx * s.bz * sm_diff_vx_over_denom;
+        st.by = s.by * mag_factor;
+        st.bz = s.bz * mag_factor;
+    }
+    const double vdotb = s.vx * s.bx + s.vy * s.by + s.vz * s.bz;
+    const double vstar_dotbstar = st.vx * st.bx + st.vy * st.by + st.vz * st.bz;
+    st.e = (alpha * s.e - s.pt * s.vx + pt_star * SM + s.bx * (vdotb - vstar_dotbstar)) / smdiff;
+}
+
+/* prj_hlld_double_star_one, src/prj_riemann.c:234-282 */
+__device__ __forceinline__ void fx_hlld_double_star(const FxHlldStar &left, const FxHlldStar &right,
+    double bx, bool right_side, FxHlldStar &ss, FxErr *err, int blk, int idx)
+{
+    const double sqrt_l = sqrt(left.rho);
+    const double sqrt_r = sqrt(right.rho);
+    if (sqrt_l + sqrt_r <= 0.0) {
+        fx_fail(err, FX_ERR_HLLD_DSTAR, blk, idx);
+    }
+    const double inv_sum = 1.0 / (sqrt_l + sqrt_r);
+    const double sign_bx = bx < 0.0 ? -1.0 : 1.0;
+    const double vy_ss = (sqrt_l * left.vy + sqrt_r * right.vy +
+        (right.by - left.by) * sign_bx) * inv_sum;
+    const double vz_ss = (sqrt_l * left.vz + sqrt_r * right.vz +
+        (right.bz - left.bz) * sign_bx) * inv_sum;
+    const double by_ss = (sqrt_l * right.by + sqrt_r * left.by +
+        sqrt_l * sqrt_r * (right.vy - left.vy) * sign_bx) * inv_sum;
+    const double bz_ss = (sqrt_l * right.bz + sqrt_r * left.bz +
+        sqrt_l * sqrt_r * (right.vz - left.vz) * sign_bx) * inv_sum;
+    const double vbdot_ss = (right_side ? right.vx : left.vx) * bx + vy_ss * by_ss + vz_ss * bz_ss;
+    if (!right_side) {
+        const double vbdot_l = left.vx * bx + left.vy * left.by + left.vz * left.bz;
+        ss = left;
+        ss.e = left.e - sqrt_l * sign_bx * (vbdot_l - vbdot_ss);
+    } else {
+        const double vbdot_r = right.vx * bx + right.vy * right.by + right.vz * right.bz;
+        ss = right;
+        ss.e = right.e + sqrt_r * sign_bx * (vbdot_r - vbdot_ss);
+    }
+    ss.vy = vy_ss;
+    ss.vz = vz_ss;
+    ss.by = by_ss;
+    ss.bz = bz_ss;
+}
+
+/* Face outputs of the MHD solver: local-frame flux (9), face velocity (3)
+ * and the two face EMF products (prj_hlld_face_outputs,
+ * src/prj_riemann.c:305-319). */
+struct FxFaceOut {
+    double F[9];
+    double v[3];
+    double bv1;
+    double bv2;
+};
+
+__device__ __forceinline__ void fx_face_outputs(double vx, double vy, double vz,
+    double bx, double by, double bz, FxFaceOut &o)
+{
+    o.v[0] = vx;
+    o.v[1] = vy;
+    o.v[2] = vz;
+    o.bv1 = bz * vx - bx * vz;
+    o.bv2 = bx * vy - by * vx;
+}
+
+/* prj_riemann_hlld, src/prj_riemann.c:321-440 */
+static __device__ __noinline__ void fx_riemann_hlld(const double *WL, const double *WR,
+    double pL, double pR, double gL, double gR, double bn, FxFaceOut &o,
+    FxErr *err, int blk, int idx)
+{
+    FxHlldState L, R;
+    fx_hlld_state(WL, pL, gL, bn, L, err, blk, idx);
+    fx_hlld_state(WR, pR, gR, bn, R, err, blk, idx);
+    const double cfL = fx_hlld_fast_speed(L, err, blk, idx);
+    const double cfR = fx_hlld_fast_speed(R, err, blk, idx);
+    const double SL = fx_min(L.vx - cfL, R.vx - cfR);
+    const double SR = fx_max(L.vx + cfL, R.vx + cfR);
+    if (!(SL < SR)) {
+        fx_fail(err, FX_ERR_HLLD_ORDER, blk, idx);
+    }
+    if (0.0 <= SL) {
+        for (int v = 0; v < 9; ++v) o.F[v] = fx_hlld_state_f(L, v);
+        fx_face_outputs(L.vx, L.vy, L.vz, L.bx, L.by, L.bz, o);
+        return;
+    }
+    if (SR <= 0.0) {
+        for (int v = 0; v < 9; ++v) o.F[v] = fx_hlld_state_f(R, v);
+        fx_face_outputs(R.vx, R.vy, R.vz, R.bx, R.by, R.bz, o);
+        return;
+    }
+    const double denom = R.rho * (SR - R.vx) - L.rho * (SL - L.vx);
+    if (fabs(denom) <= 1.0e-14 *
+        (fabs(R.rho * (SR - R.vx)) + fabs(L.rho * (SL - L.vx)) + 1.0)) {
+        fx_fail(err, FX_ERR_HLLD_DENOM, blk, idx);
+    }
+    const double SM = (R.rho * R.vx * (SR - R.vx) -
+        L.rho * L.vx * (SL - L.vx) + (L.pt - R.pt)) / denom;
+    const double pt_star_l = L.pt + L.rho * (SL - L.vx) * (SM - L.vx);
+    const double pt_star_r = R.pt + R.rho * (SR - R.vx) * (SM - R.vx);
+    const double pt_star = 0.5 * (pt_star_l + pt_star_r);
+    if (pt_star <= 0.0 || !isfinite(pt_star)) {
+        /* HLL fallback, src/prj_riemann.c:392-409 */
+        const double inv = 1.0 / (SR - SL);
+        double Uh[9];
+        for (int v = 0; v < 9; ++v) {
+            const double lf = fx_hlld_state_f(L, v);
+            const double rf = fx_hlld_state_f(R, v);
+            const double lu = fx_hlld_state_u(L, v);
+            const double ru = fx_hlld_state_u(R, v);
+            o.F[v] = (SR * lf - SL * rf + SL * SR * (ru - lu)) * inv;
+            Uh[v] = (SR * ru - SL * lu + lf - rf) * inv;
+        }
+        const double rho = Uh[0];
+        fx_face_outputs(Uh[1] / rho, Uh[2] / rho, Uh[3] / rho, Uh[6], Uh[7], Uh[8], o);
+        return;
+    }
+    const bool bn_small = (0.5 * bn * bn < FX_HLLD_SMALL * pt_star);
+    FxHlldStar Ls, Rs, ss;
+    if (0.0 <= SM) {
+        fx_hlld_outer_star(L, SL, SM, pt_star, Ls, err, blk, idx);
+        const double SLs = SM - fabs(bn) / sqrt(Ls.rho);
+        if (0.0 <= SLs || bn_small) {
+            for (int v = 0; v < 9; ++v) {
+                o.F[v] = fx_hlld_state_f(L, v) + SL * (fx_hlld_u(Ls, v) - fx_hlld_state_u(L, v));
+            }
+            fx_face_outputs(Ls.vx, Ls.vy, Ls.vz, Ls.bx, Ls.by, Ls.bz, o);
+        } else {
+            fx_hlld_outer_star(R, SR, SM, pt_star, Rs, err, blk, idx);
+            fx_hlld_double_star(Ls, Rs, bn, false, ss, err, blk, idx);
+            for (int v = 0; v < 9; ++v) {
+                const double us = fx_hlld_u(Ls, v);
+                o.F[v] = fx_hlld_state_f(L, v) + SL * (us - fx_hlld_state_u(L, v)) +
+                    SLs * (fx_hlld_u(ss, v) - us);
+            }
+            fx_face_outputs(ss.vx, ss.vy, ss.vz, ss.bx, ss.by, ss.bz, o);
+        }
+    } else {
+        fx_hlld_outer_star(R, SR, SM, pt_star, Rs, err, blk, idx);
+        const double SRs = SM + fabs(bn) / sqrt(Rs.rho);
+        if (SRs <= 0.0 || bn_small) {
+            for (int v = 0; v < 9; ++v) {
+                o.F[v] = fx_hlld_state_f(R, v) + SR * (fx_hlld_u(Rs, v) - fx_hlld_state_u(R, v));
+            }
+            fx_face_outputs(Rs.vx, Rs.vy, Rs.vz, Rs.bx, Rs.by, Rs.bz, o);
+        } else {
+            fx_hlld_outer_star(L, SL, SM, pt_star, Ls, err, blk, idx);
+            fx_hlld_double_star(Ls, Rs, bn, true, ss, err, blk, idx);
+            for (int v = 0; v < 9; ++v) {
+                const double us = fx_hlld_u(Rs, v);
+                o.F[v] = fx_hlld_state_f(R, v) + SR * (us - fx_hlld_state_u(R, v)) +
+                    SRs * (fx_hlld_u(ss, v) - us);
+            }
+            fx_face_outputs(ss.vx, ss.vy, ss.vz, ss.bx, ss.by, ss.bz, o);
+        }
+    }
+}
+
+/* ------------------------------------------------------------------------ */
+/* HLLC for the hydro build, src/prj_riemann.c:1433-1599 and the theta       */
+/* pressure-jump limiter of src/prj_riemann.c:8-17.                          */
+/* ------------------------------------------------------------------------ */
+__device__ __forceinline__ double fx_theta_limiter(double cfmax, double du, double dv, double dw)
+{
+    double theta_r = (-fx_min(du, 0.0) + cfmax) / (-fx_min(fx_min(dv, dw), 0.0) + cfmax);
+    theta_r *= theta_r;
+    return fx_min(1.0, theta_r * theta_r);
+}
+
+/* prj_riemann_state, src/prj_riemann.c:1433-1492 (hydro: 6 components) */
+__device__ __forceinline__ void fx_hllc_state(const double *W, double p, double gamma,
+    double *U, double *F, double &cs)
+{
+    const double rho = W[FX_RHO];
+    const double v1 = W[FX_V1];
+    const double v2 = W[FX_V2];
+    const double v3 = W[FX_V3];
+    const double eint = W[FX_EINT];
+    const double etot = rho * eint + 0.5 * rho * (v1 * v1 + v2 * v2 + v3 * v3);
+    U[0] = rho;
+    U[1] = rho * v1;
+    U[2] = rho * v2;
+    U[3] = rho * v3;
+    U[4] = etot;
+    U[5] = rho * W[FX_YE];
+    cs = sqrt(gamma * p / rho);
+    F[0] = rho * v1;
+    F[1] = rho * v1 * v1 + p;
+    F[2] = rho * v1 * v2;
+    F[3] = rho * v1 * v3;
+    F[4] = (etot + p) * v1;
+    F[5] = rho * W[FX_YE] * v1;
+}
+
+/* prj_riemann_hllc, src/prj_riemann.c:1494-1599; F[6], vface[3] out */
+static __device__ __noinline__ void fx_riemann_hllc(const double *WL, const double *WR,
+    double pL, double pR, double gL, double gR, double du, double dv, double dw,
+    double *flux, double *v_face)
+{
+    double UL[6], UR[6], FL[6], FR[6], Ustar[6];
+    double csL, csR;
+    fx_hllc_state(WL, pL, gL, UL, FL, csL);
+    fx_hllc_state(WR, pR, gR, UR, FR, csR);
+    const double SL = fx_min(WL[FX_V1] - csL, WR[FX_V1] - csR);
+    const double SR = fx_max(WL[FX_V1] + csL, WR[FX_V1] + csR);
+    const double cfmax = fx_max(csL, csR);
+    const double theta = fx_theta_limiter(cfmax, du, dv, dw);
+    const double SM = (theta * (pR - pL) +
+        UL[1] * (SL - WL[FX_V1]) -
+        UR[1] * (SR - WR[FX_V1])) /
+        (UL[0] * (SL - WL[FX_V1]) -
+            UR[0] * (SR - WR[FX_V1]));
+    if (0.0 <= SL) {
+        for (int v = 0; v < 6; ++v) flux[v] = FL[v];
+        v_face[0] = WL[FX_V1];
+        v_face[1] = WL[FX_V2];
+        v_face[2] = WL[FX_V3];
+        return;
+    }
+    if (SR <= 0.0) {
+        for (int v = 0; v < 6; ++v) flux[v] = FR[v];
+        v_face[0] = WR[FX_V1];
+        v_face[1] = WR[FX_V2];
+        v_face[2] = WR[FX_V3];
+        return;
+    }
+    v_face[0] = SM;
+    if (0.0 <= SM) {
+        v_face[1] = WL[FX_V2];
+        v_face[2] = WL[FX_V3];
+        for (int v = 0; v < 6; ++v) Ustar[v] = UL[v];
+        const double rho_star = UL[0] * (SL - WL[FX_V1]) / (SL - SM);
+        Ustar[0] = rho_star;
+        Ustar[1] = rho_star * SM;
+        Ustar[2] = rho_star * WL[FX_V2];
+        Ustar[3] = rho_star * WL[FX_V3];
+        const double e_over_rho = UL[4] / UL[0] +
+            (SM - WL[FX_V1]) * (SM + pL / (UL[0] * (SL - WL[FX_V1])));
+        Ustar[4] = rho_star * e_over_rho;
+        Ustar[5] = rho_star * WL[FX_YE];
+        for (int v = 0; v < 6; ++v) flux[v] = FL[v] + SL * (Ustar[v] - UL[v]);
+    } else {
+        v_face[1] = WR[FX_V2];
+        v_face[2] = WR[FX_V3];
+        for (int v = 0; v < 6; ++v) Ustar[v] = UR[v];
+        const double rho_star = UR[0] * (SR - WR[FX_V1]) / (SR - SM);
+        Ustar[0] = rho_star;
+        Ustar[1] = rho_star * SM;
+        Ustar[2] = rho_star * WR[FX_V2];
+        Ustar[3] = rho_star * WR[FX_V3];
+        const double e_over_rho = UR[4] / UR[0] +
+            (SM - WR[FX_V1]) * (SM + pR / (UR[0] * (SR - WR[FX_V1])));
+        Ustar[4] = rho_star * e_over_rho;
+        Ustar[5] = rho_star * WR[FX_YE];
+        for (int v = 0; v < 6; ++v) flux[v] = FR[v] + SR * (Ustar[v] - UR[v]);
+    }
+}
+
+/* ------------------------------------------------------------------------ */
+/* Upwind corner EMF, src/prj_mhd.c:627-718 (eta term separate).            */
+/* ------------------------------------------------------------------------ */
+__device__ __forceinline__ double fx_emf_upwind(const double f[4], const double c[4], const double vn[4])
+{
+    double emf = 0.25 * (f[0] + f[1] + f[2] + f[3]);
+    if (vn[0] > 0.0) {
+        emf += 0.25 * (f[3] - c[3]);
+    } else if (vn[0] < 0.0) {
+        emf += 0.25 * (f[1] - c[0]);
+    } else {
+        emf += 0.125 * (f[3] - c[3] + f[1] - c[0]);
+    }
+    if (vn[1] > 0.0) {
+        emf += 0.25 * (f[2] - c[1]);
+    } else if (vn[1] < 0.0) {
+        emf += 0.25 * (f[0] - c[0]);
+    } else {
+        emf += 0.125 * (f[2] - c[1] + f[0] - c[0]);
+    }
+    if (vn[2] > 0.0) {
+        emf += 0.25 * (f[3] - c[2]);
+    } else if (vn[2] < 0.0) {
+        emf += 0.25 * (f[1] - c[1]);
+    } else {
+        emf += 0.125 * (f[3] - c[2] + f[1] - c[1]);
+    }
+    if (vn[3] > 0.0) {
+        emf += 0.25 * (f[2] - c[2]);
+    } else if (vn[3] < 0.0) {
+        emf += 0.25 * (f[0] - c[3]);
+    } else {
+        emf += 0.125 * (f[2] - c[2] + f[0] - c[3]);
+    }
+    return emf;
+}
+
+/* artificial CT resistivity of one cell, src/prj_timeint.c:222-262 */
+#define FX_ETA_BOOST 1.0e12
+#define FX_ETA_RHO_FLOOR 1.0e13
+#define FX_ETA_YE_THR 0.25
+
+__device__ __forceinline__ double fx_cell_eta(double rho, double ye)
+{
+    double rho_factor = 0.0;
+    double ye_factor = 0.0;
+    if (isfinite(rho) && rho > 0.0) {
+        rho_factor = fx_max(0.0, log(rho / FX_ETA_RHO_FLOOR));
+    }
+    if (isfinite(ye) && ye > 0.0) {
+        ye_factor = fx_max(0.0, log(ye / FX_ETA_YE_THR));
+    }
+    return FX_ETA_BOOST * rho_factor * ye_factor;
+}
+
+#endif

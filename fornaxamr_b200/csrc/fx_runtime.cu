@@ -1,0 +1,976 @@
+/*
+ * Context, device mirror, step sequencing and the C ABI of fornax_b200.
+ *
+ * Step sequence (prj_timeint_stage1/2, reference src/prj_timeint.c:2732-2973):
+ *   face fluxes -> coarse/fine flux correction -> edge EMFs -> coarse/fine
+ *   EMF correction -> CT face update -> cell update -> eos fill (active) ->
+ *   ghost fill (cells, faces, bf2bc) -> eos fill (mesh).
+ * FX_FORM_PLAIN launches the per-block phases once per block, in the
+ * reference's loop order, and writes every block array the reference writes
+ * (flux, v_riemann, Bv1/Bv2, emf, mhd_rhs, eosvar).  FX_FORM_BATCHED sweeps
+ * each phase over all blocks in one launch, skips the eosvar writes (eosvar
+ * is recomputed from W on download), and replays the whole step as one CUDA
+ * graph.
+ */
+#include <cuda_runtime.h>
+
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/fornax_b200.h"
+#include "fx_kernels.h"
+#include "fx_physics.cuh"
+#include "fx_plan.h"
+
+struct fx_ctx {
+    int device = 0;
+    fx_config cfg{};
+    int nv = 9;
+    cudaStream_t stream = nullptr;
+    std::string err;
+    int sticky = 0; /* a device-side physics failure was seen */
+
+    int nblocks = 0;
+    std::vector<fx_block_desc> blocks;
+    FxPlan plan;
+    FxDev D{};
+
+    FxBlockDev *d_blk = nullptr;
+    double *d_W = nullptr, *d_Bf = nullptr, *d_flux = nullptr, *d_vr = nullptr;
+    double *d_bv1 = nullptr, *d_bv2 = nullptr, *d_emf = nullptr, *d_eos = nullptr;
+    double *d_rhs = nullptr, *d_grav = nullptr;
+    int *d_ids = nullptr;
+    int *d_active = nullptr;
+    int nactive = 0;
+    FxGop *d_cops = nullptr, *d_fops = nullptr;
+    FxCorr *d_fcorr = nullptr, *d_ecorr = nullptr;
+
+    FxErr *d_err = nullptr;
+    unsigned long long *d_red = nullptr;
+    FxCtl *d_ctl = nullptr;
+    FxErr *h_err = nullptr;
+    unsigned long long *h_red = nullptr;
+    FxCtl *h_ctl = nullptr;
+
+    cudaGraphExec_t g_step = nullptr; /* batched RK2 step, dt from the control block */
+    cudaGraphExec_t g_run = nullptr;  /* batched driver step (calc_dt + step + dt update) */
+    int last_slot = 0;                /* W slot written by the last stage */
+};
+
+namespace {
+
+int set_err(fx_ctx *c, int code, const char *fmt, ...)
+{
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    if (c) c->err = buf;
+    return code;
+}
+
+#define FX_CUDA(c, call)                                                                   \
+    do {                                                                                    \
+        cudaError_t e_ = (call);                                                            \
+        if (e_ != cudaSuccess) {                                                            \
+            return set_err((c), FX_ECUDA, "%s: %s", #call, cudaGetErrorString(e_));        \
+        }                                                                                   \
+    } while (0)
+
+const char *err_message(int code)
+{
+    switch (code) {
+    case FX_ERR_HLLD_RHO: return "prj_riemann_hlld: non-positive density";
+    case FX_ERR_HLLD_P: return "prj_riemann_hlld: non-positive gas pressure";
+    case FX_ERR_HLLD_GAMMA: return "prj_riemann_hlld: non-positive adiabatic index";
+    case FX_ERR_HLLD_DISC: return "prj_riemann_hlld: negative fast-speed discriminant";
+    case FX_ERR_HLLD_CF: return "prj_riemann_hlld: invalid fast speed";
+    case FX_ERR_HLLD_ORDER: return "prj_riemann_hlld: invalid fast-wave ordering";
+    case FX_ERR_HLLD_DENOM: return "prj_riemann_hlld: degenerate contact-speed denominator";
+    case FX_ERR_HLLD_OUTER: return "prj_riemann_hlld: outer wave coincides with contact wave";
+    case FX_ERR_HLLD_STARRHO: return "prj_riemann_hlld: invalid star density";
+    case FX_ERR_HLLD_DSTAR: return "prj_riemann_hlld: invalid double-star density weights";
+    case FX_ERR_EMF_NONFINITE: return "prj_mhd_emf_upwind: non-finite input or result";
+    case FX_ERR_BF_NONFINITE: return "prj_timeint_mhd_ct_value: non-finite updated magnetic field";
+    case FX_ERR_EOS_ZERO_RHO: return "prj_eos_fill_block: zero density";
+    case FX_ERR_ETA: return "prj_timeint_mhd_fill_eta_mask: non-finite artificial eta";
+    case FX_ERR_B_NONFINITE: return "non-finite cell-centered magnetic field";
+    case FX_ERR_TIMEOUT: return "device wait timed out";
+    default: return "unknown device failure";
+    }
+}
+
+/* reads the device error word (the caller has synchronised) */
+int check_device_error(fx_ctx *c)
+{
+    if (c->sticky) {
+        return FX_EPHYSICS;
+    }
+    FX_CUDA(c, cudaMemcpy(c->h_err, c->d_err, sizeof(FxErr), cudaMemcpyDeviceToHost));
+    if (c->h_err->code != 0) {
+        c->sticky = 1;
+        return set_err(c, FX_EPHYSICS, "%s (block %d, index %d)", err_message(c->h_err->code),
+            c->h_err->block, c->h_err->index);
+    }
+    return FX_SUCCESS;
+}
+
+int sync_and_check(fx_ctx *c)
+{
+    FX_CUDA(c, cudaStreamSynchronize(c->stream));
+    return check_device_error(c);
+}
+
+template <typename T>
+int dev_alloc(fx_ctx *c, T **p, size_t count)
+{
+    if (*p) {
+        cudaFree(*p);
+        *p = nullptr;
+    }
+    if (count == 0) {
+        return FX_SUCCESS;
+    }
+    cudaError_t e = cudaMalloc((void **)p, count * sizeof(T));
+    if (e != cudaSuccess) {
+        *p = nullptr;
+        return set_err(c, FX_ENOMEM, "cudaMalloc of %zu bytes failed: %s", count * sizeof(T),
+            cudaGetErrorString(e));
+    }
+    return FX_SUCCESS;
+}
+
+void free_graphs(fx_ctx *c)
+{
+    if (c->g_step) {
+        cudaGraphExecDestroy(c->g_step);
+        c->g_step = nullptr;
+    }
+    if (c->g_run) {
+        cudaGraphExecDestroy(c->g_run);
+        c->g_run = nullptr;
+    }
+}
+
+void free_mesh(fx_ctx *c)
+{
+    free_graphs(c);
+    cudaFree(c->d_blk);
+    cudaFree(c->d_W);
+    cudaFree(c->d_Bf);
+    cudaFree(c->d_flux);
+    cudaFree(c->d_vr);
+    cudaFree(c->d_bv1);
+    cudaFree(c->d_bv2);
+    cudaFree(c->d_emf);
+    cudaFree(c->d_eos);
+    cudaFree(c->d_rhs);
+    cudaFree(c->d_grav);
+    cudaFree(c->d_ids);
+    cudaFree(c->d_active);
+    cudaFree(c->d_cops);
+    cudaFree(c->d_fops);
+    cudaFree(c->d_fcorr);
+    cudaFree(c->d_ecorr);
+    c->d_blk = nullptr;
+    c->d_W = c->d_Bf = c->d_flux = c->d_vr = c->d_bv1 = c->d_bv2 = nullptr;
+    c->d_emf = c->d_eos = c->d_rhs = c->d_grav = nullptr;
+    c->d_ids = c->d_active = nullptr;
+    c->d_cops = c->d_fops = nullptr;
+    c->d_fcorr = c->d_ecorr = nullptr;
+    c->nblocks = 0;
+    c->nactive = 0;
+}
+
+bool has_mesh(const fx_ctx *c) { return c && c->nblocks > 0 && c->d_W; }
+
+/* ---- phase sequencing ------------------------------------------------------ */
+
+template <typename F>
+void per_block(fx_ctx *c, int form, F &&fn)
+{
+    if (form == FX_FORM_PLAIN) {
+        for (int b : c->plan.active) {
+            fn(c->d_ids + b, 1);
+        }
+    } else {
+        fn(c->d_active, c->nactive);
+    }
+}
+
+void ghost_fill(fx_ctx *c, int form, int slot)
+{
+    const FxProgram &cp = c->plan.cells;
+    for (int w = 0; w < cp.nwaves(); ++w) {
+        fx_launch_ghost_cells(c->D, c->d_cops + cp.wave_begin[w], cp.wave_begin[w + 1] - cp.wave_begin[w],
+            slot, 6, c->stream);
+    }
+    if (c->cfg.mhd) {
+        const FxProgram &fp = c->plan.faces;
+        for (int w = 0; w < fp.nwaves(); ++w) {
+            fx_launch_ghost_faces(c->D, c->d_fops + fp.wave_begin[w],
+                fp.wave_begin[w + 1] - fp.wave_begin[w], slot, c->stream);
+        }
+        per_block(c, form, [&](const int *l, int n) { fx_launch_bf2bc(c->D, l, n, slot, c->stream); });
+    }
+}
+
+/* one RK2 stage; dt is read from the control block */
+void stage_seq(fx_ctx *c, int form, int stage)
+{
+    const int src = stage == 1 ? 0 : 1; /* W / Bf slot the fluxes read */
+    const int dst = stage == 1 ? 1 : 0; /* W slot the update writes */
+    cudaStream_t s = c->stream;
+    const int full = form == FX_FORM_PLAIN ? 1 : 0;
+    per_block(c, form, [&](const int *l, int n) {
+        for (int dir = 0; dir < 3; ++dir) {
+            fx_launch_flux(c->D, l, n, dir, src, src, full, s);
+        }
+    });
+    fx_launch_flux_correct(c->D, c->d_fcorr, (int)c->plan.flux_corr.size(), s);
+    if (c->cfg.mhd) {
+        per_block(c, form, [&](const int *l, int n) { fx_launch_emf(c->D, l, n, src, src, s); });
+        fx_launch_emf_correct(c->D, c->d_ecorr, (int)c->plan.emf_corr.size(), s);
+        per_block(c, form, [&](const int *l, int n) { fx_launch_bf_update(c->D, l, n, stage, s); });
+    }
+    per_block(c, form, [&](const int *l, int n) {
+        fx_launch_cell_update(c->D, l, n, stage, c->cfg.gravity, full, s);
+    });
+    if (form == FX_FORM_PLAIN) {
+        per_block(c, form, [&](const int *l, int n) { fx_launch_eos_fill(c->D, l, n, dst, 1, s); });
+    }
+    ghost_fill(c, form, dst);
+    if (form == FX_FORM_PLAIN) {
+        per_block(c, form, [&](const int *l, int n) { fx_launch_eos_fill(c->D, l, n, dst, 0, s); });
+    }
+    c->last_slot = dst;
+}
+
+int build_step_graph(fx_ctx *c)
+{
+    if (c->g_step) {
+        return FX_SUCCESS;
+    }
+    cudaGraph_t g;
+    FX_CUDA(c, cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+    fx_launch_reset_reductions(c->D, 2, c->stream);
+    stage_seq(c, FX_FORM_BATCHED, 1);
+    stage_seq(c, FX_FORM_BATCHED, 2);
+    FX_CUDA(c, cudaStreamEndCapture(c->stream, &g));
+    cudaError_t e = cudaGraphInstantiate(&c->g_step, g, 0);
+    cudaGraphDestroy(g);
+    FX_CUDA(c, e);
+    return FX_SUCCESS;
+}
+
+int build_run_graph(fx_ctx *c, double cfl)
+{
+    if (c->g_run) {
+        return FX_SUCCESS;
+    }
+    cudaGraph_t g;
+    FX_CUDA(c, cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+    fx_launch_reset_reductions(c->D, 1, c->stream);
+    fx_launch_calc_dt(c->D, c->d_active, c->nactive, 0, cfl, c->stream);
+    fx_launch_step_begin(c->D, c->stream);
+    stage_seq(c, FX_FORM_BATCHED, 1);
+    stage_seq(c, FX_FORM_BATCHED, 2);
+    fx_launch_step_end(c->D, c->stream);
+    FX_CUDA(c, cudaStreamEndCapture(c->stream, &g));
+    cudaError_t e = cudaGraphInstantiate(&c->g_run, g, 0);
+    cudaGraphDestroy(g);
+    FX_CUDA(c, e);
+    return FX_SUCCESS;
+}
+
+int read_dt_src(fx_ctx *c, double *dt_src)
+{
+    FX_CUDA(c, cudaMemcpyAsync(c->h_red, c->d_red, 2 * sizeof(unsigned long long),
+        cudaMemcpyDeviceToHost, c->stream));
+    int rc = sync_and_check(c);
+    if (rc) return rc;
+    *dt_src = fx_key_to_double(c->h_red[1]);
+    return FX_SUCCESS;
+}
+
+size_t w_count(const fx_ctx *c) { return (size_t)FX_W_COUNT(c->nv); }
+
+} /* namespace */
+
+/* ========================================================================== */
+/* C ABI                                                                      */
+/* ========================================================================== */
+
+extern "C" {
+
+int fx_create(int device, const fx_config *cfg, fx_ctx **out)
+{
+    if (!cfg || !out) {
+        return FX_EINVAL;
+    }
+    *out = nullptr;
+    if (cfg->mhd != 0 && cfg->mhd != 1) {
+        return FX_EINVAL;
+    }
+    if (!(cfg->gamma > 0.0)) {
+        return FX_EINVAL;
+    }
+    fx_ctx *c = new fx_ctx();
+    c->device = device;
+    c->cfg = *cfg;
+    c->nv = cfg->mhd ? 9 : 6;
+    if (cudaSetDevice(device) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaMalloc((void **)&c->d_err, sizeof(FxErr)) != cudaSuccess ||
+        cudaMalloc((void **)&c->d_red, 2 * sizeof(unsigned long long)) != cudaSuccess ||
+        cudaMalloc((void **)&c->d_ctl, sizeof(FxCtl)) != cudaSuccess ||
+        cudaMallocHost((void **)&c->h_err, sizeof(FxErr)) != cudaSuccess ||
+        cudaMallocHost((void **)&c->h_red, 2 * sizeof(unsigned long long)) != cudaSuccess ||
+        cudaMallocHost((void **)&c->h_ctl, sizeof(FxCtl)) != cudaSuccess) {
+        fx_destroy(c);
+        return FX_ECUDA;
+    }
+    cudaMemset(c->d_err, 0, sizeof(FxErr));
+    cudaMemset(c->d_ctl, 0, sizeof(FxCtl));
+    cudaMemset(c->d_red, 0, 2 * sizeof(unsigned long long));
+    c->D.nv = c->nv;
+    c->D.gamma = cfg->gamma;
+    c->D.mhd_eta = cfg->mhd_eta;
+    c->D.err = c->d_err;
+    c->D.red = c->d_red;
+    c->D.ctl = c->d_ctl;
+    *out = c;
+    return FX_SUCCESS;
+}
+
+void fx_destroy(fx_ctx *c)
+{
+    if (!c) {
+        return;
+    }
+    cudaSetDevice(c->device);
+    if (c->stream) {
+        cudaStreamSynchronize(c->stream);
+    }
+    free_mesh(c);
+    cudaFree(c->d_err);
+    cudaFree(c->d_red);
+    cudaFree(c->d_ctl);
+    cudaFreeHost(c->h_err);
+    cudaFreeHost(c->h_red);
+    cudaFreeHost(c->h_ctl);
+    if (c->stream) {
+        cudaStreamDestroy(c->stream);
+    }
+    delete c;
+}
+
+int fx_last_error(const fx_ctx *c, char *buf, size_t len)
+{
+    if (!c || !buf || len == 0) {
+        return FX_EINVAL;
+    }
+    snprintf(buf, len, "%s", c->err.c_str());
+    return FX_SUCCESS;
+}
+
+int fx_sync(fx_ctx *c)
+{
+    if (!c) return FX_EINVAL;
+    return sync_and_check(c);
+}
+
+int fx_stream(fx_ctx *c, void **stream)
+{
+    if (!c || !stream) return FX_EINVAL;
+    *stream = (void *)c->stream;
+    return FX_SUCCESS;
+}
+
+int fx_set_mesh(fx_ctx *c, int nblocks, const fx_block_desc *blocks)
+{
+    if (!c || nblocks <= 0 || !blocks) {
+        return c ? set_err(c, FX_EINVAL, "fx_set_mesh: empty mesh") : FX_EINVAL;
+    }
+    if (nblocks >= (1 << 16)) {
+        return set_err(c, FX_EINVAL, "fx_set_mesh: at most 65535 blocks per device");
+    }
+    FX_CUDA(c, cudaSetDevice(c->device));
+    FX_CUDA(c, cudaStreamSynchronize(c->stream));
+    free_mesh(c);
+    std::string perr;
+    FxPlan plan;
+    if (!fx_build_plan(c->cfg, nblocks, blocks, plan, &perr)) {
+        return set_err(c, FX_EINVAL, "fx_set_mesh: %s", perr.c_str());
+    }
+    c->plan = std::move(plan);
+    c->blocks.assign(blocks, blocks + nblocks);
+    c->nblocks = nblocks;
+    c->nactive = (int)c->plan.active.size();
+
+    std::vector<FxBlockDev> hb(nblocks);
+    for (int b = 0; b < nblocks; ++b) {
+        for (int a = 0; a < 3; ++a) {
+            hb[b].xmin[a] = blocks[b].xmin[a];
+            hb[b].dx[a] = blocks[b].dx[a];
+            hb[b].area[a] = blocks[b].area[a];
+        }
+        hb[b].vol = blocks[b].vol;
+    }
+    std::vector<int> ids(nblocks);
+    for (int b = 0; b < nblocks; ++b) ids[b] = b;
+
+    const size_t nb = (size_t)nblocks;
+    int rc;
+    if ((rc = dev_alloc(c, &c->d_blk, nb))) return rc;
+    if ((rc = dev_alloc(c, &c->d_W, nb * w_count(c)))) return rc;
+    if ((rc = dev_alloc(c, &c->d_flux, nb * FX_FLUX_COUNT(c->nv)))) return rc;
+    if ((rc = dev_alloc(c, &c->d_vr, nb * FX_VR_COUNT))) return rc;
+    if ((rc = dev_alloc(c, &c->d_eos, nb * FX_EOS_COUNT))) return rc;
+    if ((rc = dev_alloc(c, &c->d_rhs, nb * FX_RHS_COUNT(c->nv)))) return rc;
+    if (c->cfg.mhd) {
+        if ((rc = dev_alloc(c, &c->d_Bf, nb * FX_BF_COUNT))) return rc;
+        if ((rc = dev_alloc(c, &c->d_bv1, nb * FX_BV_COUNT))) return rc;
+        if ((rc = dev_alloc(c, &c->d_bv2, nb * FX_BV_COUNT))) return rc;
+        if ((rc = dev_alloc(c, &c->d_emf, nb * FX_EMF_COUNT))) return rc;
+    }
+    if (c->cfg.gravity) {
+        if ((rc = dev_alloc(c, &c->d_grav, nb * FX_GRAV_COUNT))) return rc;
+        FX_CUDA(c, cudaMemset(c->d_grav, 0, nb * FX_GRAV_COUNT * sizeof(double)));
+    }
+    if ((rc = dev_alloc(c, &c->d_ids, nb))) return rc;
+    if ((rc = dev_alloc(c, &c->d_active, (size_t)c->nactive))) return rc;
+    if ((rc = dev_alloc(c, &c->d_cops, c->plan.cells.ops.size()))) return rc;
+    if ((rc = dev_alloc(c, &c->d_fops, c->plan.faces.ops.size()))) return rc;
+    if ((rc = dev_alloc(c, &c->d_fcorr, c->plan.flux_corr.size()))) return rc;
+    if ((rc = dev_alloc(c, &c->d_ecorr, c->plan.emf_corr.size()))) return rc;
+
+    /* scratch starts at zero so downloads of never-written entries are defined */
+    FX_CUDA(c, cudaMemset(c->d_W, 0, nb * w_count(c) * sizeof(double)));
+    FX_CUDA(c, cudaMemset(c->d_flux, 0, nb * FX_FLUX_COUNT(c->nv) * sizeof(double)));
+    FX_CUDA(c, cudaMemset(c->d_vr, 0, nb * FX_VR_COUNT * sizeof(double)));
+    FX_CUDA(c, cudaMemset(c->d_eos, 0, nb * FX_EOS_COUNT * sizeof(double)));
+    FX_CUDA(c, cudaMemset(c->d_rhs, 0, nb * FX_RHS_COUNT(c->nv) * sizeof(double)));
+    if (c->cfg.mhd) {
+        FX_CUDA(c, cudaMemset(c->d_Bf, 0, nb * FX_BF_COUNT * sizeof(double)));
+        FX_CUDA(c, cudaMemset(c->d_bv1, 0, nb * FX_BV_COUNT * sizeof(double)));
+        FX_CUDA(c, cudaMemset(c->d_bv2, 0, nb * FX_BV_COUNT * sizeof(double)));
+        FX_CUDA(c, cudaMemset(c->d_emf, 0, nb * FX_EMF_COUNT * sizeof(double)));
+    }
+    FX_CUDA(c, cudaMemcpy(c->d_blk, hb.data(), nb * sizeof(FxBlockDev), cudaMemcpyHostToDevice));
+    FX_CUDA(c, cudaMemcpy(c->d_ids, ids.data(), nb * sizeof(int), cudaMemcpyHostToDevice));
+    if (c->nactive) {
+        FX_CUDA(c, cudaMemcpy(c->d_active, c->plan.active.data(), (size_t)c->nactive * sizeof(int),
+            cudaMemcpyHostToDevice));
+    }
+    if (!c->plan.cells.ops.empty()) {
+        FX_CUDA(c, cudaMemcpy(c->d_cops, c->plan.cells.ops.data(), c->plan.cells.ops.size() * sizeof(FxGop),
+            cudaMemcpyHostToDevice));
+    }
+    if (!c->plan.faces.ops.empty()) {
+        FX_CUDA(c, cudaMemcpy(c->d_fops, c->plan.faces.ops.data(), c->plan.faces.ops.size() * sizeof(FxGop),
+            cudaMemcpyHostToDevice));
+    }
+    if (!c->plan.flux_corr.empty()) {
+        FX_CUDA(c, cudaMemcpy(c->d_fcorr, c->plan.flux_corr.data(), c->plan.flux_corr.size() * sizeof(FxCorr),
+            cudaMemcpyHostToDevice));
+    }
+    if (!c->plan.emf_corr.empty()) {
+        FX_CUDA(c, cudaMemcpy(c->d_ecorr, c->plan.emf_corr.data(), c->plan.emf_corr.size() * sizeof(FxCorr),
+            cudaMemcpyHostToDevice));
+    }
+    c->D.nblocks = nblocks;
+    c->D.blk = c->d_blk;
+    c->D.W = c->d_W;
+    c->D.Bf = c->d_Bf;
+    c->D.flux = c->d_flux;
+    c->D.vr = c->d_vr;
+    c->D.bv1 = c->d_bv1;
+    c->D.bv2 = c->d_bv2;
+    c->D.emf = c->d_emf;
+    c->D.eos = c->d_eos;
+    c->D.rhs = c->d_rhs;
+    c->D.grav = c->d_grav;
+    c->last_slot = 0;
+    return FX_SUCCESS;
+}
+
+int fx_plan_export(const fx_config *cfg, int nblocks, const fx_block_desc *blocks, int which,
+    int32_t *ops, int *nops, int32_t *wave_begin, int *nwaves)
+{
+    if (!cfg || nblocks <= 0 || !blocks || !nops || !nwaves || which < 0 || which > 3) {
+        return FX_EINVAL;
+    }
+    FxPlan plan;
+    std::string perr;
+    if (!fx_build_plan(*cfg, nblocks, blocks, plan, &perr)) {
+        return FX_EINVAL;
+    }
+    if (which <= 1) {
+        const FxProgram &p = which == 0 ? plan.cells : plan.faces;
+        if (ops && (int)p.ops.size() <= *nops) {
+            std::memcpy(ops, p.ops.data(), p.ops.size() * sizeof(FxGop));
+        }
+        if (wave_begin && p.nwaves() <= *nwaves) {
+            std::memcpy(wave_begin, p.wave_begin.data(), p.wave_begin.size() * sizeof(int));
+        }
+        *nops = (int)p.ops.size();
+        *nwaves = p.nwaves();
+    } else {
+        const std::vector<FxCorr> &r = which == 2 ? plan.flux_corr : plan.emf_corr;
+        if (ops && (int)r.size() <= *nops) {
+            std::memcpy(ops, r.data(), r.size() * sizeof(FxCorr));
+        }
+        *nops = (int)r.size();
+        *nwaves = 0;
+    }
+    return FX_SUCCESS;
+}
+
+int fx_upload_block(fx_ctx *c, int b, const double *W, const double *const Bf[3],
+    const double *const grav[3])
+{
+    if (!has_mesh(c)) return c ? set_err(c, FX_ENOMESH, "no mesh") : FX_EINVAL;
+    if (b < 0 || b >= c->nblocks) return set_err(c, FX_EINVAL, "block %d out of range", b);
+    if (W) {
+        FX_CUDA(c, cudaMemcpyAsync(c->d_W + (size_t)b * w_count(c), W, w_count(c) * sizeof(double),
+            cudaMemcpyHostToDevice, c->stream));
+    }
+    if (Bf && c->cfg.mhd) {
+        for (int d = 0; d < 3; ++d) {
+            if (Bf[d]) {
+                FX_CUDA(c, cudaMemcpyAsync(c->d_Bf + (size_t)b * FX_BF_COUNT + (size_t)d * FX_NSTAGES * FX_NFACES,
+                    Bf[d], (size_t)FX_NSTAGES * FX_NFACES * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+            }
+        }
+    }
+    if (grav && c->d_grav) {
+        for (int d = 0; d < 3; ++d) {
+            if (grav[d]) {
+                FX_CUDA(c, cudaMemcpyAsync(c->d_grav + (size_t)b * FX_GRAV_COUNT + (size_t)d * FX_NCELLS,
+                    grav[d], (size_t)FX_NCELLS * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+            }
+        }
+    }
+    FX_CUDA(c, cudaStreamSynchronize(c->stream));
+    return FX_SUCCESS;
+}
+
+int fx_download_block(fx_ctx *c, int b, double *W, double *eosvar, double *const Bf[3])
+{
+    if (!has_mesh(c)) return c ? set_err(c, FX_ENOMESH, "no mesh") : FX_EINVAL;
+    if (b < 0 || b >= c->nblocks) return set_err(c, FX_EINVAL, "block %d out of range", b);
+    if (W) {
+        FX_CUDA(c, cudaMemcpyAsync(W, c->d_W + (size_t)b * w_count(c), w_count(c) * sizeof(double),
+            cudaMemcpyDeviceToHost, c->stream));
+    }
+    if (eosvar) {
+        fx_launch_eos_fill(c->D, c->d_ids + b, 1, c->last_slot, 0, c->stream);
+        FX_CUDA(c, cudaMemcpyAsync(eosvar, c->d_eos + (size_t)b * FX_EOS_COUNT, FX_EOS_COUNT * sizeof(double),
+            cudaMemcpyDeviceToHost, c->stream));
+    }
+    if (Bf && c->cfg.mhd) {
+        for (int d = 0; d < 3; ++d) {
+            if (Bf[d]) {
+                FX_CUDA(c, cudaMemcpyAsync(Bf[d], c->d_Bf + (size_t)b * FX_BF_COUNT + (size_t)d * FX_NSTAGES * FX_NFACES,
+                    (size_t)FX_NSTAGES * FX_NFACES * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+            }
+        }
+    }
+    return sync_and_check(c);
+}
+
+int fx_upload_all(fx_ctx *c, const double *W_all, const double *Bf_all)
+{
+    if (!has_mesh(c)) return c ? set_err(c, FX_ENOMESH, "no mesh") : FX_EINVAL;
+    const size_t nb = (size_t)c->nblocks;
+    if (W_all) {
+        FX_CUDA(c, cudaMemcpyAsync(c->d_W, W_all, nb * w_count(c) * sizeof(double), cudaMemcpyHostToDevice,
+            c->stream));
+    }
+    if (Bf_all && c->cfg.mhd) {
+        FX_CUDA(c, cudaMemcpyAsync(c->d_Bf, Bf_all, nb * FX_BF_COUNT * sizeof(double), cudaMemcpyHostToDevice,
+            c->stream));
+    }
+    return FX_SUCCESS;
+}
+
+int fx_download_all(fx_ctx *c, double *W_all, double *Bf_all)
+{
+    if (!has_mesh(c)) return c ? set_err(c, FX_ENOMESH, "no mesh") : FX_EINVAL;
+    const size_t nb = (size_t)c->nblocks;
+    if (W_all) {
+        FX_CUDA(c, cudaMemcpyAsync(W_all, c->d_W, nb * w_count(c) * sizeof(double), cudaMemcpyDeviceToHost,
+            c->stream));
+    }
+    if (Bf_all && c->cfg.mhd) {
+        FX_CUDA(c, cudaMemcpyAsync(Bf_all, c->d_Bf, nb * FX_BF_COUNT * sizeof(double), cudaMemcpyDeviceToHost,
+            c->stream));
+    }
+    return sync_and_check(c);
+}
+
+/* slot-0 rows: W is [b][v][slot][cell], Bf is [b][d][slot][face] */
+static int copy_state(fx_ctx *c, double *dW, const double *sW, double *dB, const double *sB,
+    cudaMemcpyKind kind)
+{
+    const size_t nb = (size_t)c->nblocks;
+    if (dW && sW) {
+        FX_CUDA(c, cudaMemcpy2DAsync(dW, 2 * FX_NCELLS * sizeof(double), sW, 2 * FX_NCELLS * sizeof(double),
+            FX_NCELLS * sizeof(double), nb * (size_t)c->nv, kind, c->stream));
+    }
+    if (dB && sB && c->cfg.mhd) {
+        FX_CUDA(c, cudaMemcpy2DAsync(dB, 2 * FX_NFACES * sizeof(double), sB, 2 * FX_NFACES * sizeof(double),
+            FX_NFACES * sizeof(double), nb * 3, kind, c->stream));
+    }
+    return FX_SUCCESS;
+}
+
+int fx_upload_state(fx_ctx *c, const double *W_all, const double *Bf_all)
+{
+    if (!has_mesh(c)) return c ? set_err(c, FX_ENOMESH, "no mesh") : FX_EINVAL;
+    return copy_state(c, c->d_W, W_all, c->d_Bf, Bf_all, cudaMemcpyHostToDevice);
+}
+
+int fx_download_state(fx_ctx *c, double *W_all, double *Bf_all)
+{
+    if (!has_mesh(c)) return c ? set_err(c, FX_ENOMESH, "no mesh") : FX_EINVAL;
+    int rc = copy_state(c, W_all, c->d_W, Bf_all, c->d_Bf, cudaMemcpyDeviceToHost);
+    if (rc) return rc;
+    return FX_SUCCESS;
+}
+
+int fx_download_array(fx_ctx *c, int b, int which, int dir, double *out)
+{
+    if (!has_mesh(c)) return c ? set_err(c, FX_ENOMESH, "no mesh") : FX_EINVAL;
+    if (b < 0 || b >= c->nblocks || dir < 0 || dir > 2 || !out) {
+        return set_err(c, FX_EINVAL, "fx_download_array: bad arguments");
+    }
+    const double *src = nullptr;
+    size_t count = 0;
+    const size_t nv = (size_t)c->nv;
+    switch (which) {
+    case FX_ARR_W: src = c->d_W + (size_t)b * w_count(c); count = w_count(c); break;
+    case FX_ARR_EOSVAR: src = c->d_eos + (size_t)b * FX_EOS_COUNT; count = FX_EOS_COUNT; break;
+    case FX_ARR_RHS: src = c->d_rhs + (size_t)b * FX_RHS_COUNT(nv); count = FX_RHS_COUNT(nv); break;
+    case FX_ARR_FLUX: src = c->d_flux + (size_t)b * FX_FLUX_COUNT(nv) + (size_t)dir * nv * FX_NCELLS;
+        count = nv * FX_NCELLS; break;
+    case FX_ARR_VRIEMANN: src = c->d_vr + (size_t)b * FX_VR_COUNT + (size_t)dir * 3 * FX_NCELLS;
+        count = 3 * FX_NCELLS; break;
+    case FX_ARR_GRAV:
+        if (!c->d_grav) return set_err(c, FX_EINVAL, "no gravity arrays");
+        src = c->d_grav + (size_t)b * FX_GRAV_COUNT + (size_t)dir * FX_NCELLS; count = FX_NCELLS; break;
+    case FX_ARR_BF:
+    case FX_ARR_BV1:
+    case FX_ARR_BV2:
+    case FX_ARR_EMF:
+        if (!c->cfg.mhd) return set_err(c, FX_EINVAL, "field arrays exist only in MHD runs");
+        if (which == FX_ARR_BF) {
+            src = c->d_Bf + (size_t)b * FX_BF_COUNT + (size_t)dir * FX_NSTAGES * FX_NFACES;
+            count = (size_t)FX_NSTAGES * FX_NFACES;
+        } else if (which == FX_ARR_EMF) {
+            src = c->d_emf + (size_t)b * FX_EMF_COUNT + (size_t)dir * FX_NEDGES;
+            count = FX_NEDGES;
+        } else {
+            src = (which == FX_ARR_BV1 ? c->d_bv1 : c->d_bv2) + (size_t)b * FX_BV_COUNT + (size_t)dir * FX_NCELLS;
+            count = FX_NCELLS;
+        }
+        break;
+    default:
+        return set_err(c, FX_EINVAL, "fx_download_array: unknown array %d", which);
+    }
+    FX_CUDA(c, cudaMemcpyAsync(out, src, count * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    return sync_and_check(c);
+}
+
+/* ---- per-block reference entry points ---------------------------------------- */
+
+static int check_block(fx_ctx *c, int b)
+{
+    if (!has_mesh(c)) return c ? set_err(c, FX_ENOMESH, "no mesh") : FX_EINVAL;
+    if (b < 0 || b >= c->nblocks) return set_err(c, FX_EINVAL, "block %d out of range", b);
+    return FX_SUCCESS;
+}
+
+int fx_flux_update(fx_ctx *c, int b, int w_slot, int use_bf1)
+{
+    int rc = check_block(c, b);
+    if (rc) return rc;
+    if (w_slot < 0 || w_slot > 1 || use_bf1 < 0 || use_bf1 > 1) return set_err(c, FX_EINVAL, "bad slot");
+    fx_launch_set_dt(c->D, 0.0, c->stream);
+    for (int dir = 0; dir < 3; ++dir) {
+        fx_launch_flux(c->D, c->d_ids + b, 1, dir, w_slot, use_bf1, 1, c->stream);
+    }
+    return FX_SUCCESS;
+}
+
+int fx_mhd_update_emf(fx_ctx *c, int b, int stage)
+{
+    int rc = check_block(c, b);
+    if (rc) return rc;
+    if (!c->cfg.mhd || stage < 0 || stage > 1) return set_err(c, FX_EINVAL, "bad emf call");
+    fx_launch_set_dt(c->D, 0.0, c->stream);
+    fx_launch_emf(c->D, c->d_ids + b, 1, stage, stage, c->stream);
+    return FX_SUCCESS;
+}
+
+int fx_mhd_update_bf(fx_ctx *c, int b, int stage, double dt)
+{
+    int rc = check_block(c, b);
+    if (rc) return rc;
+    if (!c->cfg.mhd || (stage != 1 && stage != 2)) return set_err(c, FX_EINVAL, "bad bf update call");
+    fx_launch_set_dt(c->D, dt, c->stream);
+    fx_launch_bf_update(c->D, c->d_ids + b, 1, stage, c->stream);
+    return FX_SUCCESS;
+}
+
+int fx_update_cells(fx_ctx *c, int b, int stage, double dt, double *dt_src)
+{
+    int rc = check_block(c, b);
+    if (rc) return rc;
+    if (stage != 1 && stage != 2) return set_err(c, FX_EINVAL, "bad stage");
+    fx_launch_set_dt(c->D, dt, c->stream);
+    if (dt_src) fx_launch_reset_reductions(c->D, 2, c->stream);
+    fx_launch_cell_update(c->D, c->d_ids + b, 1, stage, c->cfg.gravity, 1, c->stream);
+    c->last_slot = stage == 1 ? 1 : 0;
+    if (dt_src) {
+        double v;
+        rc = read_dt_src(c, &v);
+        if (rc) return rc;
+        if (v < *dt_src) *dt_src = v;
+    }
+    return FX_SUCCESS;
+}
+
+int fx_riemann_flux_send(fx_ctx *c)
+{
+    if (!has_mesh(c)) return c ? set_err(c, FX_ENOMESH, "no mesh") : FX_EINVAL;
+    fx_launch_set_dt(c->D, 0.0, c->stream);
+    fx_launch_flux_correct(c->D, c->d_fcorr, (int)c->plan.flux_corr.size(), c->stream);
+    return FX_SUCCESS;
+}
+
+int fx_mhd_emf_send(fx_ctx *c)
+{
+    if (!has_mesh(c)) return c ? set_err(c, FX_ENOMESH, "no mesh") : FX_EINVAL;
+    fx_launch_set_dt(c->D, 0.0, c->stream);
+    fx_launch_emf_correct(c->D, c->d_ecorr, (int)c->plan.emf_corr.size(), c->stream);
+    return FX_SUCCESS;
+}
+
+int fx_eos_fill_active_cells(fx_ctx *c, int stage)
+{
+    if (!has_mesh(c)) return c ? set_err(c, FX_ENOMESH, "no mesh") : FX_EINVAL;
+    const int slot = stage > 0 ? stage - 1 : 0;
+    if (slot > 1) return set_err(c, FX_EINVAL, "bad stage");
+    fx_launch_set_dt(c->D, 0.0, c->stream);
+    fx_launch_eos_fill(c->D, c->d_active, c->nactive, slot, 1, c->stream);
+    return FX_SUCCESS;
+}
+
+int fx_eos_fill_mesh(fx_ctx *c, int stage)
+{
+    if (!has_mesh(c)) return c ? set_err(c, FX_ENOMESH, "no mesh") : FX_EINVAL;
+    const int slot = stage > 0 ? stage - 1 : 0;
+    if (slot > 1) return set_err(c, FX_EINVAL, "bad stage");
+    fx_launch_set_dt(c->D, 0.0, c->stream);
+    fx_launch_eos_fill(c->D, c->d_active, c->nactive, slot, 0, c->stream);
+    return FX_SUCCESS;
+}
+
+int fx_boundary_fill_ghosts_and_bf(fx_ctx *c, int stage, int use_bf1)
+{
+    if (!has_mesh(c)) return c ? set_err(c, FX_ENOMESH, "no mesh") : FX_EINVAL;
+    const int slot = stage > 0 ? stage - 1 : 0;
+    if (slot > 1 || use_bf1 < 0 || use_bf1 > 1) return set_err(c, FX_EINVAL, "bad stage");
+    if (c->cfg.mhd && slot != use_bf1) {
+        return set_err(c, FX_EINVAL, "fx_boundary_fill_ghosts_and_bf: W slot and Bf slot must agree");
+    }
+    fx_launch_set_dt(c->D, 0.0, c->stream);
+    ghost_fill(c, FX_FORM_BATCHED, slot);
+    return FX_SUCCESS;
+}
+
+/* ---- time integration ----------------------------------------------------------- */
+
+int fx_calc_dt(fx_ctx *c, double cfl, double *dt)
+{
+    if (!has_mesh(c)) return c ? set_err(c, FX_ENOMESH, "no mesh") : FX_EINVAL;
+    if (!dt) return set_err(c, FX_EINVAL, "null dt");
+    fx_launch_reset_reductions(c->D, 1, c->stream);
+    fx_launch_calc_dt(c->D, c->d_active, c->nactive, 0, cfl, c->stream);
+    FX_CUDA(c, cudaMemcpyAsync(c->h_red, c->d_red, 2 * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+        c->stream));
+    int rc = sync_and_check(c);
+    if (rc) return rc;
+    *dt = fx_key_to_double(c->h_red[0]);
+    return FX_SUCCESS;
+}
+
+int fx_stage(fx_ctx *c, int form, int stage, double dt, double *dt_src)
+{
+    if (!has_mesh(c)) return c ? set_err(c, FX_ENOMESH, "no mesh") : FX_EINVAL;
+    if ((form != FX_FORM_PLAIN && form != FX_FORM_BATCHED) || (stage != 1 && stage != 2)) {
+        return set_err(c, FX_EINVAL, "fx_stage: bad form or stage");
+    }
+    fx_launch_set_dt(c->D, dt, c->stream);
+    fx_launch_reset_reductions(c->D, 2, c->stream);
+    stage_seq(c, form, stage);
+    if (dt_src) return read_dt_src(c, dt_src);
+    return FX_SUCCESS;
+}
+
+int fx_step(fx_ctx *c, int form, double dt, double *dt_src)
+{
+    if (!has_mesh(c)) return c ? set_err(c, FX_ENOMESH, "no mesh") : FX_EINVAL;
+    if (form != FX_FORM_PLAIN && form != FX_FORM_BATCHED) {
+        return set_err(c, FX_EINVAL, "fx_step: bad form");
+    }
+    if (c->sticky) return FX_EPHYSICS;
+    fx_launch_set_dt(c->D, dt, c->stream);
+    if (form == FX_FORM_PLAIN) {
+        fx_launch_reset_reductions(c->D, 2, c->stream);
+        stage_seq(c, form, 1);
+        stage_seq(c, form, 2);
+    } else {
+        int rc = build_step_graph(c);
+        if (rc) return rc;
+        FX_CUDA(c, cudaGraphLaunch(c->g_step, c->stream));
+        c->last_slot = 0;
+    }
+    if (dt_src) return read_dt_src(c, dt_src);
+    return FX_SUCCESS;
+}
+
+int fx_run(fx_ctx *c, int form, int nsteps, double cfl, double dt_factor, double t_end, double *state)
+{
+    if (!has_mesh(c)) return c ? set_err(c, FX_ENOMESH, "no mesh") : FX_EINVAL;
+    if (!state || nsteps < 0) return set_err(c, FX_EINVAL, "fx_run: bad arguments");
+    if (form == FX_FORM_PLAIN) {
+        double time = state[0], dt = state[1];
+        long long step = (long long)state[2];
+        for (int n = 0; n < nsteps && time < t_end; ++n) {
+            double dt_new;
+            int rc = fx_calc_dt(c, cfl, &dt_new);
+            if (rc) return rc;
+            if (dt > 0.0) {
+                const double dt_limit = dt_factor * dt;
+                dt = dt_new <= dt_limit ? dt_new : dt_limit;
+            } else {
+                dt = dt_new;
+            }
+            double dt_step = dt;
+            if (time + dt_step > t_end) dt_step = t_end - time;
+            double dt_src = 1.0e100;
+            rc = fx_step(c, FX_FORM_PLAIN, dt_step, &dt_src);
+            if (rc) return rc;
+            if (cfl * dt_src < dt) dt = cfl * dt_src;
+            time += dt_step;
+            step += 1;
+        }
+        state[0] = time;
+        state[1] = dt;
+        state[2] = (double)step;
+        return FX_SUCCESS;
+    }
+    if (form != FX_FORM_BATCHED) return set_err(c, FX_EINVAL, "fx_run: bad form");
+    if (c->g_run && c->h_ctl->cfl != cfl) {
+        free_graphs(c);
+    }
+    FxCtl v{};
+    v.time = state[0];
+    v.dt_prev = state[1];
+    v.step = (long long)state[2];
+    v.cfl = cfl;
+    v.dt_factor = dt_factor;
+    v.t_end = t_end;
+    v.dt_src = 1.0e100;
+    *c->h_ctl = v;
+    fx_launch_set_ctl(c->D, v, c->stream);
+    int rc = build_run_graph(c, cfl);
+    if (rc) return rc;
+    for (int n = 0; n < nsteps; ++n) {
+        FX_CUDA(c, cudaGraphLaunch(c->g_run, c->stream));
+    }
+    c->last_slot = 0;
+    FX_CUDA(c, cudaMemcpyAsync(c->h_ctl, c->d_ctl, sizeof(FxCtl), cudaMemcpyDeviceToHost, c->stream));
+    rc = sync_and_check(c);
+    if (rc) return rc;
+    state[0] = c->h_ctl->time;
+    state[1] = c->h_ctl->dt_prev;
+    state[2] = (double)c->h_ctl->step;
+    c->h_ctl->cfl = cfl;
+    return FX_SUCCESS;
+}
+
+int fx_time_phase(fx_ctx *c, int phase, int reps, double dt, double *ms)
+{
+    if (!has_mesh(c)) return c ? set_err(c, FX_ENOMESH, "no mesh") : FX_EINVAL;
+    if (!ms || reps <= 0 || phase < 0 || phase > FX_PHASE_STEP) return set_err(c, FX_EINVAL, "bad phase");
+    if ((phase == FX_PHASE_EMF || phase == FX_PHASE_CT) && !c->cfg.mhd) {
+        return set_err(c, FX_EINVAL, "phase needs an MHD run");
+    }
+    if (phase == FX_PHASE_STEP) {
+        int rc = build_step_graph(c);
+        if (rc) return rc;
+    }
+    cudaStream_t s = c->stream;
+    auto launch = [&]() {
+        switch (phase) {
+        case FX_PHASE_FLUX: fx_launch_flux(c->D, c->d_active, c->nactive, 0, 0, 0, 0, s); break;
+        case FX_PHASE_EMF: fx_launch_emf(c->D, c->d_active, c->nactive, 0, 0, s); break;
+        case FX_PHASE_CT: fx_launch_bf_update(c->D, c->d_active, c->nactive, 1, s); break;
+        case FX_PHASE_CELLS: fx_launch_cell_update(c->D, c->d_active, c->nactive, 1, c->cfg.gravity, 0, s); break;
+        case FX_PHASE_GHOST: ghost_fill(c, FX_FORM_BATCHED, 1); break;
+        default: cudaGraphLaunch(c->g_step, s); break;
+        }
+    };
+    fx_launch_set_dt(c->D, dt, s);
+    launch();
+    cudaEvent_t e0, e1;
+    FX_CUDA(c, cudaEventCreate(&e0));
+    FX_CUDA(c, cudaEventCreate(&e1));
+    FX_CUDA(c, cudaEventRecord(e0, s));
+    for (int r = 0; r < reps; ++r) {
+        launch();
+    }
+    FX_CUDA(c, cudaEventRecord(e1, s));
+    FX_CUDA(c, cudaEventSynchronize(e1));
+    float t = 0.0f;
+    FX_CUDA(c, cudaEventElapsedTime(&t, e0, e1));
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    *ms = (double)t / reps;
+    if (phase == FX_PHASE_STEP) c->last_slot = 0;
+    return check_device_error(c);
+}
+
+int fx_info(fx_ctx *c, int what, long long *value)
+{
+    if (!has_mesh(c) || !value) return c ? set_err(c, FX_EINVAL, "fx_info: no mesh") : FX_EINVAL;
+    const long long cw = c->plan.cells.nwaves();
+    const long long fw = c->cfg.mhd ? c->plan.faces.nwaves() : 0;
+    const long long corr = (c->plan.flux_corr.empty() ? 0 : 1) +
+        (c->cfg.mhd && !c->plan.emf_corr.empty() ? 1 : 0);
+    const long long mhd = c->cfg.mhd ? 1 : 0;
+    switch (what) {
+    case 0: /* reset + 2 x (3 flux + emf + ct + cells + waves + bf2bc) */
+        *value = 1 + 2 * (3 + 2 * mhd + 1 + corr + cw + fw + mhd);
+        break;
+    case 1: /* set_dt + reset + 2 x per-block phases + mesh-level ghost waves */
+        *value = 2 + 2 * ((long long)c->nactive * (3 + 2 * mhd + 1 + 2 + mhd) + corr + cw + fw);
+        break;
+    case 2: *value = (long long)c->plan.cells.ops.size(); break;
+    case 3: *value = (long long)c->plan.faces.ops.size(); break;
+    case 4: *value = cw; break;
+    case 5: *value = fw; break;
+    default: return set_err(c, FX_EINVAL, "fx_info: unknown query");
+    }
+    return FX_SUCCESS;
+}
+
+} /* extern "C" */

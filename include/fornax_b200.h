@@ -1,0 +1,226 @@
+/*
+ * fornax_b200 -- B200 (sm_100a) implementation of FornaxAMR's per-block
+ * Godunov MHD update behind a plain C ABI.
+ *
+ * The library keeps a device mirror of a FornaxAMR mesh: for every block the
+ * primitive array W_mhd (2 RK stages), the face field Bf (2 stages) and the
+ * static gravity array, in exactly the reference's per-block layout
+ * (reference src/prj_defs.h:383-453), plus device-side scratch in the same
+ * layout for flux, v_riemann, Bv1/Bv2, emf, eosvar and mhd_rhs.  A host that
+ * owns prj_block data uploads it once, steps on the device, and downloads
+ * when it needs the state (I/O, diagnostics).
+ *
+ * Build variants of the reference map onto run-time settings:
+ *   PRJ_MHD=1 -> fx_config.mhd = 1 (NHYDRO = 9, HLLD, constrained transport)
+ *   PRJ_MHD=0 -> fx_config.mhd = 0 (NHYDRO = 6, HLLC)
+ * Fixed: PRJ_BLOCK_SIZE = 16, PRJ_NGHOST = 2, RECON = MC, TIME_INTEGRATION =
+ * RK2, ideal-gas EOS with a run-time adiabatic index, no radiation, no GR.
+ *
+ * Every entry point returns 0 on success and a positive FX_E* code on
+ * failure; fx_last_error() returns the message.  Device-side physics
+ * failures (the reference's exit(1) paths) are reported by the next call
+ * that synchronises (fx_sync, fx_step, fx_calc_dt, downloads) with
+ * FX_EPHYSICS and the reference's message text.
+ *
+ * Threading: one context per host thread and device; calls on a context are
+ * not thread-safe (the reference's hot path is single-threaded per rank and
+ * keeps non-reentrant static scratch, src/prj_flux.c:385, 2155-2171).
+ */
+#ifndef FORNAX_B200_H
+#define FORNAX_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define FX_API_VERSION 1
+
+/* return codes */
+#define FX_SUCCESS 0
+#define FX_EINVAL 1     /* bad argument */
+#define FX_ECUDA 2      /* CUDA runtime error */
+#define FX_ENOMESH 3    /* no mesh set */
+#define FX_EPHYSICS 4   /* device-side physics failure (reference exit path) */
+#define FX_ENOMEM 5     /* device allocation failed */
+
+/* execution forms of a step */
+#define FX_FORM_PLAIN 0    /* per-block kernel launches in the reference's loop order */
+#define FX_FORM_BATCHED 1  /* every phase swept over all blocks, replayed as one CUDA graph */
+
+/* boundary condition types, values of enum prj_bc_type (src/prj_defs.h:518-523) */
+#define FX_BC_OUTFLOW 0
+#define FX_BC_REFLECT 1
+#define FX_BC_USER 2
+#define FX_BC_PERIODIC 3
+
+/* block-level array selectors for fx_download_array */
+#define FX_ARR_W 0        /* NHYDRO * 2 * 8000, WIDX */
+#define FX_ARR_EOSVAR 1   /* 3 * 8000, EIDX (AoSoA) */
+#define FX_ARR_FLUX 4     /* per dir: NHYDRO * 8000, VIDX (AoSoA) */
+#define FX_ARR_VRIEMANN 5 /* per dir: 3 * 8000, VRIDX (AoSoA) */
+#define FX_ARR_GRAV 6     /* per dir: 8000, IDX */
+#define FX_ARR_BF 7       /* per dir: 2 * 8400, FACE_IDX */
+#define FX_ARR_BV1 8      /* per dir: 8000, IDX */
+#define FX_ARR_BV2 9      /* per dir: 8000, IDX */
+#define FX_ARR_EMF 10     /* per dir: 8820, EDGE_IDX */
+#define FX_ARR_RHS 3      /* NHYDRO * 8000, MHDVIDX (AoSoA) */
+
+typedef struct fx_ctx fx_ctx;
+
+/* One neighbour slot: the fields of prj_neighbor (src/prj_types.h:73-100)
+ * that the ghost fill and the coarse/fine corrections read. */
+typedef struct fx_slot {
+    int32_t id;         /* neighbour block index into the block array, -1 if none */
+    int32_t rel_level;  /* neighbour level minus this block's level: -1, 0, +1 */
+    int32_t type;       /* 0 none, 1 face, 2 edge, 3 corner */
+    int8_t send_loc_start[3];
+    int8_t send_loc_end[3];
+    int8_t recv_loc_start[3];
+    int8_t recv_loc_end[3];
+} fx_slot;
+
+/* One block of the mesh (prj_block, src/prj_types.h:151-213: geometry and
+ * the 56 neighbour slots). */
+typedef struct fx_block_desc {
+    int32_t id;         /* < 0: unused entry */
+    int32_t level;
+    int32_t active;     /* 1 for leaf blocks that are stepped */
+    int32_t rank;       /* must be 0 (one device, one rank) */
+    double xmin[3];
+    double xmax[3];
+    double dx[3];
+    double vol;
+    double area[3];
+    fx_slot slot[56];
+} fx_block_desc;
+
+/* Run-time configuration (compile-time switches of the reference). */
+typedef struct fx_config {
+    int32_t mhd;        /* 1: PRJ_MHD=1 build, 0: hydro build */
+    int32_t gravity;    /* 1: apply the static gravity source from uploaded grav arrays */
+    double gamma;       /* ideal-gas adiabatic index of the user EOS */
+    double coord[6];    /* domain: x1min, x1max, x2min, x2max, x3min, x3max (prj_coord) */
+    int32_t bc[6];      /* x1 inner, x1 outer, x2 inner, x2 outer, x3 inner, x3 outer */
+    double mhd_eta;     /* prj_mesh.mhd_eta */
+} fx_config;
+
+/* ---- context -------------------------------------------------------------- */
+
+/* Creates a context on `device`.  Replaces nothing: the reference has no
+ * device; this owns the stream, the device mirror and the step graphs. */
+int fx_create(int device, const fx_config *cfg, fx_ctx **out);
+void fx_destroy(fx_ctx *ctx);
+int fx_last_error(const fx_ctx *ctx, char *buf, size_t len);
+/* Waits for all queued work and reports device-side physics failures. */
+int fx_sync(fx_ctx *ctx);
+/* The CUDA stream (cudaStream_t) all work is queued on, for host-side timing. */
+int fx_stream(fx_ctx *ctx, void **stream);
+
+/* ---- mesh ------------------------------------------------------------------ */
+
+/* Mirrors the block list and neighbour slots of a prj_mesh
+ * (src/prj_types.h:465-503; slots built by prj_neighbor_compute_geometry,
+ * src/prj_mesh.c:46-243).  Allocates device storage and compiles the ghost
+ * fill of prj_boundary_fill_ghosts_and_bf (src/prj_boundary.c:1150-1241) and
+ * the coarse/fine flux and EMF corrections (src/prj_riemann.c:1700-1768,
+ * src/prj_mhd.c:1003-1029) into device programs. */
+int fx_set_mesh(fx_ctx *ctx, int nblocks, const fx_block_desc *blocks);
+
+/* Host-only inspection of the compiled ghost fill (no device needed).
+ * which = 0: cell program, 1: face program, 2: flux corrections,
+ * 3: EMF corrections.  Call with NULL buffers to get *nops and *nwaves;
+ * then ops receives 4 int32 per operation (dst, src, aux, type; 8 for the
+ * correction records) and wave_begin nwaves + 1 offsets. */
+int fx_plan_export(const fx_config *cfg, int nblocks, const fx_block_desc *blocks, int which,
+    int32_t *ops, int *nops, int32_t *wave_begin, int *nwaves);
+
+/* Host <-> device copies of one block, in the reference's per-block layout:
+ * W = block->W_mhd (NHYDRO * 2 * 8000 doubles), Bf[d] = block->Bf[d]
+ * (2 * 8400 doubles each, may be NULL for hydro), grav[d] = block->grav[d]
+ * (8000 doubles each, may be NULL). */
+int fx_upload_block(fx_ctx *ctx, int block, const double *W, const double *const Bf[3],
+    const double *const grav[3]);
+/* eosvar (3 * 8000, may be NULL) is recomputed from W of the last stage,
+ * exactly what prj_eos_fill_active_cells + prj_eos_fill_mesh leave there. */
+int fx_download_block(fx_ctx *ctx, int block, double *W, double *eosvar, double *const Bf[3]);
+/* Whole-mesh copies: W_all is nblocks consecutive W arrays, Bf_all nblocks
+ * consecutive 3 * 2 * 8400 arrays (d-major); either may be NULL. */
+int fx_upload_all(fx_ctx *ctx, const double *W_all, const double *Bf_all);
+int fx_download_all(fx_ctx *ctx, double *W_all, double *Bf_all);
+/* Same host layout as fx_upload_all / fx_download_all, but only stage slot 0
+ * of W and Bf moves: the state a host driver sees between calls to
+ * prj_timeint_step (slot 1 is the step's scratch). */
+int fx_upload_state(fx_ctx *ctx, const double *W_all, const double *Bf_all);
+int fx_download_state(fx_ctx *ctx, double *W_all, double *Bf_all);
+/* Any block array, including the step's scratch, for inspection. */
+int fx_download_array(fx_ctx *ctx, int block, int which, int dir, double *out);
+
+/* ---- reference entry points (plain, per block) ----------------------------- */
+
+/* prj_flux_update (src/prj_flux.h:4-5): face fluxes, v_riemann, Bv1/Bv2 of
+ * one block from W slot w_slot and Bf slot use_bf1. */
+int fx_flux_update(fx_ctx *ctx, int block, int w_slot, int use_bf1);
+/* prj_timeint_mhd_update_emf (src/prj_timeint.c:292-413): edge EMFs of one
+ * block at stage slot `stage`. */
+int fx_mhd_update_emf(fx_ctx *ctx, int block, int stage);
+/* prj_timeint_mhd_update_bf (src/prj_timeint.c:448-495), stage 1 or 2. */
+int fx_mhd_update_bf(fx_ctx *ctx, int block, int stage, double dt);
+/* prj_src_update + the per-cell stage update loops (src/prj_timeint.c:1255-1349,
+ * 1562-1654) of one block; folds the block's dt_src into *dt_src if non-NULL
+ * (synchronises). */
+int fx_update_cells(fx_ctx *ctx, int block, int stage, double dt, double *dt_src);
+/* prj_riemann_flux_send (src/prj_riemann.c:1700-1768). */
+int fx_riemann_flux_send(fx_ctx *ctx);
+/* prj_mhd_emf_send (src/prj_mhd.c:1003-1029). */
+int fx_mhd_emf_send(fx_ctx *ctx);
+/* prj_eos_fill_active_cells / prj_eos_fill_mesh (src/prj_eos.c:1112-1162);
+ * `stage` is the reference's stage argument (slot = stage - 1). */
+int fx_eos_fill_active_cells(fx_ctx *ctx, int stage);
+int fx_eos_fill_mesh(fx_ctx *ctx, int stage);
+/* prj_boundary_fill_ghosts_and_bf (src/prj_boundary.h:17-18). */
+int fx_boundary_fill_ghosts_and_bf(fx_ctx *ctx, int stage, int use_bf1);
+
+/* ---- time integration ------------------------------------------------------- */
+
+/* prj_timeint_calc_dt (src/prj_timeint.h:15-16): min over active cells. */
+int fx_calc_dt(fx_ctx *ctx, double cfl, double *dt);
+/* prj_timeint_stage1 / prj_timeint_stage2 (src/prj_timeint.h:17-20). */
+int fx_stage(fx_ctx *ctx, int form, int stage, double dt, double *dt_src);
+/* prj_timeint_step (src/prj_timeint.h:31-33): one RK2 step.  *dt_src (may be
+ * NULL) receives the minimum source time step.  FX_FORM_BATCHED replays a
+ * captured CUDA graph; it does not synchronise unless dt_src != NULL. */
+int fx_step(fx_ctx *ctx, int form, double dt, double *dt_src);
+/* The driver loop of src/main.c:485-562 without I/O: calc_dt, dt growth
+ * limit dt_factor, clip to t_end, step, dt_src clamp; device resident.
+ * state[0..2] = time, dt, step on entry and on return. */
+int fx_run(fx_ctx *ctx, int form, int nsteps, double cfl, double dt_factor, double t_end,
+    double *state);
+
+/* ---- measurement --------------------------------------------------------------- */
+
+/* phases for fx_time_phase: the batched sweep of one phase over all blocks */
+#define FX_PHASE_FLUX 0      /* one face-flux launch (direction x) */
+#define FX_PHASE_EMF 1       /* edge EMFs */
+#define FX_PHASE_CT 2        /* CT face update, stage 1 */
+#define FX_PHASE_CELLS 3     /* cell update, stage 1 */
+#define FX_PHASE_GHOST 4     /* ghost fill of stage slot 1 (all waves) */
+#define FX_PHASE_STEP 5      /* one batched RK2 step (graph) */
+
+/* Times `reps` back-to-back launches of one phase with CUDA events on the
+ * context's stream (after one untimed launch); *ms = average per launch.
+ * Phases 0-4 rewrite the stage-1 scratch only, so repeating them leaves the
+ * mesh state unchanged; phase 5 advances the state by reps steps with dt. */
+int fx_time_phase(fx_ctx *ctx, int phase, int reps, double dt, double *ms);
+
+/* what = 0: kernel launches per batched step, 1: per plain step,
+ * 2/3: ghost cell/face operations, 4/5: ghost cell/face waves */
+int fx_info(fx_ctx *ctx, int what, long long *value);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

@@ -107,6 +107,7 @@ class Reference:
         L.rh_eos_rey.argtypes = [C.c_double] * 3 + [dp]
         L.rh_set_gamma.argtypes = [C.c_double]
         L.rh_flux_update.argtypes = [C.c_int, C.c_int, C.c_int]
+        L.rh_fill_ghosts.argtypes = [C.c_int, C.c_int]
         L.rh_sim_time.restype = C.c_double
         L.rh_sim_dt.restype = C.c_double
         if mhd:
@@ -206,6 +207,22 @@ class Reference:
 
     def flux_update(self, b: int, w_slot: int, use_bf1: int) -> None:
         self.lib.rh_flux_update(b, w_slot, use_bf1)
+
+    def fill_ghosts(self, stage: int, use_bf1: int) -> None:
+        self.lib.rh_fill_ghosts(stage, use_bf1)
+
+    def mesh_arrays(self):
+        """(ints [n,4], geom [n,13], slots [n,56,15]) of the current mesh."""
+        nb = self.nblocks()
+        ints = np.zeros((nb, 4), dtype=np.int64)
+        geom = np.zeros((nb, 13), dtype=np.float64)
+        slots = np.zeros((nb, 56, 15), dtype=np.int64)
+        for b in range(nb):
+            i, g = self.block_geom(b)
+            ints[b] = i
+            geom[b] = g
+            slots[b] = self.block_slots(b)
+        return ints, geom, slots
 
     # -- single kernels -------------------------------------------------------
     def mc_slope(self, qm, q0, qp) -> float:

@@ -883,6 +883,15 @@ double *rh_block_array(int b, int which, int dir)
     }
 }
 
+/* The reference's ghost fill followed by its eos fill of the mesh
+ * (src/prj_timeint.c:2829-2834 with stage arguments). */
+void rh_fill_ghosts(int stage, int use_bf1)
+{
+    prj_boundary_fill_ghosts_and_bf(&g_sim.mesh, &g_mpi, &g_sim.bc, stage, use_bf1, &g_sim.eos, 0,
+        &g_sim.rad, PRJ_BOUNDARY_TIMER_SCOPE_NONE);
+    prj_eos_fill_mesh(&g_sim.mesh, &g_sim.eos, &g_mpi, stage, PRJ_EOS_CTX_MAIN);
+}
+
 /* Per-block reference phases, for phase-level parity tests. */
 void rh_flux_update(int b, int w_slot, int use_bf1)
 {

@@ -1,0 +1,117 @@
+"""Parity of the CUDA path with the reference CPU path (the oracle), through
+the C ABI.  Identical inputs: the oracle builds the workload with the
+reference's own code, the state is uploaded to the device, both sides step
+with the same dt sequence, and every block array is compared.
+
+Tolerance: the kernels evaluate the reference's double operations in the
+same order with no contraction, so agreement is expected to be bit for bit;
+the asserted bound is the north-star 1e-12 relative (per array, relative to
+its max magnitude), and bit equality is asserted where it holds by design.
+"""
+import numpy as np
+import pytest
+
+import fornaxamr_b200 as fx
+from oracle import ref as R
+from tests import helpers as H
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-12
+
+
+def make_ctx(ref, p, mhd):
+    desc = H.ref_desc(ref)
+    coord = [p.xmin[0], p.xmax[0], p.xmin[1], p.xmax[1], p.xmin[2], p.xmax[2]]
+    ctx = fx.Context(mhd, p.gamma, coord)
+    ctx.set_mesh(desc)
+    W, Bf = H.ref_state(ref)
+    for b in range(W.shape[0]):
+        ctx.upload_block(b, W[b].ravel(), None if Bf is None else [Bf[b, d].ravel() for d in range(3)])
+    return ctx
+
+
+def device_state(ctx, nb, nv, mhd):
+    W = np.empty((nb, nv, 2, H.NCELLS))
+    Bf = np.empty((nb, 3, 2, H.NFACES)) if mhd else None
+    ctx.download_all(W, Bf)
+    return W, Bf
+
+
+def assert_state_equal(ctx, ref, mhd, exact=True):
+    W_ref, Bf_ref = H.ref_state(ref)
+    W, Bf = device_state(ctx, W_ref.shape[0], W_ref.shape[1], mhd)
+    assert H.max_rel_err(W, W_ref) <= TOL
+    if mhd:
+        assert H.max_rel_err(Bf, Bf_ref) <= TOL
+    if exact:
+        assert np.array_equal(W, W_ref)
+        if mhd:
+            assert np.array_equal(Bf, Bf_ref)
+
+
+@pytest.mark.parametrize("form", [fx.FORM_PLAIN, fx.FORM_BATCHED])
+def test_fourier_mhd_steps_match_reference(ref_mhd, form):
+    p = R.params_fourier(root=2, nmodes=8, kmax=2)
+    ref_mhd.setup(p)
+    ctx = make_ctx(ref_mhd, p, True)
+    assert ctx.calc_dt(p.cfl) == ref_mhd.calc_dt()
+    n, t_ref, dt_ref, st_ref = ref_mhd.run(3)
+    t, dt, st = ctx.run(form, 3, p.cfl, p.dt_factor, p.t_end, (0.0, 0.0, 0.0))
+    assert (t, dt, st) == (t_ref, dt_ref, st_ref)
+    assert_state_equal(ctx, ref_mhd, True)
+    ctx.close()
+
+
+def test_single_stage_and_intermediates_match_reference(ref_mhd):
+    p = R.params_fourier(root=2, nmodes=6, kmax=2)
+    ref_mhd.setup(p)
+    ctx = make_ctx(ref_mhd, p, True)
+    dt = ref_mhd.calc_dt()
+    ref_src = ref_mhd.stage(1, dt)
+    src = ctx.stage(fx.FORM_PLAIN, 1, dt)
+    assert src == ref_src
+    for b in range(ref_mhd.nblocks()):
+        for d in range(3):
+            assert np.array_equal(ctx.download_array(b, fx.ARR_FLUX, d), ref_mhd.flux(b, d))
+            assert np.array_equal(ctx.download_array(b, fx.ARR_VRIEMANN, d), ref_mhd.vriemann(b, d))
+            bv1, bv2 = ref_mhd.Bv(b, d)
+            assert np.array_equal(ctx.download_array(b, fx.ARR_BV1, d), bv1)
+            assert np.array_equal(ctx.download_array(b, fx.ARR_BV2, d), bv2)
+            assert np.array_equal(ctx.download_array(b, fx.ARR_EMF, d), ref_mhd.emf(b, d))
+        assert np.array_equal(ctx.download_array(b, fx.ARR_EOSVAR), ref_mhd.eosvar(b))
+    assert_state_equal(ctx, ref_mhd, True)
+    ctx.close()
+
+
+@pytest.mark.parametrize("form", [fx.FORM_PLAIN, fx.FORM_BATCHED])
+def test_sod_hydro_matches_reference(ref_hydro, form):
+    p = R.params_sod(nblocks_x=8, t_end=0.2)
+    ref_hydro.setup(p)
+    ctx = make_ctx(ref_hydro, p, False)
+    n, t_ref, dt_ref, st_ref = ref_hydro.run(25)
+    t, dt, st = ctx.run(form, 25, p.cfl, p.dt_factor, p.t_end, (0.0, 0.0, 0.0))
+    assert (t, dt, st) == (t_ref, dt_ref, st_ref)
+    assert_state_equal(ctx, ref_hydro, False, True)
+    ctx.close()
+
+
+def test_divergence_free_at_roundoff(ref_mhd):
+    p = R.params_fourier(root=2, nmodes=8, kmax=3)
+    ref_mhd.setup(p)
+    ctx = make_ctx(ref_mhd, p, True)
+    ctx.run(fx.FORM_BATCHED, 5, p.cfl, p.dt_factor, p.t_end, (0.0, 0.0, 0.0))
+    nb = ref_mhd.nblocks()
+    W, Bf = device_state(ctx, nb, 9, True)
+    r = np.arange(16)
+    i, j, k = np.meshgrid(r, r, r, indexing="ij")
+    for b in range(nb):
+        _, g = ref_mhd.block_geom(b)
+        dx = g[6:9]
+        f = Bf[b, :, 0]
+        div = ((f[0][H.face_idx(0, i + 1, j, k)] - f[0][H.face_idx(0, i, j, k)]) / dx[0]
+               + (f[1][H.face_idx(1, i, j + 1, k)] - f[1][H.face_idx(1, i, j, k)]) / dx[1]
+               + (f[2][H.face_idx(2, i, j, k + 1)] - f[2][H.face_idx(2, i, j, k)]) / dx[2])
+        bmax = max(np.abs(f[d][H.active_faces(d)]).max() for d in range(3))
+        assert np.abs(div).max() * dx.min() / bmax <= 1e-13
+    ctx.close()
