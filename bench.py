@@ -185,6 +185,7 @@ def run_fx(args, rank, world, local_rank):
     ctx.upload_all(W0, Bf0)
     ctx.boundary_fill(1, 0)       # the driver's initial ghost fill (src/main.c:446)
     ctx.sync()
+    tuned, tune_ms = ctx.autotune()
     cfl, dt_factor, t_end = 0.4, 1.2, 1.0e30
     stream = torch.cuda.ExternalStream(ctx.stream(), device=dev)
 
@@ -258,12 +259,13 @@ def run_fx(args, rank, world, local_rank):
         e2e_ms = max_over_ranks(e0.elapsed_time(e1)) / args.e2e_steps
 
     peak, peak_kind = measured_peak_hbm()
-    # algorithmic bytes of one face-flux launch (direction x, all blocks):
-    # per face: the 8 primitive inputs of the cells its stencil owns
-    # (20 x 18 x 18 cells per 17 x 18 x 18 faces) + the face field (8 B) +
-    # outputs flux 9, v_riemann 3, Bv1, Bv2 (14 doubles)
-    faces = nb * 17 * 18 * 18
-    flux_bytes = nb * 20 * 18 * 18 * 8 * 8 + faces * 8 + faces * 14 * 8
+    # algorithmic bytes of one face-flux launch (all three directions, all
+    # blocks): per direction and block the 8 primitive inputs of the
+    # 20 x 18 x 18 stencil cells, and per face the face field (8 B) plus the
+    # outputs later phases read: 6 hydro fluxes, the normal velocity,
+    # Bv1, Bv2 (9 doubles)
+    faces = nb * 3 * 17 * 18 * 18
+    flux_bytes = nb * 3 * 20 * 18 * 18 * 8 * 8 + faces * 8 + faces * 9 * 8
     achieved = flux_bytes / (ms_flux * 1e-3) / 1e9
     traffic = flux_traffic_per_launch()
     launches_per_step = ctx.info(0) + 4
@@ -291,8 +293,9 @@ def run_fx(args, rank, world, local_rank):
             "ms_per_step": ms_plain, "value": world * ZONES / (ms_plain * 1e-3),
             "batched_over_plain": ms_plain / ms_step},
         "phases_ms": phases,
+        "autotune": {"flux_shape": tuned, "flux_ms_per_shape": [round(x, 4) for x in tune_ms[:6]]},
         "roofline": {
-            "kernel": "k_flux (face fluxes, one direction, all blocks)",
+            "kernel": "k_flux (face fluxes, three directions, all blocks)",
             "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
             "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
             "note": "FP64 HLLD issue rate bounds this kernel before HBM (see DESIGN.md)",

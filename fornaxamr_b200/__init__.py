@@ -60,14 +60,17 @@ def make_config(mhd: bool, gamma: float, coord: Sequence[float], bc: Sequence[in
 
 
 def plan_export(cfg: FxConfig, desc, which: int):
-    """Host-only dump of a compiled program: (ops [n,4] int32, wave_begin)."""
+    """Host-only dump of the compiled ghost fill: which = 0 cell ops, 1 face
+    ops, 4 cell-field ops -> (ops [n, 4 or 8] int32, wave_begin); 2/3 the
+    flux/EMF correction records; 5 compiler statistics (emitted cell ops,
+    emitted face ops, rewired copies, dead writes)."""
     L = library()
     nops = C.c_int(0)
     nwaves = C.c_int(0)
     rc = L.fx_plan_export(C.byref(cfg), len(desc), desc, which, None, C.byref(nops), None, C.byref(nwaves))
     if rc != 0:
         raise FxError(rc, "fx_plan_export failed")
-    width = 4 if which <= 1 else 8
+    width = 4 if which in (0, 1) else 1 if which == 5 else 8
     ops = np.zeros((max(nops.value, 1), width), dtype=np.int32)
     waves = np.zeros(nwaves.value + 1, dtype=np.int32)
     rc = L.fx_plan_export(C.byref(cfg), len(desc), desc, which,
@@ -227,6 +230,13 @@ class Context:
         v = C.c_double(0.0)
         self._check(self.L.fx_time_phase(self._h, phase, reps, dt, C.byref(v)))
         return v.value
+
+    def autotune(self):
+        """(chosen shape, per-shape face-kernel times in ms)."""
+        times = np.zeros(16)
+        choice = C.c_int(0)
+        self._check(self.L.fx_autotune(self._h, _dp(times), 16, C.byref(choice)))
+        return choice.value, times
 
     def info(self, what: int) -> int:
         v = C.c_longlong(0)

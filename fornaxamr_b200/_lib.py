@@ -64,6 +64,7 @@ EXPORTS = [
     "fx_update_cells", "fx_riemann_flux_send", "fx_mhd_emf_send", "fx_eos_fill_active_cells",
     "fx_eos_fill_mesh", "fx_boundary_fill_ghosts_and_bf", "fx_calc_dt", "fx_stage", "fx_step",
     "fx_run", "fx_plan_export", "fx_time_phase", "fx_info", "fx_upload_state", "fx_download_state",
+    "fx_autotune",
 ]
 PHASE_FLUX, PHASE_EMF, PHASE_CT, PHASE_CELLS, PHASE_GHOST, PHASE_STEP = range(6)
 
@@ -109,4 +110,5 @@ def load() -> C.CDLL:
                                  ip, C.POINTER(C.c_int), ip, C.POINTER(C.c_int)]
     L.fx_time_phase.argtypes = [vp, C.c_int, C.c_int, C.c_double, dp]
     L.fx_info.argtypes = [vp, C.c_int, C.POINTER(C.c_longlong)]
+    L.fx_autotune.argtypes = [vp, dp, C.c_int, C.POINTER(C.c_int)]
     return L

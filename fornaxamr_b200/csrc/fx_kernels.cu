@@ -52,13 +52,19 @@ __device__ __forceinline__ unsigned long long fx_double_key(double d)
 /* ------------------------------------------------------------------------ */
 /* Face fluxes                                                               */
 /* ------------------------------------------------------------------------ */
-template <bool MHD>
-__global__ void __launch_bounds__(128) k_flux(FxDev D, const int *__restrict__ blist, int dir,
-    int wslot, int bfslot, int full)
+/* FULL: store every component the reference stores (the drop-in form);
+ * otherwise only what later phases read (hydro flux components, the normal
+ * face velocity, Bv1/Bv2).  blockIdx.z is the sweep direction.  TPB/MINB
+ * set the launch shape (threads per CTA, resident CTAs per SM the register
+ * allocation must allow); the autotuner picks among the compiled shapes. */
+template <bool MHD, bool FULL, int TPB, int MINB>
+__global__ void __launch_bounds__(TPB, MINB) k_flux(FxDev D, const int *__restrict__ blist,
+    int wslot, int bfslot)
 {
     if (D.ctl->skip) {
         return;
     }
+    const int dir = blockIdx.z;
     const int b = blist[blockIdx.y];
     /* MHD carries one transverse ghost layer of faces for the CT EMFs
      * (src/prj_flux.c:2241-2251); hydro transverse faces are [0, 15]. */
@@ -130,13 +136,13 @@ __global__ void __launch_bounds__(128) k_flux(FxDev D, const int *__restrict__ b
         WL[FX_B1] = bn;
         WR[FX_B1] = bn;
         FxFaceOut o;
-        fx_riemann_hlld(WL, WR, pL, pR, gL, gR, bn, o, D.err, b, cR);
+        fx_riemann_hlld_folded(WL, WR, pL, pR, gL, gR, bn, o, D.err, b, cR);
 #pragma unroll
-        for (int lv = 0; lv < 9; ++lv) {
+        for (int lv = 0; lv < (FULL ? 9 : 6); ++lv) {
             D.flux[fbase + fx_bidx(9, fx_gmap(dir, lv), i, j, k)] = o.F[lv];
         }
 #pragma unroll
-        for (int m = 0; m < 3; ++m) {
+        for (int m = 0; m < (FULL ? 3 : 1); ++m) {
             D.vr[vbase + fx_bidx(3, (dir + m) % 3, i, j, k)] = o.v[m];
         }
         const size_t bvi = (size_t)b * FX_BV_COUNT + (size_t)dir * FX_NCELLS + cR;
@@ -165,11 +171,10 @@ __global__ void __launch_bounds__(128) k_flux(FxDev D, const int *__restrict__ b
             D.flux[fbase + fx_bidx(6, fx_gmap(dir, lv), i, j, k)] = F[lv];
         }
 #pragma unroll
-        for (int m = 0; m < 3; ++m) {
+        for (int m = 0; m < (FULL ? 3 : 1); ++m) {
             D.vr[vbase + fx_bidx(3, (dir + m) % 3, i, j, k)] = v[m];
         }
     }
-    (void)full;
 }
 
 /* ------------------------------------------------------------------------ */
@@ -630,13 +635,8 @@ __global__ void k_step_end(FxDev D)
  * offset (prj_reconstruct_cell_for_prolongate with use_BJ = 0) */
 __device__ double fx_prolong_cell(const double *q, int c, const double target[3]);
 
-__global__ void k_ghost_cells(FxDev D, const FxGop *__restrict__ ops, int n, int wslot, int nvg)
+__device__ __forceinline__ void fx_ghost_cell_op(const FxDev &D, const FxGop op, int wslot, int nvg)
 {
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= n || D.ctl->skip) {
-        return;
-    }
-    const FxGop op = ops[t];
     const int db = FX_CELL_BLOCK(op.dst);
     const int dc = FX_CELL_IDX(op.dst);
     const int sb = FX_CELL_BLOCK(op.src);
@@ -691,13 +691,8 @@ __global__ void k_ghost_cells(FxDev D, const FxGop *__restrict__ ops, int n, int
 __device__ __forceinline__ int fx_face_key_block(int key) { return key >> 15; }
 __device__ __forceinline__ int fx_face_key_idx(int key) { return key & 32767; }
 
-__global__ void k_ghost_faces(FxDev D, const FxGop *__restrict__ ops, int n, int bfslot)
+__device__ __forceinline__ void fx_ghost_face_op(const FxDev &D, const FxGop op, int bfslot)
 {
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= n || D.ctl->skip) {
-        return;
-    }
-    const FxGop op = ops[t];
     const int dir = op.aux & 3;
     const int db = fx_face_key_block(op.dst);
     const int df = fx_face_key_idx(op.dst);
@@ -715,33 +710,58 @@ __global__ void k_ghost_faces(FxDev D, const FxGop *__restrict__ ops, int n, int
     }
 }
 
-__global__ void k_bf2bc(FxDev D, const int *__restrict__ blist, int slot)
+/* cell-centred field of one cell from its faces: prj_mhd_bf2bc_impl
+ * (src/prj_mhd.c:555-603).  The metric factor sqrt(gamma) is 1 outside
+ * dynamical GR; the reference's division by it is exact and omitted. */
+__device__ __forceinline__ void fx_ghost_b_op(const FxDev &D, const FxBop op, int slot)
 {
-    const int b = blist[blockIdx.y];
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= FX_NCELLS || D.ctl->skip) {
-        return;
+    double v[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        const int k0 = op.f[2 * d];
+        const int k1 = op.f[2 * d + 1];
+        const double *b0 = D.Bf + (size_t)fx_face_key_block(k0) * FX_BF_COUNT +
+            ((size_t)d * FX_NSTAGES + slot) * FX_NFACES;
+        const double *b1 = D.Bf + (size_t)fx_face_key_block(k1) * FX_BF_COUNT +
+            ((size_t)d * FX_NSTAGES + slot) * FX_NFACES;
+        v[d] = 0.5 * (b0[fx_face_key_idx(k0)] + b1[fx_face_key_idx(k1)]);
     }
-    const int k = t % FX_PBS - FX_NG;
-    const int j = (t / FX_PBS) % FX_PBS - FX_NG;
-    const int i = t / (FX_PBS * FX_PBS) - FX_NG;
-    const double *bf = D.Bf + (size_t)b * FX_BF_COUNT;
-    const double *b1 = bf + (size_t)(0 * FX_NSTAGES + slot) * FX_NFACES;
-    const double *b2 = bf + (size_t)(1 * FX_NSTAGES + slot) * FX_NFACES;
-    const double *b3 = bf + (size_t)(2 * FX_NSTAGES + slot) * FX_NFACES;
-    /* the metric factor sqrt(gamma) is 1 outside dynamical GR; the
-     * reference's division by it is exact and omitted */
-    const double v1 = 0.5 * (b1[fx_face_idx(0, i, j, k)] + b1[fx_face_idx(0, i + 1, j, k)]);
-    const double v2 = 0.5 * (b2[fx_face_idx(1, i, j, k)] + b2[fx_face_idx(1, i, j + 1, k)]);
-    const double v3 = 0.5 * (b3[fx_face_idx(2, i, j, k)] + b3[fx_face_idx(2, i, j, k + 1)]);
-    const int c = fx_lidx(i, j, k);
-    if (!isfinite(v1) || !isfinite(v2) || !isfinite(v3)) {
+    const int b = FX_CELL_BLOCK(op.dst);
+    const int c = FX_CELL_IDX(op.dst);
+    if (!isfinite(v[0]) || !isfinite(v[1]) || !isfinite(v[2])) {
         fx_fail(D.err, FX_ERR_B_NONFINITE, b, c);
     }
     double *W = D.W + (size_t)b * FX_W_COUNT(9) + (size_t)slot * FX_NCELLS;
-    W[(size_t)FX_B1 * kPlane + c] = v1;
-    W[(size_t)FX_B2 * kPlane + c] = v2;
-    W[(size_t)FX_B3 * kPlane + c] = v3;
+    W[(size_t)FX_B1 * kPlane + c] = v[0];
+    W[(size_t)FX_B2 * kPlane + c] = v[1];
+    W[(size_t)FX_B3 * kPlane + c] = v[2];
+}
+
+/* one conflict-free wave of the ghost fill: CTAs [0, nbc) run cell ops,
+ * [nbc, nbc + nbf) face ops, the rest cell-field ops */
+__global__ void __launch_bounds__(256) k_ghost_wave(FxDev D, const FxGop *__restrict__ cops, int nc,
+    const FxGop *__restrict__ fops, int nf, const FxBop *__restrict__ bops, int nb, int slot, int nvg)
+{
+    if (D.ctl->skip) {
+        return;
+    }
+    const int nbc = (nc + 255) / 256;
+    const int nbf = (nf + 255) / 256;
+    int blk = blockIdx.x;
+    if (blk < nbc) {
+        const int t = blk * 256 + threadIdx.x;
+        if (t < nc) fx_ghost_cell_op(D, cops[t], slot, nvg);
+        return;
+    }
+    blk -= nbc;
+    if (blk < nbf) {
+        const int t = blk * 256 + threadIdx.x;
+        if (t < nf) fx_ghost_face_op(D, fops[t], slot);
+        return;
+    }
+    blk -= nbf;
+    const int t = blk * 256 + threadIdx.x;
+    if (t < nb) fx_ghost_b_op(D, bops[t], slot);
 }
 
 /* coarse/fine corrections */
@@ -791,17 +811,51 @@ __device__ double fx_prolong_cell(const double *q, int c, const double target[3]
 /* ------------------------------------------------------------------------ */
 static inline unsigned fx_blocks(int n, int tpb) { return (unsigned)((n + tpb - 1) / tpb); }
 
-void fx_launch_flux(const FxDev &D, const int *blist, int nlist, int dir, int wslot, int bfslot,
+/* launch shapes of the face kernel: {threads per CTA, min CTAs per SM} */
+static const int kFluxShapes[FX_FLUX_VARIANTS][2] = {{128, 4}, {128, 5}, {128, 6}, {256, 2}, {256, 3}, {64, 8}};
+
+template <bool MHD, bool FULL, int TPB, int MINB>
+static void launch_flux_shape(const FxDev &D, const int *blist, int nlist, int ndir, int wslot,
+    int bfslot, cudaStream_t s)
+{
+    const int nf = MHD ? (FX_BS + 1) * (FX_BS + 2) * (FX_BS + 2) : (FX_BS + 1) * FX_BS * FX_BS;
+    const dim3 g(fx_blocks(nf, TPB), nlist, ndir);
+    k_flux<MHD, FULL, TPB, MINB><<<g, TPB, 0, s>>>(D, blist, wslot, bfslot);
+}
+
+template <bool MHD, bool FULL>
+static void launch_flux_variant(const FxDev &D, const int *blist, int nlist, int ndir, int wslot,
+    int bfslot, int variant, cudaStream_t s)
+{
+    switch (variant) {
+    case 1: launch_flux_shape<MHD, FULL, 128, 5>(D, blist, nlist, ndir, wslot, bfslot, s); break;
+    case 2: launch_flux_shape<MHD, FULL, 128, 6>(D, blist, nlist, ndir, wslot, bfslot, s); break;
+    case 3: launch_flux_shape<MHD, FULL, 256, 2>(D, blist, nlist, ndir, wslot, bfslot, s); break;
+    case 4: launch_flux_shape<MHD, FULL, 256, 3>(D, blist, nlist, ndir, wslot, bfslot, s); break;
+    case 5: launch_flux_shape<MHD, FULL, 64, 8>(D, blist, nlist, ndir, wslot, bfslot, s); break;
+    default: launch_flux_shape<MHD, FULL, 128, 4>(D, blist, nlist, ndir, wslot, bfslot, s); break;
+    }
+}
+
+void fx_launch_flux(const FxDev &D, const int *blist, int nlist, int ndir, int wslot, int bfslot,
     int full, cudaStream_t s)
 {
     if (nlist <= 0) return;
+    const int v = D.flux_variant;
     if (D.nv == 9) {
-        const int nf = (FX_BS + 1) * (FX_BS + 2) * (FX_BS + 2);
-        k_flux<true><<<dim3(fx_blocks(nf, 128), nlist), 128, 0, s>>>(D, blist, dir, wslot, bfslot, full);
+        if (full) launch_flux_variant<true, true>(D, blist, nlist, ndir, wslot, bfslot, v, s);
+        else launch_flux_variant<true, false>(D, blist, nlist, ndir, wslot, bfslot, v, s);
     } else {
-        const int nf = (FX_BS + 1) * FX_BS * FX_BS;
-        k_flux<false><<<dim3(fx_blocks(nf, 128), nlist), 128, 0, s>>>(D, blist, dir, wslot, bfslot, full);
+        if (full) launch_flux_variant<false, true>(D, blist, nlist, ndir, wslot, bfslot, v, s);
+        else launch_flux_variant<false, false>(D, blist, nlist, ndir, wslot, bfslot, v, s);
     }
+}
+
+void fx_flux_shape(int variant, int *tpb, int *minb)
+{
+    const int v = variant >= 0 && variant < FX_FLUX_VARIANTS ? variant : 0;
+    *tpb = kFluxShapes[v][0];
+    *minb = kFluxShapes[v][1];
 }
 
 void fx_launch_emf(const FxDev &D, const int *blist, int nlist, int wslot, int bfslot, cudaStream_t s)
@@ -847,22 +901,12 @@ void fx_launch_calc_dt(const FxDev &D, const int *blist, int nlist, int wslot, d
     k_calc_dt<<<dim3(fx_blocks(FX_BS * FX_BS * FX_BS, 256), nlist), 256, 0, s>>>(D, blist, wslot, cfl);
 }
 
-void fx_launch_ghost_cells(const FxDev &D, const FxGop *ops, int n, int wslot, int nvg, cudaStream_t s)
+void fx_launch_ghost_wave(const FxDev &D, const FxGop *cops, int nc, const FxGop *fops, int nf,
+    const FxBop *bops, int nb, int slot, int nvg, cudaStream_t s)
 {
-    if (n <= 0) return;
-    k_ghost_cells<<<fx_blocks(n, 256), 256, 0, s>>>(D, ops, n, wslot, nvg);
-}
-
-void fx_launch_ghost_faces(const FxDev &D, const FxGop *ops, int n, int bfslot, cudaStream_t s)
-{
-    if (n <= 0) return;
-    k_ghost_faces<<<fx_blocks(n, 256), 256, 0, s>>>(D, ops, n, bfslot);
-}
-
-void fx_launch_bf2bc(const FxDev &D, const int *blist, int nlist, int slot, cudaStream_t s)
-{
-    if (nlist <= 0) return;
-    k_bf2bc<<<dim3(fx_blocks(FX_NCELLS, 256), nlist), 256, 0, s>>>(D, blist, slot);
+    const unsigned grid = fx_blocks(nc, 256) + fx_blocks(nf, 256) + fx_blocks(nb, 256);
+    if (grid == 0) return;
+    k_ghost_wave<<<grid, 256, 0, s>>>(D, cops, nc, fops, nf, bops, nb, slot, nvg);
 }
 
 void fx_launch_flux_correct(const FxDev &D, const FxCorr *recs, int n, cudaStream_t s)

@@ -55,7 +55,12 @@ struct FxDev {
     FxErr *err;
     unsigned long long *red;  /* [0] dt min key, [1] dt_src min key */
     FxCtl *ctl;
+    int flux_variant;         /* launch shape of the face kernel (autotuned) */
 };
+
+#define FX_FLUX_VARIANTS 6
+/* threads per CTA and min resident CTAs per SM of a face-kernel variant */
+void fx_flux_shape(int variant, int *tpb, int *minb);
 
 /* One element operation of a ghost-fill program.  dst/src pack
  * (block << 13) | cell for cell ops, or (block << 15) | face for face ops
@@ -78,6 +83,16 @@ struct FxGop {
     int32_t type;
 };
 
+/* cell-centred field of one cell from its six faces (bf2bc of one cell):
+ * dst = (block << 13) | cell; f[2d], f[2d+1] = (block << 15) | face of the
+ * lower and upper face along d (after copy propagation they may point at
+ * the faces those were copied from) */
+struct FxBop {
+    int32_t dst;
+    int32_t f[6];
+    int32_t pad;
+};
+
 /* coarse/fine correction records: dst <- 0.25 * sum of 4 (flux) or
  * 0.5 * sum of 2 (emf) source entries */
 struct FxCorr {
@@ -92,7 +107,7 @@ struct FxCorr {
 #define FX_CELL_IDX(key) ((key) & 8191)
 
 /* launchers (fx_kernels.cu); all asynchronous on `s` */
-void fx_launch_flux(const FxDev &D, const int *blist, int nlist, int dir, int wslot, int bfslot,
+void fx_launch_flux(const FxDev &D, const int *blist, int nlist, int ndir, int wslot, int bfslot,
     int full, cudaStream_t s);
 void fx_launch_emf(const FxDev &D, const int *blist, int nlist, int wslot, int bfslot, cudaStream_t s);
 void fx_launch_bf_update(const FxDev &D, const int *blist, int nlist, int stage, cudaStream_t s);
@@ -102,9 +117,9 @@ void fx_launch_eos_fill(const FxDev &D, const int *blist, int nlist, int wslot, 
     cudaStream_t s);
 void fx_launch_calc_dt(const FxDev &D, const int *blist, int nlist, int wslot, double cfl,
     cudaStream_t s);
-void fx_launch_ghost_cells(const FxDev &D, const FxGop *ops, int n, int wslot, int nvg, cudaStream_t s);
-void fx_launch_ghost_faces(const FxDev &D, const FxGop *ops, int n, int bfslot, cudaStream_t s);
-void fx_launch_bf2bc(const FxDev &D, const int *blist, int nlist, int slot, cudaStream_t s);
+/* one wave of the ghost fill (cell ops, face ops and cell-field ops) */
+void fx_launch_ghost_wave(const FxDev &D, const FxGop *cops, int nc, const FxGop *fops, int nf,
+    const FxBop *bops, int nb, int slot, int nvg, cudaStream_t s);
 void fx_launch_flux_correct(const FxDev &D, const FxCorr *recs, int n, cudaStream_t s);
 void fx_launch_emf_correct(const FxDev &D, const FxCorr *recs, int n, cudaStream_t s);
 void fx_launch_reset_reductions(const FxDev &D, int which, cudaStream_t s);

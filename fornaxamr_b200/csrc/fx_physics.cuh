@@ -444,6 +444,114 @@ static __device__ __noinline__ void fx_riemann_hlld(const double *WL, const doub
     }
 }
 
+/* Same solver with the left and right star branches folded into one code
+ * path.  With `left` = (0 <= SM), the reference's two branches
+ * (src/prj_riemann.c:413-438) are the same sequence of operations applied to
+ * the near state N = left ? L : R and the far state F = left ? R : L:
+ *   Ns = outer_star(N, S_N); a = |bn|/sqrt(Ns.rho); S_Ns = SM -/+ a;
+ *   single star if (left ? 0 <= S_Ns : S_Ns <= 0) || bn_small;
+ *   else Fs = outer_star(F, S_F) and the double star of (Ls, Rs), whose
+ *   energy update e = Ns.e -/+ sqrt(Ns.rho) sign(bn) (vb_Ns - vb_ss) uses the
+ *   near star in both branches (its normal velocity is SM on either side).
+ * Selecting operands and choosing between x - t and x + t are exact, so the
+ * result is bit-identical to fx_riemann_hlld; warps whose faces straddle
+ * SM = 0 no longer execute both branches. */
+__device__ __forceinline__ void fx_riemann_hlld_folded(const double *WL, const double *WR,
+    double pL, double pR, double gL, double gR, double bn, FxFaceOut &o,
+    FxErr *err, int blk, int idx)
+{
+    FxHlldState L, R;
+    fx_hlld_state(WL, pL, gL, bn, L, err, blk, idx);
+    fx_hlld_state(WR, pR, gR, bn, R, err, blk, idx);
+    const double cfL = fx_hlld_fast_speed(L, err, blk, idx);
+    const double cfR = fx_hlld_fast_speed(R, err, blk, idx);
+    const double SL = fx_min(L.vx - cfL, R.vx - cfR);
+    const double SR = fx_max(L.vx + cfL, R.vx + cfR);
+    if (!(SL < SR)) {
+        fx_fail(err, FX_ERR_HLLD_ORDER, blk, idx);
+    }
+    if (0.0 <= SL || SR <= 0.0) {
+        const FxHlldState &X = (0.0 <= SL) ? L : R;
+#pragma unroll
+        for (int v = 0; v < 9; ++v) o.F[v] = fx_hlld_state_f(X, v);
+        fx_face_outputs(X.vx, X.vy, X.vz, X.bx, X.by, X.bz, o);
+        return;
+    }
+    const double denom = R.rho * (SR - R.vx) - L.rho * (SL - L.vx);
+    if (fabs(denom) <= 1.0e-14 *
+        (fabs(R.rho * (SR - R.vx)) + fabs(L.rho * (SL - L.vx)) + 1.0)) {
+        fx_fail(err, FX_ERR_HLLD_DENOM, blk, idx);
+    }
+    const double SM = (R.rho * R.vx * (SR - R.vx) -
+        L.rho * L.vx * (SL - L.vx) + (L.pt - R.pt)) / denom;
+    const double pt_star_l = L.pt + L.rho * (SL - L.vx) * (SM - L.vx);
+    const double pt_star_r = R.pt + R.rho * (SR - R.vx) * (SM - R.vx);
+    const double pt_star = 0.5 * (pt_star_l + pt_star_r);
+    if (pt_star <= 0.0 || !isfinite(pt_star)) {
+        const double inv = 1.0 / (SR - SL);
+        double Uh[9];
+#pragma unroll
+        for (int v = 0; v < 9; ++v) {
+            const double lf = fx_hlld_state_f(L, v);
+            const double rf = fx_hlld_state_f(R, v);
+            const double lu = fx_hlld_state_u(L, v);
+            const double ru = fx_hlld_state_u(R, v);
+            o.F[v] = (SR * lf - SL * rf + SL * SR * (ru - lu)) * inv;
+            Uh[v] = (SR * ru - SL * lu + lf - rf) * inv;
+        }
+        const double rho = Uh[0];
+        fx_face_outputs(Uh[1] / rho, Uh[2] / rho, Uh[3] / rho, Uh[6], Uh[7], Uh[8], o);
+        return;
+    }
+    const bool bn_small = (0.5 * bn * bn < FX_HLLD_SMALL * pt_star);
+    const bool left = (0.0 <= SM);
+    const FxHlldState N = left ? L : R;
+    const double SN = left ? SL : SR;
+    FxHlldStar Ns;
+    fx_hlld_outer_star(N, SN, SM, pt_star, Ns, err, blk, idx);
+    const double a = fabs(bn) / sqrt(Ns.rho);
+    const double SNs = left ? SM - a : SM + a;
+    const bool single = (left ? (0.0 <= SNs) : (SNs <= 0.0)) || bn_small;
+    if (single) {
+#pragma unroll
+        for (int v = 0; v < 9; ++v) {
+            o.F[v] = fx_hlld_state_f(N, v) + SN * (fx_hlld_u(Ns, v) - fx_hlld_state_u(N, v));
+        }
+        fx_face_outputs(Ns.vx, Ns.vy, Ns.vz, Ns.bx, Ns.by, Ns.bz, o);
+        return;
+    }
+    const FxHlldState Fr = left ? R : L;
+    const double SF = left ? SR : SL;
+    FxHlldStar Fs;
+    fx_hlld_outer_star(Fr, SF, SM, pt_star, Fs, err, blk, idx);
+    const FxHlldStar Ls = left ? Ns : Fs;
+    const FxHlldStar Rs = left ? Fs : Ns;
+    /* prj_hlld_double_star_one, src/prj_riemann.c:234-282 */
+    const double sqrt_l = sqrt(Ls.rho);
+    const double sqrt_r = sqrt(Rs.rho);
+    if (sqrt_l + sqrt_r <= 0.0) {
+        fx_fail(err, FX_ERR_HLLD_DSTAR, blk, idx);
+    }
+    const double inv_sum = 1.0 / (sqrt_l + sqrt_r);
+    const double sign_bx = bn < 0.0 ? -1.0 : 1.0;
+    FxHlldStar ss = Ns;
+    ss.vy = (sqrt_l * Ls.vy + sqrt_r * Rs.vy + (Rs.by - Ls.by) * sign_bx) * inv_sum;
+    ss.vz = (sqrt_l * Ls.vz + sqrt_r * Rs.vz + (Rs.bz - Ls.bz) * sign_bx) * inv_sum;
+    ss.by = (sqrt_l * Rs.by + sqrt_r * Ls.by + sqrt_l * sqrt_r * (Rs.vy - Ls.vy) * sign_bx) * inv_sum;
+    ss.bz = (sqrt_l * Rs.bz + sqrt_r * Ls.bz + sqrt_l * sqrt_r * (Rs.vz - Ls.vz) * sign_bx) * inv_sum;
+    const double vbdot_ss = Ns.vx * bn + ss.vy * ss.by + ss.vz * ss.bz;
+    const double vbdot_n = Ns.vx * bn + Ns.vy * Ns.by + Ns.vz * Ns.bz;
+    const double t = (left ? sqrt_l : sqrt_r) * sign_bx * (vbdot_n - vbdot_ss);
+    ss.e = left ? Ns.e - t : Ns.e + t;
+#pragma unroll
+    for (int v = 0; v < 9; ++v) {
+        const double us = fx_hlld_u(Ns, v);
+        o.F[v] = fx_hlld_state_f(N, v) + SN * (us - fx_hlld_state_u(N, v)) +
+            SNs * (fx_hlld_u(ss, v) - us);
+    }
+    fx_face_outputs(ss.vx, ss.vy, ss.vz, ss.bx, ss.by, ss.bz, o);
+}
+
 /* ------------------------------------------------------------------------ */
 /* HLLC for the hydro build, src/prj_riemann.c:1433-1599 and the theta       */
 /* pressure-jump limiter of src/prj_riemann.c:8-17.                          */

@@ -7,24 +7,36 @@
  * "fidelity" bookkeeping that decides whether a Bf write lands
  * (src/prj_boundary.c:599-625) is itself data independent.  This file replays
  * that sequence once on the host, in the reference's exact loop order, and
- * records every write that lands as an element operation.  Operations are
- * then levelled into waves: an operation is placed one wave after the latest
- * earlier operation it conflicts with (read-after-write, write-after-read or
- * write-after-write on any element), so each wave is free of conflicts and
- * running the waves in order reproduces the reference's sequential result,
- * including which of several overlapping writers wins.
+ * records every write that lands as an element operation.  Then:
+ *
+ *  1. copy propagation: a single-source operation whose source currently
+ *     holds a value produced by a plain copy (whose own source is unchanged
+ *     since) reads that earlier source instead; chains collapse to their root;
+ *  2. dead-write elimination: an operation whose result is overwritten
+ *     before anything reads it is dropped;
+ *  3. the closing prj_mhd_bf2bc_all_mesh pass (src/prj_boundary.c:1235-1239)
+ *     becomes one operation per cell whose field may change (every ghost cell,
+ *     and interior cells with a rewritten face), reading the final faces
+ *     through the same copy chains;
+ *  4. levelling: an operation is placed one wave after the latest earlier
+ *     operation it conflicts with (read-after-write, write-after-read or
+ *     write-after-write on any element), so each wave is free of conflicts and
+ *     running the waves in order reproduces the sequential result, including
+ *     which of several overlapping writers wins.
  *
  * Cell operations carry the primitive variables 0..5 only.  In an MHD run
- * the cell-centred field in every one of the 20^3 cells is rewritten from
- * the faces by prj_mhd_bf2bc_all_mesh at the end of the fill
- * (src/prj_boundary.c:1235-1239), and every ghost operation is variable-wise,
- * so the B components of the cell operations are dead.  eosvar is not
- * transferred: for the ideal gas it is a pointwise function of W, and the
- * reference's fill leaves eosvar == eos(W) in every cell.
+ * the cell-centred field of every one of the 20^3 cells is rewritten from the
+ * faces at the end of the fill and every ghost operation is variable-wise, so
+ * the field components of the cell operations are dead; interior cells whose
+ * faces the fill does not touch already hold the face average from the cell
+ * update.  eosvar is not transferred: for the ideal gas it is a pointwise
+ * function of W, and the reference's fill leaves eosvar == eos(W) in every
+ * cell.
  */
 #include "fx_plan.h"
 
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <cstdint>
 #include <cstring>
@@ -34,53 +46,10 @@ namespace {
 enum { KIND_SAME = 3, KIND_RESTRICT = 4, KIND_PROLONG = 5 };
 enum { PHYS_FACE_ONLY = 0, PHYS_EDGE_CORNER = 2 };
 enum { FID_NONE = 0, FID_COARSER = 1, FID_SAME = 2, FID_FINER = 3 };
+enum { SPACE_CELL = 0, SPACE_FACE = 1 };
 
 const int BS = FX_BS;
 const int NG = FX_NG;
-
-/* Levels element operations into conflict-free waves. */
-class WaveBuilder {
-public:
-    explicit WaveBuilder(size_t nelem) : lw_(nelem, -1), lr_(nelem, -1) {}
-
-    void add(const FxGop &op, const int64_t *reads, int nr, int64_t write)
-    {
-        int w = 0;
-        for (int n = 0; n < nr; ++n) {
-            w = std::max(w, lw_[reads[n]] + 1);
-        }
-        w = std::max(w, lw_[write] + 1);
-        w = std::max(w, lr_[write] + 1);
-        for (int n = 0; n < nr; ++n) {
-            lr_[reads[n]] = std::max(lr_[reads[n]], w);
-        }
-        lw_[write] = w;
-        if ((int)waves_.size() <= w) {
-            waves_.resize(w + 1);
-        }
-        waves_[w].push_back(op);
-    }
-
-    void finish(FxProgram &prog)
-    {
-        prog.ops.clear();
-        prog.wave_begin.clear();
-        for (auto &wv : waves_) {
-            /* grouping by type keeps warps on one code path */
-            std::stable_sort(wv.begin(), wv.end(), [](const FxGop &a, const FxGop &b) {
-                return a.type < b.type || (a.type == b.type && a.dst < b.dst);
-            });
-            prog.wave_begin.push_back((int)prog.ops.size());
-            prog.ops.insert(prog.ops.end(), wv.begin(), wv.end());
-        }
-        prog.wave_begin.push_back((int)prog.ops.size());
-    }
-
-private:
-    std::vector<int> lw_;
-    std::vector<int> lr_;
-    std::vector<std::vector<FxGop>> waves_;
-};
 
 inline int lidx(int i, int j, int k) { return fx_lidx(i, j, k); }
 inline int fidx(int dir, int i, int j, int k) { return fx_face_idx(dir, i, j, k); }
@@ -112,13 +81,25 @@ bool face_active(int dir, int i, int j, int k)
     return true;
 }
 
+/* one landed write of the reference sequence */
+struct SeqOp {
+    FxGop op;
+    int64_t w;         /* element written */
+    int64_t src;       /* single source element, -1 for multi-source ops */
+    int src_ver;       /* producer of the source value (op index, -1 initial) */
+    int space;
+    int prod_begin;    /* producers of the values read: [prod_begin, prod_end) */
+    int prod_end;
+};
+
 class Compiler {
 public:
     Compiler(const fx_config &cfg, int nblocks, const fx_block_desc *blocks)
         : cfg_(cfg), n_(nblocks), b_(blocks),
-          cells_((size_t)nblocks * FX_NCELLS),
-          faces_((size_t)(cfg.mhd ? nblocks : 0) * 3 * FX_NFACES),
-          fid_((size_t)(cfg.mhd ? nblocks : 0) * 3 * FX_NFACES, 0)
+          ncell_((int64_t)nblocks * FX_NCELLS),
+          nface_((int64_t)(cfg.mhd ? nblocks : 0) * 3 * FX_NFACES),
+          fid_((size_t)nface_, 0),
+          ver_((size_t)(2 * ncell_ + nface_), -1)
     {
     }
 
@@ -133,12 +114,11 @@ public:
         if (!validate()) {
             return false;
         }
-        /* 1. physical face-only band of every active block */
+        /* the reference sequence */
         for (int b : plan.active) {
             physical(b, PHYS_FACE_ONLY);
         }
         if (cfg_.mhd) {
-            /* 2. fidelity reset and field boundary */
             for (int b : plan.active) {
                 init_fidelity(b);
             }
@@ -146,8 +126,6 @@ public:
                 if (!physical_bf(b)) return false;
             }
         }
-        /* 3. SAME, RESTRICT, PROLONG passes: cell sends of every block, then
-         * field sends of every block (src/prj_boundary.c:1184-1222) */
         const int passes[3] = {KIND_SAME, KIND_RESTRICT, KIND_PROLONG};
         for (int kind : passes) {
             for (int b : plan.active) {
@@ -159,7 +137,6 @@ public:
                 }
             }
         }
-        /* 4. edge/corner physical band, then the field boundary again */
         for (int b : plan.active) {
             physical(b, PHYS_EDGE_CORNER);
         }
@@ -168,8 +145,7 @@ public:
                 if (!physical_bf(b)) return false;
             }
         }
-        cells_.finish(plan.cells);
-        faces_.finish(plan.faces);
+        finish(plan);
         return true;
     }
 
@@ -199,7 +175,77 @@ private:
     }
 
     int64_t cell_elem(int b, int c) const { return (int64_t)b * FX_NCELLS + c; }
-    int64_t face_elem(int b, int dir, int f) const { return ((int64_t)b * 3 + dir) * FX_NFACES + f; }
+    int64_t cellb_elem(int b, int c) const { return ncell_ + (int64_t)b * FX_NCELLS + c; }
+    int64_t face_elem(int b, int dir, int f) const { return 2 * ncell_ + ((int64_t)b * 3 + dir) * FX_NFACES + f; }
+
+    /* ---- recording -------------------------------------------------------- */
+
+    bool is_plain_copy(const SeqOp &o) const
+    {
+        return (o.space == SPACE_CELL && o.op.type == FX_GOP_COPY) ||
+            (o.space == SPACE_FACE && o.op.type == FX_FOP_COPY);
+    }
+
+    /* follow plain-copy producers back to the oldest element that still
+     * holds the same value; returns the element and its producer */
+    void resolve(int64_t &e, int &v, long long *count) const
+    {
+        while (v >= 0) {
+            const SeqOp &p = seq_[v];
+            if (!is_plain_copy(p) || ver_[p.src] != p.src_ver) {
+                break;
+            }
+            e = p.src;
+            v = p.src_ver;
+            if (count) ++*count;
+        }
+    }
+
+    static int32_t cell_key(int64_t e) { return (int32_t)(((e / FX_NCELLS) << 13) | (e % FX_NCELLS)); }
+
+    int32_t face_key(int64_t e) const
+    {
+        const int64_t r = e - 2 * ncell_;
+        const int64_t bd = r / FX_NFACES;
+        return (int32_t)(((bd / 3) << 15) | (r % FX_NFACES));
+    }
+
+    void add_single(FxGop op, int space, int64_t src, int64_t w)
+    {
+        SeqOp s;
+        int v = ver_[src];
+        resolve(src, v, &stats_.rewired);
+        op.src = space == SPACE_CELL ? cell_key(src) : face_key(src);
+        s.op = op;
+        s.w = w;
+        s.src = src;
+        s.src_ver = v;
+        s.space = space;
+        s.prod_begin = (int)prod_.size();
+        prod_.push_back(v);
+        s.prod_end = (int)prod_.size();
+        rd_.push_back(src);
+        seq_.push_back(s);
+        ver_[w] = (int)seq_.size() - 1;
+    }
+
+    void add_multi(FxGop op, int space, const int64_t *reads, int nr, int64_t w)
+    {
+        SeqOp s;
+        s.op = op;
+        s.w = w;
+        s.src = -1;
+        s.src_ver = -1;
+        s.space = space;
+        s.prod_begin = (int)prod_.size();
+        for (int n = 0; n < nr; ++n) {
+            prod_.push_back(ver_[reads[n]]);
+            rd_.push_back(reads[n]);
+        }
+        s.prod_end = (int)prod_.size();
+        seq_.push_back(s);
+        ver_[w] = (int)seq_.size() - 1;
+    }
 
     bool on_side(const fx_block_desc &blk, int axis, int side) const
     {
@@ -255,7 +301,6 @@ private:
                     const int sc = lidx(src[0], src[1], src[2]);
                     FxGop op;
                     op.dst = FX_CELL_KEY(b, dc);
-                    op.src = FX_CELL_KEY(b, sc);
                     if (bc == FX_BC_REFLECT) {
                         op.type = FX_GOP_COPY_NEG;
                         op.aux = FX_V1 + axis;
@@ -266,8 +311,7 @@ private:
                         op.type = FX_GOP_COPY;
                         op.aux = 0;
                     }
-                    const int64_t r = cell_elem(b, sc);
-                    cells_.add(op, &r, 1, cell_elem(b, dc));
+                    add_single(op, SPACE_CELL, cell_elem(b, sc), cell_elem(b, dc));
                 }
             }
         }
@@ -302,16 +346,13 @@ private:
                         if (sl.rel_level == 0) {
                             const int sc = lidx(i + sl.send_loc_start[0], j + sl.send_loc_start[1],
                                 k + sl.send_loc_start[2]);
-                            op.src = FX_CELL_KEY(b, sc);
                             op.type = FX_GOP_COPY;
-                            const int64_t r = cell_elem(b, sc);
-                            cells_.add(op, &r, 1, cell_elem(id, dc));
+                            add_single(op, SPACE_CELL, cell_elem(b, sc), cell_elem(id, dc));
                         } else if (sl.rel_level == -1) {
                             const int si = 2 * i + sl.send_loc_start[0];
                             const int sj = 2 * j + sl.send_loc_start[1];
                             const int sk2 = 2 * k + sl.send_loc_start[2];
-                            const int sc = lidx(si, sj, sk2);
-                            op.src = FX_CELL_KEY(b, sc);
+                            op.src = FX_CELL_KEY(b, lidx(si, sj, sk2));
                             op.type = FX_GOP_RESTRICT;
                             int64_t r[8];
                             int q = 0;
@@ -319,7 +360,7 @@ private:
                                 for (int dj = 0; dj < 2; ++dj)
                                     for (int dk = 0; dk < 2; ++dk)
                                         r[q++] = cell_elem(b, lidx(si + di, sj + dj, sk2 + dk));
-                            cells_.add(op, r, 8, cell_elem(id, dc));
+                            add_multi(op, SPACE_CELL, r, 8, cell_elem(id, dc));
                         } else {
                             const int ci = i / 2 + sl.send_loc_start[0];
                             const int cj = j / 2 + sl.send_loc_start[1];
@@ -335,7 +376,7 @@ private:
                                 for (int dj = -1; dj <= 1; ++dj)
                                     for (int dk = -1; dk <= 1; ++dk)
                                         r[q++] = cell_elem(b, lidx(ci + di, cj + dj, ck + dk));
-                            cells_.add(op, r, 27, cell_elem(id, dc));
+                            add_multi(op, SPACE_CELL, r, 27, cell_elem(id, dc));
                         }
                     }
                 }
@@ -346,7 +387,7 @@ private:
 
     /* ---- face field ------------------------------------------------------ */
 
-    int &fid(int b, int dir, int f) { return fid_[face_elem(b, dir, f)]; }
+    int &fid(int b, int dir, int f) { return fid_[((int64_t)b * 3 + dir) * FX_NFACES + f]; }
 
     /* prj_boundary_init_face_fidelity, src/prj_boundary.c:840-873 */
     void init_fidelity(int b)
@@ -364,16 +405,16 @@ private:
 
     /* prj_boundary_write_bf_face, src/prj_boundary.c:599-625: a write lands
      * when its fidelity is at least the face's current fidelity. */
-    void write_face(int db, int dir, int df, const FxGop &op, const int64_t *reads, int nr, int fidelity)
+    bool lands(int db, int dir, int df, int fidelity)
     {
         int &cur = fid(db, dir, df);
         if (fidelity < cur) {
-            return;
+            return false;
         }
-        faces_.add(op, reads, nr, face_elem(db, dir, df));
         if (fidelity > cur) {
             cur = fidelity;
         }
+        return true;
     }
 
     /* prj_boundary_physical_bf + prj_boundary_apply_bf_axis
@@ -415,13 +456,12 @@ private:
                         const int fidelity = fid(b, dir, sf);
                         if (fidelity == FID_NONE) continue;
                         const int df = fidx(dir, i, j, k);
+                        if (!lands(b, dir, df, fidelity)) continue;
                         FxGop op;
                         op.dst = (b << 15) | df;
-                        op.src = (b << 15) | sf;
                         op.aux = dir;
                         op.type = FX_FOP_COPY;
-                        const int64_t r = face_elem(b, dir, sf);
-                        write_face(b, dir, df, op, &r, 1, fidelity);
+                        add_single(op, SPACE_FACE, face_elem(b, dir, sf), face_elem(b, dir, df));
                     }
                 }
             }
@@ -446,7 +486,10 @@ private:
         return true;
     }
 
-    /* prj_boundary_copy_bf_same_level, src/prj_boundary.c:627-693 */
+    /* prj_boundary_copy_bf_same_level, src/prj_boundary.c:627-693.  The
+     * reference buffers the source faces before writing; source and
+     * destination are different blocks, so element operations are
+     * equivalent. */
     void copy_same_level(int src_b, int dst_b, const fx_slot &sl)
     {
         for (int dir = 0; dir < 3; ++dir) {
@@ -463,13 +506,12 @@ private:
                         const int sf = fidx(dir, i + sl.send_loc_start[0], j + sl.send_loc_start[1],
                             k + sl.send_loc_start[2]);
                         const int df = fidx(dir, ri, rj, rk);
+                        if (!lands(dst_b, dir, df, FID_SAME)) continue;
                         FxGop op;
                         op.dst = (dst_b << 15) | df;
-                        op.src = (src_b << 15) | sf;
                         op.aux = dir;
                         op.type = FX_FOP_COPY;
-                        const int64_t r = face_elem(src_b, dir, sf);
-                        write_face(dst_b, dir, df, op, &r, 1, FID_SAME);
+                        add_single(op, SPACE_FACE, face_elem(src_b, dir, sf), face_elem(dst_b, dir, df));
                     }
                 }
             }
@@ -498,6 +540,7 @@ private:
                             2 * k + sl.send_loc_start[2]);
                         const int df = fidx(dir, i + sl.recv_loc_start[0], j + sl.recv_loc_start[1],
                             k + sl.recv_loc_start[2]);
+                        if (!lands(coarse, dir, df, FID_FINER)) continue;
                         FxGop op;
                         op.dst = (coarse << 15) | df;
                         op.src = (fine << 15) | s0;
@@ -505,19 +548,133 @@ private:
                         op.type = FX_FOP_RESTRICT;
                         const int64_t r[4] = {face_elem(fine, dir, s0), face_elem(fine, dir, s0 + o1),
                             face_elem(fine, dir, s0 + o0), face_elem(fine, dir, s0 + o0 + o1)};
-                        write_face(coarse, dir, df, op, r, 4, FID_FINER);
+                        add_multi(op, SPACE_FACE, r, 4, face_elem(coarse, dir, df));
                     }
                 }
             }
         }
     }
 
+    /* ---- optimisation and levelling -------------------------------------- */
+
+    void finish(FxPlan &plan)
+    {
+        const int nseq = (int)seq_.size();
+        /* 2. liveness in reverse order: final versions are live; an op is
+         * live when a live op reads its value */
+        std::vector<int> readers(nseq, 0);
+        std::vector<char> live(nseq, 0);
+        for (int x = nseq - 1; x >= 0; --x) {
+            const SeqOp &o = seq_[x];
+            if (seq_[x].space == SPACE_CELL) ++stats_.emitted_cell_ops;
+            else ++stats_.emitted_face_ops;
+            live[x] = (ver_[o.w] == x) || readers[x] > 0;
+            if (!live[x]) {
+                ++stats_.dead;
+                continue;
+            }
+            for (int p = o.prod_begin; p < o.prod_end; ++p) {
+                if (prod_[p] >= 0) ++readers[prod_[p]];
+            }
+        }
+        /* 3. cell-field operations */
+        std::vector<FxBop> bops;
+        std::vector<std::array<int64_t, 6>> bop_reads;
+        if (cfg_.mhd) {
+            for (int b : plan.active) {
+                for (int i = -NG; i < BS + NG; ++i) {
+                    for (int j = -NG; j < BS + NG; ++j) {
+                        for (int k = -NG; k < BS + NG; ++k) {
+                            const bool ghost = i < 0 || i >= BS || j < 0 || j >= BS || k < 0 || k >= BS;
+                            int64_t f[6] = {
+                                face_elem(b, 0, fidx(0, i, j, k)), face_elem(b, 0, fidx(0, i + 1, j, k)),
+                                face_elem(b, 1, fidx(1, i, j, k)), face_elem(b, 1, fidx(1, i, j + 1, k)),
+                                face_elem(b, 2, fidx(2, i, j, k)), face_elem(b, 2, fidx(2, i, j, k + 1))};
+                            bool touched = false;
+                            for (int q = 0; q < 6; ++q) {
+                                if (ver_[f[q]] >= 0) touched = true;
+                            }
+                            if (!ghost && !touched) continue;
+                            FxBop bo;
+                            bo.dst = FX_CELL_KEY(b, lidx(i, j, k));
+                            bo.pad = 0;
+                            std::array<int64_t, 6> rr;
+                            for (int q = 0; q < 6; ++q) {
+                                int v = ver_[f[q]];
+                                int64_t e = f[q];
+                                resolve(e, v, &stats_.rewired);
+                                bo.f[q] = face_key(e);
+                                rr[q] = e;
+                            }
+                            bops.push_back(bo);
+                            bop_reads.push_back(rr);
+                        }
+                    }
+                }
+            }
+        }
+        /* 4. levelling over cell, cell-field and face elements */
+        std::vector<int> lw((size_t)(2 * ncell_ + nface_), -1);
+        std::vector<int> lr((size_t)(2 * ncell_ + nface_), -1);
+        std::vector<std::vector<FxGop>> wc, wf;
+        std::vector<std::vector<FxBop>> wb;
+        auto place = [&](const int64_t *reads, int nr, int64_t w) {
+            int wave = 0;
+            for (int n = 0; n < nr; ++n) wave = std::max(wave, lw[reads[n]] + 1);
+            wave = std::max(wave, lw[w] + 1);
+            wave = std::max(wave, lr[w] + 1);
+            for (int n = 0; n < nr; ++n) lr[reads[n]] = std::max(lr[reads[n]], wave);
+            lw[w] = wave;
+            if ((int)wc.size() <= wave) {
+                wc.resize(wave + 1);
+                wf.resize(wave + 1);
+                wb.resize(wave + 1);
+            }
+            return wave;
+        };
+        for (int x = 0; x < nseq; ++x) {
+            if (!live[x]) continue;
+            const SeqOp &o = seq_[x];
+            const int nr = o.prod_end - o.prod_begin;
+            const int wave = place(&rd_[o.prod_begin], nr, o.w);
+            (o.space == SPACE_CELL ? wc : wf)[wave].push_back(o.op);
+        }
+        for (size_t q = 0; q < bops.size(); ++q) {
+            const int64_t w = cellb_elem(FX_CELL_BLOCK(bops[q].dst), FX_CELL_IDX(bops[q].dst));
+            const int wave = place(bop_reads[q].data(), 6, w);
+            wb[wave].push_back(bops[q]);
+        }
+        FxProgram &g = plan.ghost;
+        auto by_type = [](const FxGop &a, const FxGop &b) {
+            return a.type < b.type || (a.type == b.type && a.dst < b.dst);
+        };
+        for (size_t w = 0; w < wc.size(); ++w) {
+            std::stable_sort(wc[w].begin(), wc[w].end(), by_type);
+            std::stable_sort(wf[w].begin(), wf[w].end(), by_type);
+            g.cell_begin.push_back((int)g.cell_ops.size());
+            g.face_begin.push_back((int)g.face_ops.size());
+            g.b_begin.push_back((int)g.b_ops.size());
+            g.cell_ops.insert(g.cell_ops.end(), wc[w].begin(), wc[w].end());
+            g.face_ops.insert(g.face_ops.end(), wf[w].begin(), wf[w].end());
+            g.b_ops.insert(g.b_ops.end(), wb[w].begin(), wb[w].end());
+        }
+        g.cell_begin.push_back((int)g.cell_ops.size());
+        g.face_begin.push_back((int)g.face_ops.size());
+        g.b_begin.push_back((int)g.b_ops.size());
+        plan.stats = stats_;
+    }
+
     const fx_config &cfg_;
     int n_;
     const fx_block_desc *b_;
-    WaveBuilder cells_;
-    WaveBuilder faces_;
+    int64_t ncell_;
+    int64_t nface_;
     std::vector<int> fid_;
+    std::vector<int> ver_;       /* element -> producer op (-1: initial value) */
+    std::vector<SeqOp> seq_;
+    std::vector<int> prod_;      /* producers of the values each op reads */
+    std::vector<int64_t> rd_;    /* elements each op reads (parallel to prod_) */
+    FxPlanStats stats_;
     std::string *err_ = nullptr;
 };
 

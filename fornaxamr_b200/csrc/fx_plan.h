@@ -10,18 +10,31 @@
 #include "../../include/fornax_b200.h"
 #include "fx_kernels.h"
 
-/* A program is a list of element operations grouped into waves.  Operations
- * inside one wave touch disjoint elements (no read/write or write/write
- * overlap), so a wave runs as one parallel kernel; waves run in order. */
+/* The ghost fill as waves of element operations.  Operations inside one
+ * wave touch disjoint elements (no read/write or write/write overlap), so a
+ * wave runs as one parallel kernel; waves run in order.  Each wave holds
+ * cell operations (primitives 0..5), face operations and cell-field
+ * operations (bf2bc of one cell). */
 struct FxProgram {
-    std::vector<FxGop> ops;
-    std::vector<int> wave_begin; /* ops of wave w are [wave_begin[w], wave_begin[w+1]) */
-    int nwaves() const { return wave_begin.empty() ? 0 : (int)wave_begin.size() - 1; }
+    std::vector<FxGop> cell_ops;
+    std::vector<FxGop> face_ops;
+    std::vector<FxBop> b_ops;
+    std::vector<int> cell_begin; /* per wave: [begin, next begin) into cell_ops */
+    std::vector<int> face_begin;
+    std::vector<int> b_begin;
+    int nwaves() const { return cell_begin.empty() ? 0 : (int)cell_begin.size() - 1; }
+};
+
+struct FxPlanStats {
+    long long emitted_cell_ops = 0; /* writes that land in the reference sequence */
+    long long emitted_face_ops = 0;
+    long long rewired = 0;          /* copies redirected to an earlier source */
+    long long dead = 0;             /* overwritten before any read: dropped */
 };
 
 struct FxPlan {
-    FxProgram cells;                /* W ghost cells (primitive vars except cell B) */
-    FxProgram faces;                /* Bf ghost faces (MHD) */
+    FxProgram ghost;
+    FxPlanStats stats;
     std::vector<FxCorr> flux_corr;  /* prj_riemann_flux_send records */
     std::vector<FxCorr> emf_corr;   /* prj_mhd_emf_send records */
     std::vector<int> active;        /* active block indices in mesh order */

@@ -46,6 +46,7 @@ struct fx_ctx {
     int *d_active = nullptr;
     int nactive = 0;
     FxGop *d_cops = nullptr, *d_fops = nullptr;
+    FxBop *d_bops = nullptr;
     FxCorr *d_fcorr = nullptr, *d_ecorr = nullptr;
 
     FxErr *d_err = nullptr;
@@ -174,6 +175,8 @@ void free_mesh(fx_ctx *c)
     cudaFree(c->d_active);
     cudaFree(c->d_cops);
     cudaFree(c->d_fops);
+    cudaFree(c->d_bops);
+    c->d_bops = nullptr;
     cudaFree(c->d_fcorr);
     cudaFree(c->d_ecorr);
     c->d_blk = nullptr;
@@ -202,20 +205,17 @@ void per_block(fx_ctx *c, int form, F &&fn)
     }
 }
 
-void ghost_fill(fx_ctx *c, int form, int slot)
+/* the whole ghost fill of prj_boundary_fill_ghosts_and_bf: one launch per
+ * conflict-free wave of the compiled program (a single launch on
+ * single-level meshes) */
+void ghost_fill(fx_ctx *c, int slot)
 {
-    const FxProgram &cp = c->plan.cells;
-    for (int w = 0; w < cp.nwaves(); ++w) {
-        fx_launch_ghost_cells(c->D, c->d_cops + cp.wave_begin[w], cp.wave_begin[w + 1] - cp.wave_begin[w],
-            slot, 6, c->stream);
-    }
-    if (c->cfg.mhd) {
-        const FxProgram &fp = c->plan.faces;
-        for (int w = 0; w < fp.nwaves(); ++w) {
-            fx_launch_ghost_faces(c->D, c->d_fops + fp.wave_begin[w],
-                fp.wave_begin[w + 1] - fp.wave_begin[w], slot, c->stream);
-        }
-        per_block(c, form, [&](const int *l, int n) { fx_launch_bf2bc(c->D, l, n, slot, c->stream); });
+    const FxProgram &g = c->plan.ghost;
+    for (int w = 0; w < g.nwaves(); ++w) {
+        fx_launch_ghost_wave(c->D,
+            c->d_cops + g.cell_begin[w], g.cell_begin[w + 1] - g.cell_begin[w],
+            c->d_fops + g.face_begin[w], g.face_begin[w + 1] - g.face_begin[w],
+            c->d_bops + g.b_begin[w], g.b_begin[w + 1] - g.b_begin[w], slot, 6, c->stream);
     }
 }
 
@@ -226,11 +226,7 @@ void stage_seq(fx_ctx *c, int form, int stage)
     const int dst = stage == 1 ? 1 : 0; /* W slot the update writes */
     cudaStream_t s = c->stream;
     const int full = form == FX_FORM_PLAIN ? 1 : 0;
-    per_block(c, form, [&](const int *l, int n) {
-        for (int dir = 0; dir < 3; ++dir) {
-            fx_launch_flux(c->D, l, n, dir, src, src, full, s);
-        }
-    });
+    per_block(c, form, [&](const int *l, int n) { fx_launch_flux(c->D, l, n, 3, src, src, full, s); });
     fx_launch_flux_correct(c->D, c->d_fcorr, (int)c->plan.flux_corr.size(), s);
     if (c->cfg.mhd) {
         per_block(c, form, [&](const int *l, int n) { fx_launch_emf(c->D, l, n, src, src, s); });
@@ -243,7 +239,7 @@ void stage_seq(fx_ctx *c, int form, int stage)
     if (form == FX_FORM_PLAIN) {
         per_block(c, form, [&](const int *l, int n) { fx_launch_eos_fill(c->D, l, n, dst, 1, s); });
     }
-    ghost_fill(c, form, dst);
+    ghost_fill(c, dst);
     if (form == FX_FORM_PLAIN) {
         per_block(c, form, [&](const int *l, int n) { fx_launch_eos_fill(c->D, l, n, dst, 0, s); });
     }
@@ -444,8 +440,9 @@ int fx_set_mesh(fx_ctx *c, int nblocks, const fx_block_desc *blocks)
     }
     if ((rc = dev_alloc(c, &c->d_ids, nb))) return rc;
     if ((rc = dev_alloc(c, &c->d_active, (size_t)c->nactive))) return rc;
-    if ((rc = dev_alloc(c, &c->d_cops, c->plan.cells.ops.size()))) return rc;
-    if ((rc = dev_alloc(c, &c->d_fops, c->plan.faces.ops.size()))) return rc;
+    if ((rc = dev_alloc(c, &c->d_cops, c->plan.ghost.cell_ops.size()))) return rc;
+    if ((rc = dev_alloc(c, &c->d_fops, c->plan.ghost.face_ops.size()))) return rc;
+    if ((rc = dev_alloc(c, &c->d_bops, c->plan.ghost.b_ops.size()))) return rc;
     if ((rc = dev_alloc(c, &c->d_fcorr, c->plan.flux_corr.size()))) return rc;
     if ((rc = dev_alloc(c, &c->d_ecorr, c->plan.emf_corr.size()))) return rc;
 
@@ -467,13 +464,20 @@ int fx_set_mesh(fx_ctx *c, int nblocks, const fx_block_desc *blocks)
         FX_CUDA(c, cudaMemcpy(c->d_active, c->plan.active.data(), (size_t)c->nactive * sizeof(int),
             cudaMemcpyHostToDevice));
     }
-    if (!c->plan.cells.ops.empty()) {
-        FX_CUDA(c, cudaMemcpy(c->d_cops, c->plan.cells.ops.data(), c->plan.cells.ops.size() * sizeof(FxGop),
-            cudaMemcpyHostToDevice));
-    }
-    if (!c->plan.faces.ops.empty()) {
-        FX_CUDA(c, cudaMemcpy(c->d_fops, c->plan.faces.ops.data(), c->plan.faces.ops.size() * sizeof(FxGop),
-            cudaMemcpyHostToDevice));
+    {
+        const FxProgram &g = c->plan.ghost;
+        if (!g.cell_ops.empty()) {
+            FX_CUDA(c, cudaMemcpy(c->d_cops, g.cell_ops.data(), g.cell_ops.size() * sizeof(FxGop),
+                cudaMemcpyHostToDevice));
+        }
+        if (!g.face_ops.empty()) {
+            FX_CUDA(c, cudaMemcpy(c->d_fops, g.face_ops.data(), g.face_ops.size() * sizeof(FxGop),
+                cudaMemcpyHostToDevice));
+        }
+        if (!g.b_ops.empty()) {
+            FX_CUDA(c, cudaMemcpy(c->d_bops, g.b_ops.data(), g.b_ops.size() * sizeof(FxBop),
+                cudaMemcpyHostToDevice));
+        }
     }
     if (!c->plan.flux_corr.empty()) {
         FX_CUDA(c, cudaMemcpy(c->d_fcorr, c->plan.flux_corr.data(), c->plan.flux_corr.size() * sizeof(FxCorr),
@@ -502,7 +506,7 @@ int fx_set_mesh(fx_ctx *c, int nblocks, const fx_block_desc *blocks)
 int fx_plan_export(const fx_config *cfg, int nblocks, const fx_block_desc *blocks, int which,
     int32_t *ops, int *nops, int32_t *wave_begin, int *nwaves)
 {
-    if (!cfg || nblocks <= 0 || !blocks || !nops || !nwaves || which < 0 || which > 3) {
+    if (!cfg || nblocks <= 0 || !blocks || !nops || !nwaves || which < 0 || which > 5) {
         return FX_EINVAL;
     }
     FxPlan plan;
@@ -510,16 +514,31 @@ int fx_plan_export(const fx_config *cfg, int nblocks, const fx_block_desc *block
     if (!fx_build_plan(*cfg, nblocks, blocks, plan, &perr)) {
         return FX_EINVAL;
     }
-    if (which <= 1) {
-        const FxProgram &p = which == 0 ? plan.cells : plan.faces;
-        if (ops && (int)p.ops.size() <= *nops) {
-            std::memcpy(ops, p.ops.data(), p.ops.size() * sizeof(FxGop));
+    const FxProgram &g = plan.ghost;
+    if (which <= 1 || which == 4) {
+        const void *data = which == 0 ? (const void *)g.cell_ops.data() :
+            which == 1 ? (const void *)g.face_ops.data() : (const void *)g.b_ops.data();
+        const size_t count = which == 0 ? g.cell_ops.size() : which == 1 ? g.face_ops.size() : g.b_ops.size();
+        const size_t size = which == 4 ? sizeof(FxBop) : sizeof(FxGop);
+        const std::vector<int> &wb = which == 0 ? g.cell_begin : which == 1 ? g.face_begin : g.b_begin;
+        if (ops && (int)count <= *nops && count) {
+            std::memcpy(ops, data, count * size);
         }
-        if (wave_begin && p.nwaves() <= *nwaves) {
-            std::memcpy(wave_begin, p.wave_begin.data(), p.wave_begin.size() * sizeof(int));
+        if (wave_begin && g.nwaves() <= *nwaves) {
+            std::memcpy(wave_begin, wb.data(), wb.size() * sizeof(int));
         }
-        *nops = (int)p.ops.size();
-        *nwaves = p.nwaves();
+        *nops = (int)count;
+        *nwaves = g.nwaves();
+    } else if (which == 5) {
+        /* statistics: emitted cell ops, emitted face ops, rewired, dead */
+        if (ops && *nops >= 4) {
+            ops[0] = (int32_t)plan.stats.emitted_cell_ops;
+            ops[1] = (int32_t)plan.stats.emitted_face_ops;
+            ops[2] = (int32_t)plan.stats.rewired;
+            ops[3] = (int32_t)plan.stats.dead;
+        }
+        *nops = 4;
+        *nwaves = g.nwaves();
     } else {
         const std::vector<FxCorr> &r = which == 2 ? plan.flux_corr : plan.emf_corr;
         if (ops && (int)r.size() <= *nops) {
@@ -702,9 +721,7 @@ int fx_flux_update(fx_ctx *c, int b, int w_slot, int use_bf1)
     if (rc) return rc;
     if (w_slot < 0 || w_slot > 1 || use_bf1 < 0 || use_bf1 > 1) return set_err(c, FX_EINVAL, "bad slot");
     fx_launch_set_dt(c->D, 0.0, c->stream);
-    for (int dir = 0; dir < 3; ++dir) {
-        fx_launch_flux(c->D, c->d_ids + b, 1, dir, w_slot, use_bf1, 1, c->stream);
-    }
+    fx_launch_flux(c->D, c->d_ids + b, 1, 3, w_slot, use_bf1, 1, c->stream);
     return FX_SUCCESS;
 }
 
@@ -791,7 +808,7 @@ int fx_boundary_fill_ghosts_and_bf(fx_ctx *c, int stage, int use_bf1)
         return set_err(c, FX_EINVAL, "fx_boundary_fill_ghosts_and_bf: W slot and Bf slot must agree");
     }
     fx_launch_set_dt(c->D, 0.0, c->stream);
-    ghost_fill(c, FX_FORM_BATCHED, slot);
+    ghost_fill(c, slot);
     return FX_SUCCESS;
 }
 
@@ -921,11 +938,11 @@ int fx_time_phase(fx_ctx *c, int phase, int reps, double dt, double *ms)
     cudaStream_t s = c->stream;
     auto launch = [&]() {
         switch (phase) {
-        case FX_PHASE_FLUX: fx_launch_flux(c->D, c->d_active, c->nactive, 0, 0, 0, 0, s); break;
+        case FX_PHASE_FLUX: fx_launch_flux(c->D, c->d_active, c->nactive, 3, 0, 0, 0, s); break;
         case FX_PHASE_EMF: fx_launch_emf(c->D, c->d_active, c->nactive, 0, 0, s); break;
         case FX_PHASE_CT: fx_launch_bf_update(c->D, c->d_active, c->nactive, 1, s); break;
         case FX_PHASE_CELLS: fx_launch_cell_update(c->D, c->d_active, c->nactive, 1, c->cfg.gravity, 0, s); break;
-        case FX_PHASE_GHOST: ghost_fill(c, FX_FORM_BATCHED, 1); break;
+        case FX_PHASE_GHOST: ghost_fill(c, 1); break;
         default: cudaGraphLaunch(c->g_step, s); break;
         }
     };
@@ -949,25 +966,61 @@ int fx_time_phase(fx_ctx *c, int phase, int reps, double dt, double *ms)
     return check_device_error(c);
 }
 
+int fx_autotune(fx_ctx *c, double *times_ms, int n, int *choice)
+{
+    if (!has_mesh(c) || !choice) return c ? set_err(c, FX_EINVAL, "fx_autotune: no mesh") : FX_EINVAL;
+    cudaStream_t s = c->stream;
+    cudaEvent_t e0, e1;
+    FX_CUDA(c, cudaEventCreate(&e0));
+    FX_CUDA(c, cudaEventCreate(&e1));
+    fx_launch_set_dt(c->D, 0.0, s);
+    int best = 0;
+    double best_ms = 1.0e30;
+    for (int v = 0; v < FX_FLUX_VARIANTS; ++v) {
+        c->D.flux_variant = v;
+        fx_launch_flux(c->D, c->d_active, c->nactive, 3, 0, 0, 0, s);
+        FX_CUDA(c, cudaEventRecord(e0, s));
+        for (int r = 0; r < 3; ++r) {
+            fx_launch_flux(c->D, c->d_active, c->nactive, 3, 0, 0, 0, s);
+        }
+        FX_CUDA(c, cudaEventRecord(e1, s));
+        FX_CUDA(c, cudaEventSynchronize(e1));
+        float t = 0.0f;
+        FX_CUDA(c, cudaEventElapsedTime(&t, e0, e1));
+        const double ms = (double)t / 3.0;
+        if (times_ms && v < n) times_ms[v] = ms;
+        if (ms < best_ms) {
+            best_ms = ms;
+            best = v;
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    c->D.flux_variant = best;
+    free_graphs(c); /* captured graphs hold the previous launch shape */
+    *choice = best;
+    return check_device_error(c);
+}
+
 int fx_info(fx_ctx *c, int what, long long *value)
 {
     if (!has_mesh(c) || !value) return c ? set_err(c, FX_EINVAL, "fx_info: no mesh") : FX_EINVAL;
-    const long long cw = c->plan.cells.nwaves();
-    const long long fw = c->cfg.mhd ? c->plan.faces.nwaves() : 0;
+    const FxProgram &g = c->plan.ghost;
+    const long long gw = g.nwaves();
     const long long corr = (c->plan.flux_corr.empty() ? 0 : 1) +
         (c->cfg.mhd && !c->plan.emf_corr.empty() ? 1 : 0);
     const long long mhd = c->cfg.mhd ? 1 : 0;
     switch (what) {
-    case 0: /* reset + 2 x (3 flux + emf + ct + cells + waves + bf2bc) */
-        *value = 1 + 2 * (3 + 2 * mhd + 1 + corr + cw + fw + mhd);
+    case 0: /* reset + 2 x (flux + emf + ct + cells + ghost waves) */
+        *value = 1 + 2 * (1 + 2 * mhd + 1 + corr + gw);
         break;
-    case 1: /* set_dt + reset + 2 x per-block phases + mesh-level ghost waves */
-        *value = 2 + 2 * ((long long)c->nactive * (3 + 2 * mhd + 1 + 2 + mhd) + corr + cw + fw);
+    case 1: /* set_dt + reset + 2 x (per-block phases + eos fills) + ghost waves */
+        *value = 2 + 2 * ((long long)c->nactive * (1 + 2 * mhd + 1 + 2) + corr + gw);
         break;
-    case 2: *value = (long long)c->plan.cells.ops.size(); break;
-    case 3: *value = (long long)c->plan.faces.ops.size(); break;
-    case 4: *value = cw; break;
-    case 5: *value = fw; break;
+    case 2: *value = (long long)g.cell_ops.size(); break;
+    case 3: *value = (long long)g.face_ops.size(); break;
+    case 4: *value = gw; break;
+    case 5: *value = (long long)g.b_ops.size(); break;
     default: return set_err(c, FX_EINVAL, "fx_info: unknown query");
     }
     return FX_SUCCESS;

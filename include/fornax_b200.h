@@ -202,7 +202,7 @@ int fx_run(fx_ctx *ctx, int form, int nsteps, double cfl, double dt_factor, doub
 /* ---- measurement --------------------------------------------------------------- */
 
 /* phases for fx_time_phase: the batched sweep of one phase over all blocks */
-#define FX_PHASE_FLUX 0      /* one face-flux launch (direction x) */
+#define FX_PHASE_FLUX 0      /* one face-flux launch (all three directions) */
 #define FX_PHASE_EMF 1       /* edge EMFs */
 #define FX_PHASE_CT 2        /* CT face update, stage 1 */
 #define FX_PHASE_CELLS 3     /* cell update, stage 1 */
@@ -214,6 +214,12 @@ int fx_run(fx_ctx *ctx, int form, int nsteps, double cfl, double dt_factor, doub
  * Phases 0-4 rewrite the stage-1 scratch only, so repeating them leaves the
  * mesh state unchanged; phase 5 advances the state by reps steps with dt. */
 int fx_time_phase(fx_ctx *ctx, int phase, int reps, double dt, double *ms);
+
+/* Autotuner: times every compiled launch shape of the face-flux kernel (the
+ * dominant phase) on the current mesh and keeps the fastest for all later
+ * steps.  times_ms (may be NULL) receives up to `n` per-shape times, *choice
+ * the chosen shape.  The shapes compute identical results. */
+int fx_autotune(fx_ctx *ctx, double *times_ms, int n, int *choice);
 
 /* what = 0: kernel launches per batched step, 1: per plain step,
  * 2/3: ghost cell/face operations, 4/5: ghost cell/face waves */

@@ -87,6 +87,32 @@ def apply_face_program(Bf, ops, waves, slot):
                 raise NotImplementedError(f"face op type {t}")
 
 
+def apply_b_ops(W, Bf, bops, slot):
+    """cell-field operations: W[6+d] of dst = 0.5 (f[2d] + f[2d+1])."""
+    if len(bops) == 0:
+        return
+    db, dc = bops[:, 0] >> 13, bops[:, 0] & 8191
+    for d in range(3):
+        k0, k1 = bops[:, 1 + 2 * d], bops[:, 2 + 2 * d]
+        W[db, 6 + d, slot, dc] = 0.5 * (Bf[k0 >> 15, d, slot, k0 & 32767] + Bf[k1 >> 15, d, slot, k1 & 32767])
+
+
+def apply_ghost_program(W, Bf, cfg, desc, slot):
+    """Runs the compiled ghost fill (fx_plan_export) in numpy, wave by wave."""
+    import fornaxamr_b200 as fx
+    cops, cw = fx.plan_export(cfg, desc, 0)
+    nw = len(cw) - 1
+    if Bf is not None:
+        fops, fw = fx.plan_export(cfg, desc, 1)
+        bops, bw = fx.plan_export(cfg, desc, 4)
+    for w in range(nw):
+        apply_cell_program(W, cops[cw[w]:cw[w + 1]], [0, cw[w + 1] - cw[w]], slot, 6)
+        if Bf is not None:
+            apply_face_program(Bf, fops[fw[w]:fw[w + 1]], [0, fw[w + 1] - fw[w]], slot)
+            apply_b_ops(W, Bf, bops[bw[w]:bw[w + 1]], slot)
+    return nw
+
+
 def bf2bc(W, Bf, slot):
     r = np.arange(-NG, BS + NG)
     i, j, k = np.meshgrid(r, r, r, indexing="ij")
