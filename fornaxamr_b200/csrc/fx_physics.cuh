@@ -696,11 +696,15 @@ __device__ __forceinline__ double fx_emf_upwind(const double f[4], const double 
 
 __device__ __forceinline__ double fx_cell_eta(double rho, double ye)
 {
-    double rho_factor = 0.0;
-    double ye_factor = 0.0;
-    if (isfinite(rho) && rho > 0.0) {
-        rho_factor = fx_max(0.0, log(rho / FX_ETA_RHO_FLOOR));
+    /* max(0, log(x)) is exactly +0 for x <= 1 (log(1) = +0, log(x < 1) < 0),
+     * and 1e12 * 0 * f = +0 for any finite f >= 0: the logarithms are only
+     * evaluated for dense cells, with the reference's arithmetic. */
+    const double xr = rho / FX_ETA_RHO_FLOOR;
+    if (!(isfinite(rho) && rho > 0.0) || !(xr > 1.0)) {
+        return 0.0;
     }
+    double rho_factor = fx_max(0.0, log(xr));
+    double ye_factor = 0.0;
     if (isfinite(ye) && ye > 0.0) {
         ye_factor = fx_max(0.0, log(ye / FX_ETA_YE_THR));
     }

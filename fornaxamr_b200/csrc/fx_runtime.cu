@@ -111,7 +111,8 @@ int check_device_error(fx_ctx *c)
     if (c->sticky) {
         return FX_EPHYSICS;
     }
-    FX_CUDA(c, cudaMemcpy(c->h_err, c->d_err, sizeof(FxErr), cudaMemcpyDeviceToHost));
+    FX_CUDA(c, cudaMemcpyAsync(c->h_err, c->d_err, sizeof(FxErr), cudaMemcpyDeviceToHost, c->stream));
+    FX_CUDA(c, cudaStreamSynchronize(c->stream));
     if (c->h_err->code != 0) {
         c->sticky = 1;
         return set_err(c, FX_EPHYSICS, "%s (block %d, index %d)", err_message(c->h_err->code),
@@ -122,6 +123,7 @@ int check_device_error(fx_ctx *c)
 
 int sync_and_check(fx_ctx *c)
 {
+    FX_CUDA(c, cudaGetLastError()); /* launch failures (configuration, resources) */
     FX_CUDA(c, cudaStreamSynchronize(c->stream));
     return check_device_error(c);
 }
@@ -330,9 +332,13 @@ int fx_create(int device, const fx_config *cfg, fx_ctx **out)
         fx_destroy(c);
         return FX_ECUDA;
     }
-    cudaMemset(c->d_err, 0, sizeof(FxErr));
-    cudaMemset(c->d_ctl, 0, sizeof(FxCtl));
-    cudaMemset(c->d_red, 0, 2 * sizeof(unsigned long long));
+    cudaMemsetAsync(c->d_err, 0, sizeof(FxErr), c->stream);
+    cudaMemsetAsync(c->d_ctl, 0, sizeof(FxCtl), c->stream);
+    cudaMemsetAsync(c->d_red, 0, 2 * sizeof(unsigned long long), c->stream);
+    if (cudaStreamSynchronize(c->stream) != cudaSuccess) {
+        fx_destroy(c);
+        return FX_ECUDA;
+    }
     c->D.nv = c->nv;
     c->D.gamma = cfg->gamma;
     c->D.mhd_eta = cfg->mhd_eta;
@@ -436,7 +442,7 @@ int fx_set_mesh(fx_ctx *c, int nblocks, const fx_block_desc *blocks)
     }
     if (c->cfg.gravity) {
         if ((rc = dev_alloc(c, &c->d_grav, nb * FX_GRAV_COUNT))) return rc;
-        FX_CUDA(c, cudaMemset(c->d_grav, 0, nb * FX_GRAV_COUNT * sizeof(double)));
+        FX_CUDA(c, cudaMemsetAsync(c->d_grav, 0, nb * FX_GRAV_COUNT * sizeof(double), c->stream));
     }
     if ((rc = dev_alloc(c, &c->d_ids, nb))) return rc;
     if ((rc = dev_alloc(c, &c->d_active, (size_t)c->nactive))) return rc;
@@ -446,47 +452,50 @@ int fx_set_mesh(fx_ctx *c, int nblocks, const fx_block_desc *blocks)
     if ((rc = dev_alloc(c, &c->d_fcorr, c->plan.flux_corr.size()))) return rc;
     if ((rc = dev_alloc(c, &c->d_ecorr, c->plan.emf_corr.size()))) return rc;
 
-    /* scratch starts at zero so downloads of never-written entries are defined */
-    FX_CUDA(c, cudaMemset(c->d_W, 0, nb * w_count(c) * sizeof(double)));
-    FX_CUDA(c, cudaMemset(c->d_flux, 0, nb * FX_FLUX_COUNT(c->nv) * sizeof(double)));
-    FX_CUDA(c, cudaMemset(c->d_vr, 0, nb * FX_VR_COUNT * sizeof(double)));
-    FX_CUDA(c, cudaMemset(c->d_eos, 0, nb * FX_EOS_COUNT * sizeof(double)));
-    FX_CUDA(c, cudaMemset(c->d_rhs, 0, nb * FX_RHS_COUNT(c->nv) * sizeof(double)));
+    /* scratch starts at zero so downloads of never-written entries are
+     * defined.  Every device write goes on the context stream: the stream is
+     * non-blocking, so work on the legacy default stream would not be ordered
+     * with it. */
+    cudaStream_t s = c->stream;
+    FX_CUDA(c, cudaMemsetAsync(c->d_W, 0, nb * w_count(c) * sizeof(double), s));
+    FX_CUDA(c, cudaMemsetAsync(c->d_flux, 0, nb * FX_FLUX_COUNT(c->nv) * sizeof(double), s));
+    FX_CUDA(c, cudaMemsetAsync(c->d_vr, 0, nb * FX_VR_COUNT * sizeof(double), s));
+    FX_CUDA(c, cudaMemsetAsync(c->d_eos, 0, nb * FX_EOS_COUNT * sizeof(double), s));
+    FX_CUDA(c, cudaMemsetAsync(c->d_rhs, 0, nb * FX_RHS_COUNT(c->nv) * sizeof(double), s));
     if (c->cfg.mhd) {
-        FX_CUDA(c, cudaMemset(c->d_Bf, 0, nb * FX_BF_COUNT * sizeof(double)));
-        FX_CUDA(c, cudaMemset(c->d_bv1, 0, nb * FX_BV_COUNT * sizeof(double)));
-        FX_CUDA(c, cudaMemset(c->d_bv2, 0, nb * FX_BV_COUNT * sizeof(double)));
-        FX_CUDA(c, cudaMemset(c->d_emf, 0, nb * FX_EMF_COUNT * sizeof(double)));
+        FX_CUDA(c, cudaMemsetAsync(c->d_Bf, 0, nb * FX_BF_COUNT * sizeof(double), s));
+        FX_CUDA(c, cudaMemsetAsync(c->d_bv1, 0, nb * FX_BV_COUNT * sizeof(double), s));
+        FX_CUDA(c, cudaMemsetAsync(c->d_bv2, 0, nb * FX_BV_COUNT * sizeof(double), s));
+        FX_CUDA(c, cudaMemsetAsync(c->d_emf, 0, nb * FX_EMF_COUNT * sizeof(double), s));
     }
-    FX_CUDA(c, cudaMemcpy(c->d_blk, hb.data(), nb * sizeof(FxBlockDev), cudaMemcpyHostToDevice));
-    FX_CUDA(c, cudaMemcpy(c->d_ids, ids.data(), nb * sizeof(int), cudaMemcpyHostToDevice));
+    const cudaMemcpyKind h2d = cudaMemcpyHostToDevice;
+    FX_CUDA(c, cudaMemcpyAsync(c->d_blk, hb.data(), nb * sizeof(FxBlockDev), h2d, s));
+    FX_CUDA(c, cudaMemcpyAsync(c->d_ids, ids.data(), nb * sizeof(int), h2d, s));
     if (c->nactive) {
-        FX_CUDA(c, cudaMemcpy(c->d_active, c->plan.active.data(), (size_t)c->nactive * sizeof(int),
-            cudaMemcpyHostToDevice));
+        FX_CUDA(c, cudaMemcpyAsync(c->d_active, c->plan.active.data(), (size_t)c->nactive * sizeof(int), h2d, s));
     }
     {
         const FxProgram &g = c->plan.ghost;
         if (!g.cell_ops.empty()) {
-            FX_CUDA(c, cudaMemcpy(c->d_cops, g.cell_ops.data(), g.cell_ops.size() * sizeof(FxGop),
-                cudaMemcpyHostToDevice));
+            FX_CUDA(c, cudaMemcpyAsync(c->d_cops, g.cell_ops.data(), g.cell_ops.size() * sizeof(FxGop), h2d, s));
         }
         if (!g.face_ops.empty()) {
-            FX_CUDA(c, cudaMemcpy(c->d_fops, g.face_ops.data(), g.face_ops.size() * sizeof(FxGop),
-                cudaMemcpyHostToDevice));
+            FX_CUDA(c, cudaMemcpyAsync(c->d_fops, g.face_ops.data(), g.face_ops.size() * sizeof(FxGop), h2d, s));
         }
         if (!g.b_ops.empty()) {
-            FX_CUDA(c, cudaMemcpy(c->d_bops, g.b_ops.data(), g.b_ops.size() * sizeof(FxBop),
-                cudaMemcpyHostToDevice));
+            FX_CUDA(c, cudaMemcpyAsync(c->d_bops, g.b_ops.data(), g.b_ops.size() * sizeof(FxBop), h2d, s));
         }
     }
     if (!c->plan.flux_corr.empty()) {
-        FX_CUDA(c, cudaMemcpy(c->d_fcorr, c->plan.flux_corr.data(), c->plan.flux_corr.size() * sizeof(FxCorr),
-            cudaMemcpyHostToDevice));
+        FX_CUDA(c, cudaMemcpyAsync(c->d_fcorr, c->plan.flux_corr.data(),
+            c->plan.flux_corr.size() * sizeof(FxCorr), h2d, s));
     }
     if (!c->plan.emf_corr.empty()) {
-        FX_CUDA(c, cudaMemcpy(c->d_ecorr, c->plan.emf_corr.data(), c->plan.emf_corr.size() * sizeof(FxCorr),
-            cudaMemcpyHostToDevice));
+        FX_CUDA(c, cudaMemcpyAsync(c->d_ecorr, c->plan.emf_corr.data(),
+            c->plan.emf_corr.size() * sizeof(FxCorr), h2d, s));
     }
+    /* the host vectors must outlive the copies */
+    FX_CUDA(c, cudaStreamSynchronize(s));
     c->D.nblocks = nblocks;
     c->D.blk = c->d_blk;
     c->D.W = c->d_W;
