@@ -41,6 +41,56 @@ def active_faces(d):
     return face_idx(d, i, j, k).ravel()
 
 
+def bidx(nc, v, i, j, k):
+    """AoSoA index (4-wide k lanes) of component v of an nc-component buffer."""
+    i, j, k = (np.asarray(x) + NG for x in (i, j, k))
+    return ((((i * PBS + j) * (PBS // 4) + k // 4) * nc + v) * 4 + k % 4)
+
+
+def computed_faces(d, mhd):
+    """(i, j, k) of the faces prj_flux_update computes in direction d: normal
+    index [0, 16], transverse [-1, 16] for MHD, [0, 15] for hydro."""
+    rngs = []
+    for a in range(3):
+        if a == d:
+            rngs.append(np.arange(0, BS + 1))
+        else:
+            rngs.append(np.arange(-1, BS + 1) if mhd else np.arange(0, BS))
+    i, j, k = np.meshgrid(*rngs, indexing="ij")
+    return i.ravel(), j.ravel(), k.ravel()
+
+
+def flux_positions(d, nv, mhd):
+    i, j, k = computed_faces(d, mhd)
+    return np.concatenate([bidx(nv, v, i, j, k) for v in range(nv)])
+
+
+def vr_positions(d, mhd):
+    i, j, k = computed_faces(d, mhd)
+    return np.concatenate([bidx(3, v, i, j, k) for v in range(3)])
+
+
+def bv_positions(d):
+    i, j, k = computed_faces(d, True)
+    return lidx(i, j, k)
+
+
+def edge_idx(d, i, j, k):
+    i, j, k = (np.asarray(x) + NG for x in (i, j, k))
+    if d == 0:
+        return i * (PBS + 1) * (PBS + 1) + j * (PBS + 1) + k
+    if d == 1:
+        return i * PBS * (PBS + 1) + j * (PBS + 1) + k
+    return i * (PBS + 1) * PBS + j * PBS + k
+
+
+def emf_positions(d):
+    """edges prj_timeint_mhd_update_emf computes: [0,15] along d, [0,16] across"""
+    rngs = [np.arange(0, BS) if a == d else np.arange(0, BS + 1) for a in range(3)]
+    i, j, k = np.meshgrid(*rngs, indexing="ij")
+    return edge_idx(d, i.ravel(), j.ravel(), k.ravel())
+
+
 def apply_cell_program(W, ops, waves, slot, nvg):
     """W: [nb, nv, 2, NCELLS] (modified in place)."""
     for w in range(len(waves) - 1):
