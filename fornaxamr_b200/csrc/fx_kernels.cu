@@ -64,8 +64,10 @@ __global__ void __launch_bounds__(TPB, MINB) k_flux(FxDev D, const int *__restri
     if (D.ctl->skip) {
         return;
     }
-    const int dir = blockIdx.z;
-    const int b = blist[blockIdx.y];
+    /* grid (face chunk, direction, block): the three sweeps of a block are
+     * scheduled back to back, so its stencil cells are re-read from L2 */
+    const int dir = blockIdx.y;
+    const int b = blist[blockIdx.z];
     /* MHD carries one transverse ghost layer of faces for the CT EMFs
      * (src/prj_flux.c:2241-2251); hydro transverse faces are [0, 15]. */
     constexpr int T = MHD ? FX_BS + 2 : FX_BS;
@@ -819,7 +821,7 @@ static void launch_flux_shape(const FxDev &D, const int *blist, int nlist, int n
     int bfslot, cudaStream_t s)
 {
     const int nf = MHD ? (FX_BS + 1) * (FX_BS + 2) * (FX_BS + 2) : (FX_BS + 1) * FX_BS * FX_BS;
-    const dim3 g(fx_blocks(nf, TPB), nlist, ndir);
+    const dim3 g(fx_blocks(nf, TPB), ndir, nlist);
     k_flux<MHD, FULL, TPB, MINB><<<g, TPB, 0, s>>>(D, blist, wslot, bfslot);
 }
 
