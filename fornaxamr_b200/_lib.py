@@ -11,7 +11,8 @@ import os
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libfornax_b200.so")
 
-FX_SUCCESS, FX_EINVAL, FX_ECUDA, FX_ENOMESH, FX_EPHYSICS, FX_ENOMEM = range(6)
+FX_SUCCESS, FX_EINVAL, FX_ECUDA, FX_ENOMESH, FX_EPHYSICS, FX_ENOMEM, FX_ETOOBIG = range(7)
+NOALLOC_MAX_BLOCKS = 65536
 FORM_PLAIN, FORM_BATCHED = 0, 1
 BC_OUTFLOW, BC_REFLECT, BC_USER, BC_PERIODIC = 0, 1, 2, 3
 ARR_W, ARR_EOSVAR, ARR_RHS, ARR_FLUX, ARR_VRIEMANN, ARR_GRAV, ARR_BF, ARR_BV1, ARR_BV2, ARR_EMF = (
@@ -64,7 +65,7 @@ EXPORTS = [
     "fx_update_cells", "fx_riemann_flux_send", "fx_mhd_emf_send", "fx_eos_fill_active_cells",
     "fx_eos_fill_mesh", "fx_boundary_fill_ghosts_and_bf", "fx_calc_dt", "fx_stage", "fx_step",
     "fx_run", "fx_plan_export", "fx_time_phase", "fx_info", "fx_upload_state", "fx_download_state",
-    "fx_autotune",
+    "fx_autotune", "fx_calc_dt_noalloc",
 ]
 PHASE_FLUX, PHASE_EMF, PHASE_CT, PHASE_CELLS, PHASE_GHOST, PHASE_STEP = range(6)
 
@@ -111,4 +112,6 @@ def load() -> C.CDLL:
     L.fx_time_phase.argtypes = [vp, C.c_int, C.c_int, C.c_double, dp]
     L.fx_info.argtypes = [vp, C.c_int, C.POINTER(C.c_longlong)]
     L.fx_autotune.argtypes = [vp, dp, C.c_int, C.POINTER(C.c_int)]
+    # device pointers (W, dx, blocks, dt) and the stream pass as plain addresses
+    L.fx_calc_dt_noalloc.argtypes = [vp, C.c_int, vp, vp, C.c_int, C.c_double, C.c_double, vp, vp]
     return L

@@ -45,6 +45,7 @@ extern "C" {
 #define FX_ENOMESH 3    /* no mesh set */
 #define FX_EPHYSICS 4   /* device-side physics failure (reference exit path) */
 #define FX_ENOMEM 5     /* device allocation failed */
+#define FX_ETOOBIG 6    /* request exceeds a fixed capacity (FX_NOALLOC_MAX_BLOCKS) */
 
 /* execution forms of a step */
 #define FX_FORM_PLAIN 0    /* per-block kernel launches in the reference's loop order */
@@ -198,6 +199,40 @@ int fx_step(fx_ctx *ctx, int form, double dt, double *dt_src);
  * state[0..2] = time, dt, step on entry and on return. */
 int fx_run(fx_ctx *ctx, int form, int nsteps, double cfl, double dt_factor, double t_end,
     double *state);
+
+/* ---- allocation-free timestep ----------------------------------------------- */
+
+/* Capacity of fx_calc_dt_noalloc: at most this many listed blocks per call. */
+#define FX_NOALLOC_MAX_BLOCKS 65536
+
+/* The timestep of fx_calc_dt / prj_timeint_calc_dt (src/prj_timeint.h:15-16)
+ * for a host that keeps the block state in its own device memory and may not
+ * allocate device memory while it steps (for instance one whose device
+ * memory comes from a fixed pool sized at start-up).  No counterpart in the
+ * reference, which has no device; nothing is allocated, here or by the
+ * library calls it makes.
+ *
+ *   W       device; block b's W_mhd (2 stages, src/prj_defs.h WIDX layout,
+ *           NHYDRO = 9 if mhd else 6) at W + b * NHYDRO * 2 * 8000; stage 0
+ *           is read
+ *   dx      device; dx[3b + d] = cell width of block b along d
+ *   blocks  device; nlist block indices to reduce over (the active blocks),
+ *           or NULL for blocks 0 .. nlist-1
+ *   stream  cudaStream_t the two kernels are queued on (NULL: default stream)
+ *   dt      device; receives the minimum (1e99 if no cell gives a finite
+ *           value), stream-ordered: the call does not synchronise
+ *
+ * Returns FX_ETOOBIG, before any device work, when nlist exceeds
+ * FX_NOALLOC_MAX_BLOCKS, and FX_EINVAL for null pointers, nlist <= 0, mhd not
+ * 0/1, gamma <= 1 or cfl <= 0.  The scratch is one fixed 512 KiB device
+ * array per device, written in full by each call before it is read, so it
+ * needs no clearing.  The first call on a device resolves its address with
+ * cudaGetSymbolAddress (with that device current); make that first call
+ * before any stream capture.  Calls on one device share the scratch: two
+ * calls whose kernels overlap (different streams or host threads) race and
+ * give wrong results, so order them on one stream or serialise them. */
+int fx_calc_dt_noalloc(const double *W, int mhd, const double *dx, const int *blocks, int nlist,
+    double gamma, double cfl, void *stream, double *dt);
 
 /* ---- measurement --------------------------------------------------------------- */
 
