@@ -61,9 +61,10 @@ def make_config(mhd: bool, gamma: float, coord: Sequence[float], bc: Sequence[in
 
 def plan_export(cfg: FxConfig, desc, which: int):
     """Host-only dump of the compiled ghost fill: which = 0 cell ops, 1 face
-    ops, 4 cell-field ops -> (ops [n, 4 or 8] int32, wave_begin); 2/3 the
-    flux/EMF correction records; 5 compiler statistics (emitted cell ops,
-    emitted face ops, rewired copies, dead writes)."""
+    ops, 4 cell-field ops, 6 face-prolongation groups -> (ops [n, 4 or 8]
+    int32, wave_begin); 2/3 the flux/EMF correction records with their wave
+    offsets; 5 compiler statistics (emitted cell ops, emitted face ops,
+    rewired copies, dead writes)."""
     L = library()
     nops = C.c_int(0)
     nwaves = C.c_int(0)

@@ -633,9 +633,40 @@ __global__ void k_step_end(FxDev D)
 /* Ghost-fill programs                                                       */
 /* ------------------------------------------------------------------------ */
 
-/* limited linear prolongation from a 3x3x3 coarse stencil to a fine target
- * offset (prj_reconstruct_cell_for_prolongate with use_BJ = 0) */
-__device__ double fx_prolong_cell(const double *q, int c, const double target[3]);
+/* minmod slope of prj_reconstruct_minmod_slope (src/prj_reconstruct.h:46-62) */
+__device__ __forceinline__ double fx_minmod_slope(double qm, double q0, double qp)
+{
+    const double sl = q0 - qm;
+    const double sr = qp - q0;
+    if (sl * sr <= 0.0) {
+        return 0.0;
+    }
+    return fabs(sl) < fabs(sr) ? sl : sr;
+}
+
+/* prj_reconstruct_cell_for_prolongate_minmod (src/prj_reconstruct.h:111-143):
+ * per axis base + slope * target, combined as vx + vy + vz - 2 base; target
+ * offsets are +-1/4 of a coarse cell.  (The use_BJ = 1 limiter of the
+ * reference is not selected by any configuration of this path.) */
+__device__ __forceinline__ double fx_prolong_cell(const double *q, int c, double tx, double ty, double tz)
+{
+    const double base = q[c];
+    const double vx = base + fx_minmod_slope(q[c - FX_PBS * FX_PBS], base, q[c + FX_PBS * FX_PBS]) * tx;
+    const double vy = base + fx_minmod_slope(q[c - FX_PBS], base, q[c + FX_PBS]) * ty;
+    const double vz = base + fx_minmod_slope(q[c - 1], base, q[c + 1]) * tz;
+    return vx + vy + vz - 2.0 * base;
+}
+
+/* prj_reconstruct_face_for_prolongate_minmod (src/prj_reconstruct.h:222-246)
+ * on the face stencil of direction d about face f: tangential axes t0 < t1
+ * with face-index strides s0, s1 */
+__device__ __forceinline__ double fx_prolong_face(const double *q, int f, int s0, int s1, double t0, double t1)
+{
+    const double base = q[f];
+    const double vx = base + fx_minmod_slope(q[f - s0], base, q[f + s0]) * t0;
+    const double vy = base + fx_minmod_slope(q[f - s1], base, q[f + s1]) * t1;
+    return vx + vy - base;
+}
 
 __device__ __forceinline__ void fx_ghost_cell_op(const FxDev &D, const FxGop op, int wslot, int nvg)
 {
@@ -676,12 +707,12 @@ __device__ __forceinline__ void fx_ghost_cell_op(const FxDev &D, const FxGop op,
         }
         break;
     case FX_GOP_PROLONG: {
-        const double target[3] = {
-            (op.aux & 4) ? 0.25 : -0.25,
-            (op.aux & 2) ? 0.25 : -0.25,
-            (op.aux & 1) ? 0.25 : -0.25};
+        /* target offsets of src/prj_boundary.c:318-320 */
+        const double tx = (op.aux & 4) ? 0.25 : -0.25;
+        const double ty = (op.aux & 2) ? 0.25 : -0.25;
+        const double tz = (op.aux & 1) ? 0.25 : -0.25;
         for (int v = 0; v < nvg; ++v) {
-            Wd[(size_t)v * kPlane + dc] = fx_prolong_cell(Ws + (size_t)v * kPlane, sc, target);
+            Wd[(size_t)v * kPlane + dc] = fx_prolong_cell(Ws + (size_t)v * kPlane, sc, tx, ty, tz);
         }
         break;
     }
@@ -712,6 +743,131 @@ __device__ __forceinline__ void fx_ghost_face_op(const FxDev &D, const FxGop op,
     }
 }
 
+/* face-index offset of a unit step along axis a for faces of direction d */
+__device__ __forceinline__ int fx_face_stride(int d, int a)
+{
+    return fx_face_idx(d, a == 0, a == 1, a == 2) - fx_face_idx(d, 0, 0, 0);
+}
+
+/* One Toth-Roe group: prj_mhd_prolong_bf_from_buffer (src/prj_mhd.c:374-512)
+ * with prj_mhd_compute_buffer_inner_fluxes (src/prj_mhd.c:309-372), in the
+ * reference's operation order.  Outer faces are area-weighted fluxes; kept
+ * faces contribute their current fine value. */
+__device__ __forceinline__ void fx_ghost_prolong_group(const FxDev &D, const FxPop &op, int slot)
+{
+    const int f0[3] = {(op.pos & 31) - 2, ((op.pos >> 5) & 31) - 2, ((op.pos >> 10) & 31) - 2};
+    const int c0[3] = {((op.pos >> 15) & 31) - 2, ((op.pos >> 20) & 31) - 2, ((op.pos >> 25) & 31) - 2};
+    const FxBlockDev &fb = D.blk[op.fine];
+    const double area[3] = {fb.dx[1] * fb.dx[2], fb.dx[0] * fb.dx[2], fb.dx[0] * fb.dx[1]};
+    /* outer fluxes o[d][side][a][b] */
+    double o[3][2][2][2];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        const int t0 = d == 0 ? 1 : 0;
+        const int t1 = d == 2 ? 1 : 2;
+        double *Bfine = D.Bf + (size_t)op.fine * FX_BF_COUNT + ((size_t)d * FX_NSTAGES + slot) * FX_NFACES;
+        const double *Bc = D.Bf + (size_t)op.coarse * FX_BF_COUNT + ((size_t)d * FX_NSTAGES + slot) * FX_NFACES;
+        const int s0 = fx_face_stride(d, t0);
+        const int s1 = fx_face_stride(d, t1);
+#pragma unroll
+        for (int side = 0; side < 2; ++side) {
+            int y[3] = {c0[0], c0[1], c0[2]};
+            y[d] += side;
+            const int cf = fx_face_idx(d, y[0], y[1], y[2]);
+#pragma unroll
+            for (int a = 0; a < 2; ++a) {
+#pragma unroll
+                for (int b = 0; b < 2; ++b) {
+                    const int q = 8 * d + 4 * side + 2 * a + b;
+                    int x[3] = {f0[0], f0[1], f0[2]};
+                    x[d] += 2 * side;
+                    x[t0] += a;
+                    x[t1] += b;
+                    const int xf = fx_face_idx(d, x[0], x[1], x[2]);
+                    double flux;
+                    if ((op.keep >> q) & 1) {
+                        flux = Bfine[xf] * area[d];
+                    } else {
+                        const double value = fx_prolong_face(Bc, cf, s0, s1, a ? 0.25 : -0.25, b ? 0.25 : -0.25);
+                        flux = value * area[d];
+                        if ((op.owrite >> q) & 1) {
+                            Bfine[xf] = flux / area[d];
+                        }
+                    }
+                    o[d][side][a][b] = flux;
+                }
+            }
+        }
+    }
+    /* u[i][j][k] of the reference: u[0|2][j][k] = o[0][0|1][j][k],
+     * v[i][0|2][k] = o[1][0|1][i][k], w[i][j][0|2] = o[2][0|1][i][j] */
+    const double dx1s = fb.dx[0] * fb.dx[0];
+    const double dx2s = fb.dx[1] * fb.dx[1];
+    const double dx3s = fb.dx[2] * fb.dx[2];
+    double Uxx = 0.0, Vyy = 0.0, Wzz = 0.0, Uxyz = 0.0, Vxyz = 0.0, Wxyz = 0.0;
+#pragma unroll
+    for (int i = 0; i < 2; ++i) {
+        const double si = i ? 1.0 : -1.0;
+#pragma unroll
+        for (int j = 0; j < 2; ++j) {
+            const double sj = j ? 1.0 : -1.0;
+#pragma unroll
+            for (int k = 0; k < 2; ++k) {
+                const double sk = k ? 1.0 : -1.0;
+                const double u = o[0][i][j][k];
+                const double v = o[1][j][i][k];
+                const double w = o[2][k][i][j];
+                Uxx += si * sj * v + si * sk * w;
+                Vyy += sj * sk * w + sj * si * u;
+                Wzz += sk * si * u + sk * sj * v;
+                Uxyz += si * sj * sk * u / (dx2s + dx3s);
+                Vxyz += si * sj * sk * v / (dx1s + dx3s);
+                Wxyz += si * sj * sk * w / (dx1s + dx2s);
+            }
+        }
+    }
+    Uxx *= 0.125;
+    Vyy *= 0.125;
+    Wzz *= 0.125;
+    Uxyz *= 0.125;
+    Vxyz *= 0.125;
+    Wxyz *= 0.125;
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        const int t0 = d == 0 ? 1 : 0;
+        const int t1 = d == 2 ? 1 : 2;
+        double *Bfine = D.Bf + (size_t)op.fine * FX_BF_COUNT + ((size_t)d * FX_NSTAGES + slot) * FX_NFACES;
+#pragma unroll
+        for (int a = 0; a < 2; ++a) {
+#pragma unroll
+            for (int b = 0; b < 2; ++b) {
+                const int q = 4 * d + 2 * a + b;
+                if (!((op.iwrite >> q) & 1)) continue;
+                const double sa = a ? 1.0 : -1.0;
+                const double sb = b ? 1.0 : -1.0;
+                double flux;
+                if (d == 0) {        /* u[1][j][k], (a, b) = (j, k) */
+                    flux = 0.5 * (o[0][1][a][b] + o[0][0][a][b]) + Uxx + sb * dx3s * Vxyz + sa * dx2s * Wxyz;
+                } else if (d == 1) { /* v[i][1][k], (a, b) = (i, k) */
+                    flux = 0.5 * (o[1][1][a][b] + o[1][0][a][b]) + Vyy + sa * dx1s * Wxyz + sb * dx3s * Uxyz;
+                } else {             /* w[i][j][1], (a, b) = (i, j) */
+                    flux = 0.5 * (o[2][1][a][b] + o[2][0][a][b]) + Wzz + sb * dx2s * Uxyz + sa * dx1s * Vxyz;
+                }
+                const double value = flux / area[d];
+                int x[3] = {f0[0], f0[1], f0[2]};
+                x[d] += 1;
+                x[t0] += a;
+                x[t1] += b;
+                const int xf = fx_face_idx(d, x[0], x[1], x[2]);
+                if (!isfinite(value)) {
+                    fx_fail(D.err, FX_ERR_BF_NONFINITE, op.fine, xf);
+                }
+                Bfine[xf] = value;
+            }
+        }
+    }
+}
+
 /* cell-centred field of one cell from its faces: prj_mhd_bf2bc_impl
  * (src/prj_mhd.c:555-603).  The metric factor sqrt(gamma) is 1 outside
  * dynamical GR; the reference's division by it is exact and omitted. */
@@ -739,8 +895,20 @@ __device__ __forceinline__ void fx_ghost_b_op(const FxDev &D, const FxBop op, in
     W[(size_t)FX_B3 * kPlane + c] = v[2];
 }
 
+/* face-prolongation groups of one wave (a separate kernel: the group
+ * arithmetic would otherwise raise the register count, and so lower the
+ * occupancy, of the copy-dominated wave kernel) */
+__global__ void __launch_bounds__(128) k_ghost_groups(FxDev D, const FxPop *__restrict__ pops, int np, int slot)
+{
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= np || D.ctl->skip) {
+        return;
+    }
+    fx_ghost_prolong_group(D, pops[t], slot);
+}
+
 /* one conflict-free wave of the ghost fill: CTAs [0, nbc) run cell ops,
- * [nbc, nbc + nbf) face ops, the rest cell-field ops */
+ * then face ops and cell-field ops */
 __global__ void __launch_bounds__(256) k_ghost_wave(FxDev D, const FxGop *__restrict__ cops, int nc,
     const FxGop *__restrict__ fops, int nf, const FxBop *__restrict__ bops, int nb, int slot, int nvg)
 {
@@ -767,21 +935,21 @@ __global__ void __launch_bounds__(256) k_ghost_wave(FxDev D, const FxGop *__rest
 }
 
 /* coarse/fine corrections */
-__global__ void k_flux_correct(FxDev D, const FxCorr *__restrict__ recs, int n)
+__global__ void k_flux_correct(FxDev D, const FxCorr *__restrict__ recs, int n, int ncomp)
 {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= n * D.nv || D.ctl->skip) {
+    if (t >= n * ncomp || D.ctl->skip) {
         return;
     }
-    const int r = t / D.nv;
-    const int v = t - r * D.nv;
+    const int r = t / ncomp;
+    const int v = t - r * ncomp;
     const FxCorr rec = recs[r];
-    /* each entry is a flat index into the stacked flux array of component 0;
-     * component v sits FX_AOSOA_W * v further in the AoSoA tile */
-    const size_t off = (size_t)v * FX_AOSOA_W;
-    D.flux[rec.dst + off] = 0.25 *
-        (D.flux[rec.src[0] + off] + D.flux[rec.src[1] + off] +
-         D.flux[rec.src[2] + off] + D.flux[rec.src[3] + off]);
+    /* entries index component 0 of a block's stacked flux array; component
+     * v sits FX_AOSOA_W * v further in the AoSoA tile.  Sum order of
+     * src/prj_riemann.c:1756-1761. */
+    const double *s = D.flux + (size_t)rec.src_block * FX_FLUX_COUNT(D.nv) + (size_t)v * FX_AOSOA_W;
+    double *d = D.flux + (size_t)rec.dst_block * FX_FLUX_COUNT(D.nv) + (size_t)v * FX_AOSOA_W;
+    d[rec.dst] = 0.25 * (s[rec.src[0]] + s[rec.src[1]] + s[rec.src[2]] + s[rec.src[3]]);
 }
 
 __global__ void k_emf_correct(FxDev D, const FxCorr *__restrict__ recs, int n)
@@ -791,22 +959,18 @@ __global__ void k_emf_correct(FxDev D, const FxCorr *__restrict__ recs, int n)
         return;
     }
     const FxCorr rec = recs[t];
-    D.emf[rec.dst] = 0.5 * (D.emf[rec.src[0]] + D.emf[rec.src[1]]);
+    const double *s = D.emf + (size_t)rec.src_block * FX_EMF_COUNT;
+    /* value = 0; value += e0; value += e1; value *= 0.5 (src/prj_mhd.c:904-910):
+     * the leading 0.0 + makes a -0.0 pair sum to +0.0 */
+    double value = 0.0;
+    value += s[rec.src[0]];
+    value += s[rec.src[1]];
+    value *= 0.5;
+    D.emf[(size_t)rec.dst_block * FX_EMF_COUNT + rec.dst] = value;
 }
 
 } /* namespace */
 
-/* ------------------------------------------------------------------------ */
-/* prolongation limiter                                                      */
-/* ------------------------------------------------------------------------ */
-namespace {
-__device__ double fx_prolong_cell(const double *q, int c, const double target[3])
-{
-    /* filled in together with the AMR transfer programs */
-    (void)target;
-    return q[c];
-}
-}
 
 /* ------------------------------------------------------------------------ */
 /* launchers                                                                 */
@@ -904,17 +1068,23 @@ void fx_launch_calc_dt(const FxDev &D, const int *blist, int nlist, int wslot, d
 }
 
 void fx_launch_ghost_wave(const FxDev &D, const FxGop *cops, int nc, const FxGop *fops, int nf,
-    const FxBop *bops, int nb, int slot, int nvg, cudaStream_t s)
+    const FxPop *pops, int np, const FxBop *bops, int nb, int slot, int nvg, cudaStream_t s)
 {
+    /* the operations of a wave are conflict free: the two launches may run
+     * in either order */
     const unsigned grid = fx_blocks(nc, 256) + fx_blocks(nf, 256) + fx_blocks(nb, 256);
-    if (grid == 0) return;
-    k_ghost_wave<<<grid, 256, 0, s>>>(D, cops, nc, fops, nf, bops, nb, slot, nvg);
+    if (grid > 0) {
+        k_ghost_wave<<<grid, 256, 0, s>>>(D, cops, nc, fops, nf, bops, nb, slot, nvg);
+    }
+    if (np > 0) {
+        k_ghost_groups<<<fx_blocks(np, 128), 128, 0, s>>>(D, pops, np, slot);
+    }
 }
 
-void fx_launch_flux_correct(const FxDev &D, const FxCorr *recs, int n, cudaStream_t s)
+void fx_launch_flux_correct(const FxDev &D, const FxCorr *recs, int n, int ncomp, cudaStream_t s)
 {
     if (n <= 0) return;
-    k_flux_correct<<<fx_blocks(n * D.nv, 256), 256, 0, s>>>(D, recs, n);
+    k_flux_correct<<<fx_blocks(n * ncomp, 256), 256, 0, s>>>(D, recs, n, ncomp);
 }
 
 void fx_launch_emf_correct(const FxDev &D, const FxCorr *recs, int n, cudaStream_t s)

@@ -70,7 +70,8 @@ enum FxGopType {
     FX_GOP_COPY_NEG = 1,    /* dst <- src, normal velocity aux negated (reflect) */
     FX_GOP_COPY_USER = 2,   /* dst <- src, then v1 = 5 (reference PRJ_BC_USER) */
     FX_GOP_RESTRICT = 3,    /* dst <- 1/8 sum of the 2x2x2 cells at src */
-    FX_GOP_PROLONG = 4,     /* dst <- limited linear from the 27 cells about src */
+    FX_GOP_PROLONG = 4,     /* dst <- minmod-limited linear from src and its 6 axis neighbours,
+                               target offsets +-1/4 from aux bits 2, 1, 0 (set: +) */
     FX_FOP_COPY = 8,        /* face: dst <- src */
     FX_FOP_RESTRICT = 9,    /* face: dst <- 1/4 sum of 4 fine faces */
     FX_FOP_PROLONG = 10     /* face: divergence-free prolongation value */
@@ -93,13 +94,37 @@ struct FxBop {
     int32_t pad;
 };
 
-/* coarse/fine correction records: dst <- 0.25 * sum of 4 (flux) or
- * 0.5 * sum of 2 (emf) source entries */
-struct FxCorr {
-    int32_t dst;
-    int32_t src[4];
-    int32_t n;
+/* Divergence-preserving prolongation of the face field onto one 2x2x2 group
+ * of fine cells (prj_mhd_prolong_bf_from_buffer, src/prj_mhd.c:374-512).
+ * pos packs the fine corner (fi, fj, fk) and the coarse cell (ci, cj, ck),
+ * each biased by 2, in 5 bits apiece: fi | fj << 5 | fk << 10 | ci << 15 |
+ * cj << 20 | ck << 25.  Outer face q = 8 d + 4 s + 2 a + b is the face of
+ * direction d on side s (s = 1: index +2 along d) at tangential offsets
+ * (a, b) in increasing axis order; inner face q = 4 d + 2 a + b.  keep bit
+ * q: outer face q keeps the fine block's value (its fidelity is above
+ * COARSER); owrite bit q: outer face q is stored; iwrite bit q: inner face q
+ * is stored.  The masks come from the data-independent fidelity replay. */
+struct FxPop {
+    int32_t fine;
+    int32_t coarse;
+    int32_t pos;
+    int32_t keep;
+    int32_t owrite;
+    int32_t iwrite;
     int32_t pad[2];
+};
+
+/* coarse/fine correction records: entry dst of block dst_block <- 0.25 *
+ * sum of 4 (flux) or 0.5 * sum of 2 (emf) entries of block src_block.
+ * Indices are into one block's stacked array: dir * nv * 8000 + VIDX(0, ..)
+ * for fluxes (component v sits 4 v further), dir * 8820 + EDGE_IDX for
+ * EMFs. */
+struct FxCorr {
+    int32_t dst_block;
+    int32_t dst;
+    int32_t src_block;
+    int32_t src[4];
+    int32_t pad;
 };
 
 #define FX_CELL_KEY(b, c) (((b) << 13) | (c))
@@ -117,10 +142,12 @@ void fx_launch_eos_fill(const FxDev &D, const int *blist, int nlist, int wslot, 
     cudaStream_t s);
 void fx_launch_calc_dt(const FxDev &D, const int *blist, int nlist, int wslot, double cfl,
     cudaStream_t s);
-/* one wave of the ghost fill (cell ops, face ops and cell-field ops) */
+/* one wave of the ghost fill (cell ops, face ops, face-prolongation groups
+ * and cell-field ops) */
 void fx_launch_ghost_wave(const FxDev &D, const FxGop *cops, int nc, const FxGop *fops, int nf,
-    const FxBop *bops, int nb, int slot, int nvg, cudaStream_t s);
-void fx_launch_flux_correct(const FxDev &D, const FxCorr *recs, int n, cudaStream_t s);
+    const FxPop *pops, int np, const FxBop *bops, int nb, int slot, int nvg, cudaStream_t s);
+/* one wave of correction records; ncomp flux components per record */
+void fx_launch_flux_correct(const FxDev &D, const FxCorr *recs, int n, int ncomp, cudaStream_t s);
 void fx_launch_emf_correct(const FxDev &D, const FxCorr *recs, int n, cudaStream_t s);
 void fx_launch_reset_reductions(const FxDev &D, int which, cudaStream_t s);
 /* device-resident driver: dt selection before a step, dt_src clamp and time

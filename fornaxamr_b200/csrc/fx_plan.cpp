@@ -40,13 +40,14 @@
 #include <cmath>
 #include <cstdint>
 #include <cstring>
+#include <unordered_map>
 
 namespace {
 
 enum { KIND_SAME = 3, KIND_RESTRICT = 4, KIND_PROLONG = 5 };
 enum { PHYS_FACE_ONLY = 0, PHYS_EDGE_CORNER = 2 };
 enum { FID_NONE = 0, FID_COARSER = 1, FID_SAME = 2, FID_FINER = 3 };
-enum { SPACE_CELL = 0, SPACE_FACE = 1 };
+enum { SPACE_CELL = 0, SPACE_FACE = 1, SPACE_GROUP = 2 };
 
 const int BS = FX_BS;
 const int NG = FX_NG;
@@ -68,6 +69,12 @@ bool face_storage_ok(int dir, const int idx[3])
     return true;
 }
 
+/* cell storage bounds, src/prj_boundary.c:62-64 */
+bool cell_in_storage(int i, int j, int k)
+{
+    return i >= -NG && i < BS + NG && j >= -NG && j < BS + NG && k >= -NG && k < BS + NG;
+}
+
 /* active faces, src/prj_boundary.c:575-590 */
 bool face_active(int dir, int i, int j, int k)
 {
@@ -81,15 +88,26 @@ bool face_active(int dir, int i, int j, int k)
     return true;
 }
 
-/* one landed write of the reference sequence */
+/* one operation of the reference sequence: a landed write, or one
+ * face-prolongation group (several writes) */
 struct SeqOp {
-    FxGop op;
-    int64_t w;         /* element written */
+    FxGop op;          /* SPACE_GROUP: op.dst indexes the group table */
     int64_t src;       /* single source element, -1 for multi-source ops */
     int src_ver;       /* producer of the source value (op index, -1 initial) */
     int space;
     int prod_begin;    /* producers of the values read: [prod_begin, prod_end) */
     int prod_end;
+    int w_begin;       /* elements written: [w_begin, w_end) of the write list */
+    int w_end;
+};
+
+/* what a prolonged outer face was computed from: a recomputation with the
+ * same coarse face, target and stencil versions stores the same value */
+struct ProlongSig {
+    int op;            /* the group that stored it */
+    int64_t coarse_face;
+    int target;
+    int ver[5];
 };
 
 class Compiler {
@@ -146,6 +164,12 @@ public:
             }
         }
         finish(plan);
+        flux_corrections(plan);
+        if (cfg_.mhd) {
+            emf_corrections(plan);
+        } else {
+            plan.emf_corr_begin.assign(1, 0);
+        }
         return true;
     }
 
@@ -165,9 +189,6 @@ private:
                 if (sl.id < 0 || sl.id >= n_ || !active_block(b_[sl.id])) continue;
                 if (sl.rel_level < -1 || sl.rel_level > 1) {
                     return fail("slot rel_level outside [-1, 1] (the reference aborts: slot->rel_level unrecognized)");
-                }
-                if (sl.rel_level != 0) {
-                    return fail("coarse/fine neighbours need the AMR transfer programs, not built in this version");
                 }
             }
         }
@@ -217,7 +238,6 @@ private:
         resolve(src, v, &stats_.rewired);
         op.src = space == SPACE_CELL ? cell_key(src) : face_key(src);
         s.op = op;
-        s.w = w;
         s.src = src;
         s.src_ver = v;
         s.space = space;
@@ -225,6 +245,9 @@ private:
         prod_.push_back(v);
         s.prod_end = (int)prod_.size();
         rd_.push_back(src);
+        s.w_begin = (int)wr_.size();
+        wr_.push_back(w);
+        s.w_end = (int)wr_.size();
         seq_.push_back(s);
         ver_[w] = (int)seq_.size() - 1;
     }
@@ -233,7 +256,6 @@ private:
     {
         SeqOp s;
         s.op = op;
-        s.w = w;
         s.src = -1;
         s.src_ver = -1;
         s.space = space;
@@ -243,8 +265,38 @@ private:
             rd_.push_back(reads[n]);
         }
         s.prod_end = (int)prod_.size();
+        s.w_begin = (int)wr_.size();
+        wr_.push_back(w);
+        s.w_end = (int)wr_.size();
         seq_.push_back(s);
         ver_[w] = (int)seq_.size() - 1;
+    }
+
+    /* one face-prolongation group: reads, then writes several faces */
+    void add_group(const FxPop &p, const std::vector<int64_t> &reads, const std::vector<int64_t> &writes)
+    {
+        SeqOp s;
+        s.op.dst = (int32_t)groups_.size();
+        s.op.src = 0;
+        s.op.aux = 0;
+        s.op.type = FX_FOP_PROLONG;
+        groups_.push_back(p);
+        s.src = -1;
+        s.src_ver = -1;
+        s.space = SPACE_GROUP;
+        s.prod_begin = (int)prod_.size();
+        for (int64_t r : reads) {
+            prod_.push_back(ver_[r]);
+            rd_.push_back(r);
+        }
+        s.prod_end = (int)prod_.size();
+        s.w_begin = (int)wr_.size();
+        wr_.insert(wr_.end(), writes.begin(), writes.end());
+        s.w_end = (int)wr_.size();
+        seq_.push_back(s);
+        for (int64_t w : writes) {
+            ver_[w] = (int)seq_.size() - 1;
+        }
     }
 
     bool on_side(const fx_block_desc &blk, int axis, int side) const
@@ -370,13 +422,17 @@ private:
                             /* target offsets: (index % 2 == 0) ? -0.25 : +0.25 in C
                              * semantics (src/prj_boundary.c:318-320) */
                             op.aux = ((ai % 2 == 0) ? 0 : 4) | ((aj % 2 == 0) ? 0 : 2) | ((ak % 2 == 0) ? 0 : 1);
-                            int64_t r[27];
-                            int q = 0;
-                            for (int di = -1; di <= 1; ++di)
-                                for (int dj = -1; dj <= 1; ++dj)
-                                    for (int dk = -1; dk <= 1; ++dk)
-                                        r[q++] = cell_elem(b, lidx(ci + di, cj + dj, ck + dk));
-                            add_multi(op, SPACE_CELL, r, 27, cell_elem(id, dc));
+                            /* the 27-cell stencil is range checked
+                             * (src/prj_boundary.c:60-72); the minmod limiter
+                             * reads the centre and its six axis neighbours */
+                            if (!cell_in_storage(ci - 1, cj - 1, ck - 1) || !cell_in_storage(ci + 1, cj + 1, ck + 1)) {
+                                return fail("prj_boundary_read_value: out-of-range access");
+                            }
+                            const int64_t r[7] = {cell_elem(b, lidx(ci, cj, ck)),
+                                cell_elem(b, lidx(ci - 1, cj, ck)), cell_elem(b, lidx(ci + 1, cj, ck)),
+                                cell_elem(b, lidx(ci, cj - 1, ck)), cell_elem(b, lidx(ci, cj + 1, ck)),
+                                cell_elem(b, lidx(ci, cj, ck - 1)), cell_elem(b, lidx(ci, cj, ck + 1))};
+                            add_multi(op, SPACE_CELL, r, 7, cell_elem(id, dc));
                         }
                     }
                 }
@@ -480,7 +536,7 @@ private:
             } else if (kind == KIND_RESTRICT && sl.rel_level < 0) {
                 restrict_to_coarse(b, id, sl);
             } else if (kind == KIND_PROLONG && sl.rel_level > 0) {
-                return fail("field prolongation to finer neighbours needs the AMR transfer programs");
+                if (!prolong_to_fine(b, id, sl)) return false;
             }
         }
         return true;
@@ -555,6 +611,357 @@ private:
         }
     }
 
+    /* prj_boundary_prolong_bf_to_fine (src/prj_boundary.c:781-838): one
+     * Toth-Roe group per 2x2x2 fine cells of the receive box.  The
+     * reference buffers the coarse faces first; only the fine block is
+     * written, so reading them at group time is equivalent. */
+    bool prolong_to_fine(int coarse, int fine, const fx_slot &sl)
+    {
+        const int ni = sl.recv_loc_end[0] - sl.recv_loc_start[0];
+        const int nj = sl.recv_loc_end[1] - sl.recv_loc_start[1];
+        const int nk = sl.recv_loc_end[2] - sl.recv_loc_start[2];
+        for (int i = 0; i < ni; i += 2) {
+            for (int j = 0; j < nj; j += 2) {
+                for (int k = 0; k < nk; k += 2) {
+                    const int f[3] = {i + sl.recv_loc_start[0], j + sl.recv_loc_start[1], k + sl.recv_loc_start[2]};
+                    const int c[3] = {i / 2 + sl.send_loc_start[0], j / 2 + sl.send_loc_start[1],
+                        k / 2 + sl.send_loc_start[2]};
+                    if (!prolong_group(coarse, fine, c, f)) return false;
+                }
+            }
+        }
+        return true;
+    }
+
+    /* prj_mhd_prolong_bf_from_buffer (src/prj_mhd.c:374-512) as one group
+     * operation: 24 outer faces prolonged from the coarse faces (or kept when
+     * their fidelity is above COARSER), 12 inner faces from
+     * prj_mhd_compute_buffer_inner_fluxes (src/prj_mhd.c:309-372) */
+    bool prolong_group(int coarse, int fine, const int c[3], const int f[3])
+    {
+        for (int d = 0; d < 3; ++d) {
+            /* fine cells f, f + 1 and the coarse stencil c - 1 .. c + 1 lie
+             * in storage (the outer face f + 2 along d is then at most 18) */
+            if (f[d] < -NG || f[d] + 1 > BS + NG - 1 || c[d] - 1 < -NG || c[d] + 1 > BS + NG - 1) {
+                return fail("prj_mhd_prolong_bf_from_buffer: group outside face storage");
+            }
+        }
+        FxPop p;
+        std::memset(&p, 0, sizeof(p));
+        p.fine = fine;
+        p.coarse = coarse;
+        p.pos = (f[0] + 2) | ((f[1] + 2) << 5) | ((f[2] + 2) << 10) | ((c[0] + 2) << 15) |
+            ((c[1] + 2) << 20) | ((c[2] + 2) << 25);
+        std::vector<int64_t> reads, writes;
+        std::vector<std::pair<int64_t, ProlongSig>> sigs;
+        const int op_index = (int)seq_.size();
+        for (int d = 0; d < 3; ++d) {
+            const int t0 = d == 0 ? 1 : 0;
+            const int t1 = d == 2 ? 1 : 2;
+            for (int side = 0; side < 2; ++side) {
+                for (int a = 0; a < 2; ++a) {
+                    for (int bb = 0; bb < 2; ++bb) {
+                        const int q = 8 * d + 4 * side + 2 * a + bb;
+                        int x[3] = {f[0], f[1], f[2]};
+                        x[d] += 2 * side;
+                        x[t0] += a;
+                        x[t1] += bb;
+                        const int xf = fidx(d, x[0], x[1], x[2]);
+                        const int64_t xe = face_elem(fine, d, xf);
+                        if (fid(fine, d, xf) > FID_COARSER) {
+                            p.keep |= 1 << q;
+                            reads.push_back(xe);
+                            continue;
+                        }
+                        int y[3] = {c[0], c[1], c[2]};
+                        y[d] += side;
+                        ProlongSig sg;
+                        sg.op = op_index;
+                        sg.coarse_face = face_elem(coarse, d, fidx(d, y[0], y[1], y[2]));
+                        sg.target = 2 * a + bb;
+                        const int off[5][2] = {{0, 0}, {-1, 0}, {1, 0}, {0, -1}, {0, 1}};
+                        for (int n = 0; n < 5; ++n) {
+                            int z[3] = {y[0], y[1], y[2]};
+                            z[t0] += off[n][0];
+                            z[t1] += off[n][1];
+                            const int64_t ze = face_elem(coarse, d, fidx(d, z[0], z[1], z[2]));
+                            reads.push_back(ze);
+                            sg.ver[n] = ver_[ze];
+                        }
+                        fid(fine, d, xf) = FID_COARSER;
+                        const auto it = psig_.find(xe);
+                        if (it != psig_.end() && same_sig(it->second, sg) && ver_[xe] == it->second.op) {
+                            continue; /* recomputes the value the face already holds */
+                        }
+                        p.owrite |= 1 << q;
+                        writes.push_back(xe);
+                        sigs.emplace_back(xe, sg);
+                    }
+                }
+            }
+        }
+        for (int d = 0; d < 3; ++d) {
+            const int t0 = d == 0 ? 1 : 0;
+            const int t1 = d == 2 ? 1 : 2;
+            for (int a = 0; a < 2; ++a) {
+                for (int bb = 0; bb < 2; ++bb) {
+                    int x[3] = {f[0], f[1], f[2]};
+                    x[d] += 1;
+                    x[t0] += a;
+                    x[t1] += bb;
+                    const int xf = fidx(d, x[0], x[1], x[2]);
+                    if (!lands(fine, d, xf, FID_COARSER)) continue;
+                    p.iwrite |= 1 << (4 * d + 2 * a + bb);
+                    writes.push_back(face_elem(fine, d, xf));
+                }
+            }
+        }
+        std::sort(reads.begin(), reads.end());
+        reads.erase(std::unique(reads.begin(), reads.end()), reads.end());
+        add_group(p, reads, writes);
+        for (auto &e : sigs) {
+            psig_[e.first] = e.second;
+        }
+        return true;
+    }
+
+    static bool same_sig(const ProlongSig &a, const ProlongSig &b)
+    {
+        if (a.coarse_face != b.coarse_face || a.target != b.target) return false;
+        for (int n = 0; n < 5; ++n) {
+            if (a.ver[n] != b.ver[n]) return false;
+        }
+        return true;
+    }
+
+    /* ---- coarse/fine corrections ------------------------------------------ */
+
+    /* prj_riemann_face_axis (src/prj_riemann.c:1666-1698) */
+    static int face_axis(const fx_block_desc &blk, const double smin[3], const double smax[3], int *side)
+    {
+        int axis = -1;
+        int sd = -1;
+        for (int d = 0; d < 3; ++d) {
+            if (std::fabs(blk.xmax[d] - smin[d]) < 1.0e-12 * blk.dx[d]) {
+                if (axis >= 0) return -1;
+                axis = d;
+                sd = 1;
+            } else if (std::fabs(smax[d] - blk.xmin[d]) < 1.0e-12 * blk.dx[d]) {
+                if (axis >= 0) return -1;
+                axis = d;
+                sd = 0;
+            }
+        }
+        if (axis < 0) return -1;
+        for (int d = 0; d < 3; ++d) {
+            if (d == axis) continue;
+            const double hi = blk.xmax[d] < smax[d] ? blk.xmax[d] : smax[d];
+            const double lo = blk.xmin[d] > smin[d] ? blk.xmin[d] : smin[d];
+            if (!(hi - lo > 1.0e-12)) return -1;
+        }
+        *side = sd;
+        return axis;
+    }
+
+    /* prj_riemann_flux_send (src/prj_riemann.c:1700-1768): coarse face flux
+     * <- 0.25 (f0 + f_tan0 + f_tan1 + f_both) of the four fine faces */
+    void flux_corrections(FxPlan &plan)
+    {
+        const int nv = cfg_.mhd ? 9 : 6;
+        std::vector<FxCorr> seq;
+        std::vector<std::array<int64_t, 5>> el;
+        for (int b : plan.active) {
+            for (int n = 0; n < FX_NSLOTS; ++n) {
+                const fx_slot &sl = b_[b].slot[n];
+                if (sl.type != 1 || sl.rel_level >= 0) continue;
+                const int nid = sl.id;
+                if (nid < 0 || nid >= n_) continue;
+                int side = -1;
+                const int axis = face_axis(b_[b], b_[nid].xmin, b_[nid].xmax, &side);
+                if (axis < 0) continue;
+                const int tan0 = (axis + 1) % 3;
+                const int tan1 = (axis + 2) % 3;
+                const int n0 = sl.recv_loc_end[tan0] - sl.recv_loc_start[tan0];
+                const int n1 = sl.recv_loc_end[tan1] - sl.recv_loc_start[tan1];
+                for (int it0 = 0; it0 < n0; ++it0) {
+                    for (int it1 = 0; it1 < n1; ++it1) {
+                        int r[3], s0[3];
+                        r[axis] = side == 1 ? 0 : BS;
+                        r[tan0] = it0 + sl.recv_loc_start[tan0];
+                        r[tan1] = it1 + sl.recv_loc_start[tan1];
+                        s0[axis] = side == 1 ? BS : 0;
+                        s0[tan0] = 2 * it0 + sl.send_loc_start[tan0];
+                        s0[tan1] = 2 * it1 + sl.send_loc_start[tan1];
+                        const int add[4][2] = {{0, 0}, {1, 0}, {0, 1}, {1, 1}};
+                        FxCorr rec;
+                        std::memset(&rec, 0, sizeof(rec));
+                        std::array<int64_t, 5> e;
+                        const size_t dbase = (size_t)axis * nv * FX_NCELLS;
+                        rec.dst_block = nid;
+                        rec.dst = (int32_t)(dbase + fx_bidx(nv, 0, r[0], r[1], r[2]));
+                        rec.src_block = b;
+                        e[0] = ((int64_t)nid * 3 + axis) * FX_NCELLS + lidx(r[0], r[1], r[2]);
+                        for (int q = 0; q < 4; ++q) {
+                            int x[3] = {s0[0], s0[1], s0[2]};
+                            x[tan0] += add[q][0];
+                            x[tan1] += add[q][1];
+                            rec.src[q] = (int32_t)(dbase + fx_bidx(nv, 0, x[0], x[1], x[2]));
+                            e[1 + q] = ((int64_t)b * 3 + axis) * FX_NCELLS + lidx(x[0], x[1], x[2]);
+                        }
+                        seq.push_back(rec);
+                        el.push_back(e);
+                    }
+                }
+            }
+        }
+        level_records(seq, el, 4, plan.flux_corr, plan.flux_corr_begin);
+    }
+
+    /* prj_mhd_emf_send + prj_mhd_restrict_emf_to_coarse
+     * (src/prj_mhd.c:1003-1029, 853-965): coarse edge EMF <- 0.5 (sum of the
+     * two fine edges along it).  Every write carries fidelity FINER, the
+     * highest, so every write lands; the last writer of an edge wins. */
+    void emf_corrections(FxPlan &plan)
+    {
+        std::vector<FxCorr> seq;
+        std::vector<std::array<int64_t, 5>> el;
+        for (int b : plan.active) {
+            for (int n = 0; n < FX_NSLOTS; ++n) {
+                const fx_slot &sl = b_[b].slot[n];
+                const int nid = sl.id;
+                if (nid < 0 || nid >= n_ || sl.rel_level >= 0) continue;
+                if (!active_block(b_[nid])) continue;
+                restrict_emf(b, nid, seq, el);
+            }
+        }
+        level_records(seq, el, 2, plan.emf_corr, plan.emf_corr_begin);
+    }
+
+    void restrict_emf(int fb, int cb, std::vector<FxCorr> &seq, std::vector<std::array<int64_t, 5>> &el)
+    {
+        const fx_block_desc &fine = b_[fb];
+        const fx_block_desc &coarse = b_[cb];
+        int axis[3];
+        int touch = 0;
+        for (int d = 0; d < 3; ++d) {
+            if (std::fabs(fine.xmax[d] - coarse.xmin[d]) < 1.0e-12 * fine.dx[d]) {
+                axis[d] = 1;
+                ++touch;
+            } else if (std::fabs(coarse.xmax[d] - fine.xmin[d]) < 1.0e-12 * fine.dx[d]) {
+                axis[d] = -1;
+                ++touch;
+            } else {
+                axis[d] = 0;
+            }
+        }
+        if (touch == 0 || touch > 2) return;
+        int it_send[3] = {-100, -100, -100};
+        int it_recv[3] = {-100, -100, -100};
+        for (int d = 0; d < 3; ++d) {
+            if (axis[d] == 1) {
+                it_send[d] = BS;
+                it_recv[d] = 0;
+            }
+            if (axis[d] == -1) {
+                it_send[d] = 0;
+                it_recv[d] = BS;
+            }
+        }
+        auto emit = [&](int dir, const int snd0[3], const int snd1[3], const int rcv[3]) {
+            FxCorr rec;
+            std::memset(&rec, 0, sizeof(rec));
+            rec.dst_block = cb;
+            rec.dst = dir * FX_NEDGES + fx_edge_idx(dir, rcv[0], rcv[1], rcv[2]);
+            rec.src_block = fb;
+            rec.src[0] = dir * FX_NEDGES + fx_edge_idx(dir, snd0[0], snd0[1], snd0[2]);
+            rec.src[1] = dir * FX_NEDGES + fx_edge_idx(dir, snd1[0], snd1[1], snd1[2]);
+            std::array<int64_t, 5> e;
+            e[0] = (int64_t)cb * FX_EMF_COUNT + rec.dst;
+            e[1] = (int64_t)fb * FX_EMF_COUNT + rec.src[0];
+            e[2] = (int64_t)fb * FX_EMF_COUNT + rec.src[1];
+            e[3] = e[4] = -1;
+            seq.push_back(rec);
+            el.push_back(e);
+        };
+        for (int dir = 0; dir < 3; ++dir) {
+            if (axis[dir] != 0) continue;
+            const int i_offset =
+                (fine.xmin[dir] + fine.xmax[dir]) < (coarse.xmin[dir] + coarse.xmax[dir]) ? 0 : BS / 2;
+            const int tan0 = (dir + 1) % 3;
+            const int tan1 = (dir + 2) % 3;
+            if (axis[tan0] != 0 && axis[tan1] != 0) {
+                for (int i = 0; i < BS; i += 2) {
+                    int s0[3] = {it_send[0], it_send[1], it_send[2]};
+                    int s1[3] = {it_send[0], it_send[1], it_send[2]};
+                    s0[dir] = i;
+                    s1[dir] = i + 1;
+                    it_recv[dir] = i / 2 + i_offset;
+                    emit(dir, s0, s1, it_recv);
+                }
+            } else {
+                const int free_ax = axis[tan0] != 0 ? tan1 : tan0;
+                const int j_offset =
+                    (fine.xmin[free_ax] + fine.xmax[free_ax]) < (coarse.xmin[free_ax] + coarse.xmax[free_ax]) ?
+                    0 : BS / 2;
+                for (int i = 0; i < BS; i += 2) {
+                    for (int j = 0; j <= BS; j += 2) {
+                        it_send[free_ax] = j;
+                        it_recv[free_ax] = j / 2 + j_offset;
+                        int s0[3] = {it_send[0], it_send[1], it_send[2]};
+                        int s1[3] = {it_send[0], it_send[1], it_send[2]};
+                        s0[dir] = i;
+                        s1[dir] = i + 1;
+                        it_recv[dir] = i / 2 + i_offset;
+                        emit(dir, s0, s1, it_recv);
+                    }
+                }
+            }
+        }
+    }
+
+    /* sequential correction records -> waves: a record whose destination is
+     * overwritten before anything reads it is dropped, the rest are levelled
+     * like the ghost operations (read-after-write, write-after-read,
+     * write-after-write) */
+    static void level_records(const std::vector<FxCorr> &seq, const std::vector<std::array<int64_t, 5>> &el,
+        int nsrc, std::vector<FxCorr> &out, std::vector<int> &begin)
+    {
+        const int n = (int)seq.size();
+        std::vector<char> live(n, 0);
+        std::unordered_map<int64_t, char> needed; /* absent: the final value, needed */
+        for (int x = n - 1; x >= 0; --x) {
+            const int64_t d = el[x][0];
+            const auto it = needed.find(d);
+            live[x] = it == needed.end() || it->second;
+            needed[d] = 0;
+            if (!live[x]) continue;
+            for (int q = 1; q <= nsrc; ++q) needed[el[x][q]] = 1;
+        }
+        std::unordered_map<int64_t, int> lw, lr;
+        auto get = [](const std::unordered_map<int64_t, int> &m, int64_t k) {
+            const auto it = m.find(k);
+            return it == m.end() ? -1 : it->second;
+        };
+        std::vector<std::vector<FxCorr>> waves;
+        for (int x = 0; x < n; ++x) {
+            if (!live[x]) continue;
+            const int64_t d = el[x][0];
+            int wave = std::max(get(lw, d), get(lr, d)) + 1;
+            for (int q = 1; q <= nsrc; ++q) wave = std::max(wave, get(lw, el[x][q]) + 1);
+            for (int q = 1; q <= nsrc; ++q) lr[el[x][q]] = std::max(get(lr, el[x][q]), wave);
+            lw[d] = wave;
+            if ((int)waves.size() <= wave) waves.resize(wave + 1);
+            waves[wave].push_back(seq[x]);
+        }
+        out.clear();
+        begin.clear();
+        for (const auto &w : waves) {
+            begin.push_back((int)out.size());
+            out.insert(out.end(), w.begin(), w.end());
+        }
+        begin.push_back((int)out.size());
+    }
+
     /* ---- optimisation and levelling -------------------------------------- */
 
     void finish(FxPlan &plan)
@@ -568,7 +975,10 @@ private:
             const SeqOp &o = seq_[x];
             if (seq_[x].space == SPACE_CELL) ++stats_.emitted_cell_ops;
             else ++stats_.emitted_face_ops;
-            live[x] = (ver_[o.w] == x) || readers[x] > 0;
+            live[x] = readers[x] > 0;
+            for (int q = o.w_begin; q < o.w_end && !live[x]; ++q) {
+                live[x] = ver_[wr_[q]] == x;
+            }
             if (!live[x]) {
                 ++stats_.dead;
                 continue;
@@ -617,17 +1027,21 @@ private:
         std::vector<int> lw((size_t)(2 * ncell_ + nface_), -1);
         std::vector<int> lr((size_t)(2 * ncell_ + nface_), -1);
         std::vector<std::vector<FxGop>> wc, wf;
+        std::vector<std::vector<FxPop>> wp;
         std::vector<std::vector<FxBop>> wb;
-        auto place = [&](const int64_t *reads, int nr, int64_t w) {
+        auto place = [&](const int64_t *reads, int nr, const int64_t *writes, int nw) {
             int wave = 0;
             for (int n = 0; n < nr; ++n) wave = std::max(wave, lw[reads[n]] + 1);
-            wave = std::max(wave, lw[w] + 1);
-            wave = std::max(wave, lr[w] + 1);
+            for (int n = 0; n < nw; ++n) {
+                wave = std::max(wave, lw[writes[n]] + 1);
+                wave = std::max(wave, lr[writes[n]] + 1);
+            }
             for (int n = 0; n < nr; ++n) lr[reads[n]] = std::max(lr[reads[n]], wave);
-            lw[w] = wave;
+            for (int n = 0; n < nw; ++n) lw[writes[n]] = wave;
             if ((int)wc.size() <= wave) {
                 wc.resize(wave + 1);
                 wf.resize(wave + 1);
+                wp.resize(wave + 1);
                 wb.resize(wave + 1);
             }
             return wave;
@@ -636,12 +1050,16 @@ private:
             if (!live[x]) continue;
             const SeqOp &o = seq_[x];
             const int nr = o.prod_end - o.prod_begin;
-            const int wave = place(&rd_[o.prod_begin], nr, o.w);
-            (o.space == SPACE_CELL ? wc : wf)[wave].push_back(o.op);
+            const int wave = place(&rd_[o.prod_begin], nr, &wr_[o.w_begin], o.w_end - o.w_begin);
+            if (o.space == SPACE_GROUP) {
+                wp[wave].push_back(groups_[o.op.dst]);
+            } else {
+                (o.space == SPACE_CELL ? wc : wf)[wave].push_back(o.op);
+            }
         }
         for (size_t q = 0; q < bops.size(); ++q) {
             const int64_t w = cellb_elem(FX_CELL_BLOCK(bops[q].dst), FX_CELL_IDX(bops[q].dst));
-            const int wave = place(bop_reads[q].data(), 6, w);
+            const int wave = place(bop_reads[q].data(), 6, &w, 1);
             wb[wave].push_back(bops[q]);
         }
         FxProgram &g = plan.ghost;
@@ -653,13 +1071,16 @@ private:
             std::stable_sort(wf[w].begin(), wf[w].end(), by_type);
             g.cell_begin.push_back((int)g.cell_ops.size());
             g.face_begin.push_back((int)g.face_ops.size());
+            g.p_begin.push_back((int)g.p_ops.size());
             g.b_begin.push_back((int)g.b_ops.size());
             g.cell_ops.insert(g.cell_ops.end(), wc[w].begin(), wc[w].end());
             g.face_ops.insert(g.face_ops.end(), wf[w].begin(), wf[w].end());
+            g.p_ops.insert(g.p_ops.end(), wp[w].begin(), wp[w].end());
             g.b_ops.insert(g.b_ops.end(), wb[w].begin(), wb[w].end());
         }
         g.cell_begin.push_back((int)g.cell_ops.size());
         g.face_begin.push_back((int)g.face_ops.size());
+        g.p_begin.push_back((int)g.p_ops.size());
         g.b_begin.push_back((int)g.b_ops.size());
         plan.stats = stats_;
     }
@@ -674,6 +1095,9 @@ private:
     std::vector<SeqOp> seq_;
     std::vector<int> prod_;      /* producers of the values each op reads */
     std::vector<int64_t> rd_;    /* elements each op reads (parallel to prod_) */
+    std::vector<int64_t> wr_;    /* elements each op writes */
+    std::vector<FxPop> groups_;  /* face-prolongation groups (SPACE_GROUP ops) */
+    std::unordered_map<int64_t, ProlongSig> psig_;
     FxPlanStats stats_;
     std::string *err_ = nullptr;
 };

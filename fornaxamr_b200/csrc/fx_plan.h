@@ -13,14 +13,16 @@
 /* The ghost fill as waves of element operations.  Operations inside one
  * wave touch disjoint elements (no read/write or write/write overlap), so a
  * wave runs as one parallel kernel; waves run in order.  Each wave holds
- * cell operations (primitives 0..5), face operations and cell-field
- * operations (bf2bc of one cell). */
+ * cell operations (primitives 0..5), face operations, face-prolongation
+ * groups and cell-field operations (bf2bc of one cell). */
 struct FxProgram {
     std::vector<FxGop> cell_ops;
     std::vector<FxGop> face_ops;
+    std::vector<FxPop> p_ops;
     std::vector<FxBop> b_ops;
     std::vector<int> cell_begin; /* per wave: [begin, next begin) into cell_ops */
     std::vector<int> face_begin;
+    std::vector<int> p_begin;
     std::vector<int> b_begin;
     int nwaves() const { return cell_begin.empty() ? 0 : (int)cell_begin.size() - 1; }
 };
@@ -35,8 +37,10 @@ struct FxPlanStats {
 struct FxPlan {
     FxProgram ghost;
     FxPlanStats stats;
-    std::vector<FxCorr> flux_corr;  /* prj_riemann_flux_send records */
-    std::vector<FxCorr> emf_corr;   /* prj_mhd_emf_send records */
+    std::vector<FxCorr> flux_corr;  /* prj_riemann_flux_send records, by wave */
+    std::vector<FxCorr> emf_corr;   /* prj_mhd_emf_send records, by wave */
+    std::vector<int> flux_corr_begin; /* per wave offsets (+1 closing entry) */
+    std::vector<int> emf_corr_begin;
     std::vector<int> active;        /* active block indices in mesh order */
 };
 

@@ -14,6 +14,7 @@
  */
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
@@ -46,6 +47,7 @@ struct fx_ctx {
     int *d_active = nullptr;
     int nactive = 0;
     FxGop *d_cops = nullptr, *d_fops = nullptr;
+    FxPop *d_pops = nullptr;
     FxBop *d_bops = nullptr;
     FxCorr *d_fcorr = nullptr, *d_ecorr = nullptr;
 
@@ -177,7 +179,9 @@ void free_mesh(fx_ctx *c)
     cudaFree(c->d_active);
     cudaFree(c->d_cops);
     cudaFree(c->d_fops);
+    cudaFree(c->d_pops);
     cudaFree(c->d_bops);
+    c->d_pops = nullptr;
     c->d_bops = nullptr;
     cudaFree(c->d_fcorr);
     cudaFree(c->d_ecorr);
@@ -217,7 +221,27 @@ void ghost_fill(fx_ctx *c, int slot)
         fx_launch_ghost_wave(c->D,
             c->d_cops + g.cell_begin[w], g.cell_begin[w + 1] - g.cell_begin[w],
             c->d_fops + g.face_begin[w], g.face_begin[w + 1] - g.face_begin[w],
+            c->d_pops + g.p_begin[w], g.p_begin[w + 1] - g.p_begin[w],
             c->d_bops + g.b_begin[w], g.b_begin[w + 1] - g.b_begin[w], slot, 6, c->stream);
+    }
+}
+
+/* coarse/fine flux corrections (prj_riemann_flux_send), wave by wave;
+ * ncomp: flux components the face kernel stored */
+void flux_correct(fx_ctx *c, int ncomp, cudaStream_t s)
+{
+    const std::vector<int> &wb = c->plan.flux_corr_begin;
+    for (size_t w = 0; w + 1 < wb.size(); ++w) {
+        fx_launch_flux_correct(c->D, c->d_fcorr + wb[w], wb[w + 1] - wb[w], ncomp, s);
+    }
+}
+
+/* coarse/fine EMF corrections (prj_mhd_emf_send), wave by wave */
+void emf_correct(fx_ctx *c, cudaStream_t s)
+{
+    const std::vector<int> &wb = c->plan.emf_corr_begin;
+    for (size_t w = 0; w + 1 < wb.size(); ++w) {
+        fx_launch_emf_correct(c->D, c->d_ecorr + wb[w], wb[w + 1] - wb[w], s);
     }
 }
 
@@ -229,10 +253,10 @@ void stage_seq(fx_ctx *c, int form, int stage)
     cudaStream_t s = c->stream;
     const int full = form == FX_FORM_PLAIN ? 1 : 0;
     per_block(c, form, [&](const int *l, int n) { fx_launch_flux(c->D, l, n, 3, src, src, full, s); });
-    fx_launch_flux_correct(c->D, c->d_fcorr, (int)c->plan.flux_corr.size(), s);
+    flux_correct(c, full ? c->nv : 6, s);
     if (c->cfg.mhd) {
         per_block(c, form, [&](const int *l, int n) { fx_launch_emf(c->D, l, n, src, src, s); });
-        fx_launch_emf_correct(c->D, c->d_ecorr, (int)c->plan.emf_corr.size(), s);
+        emf_correct(c, s);
         per_block(c, form, [&](const int *l, int n) { fx_launch_bf_update(c->D, l, n, stage, s); });
     }
     per_block(c, form, [&](const int *l, int n) {
@@ -448,6 +472,7 @@ int fx_set_mesh(fx_ctx *c, int nblocks, const fx_block_desc *blocks)
     if ((rc = dev_alloc(c, &c->d_active, (size_t)c->nactive))) return rc;
     if ((rc = dev_alloc(c, &c->d_cops, c->plan.ghost.cell_ops.size()))) return rc;
     if ((rc = dev_alloc(c, &c->d_fops, c->plan.ghost.face_ops.size()))) return rc;
+    if ((rc = dev_alloc(c, &c->d_pops, c->plan.ghost.p_ops.size()))) return rc;
     if ((rc = dev_alloc(c, &c->d_bops, c->plan.ghost.b_ops.size()))) return rc;
     if ((rc = dev_alloc(c, &c->d_fcorr, c->plan.flux_corr.size()))) return rc;
     if ((rc = dev_alloc(c, &c->d_ecorr, c->plan.emf_corr.size()))) return rc;
@@ -482,6 +507,9 @@ int fx_set_mesh(fx_ctx *c, int nblocks, const fx_block_desc *blocks)
         if (!g.face_ops.empty()) {
             FX_CUDA(c, cudaMemcpyAsync(c->d_fops, g.face_ops.data(), g.face_ops.size() * sizeof(FxGop), h2d, s));
         }
+        if (!g.p_ops.empty()) {
+            FX_CUDA(c, cudaMemcpyAsync(c->d_pops, g.p_ops.data(), g.p_ops.size() * sizeof(FxPop), h2d, s));
+        }
         if (!g.b_ops.empty()) {
             FX_CUDA(c, cudaMemcpyAsync(c->d_bops, g.b_ops.data(), g.b_ops.size() * sizeof(FxBop), h2d, s));
         }
@@ -515,7 +543,7 @@ int fx_set_mesh(fx_ctx *c, int nblocks, const fx_block_desc *blocks)
 int fx_plan_export(const fx_config *cfg, int nblocks, const fx_block_desc *blocks, int which,
     int32_t *ops, int *nops, int32_t *wave_begin, int *nwaves)
 {
-    if (!cfg || nblocks <= 0 || !blocks || !nops || !nwaves || which < 0 || which > 5) {
+    if (!cfg || nblocks <= 0 || !blocks || !nops || !nwaves || which < 0 || which > 6) {
         return FX_EINVAL;
     }
     FxPlan plan;
@@ -524,12 +552,15 @@ int fx_plan_export(const fx_config *cfg, int nblocks, const fx_block_desc *block
         return FX_EINVAL;
     }
     const FxProgram &g = plan.ghost;
-    if (which <= 1 || which == 4) {
+    if (which <= 1 || which == 4 || which == 6) {
         const void *data = which == 0 ? (const void *)g.cell_ops.data() :
-            which == 1 ? (const void *)g.face_ops.data() : (const void *)g.b_ops.data();
-        const size_t count = which == 0 ? g.cell_ops.size() : which == 1 ? g.face_ops.size() : g.b_ops.size();
-        const size_t size = which == 4 ? sizeof(FxBop) : sizeof(FxGop);
-        const std::vector<int> &wb = which == 0 ? g.cell_begin : which == 1 ? g.face_begin : g.b_begin;
+            which == 1 ? (const void *)g.face_ops.data() :
+            which == 4 ? (const void *)g.b_ops.data() : (const void *)g.p_ops.data();
+        const size_t count = which == 0 ? g.cell_ops.size() : which == 1 ? g.face_ops.size() :
+            which == 4 ? g.b_ops.size() : g.p_ops.size();
+        const size_t size = which == 4 ? sizeof(FxBop) : which == 6 ? sizeof(FxPop) : sizeof(FxGop);
+        const std::vector<int> &wb = which == 0 ? g.cell_begin : which == 1 ? g.face_begin :
+            which == 4 ? g.b_begin : g.p_begin;
         if (ops && (int)count <= *nops && count) {
             std::memcpy(ops, data, count * size);
         }
@@ -550,11 +581,16 @@ int fx_plan_export(const fx_config *cfg, int nblocks, const fx_block_desc *block
         *nwaves = g.nwaves();
     } else {
         const std::vector<FxCorr> &r = which == 2 ? plan.flux_corr : plan.emf_corr;
+        const std::vector<int> &wb = which == 2 ? plan.flux_corr_begin : plan.emf_corr_begin;
+        const int nw = (int)wb.size() - 1;
         if (ops && (int)r.size() <= *nops) {
             std::memcpy(ops, r.data(), r.size() * sizeof(FxCorr));
         }
+        if (wave_begin && nw <= *nwaves) {
+            std::memcpy(wave_begin, wb.data(), wb.size() * sizeof(int));
+        }
         *nops = (int)r.size();
-        *nwaves = 0;
+        *nwaves = nw;
     }
     return FX_SUCCESS;
 }
@@ -776,7 +812,7 @@ int fx_riemann_flux_send(fx_ctx *c)
 {
     if (!has_mesh(c)) return c ? set_err(c, FX_ENOMESH, "no mesh") : FX_EINVAL;
     fx_launch_set_dt(c->D, 0.0, c->stream);
-    fx_launch_flux_correct(c->D, c->d_fcorr, (int)c->plan.flux_corr.size(), c->stream);
+    flux_correct(c, c->nv, c->stream);
     return FX_SUCCESS;
 }
 
@@ -784,7 +820,7 @@ int fx_mhd_emf_send(fx_ctx *c)
 {
     if (!has_mesh(c)) return c ? set_err(c, FX_ENOMESH, "no mesh") : FX_EINVAL;
     fx_launch_set_dt(c->D, 0.0, c->stream);
-    fx_launch_emf_correct(c->D, c->d_ecorr, (int)c->plan.emf_corr.size(), c->stream);
+    emf_correct(c, c->stream);
     return FX_SUCCESS;
 }
 
@@ -1015,9 +1051,17 @@ int fx_info(fx_ctx *c, int what, long long *value)
 {
     if (!has_mesh(c) || !value) return c ? set_err(c, FX_EINVAL, "fx_info: no mesh") : FX_EINVAL;
     const FxProgram &g = c->plan.ghost;
-    const long long gw = g.nwaves();
-    const long long corr = (c->plan.flux_corr.empty() ? 0 : 1) +
-        (c->cfg.mhd && !c->plan.emf_corr.empty() ? 1 : 0);
+    /* ghost launches: per wave one for cell/face/cell-field ops and one for
+     * face-prolongation groups, when present */
+    long long gw = 0;
+    for (int w = 0; w < g.nwaves(); ++w) {
+        const bool ops = g.cell_begin[w + 1] > g.cell_begin[w] || g.face_begin[w + 1] > g.face_begin[w] ||
+            g.b_begin[w + 1] > g.b_begin[w];
+        gw += (ops ? 1 : 0) + (g.p_begin[w + 1] > g.p_begin[w] ? 1 : 0);
+    }
+    /* correction launches: one per non-empty wave */
+    const long long corr = (long long)std::max<size_t>(c->plan.flux_corr_begin.size(), 1) - 1 +
+        (c->cfg.mhd ? (long long)std::max<size_t>(c->plan.emf_corr_begin.size(), 1) - 1 : 0);
     const long long mhd = c->cfg.mhd ? 1 : 0;
     switch (what) {
     case 0: /* reset + 2 x (flux + emf + ct + cells + ghost waves) */
@@ -1028,7 +1072,7 @@ int fx_info(fx_ctx *c, int what, long long *value)
         break;
     case 2: *value = (long long)g.cell_ops.size(); break;
     case 3: *value = (long long)g.face_ops.size(); break;
-    case 4: *value = gw; break;
+    case 4: *value = g.nwaves(); break;
     case 5: *value = (long long)g.b_ops.size(); break;
     default: return set_err(c, FX_EINVAL, "fx_info: unknown query");
     }

@@ -132,9 +132,11 @@ int fx_set_mesh(fx_ctx *ctx, int nblocks, const fx_block_desc *blocks);
 
 /* Host-only inspection of the compiled ghost fill (no device needed).
  * which = 0: cell program, 1: face program, 2: flux corrections,
- * 3: EMF corrections.  Call with NULL buffers to get *nops and *nwaves;
- * then ops receives 4 int32 per operation (dst, src, aux, type; 8 for the
- * correction records) and wave_begin nwaves + 1 offsets. */
+ * 3: EMF corrections, 4: cell-field (bf2bc) operations, 5: compiler
+ * statistics, 6: face-prolongation groups.  Call with NULL buffers to get
+ * *nops and *nwaves; then ops receives 4 int32 per operation for 0/1
+ * (dst, src, aux, type) and 8 for 2/3/4/6, and wave_begin nwaves + 1
+ * offsets. */
 int fx_plan_export(const fx_config *cfg, int nblocks, const fx_block_desc *blocks, int which,
     int32_t *ops, int *nops, int32_t *wave_begin, int *nwaves);
 
@@ -257,7 +259,8 @@ int fx_time_phase(fx_ctx *ctx, int phase, int reps, double dt, double *ms);
 int fx_autotune(fx_ctx *ctx, double *times_ms, int n, int *choice);
 
 /* what = 0: kernel launches per batched step, 1: per plain step,
- * 2/3: ghost cell/face operations, 4/5: ghost cell/face waves */
+ * 2/3: ghost cell/face operations, 4: ghost-fill waves, 5: cell-field
+ * (bf2bc) operations */
 int fx_info(fx_ctx *ctx, int what, long long *value);
 
 #ifdef __cplusplus

@@ -211,6 +211,20 @@ class Reference:
     def fill_ghosts(self, stage: int, use_bf1: int) -> None:
         self.lib.rh_fill_ghosts(stage, use_bf1)
 
+    def flux_send(self) -> None:
+        """prj_riemann_flux_send on the current flux arrays."""
+        self.lib.rh_flux_send()
+
+    def emf_send(self) -> None:
+        """prj_mhd_emf_send on the current emf arrays (no-op for hydro)."""
+        self.lib.rh_emf_send()
+
+    def set_flux(self, b: int, d: int, data: np.ndarray) -> None:
+        self._set(b, ARR_FLUX, d, data)
+
+    def set_emf(self, b: int, d: int, data: np.ndarray) -> None:
+        self._set(b, ARR_EMF, d, data)
+
     def mesh_arrays(self):
         """(ints [n,4], geom [n,13], slots [n,56,15]) of the current mesh."""
         nb = self.nblocks()
@@ -317,4 +331,31 @@ def params_fourier(root: int = 8, nmodes: int = 32, kmax: int = 4, amp_rho: floa
     p.amp_v = amp_v
     p.amp_A = amp_A
     p.seed_rho, p.seed_v, p.seed_A = seeds
+    return p
+
+
+def params_amr_blast(root: int = 8, half_width: float = 0.7, max_level: int = 2,
+                     radii=(0.4, 0.2, 0.1), gamma: float = 5.0 / 3.0) -> RhParams:
+    """Magnetised blast on a static AMR hierarchy: rho = 1, p = 0.1 outside and
+    10 inside r < 0.05 about (0.1, 0.05, 0), B = (1, 1, 0) / sqrt(2) /
+    sqrt(4 pi) through A = (0, 0, Bx y - By x).  Blocks of level l that
+    overlap the ball of radius radii[l] about the same centre are refined
+    (the block-overlaps-ball rule of problems/prj_problem_sedov.c), then the
+    reference's 2:1 balance runs."""
+    p = RhParams()
+    p.config = CFG_AMR_BLAST
+    p.root[:] = [root, root, root]
+    p.max_level = max_level
+    p.max_blocks = 200000
+    p.xmin[:] = [-half_width] * 3
+    p.xmax[:] = [half_width] * 3
+    p.gamma = gamma
+    p.cfl = 0.4
+    p.dt_factor = 1.2
+    p.t_end = 1.0e30
+    p.center[:] = [0.1, 0.05, 0.0]
+    p.refine_radius[:] = list(radii) + [0.0] * (4 - len(radii))
+    p.p_in, p.p_out, p.r_in = 10.0, 0.1, 0.05
+    b = 1.0 / np.sqrt(2.0) / np.sqrt(4.0 * np.pi)
+    p.B0[:] = [b, b, 0.0]
     return p

@@ -279,6 +279,38 @@ static void rh_ensure_allocated(prj_mesh *mesh)
     }
 }
 
+/* Zero the state arrays of every allocated block.  Refinement prolongs the
+ * parents' (not yet initialised) arrays into the children and checks them
+ * for finite values; fresh heap memory is zero, recycled memory need not be,
+ * so a second setup in one process would otherwise fail. */
+static void rh_zero_state(prj_mesh *mesh)
+{
+    int b;
+
+    for (b = 0; b < mesh->nblocks; ++b) {
+        prj_block *block = &mesh->blocks[b];
+
+        if (block->W_mhd == 0) {
+            continue;
+        }
+        memset(block->W_mhd, 0, sizeof(double) * (size_t)PRJ_NVAR_MHD_PRIM * PRJ_BLOCK_NSTAGES *
+            PRJ_BLOCK_NCELLS);
+        if (block->eosvar != 0) {
+            memset(block->eosvar, 0, sizeof(double) * (size_t)PRJ_NVAR_EOSVAR * PRJ_BLOCK_NCELLS);
+        }
+#if PRJ_MHD
+        {
+            int d;
+            for (d = 0; d < 3; ++d) {
+                if (block->Bf[d] != 0) {
+                    memset(block->Bf[d], 0, sizeof(double) * (size_t)PRJ_BLOCK_NSTAGES * PRJ_BLOCK_NFACES);
+                }
+            }
+        }
+#endif
+    }
+}
+
 /* Static refinement in the pattern of problems/prj_problem_sedov.c:139-181. */
 static void rh_static_refine(void)
 {
@@ -287,6 +319,8 @@ static void rh_static_refine(void)
     for (level = 0; level < g_sim.mesh.max_level; ++level) {
         int b;
         int any = 0;
+
+        rh_zero_state(&g_sim.mesh);
 
         for (b = 0; b < g_sim.mesh.nblocks; ++b) {
             prj_block *block = &g_sim.mesh.blocks[b];
@@ -890,6 +924,19 @@ void rh_fill_ghosts(int stage, int use_bf1)
     prj_boundary_fill_ghosts_and_bf(&g_sim.mesh, &g_mpi, &g_sim.bc, stage, use_bf1, &g_sim.eos, 0,
         &g_sim.rad, PRJ_BOUNDARY_TIMER_SCOPE_NONE);
     prj_eos_fill_mesh(&g_sim.mesh, &g_sim.eos, &g_mpi, stage, PRJ_EOS_CTX_MAIN);
+}
+
+/* The coarse/fine corrections of a stage (src/prj_timeint.c:2750, 528). */
+void rh_flux_send(void)
+{
+    prj_riemann_flux_send(&g_sim.mesh, &g_mpi);
+}
+
+void rh_emf_send(void)
+{
+#if PRJ_MHD
+    prj_mhd_emf_send(&g_sim.mesh, &g_mpi);
+#endif
 }
 
 /* Per-block reference phases, for phase-level parity tests. */

@@ -107,6 +107,18 @@ def apply_cell_program(W, ops, waves, slot, nvg):
                 if t == GOP_COPY_USER:
                     vals[s[:, 2] != 0, 1] = 5.0
                 W[db, :nvg, slot, dc] = vals
+            elif t == GOP_PROLONG:
+                tx = np.where(s[:, 2] & 4, 0.25, -0.25)[:, None]
+                ty = np.where(s[:, 2] & 2, 0.25, -0.25)[:, None]
+                tz = np.where(s[:, 2] & 1, 0.25, -0.25)[:, None]
+
+                def q(off):
+                    return W[sb[:, None], np.arange(nvg)[None, :], slot, (sc + off)[:, None]]
+                base = q(0)
+                vx = base + minmod(q(-400), base, q(400)) * tx
+                vy = base + minmod(q(-20), base, q(20)) * ty
+                vz = base + minmod(q(-1), base, q(1)) * tz
+                W[db[:, None], np.arange(nvg)[None, :], slot, dc[:, None]] = vx + vy + vz - 2.0 * base
             elif t == GOP_RESTRICT:
                 acc = None
                 for off in (0, 1, 20, 21, 400, 401, 420, 421):
@@ -137,6 +149,99 @@ def apply_face_program(Bf, ops, waves, slot):
                 raise NotImplementedError(f"face op type {t}")
 
 
+def minmod(qm, q0, qp):
+    """prj_reconstruct_minmod_slope (src/prj_reconstruct.h:46-62)."""
+    sl = q0 - qm
+    sr = qp - q0
+    return np.where(sl * sr <= 0.0, 0.0, np.where(np.abs(sl) < np.abs(sr), sl, sr))
+
+
+def face_stride(d, a):
+    u = [0, 0, 0]
+    u[a] = 1
+    return int(face_idx(d, *u) - face_idx(d, 0, 0, 0))
+
+
+def apply_prolong_groups(Bf, pops, slot, dx):
+    """Toth-Roe groups (prj_mhd_prolong_bf_from_buffer, src/prj_mhd.c:374-512)
+    of one wave, vectorised over groups.  dx: [nb, 3] cell widths."""
+    if len(pops) == 0:
+        return
+    fine, coarse, pos = pops[:, 0], pops[:, 1], pops[:, 2].astype(np.int64)
+    keep, ow, iw = pops[:, 3].astype(np.int64), pops[:, 4].astype(np.int64), pops[:, 5].astype(np.int64)
+    f0 = [(pos >> (5 * a)) & 31 for a in range(3)]
+    f0 = [x - 2 for x in f0]
+    c0 = [((pos >> (15 + 5 * a)) & 31) - 2 for a in range(3)]
+    fdx = dx[fine]
+    area = [fdx[:, 1] * fdx[:, 2], fdx[:, 0] * fdx[:, 2], fdx[:, 0] * fdx[:, 1]]
+    o = {}
+    writes = []
+    for d in range(3):
+        t0 = 1 if d == 0 else 0
+        t1 = 1 if d == 2 else 2
+        s0, s1 = face_stride(d, t0), face_stride(d, t1)
+        for side in range(2):
+            y = [c.copy() for c in c0]
+            y[d] = y[d] + side
+            cf = face_idx(d, *y)
+            for a in range(2):
+                for b in range(2):
+                    q = 8 * d + 4 * side + 2 * a + b
+                    x = [c.copy() for c in f0]
+                    x[d] = x[d] + 2 * side
+                    x[t0] = x[t0] + a
+                    x[t1] = x[t1] + b
+                    xf = face_idx(d, *x)
+                    kept = ((keep >> q) & 1).astype(bool)
+                    base = Bf[coarse, d, slot, cf]
+                    vx = base + minmod(Bf[coarse, d, slot, cf - s0], base, Bf[coarse, d, slot, cf + s0]) * (0.25 if a else -0.25)
+                    vy = base + minmod(Bf[coarse, d, slot, cf - s1], base, Bf[coarse, d, slot, cf + s1]) * (0.25 if b else -0.25)
+                    flux = (vx + vy - base) * area[d]
+                    o[d, side, a, b] = np.where(kept, Bf[fine, d, slot, xf] * area[d], flux)
+                    m = (~kept) & ((ow >> q) & 1).astype(bool)
+                    writes.append((d, fine[m], xf[m], flux[m] / area[d][m]))
+    dx1s, dx2s, dx3s = fdx[:, 0] * fdx[:, 0], fdx[:, 1] * fdx[:, 1], fdx[:, 2] * fdx[:, 2]
+    Uxx = Vyy = Wzz = Uxyz = Vxyz = Wxyz = 0.0
+    for i in range(2):
+        si = 1.0 if i else -1.0
+        for j in range(2):
+            sj = 1.0 if j else -1.0
+            for k in range(2):
+                sk = 1.0 if k else -1.0
+                u, v, w = o[0, i, j, k], o[1, j, i, k], o[2, k, i, j]
+                Uxx = Uxx + (si * sj * v + si * sk * w)
+                Vyy = Vyy + (sj * sk * w + sj * si * u)
+                Wzz = Wzz + (sk * si * u + sk * sj * v)
+                Uxyz = Uxyz + si * sj * sk * u / (dx2s + dx3s)
+                Vxyz = Vxyz + si * sj * sk * v / (dx1s + dx3s)
+                Wxyz = Wxyz + si * sj * sk * w / (dx1s + dx2s)
+    Uxx, Vyy, Wzz = Uxx * 0.125, Vyy * 0.125, Wzz * 0.125
+    Uxyz, Vxyz, Wxyz = Uxyz * 0.125, Vxyz * 0.125, Wxyz * 0.125
+    for d in range(3):
+        t0 = 1 if d == 0 else 0
+        t1 = 1 if d == 2 else 2
+        for a in range(2):
+            sa = 1.0 if a else -1.0
+            for b in range(2):
+                sb = 1.0 if b else -1.0
+                q = 4 * d + 2 * a + b
+                if d == 0:
+                    flux = 0.5 * (o[0, 1, a, b] + o[0, 0, a, b]) + Uxx + sb * dx3s * Vxyz + sa * dx2s * Wxyz
+                elif d == 1:
+                    flux = 0.5 * (o[1, 1, a, b] + o[1, 0, a, b]) + Vyy + sa * dx1s * Wxyz + sb * dx3s * Uxyz
+                else:
+                    flux = 0.5 * (o[2, 1, a, b] + o[2, 0, a, b]) + Wzz + sb * dx2s * Uxyz + sa * dx1s * Vxyz
+                x = [c.copy() for c in f0]
+                x[d] = x[d] + 1
+                x[t0] = x[t0] + a
+                x[t1] = x[t1] + b
+                xf = face_idx(d, *x)
+                m = ((iw >> q) & 1).astype(bool)
+                writes.append((d, fine[m], xf[m], (flux / area[d])[m]))
+    for d, fb, xf, val in writes:
+        Bf[fb, d, slot, xf] = val
+
+
 def apply_b_ops(W, Bf, bops, slot):
     """cell-field operations: W[6+d] of dst = 0.5 (f[2d] + f[2d+1])."""
     if len(bops) == 0:
@@ -154,13 +259,34 @@ def apply_ghost_program(W, Bf, cfg, desc, slot):
     nw = len(cw) - 1
     if Bf is not None:
         fops, fw = fx.plan_export(cfg, desc, 1)
+        pops, pw = fx.plan_export(cfg, desc, 6)
         bops, bw = fx.plan_export(cfg, desc, 4)
+        dx = np.array([[desc[b].dx[a] for a in range(3)] for b in range(len(desc))])
     for w in range(nw):
         apply_cell_program(W, cops[cw[w]:cw[w + 1]], [0, cw[w + 1] - cw[w]], slot, 6)
         if Bf is not None:
             apply_face_program(Bf, fops[fw[w]:fw[w + 1]], [0, fw[w + 1] - fw[w]], slot)
+            apply_prolong_groups(Bf, pops[pw[w]:pw[w + 1]], slot, dx)
             apply_b_ops(W, Bf, bops[bw[w]:bw[w + 1]], slot)
     return nw
+
+
+def apply_corrections(arr, recs, waves, kind, nv=9):
+    """Flux (kind 'flux': arr [nb, 3, nv*8000]) or EMF (kind 'emf': arr
+    [nb, 3, 8820]) correction records, wave by wave."""
+    for w in range(len(waves) - 1):
+        r = recs[waves[w]:waves[w + 1]].astype(np.int64)
+        if len(r) == 0:
+            continue
+        db, d_i, sb = r[:, 0], r[:, 1], r[:, 2]
+        flat = arr.reshape(arr.shape[0], -1)
+        if kind == "flux":
+            for v in range(nv):
+                off = 4 * v
+                flat[db, d_i + off] = 0.25 * (flat[sb, r[:, 3] + off] + flat[sb, r[:, 4] + off]
+                                              + flat[sb, r[:, 5] + off] + flat[sb, r[:, 6] + off])
+        else:
+            flat[db, d_i] = ((0.0 + flat[sb, r[:, 3]]) + flat[sb, r[:, 4]]) * 0.5
 
 
 def bf2bc(W, Bf, slot):

@@ -121,3 +121,72 @@ def test_divergence_free_at_roundoff(ref_mhd):
         bmax = max(np.abs(f[d][H.active_faces(d)]).max() for d in range(3))
         assert np.abs(div).max() * dx.min() / bmax <= 1e-13
     ctx.close()
+
+
+# static AMR: levels 0-2 with level-1 blocks both coarse and fine neighbours
+AMR3 = dict(root=3, radii=(0.25, 0.1))
+
+
+@pytest.mark.parametrize("form", [fx.FORM_PLAIN, fx.FORM_BATCHED])
+def test_amr_blast_mhd_steps_match_reference(ref_mhd, form):
+    p = R.params_amr_blast(**AMR3)
+    ref_mhd.setup(p)
+    ctx = make_ctx(ref_mhd, p, True)
+    assert ctx.calc_dt(p.cfl) == ref_mhd.calc_dt()
+    n, t_ref, dt_ref, st_ref = ref_mhd.run(2)
+    t, dt, st = ctx.run(form, 2, p.cfl, p.dt_factor, p.t_end, (0.0, 0.0, 0.0))
+    assert (t, dt, st) == (t_ref, dt_ref, st_ref)
+    assert_state_equal(ctx, ref_mhd, True)
+    ctx.close()
+
+
+def test_amr_stage_corrections_match_reference(ref_mhd):
+    """One stage on the AMR mesh: fluxes after prj_riemann_flux_send and EMFs
+    after prj_mhd_emf_send, at the entries the reference computes."""
+    p = R.params_amr_blast(**AMR3)
+    ref_mhd.setup(p)
+    ctx = make_ctx(ref_mhd, p, True)
+    dt = ref_mhd.calc_dt()
+    assert ctx.stage(fx.FORM_PLAIN, 1, dt) == ref_mhd.stage(1, dt)
+    ints, _, _ = ref_mhd.mesh_arrays()
+    for b in np.nonzero(ints[:, 2] == 1)[0]:
+        for d in range(3):
+            fp = H.flux_positions(d, 9, True)
+            assert np.array_equal(ctx.download_array(b, fx.ARR_FLUX, d)[fp], ref_mhd.flux(b, d)[fp])
+            ep = H.emf_positions(d)
+            assert np.array_equal(ctx.download_array(b, fx.ARR_EMF, d)[ep], ref_mhd.emf(b, d)[ep])
+    assert_state_equal(ctx, ref_mhd, True)
+    ctx.close()
+
+
+@pytest.mark.parametrize("form", [fx.FORM_PLAIN, fx.FORM_BATCHED])
+def test_amr_hydro_steps_match_reference(ref_hydro, form):
+    p = R.params_amr_blast(root=2, radii=(0.3, 0.1))
+    ref_hydro.setup(p)
+    ctx = make_ctx(ref_hydro, p, False)
+    n, t_ref, dt_ref, st_ref = ref_hydro.run(3)
+    t, dt, st = ctx.run(form, 3, p.cfl, p.dt_factor, p.t_end, (0.0, 0.0, 0.0))
+    assert (t, dt, st) == (t_ref, dt_ref, st_ref)
+    assert_state_equal(ctx, ref_hydro, False, True)
+    ctx.close()
+
+
+def test_amr_divergence_free_at_roundoff(ref_mhd):
+    p = R.params_amr_blast(**AMR3)
+    ref_mhd.setup(p)
+    ctx = make_ctx(ref_mhd, p, True)
+    ctx.run(fx.FORM_BATCHED, 4, p.cfl, p.dt_factor, p.t_end, (0.0, 0.0, 0.0))
+    nb = ref_mhd.nblocks()
+    W, Bf = device_state(ctx, nb, 9, True)
+    ints, geom, _ = ref_mhd.mesh_arrays()
+    r = np.arange(16)
+    i, j, k = np.meshgrid(r, r, r, indexing="ij")
+    bmax = max(np.abs(Bf[b, d, 0][H.active_faces(d)]).max() for b in range(nb) if ints[b, 2] == 1 for d in range(3))
+    for b in np.nonzero(ints[:, 2] == 1)[0]:
+        dx = geom[b, 6:9]
+        f = Bf[b, :, 0]
+        div = ((f[0][H.face_idx(0, i + 1, j, k)] - f[0][H.face_idx(0, i, j, k)]) / dx[0]
+               + (f[1][H.face_idx(1, i, j + 1, k)] - f[1][H.face_idx(1, i, j, k)]) / dx[1]
+               + (f[2][H.face_idx(2, i, j, k + 1)] - f[2][H.face_idx(2, i, j, k)]) / dx[2])
+        assert np.abs(div).max() * dx.min() / bmax <= 1e-13
+    ctx.close()

@@ -121,3 +121,51 @@ def test_ghost_compiler_statistics(ref_mhd):
     # every ghost cell of every block written once (8 blocks x (20^3 - 16^3))
     assert len(np.unique(cops[:, 0])) == len(cops) == 8 * (20 ** 3 - 16 ** 3)
     assert len(bops) == 8 * (20 ** 3 - 16 ** 3)
+
+
+# static AMR hierarchies of the magnetised blast: (root, radii) -> per-level
+# active blocks [0, 60, 32] (levels 1-2) and [9, 140, 32] (levels 0-2, with
+# level-1 blocks that are coarse for one neighbour and fine for another)
+AMR_CASES = [(2, (0.3, 0.1)), (3, (0.25, 0.1))]
+
+
+@pytest.mark.parametrize("root,radii", AMR_CASES)
+def test_amr_ghost_program_matches_reference(ref_mhd, root, radii):
+    p = R.params_amr_blast(root=root, radii=radii)
+    nw = _scrambled_fill_check(ref_mhd, p, True, seed=root)
+    assert nw >= 2
+
+
+def test_amr_hydro_ghost_program_matches_reference(ref_hydro):
+    p = R.params_amr_blast(root=2, radii=(0.3, 0.1))
+    _scrambled_fill_check(ref_hydro, p, False, seed=11)
+
+
+@pytest.mark.parametrize("root,radii", AMR_CASES)
+def test_amr_corrections_match_reference(ref_mhd, root, radii):
+    """prj_riemann_flux_send and prj_mhd_emf_send on scrambled flux / EMF
+    arrays against the compiled correction records."""
+    import fornaxamr_b200 as fx
+    p = R.params_amr_blast(root=root, radii=radii)
+    ref_mhd.setup(p)
+    desc, cfg = _desc_and_cfg(ref_mhd, p, True)
+    nb = ref_mhd.nblocks()
+    rng = np.random.default_rng(root)
+    flux = rng.uniform(-1.0, 1.0, size=(nb, 3, 9 * H.NCELLS))
+    emf = rng.uniform(-1.0, 1.0, size=(nb, 3, H.NEDGES))
+    emf[rng.uniform(size=emf.shape) < 0.05] = -0.0
+    for b in range(nb):
+        for d in range(3):
+            ref_mhd.set_flux(b, d, flux[b, d])
+            ref_mhd.set_emf(b, d, emf[b, d])
+    ref_mhd.flux_send()
+    ref_mhd.emf_send()
+    frec, fw = fx.plan_export(cfg, desc, 2)
+    erec, ew = fx.plan_export(cfg, desc, 3)
+    assert len(frec) > 0 and len(erec) > 0
+    H.apply_corrections(flux, frec, fw, "flux")
+    H.apply_corrections(emf, erec, ew, "emf")
+    for b in range(nb):
+        for d in range(3):
+            assert np.array_equal(flux[b, d], ref_mhd.flux(b, d))
+            assert np.array_equal(emf[b, d].view(np.int64), ref_mhd.emf(b, d).view(np.int64))
