@@ -359,3 +359,37 @@ def params_amr_blast(root: int = 8, half_width: float = 0.7, max_level: int = 2,
     b = 1.0 / np.sqrt(2.0) / np.sqrt(4.0 * np.pi)
     p.B0[:] = [b, b, 0.0]
     return p
+
+
+def params_collapse(root: int = 12, half_width: float = 1.0, max_level: int = 3,
+                    radii=(0.4, 0.2, 0.1), rho_c: float = 1.0e10, K: float = 4.6e5,
+                    beta: float = 1.0e4, gm_point: float = 0.0) -> RhParams:
+    """Collapse-like MHD with a static gravity field: rho = rho_c (1 +
+    (r/r0)^2)^-1.5 with r0 = 0.05 of the domain length, p = K rho^gamma
+    (gamma 4/3), v_r = -0.1 c_s r / (r + r0), a dipole-like loop field whose
+    central strength gives plasma beta `beta`, and g = -(gm_point +
+    M(<r)) x / r^3 written once into the blocks' grav arrays.  Blocks of
+    level l that overlap the ball of radius radii[l] about the origin are
+    refined, then 2:1 balanced."""
+    p = RhParams()
+    p.config = CFG_COLLAPSE
+    p.root[:] = [root, root, root]
+    p.max_level = max_level
+    p.max_blocks = 400000
+    p.xmin[:] = [-half_width] * 3
+    p.xmax[:] = [half_width] * 3
+    p.gamma = 4.0 / 3.0
+    p.cfl = 0.4
+    p.dt_factor = 1.2
+    p.t_end = 1.0e30
+    p.center[:] = [0.0, 0.0, 0.0]
+    p.refine_radius[:] = list(radii) + [0.0] * (4 - len(radii))
+    p.rho_c = rho_c
+    p.r0 = 0.05 * 2.0 * half_width
+    p.K = K
+    p.beta = beta
+    p.gm_point = gm_point
+    # central field 2 B0 (A_phi = B0 r0^3 R / (r^2 + r0^2)^1.5); beta = 2 p / B^2
+    p_c = K * rho_c ** p.gamma
+    p.B0[:] = [0.5 * np.sqrt(2.0 * p_c / beta), 0.0, 0.0]
+    return p

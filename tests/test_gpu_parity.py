@@ -20,14 +20,15 @@ pytestmark = pytest.mark.gpu
 TOL = 1e-12
 
 
-def make_ctx(ref, p, mhd):
+def make_ctx(ref, p, mhd, gravity=False):
     desc = H.ref_desc(ref)
     coord = [p.xmin[0], p.xmax[0], p.xmin[1], p.xmax[1], p.xmin[2], p.xmax[2]]
-    ctx = fx.Context(mhd, p.gamma, coord)
+    ctx = fx.Context(mhd, p.gamma, coord, gravity=gravity)
     ctx.set_mesh(desc)
     W, Bf = H.ref_state(ref)
     for b in range(W.shape[0]):
-        ctx.upload_block(b, W[b].ravel(), None if Bf is None else [Bf[b, d].ravel() for d in range(3)])
+        grav = [ref.grav(b, d) for d in range(3)] if gravity else None
+        ctx.upload_block(b, W[b].ravel(), None if Bf is None else [Bf[b, d].ravel() for d in range(3)], grav)
     return ctx
 
 
@@ -189,4 +190,18 @@ def test_amr_divergence_free_at_roundoff(ref_mhd):
                + (f[1][H.face_idx(1, i, j + 1, k)] - f[1][H.face_idx(1, i, j, k)]) / dx[1]
                + (f[2][H.face_idx(2, i, j, k + 1)] - f[2][H.face_idx(2, i, j, k)]) / dx[2])
         assert np.abs(div).max() * dx.min() / bmax <= 1e-13
+    ctx.close()
+
+
+@pytest.mark.parametrize("form", [fx.FORM_PLAIN, fx.FORM_BATCHED])
+def test_collapse_gravity_steps_match_reference(ref_mhd, form):
+    """4-level collapse with the static gravity source: momentum and energy
+    source terms and the dt_src clamp of the driver (src/main.c:555-560)."""
+    p = R.params_collapse(root=4)
+    ref_mhd.setup(p)
+    ctx = make_ctx(ref_mhd, p, True, gravity=True)
+    n, t_ref, dt_ref, st_ref = ref_mhd.run(2)
+    t, dt, st = ctx.run(form, 2, p.cfl, p.dt_factor, p.t_end, (0.0, 0.0, 0.0))
+    assert (t, dt, st) == (t_ref, dt_ref, st_ref)
+    assert_state_equal(ctx, ref_mhd, True)
     ctx.close()
