@@ -45,6 +45,9 @@ class Block:
     dx: List[float]
     active: int = 1
     slots: List[Slot] = field(default_factory=lambda: [Slot() for _ in range(56)])
+    refine_flag: int = 0
+    parent: int = -1
+    children: List[int] = field(default_factory=lambda: [-1] * 8)
 
     @property
     def vol(self) -> float:
@@ -146,6 +149,177 @@ def uniform_mesh(root: Sequence[int], coord: Sequence[float]) -> List[Block]:
                             b.slots[s].id = nid
                             compute_geometry(b, blocks[nid], b.slots[s])
     return blocks
+
+
+# ---- static refinement ------------------------------------------------------
+
+
+def _touch_face_edge_corner(a: Block, b: Block) -> bool:
+    """prj_boxes_touch_face_edge_corner (src/prj_amr.c:398-425)."""
+    tol = 1.0e-12
+    touches = 0
+    for ax in range(3):
+        if not (min(a.xmax[ax], b.xmax[ax]) >= max(a.xmin[ax], b.xmin[ax]) - tol):
+            return False
+        if abs(a.xmax[ax] - b.xmin[ax]) < tol or abs(b.xmax[ax] - a.xmin[ax]) < tol:
+            touches += 1
+    if touches == 0:
+        return False
+    if all(abs(a.xmin[ax] - b.xmin[ax]) < tol and abs(a.xmax[ax] - b.xmax[ax]) < tol for ax in range(3)):
+        return False
+    return True
+
+
+def _add_neighbor(a: Block, b: Block) -> None:
+    """prj_add_neighbor (src/prj_amr.c:540-573): first free slot."""
+    if any(sl.id == b.id for sl in a.slots):
+        return
+    for sl in a.slots:
+        if sl.id < 0:
+            sl.id = b.id
+            compute_geometry(a, b, sl)
+            return
+    raise ValueError("more than 56 neighbours")
+
+
+def _logical_coords(b: Block, root: Sequence[int], coord: Sequence[float]):
+    """prj_mesh_block_logical_coords (src/prj_mesh.c:1250-1288)."""
+    out = []
+    for ax in range(3):
+        lo, hi = coord[2 * ax], coord[2 * ax + 1]
+        count = float(root[ax]) * 2.0 ** b.level
+        scaled = (b.xmin[ax] - lo) * (count / (hi - lo))
+        out.append(int(scaled + 0.5))
+    return tuple(out)
+
+
+def init_neighbors(blocks: List[Block], root: Sequence[int], coord: Sequence[float]) -> None:
+    """prj_amr_init_neighbors, Morton path (src/prj_amr.c:1551-1579,
+    575-711): clear every slot list, then for each active block in index
+    order probe the candidate boxes of levels l-1, l, l+1 and register every
+    touching pair both ways in the first free slots."""
+    import math
+    for b in blocks:
+        if b.id >= 0:
+            b.slots = [Slot() for _ in range(56)]
+    lookup = {}
+    for b in blocks:
+        if b.id >= 0 and b.active == 1:
+            lookup[(b.level,) + _logical_coords(b, root, coord)] = b.id
+    for a in blocks:
+        if a.id < 0 or a.active != 1:
+            continue
+        for lev in (a.level - 1, a.level, a.level + 1):
+            if lev < 0:
+                continue
+            rng = []
+            for ax in range(3):
+                lo_c, hi_c = coord[2 * ax], coord[2 * ax + 1]
+                scale = (float(root[ax]) * 2.0 ** lev) / (hi_c - lo_c)
+                lo = (a.xmin[ax] - lo_c) * scale
+                hi = (a.xmax[ax] - lo_c) * scale
+                rng.append(range(int(math.floor(lo)) - 1, int(math.ceil(hi)) + 1))
+            for ix in rng[0]:
+                for iy in rng[1]:
+                    for iz in rng[2]:
+                        if ix < 0 or iy < 0 or iz < 0:
+                            continue
+                        nid = lookup.get((lev, ix, iy, iz), -1)
+                        if nid < 0 or nid == a.id:
+                            continue
+                        b = blocks[nid]
+                        if _touch_face_edge_corner(a, b):
+                            _add_neighbor(a, b)
+                            _add_neighbor(b, a)
+
+
+def _refine_block(blocks: List[Block], i: int, max_level: int) -> None:
+    """prj_amr_refine_block (src/prj_amr.c:2389-2497): eight children
+    appended in octant order (x fastest), the parent made inactive."""
+    p = blocks[i]
+    if p.active != 1 or p.level >= max_level:
+        return
+    xmid = [0.5 * (p.xmin[a] + p.xmax[a]) for a in range(3)]
+    for oct_ in range(8):
+        bits = (oct_ & 1, (oct_ >> 1) & 1, (oct_ >> 2) & 1)
+        xmin = [p.xmin[a] if bits[a] == 0 else xmid[a] for a in range(3)]
+        xmax = [xmid[a] if bits[a] == 0 else p.xmax[a] for a in range(3)]
+        child = Block(id=len(blocks), level=p.level + 1, xmin=xmin, xmax=xmax,
+                      dx=[p.dx[a] * 0.5 for a in range(3)], parent=p.id)
+        blocks.append(child)
+        p.children[oct_] = child.id
+    p.active = 0
+    p.refine_flag = 0
+
+
+def _enforce_two_to_one(blocks: List[Block]) -> None:
+    """prj_amr_enforce_two_to_one (src/prj_amr.c:1471-1499)."""
+    changed = True
+    while changed:
+        changed = False
+        for b in blocks:
+            if b.id < 0 or b.active != 1 or b.refine_flag <= 0:
+                continue
+            for sl in b.slots:
+                nb = blocks[sl.id] if 0 <= sl.id < len(blocks) else None
+                if nb is not None and nb.id >= 0 and nb.active == 1 and nb.level < b.level:
+                    if nb.refine_flag != 1:
+                        nb.refine_flag = 1
+                        changed = True
+
+
+def static_amr_mesh(root: Sequence[int], coord: Sequence[float], max_level: int, refine) -> List[Block]:
+    """A static AMR hierarchy built the way a problem's initial refinement
+    does it (the loop of problems/prj_problem_sedov.c:139-181): for each
+    level in turn, flag the active blocks of that level for which
+    refine(block, level) holds, enforce 2:1 balance, refine every flagged
+    block, and rebuild the neighbour slots.  Block order, child order and
+    slot order follow the reference, so the description is identical to the
+    reference mesh for the same rule."""
+    blocks = uniform_mesh(root, coord)
+    for level in range(max_level):
+        any_flag = False
+        for b in blocks:
+            if b.id < 0 or b.active != 1 or b.level != level:
+                continue
+            b.refine_flag = 0
+            if refine(b, level):
+                b.refine_flag = 1
+                any_flag = True
+        if not any_flag:
+            break
+        _enforce_two_to_one(blocks)
+        changed = False
+        i = 0
+        while i < len(blocks):
+            b = blocks[i]
+            if b.id >= 0 and b.active == 1 and b.refine_flag > 0:
+                _refine_block(blocks, i, max_level)
+                changed = changed or blocks[i].active == 0
+            i += 1
+        if not changed:
+            break
+        init_neighbors(blocks, root, coord)
+    return blocks
+
+
+def ball_refiner(center: Sequence[float], radii: Sequence[float]):
+    """Refine a level-l block when it overlaps the ball of radius radii[l]
+    about center (the block-overlaps-ball rule of problems/prj_problem_sedov.c:20-44)."""
+    def refine(b: Block, level: int) -> bool:
+        if level >= len(radii):
+            return False
+        d2 = 0.0
+        for a in range(3):
+            if b.xmin[a] > center[a]:
+                d = b.xmin[a] - center[a]
+            elif b.xmax[a] < center[a]:
+                d = center[a] - b.xmax[a]
+            else:
+                d = 0.0
+            d2 += d * d
+        return d2 < radii[level] * radii[level]
+    return refine
 
 
 def to_desc(blocks: Sequence[Block]) -> "C.Array":

@@ -164,3 +164,161 @@ def sod(blocks: Sequence[Block], gamma: float = 1.4):
             W[n, 4, s] = (p / ((gamma - 1.0) * rho)).ravel()
             W[n, 5, s] = 0.1
     return W
+
+
+# ---- static-AMR workloads ------------------------------------------------------
+
+NEDGES = (PBS + 1) * (PBS + 1) * PBS
+
+
+def _edge_index(d: int, i, j, k):
+    """EDGE_IDX of the reference layout (src/prj_defs.h)."""
+    i, j, k = i + NG, j + NG, k + NG
+    if d == 0:
+        return (i * (PBS + 1) + j) * (PBS + 1) + k
+    if d == 1:
+        return (i * PBS + j) * (PBS + 1) + k
+    return (i * (PBS + 1) + j) * PBS + k
+
+
+def _bfield_from_potential(blocks: Sequence[Block], apot, emf_records) -> np.ndarray:
+    """Bf [nb, 3, 2, NFACES] = discrete curl of A (src/prj_mhd.c:106-142).  A
+    is sampled at the edge centres of every live block, the coarse copies of
+    edges shared with finer blocks are replaced by the average of the two
+    fine edges (the EMF restriction records of prj_mhd_emf_send, given as
+    (records, wave offsets) from fx_plan_export), then differenced."""
+    nb = len(blocks)
+    E = np.zeros((nb, 3, NEDGES))
+    r = np.arange(-NG, BS + NG)
+    ei, ej, ek = np.meshgrid(r, r, r, indexing="ij")
+    for n, b in enumerate(blocks):
+        if b.id < 0 or b.active != 1:
+            continue
+        for d in range(3):
+            ex, ey, ez = np.meshgrid(_edges(b, 0, d), _edges(b, 1, d), _edges(b, 2, d), indexing="ij")
+            E[n, d][_edge_index(d, ei, ej, ek)] = apot(ex, ey, ez)[d]
+    recs, waves = emf_records
+    flat = E.reshape(nb, 3 * NEDGES)
+    for w in range(len(waves) - 1):
+        rr = recs[waves[w]:waves[w + 1]].astype(np.int64)
+        if len(rr):
+            # value = 0; value += e0; value += e1; value *= 0.5
+            flat[rr[:, 0], rr[:, 1]] = ((0.0 + flat[rr[:, 2], rr[:, 3]]) + flat[rr[:, 2], rr[:, 4]]) * 0.5
+    Bf = np.zeros((nb, 3, 2, NFACES))
+    f = np.arange(-NG, BS + NG - 1)
+    fi, fj, fk = np.meshgrid(f, f, f, indexing="ij")
+    for n, b in enumerate(blocks):
+        if b.id < 0 or b.active != 1:
+            continue
+        e1, e2, e3 = E[n, 0], E[n, 1], E[n, 2]
+        B1 = (e3[_edge_index(2, fi, fj + 1, fk)] - e3[_edge_index(2, fi, fj, fk)]) / b.dx[1] - \
+            (e2[_edge_index(1, fi, fj, fk + 1)] - e2[_edge_index(1, fi, fj, fk)]) / b.dx[2]
+        B2 = (e1[_edge_index(0, fi, fj, fk + 1)] - e1[_edge_index(0, fi, fj, fk)]) / b.dx[2] - \
+            (e3[_edge_index(2, fi + 1, fj, fk)] - e3[_edge_index(2, fi, fj, fk)]) / b.dx[0]
+        B3 = (e2[_edge_index(1, fi + 1, fj, fk)] - e2[_edge_index(1, fi, fj, fk)]) / b.dx[0] - \
+            (e1[_edge_index(0, fi, fj + 1, fk)] - e1[_edge_index(0, fi, fj, fk)]) / b.dx[1]
+        for d, Bd in enumerate((B1, B2, B3)):
+            Bf[n, d, 0][_face_index(d, fi, fj, fk)] = Bd
+            Bf[n, d, 1] = Bf[n, d, 0]
+    return Bf
+
+
+def _prim_cells(blocks: Sequence[Block], cell, nv: int) -> np.ndarray:
+    """W [nb, nv, 2, NCELLS] with both stage slots set from cell(x, y, z) ->
+    dict of variable arrays over the 20^3 cell centres of each live block."""
+    nb = len(blocks)
+    W = np.zeros((nb, nv, 2, NCELLS))
+    for n, b in enumerate(blocks):
+        if b.id < 0 or b.active != 1:
+            continue
+        x, y, z = np.meshgrid(_centers(b, 0), _centers(b, 1), _centers(b, 2), indexing="ij")
+        w = cell(x, y, z)
+        for v, a in w.items():
+            for s in range(2):
+                W[n, v, s] = np.broadcast_to(a, x.shape).ravel()
+    return W
+
+
+def amr_blast(blocks: Sequence[Block], emf_records=None, mhd: bool = True, gamma: float = 5.0 / 3.0,
+              center=(0.1, 0.05, 0.0), p_in: float = 10.0, p_out: float = 0.1, r_in: float = 0.05,
+              B0=None):
+    """Magnetised blast: rho = 1, p = p_in for r < r_in about center, p_out
+    elsewhere, v = 0, Ye = 0.1, B = (B0x, B0y, 0) through A = (0, 0,
+    B0x y - B0y x) (default B0 = (1, 1) / sqrt(2) / sqrt(4 pi)).  Returns W and,
+    for MHD, Bf; the ghost zones still need the ghost fill."""
+    if B0 is None:
+        b = 1.0 / math.sqrt(2.0) / math.sqrt(4.0 * math.pi)
+        B0 = (b, b, 0.0)
+
+    def cell(x, y, z):
+        dx, dy, dz = x - center[0], y - center[1], z - center[2]
+        r = np.sqrt(dx * dx + dy * dy + dz * dz)
+        p = np.where(r < r_in, p_in, p_out)
+        return {0: 1.0, 4: p / ((gamma - 1.0) * 1.0), 5: 0.1}
+
+    W = _prim_cells(blocks, cell, 9 if mhd else 6)
+    if not mhd:
+        return W, None
+
+    def apot(x, y, z):
+        return (np.zeros_like(x), np.zeros_like(x), B0[0] * y - B0[1] * x)
+
+    Bf = _bfield_from_potential(blocks, apot, emf_records)
+    for n in range(len(blocks)):
+        if blocks[n].active == 1:
+            bf2bc_all(W[n], Bf[n], 0)
+            bf2bc_all(W[n], Bf[n], 1)
+    return W, Bf
+
+
+def collapse(blocks: Sequence[Block], emf_records=None, half_width: float = 1.0, rho_c: float = 1.0e10,
+             K: float = 4.6e5, beta: float = 1.0e4, gm_point: float = 0.0, gamma: float = 4.0 / 3.0):
+    """Collapse-like MHD: rho = rho_c (1 + (r/r0)^2)^-1.5 with r0 = 0.05 of
+    the domain length, p = K rho^gamma, v_r = -0.1 c_s r / (r + r0), Ye = 0.1,
+    a dipole-like loop A_phi = B0 r0^3 R / (r^2 + r0^2)^1.5 with central field
+    2 B0 at plasma beta `beta`, and the static acceleration g = -(gm_point +
+    M(<r)) x / r^3 of the profile's enclosed mass.  Returns W, Bf and grav
+    [nb, 3, NCELLS] (all 20^3 cells)."""
+    r0 = 0.05 * 2.0 * half_width
+    p_c = K * rho_c ** gamma
+    B0 = 0.5 * math.sqrt(2.0 * p_c / beta)
+
+    def cell(x, y, z):
+        r = np.sqrt(x * x + y * y + z * z)
+        q = r / r0
+        s = 1.0 + q * q
+        rho = rho_c / (s * np.sqrt(s))
+        p = K * np.power(rho, gamma)
+        cs = np.sqrt(gamma * p / rho)
+        vr = -0.1 * cs * r / (r + r0)
+        with np.errstate(divide="ignore"):
+            inv_r = np.where(r > 0.0, 1.0 / r, 0.0)
+        return {0: rho, 1: vr * x * inv_r, 2: vr * y * inv_r, 3: vr * z * inv_r,
+                4: p / ((gamma - 1.0) * rho), 5: 0.1}
+
+    W = _prim_cells(blocks, cell, 9)
+
+    def apot(x, y, z):
+        r2 = x * x + y * y + z * z
+        s = r2 + r0 * r0
+        f = B0 * r0 * r0 * r0 / (s * np.sqrt(s))
+        return (-y * f, x * f, np.zeros_like(x))
+
+    Bf = _bfield_from_potential(blocks, apot, emf_records)
+    nb = len(blocks)
+    grav = np.zeros((nb, 3, NCELLS))
+    for n, b in enumerate(blocks):
+        if b.id < 0 or b.active != 1:
+            continue
+        bf2bc_all(W[n], Bf[n], 0)
+        bf2bc_all(W[n], Bf[n], 1)
+        x, y, z = np.meshgrid(_centers(b, 0), _centers(b, 1), _centers(b, 2), indexing="ij")
+        r = np.sqrt(x * x + y * y + z * z)
+        a = r / r0
+        menc = 4.0 * math.pi * rho_c * r0 * r0 * r0 * (np.arcsinh(a) - a / np.sqrt(1.0 + a * a))
+        with np.errstate(divide="ignore", invalid="ignore"):
+            gmag = np.where(r > 0.0, -(gm_point + menc) / (r * r * r), 0.0)
+        grav[n, 0] = (gmag * x).ravel()
+        grav[n, 1] = (gmag * y).ravel()
+        grav[n, 2] = (gmag * z).ravel()
+    return W, Bf, grav
