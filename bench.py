@@ -51,6 +51,10 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--amr-steps", type=int, default=10,
+                    help="batched steps of the static-AMR blast measurement (0: skip it)")
+    ap.add_argument("--collapse", action="store_true",
+                    help="also measure the 4-level gravity collapse (about 4600 blocks; slow set-up)")
     return ap.parse_args()
 
 
@@ -163,6 +167,96 @@ def flux_traffic_per_launch():
             return float(json.load(f)["dram_bytes_per_launch"])
     except (OSError, KeyError, ValueError):
         return None
+
+
+def run_amr(args, dev, kind):
+    """Batched vs plain on a static AMR hierarchy built on the host by the
+    product's mesh builder (the reference's refinement rule, 2:1 balance and
+    slot order): kind "blast" = magnetised blast, 8^3 roots on [-0.7, 0.7]^3,
+    levels refined inside r < 0.4 / 0.2 about (0.1, 0.05, 0) (3 levels);
+    kind "collapse" = gravity collapse, 12^3 roots on [-1, 1]^3, spheres
+    0.4 / 0.2 / 0.1 about the origin (4 levels).  Same metric as the headline
+    (active zones x steps / device time)."""
+    import numpy as np
+    import torch
+
+    import fornaxamr_b200 as fx
+    from fornaxamr_b200 import mesh, problems
+
+    t0 = time.time()
+    if kind == "blast":
+        hw, root, max_level, center, radii, gamma, gravity = 0.7, 8, 2, (0.1, 0.05, 0.0), (0.4, 0.2), 5.0 / 3.0, False
+    else:
+        hw, root, max_level, center, radii, gamma, gravity = 1.0, 12, 3, (0.0, 0.0, 0.0), (0.4, 0.2, 0.1), 4.0 / 3.0, True
+    coord = (-hw, hw, -hw, hw, -hw, hw)
+    blocks = mesh.static_amr_mesh((root,) * 3, coord, max_level, mesh.ball_refiner(center, radii))
+    desc = mesh.to_desc(blocks)
+    cfg = fx.make_config(True, gamma, coord)
+    recs = fx.plan_export(cfg, desc, 3)
+    t_mesh = time.time() - t0
+    if kind == "blast":
+        W0, Bf0 = problems.amr_blast(blocks, recs)
+        grav = None
+    else:
+        W0, Bf0, grav = problems.collapse(blocks, recs, half_width=hw)
+    t_init = time.time() - t0 - t_mesh
+    ctx = fx.Context(True, gamma, coord, gravity=gravity, device=dev)
+    t1 = time.time()
+    ctx.set_mesh(desc)
+    t_plan = time.time() - t1
+    ctx.upload_all(np.ascontiguousarray(W0), np.ascontiguousarray(Bf0))
+    if grav is not None:
+        for b in range(len(blocks)):
+            if blocks[b].active == 1:
+                ctx.upload_block(b, W0[b].ravel(), [Bf0[b, d].ravel() for d in range(3)],
+                                 [grav[b, d] for d in range(3)])
+    del W0, Bf0, grav
+    ctx.boundary_fill(1, 0)
+    ctx.sync()
+    ctx.autotune()
+    active = [b for b in blocks if b.active == 1]
+    zones = len(active) * 16 ** 3
+    levels = [0] * (max_level + 1)
+    for b in active:
+        levels[b.level] += 1
+    stream = torch.cuda.ExternalStream(ctx.stream(), device=dev)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    state = ctx.run(fx.FORM_BATCHED, max(args.warmup, 3), 0.4, 1.2, 1.0e30, (0.0, 0.0, 0))
+    ctx.sync()
+    torch.cuda.synchronize(dev)
+    e0.record(stream)
+    state = ctx.run(fx.FORM_BATCHED, args.amr_steps, 0.4, 1.2, 1.0e30, state)
+    e1.record(stream)
+    e1.synchronize()
+    ms_batched = e0.elapsed_time(e1) / args.amr_steps
+    dt = state[1]
+    ctx.step(fx.FORM_PLAIN, dt, want_dt_src=False)
+    ctx.sync()
+    nplain = max(1, args.plain_steps)
+    e0.record(stream)
+    for _ in range(nplain):
+        ctx.step(fx.FORM_PLAIN, dt, want_dt_src=False)
+    e1.record(stream)
+    e1.synchronize()
+    ms_plain = e0.elapsed_time(e1) / nplain
+    phases = {name: ctx.time_phase(ph, 3, dt) for name, ph in
+              (("flux_launch", 0), ("emf", 1), ("ct", 2), ("cells", 3), ("ghost", 4))}
+    out = {
+        "workload": ("magnetised blast, static AMR 3 levels" if kind == "blast" else
+                     "gravity collapse, static AMR 4 levels") + f", {len(active)} active blocks of 16^3",
+        "blocks_per_level": levels, "zones": zones,
+        "batched": {"ms_per_step": ms_batched, "value": zones / (ms_batched * 1e-3),
+                    "hbm_gbs_step": zones * BYTES_PER_ZONE_STEP / (ms_batched * 1e-3) / 1e9},
+        "plain": {"ms_per_step": ms_plain, "value": zones / (ms_plain * 1e-3)},
+        "batched_over_plain": ms_plain / ms_batched,
+        "phases_ms": phases,
+        "ghost_waves": ctx.info(4), "launches_per_batched_step": ctx.info(0) + 4,
+        "setup_s": {"mesh": round(t_mesh, 1), "initial_state": round(t_init, 1), "ghost_compiler": round(t_plan, 1)},
+        "steps": args.amr_steps,
+    }
+    ctx.close()
+    return out
 
 
 def run_fx(args, rank, world, local_rank):
@@ -350,6 +444,10 @@ def main():
         torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     line = run_fx(args, rank, world, local_rank)
     line["cpu_baseline"] = cb
+    if world == 1 and args.amr_steps > 0:
+        line["amr_blast"] = run_amr(args, local_rank, "blast")
+        if args.collapse:
+            line["amr_collapse"] = run_amr(args, local_rank, "collapse")
     if world > 1:
         import torch
         torch.distributed.barrier()

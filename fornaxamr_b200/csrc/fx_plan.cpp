@@ -92,14 +92,14 @@ bool face_active(int dir, int i, int j, int k)
  * face-prolongation group (several writes) */
 struct SeqOp {
     FxGop op;          /* SPACE_GROUP: op.dst indexes the group table */
-    int64_t src;       /* single source element, -1 for multi-source ops */
-    int src_ver;       /* producer of the source value (op index, -1 initial) */
-    int space;
-    int prod_begin;    /* producers of the values read: [prod_begin, prod_end) */
-    int prod_end;
-    int w_begin;       /* elements written: [w_begin, w_end) of the write list */
-    int w_end;
+    int32_t src_ver;   /* single-source ops: producer of the source value (op index, -1 initial) */
+    int32_t prod_begin; /* producers of the values read: [prod_begin, next op's prod_begin) */
+    int32_t w_begin;   /* elements written: [w_begin, next op's w_begin) of the write list */
+    int32_t space;
 };
+
+/* element ids: cells, cell fields and faces of all blocks in one space */
+using Elem = uint32_t;
 
 /* what a prolonged outer face was computed from: a recomputation with the
  * same coarse face, target and stencil versions stores the same value */
@@ -115,10 +115,29 @@ public:
     Compiler(const fx_config &cfg, int nblocks, const fx_block_desc *blocks)
         : cfg_(cfg), n_(nblocks), b_(blocks),
           ncell_((int64_t)nblocks * FX_NCELLS),
-          nface_((int64_t)(cfg.mhd ? nblocks : 0) * 3 * FX_NFACES),
-          fid_((size_t)nface_, 0),
-          ver_((size_t)(2 * ncell_ + nface_), -1)
+          nface_((int64_t)(cfg.mhd ? nblocks : 0) * 3 * FX_NFACES)
     {
+    }
+
+    /* the coarse/fine correction records only (no ghost-fill replay) */
+    bool run_corrections(FxPlan &plan, std::string *err)
+    {
+        err_ = err;
+        for (int b = 0; b < n_; ++b) {
+            if (active_block(b_[b])) {
+                plan.active.push_back(b);
+            }
+        }
+        if (!validate()) {
+            return false;
+        }
+        flux_corrections(plan);
+        if (cfg_.mhd) {
+            emf_corrections(plan);
+        } else {
+            plan.emf_corr_begin.assign(1, 0);
+        }
+        return true;
     }
 
     bool run(FxPlan &plan, std::string *err)
@@ -132,6 +151,14 @@ public:
         if (!validate()) {
             return false;
         }
+        fid_.assign((size_t)nface_, 0);
+        ver_.assign((size_t)(2 * ncell_ + nface_), -1);
+        /* roughly one operation per ghost cell and ghost face of a block */
+        const size_t est = plan.active.size() * (size_t)(cfg_.mhd ? 18000 : 4000);
+        seq_.reserve(est);
+        prod_.reserve(est + est / 4);
+        rd_.reserve(est + est / 4);
+        wr_.reserve(est + est / 16);
         /* the reference sequence */
         for (int b : plan.active) {
             physical(b, PHYS_FACE_ONLY);
@@ -164,6 +191,9 @@ public:
             }
         }
         finish(plan);
+        if (overflow_) {
+            return fail("ghost fill needs more than 32766 waves");
+        }
         flux_corrections(plan);
         if (cfg_.mhd) {
             emf_corrections(plan);
@@ -182,6 +212,11 @@ private:
 
     bool validate()
     {
+        /* packed keys hold a block index below 2^16 (faces: block << 15),
+         * element ids fit 32 bits */
+        if (n_ > 65535 || (uint64_t)(2 * ncell_ + nface_) >= (1ULL << 32)) {
+            return fail("mesh too large for the ghost-fill compiler (at most 65535 blocks)");
+        }
         for (int b = 0; b < n_; ++b) {
             if (!active_block(b_[b])) continue;
             for (int s = 0; s < FX_NSLOTS; ++s) {
@@ -201,6 +236,25 @@ private:
 
     /* ---- recording -------------------------------------------------------- */
 
+    int prod_end(int x) const
+    {
+        return x + 1 < (int)seq_.size() ? seq_[x + 1].prod_begin : (int)prod_.size();
+    }
+
+    int w_end(int x) const
+    {
+        return x + 1 < (int)seq_.size() ? seq_[x + 1].w_begin : (int)wr_.size();
+    }
+
+    /* source element of a single-source operation (from its packed key) */
+    int64_t src_elem(const SeqOp &o) const
+    {
+        if (o.space == SPACE_CELL) {
+            return cell_elem(FX_CELL_BLOCK(o.op.src), FX_CELL_IDX(o.op.src));
+        }
+        return face_elem(o.op.src >> 15, o.op.aux & 3, o.op.src & 32767);
+    }
+
     bool is_plain_copy(const SeqOp &o) const
     {
         return (o.space == SPACE_CELL && o.op.type == FX_GOP_COPY) ||
@@ -213,10 +267,14 @@ private:
     {
         while (v >= 0) {
             const SeqOp &p = seq_[v];
-            if (!is_plain_copy(p) || ver_[p.src] != p.src_ver) {
+            if (!is_plain_copy(p)) {
                 break;
             }
-            e = p.src;
+            const int64_t ps = src_elem(p);
+            if (ver_[ps] != p.src_ver) {
+                break;
+            }
+            e = ps;
             v = p.src_ver;
             if (count) ++*count;
         }
@@ -238,16 +296,13 @@ private:
         resolve(src, v, &stats_.rewired);
         op.src = space == SPACE_CELL ? cell_key(src) : face_key(src);
         s.op = op;
-        s.src = src;
         s.src_ver = v;
         s.space = space;
         s.prod_begin = (int)prod_.size();
         prod_.push_back(v);
-        s.prod_end = (int)prod_.size();
-        rd_.push_back(src);
+        rd_.push_back((Elem)src);
         s.w_begin = (int)wr_.size();
-        wr_.push_back(w);
-        s.w_end = (int)wr_.size();
+        wr_.push_back((Elem)w);
         seq_.push_back(s);
         ver_[w] = (int)seq_.size() - 1;
     }
@@ -256,18 +311,15 @@ private:
     {
         SeqOp s;
         s.op = op;
-        s.src = -1;
         s.src_ver = -1;
         s.space = space;
         s.prod_begin = (int)prod_.size();
         for (int n = 0; n < nr; ++n) {
             prod_.push_back(ver_[reads[n]]);
-            rd_.push_back(reads[n]);
+            rd_.push_back((Elem)reads[n]);
         }
-        s.prod_end = (int)prod_.size();
         s.w_begin = (int)wr_.size();
-        wr_.push_back(w);
-        s.w_end = (int)wr_.size();
+        wr_.push_back((Elem)w);
         seq_.push_back(s);
         ver_[w] = (int)seq_.size() - 1;
     }
@@ -281,18 +333,17 @@ private:
         s.op.aux = 0;
         s.op.type = FX_FOP_PROLONG;
         groups_.push_back(p);
-        s.src = -1;
         s.src_ver = -1;
         s.space = SPACE_GROUP;
         s.prod_begin = (int)prod_.size();
         for (int64_t r : reads) {
             prod_.push_back(ver_[r]);
-            rd_.push_back(r);
+            rd_.push_back((Elem)r);
         }
-        s.prod_end = (int)prod_.size();
         s.w_begin = (int)wr_.size();
-        wr_.insert(wr_.end(), writes.begin(), writes.end());
-        s.w_end = (int)wr_.size();
+        for (int64_t w : writes) {
+            wr_.push_back((Elem)w);
+        }
         seq_.push_back(s);
         for (int64_t w : writes) {
             ver_[w] = (int)seq_.size() - 1;
@@ -443,7 +494,7 @@ private:
 
     /* ---- face field ------------------------------------------------------ */
 
-    int &fid(int b, int dir, int f) { return fid_[((int64_t)b * 3 + dir) * FX_NFACES + f]; }
+    int8_t &fid(int b, int dir, int f) { return fid_[((int64_t)b * 3 + dir) * FX_NFACES + f]; }
 
     /* prj_boundary_init_face_fidelity, src/prj_boundary.c:840-873 */
     void init_fidelity(int b)
@@ -463,7 +514,7 @@ private:
      * when its fidelity is at least the face's current fidelity. */
     bool lands(int db, int dir, int df, int fidelity)
     {
-        int &cur = fid(db, dir, df);
+        int8_t &cur = fid(db, dir, df);
         if (fidelity < cur) {
             return false;
         }
@@ -969,27 +1020,59 @@ private:
         const int nseq = (int)seq_.size();
         /* 2. liveness in reverse order: final versions are live; an op is
          * live when a live op reads its value */
-        std::vector<int> readers(nseq, 0);
+        /* live[x]: 1 once a live op reads op x's value */
         std::vector<char> live(nseq, 0);
         for (int x = nseq - 1; x >= 0; --x) {
             const SeqOp &o = seq_[x];
             if (seq_[x].space == SPACE_CELL) ++stats_.emitted_cell_ops;
             else ++stats_.emitted_face_ops;
-            live[x] = readers[x] > 0;
-            for (int q = o.w_begin; q < o.w_end && !live[x]; ++q) {
+            const int we = w_end(x);
+            for (int q = o.w_begin; q < we && !live[x]; ++q) {
                 live[x] = ver_[wr_[q]] == x;
             }
             if (!live[x]) {
                 ++stats_.dead;
                 continue;
             }
-            for (int p = o.prod_begin; p < o.prod_end; ++p) {
-                if (prod_[p] >= 0) ++readers[prod_[p]];
+            const int pe = prod_end(x);
+            for (int p = o.prod_begin; p < pe; ++p) {
+                if (prod_[p] >= 0) live[prod_[p]] = 1;
             }
         }
-        /* 3. cell-field operations */
-        std::vector<FxBop> bops;
-        std::vector<std::array<int64_t, 6>> bop_reads;
+        /* 3. levelling over cell, cell-field and face elements: latest wave
+         * that wrote / read each element (a fill has a handful of waves, far
+         * below the int16 range) */
+        std::vector<int16_t> lw((size_t)(2 * ncell_ + nface_), -1);
+        std::vector<int16_t> lr((size_t)(2 * ncell_ + nface_), -1);
+        int nwaves = 0;
+        auto place = [&](const Elem *reads, int nr, const Elem *writes, int nw) {
+            int wave = 0;
+            for (int n = 0; n < nr; ++n) wave = std::max(wave, lw[reads[n]] + 1);
+            for (int n = 0; n < nw; ++n) {
+                wave = std::max(wave, lw[writes[n]] + 1);
+                wave = std::max(wave, lr[writes[n]] + 1);
+            }
+            if (wave >= 32767) {
+                overflow_ = true;
+                wave = 32766;
+            }
+            for (int n = 0; n < nr; ++n) lr[reads[n]] = (int16_t)std::max<int>(lr[reads[n]], wave);
+            for (int n = 0; n < nw; ++n) lw[writes[n]] = (int16_t)wave;
+            nwaves = std::max(nwaves, wave + 1);
+            return wave;
+        };
+        std::vector<int16_t> opwave(nseq, -1);
+        for (int x = 0; x < nseq; ++x) {
+            if (!live[x]) continue;
+            const SeqOp &o = seq_[x];
+            const int nr = prod_end(x) - o.prod_begin;
+            opwave[x] = (int16_t)place(rd_.data() + o.prod_begin, nr, wr_.data() + o.w_begin, w_end(x) - o.w_begin);
+        }
+        std::vector<char>().swap(live);
+        /* 4. cell-field operations (bf2bc of every ghost cell and of interior
+         * cells with a rewritten face), reading the final faces through the
+         * copy chains, levelled after the operations they read */
+        std::vector<std::vector<FxBop>> wb;
         if (cfg_.mhd) {
             for (int b : plan.active) {
                 for (int i = -NG; i < BS + NG; ++i) {
@@ -1008,80 +1091,62 @@ private:
                             FxBop bo;
                             bo.dst = FX_CELL_KEY(b, lidx(i, j, k));
                             bo.pad = 0;
-                            std::array<int64_t, 6> rr;
+                            Elem rr[6];
                             for (int q = 0; q < 6; ++q) {
                                 int v = ver_[f[q]];
                                 int64_t e = f[q];
                                 resolve(e, v, &stats_.rewired);
                                 bo.f[q] = face_key(e);
-                                rr[q] = e;
+                                rr[q] = (Elem)e;
                             }
-                            bops.push_back(bo);
-                            bop_reads.push_back(rr);
+                            const Elem w = (Elem)cellb_elem(b, lidx(i, j, k));
+                            const int wave = place(rr, 6, &w, 1);
+                            if ((int)wb.size() <= wave) wb.resize(wave + 1);
+                            wb[wave].push_back(bo);
                         }
                     }
                 }
             }
         }
-        /* 4. levelling over cell, cell-field and face elements */
-        std::vector<int> lw((size_t)(2 * ncell_ + nface_), -1);
-        std::vector<int> lr((size_t)(2 * ncell_ + nface_), -1);
-        std::vector<std::vector<FxGop>> wc, wf;
-        std::vector<std::vector<FxPop>> wp;
-        std::vector<std::vector<FxBop>> wb;
-        auto place = [&](const int64_t *reads, int nr, const int64_t *writes, int nw) {
-            int wave = 0;
-            for (int n = 0; n < nr; ++n) wave = std::max(wave, lw[reads[n]] + 1);
-            for (int n = 0; n < nw; ++n) {
-                wave = std::max(wave, lw[writes[n]] + 1);
-                wave = std::max(wave, lr[writes[n]] + 1);
-            }
-            for (int n = 0; n < nr; ++n) lr[reads[n]] = std::max(lr[reads[n]], wave);
-            for (int n = 0; n < nw; ++n) lw[writes[n]] = wave;
-            if ((int)wc.size() <= wave) {
-                wc.resize(wave + 1);
-                wf.resize(wave + 1);
-                wp.resize(wave + 1);
-                wb.resize(wave + 1);
-            }
-            return wave;
-        };
-        for (int x = 0; x < nseq; ++x) {
-            if (!live[x]) continue;
-            const SeqOp &o = seq_[x];
-            const int nr = o.prod_end - o.prod_begin;
-            const int wave = place(&rd_[o.prod_begin], nr, &wr_[o.w_begin], o.w_end - o.w_begin);
-            if (o.space == SPACE_GROUP) {
-                wp[wave].push_back(groups_[o.op.dst]);
-            } else {
-                (o.space == SPACE_CELL ? wc : wf)[wave].push_back(o.op);
-            }
-        }
-        for (size_t q = 0; q < bops.size(); ++q) {
-            const int64_t w = cellb_elem(FX_CELL_BLOCK(bops[q].dst), FX_CELL_IDX(bops[q].dst));
-            const int wave = place(bop_reads[q].data(), 6, &w, 1);
-            wb[wave].push_back(bops[q]);
-        }
+        /* 5. per-wave arrays: operations of a wave sorted by type, then
+         * destination */
         FxProgram &g = plan.ghost;
+        std::vector<int> nc(nwaves + 1, 0), nf(nwaves + 1, 0), np(nwaves + 1, 0);
+        for (int x = 0; x < nseq; ++x) {
+            if (opwave[x] < 0) continue;
+            const int sp = seq_[x].space;
+            (sp == SPACE_CELL ? nc : sp == SPACE_FACE ? nf : np)[opwave[x] + 1] += 1;
+        }
+        for (int w = 0; w < nwaves; ++w) {
+            nc[w + 1] += nc[w];
+            nf[w + 1] += nf[w];
+            np[w + 1] += np[w];
+        }
+        g.cell_ops.resize(nc[nwaves]);
+        g.face_ops.resize(nf[nwaves]);
+        g.p_ops.resize(np[nwaves]);
+        g.cell_begin.assign(nc.begin(), nc.end());
+        g.face_begin.assign(nf.begin(), nf.end());
+        g.p_begin.assign(np.begin(), np.end());
+        for (int x = 0; x < nseq; ++x) {
+            if (opwave[x] < 0) continue;
+            const SeqOp &o = seq_[x];
+            if (o.space == SPACE_CELL) g.cell_ops[nc[opwave[x]]++] = o.op;
+            else if (o.space == SPACE_FACE) g.face_ops[nf[opwave[x]]++] = o.op;
+            else g.p_ops[np[opwave[x]]++] = groups_[o.op.dst];
+        }
         auto by_type = [](const FxGop &a, const FxGop &b) {
             return a.type < b.type || (a.type == b.type && a.dst < b.dst);
         };
-        for (size_t w = 0; w < wc.size(); ++w) {
-            std::stable_sort(wc[w].begin(), wc[w].end(), by_type);
-            std::stable_sort(wf[w].begin(), wf[w].end(), by_type);
-            g.cell_begin.push_back((int)g.cell_ops.size());
-            g.face_begin.push_back((int)g.face_ops.size());
-            g.p_begin.push_back((int)g.p_ops.size());
+        g.b_begin.assign(1, 0);
+        for (int w = 0; w < nwaves; ++w) {
+            std::stable_sort(g.cell_ops.begin() + g.cell_begin[w], g.cell_ops.begin() + g.cell_begin[w + 1], by_type);
+            std::stable_sort(g.face_ops.begin() + g.face_begin[w], g.face_ops.begin() + g.face_begin[w + 1], by_type);
+            if (w < (int)wb.size()) {
+                g.b_ops.insert(g.b_ops.end(), wb[w].begin(), wb[w].end());
+            }
             g.b_begin.push_back((int)g.b_ops.size());
-            g.cell_ops.insert(g.cell_ops.end(), wc[w].begin(), wc[w].end());
-            g.face_ops.insert(g.face_ops.end(), wf[w].begin(), wf[w].end());
-            g.p_ops.insert(g.p_ops.end(), wp[w].begin(), wp[w].end());
-            g.b_ops.insert(g.b_ops.end(), wb[w].begin(), wb[w].end());
         }
-        g.cell_begin.push_back((int)g.cell_ops.size());
-        g.face_begin.push_back((int)g.face_ops.size());
-        g.p_begin.push_back((int)g.p_ops.size());
-        g.b_begin.push_back((int)g.b_ops.size());
         plan.stats = stats_;
     }
 
@@ -1090,16 +1155,17 @@ private:
     const fx_block_desc *b_;
     int64_t ncell_;
     int64_t nface_;
-    std::vector<int> fid_;
+    std::vector<int8_t> fid_;
     std::vector<int> ver_;       /* element -> producer op (-1: initial value) */
     std::vector<SeqOp> seq_;
     std::vector<int> prod_;      /* producers of the values each op reads */
-    std::vector<int64_t> rd_;    /* elements each op reads (parallel to prod_) */
-    std::vector<int64_t> wr_;    /* elements each op writes */
+    std::vector<Elem> rd_;       /* elements each op reads (parallel to prod_) */
+    std::vector<Elem> wr_;       /* elements each op writes */
     std::vector<FxPop> groups_;  /* face-prolongation groups (SPACE_GROUP ops) */
     std::unordered_map<int64_t, ProlongSig> psig_;
     FxPlanStats stats_;
     std::string *err_ = nullptr;
+    bool overflow_ = false;
 };
 
 } /* namespace */
@@ -1110,4 +1176,12 @@ bool fx_build_plan(const fx_config &cfg, int nblocks, const fx_block_desc *block
     plan = FxPlan();
     Compiler c(cfg, nblocks, blocks);
     return c.run(plan, err);
+}
+
+bool fx_build_corrections(const fx_config &cfg, int nblocks, const fx_block_desc *blocks,
+    FxPlan &plan, std::string *err)
+{
+    plan = FxPlan();
+    Compiler c(cfg, nblocks, blocks);
+    return c.run_corrections(plan, err);
 }

@@ -50,4 +50,9 @@ struct FxPlan {
 bool fx_build_plan(const fx_config &cfg, int nblocks, const fx_block_desc *blocks,
     FxPlan &plan, std::string *err);
 
+/* Only the coarse/fine flux and EMF correction records of the plan (fast:
+ * no ghost-fill replay); the other members stay empty. */
+bool fx_build_corrections(const fx_config &cfg, int nblocks, const fx_block_desc *blocks,
+    FxPlan &plan, std::string *err);
+
 #endif

@@ -548,7 +548,9 @@ int fx_plan_export(const fx_config *cfg, int nblocks, const fx_block_desc *block
     }
     FxPlan plan;
     std::string perr;
-    if (!fx_build_plan(*cfg, nblocks, blocks, plan, &perr)) {
+    const bool corr_only = which == 2 || which == 3;
+    if (!(corr_only ? fx_build_corrections(*cfg, nblocks, blocks, plan, &perr) :
+                      fx_build_plan(*cfg, nblocks, blocks, plan, &perr))) {
         return FX_EINVAL;
     }
     const FxProgram &g = plan.ghost;
