@@ -9,6 +9,9 @@
  * Comments give the C association explicitly where it matters, e.g.
  * "a * b * c" is (a*b)*c.
  *
+ * The pointwise functions are host-callable too (FX_HD), so the adjoint's
+ * building blocks can be checked against finite differences on the host.
+ *
  * Failures the reference turns into exit(1) (non-positive density, invalid
  * wave ordering, ...) are reported through fx_fail(): the first failing
  * thread records a code and its position in the device error word and the
@@ -16,6 +19,8 @@
  */
 #ifndef FX_PHYSICS_CUH
 #define FX_PHYSICS_CUH
+
+#include <cmath>
 
 #include "fx_layout.h"
 
@@ -48,21 +53,30 @@ struct FxErr {
     int aux;
 };
 
-__device__ __forceinline__ void fx_fail(FxErr *err, int code, int block, int index)
+FX_HD void fx_fail(FxErr *err, int code, int block, int index)
 {
+#ifdef __CUDA_ARCH__
     if (err != nullptr && atomicCAS(&err->code, 0, code) == 0) {
         err->block = block;
         err->index = index;
     }
+#else
+    /* host evaluation (checks of the adjoint building blocks) */
+    if (err != nullptr && err->code == 0) {
+        err->code = code;
+        err->block = block;
+        err->index = index;
+    }
+#endif
 }
 
-__device__ __forceinline__ double fx_min(double a, double b) { return a < b ? a : b; }
-__device__ __forceinline__ double fx_max(double a, double b) { return a > b ? a : b; }
+FX_HD double fx_min(double a, double b) { return a < b ? a : b; }
+FX_HD double fx_max(double a, double b) { return a > b ? a : b; }
 
 /* ------------------------------------------------------------------------ */
 /* MC limited slope, src/prj_reconstruct.h:355-375 (branchless form).        */
 /* ------------------------------------------------------------------------ */
-__device__ __forceinline__ double fx_mc_slope(double qm, double q0, double qp)
+FX_HD double fx_mc_slope(double qm, double q0, double qp)
 {
     const double sl = q0 - qm;
     const double sr = qp - q0;
@@ -81,19 +95,19 @@ __device__ __forceinline__ double fx_mc_slope(double qm, double q0, double qp)
 /* Ideal gas (problems/prj_problem_ideal_eos.h:24-32 through the USER branch */
 /* of prj_eos_rey, src/prj_eos.c:772-788).                                   */
 /* ------------------------------------------------------------------------ */
-__device__ __forceinline__ double fx_pressure(double g, double rho, double eint)
+FX_HD double fx_pressure(double g, double rho, double eint)
 {
     return (g - 1.0) * rho * eint;            /* ((g-1)*rho)*eint */
 }
 
-__device__ __forceinline__ double fx_temperature(double g, double eint)
+FX_HD double fx_temperature(double g, double eint)
 {
     return (g - 1.0) * eint / FX_IDEAL_ENERGY_SCALE;
 }
 
 /* prj_eos_prim2cons, src/prj_eos.c:2112-2151 */
 template <bool MHD>
-__device__ __forceinline__ void fx_prim2cons(const double *w, double *u)
+FX_HD void fx_prim2cons(const double *w, double *u)
 {
     const double rho = w[FX_RHO];
     const double v1 = w[FX_V1];
@@ -122,7 +136,7 @@ __device__ __forceinline__ void fx_prim2cons(const double *w, double *u)
 
 /* prj_eos_cons2prim, src/prj_eos.c:2153-2220 (no floors) */
 template <bool MHD>
-__device__ __forceinline__ void fx_cons2prim(const double *u, double *w)
+FX_HD void fx_cons2prim(const double *u, double *w)
 {
     const double rho = u[FX_RHO];
     if (rho == 0.0) {
@@ -167,7 +181,7 @@ struct FxHlldStar {
 };
 
 /* prj_hlld_fill_conserved, src/prj_riemann.c:81-94 (component v) */
-__device__ __forceinline__ double fx_hlld_u(const FxHlldStar &s, int v)
+FX_HD double fx_hlld_u(const FxHlldStar &s, int v)
 {
     switch (v) {
     case 0: return s.rho;
@@ -182,7 +196,7 @@ __device__ __forceinline__ double fx_hlld_u(const FxHlldStar &s, int v)
     }
 }
 
-__device__ __forceinline__ double fx_hlld_state_u(const FxHlldState &s, int v)
+FX_HD double fx_hlld_state_u(const FxHlldState &s, int v)
 {
     switch (v) {
     case 0: return s.rho;
@@ -198,7 +212,7 @@ __device__ __forceinline__ double fx_hlld_state_u(const FxHlldState &s, int v)
 }
 
 /* prj_hlld_fill_flux, src/prj_riemann.c:96-115 (component v) */
-__device__ __forceinline__ double fx_hlld_state_f(const FxHlldState &s, int v)
+FX_HD double fx_hlld_state_f(const FxHlldState &s, int v)
 {
     const double b2 = s.bx * s.bx + s.by * s.by + s.bz * s.bz;
     const double pt = s.p + 0.5 * b2;
@@ -220,7 +234,7 @@ __device__ __forceinline__ double fx_hlld_state_f(const FxHlldState &s, int v)
 
 /* prj_hlld_state_from_prim, src/prj_riemann.c:142-178; w is the local
  * (direction-rotated) primitive vector, the normal field is bn. */
-__device__ __forceinline__ void fx_hlld_state(const double *w, double p, double gamma, double bn,
+FX_HD void fx_hlld_state(const double *w, double p, double gamma, double bn,
     FxHlldState &s, FxErr *err, int blk, int idx)
 {
     s.rho = w[FX_RHO];
@@ -243,7 +257,7 @@ __device__ __forceinline__ void fx_hlld_state(const double *w, double p, double 
 }
 
 /* prj_hlld_fast_speed, src/prj_riemann.c:117-140 */
-__device__ __forceinline__ double fx_hlld_fast_speed(const FxHlldState &s, FxErr *err, int blk, int idx)
+FX_HD double fx_hlld_fast_speed(const FxHlldState &s, FxErr *err, int blk, int idx)
 {
     const double a2 = s.gamma * s.p / s.rho;
     const double bx2_rho = s.bx * s.bx / s.rho;
@@ -263,7 +277,7 @@ __device__ __forceinline__ double fx_hlld_fast_speed(const FxHlldState &s, FxErr
 }
 
 /* prj_hlld_outer_star, src/prj_riemann.c:185-232 */
-__device__ __forceinline__ void fx_hlld_outer_star(const FxHlldState &s, double S, double SM,
+FX_HD void fx_hlld_outer_star(const FxHlldState &s, double S, double SM,
     double pt_star, FxHlldStar &st, FxErr *err, int blk, int idx)
 {
     const double alpha = S - s.vx;
@@ -298,7 +312,7 @@ __device__ __forceinline__ void fx_hlld_outer_star(const FxHlldState &s, double 
 }
 
 /* prj_hlld_double_star_one, src/prj_riemann.c:234-282 */
-__device__ __forceinline__ void fx_hlld_double_star(const FxHlldStar &left, const FxHlldStar &right,
+FX_HD void fx_hlld_double_star(const FxHlldStar &left, const FxHlldStar &right,
     double bx, bool right_side, FxHlldStar &ss, FxErr *err, int blk, int idx)
 {
     const double sqrt_l = sqrt(left.rho);
@@ -342,7 +356,7 @@ struct FxFaceOut {
     double bv2;
 };
 
-__device__ __forceinline__ void fx_face_outputs(double vx, double vy, double vz,
+FX_HD void fx_face_outputs(double vx, double vy, double vz,
     double bx, double by, double bz, FxFaceOut &o)
 {
     o.v[0] = vx;
@@ -456,7 +470,7 @@ static __device__ __noinline__ void fx_riemann_hlld(const double *WL, const doub
  * Selecting operands and choosing between x - t and x + t are exact, so the
  * result is bit-identical to fx_riemann_hlld; warps whose faces straddle
  * SM = 0 no longer execute both branches. */
-__device__ __forceinline__ void fx_riemann_hlld_folded(const double *WL, const double *WR,
+FX_HD void fx_riemann_hlld_folded(const double *WL, const double *WR,
     double pL, double pR, double gL, double gR, double bn, FxFaceOut &o,
     FxErr *err, int blk, int idx)
 {
@@ -556,7 +570,7 @@ __device__ __forceinline__ void fx_riemann_hlld_folded(const double *WL, const d
 /* HLLC for the hydro build, src/prj_riemann.c:1433-1599 and the theta       */
 /* pressure-jump limiter of src/prj_riemann.c:8-17.                          */
 /* ------------------------------------------------------------------------ */
-__device__ __forceinline__ double fx_theta_limiter(double cfmax, double du, double dv, double dw)
+FX_HD double fx_theta_limiter(double cfmax, double du, double dv, double dw)
 {
     double theta_r = (-fx_min(du, 0.0) + cfmax) / (-fx_min(fx_min(dv, dw), 0.0) + cfmax);
     theta_r *= theta_r;
@@ -564,7 +578,7 @@ __device__ __forceinline__ double fx_theta_limiter(double cfmax, double du, doub
 }
 
 /* prj_riemann_state, src/prj_riemann.c:1433-1492 (hydro: 6 components) */
-__device__ __forceinline__ void fx_hllc_state(const double *W, double p, double gamma,
+FX_HD void fx_hllc_state(const double *W, double p, double gamma,
     double *U, double *F, double &cs)
 {
     const double rho = W[FX_RHO];
@@ -655,7 +669,7 @@ static __device__ __noinline__ void fx_riemann_hllc(const double *WL, const doub
 /* ------------------------------------------------------------------------ */
 /* Upwind corner EMF, src/prj_mhd.c:627-718 (eta term separate).            */
 /* ------------------------------------------------------------------------ */
-__device__ __forceinline__ double fx_emf_upwind(const double f[4], const double c[4], const double vn[4])
+FX_HD double fx_emf_upwind(const double f[4], const double c[4], const double vn[4])
 {
     double emf = 0.25 * (f[0] + f[1] + f[2] + f[3]);
     if (vn[0] > 0.0) {
@@ -694,7 +708,7 @@ __device__ __forceinline__ double fx_emf_upwind(const double f[4], const double 
 #define FX_ETA_RHO_FLOOR 1.0e13
 #define FX_ETA_YE_THR 0.25
 
-__device__ __forceinline__ double fx_cell_eta(double rho, double ye)
+FX_HD double fx_cell_eta(double rho, double ye)
 {
     /* max(0, log(x)) is exactly +0 for x <= 1 (log(1) = +0, log(x < 1) < 0),
      * and 1e12 * 0 * f = +0 for any finite f >= 0: the logarithms are only

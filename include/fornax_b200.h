@@ -263,6 +263,22 @@ int fx_autotune(fx_ctx *ctx, double *times_ms, int n, int *choice);
  * (bf2bc) operations */
 int fx_info(fx_ctx *ctx, int what, long long *value);
 
+/* ---- adjoint building blocks (host) ----------------------------------------- */
+
+/* Host evaluation of one face of the face-flux kernel, for checks of the
+ * discrete adjoint (no counterpart in the reference): w4[n * 9 + v] are the
+ * local-frame primitives of the four stencil cells n = 0..3 along the sweep
+ * (v = 0 rho, 1 normal velocity, 2-3 transverse velocities, 4 eint, 5 ye,
+ * 7-8 transverse field; 6 unused), bn the face-normal field.  MC
+ * reconstruction of every variable and of the cell pressures, then HLLD
+ * (prj_riemann_hlld, src/prj_riemann.c:321-440).  out[14] = local flux[9],
+ * face velocity[3], Bv1, Bv2. */
+int fx_face_eval_host(const double *w4, double bn, double gamma, double *out);
+/* Its vector-Jacobian product: w4_bar[36] and *bn_bar = out_bar^T d out /
+ * d (w4, bn), on the smooth piece the evaluation lies on. */
+int fx_face_vjp_host(const double *w4, double bn, double gamma, const double *out_bar,
+    double *w4_bar, double *bn_bar);
+
 #ifdef __cplusplus
 }
 #endif
