@@ -16,7 +16,8 @@ import numpy as np
 from . import _lib
 from ._lib import (ARR_BF, ARR_BV1, ARR_BV2, ARR_EMF, ARR_EOSVAR, ARR_FLUX, ARR_GRAV, ARR_RHS,
                    ARR_VRIEMANN, ARR_W, BC_OUTFLOW, BC_PERIODIC, BC_REFLECT, BC_USER, FORM_BATCHED,
-                   FORM_PLAIN, FxBlockDesc, FxConfig)
+                   FORM_PLAIN, PHASE_CELLS, PHASE_CT, PHASE_EMF, PHASE_FLUX, PHASE_GHOST, PHASE_STEP,
+                   FxBlockDesc, FxConfig)
 
 __all__ = ["Context", "FxError", "FORM_PLAIN", "FORM_BATCHED", "NCELLS", "NFACES", "NEDGES",
            "library", "plan_export"]
@@ -242,4 +243,31 @@ class Context:
     def info(self, what: int) -> int:
         v = C.c_longlong(0)
         self._check(self.L.fx_info(self._h, what, C.byref(v)))
+        return v.value
+
+    # ---- discrete adjoint ------------------------------------------------------
+    def adjoint_forward(self, nsteps: int, dt: float) -> None:
+        """nsteps batched RK2 steps with fixed dt, storing every stage."""
+        self._check(self.L.fx_adjoint_forward(self._h, nsteps, dt))
+
+    def adjoint_backward(self, W_bar: np.ndarray, Bf_bar: Optional[np.ndarray] = None,
+                         initial_fill: bool = False):
+        """(W_bar_out, Bf_bar_out) = d J / d (state at adjoint_forward's
+        entry) from d J / d (final state); layouts of upload_all."""
+        W_bar = np.ascontiguousarray(W_bar, dtype=np.float64)
+        Wo = np.empty_like(W_bar)
+        nb = W_bar.size // (self.nv * NSTAGES * NCELLS)
+        Bo = np.empty(nb * 3 * NSTAGES * NFACES)
+        bp = None
+        if Bf_bar is not None:
+            Bf_bar = np.ascontiguousarray(Bf_bar, dtype=np.float64)
+            bp = _dp(Bf_bar)
+        self._check(self.L.fx_adjoint_backward(self._h, _dp(W_bar), bp, _dp(Wo), _dp(Bo),
+                                               1 if initial_fill else 0))
+        return Wo, Bo
+
+    def adjoint_ms(self) -> float:
+        """Device time of the last reverse sweep (ms)."""
+        v = C.c_double(0.0)
+        self._check(self.L.fx_adjoint_time(self._h, C.byref(v)))
         return v.value

@@ -164,32 +164,69 @@ FX_HD void fxa_flux_vjp(const FxHlldState &s, const double *Fb, FxaS &sb)
     sb.ye += Fb[5] * rho * vx;
 }
 
-/* fx_hlld_state_u, all nine components */
-FX_HD void fxa_u_vjp(const FxHlldState &s, const double *ub, FxaS &sb)
+/* one component of fx_hlld_state_f: sb += w * d f_v / d s */
+FX_HD void fxa_flux_vjp_comp(const FxHlldState &s, int v, double w, FxaS &sb)
 {
-    sb.rho += ub[0] + ub[1] * s.vx + ub[2] * s.vy + ub[3] * s.vz + ub[5] * s.ye;
-    sb.vx += ub[1] * s.rho;
-    sb.vy += ub[2] * s.rho;
-    sb.vz += ub[3] * s.rho;
-    sb.e += ub[4];
-    sb.ye += ub[5] * s.rho;
-    sb.bx += ub[6];
-    sb.by += ub[7];
-    sb.bz += ub[8];
+    double Fb[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    Fb[v] = w;
+    fxa_flux_vjp(s, Fb, sb);
 }
 
-/* fx_hlld_u of a star state, all nine components */
-FX_HD void fxa_ustar_vjp(const FxHlldStar &s, const double *ub, FxaSt &sb)
+/* fx_hlld_state_u: sb += (du/ds)^T (scale * Fb) */
+FX_HD void fxa_u_vjp(const FxHlldState &s, const double *Fb, double scale, FxaS &sb)
 {
-    sb.rho += ub[0] + ub[1] * s.vx + ub[2] * s.vy + ub[3] * s.vz + ub[5] * s.ye;
-    sb.vx += ub[1] * s.rho;
-    sb.vy += ub[2] * s.rho;
-    sb.vz += ub[3] * s.rho;
-    sb.e += ub[4];
-    sb.ye += ub[5] * s.rho;
-    sb.bx += ub[6];
-    sb.by += ub[7];
-    sb.bz += ub[8];
+    sb.rho += scale * (Fb[0] + Fb[1] * s.vx + Fb[2] * s.vy + Fb[3] * s.vz + Fb[5] * s.ye);
+    sb.vx += scale * Fb[1] * s.rho;
+    sb.vy += scale * Fb[2] * s.rho;
+    sb.vz += scale * Fb[3] * s.rho;
+    sb.e += scale * Fb[4];
+    sb.ye += scale * Fb[5] * s.rho;
+    sb.bx += scale * Fb[6];
+    sb.by += scale * Fb[7];
+    sb.bz += scale * Fb[8];
+}
+
+/* one component of fx_hlld_state_u: sb += w * d u_v / d s */
+FX_HD void fxa_u_vjp_comp(const FxHlldState &s, int v, double w, FxaS &sb)
+{
+    switch (v) {
+    case 0: sb.rho += w; break;
+    case 1: sb.rho += w * s.vx; sb.vx += w * s.rho; break;
+    case 2: sb.rho += w * s.vy; sb.vy += w * s.rho; break;
+    case 3: sb.rho += w * s.vz; sb.vz += w * s.rho; break;
+    case 4: sb.e += w; break;
+    case 5: sb.rho += w * s.ye; sb.ye += w * s.rho; break;
+    case 6: sb.bx += w; break;
+    case 7: sb.by += w; break;
+    default: sb.bz += w; break;
+    }
+}
+
+/* fx_hlld_u of a star state: sb += (du/ds)^T (scale * Fb) */
+FX_HD void fxa_ustar_vjp(const FxHlldStar &s, const double *Fb, double scale, FxaSt &sb)
+{
+    sb.rho += scale * (Fb[0] + Fb[1] * s.vx + Fb[2] * s.vy + Fb[3] * s.vz + Fb[5] * s.ye);
+    sb.vx += scale * Fb[1] * s.rho;
+    sb.vy += scale * Fb[2] * s.rho;
+    sb.vz += scale * Fb[3] * s.rho;
+    sb.e += scale * Fb[4];
+    sb.ye += scale * Fb[5] * s.rho;
+    sb.bx += scale * Fb[6];
+    sb.by += scale * Fb[7];
+    sb.bz += scale * Fb[8];
+}
+
+/* sum_v Fb[v] u_v for a state and a star state */
+FX_HD double fxa_u_dot(const FxHlldState &s, const double *Fb)
+{
+    return Fb[0] * s.rho + Fb[1] * s.rho * s.vx + Fb[2] * s.rho * s.vy + Fb[3] * s.rho * s.vz + Fb[4] * s.e +
+        Fb[5] * s.rho * s.ye + Fb[6] * s.bx + Fb[7] * s.by + Fb[8] * s.bz;
+}
+
+FX_HD double fxa_ustar_dot(const FxHlldStar &s, const double *Fb)
+{
+    return Fb[0] * s.rho + Fb[1] * s.rho * s.vx + Fb[2] * s.rho * s.vy + Fb[3] * s.rho * s.vz + Fb[4] * s.e +
+        Fb[5] * s.rho * s.ye + Fb[6] * s.bx + Fb[7] * s.by + Fb[8] * s.bz;
 }
 
 /* fx_face_outputs: v = (vx, vy, vz), bv1 = bz vx - bx vz, bv2 = bx vy - by vx.
@@ -345,15 +382,13 @@ FX_HD void fxa_hlld_vjp(const double *WL, const double *WR, double pL, double pR
         const double pts = 0.5 * (ptl + ptr);
         double SMb = 0.0, ptsb = 0.0;
         if (pts <= 0.0 || !isfinite(pts)) {
-            /* HLL fallback */
+            /* HLL fallback: Uh_v = (SR ru - SL lu + lf - rf) / (SR - SL),
+             * F_v = (SR lf - SL rf + SL SR (ru - lu)) / (SR - SL) */
             const double inv = 1.0 / (SR - SL);
-            double lf[9], rf[9], lu[9], ru[9], Uh[9];
+            double Uh[9];
             for (int v = 0; v < 9; ++v) {
-                lf[v] = fx_hlld_state_f(L, v);
-                rf[v] = fx_hlld_state_f(R, v);
-                lu[v] = fx_hlld_state_u(L, v);
-                ru[v] = fx_hlld_state_u(R, v);
-                Uh[v] = (SR * ru[v] - SL * lu[v] + lf[v] - rf[v]) * inv;
+                Uh[v] = (SR * fx_hlld_state_u(R, v) - SL * fx_hlld_state_u(L, v) + fx_hlld_state_f(L, v) -
+                    fx_hlld_state_f(R, v)) * inv;
             }
             const double rho = Uh[0];
             const double vx = Uh[1] / rho, vy = Uh[2] / rho, vz = Uh[3] / rho;
@@ -367,25 +402,22 @@ FX_HD void fxa_hlld_vjp(const double *WL, const double *WR, double pL, double pR
             Uhb[6] += xb[3];
             Uhb[7] += xb[4];
             Uhb[8] += xb[5];
-            double lfb[9], rfb[9], lub[9], rub[9];
             double invb = 0.0;
             for (int v = 0; v < 9; ++v) {
+                const double lf = fx_hlld_state_f(L, v), rf = fx_hlld_state_f(R, v);
+                const double lu = fx_hlld_state_u(L, v), ru = fx_hlld_state_u(R, v);
                 const double fb = Fb[v];
-                const double du = ru[v] - lu[v];
-                lfb[v] = fb * SR * inv + Uhb[v] * inv;
-                rfb[v] = -fb * SL * inv - Uhb[v] * inv;
-                rub[v] = fb * SL * SR * inv + Uhb[v] * SR * inv;
-                lub[v] = -fb * SL * SR * inv - Uhb[v] * SL * inv;
-                SRb += fb * (lf[v] + SL * du) * inv + Uhb[v] * ru[v] * inv;
-                SLb += fb * (-rf[v] + SR * du) * inv - Uhb[v] * lu[v] * inv;
-                invb += fb * (SR * lf[v] - SL * rf[v] + SL * SR * du) + Uhb[v] * (SR * ru[v] - SL * lu[v] + lf[v] - rf[v]);
+                const double du = ru - lu;
+                SRb += fb * (lf + SL * du) * inv + Uhb[v] * ru * inv;
+                SLb += fb * (-rf + SR * du) * inv - Uhb[v] * lu * inv;
+                invb += fb * (SR * lf - SL * rf + SL * SR * du) + Uhb[v] * (SR * ru - SL * lu + lf - rf);
+                fxa_flux_vjp_comp(L, v, fb * SR * inv + Uhb[v] * inv, Lb);
+                fxa_flux_vjp_comp(R, v, -fb * SL * inv - Uhb[v] * inv, Rb);
+                fxa_u_vjp_comp(R, v, fb * SL * SR * inv + Uhb[v] * SR * inv, Rb);
+                fxa_u_vjp_comp(L, v, -fb * SL * SR * inv - Uhb[v] * SL * inv, Lb);
             }
             SRb -= invb * inv * inv;
             SLb += invb * inv * inv;
-            fxa_flux_vjp(L, lfb, Lb);
-            fxa_flux_vjp(R, rfb, Rb);
-            fxa_u_vjp(L, lub, Lb);
-            fxa_u_vjp(R, rub, Rb);
         } else {
             const bool bn_small = (0.5 * bn * bn < FX_HLLD_SMALL * pts);
             const bool left = (0.0 <= SM);
@@ -401,23 +433,14 @@ FX_HD void fxa_hlld_vjp(const double *WL, const double *WR, double pL, double pR
             const bool single = (left ? (0.0 <= SNs) : (SNs <= 0.0)) || bn_small;
             FxaSt Nsb;
             fxa_clear(Nsb);
-            double uN[9], uNs[9];
-            for (int v = 0; v < 9; ++v) {
-                uN[v] = fx_hlld_state_u(N, v);
-                uNs[v] = fx_hlld_u(Ns, v);
-            }
-            double fNb[9], uNb[9], uNsb[9];
+            const double dN = fxa_u_dot(N, Fb);
+            const double dNs = fxa_ustar_dot(Ns, Fb);
             if (single) {
                 /* F = f(N) + SN (u(Ns) - u(N)) */
-                for (int v = 0; v < 9; ++v) {
-                    fNb[v] = Fb[v];
-                    SNb += Fb[v] * (uNs[v] - uN[v]);
-                    uNsb[v] = SN * Fb[v];
-                    uNb[v] = -SN * Fb[v];
-                }
+                SNb += dNs - dN;
                 fxa_outputs_vjp(Ns.vx, Ns.vy, Ns.vz, Ns.bx, Ns.by, Ns.bz, outb, xb);
                 Nsb.vx += xb[0]; Nsb.vy += xb[1]; Nsb.vz += xb[2]; Nsb.bx += xb[3]; Nsb.by += xb[4]; Nsb.bz += xb[5];
-                fxa_ustar_vjp(Ns, uNsb, Nsb);
+                fxa_ustar_vjp(Ns, Fb, SN, Nsb);
             } else {
                 const FxHlldState &Fr = left ? R : L;
                 FxaS &Frb = left ? Rb : Lb;
@@ -445,27 +468,16 @@ FX_HD void fxa_hlld_vjp(const double *WL, const double *WR, double pL, double pR
                 const double sqn = left ? sql : sqr;
                 const double t = sqn * sgn * (vbn - vbss);
                 ss.e = left ? Ns.e - t : Ns.e + t;
-                double uss[9];
-                for (int v = 0; v < 9; ++v) {
-                    uss[v] = fx_hlld_u(ss, v);
-                }
                 /* F = f(N) + SN (u(Ns) - u(N)) + SNs (u(ss) - u(Ns)) */
-                double ussb[9];
-                double SNsb = 0.0;
-                for (int v = 0; v < 9; ++v) {
-                    fNb[v] = Fb[v];
-                    SNb += Fb[v] * (uNs[v] - uN[v]);
-                    uNsb[v] = SN * Fb[v] - SNs * Fb[v];
-                    uNb[v] = -SN * Fb[v];
-                    SNsb += Fb[v] * (uss[v] - uNs[v]);
-                    ussb[v] = SNs * Fb[v];
-                }
+                const double dss = fxa_ustar_dot(ss, Fb);
+                SNb += dNs - dN;
+                const double SNsb = dss - dNs;
                 FxaSt ssb;
                 fxa_clear(ssb);
                 fxa_outputs_vjp(ss.vx, ss.vy, ss.vz, ss.bx, ss.by, ss.bz, outb, xb);
                 ssb.vx += xb[0]; ssb.vy += xb[1]; ssb.vz += xb[2]; ssb.bx += xb[3]; ssb.by += xb[4]; ssb.bz += xb[5];
-                fxa_ustar_vjp(ss, ussb, ssb);
-                fxa_ustar_vjp(Ns, uNsb, Nsb);
+                fxa_ustar_vjp(ss, Fb, SNs, ssb);
+                fxa_ustar_vjp(Ns, Fb, SN - SNs, Nsb);
                 /* SNs = SM -/+ a, a = |bn| / sqrt(Ns.rho) */
                 SMb += SNsb;
                 const double ab = left ? -SNsb : SNsb;
@@ -554,8 +566,8 @@ FX_HD void fxa_hlld_vjp(const double *WL, const double *WR, double pL, double pR
                     SLb += SFb;
                 }
             }
-            fxa_flux_vjp(N, fNb, Nb);
-            fxa_u_vjp(N, uNb, Nb);
+            fxa_flux_vjp(N, Fb, Nb);
+            fxa_u_vjp(N, Fb, -SN, Nb);
             fxa_outer_star_vjp(N, SN, SM, pts, Nsb, Nb, SNb, SMb, ptsb);
             if (left) {
                 SLb += SNb;
@@ -621,41 +633,48 @@ FX_HD void fxa_hlld_vjp(const double *WL, const double *WR, double pL, double pR
 /* One face: MC reconstruction of the 4-cell stencil + HLLD                  */
 /* ------------------------------------------------------------------------ */
 
-/* w4[n * 9 + lv]: local-frame primitives of the stencil cells n = 0..3
- * (L-1, L, R, R+1); lv = 0 rho, 1-3 velocity (normal first), 4 eint, 5 ye,
- * 7-8 transverse field (6 unused).  Pressures are the cells' (g-1) rho eint,
- * reconstructed like the other variables (the k_flux evaluation). */
-FX_HD void fxa_face_states(const double *w4, double g, double bn, double *WL, double *WR, double &pL, double &pR)
+#ifdef __CUDACC__
+#define FXA_MEMBER __host__ __device__ __forceinline__
+#else
+#define FXA_MEMBER inline
+#endif
+
+/* The stencil of one face: cells n = 0..3 (L-1, L, R, R+1) along the sweep,
+ * local-frame primitives lv = 0 rho, 1-3 velocity (normal first), 4 eint,
+ * 5 ye, 7-8 transverse field (6 unused).  LD(n, lv) loads a value,
+ * ACC(n, lv, x) accumulates an adjoint; the kernel reads and atomically
+ * updates the block arrays, the host check uses plain arrays.  Pressures
+ * are the cells' (g-1) rho eint, reconstructed like the other variables
+ * (the k_flux evaluation). */
+template <class LD>
+FX_HD void fxa_face_states_t(const LD &ld, double g, double bn, double *WL, double *WR, double &pL, double &pR)
 {
     const int lvs[8] = {0, 1, 2, 3, 4, 5, 7, 8};
+#pragma unroll
     for (int q = 0; q < 8; ++q) {
         const int lv = lvs[q];
-        const double a = w4[0 * 9 + lv], b = w4[1 * 9 + lv], c = w4[2 * 9 + lv], d = w4[3 * 9 + lv];
+        const double a = ld(0, lv), b = ld(1, lv), c = ld(2, lv), d = ld(3, lv);
         WL[lv] = b + 0.5 * fx_mc_slope(a, b, c);
         WR[lv] = c - 0.5 * fx_mc_slope(b, c, d);
     }
     WL[FX_B1] = bn;
     WR[FX_B1] = bn;
     double p4[4];
+#pragma unroll
     for (int n = 0; n < 4; ++n) {
-        p4[n] = fx_pressure(g, w4[n * 9 + FX_RHO], w4[n * 9 + FX_EINT]);
+        p4[n] = fx_pressure(g, ld(n, FX_RHO), ld(n, FX_EINT));
     }
     pL = p4[1] + 0.5 * fx_mc_slope(p4[0], p4[1], p4[2]);
     pR = p4[2] - 0.5 * fx_mc_slope(p4[1], p4[2], p4[3]);
 }
 
-FX_HD void fxa_face_eval(const double *w4, double g, double bn, FxFaceOut &o)
+/* ob[14]: adjoints of F[9], v[3], bv1, bv2; accumulates the stencil
+ * adjoints through acc and the face-normal field's into bnb */
+template <class LD, class ACC>
+FX_HD void fxa_face_vjp_t(const LD &ld, const ACC &acc, double g, double bn, const double *ob, double &bnb)
 {
     double WL[9], WR[9], pL, pR;
-    fxa_face_states(w4, g, bn, WL, WR, pL, pR);
-    fx_riemann_hlld_folded(WL, WR, pL, pR, g, g, bn, o, nullptr, 0, 0);
-}
-
-/* ob[14]: adjoints of F[9], v[3], bv1, bv2; accumulates w4b[36], bnb */
-FX_HD void fxa_face_vjp(const double *w4, double g, double bn, const double *ob, double *w4b, double &bnb)
-{
-    double WL[9], WR[9], pL, pR;
-    fxa_face_states(w4, g, bn, WL, WR, pL, pR);
+    fxa_face_states_t(ld, g, bn, WL, WR, pL, pR);
     double WLb[9], WRb[9];
     for (int v = 0; v < 9; ++v) {
         WLb[v] = 0.0;
@@ -663,29 +682,57 @@ FX_HD void fxa_face_vjp(const double *w4, double g, double bn, const double *ob,
     }
     double pLb = 0.0, pRb = 0.0;
     fxa_hlld_vjp(WL, WR, pL, pR, g, bn, ob, WLb, WRb, pLb, pRb, bnb);
-    bnb += WLb[FX_B1] + WRb[FX_B1];
     const int lvs[8] = {0, 1, 2, 3, 4, 5, 7, 8};
+#pragma unroll
     for (int q = 0; q < 8; ++q) {
         const int lv = lvs[q];
-        const double a = w4[0 * 9 + lv], b = w4[1 * 9 + lv], c = w4[2 * 9 + lv], d = w4[3 * 9 + lv];
+        const double a = ld(0, lv), b = ld(1, lv), c = ld(2, lv), d = ld(3, lv);
         /* WL = b + 0.5 mc(a, b, c); WR = c - 0.5 mc(b, c, d) */
-        w4b[1 * 9 + lv] += WLb[lv];
-        fxa_mc_vjp(a, b, c, 0.5 * WLb[lv], w4b[0 * 9 + lv], w4b[1 * 9 + lv], w4b[2 * 9 + lv]);
-        w4b[2 * 9 + lv] += WRb[lv];
-        fxa_mc_vjp(b, c, d, -0.5 * WRb[lv], w4b[1 * 9 + lv], w4b[2 * 9 + lv], w4b[3 * 9 + lv]);
+        double ab = 0.0, bb = WLb[lv], cb = WRb[lv], db = 0.0;
+        fxa_mc_vjp(a, b, c, 0.5 * WLb[lv], ab, bb, cb);
+        fxa_mc_vjp(b, c, d, -0.5 * WRb[lv], bb, cb, db);
+        acc(0, lv, ab);
+        acc(1, lv, bb);
+        acc(2, lv, cb);
+        acc(3, lv, db);
     }
-    double p4[4], p4b[4] = {0.0, 0.0, 0.0, 0.0};
+    double rho4[4], e4[4], p4[4], p4b[4] = {0.0, 0.0, 0.0, 0.0};
     for (int n = 0; n < 4; ++n) {
-        p4[n] = fx_pressure(g, w4[n * 9 + FX_RHO], w4[n * 9 + FX_EINT]);
+        rho4[n] = ld(n, FX_RHO);
+        e4[n] = ld(n, FX_EINT);
+        p4[n] = fx_pressure(g, rho4[n], e4[n]);
     }
     p4b[1] += pLb;
     fxa_mc_vjp(p4[0], p4[1], p4[2], 0.5 * pLb, p4b[0], p4b[1], p4b[2]);
     p4b[2] += pRb;
     fxa_mc_vjp(p4[1], p4[2], p4[3], -0.5 * pRb, p4b[1], p4b[2], p4b[3]);
     for (int n = 0; n < 4; ++n) {
-        w4b[n * 9 + FX_RHO] += p4b[n] * (g - 1.0) * w4[n * 9 + FX_EINT];
-        w4b[n * 9 + FX_EINT] += p4b[n] * (g - 1.0) * w4[n * 9 + FX_RHO];
+        acc(n, FX_RHO, p4b[n] * (g - 1.0) * e4[n]);
+        acc(n, FX_EINT, p4b[n] * (g - 1.0) * rho4[n]);
     }
+}
+
+struct FxaArrayLoad {
+    const double *w;
+    FXA_MEMBER double operator()(int n, int lv) const { return w[n * 9 + lv]; }
+};
+
+struct FxaArrayAcc {
+    double *wb;
+    FXA_MEMBER void operator()(int n, int lv, double x) const { wb[n * 9 + lv] += x; }
+};
+
+/* array forms (w4[n * 9 + lv]) used by the host checks */
+FX_HD void fxa_face_eval(const double *w4, double g, double bn, FxFaceOut &o)
+{
+    double WL[9], WR[9], pL, pR;
+    fxa_face_states_t(FxaArrayLoad{w4}, g, bn, WL, WR, pL, pR);
+    fx_riemann_hlld_folded(WL, WR, pL, pR, g, g, bn, o, nullptr, 0, 0);
+}
+
+FX_HD void fxa_face_vjp(const double *w4, double g, double bn, const double *ob, double *w4b, double &bnb)
+{
+    fxa_face_vjp_t(FxaArrayLoad{w4}, FxaArrayAcc{w4b}, g, bn, ob, bnb);
 }
 
 /* ------------------------------------------------------------------------ */

@@ -168,4 +168,59 @@ static inline double fx_key_to_double(unsigned long long key)
     return d;
 }
 
+
+/* ---- discrete adjoint (fx_adjoint.cu) ------------------------------------ */
+
+/* device view of one reverse stage: the stored states before and after the
+ * stage (stacked per-block W and Bf arrays, both slots) and the adjoint
+ * arrays (same layouts; G holds, per cell, the dt-scaled adjoints of the
+ * six updated conserved variables and the adjoints of the three updated
+ * cell-field components, [b][v][cell]) */
+struct FxAdjDev {
+    const FxBlockDev *blk;
+    double gamma;
+    double dt;
+    const double *Wbef;
+    const double *Bfbef;
+    const double *Waft;
+    double *Wb;
+    double *Bfb;
+    double *G;
+    double *bvb1;
+    double *bvb2;
+    double *Eb;
+    const double *vr; /* face velocities recomputed from Wbef (normal component) */
+};
+
+#define FX_ADJ_G_COUNT (9 * FX_NCELLS)
+
+/* A ghost-fill wave transposed into gathers (its adjoint): for every element the wave reads,
+ * the list of operations reading it.  Cell sources: entries (dst cell key,
+ * kind) with kind 0 copy, 1 + v copy with variable v negated, 16 copy with
+ * v1 replaced (no sensitivity to v1).  Face sources: entries (key, kind)
+ * with kind 0 = face copy to face key dst (direction in the source's
+ * aux), 1 + d = half of cell key's field component d. */
+struct FxAdjEnt {
+    int32_t key;
+    int32_t kind;
+};
+
+struct FxAdjSrc {
+    int32_t key;   /* cell key, or face key */
+    int32_t dir;   /* faces: direction */
+    int32_t begin; /* entries [begin, end) */
+    int32_t end;
+};
+
+void fx_launch_adj_gather(const FxAdjDev &A, const FxAdjSrc *csrc, int nc, const FxAdjSrc *fsrc, int nf,
+    const FxAdjEnt *ents, int slot, cudaStream_t s);
+/* zero the wave's destinations: cell ops (variables 0-5), face ops, and the
+ * field components of cell-field ops */
+void fx_launch_adj_zero(const FxAdjDev &A, const FxGop *cops, int nc, const FxGop *fops, int nf,
+    const FxBop *bops, int nb, int slot, cudaStream_t s);
+void fx_launch_adj_cells(const FxAdjDev &A, const int *blist, int nlist, int stage, cudaStream_t s);
+void fx_launch_adj_bf(const FxAdjDev &A, const int *blist, int nlist, int stage, cudaStream_t s);
+void fx_launch_adj_emf(const FxAdjDev &A, const int *blist, int nlist, int stage, cudaStream_t s);
+void fx_launch_adj_flux(const FxAdjDev &A, const int *blist, int nlist, int stage, cudaStream_t s);
+
 #endif

@@ -19,6 +19,7 @@
 #include <cstdio>
 #include <cstring>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "../../include/fornax_b200.h"
@@ -61,6 +62,20 @@ struct fx_ctx {
     cudaGraphExec_t g_step = nullptr; /* batched RK2 step, dt from the control block */
     cudaGraphExec_t g_run = nullptr;  /* batched driver step (calc_dt + step + dt update) */
     int last_slot = 0;                /* W slot written by the last stage */
+
+    /* discrete adjoint: states after every stage of the last
+     * fx_adjoint_forward and the adjoint arrays */
+    int adj_nsteps = 0;
+    double adj_dt = 0.0;
+    double *d_ckW = nullptr, *d_ckBf = nullptr, *d_ckVr = nullptr;
+    double *d_Wb = nullptr, *d_Bfb = nullptr, *d_G = nullptr;
+    double *d_bvb1 = nullptr, *d_bvb2 = nullptr, *d_Eb = nullptr;
+    double adj_ms = 0.0;              /* device time of the last reverse sweep */
+    /* transposed ghost waves for the adjoint (built on first use) */
+    bool adj_ghost_ready = false;
+    std::vector<int> adj_cbeg, adj_fbeg;
+    FxAdjSrc *d_adj_csrc = nullptr, *d_adj_fsrc = nullptr;
+    FxAdjEnt *d_adj_ents = nullptr;
 };
 
 namespace {
@@ -191,6 +206,25 @@ void free_mesh(fx_ctx *c)
     c->d_ids = c->d_active = nullptr;
     c->d_cops = c->d_fops = nullptr;
     c->d_fcorr = c->d_ecorr = nullptr;
+    cudaFree(c->d_ckW);
+    cudaFree(c->d_ckBf);
+    cudaFree(c->d_ckVr);
+    c->d_ckVr = nullptr;
+    cudaFree(c->d_adj_csrc);
+    cudaFree(c->d_adj_fsrc);
+    cudaFree(c->d_adj_ents);
+    c->d_adj_csrc = c->d_adj_fsrc = nullptr;
+    c->d_adj_ents = nullptr;
+    c->adj_ghost_ready = false;
+    cudaFree(c->d_Wb);
+    cudaFree(c->d_Bfb);
+    cudaFree(c->d_G);
+    cudaFree(c->d_bvb1);
+    cudaFree(c->d_bvb2);
+    cudaFree(c->d_Eb);
+    c->d_ckW = c->d_ckBf = c->d_Wb = c->d_Bfb = c->d_G = nullptr;
+    c->d_bvb1 = c->d_bvb2 = c->d_Eb = nullptr;
+    c->adj_nsteps = 0;
     c->nblocks = 0;
     c->nactive = 0;
 }
@@ -1082,3 +1116,254 @@ int fx_info(fx_ctx *c, int what, long long *value)
 }
 
 } /* extern "C" */
+
+/* ---- discrete adjoint ------------------------------------------------------ */
+
+namespace {
+
+/* the reverse pass covers what the forward step does on single-level MHD
+ * meshes without gravity or resistivity: copy-type ghost operations, no
+ * coarse/fine transfers */
+int adj_supported(fx_ctx *c)
+{
+    if (!c->cfg.mhd || c->cfg.gravity || c->cfg.mhd_eta != 0.0) {
+        return set_err(c, FX_EINVAL, "the adjoint covers MHD runs without gravity or resistivity");
+    }
+    const FxProgram &g = c->plan.ghost;
+    bool ok = g.p_ops.empty() && c->plan.flux_corr.empty() && c->plan.emf_corr.empty();
+    for (const FxGop &op : g.cell_ops) {
+        ok = ok && (op.type == FX_GOP_COPY || op.type == FX_GOP_COPY_NEG || op.type == FX_GOP_COPY_USER);
+    }
+    for (const FxGop &op : g.face_ops) {
+        ok = ok && op.type == FX_FOP_COPY;
+    }
+    if (!ok) {
+        return set_err(c, FX_EINVAL, "the adjoint covers single-level meshes (no coarse/fine neighbours)");
+    }
+    return FX_SUCCESS;
+}
+
+/* the ghost program's waves transposed into gathers (FxAdjSrc / FxAdjEnt) */
+int build_adj_ghost(fx_ctx *c)
+{
+    if (c->adj_ghost_ready) {
+        return FX_SUCCESS;
+    }
+    const FxProgram &g = c->plan.ghost;
+    std::vector<FxAdjSrc> cs, fs;
+    std::vector<FxAdjEnt> ents;
+    c->adj_cbeg.assign(1, 0);
+    c->adj_fbeg.assign(1, 0);
+    std::vector<std::pair<int64_t, FxAdjEnt>> list;
+    for (int w = 0; w < g.nwaves(); ++w) {
+        list.clear();
+        for (int q = g.cell_begin[w]; q < g.cell_begin[w + 1]; ++q) {
+            const FxGop &op = g.cell_ops[q];
+            int kind = 0;
+            if (op.type == FX_GOP_COPY_NEG) kind = 1 + op.aux;
+            if (op.type == FX_GOP_COPY_USER && op.aux) kind = 16;
+            list.push_back({(int64_t)op.src, FxAdjEnt{op.dst, kind}});
+        }
+        std::stable_sort(list.begin(), list.end(),
+            [](const std::pair<int64_t, FxAdjEnt> &a, const std::pair<int64_t, FxAdjEnt> &b) { return a.first < b.first; });
+        for (size_t q = 0; q < list.size();) {
+            FxAdjSrc sr{(int32_t)list[q].first, 0, (int32_t)ents.size(), 0};
+            while (q < list.size() && list[q].first == sr.key) {
+                ents.push_back(list[q].second);
+                ++q;
+            }
+            sr.end = (int32_t)ents.size();
+            cs.push_back(sr);
+        }
+        c->adj_cbeg.push_back((int)cs.size());
+        list.clear();
+        for (int q = g.face_begin[w]; q < g.face_begin[w + 1]; ++q) {
+            const FxGop &op = g.face_ops[q];
+            list.push_back({((int64_t)op.src << 2) | (op.aux & 3), FxAdjEnt{op.dst, 0}});
+        }
+        for (int q = g.b_begin[w]; q < g.b_begin[w + 1]; ++q) {
+            const FxBop &op = g.b_ops[q];
+            for (int d = 0; d < 3; ++d) {
+                for (int h = 0; h < 2; ++h) {
+                    list.push_back({((int64_t)op.f[2 * d + h] << 2) | d, FxAdjEnt{op.dst, 1 + d}});
+                }
+            }
+        }
+        std::stable_sort(list.begin(), list.end(),
+            [](const std::pair<int64_t, FxAdjEnt> &a, const std::pair<int64_t, FxAdjEnt> &b) { return a.first < b.first; });
+        for (size_t q = 0; q < list.size();) {
+            const int64_t key = list[q].first;
+            FxAdjSrc sr{(int32_t)(key >> 2), (int32_t)(key & 3), (int32_t)ents.size(), 0};
+            while (q < list.size() && list[q].first == key) {
+                ents.push_back(list[q].second);
+                ++q;
+            }
+            sr.end = (int32_t)ents.size();
+            fs.push_back(sr);
+        }
+        c->adj_fbeg.push_back((int)fs.size());
+    }
+    int rc;
+    if ((rc = dev_alloc(c, &c->d_adj_csrc, cs.size()))) return rc;
+    if ((rc = dev_alloc(c, &c->d_adj_fsrc, fs.size()))) return rc;
+    if ((rc = dev_alloc(c, &c->d_adj_ents, ents.size()))) return rc;
+    const cudaMemcpyKind h2d = cudaMemcpyHostToDevice;
+    if (!cs.empty()) FX_CUDA(c, cudaMemcpyAsync(c->d_adj_csrc, cs.data(), cs.size() * sizeof(FxAdjSrc), h2d, c->stream));
+    if (!fs.empty()) FX_CUDA(c, cudaMemcpyAsync(c->d_adj_fsrc, fs.data(), fs.size() * sizeof(FxAdjSrc), h2d, c->stream));
+    if (!ents.empty()) FX_CUDA(c, cudaMemcpyAsync(c->d_adj_ents, ents.data(), ents.size() * sizeof(FxAdjEnt), h2d, c->stream));
+    FX_CUDA(c, cudaStreamSynchronize(c->stream));
+    c->adj_ghost_ready = true;
+    return FX_SUCCESS;
+}
+
+/* adjoint of the whole ghost fill of `slot`: waves in reverse order, each a
+ * gather into the elements it read followed by clearing its destinations */
+void adj_ghost(fx_ctx *c, const FxAdjDev &A, int slot)
+{
+    const FxProgram &g = c->plan.ghost;
+    for (int w = g.nwaves() - 1; w >= 0; --w) {
+        fx_launch_adj_gather(A, c->d_adj_csrc + c->adj_cbeg[w], c->adj_cbeg[w + 1] - c->adj_cbeg[w],
+            c->d_adj_fsrc + c->adj_fbeg[w], c->adj_fbeg[w + 1] - c->adj_fbeg[w], c->d_adj_ents, slot, c->stream);
+        fx_launch_adj_zero(A, c->d_cops + g.cell_begin[w], g.cell_begin[w + 1] - g.cell_begin[w],
+            c->d_fops + g.face_begin[w], g.face_begin[w + 1] - g.face_begin[w],
+            c->d_bops + g.b_begin[w], g.b_begin[w + 1] - g.b_begin[w], slot, c->stream);
+    }
+}
+
+/* the reverse sweep over all stored stages; the adjoint of the final
+ * state is in d_Wb / d_Bfb on entry, that of the stored initial state on
+ * return.  Device time of the sweep goes to c->adj_ms. */
+int adjoint_reverse(fx_ctx *c)
+{
+    const size_t nb = (size_t)c->nblocks;
+    const size_t wn = nb * w_count(c);
+    const size_t bn = nb * FX_BF_COUNT;
+    cudaStream_t s = c->stream;
+    FxAdjDev A{};
+    A.blk = c->d_blk;
+    A.gamma = c->cfg.gamma;
+    A.dt = c->adj_dt;
+    A.Wb = c->d_Wb;
+    A.Bfb = c->d_Bfb;
+    A.G = c->d_G;
+    A.bvb1 = c->d_bvb1;
+    A.bvb2 = c->d_bvb2;
+    A.Eb = c->d_Eb;
+    cudaEvent_t e0, e1;
+    FX_CUDA(c, cudaEventCreate(&e0));
+    FX_CUDA(c, cudaEventCreate(&e1));
+    FX_CUDA(c, cudaEventRecord(e0, s));
+    for (int n = c->adj_nsteps - 1; n >= 0; --n) {
+        for (int stage = 2; stage >= 1; --stage) {
+            const size_t k = 2 * (size_t)n + stage;
+            const int dst = stage == 1 ? 1 : 0;
+            A.Wbef = c->d_ckW + (k - 1) * wn;
+            A.Bfbef = c->d_ckBf + (k - 1) * bn;
+            A.Waft = c->d_ckW + k * wn;
+            A.vr = c->d_ckVr + (k - 1) * nb * FX_VR_COUNT;
+            adj_ghost(c, A, dst);
+            fx_launch_adj_cells(A, c->d_active, c->nactive, stage, s);
+            FX_CUDA(c, cudaMemsetAsync(c->d_Eb, 0, nb * FX_EMF_COUNT * sizeof(double), s));
+            fx_launch_adj_bf(A, c->d_active, c->nactive, stage, s);
+            FX_CUDA(c, cudaMemsetAsync(c->d_bvb1, 0, nb * FX_BV_COUNT * sizeof(double), s));
+            FX_CUDA(c, cudaMemsetAsync(c->d_bvb2, 0, nb * FX_BV_COUNT * sizeof(double), s));
+            fx_launch_adj_emf(A, c->d_active, c->nactive, stage, s);
+            fx_launch_adj_flux(A, c->d_active, c->nactive, stage, s);
+        }
+    }
+    FX_CUDA(c, cudaEventRecord(e1, s));
+    FX_CUDA(c, cudaEventSynchronize(e1));
+    float ms = 0.0f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    c->adj_ms = ms;
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    return check_device_error(c);
+}
+
+} // namespace
+
+int fx_adjoint_forward(fx_ctx *c, int nsteps, double dt)
+{
+    if (!has_mesh(c)) return c ? set_err(c, FX_ENOMESH, "no mesh") : FX_EINVAL;
+    if (nsteps < 1 || !(dt > 0.0)) return set_err(c, FX_EINVAL, "fx_adjoint_forward: nsteps >= 1 and dt > 0");
+    int rc = adj_supported(c);
+    if (rc) return rc;
+    if ((rc = build_adj_ghost(c))) return rc;
+    const size_t nb = (size_t)c->nblocks;
+    const size_t wn = nb * w_count(c);
+    const size_t bn = nb * FX_BF_COUNT;
+    const size_t nck = 2 * (size_t)nsteps + 1;
+    if (c->adj_nsteps != nsteps || !c->d_ckW) {
+        if ((rc = dev_alloc(c, &c->d_ckW, nck * wn))) return rc;
+        if ((rc = dev_alloc(c, &c->d_ckBf, nck * bn))) return rc;
+        if ((rc = dev_alloc(c, &c->d_ckVr, (nck - 1) * nb * FX_VR_COUNT))) return rc;
+    }
+    cudaStream_t s = c->stream;
+    const cudaMemcpyKind d2d = cudaMemcpyDeviceToDevice;
+    FX_CUDA(c, cudaMemcpyAsync(c->d_ckW, c->d_W, wn * sizeof(double), d2d, s));
+    FX_CUDA(c, cudaMemcpyAsync(c->d_ckBf, c->d_Bf, bn * sizeof(double), d2d, s));
+    for (int n = 0; n < nsteps; ++n) {
+        for (int stage = 1; stage <= 2; ++stage) {
+            fx_launch_set_dt(c->D, dt, s);
+            stage_seq(c, FX_FORM_BATCHED, stage);
+            const size_t k = 2 * (size_t)n + stage;
+            FX_CUDA(c, cudaMemcpyAsync(c->d_ckW + k * wn, c->d_W, wn * sizeof(double), d2d, s));
+            FX_CUDA(c, cudaMemcpyAsync(c->d_ckBf + k * bn, c->d_Bf, bn * sizeof(double), d2d, s));
+            /* the stage's face velocities: their signs pick the upwind EMF
+             * terms the reverse pass differentiates */
+            FX_CUDA(c, cudaMemcpyAsync(c->d_ckVr + (k - 1) * nb * FX_VR_COUNT, c->d_vr,
+                nb * FX_VR_COUNT * sizeof(double), d2d, s));
+        }
+    }
+    c->adj_nsteps = nsteps;
+    c->adj_dt = dt;
+    return sync_and_check(c);
+}
+
+int fx_adjoint_backward(fx_ctx *c, const double *W_bar, const double *Bf_bar, double *W_bar_out,
+    double *Bf_bar_out, int initial_fill)
+{
+    if (!has_mesh(c)) return c ? set_err(c, FX_ENOMESH, "no mesh") : FX_EINVAL;
+    if (c->adj_nsteps < 1 || !c->d_ckW) return set_err(c, FX_EINVAL, "fx_adjoint_backward: no stored forward pass");
+    if (!W_bar || !W_bar_out || !Bf_bar_out) return set_err(c, FX_EINVAL, "fx_adjoint_backward: null array");
+    const size_t nb = (size_t)c->nblocks;
+    const size_t wn = nb * w_count(c);
+    const size_t bn = nb * FX_BF_COUNT;
+    int rc;
+    if (!c->d_Wb) {
+        if ((rc = dev_alloc(c, &c->d_Wb, wn))) return rc;
+        if ((rc = dev_alloc(c, &c->d_Bfb, bn))) return rc;
+        if ((rc = dev_alloc(c, &c->d_G, nb * FX_ADJ_G_COUNT))) return rc;
+        if ((rc = dev_alloc(c, &c->d_bvb1, nb * FX_BV_COUNT))) return rc;
+        if ((rc = dev_alloc(c, &c->d_bvb2, nb * FX_BV_COUNT))) return rc;
+        if ((rc = dev_alloc(c, &c->d_Eb, nb * FX_EMF_COUNT))) return rc;
+    }
+    cudaStream_t s = c->stream;
+    FX_CUDA(c, cudaMemcpyAsync(c->d_Wb, W_bar, wn * sizeof(double), cudaMemcpyHostToDevice, s));
+    if (Bf_bar) {
+        FX_CUDA(c, cudaMemcpyAsync(c->d_Bfb, Bf_bar, bn * sizeof(double), cudaMemcpyHostToDevice, s));
+    } else {
+        FX_CUDA(c, cudaMemsetAsync(c->d_Bfb, 0, bn * sizeof(double), s));
+    }
+    FX_CUDA(c, cudaMemsetAsync(c->d_G, 0, nb * FX_ADJ_G_COUNT * sizeof(double), s));
+    rc = adjoint_reverse(c);
+    if (rc) return rc;
+    FxAdjDev A{};
+    A.blk = c->d_blk;
+    A.Wb = c->d_Wb;
+    A.Bfb = c->d_Bfb;
+    if (initial_fill) {
+        adj_ghost(c, A, 0);
+    }
+    FX_CUDA(c, cudaMemcpyAsync(W_bar_out, c->d_Wb, wn * sizeof(double), cudaMemcpyDeviceToHost, s));
+    FX_CUDA(c, cudaMemcpyAsync(Bf_bar_out, c->d_Bfb, bn * sizeof(double), cudaMemcpyDeviceToHost, s));
+    return sync_and_check(c);
+}
+
+int fx_adjoint_time(fx_ctx *c, double *ms)
+{
+    if (!c || !ms) return FX_EINVAL;
+    *ms = c->adj_ms;
+    return FX_SUCCESS;
+}

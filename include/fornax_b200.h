@@ -263,6 +263,31 @@ int fx_autotune(fx_ctx *ctx, double *times_ms, int n, int *choice);
  * (bf2bc) operations */
 int fx_info(fx_ctx *ctx, int what, long long *value);
 
+/* ---- discrete adjoint ---------------------------------------------------------- */
+
+/* No counterpart in the reference (it has no adjoint): reverse-mode
+ * derivatives of the batched RK2 step for single-level MHD meshes without
+ * gravity or resistivity.
+ *
+ * fx_adjoint_forward runs nsteps batched RK2 steps with the fixed time step
+ * dt from the current state and stores the state after every stage (W and
+ * Bf, both slots) and the stage's face velocities: (2 nsteps + 1) * nblocks
+ * * (9 * 2 * 8000 + 3 * 2 * 8400) + 2 nsteps * nblocks * 72000 doubles of
+ * device memory. */
+int fx_adjoint_forward(fx_ctx *ctx, int nsteps, double dt);
+/* Reverse pass over the stored steps.  W_bar / Bf_bar (host, the layout of
+ * fx_upload_all; Bf_bar may be NULL for zero) hold d J / d (final state);
+ * W_bar_out / Bf_bar_out receive d J / d (state at fx_adjoint_forward's
+ * entry).  With initial_fill = 1 the adjoint of one more ghost fill of slot
+ * 0 is applied last, so the result is with respect to the state before the
+ * driver's initial fill (the ghost entries then carry no sensitivity).
+ * Limiter and Riemann-fan branches are those of the stored forward pass. */
+int fx_adjoint_backward(fx_ctx *ctx, const double *W_bar, const double *Bf_bar, double *W_bar_out,
+    double *Bf_bar_out, int initial_fill);
+/* Device time (ms, CUDA events) of the last reverse sweep, without the
+ * host transfers. */
+int fx_adjoint_time(fx_ctx *ctx, double *ms);
+
 /* ---- adjoint building blocks (host) ----------------------------------------- */
 
 /* Host evaluation of one face of the face-flux kernel, for checks of the
