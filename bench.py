@@ -161,12 +161,15 @@ def measured_peak_hbm():
 
 def flux_traffic_per_launch():
     """DRAM bytes of one face-flux launch from the committed ncu summary, or None."""
-    path = os.path.join(HERE, "profiles", "flux_traffic.json")
+    path = os.path.join(HERE, "profiles", "k_flux_traffic_fourier128.txt")
     try:
         with open(path) as f:
-            return float(json.load(f)["dram_bytes_per_launch"])
-    except (OSError, KeyError, ValueError):
-        return None
+            for line in f:
+                if line.startswith("dram_bytes_per_launch:"):
+                    return float(line.split(":", 1)[1])
+    except (OSError, ValueError):
+        pass
+    return None
 
 
 def run_amr(args, dev, kind):
@@ -257,6 +260,39 @@ def run_amr(args, dev, kind):
     }
     ctx.close()
     return out
+
+
+def run_adjoint(args, dev):
+    """Cost of the discrete adjoint on the 64^3 workload (4^3 blocks of 16^3,
+    seeded Fourier-mode MHD with amplitude 0.01, |k|_inf <= 3): device time
+    of the reverse sweep over 10 RK2 steps per step, against one batched
+    forward step."""
+    import numpy as np
+    import torch
+
+    import fornaxamr_b200 as fx
+    from fornaxamr_b200 import mesh, problems
+
+    coord = (0.0, 1.0, 0.0, 1.0, 0.0, 1.0)
+    blocks = mesh.uniform_mesh((4, 4, 4), coord)
+    W0, Bf0 = problems.fourier_mhd(blocks, nmodes=32, kmax=3, amp_rho=0.01, amp_v=0.01, amp_A=0.005)
+    ctx = fx.Context(True, 5.0 / 3.0, coord, device=dev)
+    ctx.set_mesh(mesh.to_desc(blocks))
+    ctx.upload_all(np.ascontiguousarray(W0), np.ascontiguousarray(Bf0))
+    ctx.boundary_fill(1, 0)
+    dt = ctx.calc_dt(0.4)
+    nsteps = 10
+    ctx.adjoint_forward(nsteps, dt)
+    seed = np.full(W0.size, 1.0e-3)
+    ms = []
+    for _ in range(3):
+        ctx.adjoint_backward(seed)
+        ms.append(ctx.adjoint_ms() / nsteps)
+    ms_adj = min(ms)
+    ms_fwd = ctx.time_phase(fx.PHASE_STEP, 20, dt)
+    ctx.close()
+    return {"workload": "64^3 MHD (4^3 blocks), 10 RK2 steps, fixed dt", "ms_per_step_adjoint": ms_adj,
+            "ms_per_step_forward": ms_fwd, "adjoint_over_forward": ms_adj / ms_fwd}
 
 
 def run_fx(args, rank, world, local_rank):
@@ -444,6 +480,8 @@ def main():
         torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     line = run_fx(args, rank, world, local_rank)
     line["cpu_baseline"] = cb
+    if world == 1:
+        line["adjoint"] = run_adjoint(args, local_rank)
     if world == 1 and args.amr_steps > 0:
         line["amr_blast"] = run_amr(args, local_rank, "blast")
         if args.collapse:

@@ -1,12 +1,20 @@
-"""Run the Fourier-mode MHD workload on the device.
+"""Run one of the measured workloads on the device (the small, self-contained
+cases the kernel profiles are taken on).
 
-    python -m fornaxamr_b200.workload [--root R] [--steps N] [--form batched|plain]
+    python -m fornaxamr_b200.workload [--problem fourier|blast|collapse]
+        [--root R] [--steps N] [--form batched|plain] [--adjoint N]
 
-Builds a uniform root^3 mesh of 16^3 blocks on [0,1]^3, generates the
-seeded Fourier-mode initial state (fornaxamr_b200.problems.fourier_mhd), runs
-the driver's initial ghost fill and N driver steps (calc_dt + RK2 step), and
-prints the device time per step.  Used as the small, self-contained case for
-kernel profiles.
+fourier: uniform root^3 mesh of 16^3 blocks on [0,1]^3 with the seeded
+Fourier-mode MHD state (fornaxamr_b200.problems.fourier_mhd).
+blast: static AMR magnetised blast, root^3 roots on [-0.7, 0.7]^3, levels
+refined inside r < 0.4 and 0.2 about (0.1, 0.05, 0).
+collapse: static AMR gravity collapse, root^3 roots on [-1, 1]^3, spheres
+0.4 / 0.2 / 0.1 about the origin.
+
+Runs the driver's initial ghost fill and N driver steps (calc_dt + RK2 step)
+and prints the time per step.  With --adjoint N (fourier only, amplitude
+0.01, |k| <= 3) it runs N fixed-dt steps storing every stage, then one
+reverse sweep, and prints the reverse sweep's device time per step.
 """
 from __future__ import annotations
 
@@ -18,30 +26,68 @@ import numpy as np
 
 def main():
     ap = argparse.ArgumentParser()
+    ap.add_argument("--problem", default="fourier", choices=["fourier", "blast", "collapse"])
     ap.add_argument("--root", type=int, default=4)
     ap.add_argument("--steps", type=int, default=2)
     ap.add_argument("--form", default="batched", choices=["batched", "plain"])
     ap.add_argument("--modes", type=int, default=32)
+    ap.add_argument("--adjoint", type=int, default=0)
     args = ap.parse_args()
 
     import fornaxamr_b200 as fx
     from fornaxamr_b200 import mesh, problems
 
-    coord = (0.0, 1.0, 0.0, 1.0, 0.0, 1.0)
-    blocks = mesh.uniform_mesh((args.root,) * 3, coord)
-    W, Bf = problems.fourier_mhd(blocks, nmodes=args.modes)
-    ctx = fx.Context(True, 5.0 / 3.0, coord)
+    grav = None
+    gamma = 5.0 / 3.0
+    gravity = False
+    if args.problem == "fourier":
+        coord = (0.0, 1.0, 0.0, 1.0, 0.0, 1.0)
+        blocks = mesh.uniform_mesh((args.root,) * 3, coord)
+        if args.adjoint:
+            W, Bf = problems.fourier_mhd(blocks, nmodes=args.modes, kmax=3, amp_rho=0.01, amp_v=0.01, amp_A=0.005)
+        else:
+            W, Bf = problems.fourier_mhd(blocks, nmodes=args.modes)
+    else:
+        hw = 0.7 if args.problem == "blast" else 1.0
+        coord = (-hw, hw, -hw, hw, -hw, hw)
+        if args.problem == "blast":
+            blocks = mesh.static_amr_mesh((args.root,) * 3, coord, 2,
+                                          mesh.ball_refiner((0.1, 0.05, 0.0), (0.4, 0.2)))
+        else:
+            blocks = mesh.static_amr_mesh((args.root,) * 3, coord, 3,
+                                          mesh.ball_refiner((0.0, 0.0, 0.0), (0.4, 0.2, 0.1)))
+        recs = fx.plan_export(fx.make_config(True, gamma, coord), mesh.to_desc(blocks), 3)
+        if args.problem == "blast":
+            W, Bf = problems.amr_blast(blocks, recs)
+        else:
+            gamma = 4.0 / 3.0
+            gravity = True
+            W, Bf, grav = problems.collapse(blocks, recs, half_width=hw)
+    ctx = fx.Context(True, gamma, coord, gravity=gravity)
     ctx.set_mesh(mesh.to_desc(blocks))
     ctx.upload_all(np.ascontiguousarray(W), np.ascontiguousarray(Bf))
+    if grav is not None:
+        for b in range(len(blocks)):
+            if blocks[b].active == 1:
+                ctx.upload_block(b, W[b].ravel(), [Bf[b, d].ravel() for d in range(3)],
+                                 [grav[b, d] for d in range(3)])
     ctx.boundary_fill(1, 0)
     ctx.sync()
+    zones = sum(1 for b in blocks if b.active == 1) * 4096
+    if args.adjoint:
+        dt = ctx.calc_dt(0.4)
+        ctx.adjoint_forward(args.adjoint, dt)
+        ctx.adjoint_backward(np.full(W.size, 1.0e-3))
+        print(f"{len(blocks)} blocks, adjoint of {args.adjoint} steps: "
+              f"{ctx.adjoint_ms() / args.adjoint:.3f} ms/step (reverse sweep, device)")
+        ctx.close()
+        return
     form = fx.FORM_BATCHED if args.form == "batched" else fx.FORM_PLAIN
     t0 = time.perf_counter()
     state = ctx.run(form, args.steps, 0.4, 1.2, 1.0e30, (0.0, 0.0, 0))
     ctx.sync()
     dt = time.perf_counter() - t0
-    zones = len(blocks) * 4096
-    print(f"{len(blocks)} blocks, {args.steps} steps ({args.form}): t={state[0]:.6e} "
+    print(f"{len(blocks)} blocks ({zones // 4096} active), {args.steps} steps ({args.form}): t={state[0]:.6e} "
           f"wall {1e3 * dt / max(args.steps, 1):.3f} ms/step, {zones * args.steps / dt:.3e} zone-updates/s")
     ctx.close()
 
