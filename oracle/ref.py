@@ -64,6 +64,7 @@ class RhParams(C.Structure):
         ("K", C.c_double),
         ("beta", C.c_double),
         ("gm_point", C.c_double),
+        ("bc", C.c_int * 6),
     ]
 
 

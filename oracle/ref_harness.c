@@ -114,6 +114,7 @@ typedef struct rh_params {
     double K;
     double beta;
     double gm_point;
+    int bc[6];          /* prj_bc_type per side: x1 inner, x1 outer, ..., x3 outer (0 outflow) */
 } rh_params;
 
 static prj_sim g_sim;
@@ -612,12 +613,12 @@ static void rh_set_defaults(void)
     g_sim.coord.x2max = g_par.xmax[1];
     g_sim.coord.x3min = g_par.xmin[2];
     g_sim.coord.x3max = g_par.xmax[2];
-    g_sim.bc.bc_x1_inner = PRJ_BC_OUTFLOW;
-    g_sim.bc.bc_x1_outer = PRJ_BC_OUTFLOW;
-    g_sim.bc.bc_x2_inner = PRJ_BC_OUTFLOW;
-    g_sim.bc.bc_x2_outer = PRJ_BC_OUTFLOW;
-    g_sim.bc.bc_x3_inner = PRJ_BC_OUTFLOW;
-    g_sim.bc.bc_x3_outer = PRJ_BC_OUTFLOW;
+    g_sim.bc.bc_x1_inner = g_par.bc[0];
+    g_sim.bc.bc_x1_outer = g_par.bc[1];
+    g_sim.bc.bc_x2_inner = g_par.bc[2];
+    g_sim.bc.bc_x2_outer = g_par.bc[3];
+    g_sim.bc.bc_x3_inner = g_par.bc[4];
+    g_sim.bc.bc_x3_outer = g_par.bc[5];
     g_sim.cfl = g_par.cfl;
     g_sim.dt_factor = g_par.dt_factor;
     g_sim.t_end = g_par.t_end;

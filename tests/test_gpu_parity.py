@@ -23,7 +23,7 @@ TOL = 1e-12
 def make_ctx(ref, p, mhd, gravity=False):
     desc = H.ref_desc(ref)
     coord = [p.xmin[0], p.xmax[0], p.xmin[1], p.xmax[1], p.xmin[2], p.xmax[2]]
-    ctx = fx.Context(mhd, p.gamma, coord, gravity=gravity)
+    ctx = fx.Context(mhd, p.gamma, coord, bc=tuple(p.bc), gravity=gravity)
     ctx.set_mesh(desc)
     W, Bf = H.ref_state(ref)
     for b in range(W.shape[0]):
@@ -205,3 +205,22 @@ def test_collapse_gravity_steps_match_reference(ref_mhd, form):
     assert (t, dt, st) == (t_ref, dt_ref, st_ref)
     assert_state_equal(ctx, ref_mhd, True)
     ctx.close()
+
+
+@pytest.mark.parametrize("form", [fx.FORM_PLAIN, fx.FORM_BATCHED])
+def test_sod_hydro_reflect_and_user_boundaries_match_reference(ref_hydro, form):
+    """Sod tube between reflecting walls in x, and with a user band at x1
+    inner plus reflecting walls elsewhere; 4 x 2 x 2 blocks, 25 driver
+    steps."""
+    for bc in ((1, 1, 0, 0, 0, 0), (2, 1, 1, 1, 0, 0)):
+        p = R.params_sod(nblocks_x=4)
+        p.root[:] = [4, 2, 2]
+        p.xmax[:] = [1.0, 0.5, 0.5]
+        p.bc[:] = list(bc)
+        ref_hydro.setup(p)
+        ctx = make_ctx(ref_hydro, p, False)
+        n, t_ref, dt_ref, st_ref = ref_hydro.run(25)
+        t, dt, st = ctx.run(form, 25, p.cfl, p.dt_factor, p.t_end, (0.0, 0.0, 0.0))
+        assert (t, dt, st) == (t_ref, dt_ref, st_ref)
+        assert_state_equal(ctx, ref_hydro, False, True)
+        ctx.close()

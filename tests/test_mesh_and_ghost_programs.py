@@ -16,7 +16,7 @@ def _desc_and_cfg(ref, p, mhd):
     import fornaxamr_b200 as fx
     desc = H.ref_desc(ref)
     coord = [p.xmin[0], p.xmax[0], p.xmin[1], p.xmax[1], p.xmin[2], p.xmax[2]]
-    return desc, fx.make_config(mhd, p.gamma, coord)
+    return desc, fx.make_config(mhd, p.gamma, coord, bc=tuple(p.bc))
 
 
 @pytest.mark.parametrize("root", [(2, 2, 2), (3, 2, 1), (1, 1, 1)])
@@ -169,3 +169,14 @@ def test_amr_corrections_match_reference(ref_mhd, root, radii):
         for d in range(3):
             assert np.array_equal(flux[b, d], ref_mhd.flux(b, d))
             assert np.array_equal(emf[b, d].view(np.int64), ref_mhd.emf(b, d).view(np.int64))
+
+
+@pytest.mark.parametrize("bc", [(1, 1, 0, 0, 0, 0), (2, 0, 1, 1, 0, 0), (1, 2, 0, 0, 1, 1)])
+def test_hydro_reflect_and_user_boundaries_match_reference(ref_hydro, bc):
+    """Reflecting (normal velocity negated) and user (v1 set) boundary bands,
+    src/prj_boundary.c:413-530, on a 4 x 2 x 2 hydro mesh."""
+    p = R.params_sod(nblocks_x=4)
+    p.root[:] = [4, 2, 2]
+    p.xmax[:] = [1.0, 0.5, 0.5]
+    p.bc[:] = list(bc)
+    _scrambled_fill_check(ref_hydro, p, False, seed=sum(bc))
