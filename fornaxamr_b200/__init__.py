@@ -240,6 +240,10 @@ class Context:
         self._check(self.L.fx_autotune(self._h, _dp(times), 16, C.byref(choice)))
         return choice.value, times
 
+    def set_flux_shape(self, variant: int) -> None:
+        """Force a face-kernel launch shape (see fx_set_flux_shape)."""
+        self._check(self.L.fx_set_flux_shape(self._h, variant))
+
     def info(self, what: int) -> int:
         v = C.c_longlong(0)
         self._check(self.L.fx_info(self._h, what, C.byref(v)))

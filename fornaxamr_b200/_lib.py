@@ -66,7 +66,7 @@ EXPORTS = [
     "fx_eos_fill_mesh", "fx_boundary_fill_ghosts_and_bf", "fx_calc_dt", "fx_stage", "fx_step",
     "fx_run", "fx_plan_export", "fx_time_phase", "fx_info", "fx_upload_state", "fx_download_state",
     "fx_autotune", "fx_calc_dt_noalloc", "fx_face_eval_host", "fx_face_vjp_host",
-    "fx_adjoint_forward", "fx_adjoint_backward", "fx_adjoint_time",
+    "fx_adjoint_forward", "fx_adjoint_backward", "fx_adjoint_time", "fx_set_flux_shape",
 ]
 PHASE_FLUX, PHASE_EMF, PHASE_CT, PHASE_CELLS, PHASE_GHOST, PHASE_STEP = range(6)
 
@@ -113,6 +113,7 @@ def load() -> C.CDLL:
     L.fx_time_phase.argtypes = [vp, C.c_int, C.c_int, C.c_double, dp]
     L.fx_info.argtypes = [vp, C.c_int, C.POINTER(C.c_longlong)]
     L.fx_autotune.argtypes = [vp, dp, C.c_int, C.POINTER(C.c_int)]
+    L.fx_set_flux_shape.argtypes = [vp, C.c_int]
     # device pointers (W, dx, blocks, dt) and the stream pass as plain addresses
     L.fx_calc_dt_noalloc.argtypes = [vp, C.c_int, vp, vp, C.c_int, C.c_double, C.c_double, vp, vp]
     L.fx_adjoint_forward.argtypes = [vp, C.c_int, C.c_double]

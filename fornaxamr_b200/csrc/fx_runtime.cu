@@ -1083,6 +1083,17 @@ int fx_autotune(fx_ctx *c, double *times_ms, int n, int *choice)
     return check_device_error(c);
 }
 
+int fx_set_flux_shape(fx_ctx *c, int variant)
+{
+    if (!c) return FX_EINVAL;
+    if (variant < 0 || variant >= FX_FLUX_VARIANTS) {
+        return set_err(c, FX_EINVAL, "fx_set_flux_shape: variant %d outside [0, %d)", variant, FX_FLUX_VARIANTS);
+    }
+    c->D.flux_variant = variant;
+    free_graphs(c);
+    return FX_SUCCESS;
+}
+
 int fx_info(fx_ctx *c, int what, long long *value)
 {
     if (!has_mesh(c) || !value) return c ? set_err(c, FX_EINVAL, "fx_info: no mesh") : FX_EINVAL;

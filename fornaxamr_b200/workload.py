@@ -2,7 +2,7 @@
 cases the kernel profiles are taken on).
 
     python -m fornaxamr_b200.workload [--problem fourier|blast|collapse]
-        [--root R] [--steps N] [--form batched|plain] [--adjoint N]
+        [--root R] [--steps N] [--form batched|plain] [--adjoint N] [--shape S]
 
 fourier: uniform root^3 mesh of 16^3 blocks on [0,1]^3 with the seeded
 Fourier-mode MHD state (fornaxamr_b200.problems.fourier_mhd).
@@ -32,6 +32,7 @@ def main():
     ap.add_argument("--form", default="batched", choices=["batched", "plain"])
     ap.add_argument("--modes", type=int, default=32)
     ap.add_argument("--adjoint", type=int, default=0)
+    ap.add_argument("--shape", type=int, default=-1, help="force a face-kernel launch shape (fx_set_flux_shape)")
     args = ap.parse_args()
 
     import fornaxamr_b200 as fx
@@ -73,6 +74,8 @@ def main():
                                  [grav[b, d] for d in range(3)])
     ctx.boundary_fill(1, 0)
     ctx.sync()
+    if args.shape >= 0:
+        ctx.set_flux_shape(args.shape)
     zones = sum(1 for b in blocks if b.active == 1) * 4096
     if args.adjoint:
         dt = ctx.calc_dt(0.4)

@@ -257,6 +257,10 @@ int fx_time_phase(fx_ctx *ctx, int phase, int reps, double dt, double *ms);
  * steps.  times_ms (may be NULL) receives up to `n` per-shape times, *choice
  * the chosen shape.  The shapes compute identical results. */
 int fx_autotune(fx_ctx *ctx, double *times_ms, int n, int *choice);
+/* Forces face-kernel launch shape `variant` (0 .. 5, the autotuner's
+ * choices: one thread per face at various CTA sizes and register budgets).
+ * All shapes compute identical results. */
+int fx_set_flux_shape(fx_ctx *ctx, int variant);
 
 /* what = 0: kernel launches per batched step, 1: per plain step,
  * 2/3: ghost cell/face operations, 4: ghost-fill waves, 5: cell-field

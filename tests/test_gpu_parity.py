@@ -224,3 +224,18 @@ def test_sod_hydro_reflect_and_user_boundaries_match_reference(ref_hydro, form):
         assert (t, dt, st) == (t_ref, dt_ref, st_ref)
         assert_state_equal(ctx, ref_hydro, False, True)
         ctx.close()
+
+
+@pytest.mark.parametrize("shape", range(6))
+def test_every_face_kernel_shape_is_bit_identical(ref_mhd, shape):
+    """Every launch shape the autotuner chooses among reproduces the
+    reference."""
+    p = R.params_fourier(root=2, nmodes=8, kmax=2)
+    ref_mhd.setup(p)
+    ctx = make_ctx(ref_mhd, p, True)
+    ctx.set_flux_shape(shape)
+    n, t_ref, dt_ref, st_ref = ref_mhd.run(2)
+    t, dt, st = ctx.run(fx.FORM_BATCHED, 2, p.cfl, p.dt_factor, p.t_end, (0.0, 0.0, 0.0))
+    assert (t, dt, st) == (t_ref, dt_ref, st_ref)
+    assert_state_equal(ctx, ref_mhd, True)
+    ctx.close()
