@@ -17,10 +17,12 @@ from . import _lib
 from ._lib import (ARR_BF, ARR_BV1, ARR_BV2, ARR_EMF, ARR_EOSVAR, ARR_FLUX, ARR_GRAV, ARR_RHS,
                    ARR_VRIEMANN, ARR_W, BC_OUTFLOW, BC_PERIODIC, BC_REFLECT, BC_USER, FORM_BATCHED,
                    FORM_PLAIN, PHASE_CELLS, PHASE_CT, PHASE_EMF, PHASE_FLUX, PHASE_GHOST, PHASE_STEP,
-                   FxBlockDesc, FxConfig)
+                   AMR_FRACTIONAL_JUMP, AMR_LOEHNER, AMR_PRESSURE_SCALE_HEIGHT, AMR_VAR_DENSITY,
+                   AMR_VAR_PRESSURE, AMR_VAR_TEMPERATURE, AMR_VELOCITY, FxAmrConfig, FxBlockDesc,
+                   FxConfig)
 
 __all__ = ["Context", "FxError", "FORM_PLAIN", "FORM_BATCHED", "NCELLS", "NFACES", "NEDGES",
-           "library", "plan_export"]
+           "library", "plan_export", "amr_config", "amr_remesh_host"]
 
 NCELLS = 20 ** 3
 NFACES = 21 * 20 * 20
@@ -58,6 +60,63 @@ def make_config(mhd: bool, gamma: float, coord: Sequence[float], bc: Sequence[in
         cfg.bc[n] = int(bc[n])
     cfg.mhd_eta = float(mhd_eta)
     return cfg
+
+
+def amr_config(root_nx: Sequence[int], max_level: int, criteria: Sequence[dict] = (),
+               max_blocks: int = 65535, min_dx: float = 0.0, reach_density: float = -1.0,
+               E_floor: float = -1.0) -> FxAmrConfig:
+    """fx_amr_config from up to four criteria, each a dict with keys
+    estimator (AMR_*), refine, derefine and optionally var (Loehner or jump
+    variable, AMR_VAR_*) and eps; unset fields take the reference's defaults
+    (src/prj_io.c:341-355: thresholds 0.5 / 0.2, pressure, eps 0.1)."""
+    a = FxAmrConfig()
+    for d in range(3):
+        a.root_nx[d] = int(root_nx[d])
+    a.max_level = int(max_level)
+    a.max_blocks = int(max_blocks)
+    a.min_dx = float(min_dx)
+    a.reach_density = float(reach_density)
+    a.E_floor = float(E_floor)
+    for n in range(_lib.AMR_N):
+        k = a.crit[n]
+        k.set = 0
+        k.estimator = AMR_LOEHNER
+        k.lohner_var = AMR_VAR_PRESSURE
+        k.jump_var = AMR_VAR_PRESSURE
+        k.refine_thresh = 0.5
+        k.derefine_thresh = 0.2
+        k.lohner_eps = 0.1
+    for n, c in enumerate(criteria):
+        k = a.crit[n]
+        k.set = 1
+        k.estimator = int(c["estimator"])
+        k.refine_thresh = float(c.get("refine", 0.5))
+        k.derefine_thresh = float(c.get("derefine", 0.2))
+        var = int(c.get("var", AMR_VAR_PRESSURE))
+        k.lohner_var = var
+        k.jump_var = min(var, 1)
+        k.lohner_eps = float(c.get("eps", 0.1))
+    return a
+
+
+def amr_remesh_host(cfg: FxConfig, amr: FxAmrConfig, desc, votes: np.ndarray, capacity: int = 0):
+    """Host-only block-tree half of prj_amr_adapt for given pass-1 votes
+    (int32 [nblocks, 3]): returns (flags after the tag caps, new desc)."""
+    L = library()
+    nb = len(desc)
+    cap = capacity or max(4 * nb, nb + 64)
+    out = (FxBlockDesc * cap)()
+    flags = np.zeros(nb, dtype=np.int32)
+    v = np.ascontiguousarray(votes, dtype=np.int32).reshape(-1)
+    nout = C.c_int(0)
+    ip = C.POINTER(C.c_int32)
+    rc = L.fx_amr_remesh_host(C.byref(cfg), C.byref(amr), nb, desc, v.ctypes.data_as(ip),
+                              flags.ctypes.data_as(ip), cap, out, C.byref(nout))
+    if rc != 0:
+        raise FxError(rc, "fx_amr_remesh_host failed")
+    res = (FxBlockDesc * nout.value)()
+    C.memmove(res, out, C.sizeof(FxBlockDesc) * nout.value)
+    return flags, res
 
 
 def plan_export(cfg: FxConfig, desc, which: int):
@@ -250,6 +309,42 @@ class Context:
         return v.value
 
     # ---- discrete adjoint ------------------------------------------------------
+    # -- dynamic AMR ------------------------------------------------------------------
+    def amr_configure(self, amr: FxAmrConfig) -> None:
+        self._check(self.L.fx_amr_configure(self._h, C.byref(amr)))
+
+    def amr_tag(self) -> np.ndarray:
+        """prj_amr_tag's refine_flag per block entry (after the caps)."""
+        out = np.zeros(self.nblocks, dtype=np.int32)
+        self._check(self.L.fx_amr_tag(self._h, out.ctypes.data_as(C.POINTER(C.c_int32))))
+        return out
+
+    def amr_adapt(self) -> bool:
+        """prj_amr_adapt plus the driver's refill; True if the mesh changed."""
+        ch = C.c_int(0)
+        self._check(self.L.fx_amr_adapt(self._h, C.byref(ch)))
+        if ch.value:
+            self.nblocks = self.mesh_size()
+        return bool(ch.value)
+
+    def mesh_size(self) -> int:
+        n = C.c_int(0)
+        self._check(self.L.fx_get_mesh(self._h, 0, None, C.byref(n)))
+        return n.value
+
+    def get_mesh(self):
+        """The mirrored mesh as a ctypes fx_block_desc array."""
+        n = self.mesh_size()
+        out = (FxBlockDesc * n)()
+        m = C.c_int(0)
+        self._check(self.L.fx_get_mesh(self._h, n, out, C.byref(m)))
+        return out
+
+    def amr_energy_injected(self) -> float:
+        e = C.c_double(0.0)
+        self._check(self.L.fx_amr_energy_injected(self._h, C.byref(e)))
+        return e.value
+
     def adjoint_forward(self, nsteps: int, dt: float) -> None:
         """nsteps batched RK2 steps with fixed dt, storing every stage."""
         self._check(self.L.fx_adjoint_forward(self._h, nsteps, dt))

@@ -43,6 +43,9 @@ class FxBlockDesc(C.Structure):
         ("vol", C.c_double),
         ("area", C.c_double * 3),
         ("slot", FxSlot * 56),
+        ("parent", C.c_int32),
+        ("children", C.c_int32 * 8),
+        ("can_refine", C.c_int32),
     ]
 
 
@@ -57,6 +60,36 @@ class FxConfig(C.Structure):
     ]
 
 
+AMR_N = 4
+AMR_LOEHNER, AMR_VELOCITY, AMR_PRESSURE_SCALE_HEIGHT, AMR_FRACTIONAL_JUMP = 0, 1, 2, 3
+AMR_VAR_DENSITY, AMR_VAR_PRESSURE, AMR_VAR_TEMPERATURE = 0, 1, 2
+
+
+class FxAmrCriterion(C.Structure):
+    _fields_ = [
+        ("set", C.c_int32),
+        ("estimator", C.c_int32),
+        ("lohner_var", C.c_int32),
+        ("jump_var", C.c_int32),
+        ("refine_thresh", C.c_double),
+        ("derefine_thresh", C.c_double),
+        ("lohner_eps", C.c_double),
+    ]
+
+
+class FxAmrConfig(C.Structure):
+    _fields_ = [
+        ("root_nx", C.c_int32 * 3),
+        ("max_level", C.c_int32),
+        ("max_blocks", C.c_int32),
+        ("pad", C.c_int32),
+        ("min_dx", C.c_double),
+        ("reach_density", C.c_double),
+        ("E_floor", C.c_double),
+        ("crit", FxAmrCriterion * AMR_N),
+    ]
+
+
 # every entry point declared in include/fornax_b200.h
 EXPORTS = [
     "fx_create", "fx_destroy", "fx_last_error", "fx_sync", "fx_stream", "fx_set_mesh",
@@ -67,6 +100,8 @@ EXPORTS = [
     "fx_run", "fx_plan_export", "fx_time_phase", "fx_info", "fx_upload_state", "fx_download_state",
     "fx_autotune", "fx_calc_dt_noalloc", "fx_face_eval_host", "fx_face_vjp_host",
     "fx_adjoint_forward", "fx_adjoint_backward", "fx_adjoint_time", "fx_set_flux_shape",
+    "fx_amr_configure", "fx_amr_tag", "fx_amr_adapt", "fx_get_mesh", "fx_amr_energy_injected",
+    "fx_amr_remesh_host",
 ]
 PHASE_FLUX, PHASE_EMF, PHASE_CT, PHASE_CELLS, PHASE_GHOST, PHASE_STEP = range(6)
 
@@ -121,4 +156,11 @@ def load() -> C.CDLL:
     L.fx_adjoint_time.argtypes = [vp, dp]
     L.fx_face_eval_host.argtypes = [dp, C.c_double, C.c_double, dp]
     L.fx_face_vjp_host.argtypes = [dp, C.c_double, C.c_double, dp, dp, dp]
+    L.fx_amr_configure.argtypes = [vp, C.POINTER(FxAmrConfig)]
+    L.fx_amr_tag.argtypes = [vp, ip]
+    L.fx_amr_adapt.argtypes = [vp, C.POINTER(C.c_int)]
+    L.fx_get_mesh.argtypes = [vp, C.c_int, C.POINTER(FxBlockDesc), C.POINTER(C.c_int)]
+    L.fx_amr_energy_injected.argtypes = [vp, dp]
+    L.fx_amr_remesh_host.argtypes = [C.POINTER(FxConfig), C.POINTER(FxAmrConfig), C.c_int, C.POINTER(FxBlockDesc),
+                                     ip, ip, C.c_int, C.POINTER(FxBlockDesc), C.POINTER(C.c_int)]
     return L

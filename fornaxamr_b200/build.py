@@ -22,7 +22,8 @@ BUILD = os.path.join(HERE, "_build")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-std=c++17", "--fmad=false", "-lineinfo", "-Xcompiler", "-fPIC",
               "-Xcompiler", "-O2", "--expt-relaxed-constexpr"]
-SOURCES = ["fx_kernels.cu", "fx_runtime.cu", "fx_plan.cpp", "fx_noalloc.cu", "fx_adjoint.cu"]
+SOURCES = ["fx_kernels.cu", "fx_runtime.cu", "fx_plan.cpp", "fx_noalloc.cu", "fx_adjoint.cu", "fx_amr.cu",
+           "fx_amr_host.cpp"]
 
 
 def nvcc() -> str:

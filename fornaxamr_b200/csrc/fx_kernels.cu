@@ -633,17 +633,6 @@ __global__ void k_step_end(FxDev D)
 /* Ghost-fill programs                                                       */
 /* ------------------------------------------------------------------------ */
 
-/* minmod slope of prj_reconstruct_minmod_slope (src/prj_reconstruct.h:46-62) */
-__device__ __forceinline__ double fx_minmod_slope(double qm, double q0, double qp)
-{
-    const double sl = q0 - qm;
-    const double sr = qp - q0;
-    if (sl * sr <= 0.0) {
-        return 0.0;
-    }
-    return fabs(sl) < fabs(sr) ? sl : sr;
-}
-
 /* prj_reconstruct_cell_for_prolongate_minmod (src/prj_reconstruct.h:111-143):
  * per axis base + slope * target, combined as vx + vy + vz - 2 base; target
  * offsets are +-1/4 of a coarse cell.  (The use_BJ = 1 limiter of the
@@ -1076,6 +1065,13 @@ void fx_launch_ghost_wave(const FxDev &D, const FxGop *cops, int nc, const FxGop
     if (grid > 0) {
         k_ghost_wave<<<grid, 256, 0, s>>>(D, cops, nc, fops, nf, bops, nb, slot, nvg);
     }
+    if (np > 0) {
+        k_ghost_groups<<<fx_blocks(np, 128), 128, 0, s>>>(D, pops, np, slot);
+    }
+}
+
+void fx_launch_prolong_groups(const FxDev &D, const FxPop *pops, int np, int slot, cudaStream_t s)
+{
     if (np > 0) {
         k_ghost_groups<<<fx_blocks(np, 128), 128, 0, s>>>(D, pops, np, slot);
     }

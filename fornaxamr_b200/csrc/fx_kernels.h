@@ -223,4 +223,68 @@ void fx_launch_adj_bf(const FxAdjDev &A, const int *blist, int nlist, int stage,
 void fx_launch_adj_emf(const FxAdjDev &A, const int *blist, int nlist, int stage, cudaStream_t s);
 void fx_launch_adj_flux(const FxAdjDev &A, const int *blist, int nlist, int stage, cudaStream_t s);
 
+/* ---- dynamic AMR ----------------------------------------------------------- */
+
+/* refinement criteria of prj_amr_tag, the set entries of the reference's
+ * amr_* arrays in index order */
+struct FxAmrTagCfg {
+    int ncrit;
+    int est[4];        /* estimator */
+    int var[4];        /* Loehner variable (estimator 0) or jump variable (3) */
+    double rthr[4];    /* refine threshold, <= 0: not summed for refinement */
+    double dthr[4];    /* derefine threshold, <= 0: not summed for derefinement */
+    double eps[4];     /* Loehner epsilon */
+    double reach;      /* amr_reach_highest_level_at_density, <= 0: off */
+    int has_derefine;  /* some criterion has a derefine threshold > 0 */
+    int pad;
+};
+
+/* a child block to fill from its parent (oct: octant, x fastest) */
+struct FxAmrChildJob {
+    int32_t child;
+    int32_t parent;
+    int32_t oct;
+    int32_t pad;
+};
+
+/* one face layer (16 x 16 faces of direction dir) a new child copies from
+ * a finer neighbour of its parent: side 1 writes child index 16 from the
+ * neighbour's index 0, side 0 index 0 from index 16 */
+struct FxAmrCopyJob {
+    int32_t child;
+    int32_t src;
+    int32_t dir;
+    int32_t side;
+};
+
+/* a parent to fill from its eight children */
+struct FxAmrParentJob {
+    int32_t parent;
+    int32_t children[8];
+    int32_t pad[3];
+};
+
+/* votes[3 i .. 3 i + 2] = refine vote, derefine vote, boundary side mask of
+ * block list[i] (pass 1 of prj_amr_tag); has_parent[i]: the block may
+ * derefine */
+void fx_launch_amr_tag(const FxDev &D, const int *list, const int *has_parent, int n,
+    const FxAmrTagCfg &cfg, int32_t *votes, cudaStream_t s);
+/* zeroes W, Bf, eosvar and grav of the listed blocks (prj_zero_block_arrays) */
+void fx_launch_amr_zero(const FxDev &D, const int *blocks, int n, cudaStream_t s);
+/* both stage slots of every job */
+void fx_launch_amr_copy_faces(const FxDev &D, const FxAmrCopyJob *jobs, int n, cudaStream_t s);
+/* Toth-Roe groups of the ghost fill kernel, for one stage slot */
+void fx_launch_prolong_groups(const FxDev &D, const FxPop *pops, int np, int slot, cudaStream_t s);
+/* conserved prolongation, face-average field, cons2prim and energy floor of
+ * new children; inj (4096 per job) receives the floor's energy per cell
+ * when E_floor > 0 */
+void fx_launch_amr_prolong_cells(const FxDev &D, const FxAmrChildJob *jobs, int n, double E_floor,
+    double *inj, cudaStream_t s);
+/* face restriction of both stage slots onto re-activated parents */
+void fx_launch_amr_restrict_faces(const FxDev &D, const FxAmrParentJob *jobs, int n, cudaStream_t s);
+/* volume-weighted conserved restriction, face-average field, cons2prim and
+ * energy floor of re-activated parents */
+void fx_launch_amr_restrict_cells(const FxDev &D, const FxAmrParentJob *jobs, int n, double E_floor,
+    double *inj, cudaStream_t s);
+
 #endif

@@ -43,7 +43,8 @@ enum fx_err_code {
     FX_ERR_EOS_ZERO_RHO = 13,  /* prj_eos.c:248-250 zero density in eos fill */
     FX_ERR_ETA = 14,           /* prj_timeint.c:255-257, 279-281 */
     FX_ERR_B_NONFINITE = 15,   /* prj_timeint.c:506-508, prj_mhd.c:593-595 */
-    FX_ERR_TIMEOUT = 16        /* a bounded device wait gave up */
+    FX_ERR_TIMEOUT = 16,       /* a bounded device wait gave up */
+    FX_ERR_AMR_NONFINITE = 17  /* prj_amr.c:1892-1896, 2186-2189 non-finite field in a remesh */
 };
 
 struct FxErr {
@@ -103,6 +104,17 @@ FX_HD double fx_pressure(double g, double rho, double eint)
 FX_HD double fx_temperature(double g, double eint)
 {
     return (g - 1.0) * eint / FX_IDEAL_ENERGY_SCALE;
+}
+
+/* minmod slope of prj_reconstruct_minmod_slope (src/prj_reconstruct.h:46-62) */
+FX_HD double fx_minmod_slope(double qm, double q0, double qp)
+{
+    const double sl = q0 - qm;
+    const double sr = qp - q0;
+    if (sl * sr <= 0.0) {
+        return 0.0;
+    }
+    return fabs(sl) < fabs(sr) ? sl : sr;
 }
 
 /* prj_eos_prim2cons, src/prj_eos.c:2112-2151 */

@@ -25,6 +25,7 @@
 #include "../../include/fornax_b200.h"
 #include "fx_kernels.h"
 #include "fx_physics.cuh"
+#include "fx_amr.h"
 #include "fx_plan.h"
 
 struct fx_ctx {
@@ -76,6 +77,12 @@ struct fx_ctx {
     std::vector<int> adj_cbeg, adj_fbeg;
     FxAdjSrc *d_adj_csrc = nullptr, *d_adj_fsrc = nullptr;
     FxAdjEnt *d_adj_ents = nullptr;
+
+    int cap = 0;                      /* blocks the per-block device arrays hold */
+    /* dynamic AMR */
+    bool amr_set = false;
+    fx_amr_config amr{};
+    double E_injected = 0.0;          /* eos->E_injected of the remesh floors */
 };
 
 namespace {
@@ -118,6 +125,7 @@ const char *err_message(int code)
     case FX_ERR_ETA: return "prj_timeint_mhd_fill_eta_mask: non-finite artificial eta";
     case FX_ERR_B_NONFINITE: return "non-finite cell-centered magnetic field";
     case FX_ERR_TIMEOUT: return "device wait timed out";
+    case FX_ERR_AMR_NONFINITE: return "prj_amr_mhd: non-finite magnetic field in a remesh";
     default: return "unknown device failure";
     }
 }
@@ -227,6 +235,7 @@ void free_mesh(fx_ctx *c)
     c->adj_nsteps = 0;
     c->nblocks = 0;
     c->nactive = 0;
+    c->cap = 0;
 }
 
 bool has_mesh(const fx_ctx *c) { return c && c->nblocks > 0 && c->d_W; }
@@ -355,6 +364,274 @@ int read_dt_src(fx_ctx *c, double *dt_src)
 
 size_t w_count(const fx_ctx *c) { return (size_t)FX_W_COUNT(c->nv); }
 
+/* (Re)allocates the per-block arrays for `cap` blocks.  The first `keep`
+ * blocks of every array move over from the old allocation; the rest starts
+ * at zero, so downloads of never-written entries are defined.  Every device
+ * write goes on the context stream: the stream is non-blocking, so work on
+ * the legacy default stream would not be ordered with it. */
+template <typename T>
+int regrow(fx_ctx *c, T **p, size_t per_block, int cap, int keep)
+{
+    T *old = *p;
+    T *fresh = nullptr;
+    const size_t n = per_block * (size_t)cap;
+    if (n) {
+        cudaError_t e = cudaMalloc((void **)&fresh, n * sizeof(T));
+        if (e != cudaSuccess) {
+            return set_err(c, FX_ENOMEM, "cudaMalloc of %zu bytes failed: %s", n * sizeof(T), cudaGetErrorString(e));
+        }
+        const size_t k = per_block * (size_t)keep;
+        if (k && old) {
+            FX_CUDA(c, cudaMemcpyAsync(fresh, old, k * sizeof(T), cudaMemcpyDeviceToDevice, c->stream));
+        }
+        FX_CUDA(c, cudaMemsetAsync(fresh + k, 0, (n - k) * sizeof(T), c->stream));
+    }
+    if (old) {
+        FX_CUDA(c, cudaStreamSynchronize(c->stream));
+        cudaFree(old);
+    }
+    *p = fresh;
+    return FX_SUCCESS;
+}
+
+int alloc_block_arrays(fx_ctx *c, int cap, int keep)
+{
+    int rc;
+    if ((rc = regrow(c, &c->d_blk, 1, cap, keep))) return rc;
+    if ((rc = regrow(c, &c->d_W, w_count(c), cap, keep))) return rc;
+    if ((rc = regrow(c, &c->d_flux, (size_t)FX_FLUX_COUNT(c->nv), cap, keep))) return rc;
+    if ((rc = regrow(c, &c->d_vr, (size_t)FX_VR_COUNT, cap, keep))) return rc;
+    if ((rc = regrow(c, &c->d_eos, (size_t)FX_EOS_COUNT, cap, keep))) return rc;
+    if ((rc = regrow(c, &c->d_rhs, (size_t)FX_RHS_COUNT(c->nv), cap, keep))) return rc;
+    if (c->cfg.mhd) {
+        if ((rc = regrow(c, &c->d_Bf, (size_t)FX_BF_COUNT, cap, keep))) return rc;
+        if ((rc = regrow(c, &c->d_bv1, (size_t)FX_BV_COUNT, cap, keep))) return rc;
+        if ((rc = regrow(c, &c->d_bv2, (size_t)FX_BV_COUNT, cap, keep))) return rc;
+        if ((rc = regrow(c, &c->d_emf, (size_t)FX_EMF_COUNT, cap, keep))) return rc;
+    }
+    if (c->cfg.gravity) {
+        if ((rc = regrow(c, &c->d_grav, (size_t)FX_GRAV_COUNT, cap, keep))) return rc;
+    }
+    if ((rc = regrow(c, &c->d_ids, 1, cap, 0))) return rc;
+    c->cap = cap;
+    return FX_SUCCESS;
+}
+
+/* Uploads the block geometry, the block and active lists and the compiled
+ * programs of c->plan for the mesh in c->blocks, and points the device view
+ * at the current arrays. */
+int install_tables(fx_ctx *c)
+{
+    const int nblocks = c->nblocks;
+    std::vector<FxBlockDev> hb(nblocks);
+    for (int b = 0; b < nblocks; ++b) {
+        for (int a = 0; a < 3; ++a) {
+            hb[b].xmin[a] = c->blocks[b].xmin[a];
+            hb[b].dx[a] = c->blocks[b].dx[a];
+            hb[b].area[a] = c->blocks[b].area[a];
+        }
+        hb[b].vol = c->blocks[b].vol;
+    }
+    std::vector<int> ids(nblocks);
+    for (int b = 0; b < nblocks; ++b) ids[b] = b;
+    int rc;
+    if ((rc = dev_alloc(c, &c->d_active, (size_t)c->nactive))) return rc;
+    if ((rc = dev_alloc(c, &c->d_cops, c->plan.ghost.cell_ops.size()))) return rc;
+    if ((rc = dev_alloc(c, &c->d_fops, c->plan.ghost.face_ops.size()))) return rc;
+    if ((rc = dev_alloc(c, &c->d_pops, c->plan.ghost.p_ops.size()))) return rc;
+    if ((rc = dev_alloc(c, &c->d_bops, c->plan.ghost.b_ops.size()))) return rc;
+    if ((rc = dev_alloc(c, &c->d_fcorr, c->plan.flux_corr.size()))) return rc;
+    if ((rc = dev_alloc(c, &c->d_ecorr, c->plan.emf_corr.size()))) return rc;
+    cudaStream_t s = c->stream;
+    const cudaMemcpyKind h2d = cudaMemcpyHostToDevice;
+    FX_CUDA(c, cudaMemcpyAsync(c->d_blk, hb.data(), (size_t)nblocks * sizeof(FxBlockDev), h2d, s));
+    FX_CUDA(c, cudaMemcpyAsync(c->d_ids, ids.data(), (size_t)nblocks * sizeof(int), h2d, s));
+    if (c->nactive) {
+        FX_CUDA(c, cudaMemcpyAsync(c->d_active, c->plan.active.data(), (size_t)c->nactive * sizeof(int), h2d, s));
+    }
+    const FxProgram &g = c->plan.ghost;
+    if (!g.cell_ops.empty()) {
+        FX_CUDA(c, cudaMemcpyAsync(c->d_cops, g.cell_ops.data(), g.cell_ops.size() * sizeof(FxGop), h2d, s));
+    }
+    if (!g.face_ops.empty()) {
+        FX_CUDA(c, cudaMemcpyAsync(c->d_fops, g.face_ops.data(), g.face_ops.size() * sizeof(FxGop), h2d, s));
+    }
+    if (!g.p_ops.empty()) {
+        FX_CUDA(c, cudaMemcpyAsync(c->d_pops, g.p_ops.data(), g.p_ops.size() * sizeof(FxPop), h2d, s));
+    }
+    if (!g.b_ops.empty()) {
+        FX_CUDA(c, cudaMemcpyAsync(c->d_bops, g.b_ops.data(), g.b_ops.size() * sizeof(FxBop), h2d, s));
+    }
+    if (!c->plan.flux_corr.empty()) {
+        FX_CUDA(c, cudaMemcpyAsync(c->d_fcorr, c->plan.flux_corr.data(),
+            c->plan.flux_corr.size() * sizeof(FxCorr), h2d, s));
+    }
+    if (!c->plan.emf_corr.empty()) {
+        FX_CUDA(c, cudaMemcpyAsync(c->d_ecorr, c->plan.emf_corr.data(),
+            c->plan.emf_corr.size() * sizeof(FxCorr), h2d, s));
+    }
+    /* the host vectors must outlive the copies */
+    FX_CUDA(c, cudaStreamSynchronize(s));
+    c->D.nblocks = nblocks;
+    c->D.blk = c->d_blk;
+    c->D.W = c->d_W;
+    c->D.Bf = c->d_Bf;
+    c->D.flux = c->d_flux;
+    c->D.vr = c->d_vr;
+    c->D.bv1 = c->d_bv1;
+    c->D.bv2 = c->d_bv2;
+    c->D.emf = c->d_emf;
+    c->D.eos = c->d_eos;
+    c->D.rhs = c->d_rhs;
+    c->D.grav = c->d_grav;
+    return FX_SUCCESS;
+}
+
+} /* namespace */
+
+/* dynamic AMR helpers */
+namespace {
+
+bool amr_config_ok(const fx_amr_config &a, std::string *why)
+{
+    for (int d = 0; d < 3; ++d) {
+        if (a.root_nx[d] <= 0) {
+            *why = "root_nx must be positive";
+            return false;
+        }
+    }
+    for (int n = 0; n < FX_AMR_N; ++n) {
+        const fx_amr_criterion &k = a.crit[n];
+        if (!k.set) continue;
+        if (k.estimator < FX_AMR_LOEHNER || k.estimator > FX_AMR_FRACTIONAL_JUMP) {
+            *why = "unsupported estimator " + std::to_string(k.estimator);
+            return false;
+        }
+        if (k.lohner_var < 0 || k.lohner_var > 2 || k.jump_var < 0 || k.jump_var > 1) {
+            *why = "bad estimator variable";
+            return false;
+        }
+    }
+    return true;
+}
+
+FxAmrTagCfg tag_config(const fx_amr_config &a)
+{
+    FxAmrTagCfg t;
+    std::memset(&t, 0, sizeof(t));
+    for (int n = 0; n < FX_AMR_N; ++n) {
+        const fx_amr_criterion &k = a.crit[n];
+        if (!k.set) continue;
+        const int m = t.ncrit++;
+        t.est[m] = k.estimator;
+        t.var[m] = k.estimator == FX_AMR_FRACTIONAL_JUMP ? k.jump_var : k.lohner_var;
+        t.rthr[m] = k.refine_thresh;
+        t.dthr[m] = k.derefine_thresh;
+        t.eps[m] = k.lohner_eps;
+        if (k.derefine_thresh > 0.0) t.has_derefine = 1;
+    }
+    t.reach = a.reach_density;
+    return t;
+}
+
+/* device buffer holding a copy of a host vector for the duration of a call */
+template <typename T>
+struct DevVec {
+    T *p = nullptr;
+    ~DevVec() { cudaFree(p); }
+    int load(fx_ctx *c, const std::vector<T> &v)
+    {
+        if (v.empty()) return FX_SUCCESS;
+        FX_CUDA(c, cudaMalloc((void **)&p, v.size() * sizeof(T)));
+        FX_CUDA(c, cudaMemcpyAsync(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, c->stream));
+        return FX_SUCCESS;
+    }
+};
+
+/* pass 1 of prj_amr_tag on the device: three int32 per block entry */
+int amr_votes(fx_ctx *c, std::vector<int32_t> &votes)
+{
+    const int n = c->nactive;
+    std::vector<int> hp(n);
+    for (int i = 0; i < n; ++i) hp[i] = c->blocks[c->plan.active[i]].parent >= 0 ? 1 : 0;
+    DevVec<int> d_hp;
+    DevVec<int32_t> d_votes;
+    int rc;
+    if ((rc = d_hp.load(c, hp))) return rc;
+    std::vector<int32_t> hv((size_t)3 * n, 0);
+    if ((rc = d_votes.load(c, hv))) return rc;
+    fx_launch_amr_tag(c->D, c->d_active, d_hp.p, n, tag_config(c->amr), d_votes.p, c->stream);
+    if (n) {
+        FX_CUDA(c, cudaMemcpyAsync(hv.data(), d_votes.p, hv.size() * sizeof(int32_t), cudaMemcpyDeviceToHost,
+            c->stream));
+    }
+    if ((rc = sync_and_check(c))) return rc;
+    votes.assign((size_t)3 * c->nblocks, 0);
+    for (int i = 0; i < n; ++i) {
+        const int b = c->plan.active[i];
+        for (int q = 0; q < 3; ++q) votes[3 * b + q] = hv[3 * i + q];
+    }
+    return FX_SUCCESS;
+}
+
+/* Toth-Roe groups that prolong a new child's faces from its parent: 8^3
+ * coarse cells of the child's octant, outer faces kept where the child
+ * copied a finer neighbour's layer, every face stored once */
+void child_groups(const FxAmrRefine &r, std::vector<FxPop> &out)
+{
+    const int o[3] = {(r.oct & 1) * 8, ((r.oct >> 1) & 1) * 8, ((r.oct >> 2) & 1) * 8};
+    for (int ci = o[0]; ci < o[0] + 8; ++ci) {
+        for (int cj = o[1]; cj < o[1] + 8; ++cj) {
+            for (int ck = o[2]; ck < o[2] + 8; ++ck) {
+                const int f[3] = {2 * (ci - o[0]), 2 * (cj - o[1]), 2 * (ck - o[2])};
+                FxPop p;
+                std::memset(&p, 0, sizeof(p));
+                p.fine = r.child;
+                p.coarse = r.parent;
+                p.pos = (f[0] + 2) | ((f[1] + 2) << 5) | ((f[2] + 2) << 10) | ((ci + 2) << 15) |
+                    ((cj + 2) << 20) | ((ck + 2) << 25);
+                for (int d = 0; d < 3; ++d) {
+                    for (int side = 0; side < 2; ++side) {
+                        const int x = f[d] + 2 * side;
+                        const bool keep = (x == FX_BS && r.copy_src[2 * d + 1] >= 0) ||
+                            (x == 0 && r.copy_src[2 * d] >= 0);
+                        const bool store = side == 0 || x == FX_BS;
+                        for (int q = 0; q < 4; ++q) {
+                            const int bit = 8 * d + 4 * side + q;
+                            if (keep) p.keep |= 1 << bit;
+                            else if (store) p.owrite |= 1 << bit;
+                        }
+                    }
+                }
+                p.iwrite = 0xFFF;
+                out.push_back(p);
+            }
+        }
+    }
+}
+
+void drop_adjoint(fx_ctx *c)
+{
+    cudaFree(c->d_ckW);
+    cudaFree(c->d_ckBf);
+    cudaFree(c->d_ckVr);
+    cudaFree(c->d_adj_csrc);
+    cudaFree(c->d_adj_fsrc);
+    cudaFree(c->d_adj_ents);
+    cudaFree(c->d_Wb);
+    cudaFree(c->d_Bfb);
+    cudaFree(c->d_G);
+    cudaFree(c->d_bvb1);
+    cudaFree(c->d_bvb2);
+    cudaFree(c->d_Eb);
+    c->d_ckW = c->d_ckBf = c->d_ckVr = nullptr;
+    c->d_adj_csrc = c->d_adj_fsrc = nullptr;
+    c->d_adj_ents = nullptr;
+    c->d_Wb = c->d_Bfb = c->d_G = c->d_bvb1 = c->d_bvb2 = c->d_Eb = nullptr;
+    c->adj_ghost_ready = false;
+    c->adj_nsteps = 0;
+}
+
 } /* namespace */
 
 /* ========================================================================== */
@@ -471,105 +748,9 @@ int fx_set_mesh(fx_ctx *c, int nblocks, const fx_block_desc *blocks)
     c->blocks.assign(blocks, blocks + nblocks);
     c->nblocks = nblocks;
     c->nactive = (int)c->plan.active.size();
-
-    std::vector<FxBlockDev> hb(nblocks);
-    for (int b = 0; b < nblocks; ++b) {
-        for (int a = 0; a < 3; ++a) {
-            hb[b].xmin[a] = blocks[b].xmin[a];
-            hb[b].dx[a] = blocks[b].dx[a];
-            hb[b].area[a] = blocks[b].area[a];
-        }
-        hb[b].vol = blocks[b].vol;
-    }
-    std::vector<int> ids(nblocks);
-    for (int b = 0; b < nblocks; ++b) ids[b] = b;
-
-    const size_t nb = (size_t)nblocks;
     int rc;
-    if ((rc = dev_alloc(c, &c->d_blk, nb))) return rc;
-    if ((rc = dev_alloc(c, &c->d_W, nb * w_count(c)))) return rc;
-    if ((rc = dev_alloc(c, &c->d_flux, nb * FX_FLUX_COUNT(c->nv)))) return rc;
-    if ((rc = dev_alloc(c, &c->d_vr, nb * FX_VR_COUNT))) return rc;
-    if ((rc = dev_alloc(c, &c->d_eos, nb * FX_EOS_COUNT))) return rc;
-    if ((rc = dev_alloc(c, &c->d_rhs, nb * FX_RHS_COUNT(c->nv)))) return rc;
-    if (c->cfg.mhd) {
-        if ((rc = dev_alloc(c, &c->d_Bf, nb * FX_BF_COUNT))) return rc;
-        if ((rc = dev_alloc(c, &c->d_bv1, nb * FX_BV_COUNT))) return rc;
-        if ((rc = dev_alloc(c, &c->d_bv2, nb * FX_BV_COUNT))) return rc;
-        if ((rc = dev_alloc(c, &c->d_emf, nb * FX_EMF_COUNT))) return rc;
-    }
-    if (c->cfg.gravity) {
-        if ((rc = dev_alloc(c, &c->d_grav, nb * FX_GRAV_COUNT))) return rc;
-        FX_CUDA(c, cudaMemsetAsync(c->d_grav, 0, nb * FX_GRAV_COUNT * sizeof(double), c->stream));
-    }
-    if ((rc = dev_alloc(c, &c->d_ids, nb))) return rc;
-    if ((rc = dev_alloc(c, &c->d_active, (size_t)c->nactive))) return rc;
-    if ((rc = dev_alloc(c, &c->d_cops, c->plan.ghost.cell_ops.size()))) return rc;
-    if ((rc = dev_alloc(c, &c->d_fops, c->plan.ghost.face_ops.size()))) return rc;
-    if ((rc = dev_alloc(c, &c->d_pops, c->plan.ghost.p_ops.size()))) return rc;
-    if ((rc = dev_alloc(c, &c->d_bops, c->plan.ghost.b_ops.size()))) return rc;
-    if ((rc = dev_alloc(c, &c->d_fcorr, c->plan.flux_corr.size()))) return rc;
-    if ((rc = dev_alloc(c, &c->d_ecorr, c->plan.emf_corr.size()))) return rc;
-
-    /* scratch starts at zero so downloads of never-written entries are
-     * defined.  Every device write goes on the context stream: the stream is
-     * non-blocking, so work on the legacy default stream would not be ordered
-     * with it. */
-    cudaStream_t s = c->stream;
-    FX_CUDA(c, cudaMemsetAsync(c->d_W, 0, nb * w_count(c) * sizeof(double), s));
-    FX_CUDA(c, cudaMemsetAsync(c->d_flux, 0, nb * FX_FLUX_COUNT(c->nv) * sizeof(double), s));
-    FX_CUDA(c, cudaMemsetAsync(c->d_vr, 0, nb * FX_VR_COUNT * sizeof(double), s));
-    FX_CUDA(c, cudaMemsetAsync(c->d_eos, 0, nb * FX_EOS_COUNT * sizeof(double), s));
-    FX_CUDA(c, cudaMemsetAsync(c->d_rhs, 0, nb * FX_RHS_COUNT(c->nv) * sizeof(double), s));
-    if (c->cfg.mhd) {
-        FX_CUDA(c, cudaMemsetAsync(c->d_Bf, 0, nb * FX_BF_COUNT * sizeof(double), s));
-        FX_CUDA(c, cudaMemsetAsync(c->d_bv1, 0, nb * FX_BV_COUNT * sizeof(double), s));
-        FX_CUDA(c, cudaMemsetAsync(c->d_bv2, 0, nb * FX_BV_COUNT * sizeof(double), s));
-        FX_CUDA(c, cudaMemsetAsync(c->d_emf, 0, nb * FX_EMF_COUNT * sizeof(double), s));
-    }
-    const cudaMemcpyKind h2d = cudaMemcpyHostToDevice;
-    FX_CUDA(c, cudaMemcpyAsync(c->d_blk, hb.data(), nb * sizeof(FxBlockDev), h2d, s));
-    FX_CUDA(c, cudaMemcpyAsync(c->d_ids, ids.data(), nb * sizeof(int), h2d, s));
-    if (c->nactive) {
-        FX_CUDA(c, cudaMemcpyAsync(c->d_active, c->plan.active.data(), (size_t)c->nactive * sizeof(int), h2d, s));
-    }
-    {
-        const FxProgram &g = c->plan.ghost;
-        if (!g.cell_ops.empty()) {
-            FX_CUDA(c, cudaMemcpyAsync(c->d_cops, g.cell_ops.data(), g.cell_ops.size() * sizeof(FxGop), h2d, s));
-        }
-        if (!g.face_ops.empty()) {
-            FX_CUDA(c, cudaMemcpyAsync(c->d_fops, g.face_ops.data(), g.face_ops.size() * sizeof(FxGop), h2d, s));
-        }
-        if (!g.p_ops.empty()) {
-            FX_CUDA(c, cudaMemcpyAsync(c->d_pops, g.p_ops.data(), g.p_ops.size() * sizeof(FxPop), h2d, s));
-        }
-        if (!g.b_ops.empty()) {
-            FX_CUDA(c, cudaMemcpyAsync(c->d_bops, g.b_ops.data(), g.b_ops.size() * sizeof(FxBop), h2d, s));
-        }
-    }
-    if (!c->plan.flux_corr.empty()) {
-        FX_CUDA(c, cudaMemcpyAsync(c->d_fcorr, c->plan.flux_corr.data(),
-            c->plan.flux_corr.size() * sizeof(FxCorr), h2d, s));
-    }
-    if (!c->plan.emf_corr.empty()) {
-        FX_CUDA(c, cudaMemcpyAsync(c->d_ecorr, c->plan.emf_corr.data(),
-            c->plan.emf_corr.size() * sizeof(FxCorr), h2d, s));
-    }
-    /* the host vectors must outlive the copies */
-    FX_CUDA(c, cudaStreamSynchronize(s));
-    c->D.nblocks = nblocks;
-    c->D.blk = c->d_blk;
-    c->D.W = c->d_W;
-    c->D.Bf = c->d_Bf;
-    c->D.flux = c->d_flux;
-    c->D.vr = c->d_vr;
-    c->D.bv1 = c->d_bv1;
-    c->D.bv2 = c->d_bv2;
-    c->D.emf = c->d_emf;
-    c->D.eos = c->d_eos;
-    c->D.rhs = c->d_rhs;
-    c->D.grav = c->d_grav;
+    if ((rc = alloc_block_arrays(c, nblocks, 0))) return rc;
+    if ((rc = install_tables(c))) return rc;
     c->last_slot = 0;
     return FX_SUCCESS;
 }
@@ -1091,6 +1272,225 @@ int fx_set_flux_shape(fx_ctx *c, int variant)
     }
     c->D.flux_variant = variant;
     free_graphs(c);
+    return FX_SUCCESS;
+}
+
+/* ---- dynamic AMR ---------------------------------------------------------------- */
+
+int fx_amr_configure(fx_ctx *c, const fx_amr_config *amr)
+{
+    if (!c || !amr) return c ? set_err(c, FX_EINVAL, "fx_amr_configure: null config") : FX_EINVAL;
+    std::string why;
+    if (!amr_config_ok(*amr, &why)) return set_err(c, FX_EINVAL, "fx_amr_configure: %s", why.c_str());
+    c->amr = *amr;
+    c->amr_set = true;
+    return FX_SUCCESS;
+}
+
+int fx_amr_tag(fx_ctx *c, int32_t *refine_flag)
+{
+    if (!has_mesh(c)) return c ? set_err(c, FX_ENOMESH, "no mesh") : FX_EINVAL;
+    if (!c->amr_set) return set_err(c, FX_EINVAL, "fx_amr_tag: fx_amr_configure first");
+    if (!refine_flag) return set_err(c, FX_EINVAL, "fx_amr_tag: null output");
+    std::vector<int32_t> votes;
+    int rc;
+    fx_launch_set_dt(c->D, 0.0, c->stream);
+    if ((rc = amr_votes(c, votes))) return rc;
+    fx_amr_flags(c->amr, c->nblocks, c->blocks.data(), votes.data(), refine_flag);
+    return FX_SUCCESS;
+}
+
+int fx_amr_adapt(fx_ctx *c, int *changed)
+{
+    if (!has_mesh(c)) return c ? set_err(c, FX_ENOMESH, "no mesh") : FX_EINVAL;
+    if (!c->amr_set) return set_err(c, FX_EINVAL, "fx_amr_adapt: fx_amr_configure first");
+    if (changed) *changed = 0;
+    int rc;
+    fx_launch_set_dt(c->D, 0.0, c->stream);
+    std::vector<int32_t> votes;
+    if ((rc = amr_votes(c, votes))) return rc;
+    FxAmrResult res;
+    std::string err;
+    const int capacity = std::min(c->amr.max_blocks > 0 ? c->amr.max_blocks : 65535, 65535);
+    if ((rc = fx_amr_remesh(c->cfg, c->amr, c->nblocks, c->blocks.data(), votes.data(), capacity, res, &err))) {
+        return set_err(c, rc, "fx_amr_adapt: %s", err.c_str());
+    }
+    if (!res.changed) {
+        return FX_SUCCESS;
+    }
+    const int nb = (int)res.blocks.size();
+    if (nb > c->cap) {
+        const int grown = std::min(std::max(nb, c->cap + c->cap / 4), capacity);
+        if ((rc = alloc_block_arrays(c, grown, c->nblocks))) return rc;
+        c->D.blk = c->d_blk;
+        c->D.W = c->d_W;
+        c->D.Bf = c->d_Bf;
+        c->D.flux = c->d_flux;
+        c->D.vr = c->d_vr;
+        c->D.bv1 = c->d_bv1;
+        c->D.bv2 = c->d_bv2;
+        c->D.emf = c->d_emf;
+        c->D.eos = c->d_eos;
+        c->D.rhs = c->d_rhs;
+        c->D.grav = c->d_grav;
+    }
+    /* geometry of the new block list, read by the data kernels */
+    std::vector<FxBlockDev> hb(nb);
+    for (int b = 0; b < nb; ++b) {
+        for (int a = 0; a < 3; ++a) {
+            hb[b].xmin[a] = res.blocks[b].xmin[a];
+            hb[b].dx[a] = res.blocks[b].dx[a];
+            hb[b].area[a] = res.blocks[b].area[a];
+        }
+        hb[b].vol = res.blocks[b].vol;
+    }
+    FX_CUDA(c, cudaMemcpyAsync(c->d_blk, hb.data(), (size_t)nb * sizeof(FxBlockDev), cudaMemcpyHostToDevice,
+        c->stream));
+    c->D.nblocks = nb;
+
+    /* device jobs */
+    std::vector<int> children;
+    std::vector<FxAmrChildJob> cjobs;
+    std::vector<FxAmrCopyJob> copies;
+    std::vector<FxPop> pops;
+    for (const FxAmrRefine &r : res.refine) {
+        children.push_back(r.child);
+        FxAmrChildJob j;
+        j.child = r.child;
+        j.parent = r.parent;
+        j.oct = r.oct;
+        j.pad = 0;
+        cjobs.push_back(j);
+        if (c->cfg.mhd) {
+            for (int q = 0; q < 6; ++q) {
+                if (r.copy_src[q] < 0) continue;
+                FxAmrCopyJob cp;
+                cp.child = r.child;
+                cp.src = r.copy_src[q];
+                cp.dir = q / 2;
+                cp.side = q % 2;
+                copies.push_back(cp);
+            }
+            child_groups(r, pops);
+        }
+    }
+    std::vector<FxAmrParentJob> pjobs;
+    for (const FxAmrCoarsen &k : res.coarsen) {
+        FxAmrParentJob j;
+        std::memset(&j, 0, sizeof(j));
+        j.parent = k.parent;
+        for (int o = 0; o < 8; ++o) j.children[o] = k.children[o];
+        pjobs.push_back(j);
+    }
+    DevVec<int> d_children;
+    DevVec<FxAmrChildJob> d_cjobs;
+    DevVec<FxAmrCopyJob> d_copies;
+    DevVec<FxPop> d_pops;
+    DevVec<FxAmrParentJob> d_pjobs;
+    if ((rc = d_children.load(c, children))) return rc;
+    if ((rc = d_cjobs.load(c, cjobs))) return rc;
+    if ((rc = d_copies.load(c, copies))) return rc;
+    if ((rc = d_pops.load(c, pops))) return rc;
+    if ((rc = d_pjobs.load(c, pjobs))) return rc;
+    const double floor = c->amr.E_floor;
+    const size_t ninj = floor > 0.0 ? (cjobs.size() + pjobs.size()) * (size_t)(FX_BS * FX_BS * FX_BS) : 0;
+    double *d_inj = nullptr;
+    if (ninj) FX_CUDA(c, cudaMalloc((void **)&d_inj, ninj * sizeof(double)));
+    cudaStream_t s = c->stream;
+    fx_launch_amr_zero(c->D, d_children.p, (int)children.size(), s);
+    if (c->cfg.mhd) {
+        fx_launch_amr_copy_faces(c->D, d_copies.p, (int)copies.size(), s);
+        fx_launch_prolong_groups(c->D, d_pops.p, (int)pops.size(), 0, s);
+        fx_launch_prolong_groups(c->D, d_pops.p, (int)pops.size(), 1, s);
+    }
+    fx_launch_amr_prolong_cells(c->D, d_cjobs.p, (int)cjobs.size(), floor, d_inj, s);
+    fx_launch_amr_restrict_faces(c->D, d_pjobs.p, (int)pjobs.size(), s);
+    fx_launch_amr_restrict_cells(c->D, d_pjobs.p, (int)pjobs.size(), floor,
+        d_inj ? d_inj + cjobs.size() * (size_t)(FX_BS * FX_BS * FX_BS) : nullptr, s);
+    FX_CUDA(c, cudaGetLastError());
+
+    /* the ghost fill of the new mesh compiles while the device moves data */
+    FxPlan plan;
+    if (!fx_build_plan(c->cfg, nb, res.blocks.data(), plan, &err)) {
+        cudaFree(d_inj);
+        return set_err(c, FX_EINVAL, "fx_amr_adapt: %s", err.c_str());
+    }
+    free_graphs(c);
+    drop_adjoint(c);
+    c->plan = std::move(plan);
+    c->blocks = std::move(res.blocks);
+    c->nblocks = nb;
+    c->nactive = (int)c->plan.active.size();
+    if ((rc = install_tables(c))) {
+        cudaFree(d_inj);
+        return rc;
+    }
+    /* the driver's refill of a changed mesh (src/main.c:599-606) */
+    fx_launch_set_dt(c->D, 0.0, s);
+    fx_launch_eos_fill(c->D, c->d_active, c->nactive, 0, 1, s);
+    ghost_fill(c, 0);
+    fx_launch_eos_fill(c->D, c->d_active, c->nactive, 0, 0, s);
+    c->last_slot = 0;
+    if (ninj) {
+        /* prj_sync_primitive_from_conserved sums the floor's energy over the
+         * regenerated blocks in block order, cells in (i, j, k) order */
+        std::vector<double> inj(ninj);
+        FX_CUDA(c, cudaMemcpyAsync(inj.data(), d_inj, ninj * sizeof(double), cudaMemcpyDeviceToHost, s));
+        rc = sync_and_check(c);
+        cudaFree(d_inj);
+        if (rc) return rc;
+        std::vector<std::pair<int, size_t>> order;
+        for (size_t j = 0; j < cjobs.size(); ++j) order.emplace_back(cjobs[j].child, j);
+        for (size_t j = 0; j < pjobs.size(); ++j) order.emplace_back(pjobs[j].parent, cjobs.size() + j);
+        std::sort(order.begin(), order.end());
+        double local = 0.0;
+        for (const auto &e : order) {
+            const double *v = inj.data() + e.second * (size_t)(FX_BS * FX_BS * FX_BS);
+            for (int q = 0; q < FX_BS * FX_BS * FX_BS; ++q) local += v[q];
+        }
+        if (local != 0.0) c->E_injected += local;
+    } else if ((rc = sync_and_check(c))) {
+        return rc;
+    }
+    if (changed) *changed = 1;
+    return FX_SUCCESS;
+}
+
+int fx_get_mesh(fx_ctx *c, int capacity, fx_block_desc *out, int *nblocks)
+{
+    if (!c || !nblocks) return c ? set_err(c, FX_EINVAL, "fx_get_mesh: null argument") : FX_EINVAL;
+    *nblocks = c->nblocks;
+    if (out && capacity >= c->nblocks && c->nblocks) {
+        std::memcpy(out, c->blocks.data(), (size_t)c->nblocks * sizeof(fx_block_desc));
+    }
+    return FX_SUCCESS;
+}
+
+int fx_amr_energy_injected(fx_ctx *c, double *e)
+{
+    if (!c || !e) return c ? set_err(c, FX_EINVAL, "null argument") : FX_EINVAL;
+    *e = c->E_injected;
+    return FX_SUCCESS;
+}
+
+int fx_amr_remesh_host(const fx_config *cfg, const fx_amr_config *amr, int nblocks, const fx_block_desc *in,
+    const int32_t *votes, int32_t *flags, int capacity, fx_block_desc *out, int *nout)
+{
+    if (!cfg || !amr || nblocks <= 0 || !in || !votes || !out || !nout || capacity <= 0) return FX_EINVAL;
+    std::string why;
+    if (!amr_config_ok(*amr, &why)) return FX_EINVAL;
+    FxAmrResult res;
+    const int rc = fx_amr_remesh(*cfg, *amr, nblocks, in, votes, capacity, res, &why);
+    if (rc) return rc;
+    if (flags) std::memcpy(flags, res.flags.data(), (size_t)nblocks * sizeof(int32_t));
+    if (!res.changed) {
+        std::memcpy(out, in, (size_t)nblocks * sizeof(fx_block_desc));
+        *nout = nblocks;
+        return FX_SUCCESS;
+    }
+    if ((int)res.blocks.size() > capacity) return FX_ETOOBIG;
+    std::memcpy(out, res.blocks.data(), res.blocks.size() * sizeof(fx_block_desc));
+    *nout = (int)res.blocks.size();
     return FX_SUCCESS;
 }
 

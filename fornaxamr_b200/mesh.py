@@ -339,6 +339,10 @@ def to_desc(blocks: Sequence[Block]) -> "C.Array":
         area = b.area
         for a in range(3):
             d.area[a] = area[a]
+        d.parent = b.parent
+        for o in range(8):
+            d.children[o] = b.children[o]
+        d.can_refine = 1
         for s, sl in enumerate(b.slots):
             ds = d.slot[s]
             ds.id = sl.id
@@ -352,15 +356,26 @@ def to_desc(blocks: Sequence[Block]) -> "C.Array":
     return arr
 
 
-def desc_from_arrays(ints: np.ndarray, geom: np.ndarray, slots: np.ndarray) -> "C.Array":
+def desc_from_arrays(ints: np.ndarray, geom: np.ndarray, slots: np.ndarray, tree=None) -> "C.Array":
     """fx_block_desc array from packed arrays: ints[n] = (id, level, active,
     rank), geom[n] = (xmin3, xmax3, dx3, vol, area3), slots[n] = 56 x 15
-    (id, rel_level, type, send_start3, send_end3, recv_start3, recv_end3)."""
+    (id, rel_level, type, send_start3, send_end3, recv_start3, recv_end3),
+    tree[n] (optional) = (parent, children8[, refine_flag, can_refine])."""
     nb = ints.shape[0]
     arr = (FxBlockDesc * nb)()
     for n in range(nb):
         d = arr[n]
         d.id, d.level, d.active, d.rank = (int(x) for x in ints[n, :4])
+        if tree is not None:
+            d.parent = int(tree[n, 0])
+            for o in range(8):
+                d.children[o] = int(tree[n, 1 + o])
+            d.can_refine = int(tree[n, 10]) if tree.shape[1] > 10 else 1
+        else:
+            d.parent = -1
+            for o in range(8):
+                d.children[o] = -1
+            d.can_refine = 1
         for a in range(3):
             d.xmin[a] = float(geom[n, a])
             d.xmax[a] = float(geom[n, 3 + a])
@@ -377,6 +392,17 @@ def desc_from_arrays(ints: np.ndarray, geom: np.ndarray, slots: np.ndarray) -> "
                 ds.recv_loc_start[a] = int(row[9 + a])
                 ds.recv_loc_end[a] = int(row[12 + a])
     return arr
+
+
+def desc_tree(arr) -> np.ndarray:
+    """(parent, children8, can_refine) per entry, int64 [n, 10]."""
+    out = np.zeros((len(arr), 10), dtype=np.int64)
+    for n in range(len(arr)):
+        d = arr[n]
+        out[n, 0] = d.parent
+        out[n, 1:9] = d.children[:]
+        out[n, 9] = d.can_refine
+    return out
 
 
 def desc_to_arrays(arr) -> tuple:

@@ -83,8 +83,8 @@ typedef struct fx_slot {
     int8_t recv_loc_end[3];
 } fx_slot;
 
-/* One block of the mesh (prj_block, src/prj_types.h:151-213: geometry and
- * the 56 neighbour slots). */
+/* One block of the mesh (prj_block, src/prj_types.h:151-213: geometry,
+ * the 56 neighbour slots and the refinement tree). */
 typedef struct fx_block_desc {
     int32_t id;         /* < 0: unused entry */
     int32_t level;
@@ -96,6 +96,9 @@ typedef struct fx_block_desc {
     double vol;
     double area[3];
     fx_slot slot[56];
+    int32_t parent;     /* parent block index, -1 for root blocks */
+    int32_t children[8];/* child block indices in octant order (x fastest), -1 if none */
+    int32_t can_refine; /* prj_block.can_refine: 0 keeps the block from refining */
 } fx_block_desc;
 
 /* Run-time configuration (compile-time switches of the reference). */
@@ -235,6 +238,72 @@ int fx_run(fx_ctx *ctx, int form, int nsteps, double cfl, double dt_factor, doub
  * give wrong results, so order them on one stream or serialise them. */
 int fx_calc_dt_noalloc(const double *W, int mhd, const double *dx, const int *blocks, int nlist,
     double gamma, double cfl, void *stream, double *dt);
+
+/* ---- dynamic AMR ---------------------------------------------------------------- */
+
+/* Refinement criteria: the amr_* arrays of prj_mesh (src/prj_types.h:482-490),
+ * PRJ_AMR_N = 4 entries, summed as sum_n indicator_n / thresh_n per cell. */
+#define FX_AMR_N 4
+#define FX_AMR_LOEHNER 0                /* PRJ_AMR_ESTIMATOR_LOEHNER */
+#define FX_AMR_VELOCITY 1               /* PRJ_AMR_ESTIMATOR_VELOCITY */
+#define FX_AMR_PRESSURE_SCALE_HEIGHT 2  /* PRJ_AMR_ESTIMATOR_PRESSURE_SCALE_HEIGHT */
+#define FX_AMR_FRACTIONAL_JUMP 3        /* PRJ_AMR_ESTIMATOR_FRACTIONAL_JUMP */
+#define FX_AMR_VAR_DENSITY 0            /* Loehner / jump variable: density */
+#define FX_AMR_VAR_PRESSURE 1           /* gas + magnetic pressure */
+#define FX_AMR_VAR_TEMPERATURE 2        /* Loehner only */
+
+typedef struct fx_amr_criterion {
+    int32_t set;             /* amr_criterion_set */
+    int32_t estimator;       /* FX_AMR_LOEHNER .. FX_AMR_FRACTIONAL_JUMP */
+    int32_t lohner_var;      /* amr_lohner_var */
+    int32_t jump_var;        /* amr_fractional_jump_var */
+    double refine_thresh;    /* <= 0: not a refinement criterion */
+    double derefine_thresh;  /* <= 0: not a derefinement criterion */
+    double lohner_eps;
+} fx_amr_criterion;
+
+typedef struct fx_amr_config {
+    int32_t root_nx[3];      /* prj_mesh.root_nx: root blocks per axis */
+    int32_t max_level;       /* < 0: unlimited */
+    int32_t max_blocks;      /* prj_mesh.nblocks_max: capacity of the block array */
+    int32_t pad;
+    double min_dx;           /* <= 0: no cell-size floor */
+    double reach_density;    /* amr_reach_highest_level_at_density, <= 0: off */
+    double E_floor;          /* internal-energy floor after a remesh, <= 0: off */
+    fx_amr_criterion crit[FX_AMR_N];
+} fx_amr_config;
+
+/* Sets the refinement parameters and the refinement tree of the mirrored
+ * mesh (the parent/children/can_refine of the last fx_set_mesh).  The
+ * Barth-Jespersen prolongation limiter (use_BJ), the angular-resolution cap
+ * and the Z4c estimator are not supported. */
+int fx_amr_configure(fx_ctx *ctx, const fx_amr_config *amr);
+/* prj_amr_tag (src/prj_amr.c:1581-1782) on the device state (W slot 0 after a
+ * step or a fill): refine_flag[b] for every block entry (+1 refine, -1
+ * derefine, 0 keep) after the per-block caps, before 2:1 balance. */
+int fx_amr_tag(fx_ctx *ctx, int32_t *refine_flag);
+/* prj_amr_adapt (src/prj_amr.c:2576-2706) followed by the driver's refill of
+ * a changed mesh (src/main.c:599-606): tags on the device, balances and
+ * rebuilds the block tree and neighbour slots on the host, prolongs and
+ * restricts the cell and face data on the device, recompiles the ghost fill
+ * and fills the ghosts of slot 0.  *changed = 1 if the mesh changed. */
+int fx_amr_adapt(fx_ctx *ctx, int *changed);
+/* The mirrored mesh: *nblocks entries (unused ones have id < 0) are written
+ * to out if capacity allows; *nblocks is always set. */
+int fx_get_mesh(fx_ctx *ctx, int capacity, fx_block_desc *out, int *nblocks);
+/* Energy added by the E_floor of all remeshes so far (eos->E_injected). */
+int fx_amr_energy_injected(fx_ctx *ctx, double *e);
+
+/* Host-only remesh (no device): the block-tree half of prj_amr_adapt for
+ * given per-block tag votes.  votes[3 b .. 3 b + 2] = refine vote (0/1),
+ * derefine vote (0/-1) and the boundary side mask of block b, as pass 1 of
+ * prj_amr_tag leaves them.  flags (nblocks, may be NULL) receives the tag
+ * result (after the caps); out (capacity entries) the adapted mesh, *nout
+ * its block count.  Returns FX_ETOOBIG when the mesh outgrows
+ * amr->max_blocks or capacity. */
+int fx_amr_remesh_host(const fx_config *cfg, const fx_amr_config *amr, int nblocks,
+    const fx_block_desc *in, const int32_t *votes, int32_t *flags, int capacity, fx_block_desc *out,
+    int *nout);
 
 /* ---- measurement --------------------------------------------------------------- */
 

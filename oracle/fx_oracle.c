@@ -867,3 +867,272 @@ double fxo_step_block(int nv, double gamma, const double *dx, double *W, double 
     }
     return dt_src;
 }
+
+/* ---- dynamic AMR: pass 1 of prj_amr_tag (src/prj_amr.c:1611-1705) ------- */
+
+/* one refinement criterion, the amr_* arrays of prj_mesh (src/prj_types.h:482-490) */
+typedef struct fxo_amr_crit {
+    int set;
+    int estimator;   /* 0 Loehner, 1 velocity, 2 pressure scale height, 3 fractional jump */
+    int lohner_var;  /* 0 density, 1 pressure, 2 temperature */
+    int jump_var;    /* 0 density, 1 pressure */
+    double refine_thresh;
+    double derefine_thresh;
+    double lohner_eps;
+} fxo_amr_crit;
+
+typedef struct tagblk {
+    int nv;
+    double gamma;
+    const double *W;      /* slot 0 is read */
+    const double *grav;   /* 3 x 8000 or NULL */
+    const double *dx;
+} tagblk;
+
+/* storage index clamp of prj_amr_clamp_storage_index (src/prj_amr.c:713-722) */
+static int clampi(int i)
+{
+    if (i < -NG) return -NG;
+    if (i >= BS + NG) return BS + NG - 1;
+    return i;
+}
+
+static double t_prim(const tagblk *t, int v, int i, int j, int k)
+{
+    return t->W[(size_t)v * PLANE + lidx(clampi(i), clampi(j), clampi(k))];
+}
+
+/* eosvar pressure / temperature / gamma of the ideal gas at a cell (what
+ * prj_eos_fill_mesh leaves there) */
+static double t_gas_p(const tagblk *t, int i, int j, int k)
+{
+    int c = lidx(i, j, k);
+    return (t->gamma - 1.0) * t->W[c] * t->W[(size_t)4 * PLANE + c];
+}
+
+/* prj_amr_total_pressure_non_gr_at (src/prj_amr.c:805-819); unclamped */
+static double t_ptot(const tagblk *t, int i, int j, int k)
+{
+    double p = t_gas_p(t, i, j, k);
+    if (t->nv == 9) {
+        int c = lidx(i, j, k);
+        double b1 = t->W[(size_t)6 * PLANE + c];
+        double b2 = t->W[(size_t)7 * PLANE + c];
+        double b3 = t->W[(size_t)8 * PLANE + c];
+        p += 0.5 * (b1 * b1 + b2 * b2 + b3 * b3);
+    }
+    return p;
+}
+
+/* prj_loehner_cell_value (src/prj_amr.c:930-942): density and total
+ * pressure clamp the index, temperature does not */
+static double t_lohner_value(const tagblk *t, int var, int i, int j, int k)
+{
+    if (var == 0) return t_prim(t, 0, i, j, k);
+    if (var == 2) {
+        int c = lidx(i, j, k);
+        return (t->gamma - 1.0) * t->W[(size_t)4 * PLANE + c] / 0.95655684e18;
+    }
+    return t_ptot(t, clampi(i), clampi(j), clampi(k));
+}
+
+/* prj_loehner_cell_indicator (src/prj_amr.c:944-1005) */
+static double t_lohner(const tagblk *t, int var, double eps, int i, int j, int k)
+{
+    double u0 = t_lohner_value(t, var, i, j, k);
+    double uxm = t_lohner_value(t, var, i - 1, j, k);
+    double uxp = t_lohner_value(t, var, i + 1, j, k);
+    double uym = t_lohner_value(t, var, i, j - 1, k);
+    double uyp = t_lohner_value(t, var, i, j + 1, k);
+    double uzm = t_lohner_value(t, var, i, j, k - 1);
+    double uzp = t_lohner_value(t, var, i, j, k + 1);
+    double num_x = uxp - 2.0 * u0 + uxm;
+    double num_y = uyp - 2.0 * u0 + uym;
+    double num_z = uzp - 2.0 * u0 + uzm;
+    double num_xy = 0.25 * (t_lohner_value(t, var, i + 1, j + 1, k) - t_lohner_value(t, var, i + 1, j - 1, k) -
+        t_lohner_value(t, var, i - 1, j + 1, k) + t_lohner_value(t, var, i - 1, j - 1, k));
+    double num_xz = 0.25 * (t_lohner_value(t, var, i + 1, j, k + 1) - t_lohner_value(t, var, i + 1, j, k - 1) -
+        t_lohner_value(t, var, i - 1, j, k + 1) + t_lohner_value(t, var, i - 1, j, k - 1));
+    double num_yz = 0.25 * (t_lohner_value(t, var, i, j + 1, k + 1) - t_lohner_value(t, var, i, j + 1, k - 1) -
+        t_lohner_value(t, var, i, j - 1, k + 1) + t_lohner_value(t, var, i, j - 1, k - 1));
+    double den_x = fabs(uxp - u0) + fabs(u0 - uxm) + eps * (fabs(uxp) + 2.0 * fabs(u0) + fabs(uxm));
+    double den_y = fabs(uyp - u0) + fabs(u0 - uym) + eps * (fabs(uyp) + 2.0 * fabs(u0) + fabs(uym));
+    double den_z = fabs(uzp - u0) + fabs(u0 - uzm) + eps * (fabs(uzp) + 2.0 * fabs(u0) + fabs(uzm));
+    double numerator = num_x * num_x + num_y * num_y + num_z * num_z +
+        2.0 * (num_xy * num_xy + num_xz * num_xz + num_yz * num_yz);
+    double denominator = den_x * den_x + den_y * den_y + den_z * den_z + 1.0e-14;
+    return sqrt(numerator / denominator);
+}
+
+/* prj_block_sound_speed_at (src/prj_amr.c:840-862) */
+static double t_sound_speed(const tagblk *t, int i, int j, int k)
+{
+    double rho = t_prim(t, 0, i, j, k);
+    double eint = t_prim(t, 4, i, j, k);
+    double p;
+    if (rho <= 0.0 || eint < 0.0) return 0.0;
+    p = t_ptot(t, clampi(i), clampi(j), clampi(k));
+    if (p <= 0.0 || t->gamma <= 0.0) return 0.0;
+    return sqrt(t->gamma * p / rho);
+}
+
+/* prj_velocity_cell_indicator (src/prj_amr.c:1007-1038) */
+static double t_velocity(const tagblk *t, int i, int j, int k)
+{
+    double v1 = t_prim(t, 1, i, j, k);
+    double v2 = t_prim(t, 2, i, j, k);
+    double v3 = t_prim(t, 3, i, j, k);
+    double cs = t_sound_speed(t, i, j, k);
+    double m = 0.0;
+    int axis, side;
+    for (axis = 0; axis < 3; ++axis) {
+        for (side = -1; side <= 1; side += 2) {
+            int di = axis == 0 ? side : 0;
+            int dj = axis == 1 ? side : 0;
+            int dk = axis == 2 ? side : 0;
+            double dv1 = v1 - t_prim(t, 1, i + di, j + dj, k + dk);
+            double dv2 = v2 - t_prim(t, 2, i + di, j + dj, k + dk);
+            double dv3 = v3 - t_prim(t, 3, i + di, j + dj, k + dk);
+            double dv = sqrt(dv1 * dv1 + dv2 * dv2 + dv3 * dv3) / (cs + 1.0e-14);
+            m = dmax(m, dv);
+        }
+    }
+    return m;
+}
+
+/* prj_pressure_scale_height_cell_indicator, non-GR branch (src/prj_amr.c:1065-1144) */
+static double t_scale_height(const tagblk *t, int i, int j, int k)
+{
+    int c = lidx(i, j, k);
+    double rho, p, g1, g2, g3, accel, cs, hp;
+    if (t->grav == 0) return 0.0;
+    rho = t_prim(t, 0, i, j, k);
+    p = t_ptot(t, i, j, k);
+    g1 = t->grav[c];
+    g2 = t->grav[NCELLS + c];
+    g3 = t->grav[2 * NCELLS + c];
+    accel = sqrt(g1 * g1 + g2 * g2 + g3 * g3);
+    cs = t->dx[0];
+    if (t->dx[1] > cs) cs = t->dx[1];
+    if (t->dx[2] > cs) cs = t->dx[2];
+    if (rho <= 0.0 || p <= 0.0 || accel <= 0.0) return 0.0;
+    hp = p / (rho * accel);
+    if (hp <= 0.0) return 0.0;
+    return cs / hp;
+}
+
+/* prj_fractional_jump_cell_indicator (src/prj_amr.c:1146-1202); unclamped */
+static double t_jump_value(const tagblk *t, int var, int i, int j, int k)
+{
+    if (var == 1) return t_ptot(t, i, j, k);
+    return t->W[lidx(i, j, k)];
+}
+
+static double t_jump(const tagblk *t, int var, int i, int j, int k)
+{
+    double q0 = t_jump_value(t, var, i, j, k);
+    double m = 0.0;
+    int di, dj, dk;
+    if (q0 <= 0.0) return 0.0;
+    for (di = -1; di <= 1; ++di) {
+        for (dj = -1; dj <= 1; ++dj) {
+            for (dk = -1; dk <= 1; ++dk) {
+                double q, den;
+                if (di == 0 && dj == 0 && dk == 0) continue;
+                q = t_jump_value(t, var, i + di, j + dj, k + dk);
+                if (q <= 0.0) continue;
+                den = q0 < q ? q0 : q;
+                m = dmax(m, fabs(q0 - q) / (den + 1.0e-14));
+            }
+        }
+    }
+    return m;
+}
+
+/* prj_amr_cell_indicator_for_estimator (src/prj_amr.c:1204-1221) */
+static double t_indicator(const tagblk *t, const fxo_amr_crit *c, int i, int j, int k)
+{
+    if (c->estimator == 3) return t_jump(t, c->jump_var, i, j, k);
+    if (c->estimator == 2) return t_scale_height(t, i, j, k);
+    if (c->estimator == 1) return t_velocity(t, i, j, k);
+    return t_lohner(t, c->lohner_var, c->lohner_eps, i, j, k);
+}
+
+/* prj_amr_refine_boundary_mask_for_cell (src/prj_amr.c:120-144), buffer 2 */
+static unsigned t_cell_mask(int i, int j, int k)
+{
+    unsigned m = 0u;
+    if (i < 2) m |= 1u;
+    if (i >= BS - 2) m |= 2u;
+    if (j < 2) m |= 4u;
+    if (j >= BS - 2) m |= 8u;
+    if (k < 2) m |= 16u;
+    if (k >= BS - 2) m |= 32u;
+    return m;
+}
+
+/* Pass 1 of prj_amr_tag for one active block: out[0] refine vote (0/1),
+ * out[1] derefine vote (0/-1), out[2] boundary side mask. */
+void fxo_amr_vote(int nv, double gamma, const double *W, const double *grav, const double *dx,
+    int has_parent, const fxo_amr_crit *crit, int ncrit, double reach_density, int *out)
+{
+    tagblk t;
+    int refine = 0;
+    int derefine = has_parent ? 1 : 0;
+    int has_refine = 0, has_derefine = 0;
+    unsigned mask = 0u;
+    int i, j, k, n;
+
+    t.nv = nv;
+    t.gamma = gamma;
+    t.W = W;
+    t.grav = grav;
+    t.dx = dx;
+    for (i = 0; i < BS; ++i) {
+        for (j = 0; j < BS; ++j) {
+            for (k = 0; k < BS; ++k) {
+                unsigned cm = t_cell_mask(i, j, k);
+                double sum = 0.0;
+                if (refine != 0 && cm == 0u) continue;
+                if (reach_density > 0.0 && W[lidx(i, j, k)] > reach_density) {
+                    has_refine = 1;
+                    refine = 1;
+                    derefine = 0;
+                    mask |= cm;
+                }
+                for (n = 0; n < ncrit; ++n) {
+                    if (crit[n].set == 0 || crit[n].refine_thresh <= 0.0) continue;
+                    has_refine = 1;
+                    sum += t_indicator(&t, &crit[n], i, j, k) / crit[n].refine_thresh;
+                }
+                if (sum > 1.0) {
+                    refine = 1;
+                    mask |= cm;
+                }
+            }
+        }
+    }
+    if (derefine != 0) {
+        for (i = -1; i <= BS && derefine != 0; ++i) {
+            for (j = -1; j <= BS && derefine != 0; ++j) {
+                for (k = -1; k <= BS; ++k) {
+                    double sum = 0.0;
+                    for (n = 0; n < ncrit; ++n) {
+                        if (crit[n].set == 0 || crit[n].derefine_thresh <= 0.0) continue;
+                        has_derefine = 1;
+                        sum += t_indicator(&t, &crit[n], i, j, k) / crit[n].derefine_thresh;
+                    }
+                    if (sum >= 1.0) {
+                        derefine = 0;
+                        break;
+                    }
+                }
+            }
+        }
+    }
+    if (has_refine == 0) refine = 0;
+    if (has_derefine == 0) derefine = 0;
+    out[0] = refine ? 1 : 0;
+    out[1] = derefine ? -1 : 0;
+    out[2] = (int)mask;
+}

@@ -68,6 +68,57 @@ class RhParams(C.Structure):
     ]
 
 
+AMR_N = 4
+EST_LOEHNER, EST_VELOCITY, EST_PRESSURE_SCALE_HEIGHT, EST_FRACTIONAL_JUMP = 0, 1, 2, 3
+LOHNER_DENSITY, LOHNER_PRESSURE, LOHNER_TEMPERATURE = 0, 1, 2
+JUMP_DENSITY, JUMP_PRESSURE = 0, 1
+
+
+class RhAmr(C.Structure):
+    """Dynamic-AMR parameters of prj_mesh (src/prj_types.h:465-503)."""
+    _fields_ = [
+        ("max_level", C.c_int),
+        ("min_dx", C.c_double),
+        ("reach_density", C.c_double),
+        ("E_floor", C.c_double),
+        ("set", C.c_int * AMR_N),
+        ("estimator", C.c_int * AMR_N),
+        ("lohner_var", C.c_int * AMR_N),
+        ("jump_var", C.c_int * AMR_N),
+        ("refine_thresh", C.c_double * AMR_N),
+        ("derefine_thresh", C.c_double * AMR_N),
+        ("lohner_eps", C.c_double * AMR_N),
+    ]
+
+
+def amr_params(max_level: int, criteria, min_dx: float = 0.0, reach_density: float = -1.0,
+               E_floor: float = -1.0) -> RhAmr:
+    """criteria: up to four dicts with keys estimator, refine, derefine and
+    optionally lohner_var, jump_var, eps (defaults of src/prj_io.c:341-355)."""
+    a = RhAmr()
+    a.max_level = max_level
+    a.min_dx = min_dx
+    a.reach_density = reach_density
+    a.E_floor = E_floor
+    for n in range(AMR_N):
+        a.set[n] = 0
+        a.estimator[n] = EST_LOEHNER
+        a.lohner_var[n] = LOHNER_PRESSURE
+        a.jump_var[n] = JUMP_PRESSURE
+        a.refine_thresh[n] = 0.5
+        a.derefine_thresh[n] = 0.2
+        a.lohner_eps[n] = 0.1
+    for n, c in enumerate(criteria):
+        a.set[n] = 1
+        a.estimator[n] = c["estimator"]
+        a.refine_thresh[n] = c.get("refine", 0.5)
+        a.derefine_thresh[n] = c.get("derefine", 0.2)
+        a.lohner_var[n] = c.get("lohner_var", LOHNER_PRESSURE)
+        a.jump_var[n] = c.get("jump_var", JUMP_PRESSURE)
+        a.lohner_eps[n] = c.get("eps", 0.1)
+    return a
+
+
 def lib_path(mhd: bool) -> str:
     return os.path.join(REF_DIR, "libprjref_mhd.so" if mhd else "libprjref_hydro.so")
 
@@ -110,6 +161,13 @@ class Reference:
         L.rh_flux_update.argtypes = [C.c_int, C.c_int, C.c_int]
         L.rh_fill_ghosts.argtypes = [C.c_int, C.c_int]
         L.rh_sim_time.restype = C.c_double
+        L.rh_amr_configure.argtypes = [C.POINTER(RhAmr)]
+        L.rh_amr_tag.argtypes = [ip]
+        L.rh_amr_adapt.restype = C.c_int
+        L.rh_run_amr.argtypes = [C.c_int, C.c_int, dp]
+        L.rh_run_amr.restype = C.c_int
+        L.rh_block_tree.argtypes = [C.c_int, ip]
+        L.rh_E_injected.restype = C.c_double
         L.rh_sim_dt.restype = C.c_double
         if mhd:
             L.rh_hlld.argtypes = [dp, dp] + [C.c_double] * 5 + [dp]
@@ -143,6 +201,36 @@ class Reference:
 
     def time_steps(self, nsteps: int, dt: float) -> float:
         return self.lib.rh_time_steps(nsteps, dt)
+
+    # -- dynamic AMR ------------------------------------------------------------
+    def amr_configure(self, a: RhAmr) -> None:
+        self.lib.rh_amr_configure(C.byref(a))
+
+    def amr_tag(self) -> np.ndarray:
+        """refine_flag of every block after prj_amr_tag (before 2:1 balance)."""
+        out = (C.c_int * self.nblocks())()
+        self.lib.rh_amr_tag(out)
+        return np.array(out[:], dtype=np.int32)
+
+    def amr_adapt(self) -> int:
+        return self.lib.rh_amr_adapt()
+
+    def run_amr(self, nsteps: int, interval: int):
+        st = (C.c_double * 4)()
+        n = self.lib.rh_run_amr(nsteps, interval, st)
+        return n, st[0], st[1], int(st[2]), int(st[3])
+
+    def block_tree(self, b: int) -> np.ndarray:
+        """parent, children[8], refine_flag, can_refine"""
+        out = (C.c_int * 11)()
+        self.lib.rh_block_tree(b, out)
+        return np.array(out[:], dtype=np.int32)
+
+    def tree_arrays(self) -> np.ndarray:
+        return np.stack([self.block_tree(b) for b in range(self.nblocks())])
+
+    def E_injected(self) -> float:
+        return self.lib.rh_E_injected()
 
     # -- mesh description -----------------------------------------------------
     def nblocks(self) -> int:

@@ -1024,3 +1024,143 @@ void rh_eos_rey(double rho, double eint, double ye, double *out)
     out[1] = q[PRJ_EOS_PRESSURE];
     out[2] = q[PRJ_EOS_GAMMA];
 }
+
+/* ------------------------------------------------------------------------ */
+/* Dynamic AMR (src/prj_amr.c) driven the way src/main.c:565-607 drives it.   */
+/* ------------------------------------------------------------------------ */
+
+typedef struct rh_amr {
+    int max_level;
+    double min_dx;
+    double reach_density;   /* amr_reach_highest_level_at_density */
+    double E_floor;
+    int set[PRJ_AMR_N];
+    int estimator[PRJ_AMR_N];
+    int lohner_var[PRJ_AMR_N];
+    int jump_var[PRJ_AMR_N];
+    double refine_thresh[PRJ_AMR_N];
+    double derefine_thresh[PRJ_AMR_N];
+    double lohner_eps[PRJ_AMR_N];
+} rh_amr;
+
+int rh_amr_n(void) { return PRJ_AMR_N; }
+
+void rh_amr_configure(const rh_amr *a)
+{
+    int n;
+
+    g_sim.mesh.max_level = a->max_level;
+    g_sim.mesh.min_dx = a->min_dx;
+    g_sim.mesh.amr_reach_highest_level_at_density = a->reach_density;
+    g_sim.mesh.E_floor = a->E_floor;
+    g_sim.mesh.use_BJ = 0;
+    g_sim.mesh.use_amr_angular_resolution_limit = 0;
+    g_sim.mesh.amr_init_refine_fn = 0;
+    for (n = 0; n < PRJ_AMR_N; ++n) {
+        g_sim.mesh.amr_criterion_set[n] = a->set[n];
+        g_sim.mesh.amr_estimator[n] = a->estimator[n];
+        g_sim.mesh.amr_lohner_var[n] = a->lohner_var[n];
+        g_sim.mesh.amr_fractional_jump_var[n] = a->jump_var[n];
+        g_sim.mesh.amr_refine_thresh[n] = a->refine_thresh[n];
+        g_sim.mesh.amr_derefine_thresh[n] = a->derefine_thresh[n];
+        g_sim.mesh.amr_lohner_eps[n] = a->lohner_eps[n];
+    }
+}
+
+/* prj_amr_tag alone: flags[b] = refine_flag of every block afterwards (the
+ * votes after the caps, before 2:1 balance).  The flags are cleared again. */
+void rh_amr_tag(int *flags)
+{
+    int b;
+
+    prj_amr_tag(&g_sim.mesh, &g_sim.eos, &g_mpi);
+    for (b = 0; b < g_sim.mesh.nblocks; ++b) {
+        flags[b] = g_sim.mesh.blocks[b].refine_flag;
+        if (g_sim.mesh.blocks[b].id >= 0) {
+            g_sim.mesh.blocks[b].refine_flag = 0;
+        }
+    }
+}
+
+/* prj_amr_adapt followed by the driver's refill after a changed mesh
+ * (src/main.c:571-606 without output, radiation and gravity).  Returns the
+ * block_changed flag. */
+int rh_amr_adapt(void)
+{
+    int changed = prj_amr_adapt(&g_sim.mesh, &g_sim.eos, &g_mpi);
+
+    if (changed) {
+        prj_mpi_rebalance(&g_sim.mesh, &g_mpi);
+        prj_eos_fill_active_cells(&g_sim.mesh, &g_sim.eos, &g_mpi, 1, PRJ_EOS_CTX_AMR);
+        prj_boundary_fill_ghosts_and_bf(&g_sim.mesh, &g_mpi, &g_sim.bc, 1, 0,
+            &g_sim.eos, 0, &g_sim.rad, PRJ_BOUNDARY_TIMER_SCOPE_NONE);
+        prj_eos_fill_mesh(&g_sim.mesh, &g_sim.eos, &g_mpi, 1, PRJ_EOS_CTX_AMR);
+    }
+    return changed;
+}
+
+/* The driver loop of src/main.c:485-607 with an adapt every amr_interval
+ * steps (counted by the global step number).  state as rh_run; state[3]
+ * counts the adapts that changed the mesh. */
+int rh_run_amr(int nsteps, int amr_interval, double *state)
+{
+    int n = 0;
+    int changes = 0;
+
+    while (g_sim.time < g_sim.t_end && n < nsteps) {
+        double dt_new = rh_calc_dt();
+        double dt_step;
+        double dt_src = 1.0e100;
+
+        if (g_sim.dt > 0.0) {
+            double dt_limit = g_sim.dt_factor * g_sim.dt;
+
+            g_sim.dt = dt_new <= dt_limit ? dt_new : dt_limit;
+        } else {
+            g_sim.dt = dt_new;
+        }
+        dt_step = g_sim.dt;
+        if (g_sim.time + dt_step > g_sim.t_end) {
+            dt_step = g_sim.t_end - g_sim.time;
+        }
+        rh_step(dt_step, &dt_src);
+        if (g_sim.cfl * dt_src < g_sim.dt) {
+            g_sim.dt = g_sim.cfl * dt_src;
+        }
+        g_sim.time += dt_step;
+        g_sim.step += 1;
+        n += 1;
+        if (amr_interval > 0 && g_sim.step % amr_interval == 0) {
+            changes += rh_amr_adapt();
+        }
+    }
+    if (state != 0) {
+        state[0] = g_sim.time;
+        state[1] = g_sim.dt;
+        state[2] = (double)g_sim.step;
+        state[3] = (double)changes;
+    }
+    return n;
+}
+
+/* out[0] parent, out[1..8] children, out[9] refine_flag, out[10] can_refine */
+int rh_block_tree(int b, int *out)
+{
+    const prj_block *block;
+    int n;
+
+    if (!g_ready || b < 0 || b >= g_sim.mesh.nblocks) {
+        return 1;
+    }
+    block = &g_sim.mesh.blocks[b];
+    out[0] = block->parent;
+    for (n = 0; n < 8; ++n) {
+        out[1 + n] = block->children[n];
+    }
+    out[9] = block->refine_flag;
+    out[10] = block->can_refine;
+    return 0;
+}
+
+double rh_E_injected(void) { return g_sim.eos.E_injected; }
+int rh_max_blocks(void) { return g_sim.mesh.nblocks_max; }

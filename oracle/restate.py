@@ -13,6 +13,19 @@ PATH = os.path.join(HERE, "_ref", "libfxoracle.so")
 _dp = C.POINTER(C.c_double)
 
 
+class AmrCrit(C.Structure):
+    """fxo_amr_crit: one refinement criterion."""
+    _fields_ = [
+        ("set", C.c_int),
+        ("estimator", C.c_int),
+        ("lohner_var", C.c_int),
+        ("jump_var", C.c_int),
+        ("refine_thresh", C.c_double),
+        ("derefine_thresh", C.c_double),
+        ("lohner_eps", C.c_double),
+    ]
+
+
 def available() -> bool:
     return os.path.exists(PATH)
 
@@ -37,6 +50,8 @@ class Restatement:
         L.fxo_calc_dt.restype = C.c_double
         L.fxo_step_block.argtypes = [C.c_int, C.c_double, _dp, _dp, _dp, C.c_double]
         L.fxo_step_block.restype = C.c_double
+        L.fxo_amr_vote.argtypes = [C.c_int, C.c_double, _dp, _dp, _dp, C.c_int, C.POINTER(AmrCrit), C.c_int,
+                                   C.c_double, C.POINTER(C.c_int)]
 
     @staticmethod
     def _p(a):
@@ -97,3 +112,32 @@ class Restatement:
         dx = np.ascontiguousarray(dx, np.float64)
         bp = self._p(Bf) if Bf is not None else None
         return self.lib.fxo_step_block(nv, gamma, self._p(dx), self._p(W), bp, dt)
+
+    def amr_votes(self, nv, gamma, W, grav, dx, active, parent, crits, reach=-1.0):
+        """Pass 1 of prj_amr_tag for every block: int32 [nb, 3] (refine vote,
+        derefine vote, boundary mask; zeros for inactive entries).  W is
+        [nb, nv, 2, 8000]; grav [nb, 3, 8000] or None; crits a list of dicts
+        (estimator, refine, derefine, var, eps)."""
+        arr = (AmrCrit * max(len(crits), 1))()
+        for n, c in enumerate(crits):
+            arr[n].set = 1
+            arr[n].estimator = int(c["estimator"])
+            var = int(c.get("var", 1))
+            arr[n].lohner_var = var
+            arr[n].jump_var = min(var, 1)
+            arr[n].refine_thresh = float(c.get("refine", 0.5))
+            arr[n].derefine_thresh = float(c.get("derefine", 0.2))
+            arr[n].lohner_eps = float(c.get("eps", 0.1))
+        nb = W.shape[0]
+        out = np.zeros((nb, 3), dtype=np.int32)
+        o = (C.c_int * 3)()
+        for b in range(nb):
+            if not active[b]:
+                continue
+            w = np.ascontiguousarray(W[b], np.float64)
+            g = None if grav is None else self._p(np.ascontiguousarray(grav[b], np.float64))
+            d = np.ascontiguousarray(dx[b], np.float64)
+            self.lib.fxo_amr_vote(nv, gamma, self._p(w), g, self._p(d), 1 if parent[b] >= 0 else 0,
+                                  arr, len(crits), reach, o)
+            out[b] = o[:]
+        return out

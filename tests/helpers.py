@@ -300,18 +300,26 @@ def bf2bc(W, Bf, slot):
 
 
 def ref_state(ref):
+    """W [nb, nv, 2, 8000] and Bf [nb, 3, 2, 8400] of every block entry;
+    entries without storage (freed by a coarsening) read as zeros."""
     nb = ref.nblocks()
-    W = np.stack([ref.W(b).reshape(ref.nhydro, 2, NCELLS) for b in range(nb)])
-    Bf = None
-    if ref.mhd:
-        Bf = np.stack([np.stack([ref.Bf(b, d).reshape(2, NFACES) for d in range(3)]) for b in range(nb)])
+    W = np.zeros((nb, ref.nhydro, 2, NCELLS))
+    Bf = np.zeros((nb, 3, 2, NFACES)) if ref.mhd else None
+    for b in range(nb):
+        try:
+            W[b] = ref.W(b).reshape(ref.nhydro, 2, NCELLS)
+        except ValueError:
+            continue
+        if ref.mhd:
+            for d in range(3):
+                Bf[b, d] = ref.Bf(b, d).reshape(2, NFACES)
     return W, Bf
 
 
 def ref_desc(ref):
     from fornaxamr_b200 import mesh
     ints, geom, slots = ref.mesh_arrays()
-    return mesh.desc_from_arrays(ints, geom, slots)
+    return mesh.desc_from_arrays(ints, geom, slots, ref.tree_arrays())
 
 
 def max_rel_err(a, b, floor=1e-300):

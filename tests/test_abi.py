@@ -33,8 +33,11 @@ def test_library_exports_every_declared_symbol():
 def test_struct_layout_matches_header():
     from fornaxamr_b200._lib import FxBlockDesc, FxConfig, FxSlot
     assert ctypes.sizeof(FxSlot) == 24
-    assert ctypes.sizeof(FxBlockDesc) == 16 + 13 * 8 + 56 * 24
+    assert ctypes.sizeof(FxBlockDesc) == 16 + 13 * 8 + 56 * 24 + 10 * 4
     assert ctypes.sizeof(FxConfig) == 8 + 8 + 48 + 24 + 8
+    from fornaxamr_b200._lib import FxAmrConfig, FxAmrCriterion
+    assert ctypes.sizeof(FxAmrCriterion) == 16 + 24
+    assert ctypes.sizeof(FxAmrConfig) == 24 + 24 + 4 * 40
 
 
 def test_invalid_arguments_are_rejected_without_device():
