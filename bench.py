@@ -51,6 +51,12 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--amr-interval", type=int, default=10,
+                    help="steps between adapts of the dynamic-AMR key")
+    ap.add_argument("--amr-dynamic-adapts", type=int, default=2,
+                    help="adapts in the dynamic-AMR key (0: skip it)")
+    ap.add_argument("--ref-adapt", action="store_true",
+                    help="also time the reference's adapt on the dynamic-AMR mesh (about a minute of CPU)")
     ap.add_argument("--amr-steps", type=int, default=10,
                     help="batched steps of the static-AMR blast measurement (0: skip it)")
     ap.add_argument("--collapse", action="store_true",
@@ -73,6 +79,30 @@ def _cpu_worker(args):
         r.time_steps(warm, dt)
     secs = r.time_steps(nsteps, dt)
     return nsteps * (root ** 3) * 4096, secs
+
+
+def _ref_adapt_worker(_):
+    from oracle import ref as R
+    r = R.Reference(True)
+    r.setup(R.params_amr_blast(root=8, max_level=2, radii=(0.4, 0.2)))
+    r.amr_configure(R.amr_params(3, [dict(estimator=R.EST_LOEHNER, refine=0.3, derefine=0.1,
+                                          lohner_var=R.LOHNER_PRESSURE)]))
+    nb = r.nblocks()
+    t0 = time.perf_counter()
+    changed = r.amr_adapt()
+    return time.perf_counter() - t0, nb, r.nblocks(), changed
+
+
+def ref_adapt_sample():
+    """The reference's prj_amr_adapt plus the driver's refill (one core, the
+    serial reference C core) on the 2352-block blast mesh of the dynamic-AMR
+    key, from its initial state."""
+    ctx = mp.get_context("spawn")
+    with ctx.Pool(1) as pool:
+        secs, nb0, nb1, changed = pool.map(_ref_adapt_worker, [0])[0]
+    return {"seconds": secs, "blocks_before": nb0, "blocks_after": nb1, "changed": bool(changed), "cores": 1,
+            "sample": "prj_amr_adapt + eos/ghost refill of src/main.c:571-606, blast 8^3 roots, 3 levels, "
+                      "Loehner pressure 0.3 / 0.1 up to level 3, initial state"}
 
 
 def cpu_reference(steps: int, warmup: int, seconds: float):
@@ -260,6 +290,72 @@ def run_amr(args, dev, kind):
     }
     ctx.close()
     return out
+
+
+def run_amr_dynamic(args, dev):
+    """Dynamic AMR: the 3-level magnetised blast of run_amr (8^3 roots, 2352
+    blocks) stepped with prj_amr_adapt every `interval` steps (Loehner
+    pressure criterion, refine 0.3 / derefine 0.1, up to level 3), the driver
+    loop of src/main.c.  Wall time per step includes the adapts (device tag,
+    host remesh and ghost-fill compile, device prolongation / restriction,
+    refill); the adapt phases are reported separately."""
+    import numpy as np
+    import torch
+
+    import fornaxamr_b200 as fx
+    from fornaxamr_b200 import mesh, problems
+
+    hw, root = 0.7, 8
+    coord = (-hw, hw, -hw, hw, -hw, hw)
+    blocks = mesh.static_amr_mesh((root,) * 3, coord, 2, mesh.ball_refiner((0.1, 0.05, 0.0), (0.4, 0.2)))
+    desc = mesh.to_desc(blocks)
+    recs = fx.plan_export(fx.make_config(True, 5.0 / 3.0, coord), desc, 3)
+    W0, Bf0 = problems.amr_blast(blocks, recs)
+    ctx = fx.Context(True, 5.0 / 3.0, coord, device=dev)
+    ctx.set_mesh(desc)
+    ctx.upload_all(np.ascontiguousarray(W0), np.ascontiguousarray(Bf0))
+    del W0, Bf0
+    ctx.boundary_fill(1, 0)
+    ctx.amr_configure(fx.amr_config((root,) * 3, 3, [
+        dict(estimator=fx.AMR_LOEHNER, refine=0.3, derefine=0.1, var=fx.AMR_VAR_PRESSURE)]))
+    interval = args.amr_interval
+    state = ctx.run(fx.FORM_BATCHED, max(args.warmup, 3), 0.4, 1.2, 1.0e30, (0.0, 0.0, 0))
+    ctx.sync()
+    torch.cuda.synchronize(dev)
+    stream = torch.cuda.ExternalStream(ctx.stream(), device=dev)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    adapts, step_ms, zone_steps = [], [], 0
+    t0 = time.perf_counter()
+    for _ in range(args.amr_dynamic_adapts):
+        nact = sum(1 for b in ctx.get_mesh() if b.id >= 0 and b.active == 1)
+        e0.record(stream)
+        state = ctx.run(fx.FORM_BATCHED, interval, 0.4, 1.2, 1.0e30, state)
+        e1.record(stream)
+        e1.synchronize()
+        step_ms.append(e0.elapsed_time(e1) / interval)
+        zone_steps += nact * 4096 * interval
+        changed = ctx.amr_adapt()
+        t = ctx.amr_timings()
+        t["changed"] = bool(changed)
+        t["blocks_after"] = ctx.nblocks
+        adapts.append(t)
+    wall = time.perf_counter() - t0
+    msh = ctx.get_mesh()
+    levels = {}
+    for b in msh:
+        if b.id >= 0 and b.active == 1:
+            levels[b.level] = levels.get(b.level, 0) + 1
+    ctx.close()
+    nsteps = interval * args.amr_dynamic_adapts
+    return {"workload": "magnetised blast, 8^3 roots, 3 static levels then adapts every "
+                        f"{interval} steps up to level 3 (Loehner pressure 0.3 / 0.1)",
+            "steps": nsteps, "interval": interval,
+            "wall_ms_per_step": 1e3 * wall / nsteps,
+            "value_wall": zone_steps / wall,
+            "device_ms_per_step": step_ms,
+            "adapt_ms": [{k: (round(v, 2) if isinstance(v, float) else v) for k, v in a.items()} for a in adapts],
+            "active_blocks_per_level_end": [levels.get(l, 0) for l in range(4)]}
 
 
 def run_adjoint(args, dev):
@@ -472,6 +568,12 @@ def main():
         except Exception as exc:  # oracle missing on this machine
             cb = {"value": None, "unit": UNIT, "cores": 0, "kind": "reference",
                   "sample": f"unavailable: {exc}"}
+    ra = None
+    if rank == 0 and world == 1 and args.ref_adapt:
+        try:
+            ra = ref_adapt_sample()
+        except Exception as exc:
+            ra = {"seconds": None, "sample": f"unavailable: {exc}"}
     if world > 1:
         import datetime
 
@@ -486,6 +588,10 @@ def main():
         line["amr_blast"] = run_amr(args, local_rank, "blast")
         if args.collapse:
             line["amr_collapse"] = run_amr(args, local_rank, "collapse")
+    if world == 1 and args.amr_dynamic_adapts > 0:
+        line["amr_dynamic"] = run_amr_dynamic(args, local_rank)
+        if ra is not None:
+            line["amr_dynamic"]["reference_adapt"] = ra
     if world > 1:
         import torch
         torch.distributed.barrier()

@@ -340,6 +340,30 @@ class Context:
         self._check(self.L.fx_get_mesh(self._h, n, out, C.byref(m)))
         return out
 
+    def amr_timings(self) -> dict:
+        """Host wall time (ms) of the phases of the last amr_adapt."""
+        ms = (C.c_double * 6)()
+        self._check(self.L.fx_amr_timings(self._h, ms))
+        return dict(zip(("tag", "remesh", "data", "compile", "refill", "total"), ms[:]))
+
+    def run_amr(self, form: int, nsteps: int, interval: int, cfl: float, dt_factor: float, t_end: float,
+                state):
+        """The driver loop of src/main.c:485-607 with prj_amr_adapt every
+        `interval` steps (by the global step number in state[2]); returns
+        (state, number of adapts that changed the mesh)."""
+        changes = 0
+        done = 0
+        while done < nsteps:
+            step = int(state[2])
+            n = min(nsteps - done, interval - step % interval) if interval > 0 else nsteps - done
+            state = self.run(form, n, cfl, dt_factor, t_end, state)
+            done += n
+            if state[2] == step:  # t_end reached
+                break
+            if interval > 0 and int(state[2]) % interval == 0:
+                changes += int(self.amr_adapt())
+        return state, changes
+
     def amr_energy_injected(self) -> float:
         e = C.c_double(0.0)
         self._check(self.L.fx_amr_energy_injected(self._h, C.byref(e)))

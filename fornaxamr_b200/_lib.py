@@ -101,7 +101,7 @@ EXPORTS = [
     "fx_autotune", "fx_calc_dt_noalloc", "fx_face_eval_host", "fx_face_vjp_host",
     "fx_adjoint_forward", "fx_adjoint_backward", "fx_adjoint_time", "fx_set_flux_shape",
     "fx_amr_configure", "fx_amr_tag", "fx_amr_adapt", "fx_get_mesh", "fx_amr_energy_injected",
-    "fx_amr_remesh_host",
+    "fx_amr_remesh_host", "fx_amr_timings",
 ]
 PHASE_FLUX, PHASE_EMF, PHASE_CT, PHASE_CELLS, PHASE_GHOST, PHASE_STEP = range(6)
 
@@ -161,6 +161,7 @@ def load() -> C.CDLL:
     L.fx_amr_adapt.argtypes = [vp, C.POINTER(C.c_int)]
     L.fx_get_mesh.argtypes = [vp, C.c_int, C.POINTER(FxBlockDesc), C.POINTER(C.c_int)]
     L.fx_amr_energy_injected.argtypes = [vp, dp]
+    L.fx_amr_timings.argtypes = [vp, dp]
     L.fx_amr_remesh_host.argtypes = [C.POINTER(FxConfig), C.POINTER(FxAmrConfig), C.c_int, C.POINTER(FxBlockDesc),
                                      ip, ip, C.c_int, C.POINTER(FxBlockDesc), C.POINTER(C.c_int)]
     return L

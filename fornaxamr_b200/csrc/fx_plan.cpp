@@ -40,9 +40,27 @@
 #include <cmath>
 #include <cstdint>
 #include <cstring>
+#include <thread>
 #include <unordered_map>
 
 namespace {
+
+/* worker threads for the data-parallel parts of the compiler */
+int compile_threads()
+{
+    const unsigned n = std::thread::hardware_concurrency();
+    return (int)std::max(1u, std::min(n, 32u));
+}
+
+/* runs fn(t) for t in [0, n) on n threads (the calling thread takes t = 0) */
+template <typename F>
+void parallel_for(int n, F fn)
+{
+    std::vector<std::thread> th;
+    for (int t = 1; t < n; ++t) th.emplace_back(fn, t);
+    fn(0);
+    for (auto &x : th) x.join();
+}
 
 enum { KIND_SAME = 3, KIND_RESTRICT = 4, KIND_PROLONG = 5 };
 enum { PHYS_FACE_ONLY = 0, PHYS_EDGE_CORNER = 2 };
@@ -153,8 +171,10 @@ public:
         }
         fid_.assign((size_t)nface_, 0);
         ver_.assign((size_t)(2 * ncell_ + nface_), -1);
-        /* roughly one operation per ghost cell and ghost face of a block */
-        const size_t est = plan.active.size() * (size_t)(cfg_.mhd ? 18000 : 4000);
+        /* the replay records about 36000 operations per block with a field
+         * (ghost cells, ghost faces, groups, and the writes later found
+         * dead), 4000 without */
+        const size_t est = plan.active.size() * (size_t)(cfg_.mhd ? 40000 : 4000);
         seq_.reserve(est);
         prod_.reserve(est + est / 4);
         rd_.reserve(est + est / 4);
@@ -231,7 +251,6 @@ private:
     }
 
     int64_t cell_elem(int b, int c) const { return (int64_t)b * FX_NCELLS + c; }
-    int64_t cellb_elem(int b, int c) const { return ncell_ + (int64_t)b * FX_NCELLS + c; }
     int64_t face_elem(int b, int dir, int f) const { return 2 * ncell_ + ((int64_t)b * 3 + dir) * FX_NFACES + f; }
 
     /* ---- recording -------------------------------------------------------- */
@@ -703,8 +722,12 @@ private:
         p.coarse = coarse;
         p.pos = (f[0] + 2) | ((f[1] + 2) << 5) | ((f[2] + 2) << 10) | ((c[0] + 2) << 15) |
             ((c[1] + 2) << 20) | ((c[2] + 2) << 25);
-        std::vector<int64_t> reads, writes;
-        std::vector<std::pair<int64_t, ProlongSig>> sigs;
+        std::vector<int64_t> &reads = g_reads_;
+        std::vector<int64_t> &writes = g_writes_;
+        std::vector<std::pair<int64_t, ProlongSig>> &sigs = g_sigs_;
+        reads.clear();
+        writes.clear();
+        sigs.clear();
         const int op_index = (int)seq_.size();
         for (int d = 0; d < 3; ++d) {
             const int t0 = d == 0 ? 1 : 0;
@@ -978,29 +1001,40 @@ private:
         int nsrc, std::vector<FxCorr> &out, std::vector<int> &begin)
     {
         const int n = (int)seq.size();
+        const int stride = 1 + nsrc;
+        /* dense element numbers */
+        std::vector<int64_t> keys;
+        keys.reserve((size_t)n * stride);
+        for (int x = 0; x < n; ++x) {
+            for (int q = 0; q < stride; ++q) keys.push_back(el[x][q]);
+        }
+        std::vector<int64_t> uniq(keys);
+        std::sort(uniq.begin(), uniq.end());
+        uniq.erase(std::unique(uniq.begin(), uniq.end()), uniq.end());
+        std::vector<int32_t> ids(keys.size());
+        for (size_t q = 0; q < keys.size(); ++q) {
+            ids[q] = (int32_t)(std::lower_bound(uniq.begin(), uniq.end(), keys[q]) - uniq.begin());
+        }
+        std::vector<int64_t>().swap(keys);
+        const size_t m = uniq.size();
         std::vector<char> live(n, 0);
-        std::unordered_map<int64_t, char> needed; /* absent: the final value, needed */
+        std::vector<char> needed(m, 2); /* 2: not yet seen from the end (a final value, needed) */
         for (int x = n - 1; x >= 0; --x) {
-            const int64_t d = el[x][0];
-            const auto it = needed.find(d);
-            live[x] = it == needed.end() || it->second;
+            const int32_t d = ids[(size_t)x * stride];
+            live[x] = needed[d] != 0;
             needed[d] = 0;
             if (!live[x]) continue;
-            for (int q = 1; q <= nsrc; ++q) needed[el[x][q]] = 1;
+            for (int q = 1; q <= nsrc; ++q) needed[ids[(size_t)x * stride + q]] = 1;
         }
-        std::unordered_map<int64_t, int> lw, lr;
-        auto get = [](const std::unordered_map<int64_t, int> &m, int64_t k) {
-            const auto it = m.find(k);
-            return it == m.end() ? -1 : it->second;
-        };
+        std::vector<int> lw(m, -1), lr(m, -1);
         std::vector<std::vector<FxCorr>> waves;
         for (int x = 0; x < n; ++x) {
             if (!live[x]) continue;
-            const int64_t d = el[x][0];
-            int wave = std::max(get(lw, d), get(lr, d)) + 1;
-            for (int q = 1; q <= nsrc; ++q) wave = std::max(wave, get(lw, el[x][q]) + 1);
-            for (int q = 1; q <= nsrc; ++q) lr[el[x][q]] = std::max(get(lr, el[x][q]), wave);
-            lw[d] = wave;
+            const int32_t *e = &ids[(size_t)x * stride];
+            int wave = std::max(lw[e[0]], lr[e[0]]) + 1;
+            for (int q = 1; q <= nsrc; ++q) wave = std::max(wave, lw[e[q]] + 1);
+            for (int q = 1; q <= nsrc; ++q) lr[e[q]] = std::max(lr[e[q]], wave);
+            lw[e[0]] = wave;
             if ((int)waves.size() <= wave) waves.resize(wave + 1);
             waves[wave].push_back(seq[x]);
         }
@@ -1071,77 +1105,101 @@ private:
         std::vector<char>().swap(live);
         /* 4. cell-field operations (bf2bc of every ghost cell and of interior
          * cells with a rewritten face), reading the final faces through the
-         * copy chains, levelled after the operations they read */
+         * copy chains, levelled after the operations they read.  Each writes
+         * its own cell-field element, which nothing else touches, and reads
+         * only final face versions, so its wave is max(lw[faces]) + 1 and
+         * blocks are independent: they run on worker threads and are merged
+         * in block order. */
         std::vector<std::vector<FxBop>> wb;
         if (cfg_.mhd) {
-            for (int b : plan.active) {
-                for (int i = -NG; i < BS + NG; ++i) {
-                    for (int j = -NG; j < BS + NG; ++j) {
-                        for (int k = -NG; k < BS + NG; ++k) {
-                            const bool ghost = i < 0 || i >= BS || j < 0 || j >= BS || k < 0 || k >= BS;
-                            int64_t f[6] = {
-                                face_elem(b, 0, fidx(0, i, j, k)), face_elem(b, 0, fidx(0, i + 1, j, k)),
-                                face_elem(b, 1, fidx(1, i, j, k)), face_elem(b, 1, fidx(1, i, j + 1, k)),
-                                face_elem(b, 2, fidx(2, i, j, k)), face_elem(b, 2, fidx(2, i, j, k + 1))};
-                            bool touched = false;
-                            for (int q = 0; q < 6; ++q) {
-                                if (ver_[f[q]] >= 0) touched = true;
+            const int nt = compile_threads();
+            const int na = (int)plan.active.size();
+            std::vector<std::vector<std::pair<int16_t, FxBop>>> part(nt);
+            std::vector<long long> rew(nt, 0);
+            parallel_for(nt, [&](int t) {
+                std::vector<std::pair<int16_t, FxBop>> &out = part[t];
+                for (int ai = (int)((int64_t)na * t / nt); ai < (int)((int64_t)na * (t + 1) / nt); ++ai) {
+                    const int b = plan.active[ai];
+                    for (int i = -NG; i < BS + NG; ++i) {
+                        for (int j = -NG; j < BS + NG; ++j) {
+                            for (int k = -NG; k < BS + NG; ++k) {
+                                const bool ghost = i < 0 || i >= BS || j < 0 || j >= BS || k < 0 || k >= BS;
+                                int64_t f[6] = {
+                                    face_elem(b, 0, fidx(0, i, j, k)), face_elem(b, 0, fidx(0, i + 1, j, k)),
+                                    face_elem(b, 1, fidx(1, i, j, k)), face_elem(b, 1, fidx(1, i, j + 1, k)),
+                                    face_elem(b, 2, fidx(2, i, j, k)), face_elem(b, 2, fidx(2, i, j, k + 1))};
+                                bool touched = false;
+                                for (int q = 0; q < 6; ++q) {
+                                    if (ver_[f[q]] >= 0) touched = true;
+                                }
+                                if (!ghost && !touched) continue;
+                                FxBop bo;
+                                bo.dst = FX_CELL_KEY(b, lidx(i, j, k));
+                                bo.pad = 0;
+                                int wave = 0;
+                                for (int q = 0; q < 6; ++q) {
+                                    int v = ver_[f[q]];
+                                    int64_t e = f[q];
+                                    resolve(e, v, &rew[t]);
+                                    bo.f[q] = face_key(e);
+                                    wave = std::max(wave, lw[(Elem)e] + 1);
+                                }
+                                out.emplace_back((int16_t)wave, bo);
                             }
-                            if (!ghost && !touched) continue;
-                            FxBop bo;
-                            bo.dst = FX_CELL_KEY(b, lidx(i, j, k));
-                            bo.pad = 0;
-                            Elem rr[6];
-                            for (int q = 0; q < 6; ++q) {
-                                int v = ver_[f[q]];
-                                int64_t e = f[q];
-                                resolve(e, v, &stats_.rewired);
-                                bo.f[q] = face_key(e);
-                                rr[q] = (Elem)e;
-                            }
-                            const Elem w = (Elem)cellb_elem(b, lidx(i, j, k));
-                            const int wave = place(rr, 6, &w, 1);
-                            if ((int)wb.size() <= wave) wb.resize(wave + 1);
-                            wb[wave].push_back(bo);
                         }
                     }
                 }
+            });
+            for (int t = 0; t < nt; ++t) {
+                stats_.rewired += rew[t];
+                for (const auto &e : part[t]) {
+                    const int wave = e.first;
+                    nwaves = std::max(nwaves, wave + 1);
+                    if ((int)wb.size() <= wave) wb.resize(wave + 1);
+                    wb[wave].push_back(e.second);
+                }
+                std::vector<std::pair<int16_t, FxBop>>().swap(part[t]);
             }
         }
-        /* 5. per-wave arrays: operations of a wave sorted by type, then
-         * destination */
+        std::vector<int16_t>().swap(lw);
+        std::vector<int16_t>().swap(lr);
+        /* 5. per-wave arrays: a counting sort of the operations by (wave,
+         * type), replay order kept within a bucket (the replay visits each
+         * destination box in storage order) */
         FxProgram &g = plan.ghost;
-        std::vector<int> nc(nwaves + 1, 0), nf(nwaves + 1, 0), np(nwaves + 1, 0);
+        constexpr int NT = 16; /* op type values are below 16 */
+        std::vector<int> nc((size_t)nwaves * NT + 1, 0), nf((size_t)nwaves * NT + 1, 0), np(nwaves + 1, 0);
         for (int x = 0; x < nseq; ++x) {
             if (opwave[x] < 0) continue;
-            const int sp = seq_[x].space;
-            (sp == SPACE_CELL ? nc : sp == SPACE_FACE ? nf : np)[opwave[x] + 1] += 1;
+            const SeqOp &o = seq_[x];
+            if (o.space == SPACE_CELL) ++nc[(size_t)opwave[x] * NT + o.op.type + 1];
+            else if (o.space == SPACE_FACE) ++nf[(size_t)opwave[x] * NT + o.op.type + 1];
+            else ++np[opwave[x] + 1];
         }
-        for (int w = 0; w < nwaves; ++w) {
-            nc[w + 1] += nc[w];
-            nf[w + 1] += nf[w];
-            np[w + 1] += np[w];
+        for (size_t q = 0; q + 1 < nc.size(); ++q) {
+            nc[q + 1] += nc[q];
+            nf[q + 1] += nf[q];
         }
-        g.cell_ops.resize(nc[nwaves]);
-        g.face_ops.resize(nf[nwaves]);
+        for (int w = 0; w < nwaves; ++w) np[w + 1] += np[w];
+        g.cell_ops.resize(nc.back());
+        g.face_ops.resize(nf.back());
         g.p_ops.resize(np[nwaves]);
-        g.cell_begin.assign(nc.begin(), nc.end());
-        g.face_begin.assign(nf.begin(), nf.end());
+        g.cell_begin.resize(nwaves + 1);
+        g.face_begin.resize(nwaves + 1);
+        for (int w = 0; w <= nwaves; ++w) {
+            g.cell_begin[w] = nc[(size_t)w * NT];
+            g.face_begin[w] = nf[(size_t)w * NT];
+        }
         g.p_begin.assign(np.begin(), np.end());
         for (int x = 0; x < nseq; ++x) {
             if (opwave[x] < 0) continue;
             const SeqOp &o = seq_[x];
-            if (o.space == SPACE_CELL) g.cell_ops[nc[opwave[x]]++] = o.op;
-            else if (o.space == SPACE_FACE) g.face_ops[nf[opwave[x]]++] = o.op;
+            if (o.space == SPACE_CELL) g.cell_ops[nc[(size_t)opwave[x] * NT + o.op.type]++] = o.op;
+            else if (o.space == SPACE_FACE) g.face_ops[nf[(size_t)opwave[x] * NT + o.op.type]++] = o.op;
             else g.p_ops[np[opwave[x]]++] = groups_[o.op.dst];
         }
-        auto by_type = [](const FxGop &a, const FxGop &b) {
-            return a.type < b.type || (a.type == b.type && a.dst < b.dst);
-        };
         g.b_begin.assign(1, 0);
         for (int w = 0; w < nwaves; ++w) {
-            std::stable_sort(g.cell_ops.begin() + g.cell_begin[w], g.cell_ops.begin() + g.cell_begin[w + 1], by_type);
-            std::stable_sort(g.face_ops.begin() + g.face_begin[w], g.face_ops.begin() + g.face_begin[w + 1], by_type);
             if (w < (int)wb.size()) {
                 g.b_ops.insert(g.b_ops.end(), wb[w].begin(), wb[w].end());
             }
@@ -1163,6 +1221,8 @@ private:
     std::vector<Elem> wr_;       /* elements each op writes */
     std::vector<FxPop> groups_;  /* face-prolongation groups (SPACE_GROUP ops) */
     std::unordered_map<int64_t, ProlongSig> psig_;
+    std::vector<int64_t> g_reads_, g_writes_;             /* prolong_group scratch */
+    std::vector<std::pair<int64_t, ProlongSig>> g_sigs_;
     FxPlanStats stats_;
     std::string *err_ = nullptr;
     bool overflow_ = false;

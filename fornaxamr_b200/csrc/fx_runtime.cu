@@ -15,6 +15,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <chrono>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
@@ -83,6 +84,7 @@ struct fx_ctx {
     bool amr_set = false;
     fx_amr_config amr{};
     double E_injected = 0.0;          /* eos->E_injected of the remesh floors */
+    double amr_ms[6] = {0, 0, 0, 0, 0, 0}; /* host wall time of the phases of the last adapt */
 };
 
 namespace {
@@ -1306,18 +1308,27 @@ int fx_amr_adapt(fx_ctx *c, int *changed)
     if (!c->amr_set) return set_err(c, FX_EINVAL, "fx_amr_adapt: fx_amr_configure first");
     if (changed) *changed = 0;
     int rc;
+    using clk = std::chrono::steady_clock;
+    auto ms_since = [](clk::time_point t) { return std::chrono::duration<double, std::milli>(clk::now() - t).count(); };
+    const clk::time_point t_start = clk::now();
+    for (double &x : c->amr_ms) x = 0.0;
     fx_launch_set_dt(c->D, 0.0, c->stream);
     std::vector<int32_t> votes;
     if ((rc = amr_votes(c, votes))) return rc;
+    c->amr_ms[0] = ms_since(t_start);
+    clk::time_point t = clk::now();
     FxAmrResult res;
     std::string err;
     const int capacity = std::min(c->amr.max_blocks > 0 ? c->amr.max_blocks : 65535, 65535);
     if ((rc = fx_amr_remesh(c->cfg, c->amr, c->nblocks, c->blocks.data(), votes.data(), capacity, res, &err))) {
         return set_err(c, rc, "fx_amr_adapt: %s", err.c_str());
     }
+    c->amr_ms[1] = ms_since(t);
     if (!res.changed) {
+        c->amr_ms[5] = ms_since(t_start);
         return FX_SUCCESS;
     }
+    t = clk::now();
     const int nb = (int)res.blocks.size();
     if (nb > c->cap) {
         const int grown = std::min(std::max(nb, c->cap + c->cap / 4), capacity);
@@ -1408,8 +1419,10 @@ int fx_amr_adapt(fx_ctx *c, int *changed)
     fx_launch_amr_restrict_cells(c->D, d_pjobs.p, (int)pjobs.size(), floor,
         d_inj ? d_inj + cjobs.size() * (size_t)(FX_BS * FX_BS * FX_BS) : nullptr, s);
     FX_CUDA(c, cudaGetLastError());
+    c->amr_ms[2] = ms_since(t);
 
     /* the ghost fill of the new mesh compiles while the device moves data */
+    t = clk::now();
     FxPlan plan;
     if (!fx_build_plan(c->cfg, nb, res.blocks.data(), plan, &err)) {
         cudaFree(d_inj);
@@ -1421,6 +1434,8 @@ int fx_amr_adapt(fx_ctx *c, int *changed)
     c->blocks = std::move(res.blocks);
     c->nblocks = nb;
     c->nactive = (int)c->plan.active.size();
+    c->amr_ms[3] = ms_since(t);
+    t = clk::now();
     if ((rc = install_tables(c))) {
         cudaFree(d_inj);
         return rc;
@@ -1452,7 +1467,16 @@ int fx_amr_adapt(fx_ctx *c, int *changed)
     } else if ((rc = sync_and_check(c))) {
         return rc;
     }
+    c->amr_ms[4] = ms_since(t);
+    c->amr_ms[5] = ms_since(t_start);
     if (changed) *changed = 1;
+    return FX_SUCCESS;
+}
+
+int fx_amr_timings(fx_ctx *c, double *ms)
+{
+    if (!c || !ms) return c ? set_err(c, FX_EINVAL, "null argument") : FX_EINVAL;
+    for (int q = 0; q < 6; ++q) ms[q] = c->amr_ms[q];
     return FX_SUCCESS;
 }
 

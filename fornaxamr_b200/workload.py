@@ -3,6 +3,7 @@ cases the kernel profiles are taken on).
 
     python -m fornaxamr_b200.workload [--problem fourier|blast|collapse]
         [--root R] [--steps N] [--form batched|plain] [--adjoint N] [--shape S]
+        [--amr-interval K [--max-level L]]
 
 fourier: uniform root^3 mesh of 16^3 blocks on [0,1]^3 with the seeded
 Fourier-mode MHD state (fornaxamr_b200.problems.fourier_mhd).
@@ -12,7 +13,9 @@ collapse: static AMR gravity collapse, root^3 roots on [-1, 1]^3, spheres
 0.4 / 0.2 / 0.1 about the origin.
 
 Runs the driver's initial ghost fill and N driver steps (calc_dt + RK2 step)
-and prints the time per step.  With --adjoint N (fourier only, amplitude
+and prints the time per step.  With --amr-interval K the mesh adapts every K
+steps (prj_amr_adapt with a Loehner pressure criterion, refine 0.3 /
+derefine 0.1, up to level L, default 3) and the adapt phases are printed.  With --adjoint N (fourier only, amplitude
 0.01, |k| <= 3) it runs N fixed-dt steps storing every stage, then one
 reverse sweep, and prints the reverse sweep's device time per step.
 """
@@ -33,6 +36,8 @@ def main():
     ap.add_argument("--modes", type=int, default=32)
     ap.add_argument("--adjoint", type=int, default=0)
     ap.add_argument("--shape", type=int, default=-1, help="force a face-kernel launch shape (fx_set_flux_shape)")
+    ap.add_argument("--amr-interval", type=int, default=0)
+    ap.add_argument("--max-level", type=int, default=3)
     args = ap.parse_args()
 
     import fornaxamr_b200 as fx
@@ -86,6 +91,22 @@ def main():
         ctx.close()
         return
     form = fx.FORM_BATCHED if args.form == "batched" else fx.FORM_PLAIN
+    if args.amr_interval > 0:
+        ctx.amr_configure(fx.amr_config((args.root,) * 3, args.max_level, [
+            dict(estimator=fx.AMR_LOEHNER, refine=0.3, derefine=0.1, var=fx.AMR_VAR_PRESSURE)]))
+        state = (0.0, 0.0, 0)
+        t0 = time.perf_counter()
+        for _ in range(max(args.steps // args.amr_interval, 1)):
+            state = ctx.run(form, args.amr_interval, 0.4, 1.2, 1.0e30, state)
+            changed = ctx.amr_adapt()
+            t = ctx.amr_timings()
+            print(f"step {int(state[2])}: adapt changed={changed} blocks={ctx.nblocks} " +
+                  " ".join(f"{k}={v:.1f}ms" for k, v in t.items()), flush=True)
+        ctx.sync()
+        dt = time.perf_counter() - t0
+        print(f"{int(state[2])} steps with adapts every {args.amr_interval}: wall {1e3 * dt / max(int(state[2]), 1):.3f} ms/step")
+        ctx.close()
+        return
     t0 = time.perf_counter()
     state = ctx.run(form, args.steps, 0.4, 1.2, 1.0e30, (0.0, 0.0, 0))
     ctx.sync()

@@ -293,6 +293,12 @@ int fx_amr_adapt(fx_ctx *ctx, int *changed);
 int fx_get_mesh(fx_ctx *ctx, int capacity, fx_block_desc *out, int *nblocks);
 /* Energy added by the E_floor of all remeshes so far (eos->E_injected). */
 int fx_amr_energy_injected(fx_ctx *ctx, double *e);
+/* Host wall time (ms) of the phases of the last fx_amr_adapt: ms[0] device
+ * tag (with its read-back), ms[1] host remesh, ms[2] data moves queued
+ * (and any array growth), ms[3] ghost-fill compile of the new mesh (the data
+ * moves run on the device meanwhile), ms[4] tables, refill and
+ * synchronisation, ms[5] total. */
+int fx_amr_timings(fx_ctx *ctx, double *ms);
 
 /* Host-only remesh (no device): the block-tree half of prj_amr_adapt for
  * given per-block tag votes.  votes[3 b .. 3 b + 2] = refine vote (0/1),

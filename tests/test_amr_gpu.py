@@ -133,12 +133,10 @@ def test_driver_loop_with_adapts_matches_reference(ref_mhd):
     configure(ctx, ref_mhd, p, [dict(estimator=L, refine=0.25, derefine=0.1, var=1),
                                 dict(estimator=R.EST_VELOCITY, refine=0.5, derefine=0.05)], 2)
     n, t_ref, dt_ref, st_ref, changes = ref_mhd.run_amr(6, 2)
-    state = (0.0, 0.0, 0.0)
-    mine = 0
-    for _ in range(3):
-        state = ctx.run(fx.FORM_BATCHED, 2, p.cfl, p.dt_factor, p.t_end, state)
-        mine += int(ctx.amr_adapt())
+    state, mine = ctx.run_amr(fx.FORM_BATCHED, 6, 2, p.cfl, p.dt_factor, p.t_end, (0.0, 0.0, 0.0))
     assert mine == changes and changes >= 1
+    t = ctx.amr_timings()
+    assert t["total"] > 0.0 and t["compile"] > 0.0
     assert state == (t_ref, dt_ref, st_ref)
     assert_mesh_equal(ctx, ref_mhd)
     assert_active_state_equal(ctx, ref_mhd, True)
