@@ -54,6 +54,61 @@ int compile_threads()
 
 /* runs fn(t) for t in [0, n) on n threads (the calling thread takes t = 0) */
 template <typename F>
+void parallel_for(int n, F fn);
+
+/* stable sort of ops by destination key (keys are below 2^31; face keys
+ * repeat across the three face directions): a parallel stable
+ * most-significant pass on key >> 13 (the block, with two face bits), then
+ * each bin stable-sorted on its own */
+void sort_by_dst(FxGop *a, size_t n, int nt)
+{
+    if (n < 2) return;
+    uint32_t top = 0;
+    for (size_t q = 0; q < n; ++q) top = std::max(top, (uint32_t)a[q].dst >> 13);
+    const size_t nbins = (size_t)top + 1;
+    nt = (int)std::max<size_t>(1, std::min<size_t>((size_t)nt, n / 65536 + 1));
+    std::vector<size_t> cnt((size_t)nt * nbins, 0);
+    auto chunk = [&](int t, size_t &lo, size_t &hi) {
+        lo = n * (size_t)t / (size_t)nt;
+        hi = n * (size_t)(t + 1) / (size_t)nt;
+    };
+    parallel_for(nt, [&](int t) {
+        size_t lo, hi;
+        chunk(t, lo, hi);
+        size_t *c = cnt.data() + (size_t)t * nbins;
+        for (size_t q = lo; q < hi; ++q) ++c[(uint32_t)a[q].dst >> 13];
+    });
+    /* exclusive offsets: bin-major, thread-minor (keeps the scatter stable) */
+    std::vector<size_t> bin_begin(nbins + 1, 0);
+    size_t run = 0;
+    for (size_t bin = 0; bin < nbins; ++bin) {
+        bin_begin[bin] = run;
+        for (int t = 0; t < nt; ++t) {
+            const size_t v = cnt[(size_t)t * nbins + bin];
+            cnt[(size_t)t * nbins + bin] = run;
+            run += v;
+        }
+    }
+    bin_begin[nbins] = run;
+    std::vector<FxGop> tmp(n);
+    parallel_for(nt, [&](int t) {
+        size_t lo, hi;
+        chunk(t, lo, hi);
+        size_t *c = cnt.data() + (size_t)t * nbins;
+        for (size_t q = lo; q < hi; ++q) tmp[c[(uint32_t)a[q].dst >> 13]++] = a[q];
+    });
+    parallel_for(nt, [&](int t) {
+        for (size_t bin = (size_t)t; bin < nbins; bin += (size_t)nt) {
+            FxGop *x = tmp.data() + bin_begin[bin];
+            const size_t m = bin_begin[bin + 1] - bin_begin[bin];
+            std::stable_sort(x, x + m, [](const FxGop &u, const FxGop &v) { return u.dst < v.dst; });
+            std::memcpy(a + bin_begin[bin], x, m * sizeof(FxGop));
+        }
+    });
+}
+
+/* runs fn(t) for t in [0, n) on n threads (the calling thread takes t = 0) */
+template <typename F>
 void parallel_for(int n, F fn)
 {
     std::vector<std::thread> th;
@@ -1197,6 +1252,21 @@ private:
             if (o.space == SPACE_CELL) g.cell_ops[nc[(size_t)opwave[x] * NT + o.op.type]++] = o.op;
             else if (o.space == SPACE_FACE) g.face_ops[nf[(size_t)opwave[x] * NT + o.op.type]++] = o.op;
             else g.p_ops[np[opwave[x]]++] = groups_[o.op.dst];
+        }
+        /* within a (wave, type) bucket, destination order: neighbouring
+         * threads of the fill kernel then store to neighbouring addresses */
+        {
+            std::vector<std::pair<FxGop *, size_t>> buckets;
+            for (size_t q = 0; q + 1 < nc.size(); ++q) {
+                const int lo = q == 0 ? 0 : nc[q - 1];
+                if (nc[q] > lo) buckets.emplace_back(g.cell_ops.data() + lo, (size_t)(nc[q] - lo));
+            }
+            for (size_t q = 0; q + 1 < nf.size(); ++q) {
+                const int lo = q == 0 ? 0 : nf[q - 1];
+                if (nf[q] > lo) buckets.emplace_back(g.face_ops.data() + lo, (size_t)(nf[q] - lo));
+            }
+            const int nt = compile_threads();
+            for (const auto &bk : buckets) sort_by_dst(bk.first, bk.second, nt);
         }
         g.b_begin.assign(1, 0);
         for (int w = 0; w < nwaves; ++w) {

@@ -135,11 +135,10 @@ def test_driver_loop_with_adapts_matches_reference(ref_mhd):
     n, t_ref, dt_ref, st_ref, changes = ref_mhd.run_amr(6, 2)
     state, mine = ctx.run_amr(fx.FORM_BATCHED, 6, 2, p.cfl, p.dt_factor, p.t_end, (0.0, 0.0, 0.0))
     assert mine == changes and changes >= 1
-    t = ctx.amr_timings()
-    assert t["total"] > 0.0 and t["compile"] > 0.0
     assert state == (t_ref, dt_ref, st_ref)
     assert_mesh_equal(ctx, ref_mhd)
     assert_active_state_equal(ctx, ref_mhd, True)
+    assert ctx.amr_timings()["total"] > 0.0
     ctx.close()
 
 
