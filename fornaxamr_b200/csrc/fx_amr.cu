@@ -18,10 +18,11 @@
  *   k_amr_restrict_cells  prj_amr_restrict, src/prj_amr.c:2310-2387, then the
  *                         same field and primitive sync
  *
- * One CTA per block: the tag reduces its votes in shared memory, the
- * prolongation stages the parent's conserved octant (10^3 cells with the
- * stencil halo) in shared memory, the restriction replays the reference's
- * overlap loops per parent cell.
+ * The tag runs one CTA per block and reduces its votes in shared memory;
+ * the prolongation stages the parent's conserved octant (10^3 cells with
+ * the stencil halo) in shared memory, one CTA per child; the restriction
+ * replays the reference's overlap loops per parent cell, one CTA per
+ * (parent, i plane).
  */
 #include <cuda_runtime.h>
 
@@ -462,60 +463,59 @@ __global__ void __launch_bounds__(256) k_amr_restrict_faces(FxDev D, const FxAmr
 }
 
 /* prj_amr_restrict's overlap loops per parent cell, every conserved
- * variable at once (each keeps the reference's summation order) */
+ * variable at once (each keeps the reference's summation order); one CTA
+ * per (parent, i plane), one thread per (j, k) */
 template <bool MHD>
 __global__ void __launch_bounds__(256) k_amr_restrict_cells(FxDev D, const FxAmrParentJob *__restrict__ jobs,
     double E_floor, double *inj)
 {
     constexpr int NV = MHD ? 9 : 6;
-    const FxAmrParentJob J = jobs[blockIdx.x];
+    const FxAmrParentJob J = jobs[blockIdx.y];
     const FxBlockDev P = D.blk[J.parent];
-    double *injb = (inj != nullptr && E_floor > 0.0) ? inj + (size_t)blockIdx.x * FX_BS * FX_BS * FX_BS : nullptr;
-    for (int t = threadIdx.x; t < FX_BS * FX_BS * FX_BS; t += blockDim.x) {
-        const int i = t >> 8, j = (t >> 4) & 15, k = t & 15;
-        const double pvol = P.dx[0] * P.dx[1] * P.dx[2];
-        const double pxmin = P.xmin[0] + (double)i * P.dx[0];
-        const double pxmax = pxmin + P.dx[0];
-        const double pymin = P.xmin[1] + (double)j * P.dx[1];
-        const double pymax = pymin + P.dx[1];
-        const double pzmin = P.xmin[2] + (double)k * P.dx[2];
-        const double pzmax = pzmin + P.dx[2];
-        double sum[FX_MAXVAR];
-        for (int v = 0; v < NV; ++v) sum[v] = 0.0;
-        for (int oct = 0; oct < 8; ++oct) {
-            const int cb = J.children[oct];
-            const FxBlockDev C = D.blk[cb];
-            const double *Wc = D.W + (size_t)cb * FX_W_COUNT(D.nv);
-            for (int fi = 0; fi < FX_BS; ++fi) {
-                const double fxmin = C.xmin[0] + (double)fi * C.dx[0];
-                const double fxmax = fxmin + C.dx[0];
-                const double xover = (pxmax < fxmax ? pxmax : fxmax) - (pxmin > fxmin ? pxmin : fxmin);
-                if (xover <= 0.0) continue;
-                for (int fj = 0; fj < FX_BS; ++fj) {
-                    const double fymin = C.xmin[1] + (double)fj * C.dx[1];
-                    const double fymax = fymin + C.dx[1];
-                    const double yover = (pymax < fymax ? pymax : fymax) - (pymin > fymin ? pymin : fymin);
-                    if (yover <= 0.0) continue;
-                    for (int fk = 0; fk < FX_BS; ++fk) {
-                        const double fzmin = C.xmin[2] + (double)fk * C.dx[2];
-                        const double fzmax = fzmin + C.dx[2];
-                        const double zover = (pzmax < fzmax ? pzmax : fzmax) - (pzmin > fzmin ? pzmin : fzmin);
-                        if (zover > 0.0) {
-                            const double ov = xover * yover * zover;
-                            const int c = fx_lidx(fi, fj, fk);
-                            double w[FX_MAXVAR], u[FX_MAXVAR];
-                            for (int v = 0; v < NV; ++v) w[v] = Wc[(size_t)v * kPlane + c];
-                            fx_prim2cons<MHD>(w, u);
-                            for (int v = 0; v < NV; ++v) sum[v] += u[v] * ov;
-                        }
+    double *injb = (inj != nullptr && E_floor > 0.0) ? inj + (size_t)blockIdx.y * FX_BS * FX_BS * FX_BS : nullptr;
+    const int i = blockIdx.x, j = threadIdx.x >> 4, k = threadIdx.x & 15;
+    const double pvol = P.dx[0] * P.dx[1] * P.dx[2];
+    const double pxmin = P.xmin[0] + (double)i * P.dx[0];
+    const double pxmax = pxmin + P.dx[0];
+    const double pymin = P.xmin[1] + (double)j * P.dx[1];
+    const double pymax = pymin + P.dx[1];
+    const double pzmin = P.xmin[2] + (double)k * P.dx[2];
+    const double pzmax = pzmin + P.dx[2];
+    double sum[FX_MAXVAR];
+    for (int v = 0; v < NV; ++v) sum[v] = 0.0;
+    for (int oct = 0; oct < 8; ++oct) {
+        const int cb = J.children[oct];
+        const FxBlockDev C = D.blk[cb];
+        const double *Wc = D.W + (size_t)cb * FX_W_COUNT(D.nv);
+        for (int fi = 0; fi < FX_BS; ++fi) {
+            const double fxmin = C.xmin[0] + (double)fi * C.dx[0];
+            const double fxmax = fxmin + C.dx[0];
+            const double xover = (pxmax < fxmax ? pxmax : fxmax) - (pxmin > fxmin ? pxmin : fxmin);
+            if (xover <= 0.0) continue;
+            for (int fj = 0; fj < FX_BS; ++fj) {
+                const double fymin = C.xmin[1] + (double)fj * C.dx[1];
+                const double fymax = fymin + C.dx[1];
+                const double yover = (pymax < fymax ? pymax : fymax) - (pymin > fymin ? pymin : fymin);
+                if (yover <= 0.0) continue;
+                for (int fk = 0; fk < FX_BS; ++fk) {
+                    const double fzmin = C.xmin[2] + (double)fk * C.dx[2];
+                    const double fzmax = fzmin + C.dx[2];
+                    const double zover = (pzmax < fzmax ? pzmax : fzmax) - (pzmin > fzmin ? pzmin : fzmin);
+                    if (zover > 0.0) {
+                        const double ov = xover * yover * zover;
+                        const int c = fx_lidx(fi, fj, fk);
+                        double w[FX_MAXVAR], u[FX_MAXVAR];
+                        for (int v = 0; v < NV; ++v) w[v] = Wc[(size_t)v * kPlane + c];
+                        fx_prim2cons<MHD>(w, u);
+                        for (int v = 0; v < NV; ++v) sum[v] += u[v] * ov;
                     }
                 }
             }
         }
-        double u[FX_MAXVAR];
-        for (int v = 0; v < NV; ++v) u[v] = sum[v] / pvol;
-        store_cell<MHD>(D, J.parent, i, j, k, u, E_floor, injb);
     }
+    double u[FX_MAXVAR];
+    for (int v = 0; v < NV; ++v) u[v] = sum[v] / pvol;
+    store_cell<MHD>(D, J.parent, i, j, k, u, E_floor, injb);
 }
 
 } /* namespace */
@@ -569,8 +569,8 @@ void fx_launch_amr_restrict_cells(const FxDev &D, const FxAmrParentJob *jobs, in
 {
     if (n <= 0) return;
     if (D.nv == 9) {
-        k_amr_restrict_cells<true><<<n, 256, 0, s>>>(D, jobs, E_floor, inj);
+        k_amr_restrict_cells<true><<<dim3(FX_BS, n), 256, 0, s>>>(D, jobs, E_floor, inj);
     } else {
-        k_amr_restrict_cells<false><<<n, 256, 0, s>>>(D, jobs, E_floor, inj);
+        k_amr_restrict_cells<false><<<dim3(FX_BS, n), 256, 0, s>>>(D, jobs, E_floor, inj);
     }
 }
