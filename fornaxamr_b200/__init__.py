@@ -18,8 +18,8 @@ from ._lib import (ARR_BF, ARR_BV1, ARR_BV2, ARR_EMF, ARR_EOSVAR, ARR_FLUX, ARR_
                    ARR_VRIEMANN, ARR_W, BC_OUTFLOW, BC_PERIODIC, BC_REFLECT, BC_USER, FORM_BATCHED,
                    FORM_PLAIN, PHASE_CELLS, PHASE_CT, PHASE_EMF, PHASE_FLUX, PHASE_GHOST, PHASE_STEP,
                    AMR_FRACTIONAL_JUMP, AMR_LOEHNER, AMR_PRESSURE_SCALE_HEIGHT, AMR_VAR_DENSITY,
-                   AMR_VAR_PRESSURE, AMR_VAR_TEMPERATURE, AMR_VELOCITY, FxAmrConfig, FxBlockDesc,
-                   FxConfig)
+                   AMR_VAR_PRESSURE, AMR_VAR_TEMPERATURE, AMR_VELOCITY, INT_ESSPRK10_4, INT_RK2,
+                   RECON_MC, RECON_WENO3, FxAmrConfig, FxBlockDesc, FxConfig)
 
 __all__ = ["Context", "FxError", "FORM_PLAIN", "FORM_BATCHED", "NCELLS", "NFACES", "NEDGES",
            "library", "plan_export", "amr_config", "amr_remesh_host"]
@@ -50,8 +50,11 @@ def _dp(a: np.ndarray):
 
 
 def make_config(mhd: bool, gamma: float, coord: Sequence[float], bc: Sequence[int] = (0,) * 6,
-                gravity: bool = False, mhd_eta: float = 0.0) -> FxConfig:
+                gravity: bool = False, mhd_eta: float = 0.0, recon: int = RECON_MC,
+                integrator: int = INT_RK2) -> FxConfig:
     cfg = FxConfig()
+    cfg.recon = int(recon)
+    cfg.integrator = int(integrator)
     cfg.mhd = 1 if mhd else 0
     cfg.gravity = 1 if gravity else 0
     cfg.gamma = float(gamma)
@@ -146,11 +149,14 @@ class Context:
     """One device context (fx_ctx) with a mesh mirror."""
 
     def __init__(self, mhd: bool, gamma: float, coord: Sequence[float], bc: Sequence[int] = (0,) * 6,
-                 gravity: bool = False, mhd_eta: float = 0.0, device: int = 0):
+                 gravity: bool = False, mhd_eta: float = 0.0, device: int = 0, recon: int = RECON_MC,
+                 integrator: int = INT_RK2):
         self.L = library()
         self.mhd = bool(mhd)
         self.nv = 9 if mhd else 6
-        self.cfg = make_config(mhd, gamma, coord, bc, gravity, mhd_eta)
+        # stage slots of the block W / Bf arrays: 2 (RK2) or 3 (eSSPRK10_4)
+        self.ns = 3 if integrator == INT_ESSPRK10_4 else 2
+        self.cfg = make_config(mhd, gamma, coord, bc, gravity, mhd_eta, recon, integrator)
         self._h = C.c_void_p()
         rc = self.L.fx_create(device, C.byref(self.cfg), C.byref(self._h))
         if rc != 0:
@@ -204,12 +210,12 @@ class Context:
         self._check(self.L.fx_upload_block(self._h, b, _dp(W), bfp, gp))
 
     def download_block(self, b: int):
-        W = np.empty(self.nv * NSTAGES * NCELLS)
+        W = np.empty(self.nv * self.ns * NCELLS)
         eos = np.empty(3 * NCELLS)
         bfp = None
         Bf = None
         if self.mhd:
-            Bf = [np.empty(NSTAGES * NFACES) for _ in range(3)]
+            Bf = [np.empty(self.ns * NFACES) for _ in range(3)]
             bfp = (C.POINTER(C.c_double) * 3)(*[_dp(x) for x in Bf])
         self._check(self.L.fx_download_block(self._h, b, _dp(W), _dp(eos), bfp))
         return W, eos, Bf
@@ -225,9 +231,9 @@ class Context:
         self._check(self.L.fx_download_all(self._h, w, f))
 
     def download_array(self, b: int, which: int, dir_: int = 0) -> np.ndarray:
-        sizes = {ARR_W: self.nv * NSTAGES * NCELLS, ARR_EOSVAR: 3 * NCELLS, ARR_RHS: self.nv * NCELLS,
+        sizes = {ARR_W: self.nv * self.ns * NCELLS, ARR_EOSVAR: 3 * NCELLS, ARR_RHS: self.nv * NCELLS,
                  ARR_FLUX: self.nv * NCELLS, ARR_VRIEMANN: 3 * NCELLS, ARR_GRAV: NCELLS,
-                 ARR_BF: NSTAGES * NFACES, ARR_BV1: NCELLS, ARR_BV2: NCELLS, ARR_EMF: NEDGES}
+                 ARR_BF: self.ns * NFACES, ARR_BV1: NCELLS, ARR_BV2: NCELLS, ARR_EMF: NEDGES}
         out = np.empty(sizes[which])
         self._check(self.L.fx_download_array(self._h, b, which, dir_, _dp(out)))
         return out

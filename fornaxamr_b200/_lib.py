@@ -57,8 +57,13 @@ class FxConfig(C.Structure):
         ("coord", C.c_double * 6),
         ("bc", C.c_int32 * 6),
         ("mhd_eta", C.c_double),
+        ("recon", C.c_int32),
+        ("integrator", C.c_int32),
     ]
 
+
+RECON_MC, RECON_WENO3 = 0, 1
+INT_RK2, INT_ESSPRK10_4 = 0, 1
 
 AMR_N = 4
 AMR_LOEHNER, AMR_VELOCITY, AMR_PRESSURE_SCALE_HEIGHT, AMR_FRACTIONAL_JUMP = 0, 1, 2, 3

@@ -279,17 +279,37 @@ __global__ void k_amr_zero(FxDev D, const int *__restrict__ blocks)
     const size_t nbf = D.Bf ? (size_t)FX_BF_COUNT : 0;
     const size_t ne = (size_t)FX_EOS_COUNT;
     const size_t ng = D.grav ? (size_t)FX_GRAV_COUNT : 0;
-    const size_t total = nw + nbf + ne + ng;
+    const size_t nw2 = D.W2 ? (size_t)D.nv * FX_NCELLS : 0;
+    const size_t nb2 = D.Bf2 ? (size_t)3 * FX_NFACES : 0;
+    const size_t total = nw + nbf + ne + ng + nw2 + nb2;
     for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (size_t)gridDim.x * blockDim.x) {
-        if (e < nw) {
-            D.W[(size_t)b * nw + e] = 0.0;
-        } else if (e < nw + nbf) {
-            D.Bf[(size_t)b * FX_BF_COUNT + (e - nw)] = 0.0;
-        } else if (e < nw + nbf + ne) {
-            D.eos[(size_t)b * FX_EOS_COUNT + (e - nw - nbf)] = 0.0;
-        } else {
-            D.grav[(size_t)b * FX_GRAV_COUNT + (e - nw - nbf - ne)] = 0.0;
+        size_t q = e;
+        if (q < nw) {
+            D.W[(size_t)b * nw + q] = 0.0;
+            continue;
         }
+        q -= nw;
+        if (q < nbf) {
+            D.Bf[(size_t)b * FX_BF_COUNT + q] = 0.0;
+            continue;
+        }
+        q -= nbf;
+        if (q < ne) {
+            D.eos[(size_t)b * FX_EOS_COUNT + q] = 0.0;
+            continue;
+        }
+        q -= ne;
+        if (q < ng) {
+            D.grav[(size_t)b * FX_GRAV_COUNT + q] = 0.0;
+            continue;
+        }
+        q -= ng;
+        if (q < nw2) {
+            D.W2[(size_t)b * nw2 + q] = 0.0;
+            continue;
+        }
+        q -= nw2;
+        D.Bf2[(size_t)b * nb2 + q] = 0.0;
     }
 }
 

@@ -17,6 +17,7 @@
  */
 #include <cuda_runtime.h>
 
+#include "../../include/fornax_b200.h"
 #include "fx_kernels.h"
 #include "fx_physics.cuh"
 
@@ -57,7 +58,23 @@ __device__ __forceinline__ unsigned long long fx_double_key(double d)
  * face velocity, Bv1/Bv2).  blockIdx.z is the sweep direction.  TPB/MINB
  * set the launch shape (threads per CTA, resident CTAs per SM the register
  * allocation must allow); the autotuner picks among the compiled shapes. */
-template <bool MHD, bool FULL, int TPB, int MINB>
+/* left state of the face from cells (qm, q0, q1), right state from (q0,
+ * q1, q2): MC slopes (the reference's fast path, prj_flux_recon_var_mc:
+ * q +- 0.5 slope) or WENO-Z3 face values (its per-face path,
+ * src/prj_flux.c:440-475) */
+template <int RECON>
+__device__ __forceinline__ void fx_recon_pair(double qm, double q0, double q1, double q2, double &wl, double &wr)
+{
+    if (RECON == FX_RECON_WENO3) {
+        wl = fx_weno3_face(qm, q0, q1, 0.5);
+        wr = fx_weno3_face(q0, q1, q2, -0.5);
+    } else {
+        wl = q0 + 0.5 * fx_mc_slope(qm, q0, q1);
+        wr = q1 - 0.5 * fx_mc_slope(q0, q1, q2);
+    }
+}
+
+template <bool MHD, bool FULL, int TPB, int MINB, int RECON>
 __global__ void __launch_bounds__(TPB, MINB) k_flux(FxDev D, const int *__restrict__ blist,
     int wslot, int bfslot)
 {
@@ -101,10 +118,8 @@ __global__ void __launch_bounds__(TPB, MINB) k_flux(FxDev D, const int *__restri
         q = Wb + (size_t)FX_EINT * kPlane;
         eint4[0] = q[cL - s]; eint4[1] = q[cL]; eint4[2] = q[cR]; eint4[3] = q[cR + s];
     }
-    WL[FX_RHO] = rho4[1] + 0.5 * fx_mc_slope(rho4[0], rho4[1], rho4[2]);
-    WR[FX_RHO] = rho4[2] - 0.5 * fx_mc_slope(rho4[1], rho4[2], rho4[3]);
-    WL[FX_EINT] = eint4[1] + 0.5 * fx_mc_slope(eint4[0], eint4[1], eint4[2]);
-    WR[FX_EINT] = eint4[2] - 0.5 * fx_mc_slope(eint4[1], eint4[2], eint4[3]);
+    fx_recon_pair<RECON>(rho4[0], rho4[1], rho4[2], rho4[3], WL[FX_RHO], WR[FX_RHO]);
+    fx_recon_pair<RECON>(eint4[0], eint4[1], eint4[2], eint4[3], WL[FX_EINT], WR[FX_EINT]);
 #pragma unroll
     for (int lv = 1; lv < nv; ++lv) {
         if (lv == FX_EINT || (MHD && lv == FX_B1)) {
@@ -115,20 +130,23 @@ __global__ void __launch_bounds__(TPB, MINB) k_flux(FxDev D, const int *__restri
         const double q0 = q[cL];
         const double q1 = q[cR];
         const double q2 = q[cR + s];
-        WL[lv] = q0 + 0.5 * fx_mc_slope(qm, q0, q1);
-        WR[lv] = q1 - 0.5 * fx_mc_slope(q0, q1, q2);
+        fx_recon_pair<RECON>(qm, q0, q1, q2, WL[lv], WR[lv]);
     }
     double p4[4];
 #pragma unroll
     for (int n = 0; n < 4; ++n) {
         p4[n] = fx_pressure(g, rho4[n], eint4[n]);
     }
-    const double pL = p4[1] + 0.5 * fx_mc_slope(p4[0], p4[1], p4[2]);
-    const double pR = p4[2] - 0.5 * fx_mc_slope(p4[1], p4[2], p4[3]);
+    double pL, pR;
+    fx_recon_pair<RECON>(p4[0], p4[1], p4[2], p4[3], pL, pR);
     /* gamma is uniform for the ideal gas: its MC slope is exactly 0, so the
-     * reconstructed face values equal g bit for bit. */
-    const double gL = g;
-    const double gR = g;
+     * MC face values equal g bit for bit; the WENO-Z3 weights of a constant
+     * stencil are evaluated as the reference does (their sum need not be 1) */
+    double gL = g, gR = g;
+    if (RECON == FX_RECON_WENO3) {
+        gL = fx_weno3_face(g, g, g, 0.5);
+        gR = fx_weno3_face(g, g, g, -0.5);
+    }
 
     const size_t fbase = (size_t)b * FX_FLUX_COUNT(nv) + (size_t)dir * nv * FX_NCELLS;
     const size_t vbase = (size_t)b * FX_VR_COUNT + (size_t)dir * 3 * FX_NCELLS;
@@ -300,7 +318,7 @@ __global__ void __launch_bounds__(128) k_bf_update(FxDev D, const int *__restric
     if (D.ctl->skip) {
         return;
     }
-    const double dt = D.ctl->dt;
+    const double dt = D.ctl->dt_stage;
     const int b = blist[blockIdx.y];
     constexpr int NF = (FX_BS + 1) * FX_BS * FX_BS;
     int t = blockIdx.x * blockDim.x + threadIdx.x;
@@ -315,7 +333,7 @@ __global__ void __launch_bounds__(128) k_bf_update(FxDev D, const int *__restric
     t /= x2;
     const int j = t % x1;
     const int i = t / x1;
-    const int src_slot = stage == 1 ? 0 : 1;
+    const int src_slot = stage == 2 ? 1 : 0;
     const int dst_slot = stage == 1 ? 1 : 0;
     double *bf = D.Bf + (size_t)b * FX_BF_COUNT;
     const double *e = D.emf + (size_t)b * FX_EMF_COUNT;
@@ -347,6 +365,9 @@ __global__ void __launch_bounds__(128) k_bf_update(FxDev D, const int *__restric
 /* ------------------------------------------------------------------------ */
 /* Cell update (flux divergence + sources + RK2 combine + cons2prim)         */
 /* ------------------------------------------------------------------------ */
+/* STAGE 1 / 2: the RK2 stages; STAGE 0: the stage-1 arithmetic written in
+ * place to slot 0 with the field of Bf slot 0 (an eSSPRK substep,
+ * prj_timeint_eSSPRK_step, src/prj_timeint.c:2484-2508) */
 template <bool MHD, int STAGE>
 __global__ void __launch_bounds__(128) k_cell_update(FxDev D, const int *__restrict__ blist,
     int gravity, int store_rhs)
@@ -354,7 +375,7 @@ __global__ void __launch_bounds__(128) k_cell_update(FxDev D, const int *__restr
     if (D.ctl->skip) {
         return;
     }
-    const double dt = D.ctl->dt;
+    const double dt = D.ctl->dt_stage;
     const int b = blist[blockIdx.y];
     constexpr int nv = MHD ? 9 : 6;
     int t = blockIdx.x * blockDim.x + threadIdx.x;
@@ -397,7 +418,7 @@ __global__ void __launch_bounds__(128) k_cell_update(FxDev D, const int *__restr
         rhs[v] = 0.0;
     }
     if (gravity) {
-        const double *Ws = W + (size_t)(STAGE == 1 ? 0 : 1) * FX_NCELLS;
+        const double *Ws = W + (size_t)(STAGE == 2 ? 1 : 0) * FX_NCELLS;
         const double *g = D.grav + (size_t)b * FX_GRAV_COUNT;
         const double g1 = g[c];
         const double g2 = g[FX_NCELLS + c];
@@ -427,7 +448,7 @@ __global__ void __launch_bounds__(128) k_cell_update(FxDev D, const int *__restr
     const double dt_src = 0.02 * u[FX_ETOT] / (fabs(rhs[FX_ETOT]) + 1.0e-50);
 
     double un[9];
-    if (STAGE == 1) {
+    if (STAGE != 2) {
 #pragma unroll
         for (int v = 0; v < 6; ++v) {
             un[v] = u[v] + dt * (rhs[v] + fluxdiv[v]);
@@ -449,7 +470,7 @@ __global__ void __launch_bounds__(128) k_cell_update(FxDev D, const int *__restr
     }
     if (MHD) {
         /* cell B from the updated faces, src/prj_timeint.c:498-510 */
-        const int bslot = STAGE == 1 ? 1 : 0;
+        const int bslot = STAGE == 1 ? 1 : 0;  /* slot the CT update wrote */
         const double *bf = D.Bf + (size_t)b * FX_BF_COUNT;
         const double *b1 = bf + (size_t)(0 * FX_NSTAGES + bslot) * FX_NFACES;
         const double *b2 = bf + (size_t)(1 * FX_NSTAGES + bslot) * FX_NFACES;
@@ -598,7 +619,8 @@ __global__ void k_step_begin(FxDev D)
         return;
     }
     c->skip = 0;
-    const double dt_new = fx_key_double(D.red[0]);
+    /* prj_timeint_calc_dt's minimum, times 6 for eSSPRK10_4 */
+    const double dt_new = fx_key_double(D.red[0]) * c->dt_mult;
     if (c->dt_prev > 0.0) {
         const double dt_limit = c->dt_factor * c->dt_prev;
         c->dt_prev = dt_new <= dt_limit ? dt_new : dt_limit;
@@ -610,6 +632,7 @@ __global__ void k_step_begin(FxDev D)
         dt_step = c->t_end - c->time;
     }
     c->dt = dt_step;
+    c->dt_stage = dt_step;
     D.red[1] = fx_double_key(1.0e100);
 }
 
@@ -962,6 +985,127 @@ __global__ void k_emf_correct(FxDev D, const FxCorr *__restrict__ recs, int n)
 
 
 /* ------------------------------------------------------------------------ */
+/* eSSPRK stored states (prj_timeint_eSSPRK_save_state / _blend_with_saved,  */
+/* src/prj_timeint.c:2311-2444)                                              */
+/* ------------------------------------------------------------------------ */
+
+__device__ __forceinline__ double *fx_saved_w(const FxDev &D, int b, int which)
+{
+    return which == 1 ? D.W + (size_t)b * FX_W_COUNT(D.nv) + FX_NCELLS
+                      : D.W2 + (size_t)b * D.nv * FX_NCELLS;
+}
+
+/* saved face array of direction d: stride of its faces is FX_NFACES */
+__device__ __forceinline__ double *fx_saved_bf(const FxDev &D, int b, int d, int which)
+{
+    return which == 1 ? D.Bf + (size_t)b * FX_BF_COUNT + ((size_t)d * FX_NSTAGES + 1) * FX_NFACES
+                      : D.Bf2 + ((size_t)b * 3 + d) * FX_NFACES;
+}
+
+/* W of the active cells (all variables) and every face of slot 0 */
+__global__ void k_essprk_save(FxDev D, const int *__restrict__ blist, int which)
+{
+    if (D.ctl->skip) {
+        return;
+    }
+    const int b = blist[blockIdx.y];
+    const int nv = D.nv;
+    const int ncell = FX_BS * FX_BS * FX_BS;
+    const int nface = D.Bf ? 3 * FX_NFACES : 0;
+    const double *W0 = D.W + (size_t)b * FX_W_COUNT(nv);
+    double *Ws = fx_saved_w(D, b, which);
+    const size_t wstride = which == 1 ? (size_t)FX_NSTAGES * FX_NCELLS : (size_t)FX_NCELLS;
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < nv * ncell + nface; t += gridDim.x * blockDim.x) {
+        if (t < nv * ncell) {
+            const int v = t / ncell;
+            const int r = t - v * ncell;
+            const int c = fx_lidx(r >> 8, (r >> 4) & 15, r & 15);
+            Ws[(size_t)v * wstride + c] = W0[(size_t)v * kPlane + c];
+        } else {
+            const int q = t - nv * ncell;
+            const int d = q / FX_NFACES;
+            const int f = q - d * FX_NFACES;
+            fx_saved_bf(D, b, d, which)[f] = D.Bf[(size_t)b * FX_BF_COUNT + (size_t)d * FX_NSTAGES * FX_NFACES + f];
+        }
+    }
+}
+
+/* prj_timeint_eSSPRK_blend_bf: active faces of slot 0 <- w saved + (1 - w) slot 0 */
+__global__ void __launch_bounds__(128) k_essprk_blend_faces(FxDev D, const int *__restrict__ blist, int which,
+    double w)
+{
+    if (D.ctl->skip) {
+        return;
+    }
+    const int b = blist[blockIdx.y];
+    constexpr int NF = (FX_BS + 1) * FX_BS * FX_BS;
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= 3 * NF) {
+        return;
+    }
+    const int dir = t / NF;
+    t -= dir * NF;
+    const int x2 = dir == 2 ? FX_BS + 1 : FX_BS;
+    const int x1 = dir == 1 ? FX_BS + 1 : FX_BS;
+    const int k = t % x2;
+    t /= x2;
+    const int j = t % x1;
+    const int i = t / x1;
+    const int f = fx_face_idx(dir, i, j, k);
+    const double cw = 1.0 - w;
+    double *bf0 = D.Bf + (size_t)b * FX_BF_COUNT + (size_t)dir * FX_NSTAGES * FX_NFACES;
+    bf0[f] = w * fx_saved_bf(D, b, dir, which)[f] + cw * bf0[f];
+}
+
+/* prj_timeint_eSSPRK_final_cell: conserved blend, field from the blended
+ * faces, cons2prim into slot 0 */
+template <bool MHD>
+__global__ void __launch_bounds__(128) k_essprk_blend_cells(FxDev D, const int *__restrict__ blist, int which,
+    double w)
+{
+    if (D.ctl->skip) {
+        return;
+    }
+    const int b = blist[blockIdx.y];
+    constexpr int nv = MHD ? 9 : 6;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= FX_BS * FX_BS * FX_BS) {
+        return;
+    }
+    const int i = t >> 8, j = (t >> 4) & 15, k = t & 15;
+    const int c = fx_lidx(i, j, k);
+    double *W0 = D.W + (size_t)b * FX_W_COUNT(nv);
+    const double *Ws = fx_saved_w(D, b, which);
+    const size_t wstride = which == 1 ? (size_t)FX_NSTAGES * FX_NCELLS : (size_t)FX_NCELLS;
+    const double cw = 1.0 - w;
+    double x[9], u[9], us[9];
+#pragma unroll
+    for (int v = 0; v < nv; ++v) x[v] = W0[(size_t)v * kPlane + c];
+    fx_prim2cons<MHD>(x, u);
+#pragma unroll
+    for (int v = 0; v < nv; ++v) x[v] = Ws[(size_t)v * wstride + c];
+    fx_prim2cons<MHD>(x, us);
+#pragma unroll
+    for (int v = 0; v < nv; ++v) u[v] = w * us[v] + cw * u[v];
+    if (MHD) {
+        /* prj_timeint_mhd_set_cons_b_from_bf (src/prj_timeint.c:498-510) on slot 0 */
+        const double *bf = D.Bf + (size_t)b * FX_BF_COUNT;
+        const double *b1 = bf;
+        const double *b2 = bf + (size_t)1 * FX_NSTAGES * FX_NFACES;
+        const double *b3 = bf + (size_t)2 * FX_NSTAGES * FX_NFACES;
+        u[FX_B1] = 0.5 * (b1[fx_face_idx(0, i, j, k)] + b1[fx_face_idx(0, i + 1, j, k)]);
+        u[FX_B2] = 0.5 * (b2[fx_face_idx(1, i, j, k)] + b2[fx_face_idx(1, i, j + 1, k)]);
+        u[FX_B3] = 0.5 * (b3[fx_face_idx(2, i, j, k)] + b3[fx_face_idx(2, i, j, k + 1)]);
+        if (!isfinite(u[FX_B1]) || !isfinite(u[FX_B2]) || !isfinite(u[FX_B3])) {
+            fx_fail(D.err, FX_ERR_B_NONFINITE, b, c);
+        }
+    }
+    fx_cons2prim<MHD>(u, x);
+#pragma unroll
+    for (int v = 0; v < nv; ++v) W0[(size_t)v * kPlane + c] = x[v];
+}
+
+/* ------------------------------------------------------------------------ */
 /* launchers                                                                 */
 /* ------------------------------------------------------------------------ */
 static inline unsigned fx_blocks(int n, int tpb) { return (unsigned)((n + tpb - 1) / tpb); }
@@ -969,19 +1113,25 @@ static inline unsigned fx_blocks(int n, int tpb) { return (unsigned)((n + tpb - 
 /* launch shapes of the face kernel: {threads per CTA, min CTAs per SM} */
 static const int kFluxShapes[FX_FLUX_VARIANTS][2] = {{128, 4}, {128, 5}, {128, 6}, {256, 2}, {256, 3}, {64, 8}};
 
-template <bool MHD, bool FULL, int TPB, int MINB>
+template <bool MHD, bool FULL, int TPB, int MINB, int RECON = FX_RECON_MC>
 static void launch_flux_shape(const FxDev &D, const int *blist, int nlist, int ndir, int wslot,
     int bfslot, cudaStream_t s)
 {
     const int nf = MHD ? (FX_BS + 1) * (FX_BS + 2) * (FX_BS + 2) : (FX_BS + 1) * FX_BS * FX_BS;
     const dim3 g(fx_blocks(nf, TPB), ndir, nlist);
-    k_flux<MHD, FULL, TPB, MINB><<<g, TPB, 0, s>>>(D, blist, wslot, bfslot);
+    k_flux<MHD, FULL, TPB, MINB, RECON><<<g, TPB, 0, s>>>(D, blist, wslot, bfslot);
 }
 
+/* WENO-Z3 is compiled in one launch shape (the autotuner's variants all map
+ * to it); MC in all of them */
 template <bool MHD, bool FULL>
 static void launch_flux_variant(const FxDev &D, const int *blist, int nlist, int ndir, int wslot,
     int bfslot, int variant, cudaStream_t s)
 {
+    if (D.recon == FX_RECON_WENO3) {
+        launch_flux_shape<MHD, FULL, 128, 4, FX_RECON_WENO3>(D, blist, nlist, ndir, wslot, bfslot, s);
+        return;
+    }
     switch (variant) {
     case 1: launch_flux_shape<MHD, FULL, 128, 5>(D, blist, nlist, ndir, wslot, bfslot, s); break;
     case 2: launch_flux_shape<MHD, FULL, 128, 6>(D, blist, nlist, ndir, wslot, bfslot, s); break;
@@ -1034,10 +1184,12 @@ void fx_launch_cell_update(const FxDev &D, const int *blist, int nlist, int stag
     const dim3 grid(fx_blocks(FX_BS * FX_BS * FX_BS, 128), nlist);
     if (D.nv == 9) {
         if (stage == 1) k_cell_update<true, 1><<<grid, 128, 0, s>>>(D, blist, gravity, store_rhs);
-        else k_cell_update<true, 2><<<grid, 128, 0, s>>>(D, blist, gravity, store_rhs);
+        else if (stage == 2) k_cell_update<true, 2><<<grid, 128, 0, s>>>(D, blist, gravity, store_rhs);
+        else k_cell_update<true, 0><<<grid, 128, 0, s>>>(D, blist, gravity, store_rhs);
     } else {
         if (stage == 1) k_cell_update<false, 1><<<grid, 128, 0, s>>>(D, blist, gravity, store_rhs);
-        else k_cell_update<false, 2><<<grid, 128, 0, s>>>(D, blist, gravity, store_rhs);
+        else if (stage == 2) k_cell_update<false, 2><<<grid, 128, 0, s>>>(D, blist, gravity, store_rhs);
+        else k_cell_update<false, 0><<<grid, 128, 0, s>>>(D, blist, gravity, store_rhs);
     }
 }
 
@@ -1108,7 +1260,13 @@ namespace {
 __global__ void k_set_dt(FxDev D, double dt)
 {
     D.ctl->dt = dt;
+    D.ctl->dt_stage = dt;
     D.ctl->skip = 0;
+}
+
+__global__ void k_stage_dt(FxDev D, double divisor)
+{
+    D.ctl->dt_stage = D.ctl->dt / divisor;
 }
 
 __global__ void k_set_ctl(FxDev D, FxCtl v)
@@ -1120,6 +1278,31 @@ __global__ void k_set_ctl(FxDev D, FxCtl v)
 void fx_launch_set_dt(const FxDev &D, double dt, cudaStream_t s)
 {
     k_set_dt<<<1, 1, 0, s>>>(D, dt);
+}
+
+void fx_launch_stage_dt(const FxDev &D, double divisor, cudaStream_t s)
+{
+    k_stage_dt<<<1, 1, 0, s>>>(D, divisor);
+}
+
+void fx_launch_essprk_save(const FxDev &D, const int *blist, int nlist, int which, cudaStream_t s)
+{
+    if (nlist <= 0) return;
+    k_essprk_save<<<dim3(32, nlist), 256, 0, s>>>(D, blist, which);
+}
+
+void fx_launch_essprk_blend(const FxDev &D, const int *blist, int nlist, int which, double w, cudaStream_t s)
+{
+    if (nlist <= 0) return;
+    if (D.nv == 9) {
+        const int nf = 3 * (FX_BS + 1) * FX_BS * FX_BS;
+        k_essprk_blend_faces<<<dim3(fx_blocks(nf, 128), nlist), 128, 0, s>>>(D, blist, which, w);
+        k_essprk_blend_cells<true><<<dim3(fx_blocks(FX_BS * FX_BS * FX_BS, 128), nlist), 128, 0, s>>>(
+            D, blist, which, w);
+    } else {
+        k_essprk_blend_cells<false><<<dim3(fx_blocks(FX_BS * FX_BS * FX_BS, 128), nlist), 128, 0, s>>>(
+            D, blist, which, w);
+    }
 }
 
 void fx_launch_set_ctl(const FxDev &D, FxCtl value, cudaStream_t s)

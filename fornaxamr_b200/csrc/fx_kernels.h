@@ -25,6 +25,8 @@ struct FxCtl {
     long long step;
     int skip;
     int pad;
+    double dt_stage;  /* dt of the stage kernels: dt (RK2) or dt / 6 (eSSPRK10_4 substeps) */
+    double dt_mult;   /* factor on the CFL minimum: 1 (RK2) or 6 (eSSPRK10_4) */
 };
 
 /* per-block geometry on the device */
@@ -56,6 +58,9 @@ struct FxDev {
     unsigned long long *red;  /* [0] dt min key, [1] dt_src min key */
     FxCtl *ctl;
     int flux_variant;         /* launch shape of the face kernel (autotuned) */
+    int recon;                /* FX_RECON_MC or FX_RECON_WENO3 */
+    double *W2;   /* eSSPRK10_4 stage slot 2 of W: [b][v][cell] (null for RK2) */
+    double *Bf2;  /* eSSPRK10_4 stage slot 2 of Bf: [b][dir][face] (null for RK2 or hydro) */
 };
 
 #define FX_FLUX_VARIANTS 6
@@ -135,9 +140,22 @@ struct FxCorr {
 void fx_launch_flux(const FxDev &D, const int *blist, int nlist, int ndir, int wslot, int bfslot,
     int full, cudaStream_t s);
 void fx_launch_emf(const FxDev &D, const int *blist, int nlist, int wslot, int bfslot, cudaStream_t s);
+/* stage 1, 2: the RK2 stages; stage 0: an eSSPRK forward-Euler substep in
+ * place on slot 0 (prj_timeint_mhd_update_bf stage 0 and the stage-1 cell
+ * update writing slot 0) */
 void fx_launch_bf_update(const FxDev &D, const int *blist, int nlist, int stage, cudaStream_t s);
 void fx_launch_cell_update(const FxDev &D, const int *blist, int nlist, int stage,
     int gravity, int store_rhs, cudaStream_t s);
+/* dt_stage = dt / divisor in the control block */
+void fx_launch_stage_dt(const FxDev &D, double divisor, cudaStream_t s);
+/* prj_timeint_eSSPRK_save_state (src/prj_timeint.c:2311-2352): W of the
+ * active cells and every Bf face of slot 0 into saved state `which` (1: slot
+ * 1, 2: W2 / Bf2) */
+void fx_launch_essprk_save(const FxDev &D, const int *blist, int nlist, int which, cudaStream_t s);
+/* prj_timeint_eSSPRK_blend_with_saved, cell and face part
+ * (src/prj_timeint.c:2354-2444): slot 0 <- w saved + (1 - w) slot 0 */
+void fx_launch_essprk_blend(const FxDev &D, const int *blist, int nlist, int which, double w,
+    cudaStream_t s);
 void fx_launch_eos_fill(const FxDev &D, const int *blist, int nlist, int wslot, int active_only,
     cudaStream_t s);
 void fx_launch_calc_dt(const FxDev &D, const int *blist, int nlist, int wslot, double cfl,

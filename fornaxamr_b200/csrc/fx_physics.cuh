@@ -106,6 +106,30 @@ FX_HD double fx_temperature(double g, double eint)
     return (g - 1.0) * eint / FX_IDEAL_ENERGY_SCALE;
 }
 
+/* WENO-Z3 face value of prj_reconstruct_weno3_face (src/prj_reconstruct.h:383-423):
+ * target +0.5 gives the i+1/2 (left) state of cell (qm, q0, qp), -0.5 the
+ * i-1/2 (right) state; Z weights alpha_k = gamma_k (1 + tau3 / (eps + beta_k)) */
+FX_HD double fx_weno3_face(double qm, double q0, double qp, double target)
+{
+    const double eps = 1.0e-40;
+    const double p0 = q0 + target * (q0 - qm);
+    const double p1 = q0 + target * (qp - q0);
+    const double dl = q0 - qm;
+    const double dr = qp - q0;
+    const double beta0 = dl * dl;
+    const double beta1 = dr * dr;
+    double tau3 = beta0 - beta1;
+    if (tau3 < 0.0) {
+        tau3 = -tau3;
+    }
+    const double gamma0 = target > 0.0 ? 1.0 / 3.0 : 2.0 / 3.0;
+    const double gamma1 = target > 0.0 ? 2.0 / 3.0 : 1.0 / 3.0;
+    const double alpha0 = gamma0 * (1.0 + tau3 / (eps + beta0));
+    const double alpha1 = gamma1 * (1.0 + tau3 / (eps + beta1));
+    const double sum = alpha0 + alpha1;
+    return (alpha0 * p0 + alpha1 * p1) / sum;
+}
+
 /* minmod slope of prj_reconstruct_minmod_slope (src/prj_reconstruct.h:46-62) */
 FX_HD double fx_minmod_slope(double qm, double q0, double qp)
 {

@@ -46,6 +46,7 @@ struct fx_ctx {
     double *d_W = nullptr, *d_Bf = nullptr, *d_flux = nullptr, *d_vr = nullptr;
     double *d_bv1 = nullptr, *d_bv2 = nullptr, *d_emf = nullptr, *d_eos = nullptr;
     double *d_rhs = nullptr, *d_grav = nullptr;
+    double *d_W2 = nullptr, *d_Bf2 = nullptr; /* eSSPRK10_4 stage slot 2 */
     int *d_ids = nullptr;
     int *d_active = nullptr;
     int nactive = 0;
@@ -200,6 +201,9 @@ void free_mesh(fx_ctx *c)
     cudaFree(c->d_eos);
     cudaFree(c->d_rhs);
     cudaFree(c->d_grav);
+    cudaFree(c->d_W2);
+    cudaFree(c->d_Bf2);
+    c->d_W2 = c->d_Bf2 = nullptr;
     cudaFree(c->d_ids);
     cudaFree(c->d_active);
     cudaFree(c->d_cops);
@@ -317,6 +321,76 @@ void stage_seq(fx_ctx *c, int form, int stage)
     c->last_slot = dst;
 }
 
+/* the refill after a substep or a blend: eos (active) -> ghost fill -> eos
+ * (mesh) on slot 0 */
+void refill0(fx_ctx *c, int form)
+{
+    cudaStream_t s = c->stream;
+    if (form == FX_FORM_PLAIN) {
+        per_block(c, form, [&](const int *l, int n) { fx_launch_eos_fill(c->D, l, n, 0, 1, s); });
+    }
+    ghost_fill(c, 0);
+    if (form == FX_FORM_PLAIN) {
+        per_block(c, form, [&](const int *l, int n) { fx_launch_eos_fill(c->D, l, n, 0, 0, s); });
+    }
+}
+
+/* one forward-Euler substep in place on slot 0, prj_timeint_eSSPRK_step
+ * (src/prj_timeint.c:2452-2550); dt_stage holds dt / 6 */
+void essprk_substep(fx_ctx *c, int form)
+{
+    cudaStream_t s = c->stream;
+    const int full = form == FX_FORM_PLAIN ? 1 : 0;
+    per_block(c, form, [&](const int *l, int n) { fx_launch_flux(c->D, l, n, 3, 0, 0, full, s); });
+    flux_correct(c, full ? c->nv : 6, s);
+    if (c->cfg.mhd) {
+        per_block(c, form, [&](const int *l, int n) { fx_launch_emf(c->D, l, n, 0, 0, s); });
+        emf_correct(c, s);
+        per_block(c, form, [&](const int *l, int n) { fx_launch_bf_update(c->D, l, n, 0, s); });
+    }
+    per_block(c, form, [&](const int *l, int n) {
+        fx_launch_cell_update(c->D, l, n, 0, c->cfg.gravity, full, s);
+    });
+    refill0(c, form);
+}
+
+void essprk_blend(fx_ctx *c, int form, int which, double w)
+{
+    per_block(c, form, [&](const int *l, int n) { fx_launch_essprk_blend(c->D, l, n, which, w, c->stream); });
+    refill0(c, form);
+}
+
+void essprk_save(fx_ctx *c, int form, int which)
+{
+    per_block(c, form, [&](const int *l, int n) { fx_launch_essprk_save(c->D, l, n, which, c->stream); });
+}
+
+/* prj_timeint_eSSPRK10_4_advance (src/prj_timeint.c:2671-2729): Ketcheson's
+ * eSSPRK(10,4) in its low-storage form with the reference's blend weights */
+void essprk_seq(fx_ctx *c, int form)
+{
+    fx_launch_stage_dt(c->D, 6.0, c->stream);
+    essprk_save(c, form, 1);
+    for (int n = 0; n < 5; ++n) essprk_substep(c, form);
+    essprk_save(c, form, 2);
+    essprk_blend(c, form, 1, 3.0 / 5.0);
+    for (int n = 0; n < 5; ++n) essprk_substep(c, form);
+    essprk_blend(c, form, 2, 3.0 / 8.0);
+    essprk_blend(c, form, 1, 1.0 / 25.0);
+    c->last_slot = 0;
+}
+
+/* prj_timeint_step: the two RK2 stages or the eSSPRK10_4 advance */
+void step_seq(fx_ctx *c, int form)
+{
+    if (c->cfg.integrator == FX_INT_ESSPRK10_4) {
+        essprk_seq(c, form);
+    } else {
+        stage_seq(c, form, 1);
+        stage_seq(c, form, 2);
+    }
+}
+
 int build_step_graph(fx_ctx *c)
 {
     if (c->g_step) {
@@ -325,8 +399,7 @@ int build_step_graph(fx_ctx *c)
     cudaGraph_t g;
     FX_CUDA(c, cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
     fx_launch_reset_reductions(c->D, 2, c->stream);
-    stage_seq(c, FX_FORM_BATCHED, 1);
-    stage_seq(c, FX_FORM_BATCHED, 2);
+    step_seq(c, FX_FORM_BATCHED);
     FX_CUDA(c, cudaStreamEndCapture(c->stream, &g));
     cudaError_t e = cudaGraphInstantiate(&c->g_step, g, 0);
     cudaGraphDestroy(g);
@@ -344,8 +417,7 @@ int build_run_graph(fx_ctx *c, double cfl)
     fx_launch_reset_reductions(c->D, 1, c->stream);
     fx_launch_calc_dt(c->D, c->d_active, c->nactive, 0, cfl, c->stream);
     fx_launch_step_begin(c->D, c->stream);
-    stage_seq(c, FX_FORM_BATCHED, 1);
-    stage_seq(c, FX_FORM_BATCHED, 2);
+    step_seq(c, FX_FORM_BATCHED);
     fx_launch_step_end(c->D, c->stream);
     FX_CUDA(c, cudaStreamEndCapture(c->stream, &g));
     cudaError_t e = cudaGraphInstantiate(&c->g_run, g, 0);
@@ -365,6 +437,86 @@ int read_dt_src(fx_ctx *c, double *dt_src)
 }
 
 size_t w_count(const fx_ctx *c) { return (size_t)FX_W_COUNT(c->nv); }
+
+/* stage slots of the host's block arrays: 2 (RK2), 3 (eSSPRK10_4).  The
+ * device keeps slots 0-1 in the stacked W / Bf arrays and slot 2 in W2 /
+ * Bf2. */
+int host_ns(const fx_ctx *c) { return c->cfg.integrator == FX_INT_ESSPRK10_4 ? 3 : 2; }
+
+/* factor of prj_timeint_calc_dt on the CFL minimum (src/prj_timeint.c:2246-2253) */
+double dt_mult(const fx_ctx *c) { return c->cfg.integrator == FX_INT_ESSPRK10_4 ? 6.0 : 1.0; }
+
+/* W of blocks [b0, b0 + nb) between host (host_ns slots per variable) and
+ * device; state_only: slot 0 only */
+int xfer_w(fx_ctx *c, int b0, int nb, double *host, cudaMemcpyKind kind, bool state_only)
+{
+    const int ns = host_ns(c);
+    const size_t rows = (size_t)nb * c->nv;
+    const size_t cell = sizeof(double) * FX_NCELLS;
+    double *dev = c->d_W + (size_t)b0 * w_count(c);
+    const int nslot = state_only ? 1 : 2;
+    if (kind == cudaMemcpyHostToDevice) {
+        FX_CUDA(c, cudaMemcpy2DAsync(dev, 2 * cell, host, ns * cell, nslot * cell, rows, kind, c->stream));
+    } else {
+        FX_CUDA(c, cudaMemcpy2DAsync(host, ns * cell, dev, 2 * cell, nslot * cell, rows, kind, c->stream));
+    }
+    if (ns == 3 && !state_only) {
+        double *d2 = c->d_W2 + (size_t)b0 * c->nv * FX_NCELLS;
+        if (kind == cudaMemcpyHostToDevice) {
+            FX_CUDA(c, cudaMemcpy2DAsync(d2, cell, host + 2 * FX_NCELLS, 3 * cell, cell, rows, kind, c->stream));
+        } else {
+            FX_CUDA(c, cudaMemcpy2DAsync(host + 2 * FX_NCELLS, 3 * cell, d2, cell, cell, rows, kind, c->stream));
+        }
+    }
+    return FX_SUCCESS;
+}
+
+/* Bf of blocks [b0, b0 + nb), rows (block, direction) */
+int xfer_bf(fx_ctx *c, int b0, int nb, double *host, cudaMemcpyKind kind, bool state_only)
+{
+    const int ns = host_ns(c);
+    const size_t rows = (size_t)nb * 3;
+    const size_t face = sizeof(double) * FX_NFACES;
+    double *dev = c->d_Bf + (size_t)b0 * FX_BF_COUNT;
+    const int nslot = state_only ? 1 : 2;
+    if (kind == cudaMemcpyHostToDevice) {
+        FX_CUDA(c, cudaMemcpy2DAsync(dev, 2 * face, host, ns * face, nslot * face, rows, kind, c->stream));
+    } else {
+        FX_CUDA(c, cudaMemcpy2DAsync(host, ns * face, dev, 2 * face, nslot * face, rows, kind, c->stream));
+    }
+    if (ns == 3 && !state_only) {
+        double *d2 = c->d_Bf2 + (size_t)b0 * 3 * FX_NFACES;
+        if (kind == cudaMemcpyHostToDevice) {
+            FX_CUDA(c, cudaMemcpy2DAsync(d2, face, host + 2 * FX_NFACES, 3 * face, face, rows, kind, c->stream));
+        } else {
+            FX_CUDA(c, cudaMemcpy2DAsync(host + 2 * FX_NFACES, 3 * face, d2, face, face, rows, kind, c->stream));
+        }
+    }
+    return FX_SUCCESS;
+}
+
+/* one direction of one block's Bf (block->Bf[d]: host_ns slots) */
+int xfer_bf_dir(fx_ctx *c, int b, int d, double *host, cudaMemcpyKind kind)
+{
+    const int ns = host_ns(c);
+    double *dev = c->d_Bf + (size_t)b * FX_BF_COUNT + (size_t)d * FX_NSTAGES * FX_NFACES;
+    const size_t n2 = (size_t)2 * FX_NFACES * sizeof(double);
+    if (kind == cudaMemcpyHostToDevice) {
+        FX_CUDA(c, cudaMemcpyAsync(dev, host, n2, kind, c->stream));
+    } else {
+        FX_CUDA(c, cudaMemcpyAsync(host, dev, n2, kind, c->stream));
+    }
+    if (ns == 3) {
+        double *d2 = c->d_Bf2 + ((size_t)b * 3 + d) * FX_NFACES;
+        const size_t n1 = (size_t)FX_NFACES * sizeof(double);
+        if (kind == cudaMemcpyHostToDevice) {
+            FX_CUDA(c, cudaMemcpyAsync(d2, host + 2 * FX_NFACES, n1, kind, c->stream));
+        } else {
+            FX_CUDA(c, cudaMemcpyAsync(host + 2 * FX_NFACES, d2, n1, kind, c->stream));
+        }
+    }
+    return FX_SUCCESS;
+}
 
 /* (Re)allocates the per-block arrays for `cap` blocks.  The first `keep`
  * blocks of every array move over from the old allocation; the rest starts
@@ -413,6 +565,10 @@ int alloc_block_arrays(fx_ctx *c, int cap, int keep)
     }
     if (c->cfg.gravity) {
         if ((rc = regrow(c, &c->d_grav, (size_t)FX_GRAV_COUNT, cap, keep))) return rc;
+    }
+    if (c->cfg.integrator == FX_INT_ESSPRK10_4) {
+        if ((rc = regrow(c, &c->d_W2, (size_t)c->nv * FX_NCELLS, cap, keep))) return rc;
+        if (c->cfg.mhd && (rc = regrow(c, &c->d_Bf2, (size_t)3 * FX_NFACES, cap, keep))) return rc;
     }
     if ((rc = regrow(c, &c->d_ids, 1, cap, 0))) return rc;
     c->cap = cap;
@@ -486,6 +642,8 @@ int install_tables(fx_ctx *c)
     c->D.eos = c->d_eos;
     c->D.rhs = c->d_rhs;
     c->D.grav = c->d_grav;
+    c->D.W2 = c->d_W2;
+    c->D.Bf2 = c->d_Bf2;
     return FX_SUCCESS;
 }
 
@@ -654,6 +812,10 @@ int fx_create(int device, const fx_config *cfg, fx_ctx **out)
     if (!(cfg->gamma > 0.0)) {
         return FX_EINVAL;
     }
+    if ((cfg->recon != FX_RECON_MC && cfg->recon != FX_RECON_WENO3) ||
+        (cfg->integrator != FX_INT_RK2 && cfg->integrator != FX_INT_ESSPRK10_4)) {
+        return FX_EINVAL;
+    }
     fx_ctx *c = new fx_ctx();
     c->device = device;
     c->cfg = *cfg;
@@ -682,6 +844,17 @@ int fx_create(int device, const fx_config *cfg, fx_ctx **out)
     c->D.err = c->d_err;
     c->D.red = c->d_red;
     c->D.ctl = c->d_ctl;
+    c->D.recon = cfg->recon;
+    {
+        FxCtl v{};
+        v.dt_mult = dt_mult(c);
+        *c->h_ctl = v;
+        fx_launch_set_ctl(c->D, v, c->stream);
+        if (cudaStreamSynchronize(c->stream) != cudaSuccess) {
+            fx_destroy(c);
+            return FX_ECUDA;
+        }
+    }
     *out = c;
     return FX_SUCCESS;
 }
@@ -819,16 +992,11 @@ int fx_upload_block(fx_ctx *c, int b, const double *W, const double *const Bf[3]
 {
     if (!has_mesh(c)) return c ? set_err(c, FX_ENOMESH, "no mesh") : FX_EINVAL;
     if (b < 0 || b >= c->nblocks) return set_err(c, FX_EINVAL, "block %d out of range", b);
-    if (W) {
-        FX_CUDA(c, cudaMemcpyAsync(c->d_W + (size_t)b * w_count(c), W, w_count(c) * sizeof(double),
-            cudaMemcpyHostToDevice, c->stream));
-    }
+    int rc;
+    if (W && (rc = xfer_w(c, b, 1, const_cast<double *>(W), cudaMemcpyHostToDevice, false))) return rc;
     if (Bf && c->cfg.mhd) {
         for (int d = 0; d < 3; ++d) {
-            if (Bf[d]) {
-                FX_CUDA(c, cudaMemcpyAsync(c->d_Bf + (size_t)b * FX_BF_COUNT + (size_t)d * FX_NSTAGES * FX_NFACES,
-                    Bf[d], (size_t)FX_NSTAGES * FX_NFACES * sizeof(double), cudaMemcpyHostToDevice, c->stream));
-            }
+            if (Bf[d] && (rc = xfer_bf_dir(c, b, d, const_cast<double *>(Bf[d]), cudaMemcpyHostToDevice))) return rc;
         }
     }
     if (grav && c->d_grav) {
@@ -847,10 +1015,8 @@ int fx_download_block(fx_ctx *c, int b, double *W, double *eosvar, double *const
 {
     if (!has_mesh(c)) return c ? set_err(c, FX_ENOMESH, "no mesh") : FX_EINVAL;
     if (b < 0 || b >= c->nblocks) return set_err(c, FX_EINVAL, "block %d out of range", b);
-    if (W) {
-        FX_CUDA(c, cudaMemcpyAsync(W, c->d_W + (size_t)b * w_count(c), w_count(c) * sizeof(double),
-            cudaMemcpyDeviceToHost, c->stream));
-    }
+    int rc;
+    if (W && (rc = xfer_w(c, b, 1, W, cudaMemcpyDeviceToHost, false))) return rc;
     if (eosvar) {
         fx_launch_eos_fill(c->D, c->d_ids + b, 1, c->last_slot, 0, c->stream);
         FX_CUDA(c, cudaMemcpyAsync(eosvar, c->d_eos + (size_t)b * FX_EOS_COUNT, FX_EOS_COUNT * sizeof(double),
@@ -858,10 +1024,7 @@ int fx_download_block(fx_ctx *c, int b, double *W, double *eosvar, double *const
     }
     if (Bf && c->cfg.mhd) {
         for (int d = 0; d < 3; ++d) {
-            if (Bf[d]) {
-                FX_CUDA(c, cudaMemcpyAsync(Bf[d], c->d_Bf + (size_t)b * FX_BF_COUNT + (size_t)d * FX_NSTAGES * FX_NFACES,
-                    (size_t)FX_NSTAGES * FX_NFACES * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
-            }
+            if (Bf[d] && (rc = xfer_bf_dir(c, b, d, Bf[d], cudaMemcpyDeviceToHost))) return rc;
         }
     }
     return sync_and_check(c);
@@ -870,60 +1033,38 @@ int fx_download_block(fx_ctx *c, int b, double *W, double *eosvar, double *const
 int fx_upload_all(fx_ctx *c, const double *W_all, const double *Bf_all)
 {
     if (!has_mesh(c)) return c ? set_err(c, FX_ENOMESH, "no mesh") : FX_EINVAL;
-    const size_t nb = (size_t)c->nblocks;
-    if (W_all) {
-        FX_CUDA(c, cudaMemcpyAsync(c->d_W, W_all, nb * w_count(c) * sizeof(double), cudaMemcpyHostToDevice,
-            c->stream));
-    }
-    if (Bf_all && c->cfg.mhd) {
-        FX_CUDA(c, cudaMemcpyAsync(c->d_Bf, Bf_all, nb * FX_BF_COUNT * sizeof(double), cudaMemcpyHostToDevice,
-            c->stream));
-    }
+    int rc;
+    if (W_all && (rc = xfer_w(c, 0, c->nblocks, const_cast<double *>(W_all), cudaMemcpyHostToDevice, false))) return rc;
+    if (Bf_all && c->cfg.mhd &&
+        (rc = xfer_bf(c, 0, c->nblocks, const_cast<double *>(Bf_all), cudaMemcpyHostToDevice, false))) return rc;
     return FX_SUCCESS;
 }
 
 int fx_download_all(fx_ctx *c, double *W_all, double *Bf_all)
 {
     if (!has_mesh(c)) return c ? set_err(c, FX_ENOMESH, "no mesh") : FX_EINVAL;
-    const size_t nb = (size_t)c->nblocks;
-    if (W_all) {
-        FX_CUDA(c, cudaMemcpyAsync(W_all, c->d_W, nb * w_count(c) * sizeof(double), cudaMemcpyDeviceToHost,
-            c->stream));
-    }
-    if (Bf_all && c->cfg.mhd) {
-        FX_CUDA(c, cudaMemcpyAsync(Bf_all, c->d_Bf, nb * FX_BF_COUNT * sizeof(double), cudaMemcpyDeviceToHost,
-            c->stream));
-    }
+    int rc;
+    if (W_all && (rc = xfer_w(c, 0, c->nblocks, W_all, cudaMemcpyDeviceToHost, false))) return rc;
+    if (Bf_all && c->cfg.mhd && (rc = xfer_bf(c, 0, c->nblocks, Bf_all, cudaMemcpyDeviceToHost, false))) return rc;
     return sync_and_check(c);
-}
-
-/* slot-0 rows: W is [b][v][slot][cell], Bf is [b][d][slot][face] */
-static int copy_state(fx_ctx *c, double *dW, const double *sW, double *dB, const double *sB,
-    cudaMemcpyKind kind)
-{
-    const size_t nb = (size_t)c->nblocks;
-    if (dW && sW) {
-        FX_CUDA(c, cudaMemcpy2DAsync(dW, 2 * FX_NCELLS * sizeof(double), sW, 2 * FX_NCELLS * sizeof(double),
-            FX_NCELLS * sizeof(double), nb * (size_t)c->nv, kind, c->stream));
-    }
-    if (dB && sB && c->cfg.mhd) {
-        FX_CUDA(c, cudaMemcpy2DAsync(dB, 2 * FX_NFACES * sizeof(double), sB, 2 * FX_NFACES * sizeof(double),
-            FX_NFACES * sizeof(double), nb * 3, kind, c->stream));
-    }
-    return FX_SUCCESS;
 }
 
 int fx_upload_state(fx_ctx *c, const double *W_all, const double *Bf_all)
 {
     if (!has_mesh(c)) return c ? set_err(c, FX_ENOMESH, "no mesh") : FX_EINVAL;
-    return copy_state(c, c->d_W, W_all, c->d_Bf, Bf_all, cudaMemcpyHostToDevice);
+    int rc;
+    if (W_all && (rc = xfer_w(c, 0, c->nblocks, const_cast<double *>(W_all), cudaMemcpyHostToDevice, true))) return rc;
+    if (Bf_all && c->cfg.mhd &&
+        (rc = xfer_bf(c, 0, c->nblocks, const_cast<double *>(Bf_all), cudaMemcpyHostToDevice, true))) return rc;
+    return FX_SUCCESS;
 }
 
 int fx_download_state(fx_ctx *c, double *W_all, double *Bf_all)
 {
     if (!has_mesh(c)) return c ? set_err(c, FX_ENOMESH, "no mesh") : FX_EINVAL;
-    int rc = copy_state(c, W_all, c->d_W, Bf_all, c->d_Bf, cudaMemcpyDeviceToHost);
-    if (rc) return rc;
+    int rc;
+    if (W_all && (rc = xfer_w(c, 0, c->nblocks, W_all, cudaMemcpyDeviceToHost, true))) return rc;
+    if (Bf_all && c->cfg.mhd && (rc = xfer_bf(c, 0, c->nblocks, Bf_all, cudaMemcpyDeviceToHost, true))) return rc;
     return FX_SUCCESS;
 }
 
@@ -937,7 +1078,10 @@ int fx_download_array(fx_ctx *c, int b, int which, int dir, double *out)
     size_t count = 0;
     const size_t nv = (size_t)c->nv;
     switch (which) {
-    case FX_ARR_W: src = c->d_W + (size_t)b * w_count(c); count = w_count(c); break;
+    case FX_ARR_W: {
+        int rc = xfer_w(c, b, 1, out, cudaMemcpyDeviceToHost, false);
+        return rc ? rc : sync_and_check(c);
+    }
     case FX_ARR_EOSVAR: src = c->d_eos + (size_t)b * FX_EOS_COUNT; count = FX_EOS_COUNT; break;
     case FX_ARR_RHS: src = c->d_rhs + (size_t)b * FX_RHS_COUNT(nv); count = FX_RHS_COUNT(nv); break;
     case FX_ARR_FLUX: src = c->d_flux + (size_t)b * FX_FLUX_COUNT(nv) + (size_t)dir * nv * FX_NCELLS;
@@ -953,8 +1097,8 @@ int fx_download_array(fx_ctx *c, int b, int which, int dir, double *out)
     case FX_ARR_EMF:
         if (!c->cfg.mhd) return set_err(c, FX_EINVAL, "field arrays exist only in MHD runs");
         if (which == FX_ARR_BF) {
-            src = c->d_Bf + (size_t)b * FX_BF_COUNT + (size_t)dir * FX_NSTAGES * FX_NFACES;
-            count = (size_t)FX_NSTAGES * FX_NFACES;
+            int rc = xfer_bf_dir(c, b, dir, out, cudaMemcpyDeviceToHost);
+            return rc ? rc : sync_and_check(c);
         } else if (which == FX_ARR_EMF) {
             src = c->d_emf + (size_t)b * FX_EMF_COUNT + (size_t)dir * FX_NEDGES;
             count = FX_NEDGES;
@@ -1088,13 +1232,14 @@ int fx_calc_dt(fx_ctx *c, double cfl, double *dt)
         c->stream));
     int rc = sync_and_check(c);
     if (rc) return rc;
-    *dt = fx_key_to_double(c->h_red[0]);
+    *dt = fx_key_to_double(c->h_red[0]) * dt_mult(c);
     return FX_SUCCESS;
 }
 
 int fx_stage(fx_ctx *c, int form, int stage, double dt, double *dt_src)
 {
     if (!has_mesh(c)) return c ? set_err(c, FX_ENOMESH, "no mesh") : FX_EINVAL;
+    if (c->cfg.integrator != FX_INT_RK2) return set_err(c, FX_EINVAL, "fx_stage: RK2 stages only");
     if ((form != FX_FORM_PLAIN && form != FX_FORM_BATCHED) || (stage != 1 && stage != 2)) {
         return set_err(c, FX_EINVAL, "fx_stage: bad form or stage");
     }
@@ -1115,8 +1260,7 @@ int fx_step(fx_ctx *c, int form, double dt, double *dt_src)
     fx_launch_set_dt(c->D, dt, c->stream);
     if (form == FX_FORM_PLAIN) {
         fx_launch_reset_reductions(c->D, 2, c->stream);
-        stage_seq(c, form, 1);
-        stage_seq(c, form, 2);
+        step_seq(c, form);
     } else {
         int rc = build_step_graph(c);
         if (rc) return rc;
@@ -1170,6 +1314,7 @@ int fx_run(fx_ctx *c, int form, int nsteps, double cfl, double dt_factor, double
     v.dt_factor = dt_factor;
     v.t_end = t_end;
     v.dt_src = 1.0e100;
+    v.dt_mult = dt_mult(c);
     *c->h_ctl = v;
     fx_launch_set_ctl(c->D, v, c->stream);
     int rc = build_run_graph(c, cfl);
@@ -1344,6 +1489,8 @@ int fx_amr_adapt(fx_ctx *c, int *changed)
         c->D.eos = c->d_eos;
         c->D.rhs = c->d_rhs;
         c->D.grav = c->d_grav;
+        c->D.W2 = c->d_W2;
+        c->D.Bf2 = c->d_Bf2;
     }
     /* geometry of the new block list, read by the data kernels */
     std::vector<FxBlockDev> hb(nb);
@@ -1534,9 +1681,16 @@ int fx_info(fx_ctx *c, int what, long long *value)
     const long long corr = (long long)std::max<size_t>(c->plan.flux_corr_begin.size(), 1) - 1 +
         (c->cfg.mhd ? (long long)std::max<size_t>(c->plan.emf_corr_begin.size(), 1) - 1 : 0);
     const long long mhd = c->cfg.mhd ? 1 : 0;
+    const bool ess = c->cfg.integrator == FX_INT_ESSPRK10_4;
     switch (what) {
-    case 0: /* reset + 2 x (flux + emf + ct + cells + ghost waves) */
-        *value = 1 + 2 * (1 + 2 * mhd + 1 + corr + gw);
+    case 0:
+        if (ess) {
+            /* reset + stage dt + 2 saves + 10 x (flux + emf + ct + cells +
+             * ghost waves) + 3 x (blend + ghost waves) */
+            *value = 2 + 2 + 10 * (1 + 2 * mhd + 1 + corr + gw) + 3 * (1 + mhd + gw);
+        } else { /* reset + 2 x (flux + emf + ct + cells + ghost waves) */
+            *value = 1 + 2 * (1 + 2 * mhd + 1 + corr + gw);
+        }
         break;
     case 1: /* set_dt + reset + 2 x (per-block phases + eos fills) + ghost waves */
         *value = 2 + 2 * ((long long)c->nactive * (1 + 2 * mhd + 1 + 2) + corr + gw);
@@ -1563,6 +1717,9 @@ int adj_supported(fx_ctx *c)
 {
     if (!c->cfg.mhd || c->cfg.gravity || c->cfg.mhd_eta != 0.0) {
         return set_err(c, FX_EINVAL, "the adjoint covers MHD runs without gravity or resistivity");
+    }
+    if (c->cfg.integrator != FX_INT_RK2 || c->cfg.recon != FX_RECON_MC) {
+        return set_err(c, FX_EINVAL, "the adjoint covers the RK2 / MC build");
     }
     const FxProgram &g = c->plan.ghost;
     bool ok = g.p_ops.empty() && c->plan.flux_corr.empty() && c->plan.emf_corr.empty();

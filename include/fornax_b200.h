@@ -13,8 +13,11 @@
  * Build variants of the reference map onto run-time settings:
  *   PRJ_MHD=1 -> fx_config.mhd = 1 (NHYDRO = 9, HLLD, constrained transport)
  *   PRJ_MHD=0 -> fx_config.mhd = 0 (NHYDRO = 6, HLLC)
- * Fixed: PRJ_BLOCK_SIZE = 16, PRJ_NGHOST = 2, RECON = MC, TIME_INTEGRATION =
- * RK2, ideal-gas EOS with a run-time adiabatic index, no radiation, no GR.
+ *   PRJ_RECON_HYDRO -> fx_config.recon (MC or WENO-Z3)
+ *   TIME_INTEGRATION -> fx_config.integrator (RK2 or eSSPRK10_4)
+ * Fixed: PRJ_BLOCK_SIZE = 16, PRJ_NGHOST = 2, ideal-gas EOS with a run-time
+ * adiabatic index, no radiation, no GR.  The number of stage slots of the
+ * block W and Bf arrays (NS below) is 2 for RK2 and 3 for eSSPRK10_4.
  *
  * Every entry point returns 0 on success and a positive FX_E* code on
  * failure; fx_last_error() returns the message.  Device-side physics
@@ -101,6 +104,15 @@ typedef struct fx_block_desc {
     int32_t can_refine; /* prj_block.can_refine: 0 keeps the block from refining */
 } fx_block_desc;
 
+/* reconstruction (PRJ_RECON_HYDRO, src/prj_defs.h:299-301) */
+#define FX_RECON_MC 0      /* PRJ_RECON_MC: monotonised-central slopes */
+#define FX_RECON_WENO3 1   /* PRJ_RECON_WENO3: WENO-Z3 face values (src/prj_reconstruct.h:383-423) */
+/* time integration (TIME_INTEGRATION, src/prj_defs.h:135-150) */
+#define FX_INT_RK2 0           /* RK2: two stages, block arrays with 2 stage slots */
+#define FX_INT_ESSPRK10_4 1    /* eSSPRK10_4 (the reference's default): ten forward-Euler
+                                * substeps of dt / 6 with three stored states; block W and
+                                * Bf arrays carry 3 stage slots (PRJ_BLOCK_NSTAGES = 3) */
+
 /* Run-time configuration (compile-time switches of the reference). */
 typedef struct fx_config {
     int32_t mhd;        /* 1: PRJ_MHD=1 build, 0: hydro build */
@@ -109,6 +121,8 @@ typedef struct fx_config {
     double coord[6];    /* domain: x1min, x1max, x2min, x2max, x3min, x3max (prj_coord) */
     int32_t bc[6];      /* x1 inner, x1 outer, x2 inner, x2 outer, x3 inner, x3 outer */
     double mhd_eta;     /* prj_mesh.mhd_eta */
+    int32_t recon;      /* FX_RECON_MC or FX_RECON_WENO3 */
+    int32_t integrator; /* FX_INT_RK2 or FX_INT_ESSPRK10_4 */
 } fx_config;
 
 /* ---- context -------------------------------------------------------------- */
@@ -144,16 +158,16 @@ int fx_plan_export(const fx_config *cfg, int nblocks, const fx_block_desc *block
     int32_t *ops, int *nops, int32_t *wave_begin, int *nwaves);
 
 /* Host <-> device copies of one block, in the reference's per-block layout:
- * W = block->W_mhd (NHYDRO * 2 * 8000 doubles), Bf[d] = block->Bf[d]
- * (2 * 8400 doubles each, may be NULL for hydro), grav[d] = block->grav[d]
- * (8000 doubles each, may be NULL). */
+ * W = block->W_mhd (NHYDRO * NS * 8000 doubles), Bf[d] = block->Bf[d]
+ * (NS * 8400 doubles each, may be NULL for hydro), grav[d] = block->grav[d]
+ * (8000 doubles each, may be NULL); NS = 2 (RK2) or 3 (eSSPRK10_4). */
 int fx_upload_block(fx_ctx *ctx, int block, const double *W, const double *const Bf[3],
     const double *const grav[3]);
 /* eosvar (3 * 8000, may be NULL) is recomputed from W of the last stage,
  * exactly what prj_eos_fill_active_cells + prj_eos_fill_mesh leave there. */
 int fx_download_block(fx_ctx *ctx, int block, double *W, double *eosvar, double *const Bf[3]);
 /* Whole-mesh copies: W_all is nblocks consecutive W arrays, Bf_all nblocks
- * consecutive 3 * 2 * 8400 arrays (d-major); either may be NULL. */
+ * consecutive 3 * NS * 8400 arrays (d-major); either may be NULL. */
 int fx_upload_all(fx_ctx *ctx, const double *W_all, const double *Bf_all);
 int fx_download_all(fx_ctx *ctx, double *W_all, double *Bf_all);
 /* Same host layout as fx_upload_all / fx_download_all, but only stage slot 0
@@ -191,13 +205,16 @@ int fx_boundary_fill_ghosts_and_bf(fx_ctx *ctx, int stage, int use_bf1);
 
 /* ---- time integration ------------------------------------------------------- */
 
-/* prj_timeint_calc_dt (src/prj_timeint.h:15-16): min over active cells. */
+/* prj_timeint_calc_dt (src/prj_timeint.h:15-16): min over active cells
+ * (times 6 for eSSPRK10_4, src/prj_timeint.c:2250-2251). */
 int fx_calc_dt(fx_ctx *ctx, double cfl, double *dt);
-/* prj_timeint_stage1 / prj_timeint_stage2 (src/prj_timeint.h:17-20). */
+/* prj_timeint_stage1 / prj_timeint_stage2 (src/prj_timeint.h:17-20); RK2 only. */
 int fx_stage(fx_ctx *ctx, int form, int stage, double dt, double *dt_src);
-/* prj_timeint_step (src/prj_timeint.h:31-33): one RK2 step.  *dt_src (may be
- * NULL) receives the minimum source time step.  FX_FORM_BATCHED replays a
- * captured CUDA graph; it does not synchronise unless dt_src != NULL. */
+/* prj_timeint_step (src/prj_timeint.h:31-33): one RK2 step, or one
+ * eSSPRK10_4 step (prj_timeint_eSSPRK10_4_advance, src/prj_timeint.c:2671-2729).
+ * *dt_src (may be NULL) receives the minimum source time step.
+ * FX_FORM_BATCHED replays a captured CUDA graph; it does not synchronise
+ * unless dt_src != NULL. */
 int fx_step(fx_ctx *ctx, int form, double dt, double *dt_src);
 /* The driver loop of src/main.c:485-562 without I/O: calc_dt, dt growth
  * limit dt_factor, clip to t_end, step, dt_src clamp; device resident.

@@ -1136,3 +1136,28 @@ void fxo_amr_vote(int nv, double gamma, const double *W, const double *grav, con
     out[1] = derefine ? -1 : 0;
     out[2] = (int)mask;
 }
+
+/* ---- WENO-Z3 face value (src/prj_reconstruct.h:383-423) ----------------- */
+double fxo_weno3_face(double qm, double q0, double qp, double target)
+{
+    const double eps = 1.0e-40;
+    double p0 = q0 + target * (q0 - qm);
+    double p1 = q0 + target * (qp - q0);
+    double dl = q0 - qm;
+    double dr = qp - q0;
+    double beta0 = dl * dl;
+    double beta1 = dr * dr;
+    double tau3 = beta0 - beta1;
+    double g0, g1, a0, a1;
+    if (tau3 < 0.0) tau3 = -tau3;
+    if (target > 0.0) {
+        g0 = 1.0 / 3.0;
+        g1 = 2.0 / 3.0;
+    } else {
+        g0 = 2.0 / 3.0;
+        g1 = 1.0 / 3.0;
+    }
+    a0 = g0 * (1.0 + tau3 / (eps + beta0));
+    a1 = g1 * (1.0 + tau3 / (eps + beta1));
+    return (a0 * p0 + a1 * p1) / (a0 + a1);
+}

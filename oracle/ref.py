@@ -119,19 +119,21 @@ def amr_params(max_level: int, criteria, min_dx: float = 0.0, reach_density: flo
     return a
 
 
-def lib_path(mhd: bool) -> str:
-    return os.path.join(REF_DIR, "libprjref_mhd.so" if mhd else "libprjref_hydro.so")
+def lib_path(mhd: bool, variant: str = "") -> str:
+    """variant: "" (RK2, MC), "weno3", "ess" (eSSPRK10_4), "ess_weno3"."""
+    name = ("mhd" if mhd else "hydro") + ("_" + variant if variant else "")
+    return os.path.join(REF_DIR, f"libprjref_{name}.so")
 
 
-def available(mhd: bool = True) -> bool:
-    return os.path.exists(lib_path(mhd))
+def available(mhd: bool = True, variant: str = "") -> bool:
+    return os.path.exists(lib_path(mhd, variant))
 
 
 class Reference:
     """One loaded copy of the reference core (one build variant)."""
 
-    def __init__(self, mhd: bool = True):
-        path = lib_path(mhd)
+    def __init__(self, mhd: bool = True, variant: str = ""):
+        path = lib_path(mhd, variant)
         if not os.path.exists(path):
             raise FileNotFoundError(f"oracle library missing: {path} (run make -C oracle)")
         self.mhd = mhd
@@ -168,12 +170,15 @@ class Reference:
         L.rh_run_amr.restype = C.c_int
         L.rh_block_tree.argtypes = [C.c_int, ip]
         L.rh_E_injected.restype = C.c_double
+        L.rh_weno3_face.argtypes = [C.c_double] * 4
+        L.rh_weno3_face.restype = C.c_double
         L.rh_sim_dt.restype = C.c_double
         if mhd:
             L.rh_hlld.argtypes = [dp, dp] + [C.c_double] * 5 + [dp]
             L.rh_emf_upwind.argtypes = [dp, dp, dp]
             L.rh_emf_upwind.restype = C.c_double
         self.nhydro = L.rh_nhydro()
+        self.nstages = L.rh_nstages()
 
     # -- set-up and stepping ------------------------------------------------
     def setup(self, params: RhParams) -> None:
@@ -262,7 +267,7 @@ class Reference:
         dst[:] = data.ravel()
 
     def W(self, b: int) -> np.ndarray:
-        return self._arr(b, ARR_W, 0, self.nhydro * NSTAGES * NCELLS)
+        return self._arr(b, ARR_W, 0, self.nhydro * self.nstages * NCELLS)
 
     def set_W(self, b: int, data: np.ndarray) -> None:
         self._set(b, ARR_W, 0, data)
@@ -283,7 +288,7 @@ class Reference:
         return self._arr(b, ARR_RHS, 0, self.nhydro * NCELLS)
 
     def Bf(self, b: int, d: int) -> np.ndarray:
-        return self._arr(b, ARR_BF, d, NSTAGES * NFACES)
+        return self._arr(b, ARR_BF, d, self.nstages * NFACES)
 
     def set_Bf(self, b: int, d: int, data: np.ndarray) -> None:
         self._set(b, ARR_BF, d, data)
@@ -330,6 +335,9 @@ class Reference:
     # -- single kernels -------------------------------------------------------
     def mc_slope(self, qm, q0, qp) -> float:
         return self.lib.rh_mc_slope(qm, q0, qp)
+
+    def weno3_face(self, qm, q0, qp, target) -> float:
+        return self.lib.rh_weno3_face(qm, q0, qp, target)
 
     def hlld(self, WL, WR, pL, pR, gL, gR, bn) -> np.ndarray:
         wl = np.ascontiguousarray(WL, dtype=np.float64)

@@ -1164,3 +1164,9 @@ int rh_block_tree(int b, int *out)
 
 double rh_E_injected(void) { return g_sim.eos.E_injected; }
 int rh_max_blocks(void) { return g_sim.mesh.nblocks_max; }
+
+/* WENO-Z3 face value of the reference (src/prj_reconstruct.h:383-423) */
+double rh_weno3_face(double qm, double q0, double qp, double target)
+{
+    return prj_reconstruct_weno3_face(qm, q0, qp, target);
+}

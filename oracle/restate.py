@@ -37,6 +37,8 @@ class Restatement:
         L = self.lib = C.CDLL(PATH, mode=C.RTLD_LOCAL)
         L.fxo_mc_slope.argtypes = [C.c_double] * 3
         L.fxo_mc_slope.restype = C.c_double
+        L.fxo_weno3_face.argtypes = [C.c_double] * 4
+        L.fxo_weno3_face.restype = C.c_double
         L.fxo_hlld.argtypes = [_dp, _dp] + [C.c_double] * 5 + [_dp]
         L.fxo_hlld.restype = C.c_int
         L.fxo_hllc.argtypes = [_dp, _dp] + [C.c_double] * 7 + [_dp]
@@ -59,6 +61,9 @@ class Restatement:
 
     def mc_slope(self, qm, q0, qp):
         return self.lib.fxo_mc_slope(qm, q0, qp)
+
+    def weno3_face(self, qm, q0, qp, target):
+        return self.lib.fxo_weno3_face(qm, q0, qp, target)
 
     def hlld(self, WL, WR, pL, pR, gL, gR, bn):
         wl = np.ascontiguousarray(WL, np.float64).copy()

@@ -303,16 +303,17 @@ def ref_state(ref):
     """W [nb, nv, 2, 8000] and Bf [nb, 3, 2, 8400] of every block entry;
     entries without storage (freed by a coarsening) read as zeros."""
     nb = ref.nblocks()
-    W = np.zeros((nb, ref.nhydro, 2, NCELLS))
-    Bf = np.zeros((nb, 3, 2, NFACES)) if ref.mhd else None
+    ns = ref.nstages
+    W = np.zeros((nb, ref.nhydro, ns, NCELLS))
+    Bf = np.zeros((nb, 3, ns, NFACES)) if ref.mhd else None
     for b in range(nb):
         try:
-            W[b] = ref.W(b).reshape(ref.nhydro, 2, NCELLS)
+            W[b] = ref.W(b).reshape(ref.nhydro, ns, NCELLS)
         except ValueError:
             continue
         if ref.mhd:
             for d in range(3):
-                Bf[b, d] = ref.Bf(b, d).reshape(2, NFACES)
+                Bf[b, d] = ref.Bf(b, d).reshape(ns, NFACES)
     return W, Bf
 
 
