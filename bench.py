@@ -55,6 +55,8 @@ def parse():
                     help="steps between adapts of the dynamic-AMR key")
     ap.add_argument("--amr-dynamic-adapts", type=int, default=2,
                     help="adapts in the dynamic-AMR key (0: skip it)")
+    ap.add_argument("--no-variants", dest="variants", action="store_false",
+                    help="skip the WENO-Z3 / eSSPRK10_4 variant measurements")
     ap.add_argument("--ref-adapt", action="store_true",
                     help="also time the reference's adapt on the dynamic-AMR mesh (about a minute of CPU)")
     ap.add_argument("--amr-steps", type=int, default=10,
@@ -79,6 +81,27 @@ def _cpu_worker(args):
         r.time_steps(warm, dt)
     secs = r.time_steps(nsteps, dt)
     return nsteps * (root ** 3) * 4096, secs
+
+
+def _cpu_variant_worker(variant):
+    from oracle import ref as R
+    r = R.Reference(True, variant)
+    p = R.params_fourier(root=2)
+    r.setup(p)
+    dt = r.calc_dt()
+    r.time_steps(1, dt)
+    n = 2
+    secs = r.time_steps(n, dt)
+    return variant, n * 8 * 4096 / secs
+
+
+def cpu_variants():
+    """One core of the reference C core per build variant, on a 2^3-block
+    (32^3-zone) instance of the workload recipe, two timed steps each."""
+    ctx = mp.get_context("spawn")
+    with ctx.Pool(3) as pool:
+        res = pool.map(_cpu_variant_worker, ["weno3", "ess", "ess_weno3"])
+    return {v: {"value": x, "unit": UNIT, "cores": 1} for v, x in res}
 
 
 def _ref_adapt_worker(_):
@@ -358,6 +381,54 @@ def run_amr_dynamic(args, dev):
             "active_blocks_per_level_end": [levels.get(l, 0) for l in range(4)]}
 
 
+def run_variants(args, dev, cpu):
+    """The headline workload (128^3 Fourier MHD, 512 blocks) in the
+    reference's other build variants: WENO-Z3 reconstruction, the
+    eSSPRK10_4 integrator (ten substeps of dt / 6 per step, three stored
+    states) and both.  Batched form, device time per driver step (each step
+    advances by its own dt: eSSPRK's dt is 6x RK2's CFL step)."""
+    import numpy as np
+    import torch
+
+    import fornaxamr_b200 as fx
+    from fornaxamr_b200 import mesh, problems
+
+    coord = (0.0, 1.0, 0.0, 1.0, 0.0, 1.0)
+    blocks = mesh.uniform_mesh((ROOT, ROOT, ROOT), coord)
+    W0, Bf0 = problems.fourier_mhd(blocks)
+    out = {}
+    for name, recon, integ in (("weno3", fx.RECON_WENO3, fx.INT_RK2), ("ess", fx.RECON_MC, fx.INT_ESSPRK10_4),
+                               ("ess_weno3", fx.RECON_WENO3, fx.INT_ESSPRK10_4)):
+        ctx = fx.Context(True, 5.0 / 3.0, coord, device=dev, recon=recon, integrator=integ)
+        ctx.set_mesh(mesh.to_desc(blocks))
+        ns = ctx.ns
+        W = np.zeros((len(blocks), 9, ns, fx.NCELLS))
+        Bf = np.zeros((len(blocks), 3, ns, fx.NFACES))
+        W[:, :, 0] = W0[:, :, 0]
+        Bf[:, :, 0] = Bf0[:, :, 0]
+        ctx.upload_state(W, Bf)
+        ctx.boundary_fill(1, 0)
+        ctx.autotune()
+        stream = torch.cuda.ExternalStream(ctx.stream(), device=dev)
+        state = ctx.run(fx.FORM_BATCHED, max(args.warmup, 3), 0.4, 1.2, 1.0e30, (0.0, 0.0, 0))
+        ctx.sync()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        n = 4
+        e0.record(stream)
+        state = ctx.run(fx.FORM_BATCHED, n, 0.4, 1.2, 1.0e30, state)
+        e1.record(stream)
+        e1.synchronize()
+        ms = e0.elapsed_time(e1) / n
+        out[name] = {"ms_per_step": ms, "value": ZONES / (ms * 1e-3), "unit": UNIT,
+                     "dt": state[1], "launches_per_step": ctx.info(0),
+                     "flux_launch_ms": ctx.time_phase(fx.PHASE_FLUX, 5, state[1])}
+        if cpu and name in cpu:
+            out[name]["cpu_reference_1core"] = cpu[name]
+        ctx.close()
+    return out
+
+
 def run_adjoint(args, dev):
     """Cost of the discrete adjoint on the 64^3 workload (4^3 blocks of 16^3,
     seeded Fourier-mode MHD with amplitude 0.01, |k|_inf <= 3): device time
@@ -568,6 +639,12 @@ def main():
         except Exception as exc:  # oracle missing on this machine
             cb = {"value": None, "unit": UNIT, "cores": 0, "kind": "reference",
                   "sample": f"unavailable: {exc}"}
+    cv = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline and args.variants:
+        try:
+            cv = cpu_variants()
+        except Exception as exc:
+            cv = {"unavailable": str(exc)}
     ra = None
     if rank == 0 and world == 1 and args.ref_adapt:
         try:
@@ -584,6 +661,8 @@ def main():
     line["cpu_baseline"] = cb
     if world == 1:
         line["adjoint"] = run_adjoint(args, local_rank)
+    if world == 1 and args.variants:
+        line["variants"] = run_variants(args, local_rank, cv)
     if world == 1 and args.amr_steps > 0:
         line["amr_blast"] = run_amr(args, local_rank, "blast")
         if args.collapse:

@@ -230,6 +230,20 @@ class Context:
         f = None if Bf_all is None else _dp(Bf_all)
         self._check(self.L.fx_download_all(self._h, w, f))
 
+    def upload_state(self, W_all: Optional[np.ndarray], Bf_all: Optional[np.ndarray]) -> None:
+        """Stage slot 0 only (the layout of upload_all, ns slots per block)."""
+        Wc = None if W_all is None else np.ascontiguousarray(W_all, dtype=np.float64)
+        Bc = None if Bf_all is None else np.ascontiguousarray(Bf_all, dtype=np.float64)
+        self._check(self.L.fx_upload_state(self._h, None if Wc is None else _dp(Wc),
+                                           None if Bc is None else _dp(Bc)))
+        self.sync()  # the host arrays must outlive the copies
+
+    def download_state(self, W_all: Optional[np.ndarray], Bf_all: Optional[np.ndarray]) -> None:
+        w = None if W_all is None else _dp(W_all)
+        f = None if Bf_all is None else _dp(Bf_all)
+        self._check(self.L.fx_download_state(self._h, w, f))
+        self.sync()
+
     def download_array(self, b: int, which: int, dir_: int = 0) -> np.ndarray:
         sizes = {ARR_W: self.nv * self.ns * NCELLS, ARR_EOSVAR: 3 * NCELLS, ARR_RHS: self.nv * NCELLS,
                  ARR_FLUX: self.nv * NCELLS, ARR_VRIEMANN: 3 * NCELLS, ARR_GRAV: NCELLS,

@@ -3,7 +3,7 @@ cases the kernel profiles are taken on).
 
     python -m fornaxamr_b200.workload [--problem fourier|blast|collapse]
         [--root R] [--steps N] [--form batched|plain] [--adjoint N] [--shape S]
-        [--amr-interval K [--max-level L]]
+        [--amr-interval K [--max-level L]] [--variant rk2|weno3|ess|ess_weno3]
 
 fourier: uniform root^3 mesh of 16^3 blocks on [0,1]^3 with the seeded
 Fourier-mode MHD state (fornaxamr_b200.problems.fourier_mhd).
@@ -15,7 +15,9 @@ collapse: static AMR gravity collapse, root^3 roots on [-1, 1]^3, spheres
 Runs the driver's initial ghost fill and N driver steps (calc_dt + RK2 step)
 and prints the time per step.  With --amr-interval K the mesh adapts every K
 steps (prj_amr_adapt with a Loehner pressure criterion, refine 0.3 /
-derefine 0.1, up to level L, default 3) and the adapt phases are printed.  With --adjoint N (fourier only, amplitude
+derefine 0.1, up to level L, default 3) and the adapt phases are printed.
+--variant selects the reference build variant: WENO-Z3 reconstruction
+(weno3), the eSSPRK10_4 integrator (ess) or both (ess_weno3).  With --adjoint N (fourier only, amplitude
 0.01, |k| <= 3) it runs N fixed-dt steps storing every stage, then one
 reverse sweep, and prints the reverse sweep's device time per step.
 """
@@ -37,8 +39,11 @@ def main():
     ap.add_argument("--adjoint", type=int, default=0)
     ap.add_argument("--shape", type=int, default=-1, help="force a face-kernel launch shape (fx_set_flux_shape)")
     ap.add_argument("--amr-interval", type=int, default=0)
+    ap.add_argument("--variant", default="rk2", choices=["rk2", "weno3", "ess", "ess_weno3"])
     ap.add_argument("--max-level", type=int, default=3)
     args = ap.parse_args()
+    if args.variant != "rk2" and args.problem == "collapse":
+        ap.error("--variant applies to the fourier and blast problems")
 
     import fornaxamr_b200 as fx
     from fornaxamr_b200 import mesh, problems
@@ -69,9 +74,18 @@ def main():
             gamma = 4.0 / 3.0
             gravity = True
             W, Bf, grav = problems.collapse(blocks, recs, half_width=hw)
-    ctx = fx.Context(True, gamma, coord, gravity=gravity)
+    recon = fx.RECON_WENO3 if "weno3" in args.variant else fx.RECON_MC
+    integ = fx.INT_ESSPRK10_4 if args.variant.startswith("ess") else fx.INT_RK2
+    ctx = fx.Context(True, gamma, coord, gravity=gravity, recon=recon, integrator=integ)
     ctx.set_mesh(mesh.to_desc(blocks))
-    ctx.upload_all(np.ascontiguousarray(W), np.ascontiguousarray(Bf))
+    if ctx.ns == 2:
+        ctx.upload_all(np.ascontiguousarray(W), np.ascontiguousarray(Bf))
+    else:
+        W3 = np.zeros(W.shape[:2] + (3,) + W.shape[3:])
+        B3 = np.zeros(Bf.shape[:2] + (3,) + Bf.shape[3:])
+        W3[:, :, 0] = W[:, :, 0]
+        B3[:, :, 0] = Bf[:, :, 0]
+        ctx.upload_state(W3, B3)
     if grav is not None:
         for b in range(len(blocks)):
             if blocks[b].active == 1:
