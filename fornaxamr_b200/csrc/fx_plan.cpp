@@ -174,6 +174,59 @@ struct SeqOp {
 /* element ids: cells, cell fields and faces of all blocks in one space */
 using Elem = uint32_t;
 
+/* open-addressing map from a face element to the signature of the value
+ * a face-prolongation group stored there (linear probing, grows at half
+ * load; keys are element ids, never ~0) */
+template <typename V>
+class ElemMap {
+public:
+    V *find(uint64_t key)
+    {
+        if (keys_.empty()) return nullptr;
+        for (size_t i = slot(key);; i = (i + 1) & (keys_.size() - 1)) {
+            if (keys_[i] == key) return &vals_[i];
+            if (keys_[i] == kEmpty) return nullptr;
+        }
+    }
+    void put(uint64_t key, const V &v)
+    {
+        if (2 * (n_ + 1) > keys_.size()) grow();
+        for (size_t i = slot(key);; i = (i + 1) & (keys_.size() - 1)) {
+            if (keys_[i] == key) {
+                vals_[i] = v;
+                return;
+            }
+            if (keys_[i] == kEmpty) {
+                keys_[i] = key;
+                vals_[i] = v;
+                ++n_;
+                return;
+            }
+        }
+    }
+
+private:
+    static constexpr uint64_t kEmpty = ~0ULL;
+    size_t slot(uint64_t key) const { return (size_t)((key * 0x9E3779B97F4A7C15ULL) >> 20) & (keys_.size() - 1); }
+    void grow()
+    {
+        std::vector<uint64_t> ok;
+        std::vector<V> ov;
+        ok.swap(keys_);
+        ov.swap(vals_);
+        const size_t cap = ok.empty() ? 1024 : 2 * ok.size();
+        keys_.assign(cap, kEmpty);
+        vals_.resize(cap);
+        n_ = 0;
+        for (size_t i = 0; i < ok.size(); ++i) {
+            if (ok[i] != kEmpty) put(ok[i], ov[i]);
+        }
+    }
+    std::vector<uint64_t> keys_;
+    std::vector<V> vals_;
+    size_t n_ = 0;
+};
+
 /* what a prolonged outer face was computed from: a recomputation with the
  * same coarse face, target and stencil versions stores the same value */
 struct ProlongSig {
@@ -788,6 +841,22 @@ private:
             const int t0 = d == 0 ? 1 : 0;
             const int t1 = d == 2 ? 1 : 2;
             for (int side = 0; side < 2; ++side) {
+                /* the coarse face and its four tangential neighbours are the
+                 * stencil of all four outer faces of this side */
+                int y[3] = {c[0], c[1], c[2]};
+                y[d] += side;
+                const int64_t cf = face_elem(coarse, d, fidx(d, y[0], y[1], y[2]));
+                int64_t ze[5];
+                int zv[5];
+                bool stencil_read = false;
+                const int off[5][2] = {{0, 0}, {-1, 0}, {1, 0}, {0, -1}, {0, 1}};
+                for (int n = 0; n < 5; ++n) {
+                    int z[3] = {y[0], y[1], y[2]};
+                    z[t0] += off[n][0];
+                    z[t1] += off[n][1];
+                    ze[n] = face_elem(coarse, d, fidx(d, z[0], z[1], z[2]));
+                    zv[n] = ver_[ze[n]];
+                }
                 for (int a = 0; a < 2; ++a) {
                     for (int bb = 0; bb < 2; ++bb) {
                         const int q = 8 * d + 4 * side + 2 * a + bb;
@@ -802,24 +871,18 @@ private:
                             reads.push_back(xe);
                             continue;
                         }
-                        int y[3] = {c[0], c[1], c[2]};
-                        y[d] += side;
+                        if (!stencil_read) {
+                            for (int n = 0; n < 5; ++n) reads.push_back(ze[n]);
+                            stencil_read = true;
+                        }
                         ProlongSig sg;
                         sg.op = op_index;
-                        sg.coarse_face = face_elem(coarse, d, fidx(d, y[0], y[1], y[2]));
+                        sg.coarse_face = cf;
                         sg.target = 2 * a + bb;
-                        const int off[5][2] = {{0, 0}, {-1, 0}, {1, 0}, {0, -1}, {0, 1}};
-                        for (int n = 0; n < 5; ++n) {
-                            int z[3] = {y[0], y[1], y[2]};
-                            z[t0] += off[n][0];
-                            z[t1] += off[n][1];
-                            const int64_t ze = face_elem(coarse, d, fidx(d, z[0], z[1], z[2]));
-                            reads.push_back(ze);
-                            sg.ver[n] = ver_[ze];
-                        }
+                        for (int n = 0; n < 5; ++n) sg.ver[n] = zv[n];
                         fid(fine, d, xf) = FID_COARSER;
-                        const auto it = psig_.find(xe);
-                        if (it != psig_.end() && same_sig(it->second, sg) && ver_[xe] == it->second.op) {
+                        const ProlongSig *prev = psig_.find((uint64_t)xe);
+                        if (prev != nullptr && same_sig(*prev, sg) && ver_[xe] == prev->op) {
                             continue; /* recomputes the value the face already holds */
                         }
                         p.owrite |= 1 << q;
@@ -849,7 +912,7 @@ private:
         reads.erase(std::unique(reads.begin(), reads.end()), reads.end());
         add_group(p, reads, writes);
         for (auto &e : sigs) {
-            psig_[e.first] = e.second;
+            psig_.put((uint64_t)e.first, e.second);
         }
         return true;
     }
@@ -1290,7 +1353,7 @@ private:
     std::vector<Elem> rd_;       /* elements each op reads (parallel to prod_) */
     std::vector<Elem> wr_;       /* elements each op writes */
     std::vector<FxPop> groups_;  /* face-prolongation groups (SPACE_GROUP ops) */
-    std::unordered_map<int64_t, ProlongSig> psig_;
+    ElemMap<ProlongSig> psig_;
     std::vector<int64_t> g_reads_, g_writes_;             /* prolong_group scratch */
     std::vector<std::pair<int64_t, ProlongSig>> g_sigs_;
     FxPlanStats stats_;
