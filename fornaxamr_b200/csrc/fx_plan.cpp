@@ -1228,27 +1228,43 @@ private:
          * only final face versions, so its wave is max(lw[faces]) + 1 and
          * blocks are independent: they run on worker threads and are merged
          * in block order. */
-        std::vector<std::vector<FxBop>> wb;
+        std::vector<FxBop> bops_all;
+        std::vector<int> bops_begin;
         if (cfg_.mhd) {
             const int nt = compile_threads();
             const int na = (int)plan.active.size();
             std::vector<std::vector<std::pair<int16_t, FxBop>>> part(nt);
+            std::vector<std::vector<int>> cnt(nt);
             std::vector<long long> rew(nt, 0);
             parallel_for(nt, [&](int t) {
                 std::vector<std::pair<int16_t, FxBop>> &out = part[t];
+                /* per block: every face resolved once through its copy chain */
+                std::vector<int32_t> fkey(3 * FX_NFACES);
+                std::vector<int16_t> fwave(3 * FX_NFACES);
+                std::vector<char> ftouch(3 * FX_NFACES);
                 for (int ai = (int)((int64_t)na * t / nt); ai < (int)((int64_t)na * (t + 1) / nt); ++ai) {
                     const int b = plan.active[ai];
+                    for (int d = 0; d < 3; ++d) {
+                        for (int f = 0; f < FX_NFACES; ++f) {
+                            int64_t e = face_elem(b, d, f);
+                            int v = ver_[e];
+                            ftouch[d * FX_NFACES + f] = v >= 0;
+                            resolve(e, v, &rew[t]);
+                            fkey[d * FX_NFACES + f] = face_key(e);
+                            fwave[d * FX_NFACES + f] = (int16_t)(lw[(Elem)e] + 1);
+                        }
+                    }
                     for (int i = -NG; i < BS + NG; ++i) {
                         for (int j = -NG; j < BS + NG; ++j) {
                             for (int k = -NG; k < BS + NG; ++k) {
                                 const bool ghost = i < 0 || i >= BS || j < 0 || j >= BS || k < 0 || k >= BS;
-                                int64_t f[6] = {
-                                    face_elem(b, 0, fidx(0, i, j, k)), face_elem(b, 0, fidx(0, i + 1, j, k)),
-                                    face_elem(b, 1, fidx(1, i, j, k)), face_elem(b, 1, fidx(1, i, j + 1, k)),
-                                    face_elem(b, 2, fidx(2, i, j, k)), face_elem(b, 2, fidx(2, i, j, k + 1))};
+                                const int f[6] = {
+                                    fidx(0, i, j, k), fidx(0, i + 1, j, k),
+                                    FX_NFACES + fidx(1, i, j, k), FX_NFACES + fidx(1, i, j + 1, k),
+                                    2 * FX_NFACES + fidx(2, i, j, k), 2 * FX_NFACES + fidx(2, i, j, k + 1)};
                                 bool touched = false;
                                 for (int q = 0; q < 6; ++q) {
-                                    if (ver_[f[q]] >= 0) touched = true;
+                                    if (ftouch[f[q]]) touched = true;
                                 }
                                 if (!ghost && !touched) continue;
                                 FxBop bo;
@@ -1256,28 +1272,40 @@ private:
                                 bo.pad = 0;
                                 int wave = 0;
                                 for (int q = 0; q < 6; ++q) {
-                                    int v = ver_[f[q]];
-                                    int64_t e = f[q];
-                                    resolve(e, v, &rew[t]);
-                                    bo.f[q] = face_key(e);
-                                    wave = std::max(wave, lw[(Elem)e] + 1);
+                                    bo.f[q] = fkey[f[q]];
+                                    wave = std::max(wave, (int)fwave[f[q]]);
                                 }
                                 out.emplace_back((int16_t)wave, bo);
+                                if ((int)cnt[t].size() <= wave) cnt[t].resize(wave + 1, 0);
+                                ++cnt[t][wave];
                             }
                         }
                     }
                 }
             });
+            int nbw = 0;
             for (int t = 0; t < nt; ++t) {
                 stats_.rewired += rew[t];
-                for (const auto &e : part[t]) {
-                    const int wave = e.first;
-                    nwaves = std::max(nwaves, wave + 1);
-                    if ((int)wb.size() <= wave) wb.resize(wave + 1);
-                    wb[wave].push_back(e.second);
-                }
-                std::vector<std::pair<int16_t, FxBop>>().swap(part[t]);
+                nbw = std::max(nbw, (int)cnt[t].size());
             }
+            nwaves = std::max(nwaves, nbw);
+            /* wave-major, thread-minor placement (block order within a wave) */
+            std::vector<std::vector<size_t>> at(nt, std::vector<size_t>(nbw, 0));
+            bops_begin.assign(nbw + 1, 0);
+            size_t run = 0;
+            for (int w = 0; w < nbw; ++w) {
+                bops_begin[w] = (int)run;
+                for (int t = 0; t < nt; ++t) {
+                    at[t][w] = run;
+                    run += w < (int)cnt[t].size() ? cnt[t][w] : 0;
+                }
+            }
+            bops_begin[nbw] = (int)run;
+            bops_all.resize(run);
+            parallel_for(nt, [&](int t) {
+                for (const auto &e : part[t]) bops_all[at[t][e.first]++] = e.second;
+                std::vector<std::pair<int16_t, FxBop>>().swap(part[t]);
+            });
         }
         std::vector<int16_t>().swap(lw);
         std::vector<int16_t>().swap(lr);
@@ -1331,12 +1359,10 @@ private:
             const int nt = compile_threads();
             for (const auto &bk : buckets) sort_by_dst(bk.first, bk.second, nt);
         }
+        g.b_ops.swap(bops_all);
         g.b_begin.assign(1, 0);
         for (int w = 0; w < nwaves; ++w) {
-            if (w < (int)wb.size()) {
-                g.b_ops.insert(g.b_ops.end(), wb[w].begin(), wb[w].end());
-            }
-            g.b_begin.push_back((int)g.b_ops.size());
+            g.b_begin.push_back(w + 1 < (int)bops_begin.size() ? bops_begin[w + 1] : (int)g.b_ops.size());
         }
         plan.stats = stats_;
     }
