@@ -40,8 +40,10 @@
 #include <cmath>
 #include <cstdint>
 #include <cstring>
+#include <memory>
 #include <thread>
 #include <unordered_map>
+#include <utility>
 
 namespace {
 
@@ -174,6 +176,40 @@ struct SeqOp {
 /* element ids: cells, cell fields and faces of all blocks in one space */
 using Elem = uint32_t;
 
+/* an allocator whose resize leaves new elements uninitialised, so that the
+ * threads which fill a grown buffer are the first to touch its pages */
+template <class T>
+struct UninitAlloc : std::allocator<T> {
+    template <class U>
+    struct rebind {
+        using other = UninitAlloc<U>;
+    };
+    UninitAlloc() = default;
+    template <class U>
+    UninitAlloc(const UninitAlloc<U> &) noexcept {}
+    template <class U, class... A>
+    void construct(U *p, A &&...a)
+    {
+        if constexpr (sizeof...(A) == 0) {
+            ::new ((void *)p) U;
+        } else {
+            ::new ((void *)p) U(std::forward<A>(a)...);
+        }
+    }
+};
+template <class T>
+using Buf = std::vector<T, UninitAlloc<T>>;
+
+/* operations recorded by one worker thread of a parallel replay phase,
+ * merged into the sequence afterwards (indices relative to these vectors) */
+struct Rec {
+    Buf<SeqOp> seq;
+    Buf<int> prod;
+    Buf<Elem> rd;
+    Buf<Elem> wr;
+    long long rewired = 0;
+};
+
 /* open-addressing map from a face element to the signature of the value
  * a face-prolongation group stored there (linear probing, grows at half
  * load; keys are element ids, never ~0) */
@@ -301,10 +337,12 @@ public:
         }
         const int passes[3] = {KIND_SAME, KIND_RESTRICT, KIND_PROLONG};
         for (int kind : passes) {
-            for (int b : plan.active) {
-                if (!send_cells(b, kind)) return false;
+            if (kind != KIND_SAME || !same_pass_parallel(plan, false)) {
+                for (int b : plan.active) {
+                    if (!send_cells(b, kind)) return false;
+                }
             }
-            if (cfg_.mhd) {
+            if (cfg_.mhd && (kind != KIND_SAME || !same_pass_parallel(plan, true))) {
                 for (int b : plan.active) {
                     if (!send_faces(b, kind)) return false;
                 }
@@ -416,22 +454,163 @@ private:
         return (int32_t)(((bd / 3) << 15) | (r % FX_NFACES));
     }
 
-    void add_single(FxGop op, int space, int64_t src, int64_t w)
+    /* r != nullptr: record into a worker's buffer; the element versions are
+     * set when the buffers are merged (parallel phases never read an element
+     * they write) */
+    void add_single(FxGop op, int space, int64_t src, int64_t w, Rec *r = nullptr)
     {
         SeqOp s;
         int v = ver_[src];
-        resolve(src, v, &stats_.rewired);
+        resolve(src, v, r ? &r->rewired : &stats_.rewired);
         op.src = space == SPACE_CELL ? cell_key(src) : face_key(src);
         s.op = op;
         s.src_ver = v;
         s.space = space;
-        s.prod_begin = (int)prod_.size();
-        prod_.push_back(v);
-        rd_.push_back((Elem)src);
-        s.w_begin = (int)wr_.size();
-        wr_.push_back((Elem)w);
-        seq_.push_back(s);
-        ver_[w] = (int)seq_.size() - 1;
+        Buf<SeqOp> &seq = r ? r->seq : seq_;
+        Buf<int> &prod = r ? r->prod : prod_;
+        Buf<Elem> &rd = r ? r->rd : rd_;
+        Buf<Elem> &wr = r ? r->wr : wr_;
+        s.prod_begin = (int)prod.size();
+        prod.push_back(v);
+        rd.push_back((Elem)src);
+        s.w_begin = (int)wr.size();
+        wr.push_back((Elem)w);
+        seq.push_back(s);
+        if (!r) ver_[w] = (int)seq_.size() - 1;
+    }
+
+    /* appends the workers' buffers in worker order and sets the versions of
+     * the elements they wrote; workers own disjoint destination blocks, so
+     * each copies its part and sets its versions in parallel */
+    void merge(std::vector<Rec> &recs)
+    {
+        const int nr = (int)recs.size();
+        std::vector<size_t> sb(nr + 1), pb(nr + 1), wb(nr + 1);
+        sb[0] = seq_.size();
+        pb[0] = prod_.size();
+        wb[0] = wr_.size();
+        for (int t = 0; t < nr; ++t) {
+            sb[t + 1] = sb[t] + recs[t].seq.size();
+            pb[t + 1] = pb[t] + recs[t].prod.size();
+            wb[t + 1] = wb[t] + recs[t].wr.size();
+            stats_.rewired += recs[t].rewired;
+        }
+        seq_.resize(sb[nr]);
+        prod_.resize(pb[nr]);
+        rd_.resize(pb[nr]);
+        wr_.resize(wb[nr]);
+        parallel_for(nr, [&](int t) {
+            Rec &r = recs[t];
+            std::copy(r.prod.begin(), r.prod.end(), prod_.begin() + pb[t]);
+            std::copy(r.rd.begin(), r.rd.end(), rd_.begin() + pb[t]);
+            std::copy(r.wr.begin(), r.wr.end(), wr_.begin() + wb[t]);
+            for (size_t q = 0; q < r.seq.size(); ++q) {
+                SeqOp x = r.seq[q];
+                x.prod_begin += (int)pb[t];
+                x.w_begin += (int)wb[t];
+                seq_[sb[t] + q] = x;
+                ver_[wr_[x.w_begin]] = (int)(sb[t] + q);
+            }
+            r = Rec();
+        });
+    }
+
+    /* The SAME pass of cell sends (faces = false) or field sends (true) with
+     * the work split by destination block: every operation writes a ghost
+     * element of its destination and reads active elements that no ghost
+     * operation writes, so operations into different destinations commute
+     * and each destination keeps the reference's (source block, slot)
+     * order. */
+    /* true when every element a same-level slot copies from is active:
+     * a copy writes only ghost cells or inactive faces, so no copy of the
+     * pass then reads what another one writes */
+    static bool same_sources_active(const fx_slot &sl, bool faces)
+    {
+        for (int dir = 0; dir < (faces ? 3 : 1); ++dir) {
+            const int ext = faces ? 1 : 0;
+            const int ni = sl.recv_loc_end[0] - sl.recv_loc_start[0] + (ext && dir == 0 ? 1 : 0);
+            const int nj = sl.recv_loc_end[1] - sl.recv_loc_start[1] + (ext && dir == 1 ? 1 : 0);
+            const int nk = sl.recv_loc_end[2] - sl.recv_loc_start[2] + (ext && dir == 2 ? 1 : 0);
+            for (int i = 0; i < ni; ++i) {
+                for (int j = 0; j < nj; ++j) {
+                    for (int k = 0; k < nk; ++k) {
+                        const int si = i + sl.send_loc_start[0];
+                        const int sj = j + sl.send_loc_start[1];
+                        const int sk = k + sl.send_loc_start[2];
+                        if (!faces) {
+                            if (si < 0 || si >= BS || sj < 0 || sj >= BS || sk < 0 || sk >= BS) return false;
+                        } else if (!face_active(dir, i + sl.recv_loc_start[0], j + sl.recv_loc_start[1],
+                                       k + sl.recv_loc_start[2]) && !face_active(dir, si, sj, sk)) {
+                            return false;
+                        }
+                    }
+                }
+            }
+        }
+        return true;
+    }
+
+    /* returns false (nothing recorded) when a source may be written in the
+     * pass; the caller then replays it in the reference's order */
+    bool same_pass_parallel(const FxPlan &plan, bool faces)
+    {
+        std::vector<std::vector<std::pair<int, int>>> in(n_);
+        long long work = 0;
+        for (int b : plan.active) {
+            for (int n = 0; n < FX_NSLOTS; ++n) {
+                const fx_slot &sl = b_[b].slot[n];
+                if (sl.id < 0 || sl.id >= n_ || !active_block(b_[sl.id]) || sl.rel_level != 0) continue;
+                in[sl.id].emplace_back(b, n);
+                ++work;
+            }
+        }
+        std::vector<int> dests;
+        for (int d : plan.active) {
+            if (!in[d].empty()) dests.push_back(d);
+        }
+        const int nt = std::max(1, std::min(compile_threads(), (int)dests.size()));
+        std::vector<char> ok(nt, 1);
+        parallel_for(nt, [&](int t) {
+            for (size_t q = (size_t)t; q < dests.size() && ok[t]; q += nt) {
+                for (const auto &e : in[dests[q]]) {
+                    if (!same_sources_active(b_[e.first].slot[e.second], faces)) {
+                        ok[t] = 0;
+                        break;
+                    }
+                }
+            }
+        });
+        for (char c : ok) {
+            if (!c) return false;
+        }
+        /* contiguous destination ranges of about equal slot counts */
+        std::vector<size_t> cut(nt + 1, dests.size());
+        cut[0] = 0;
+        {
+            long long acc = 0;
+            int t = 1;
+            for (size_t q = 0; q < dests.size() && t < nt; ++q) {
+                acc += (long long)in[dests[q]].size();
+                if (acc * nt >= work * t) cut[t++] = q + 1;
+            }
+        }
+        std::vector<Rec> recs(nt);
+        parallel_for(nt, [&](int t) {
+            Rec &r = recs[t];
+            for (size_t q = cut[t]; q < cut[t + 1]; ++q) {
+                const int d = dests[q];
+                for (const auto &e : in[d]) {
+                    const fx_slot &sl = b_[e.first].slot[e.second];
+                    if (faces) {
+                        copy_same_level(e.first, d, sl, &r);
+                    } else {
+                        cells_same_level(e.first, sl, &r);
+                    }
+                }
+            }
+        });
+        merge(recs);
+        return true;
     }
 
     void add_multi(FxGop op, int space, const int64_t *reads, int nr, int64_t w)
@@ -547,6 +726,31 @@ private:
         }
     }
 
+    /* the copies of one same-level slot of prj_boundary_send
+     * (src/prj_boundary.c:270-285) */
+    void cells_same_level(int b, const fx_slot &sl, Rec *r)
+    {
+        const int id = sl.id;
+        const int ni = sl.recv_loc_end[0] - sl.recv_loc_start[0];
+        const int nj = sl.recv_loc_end[1] - sl.recv_loc_start[1];
+        const int nk = sl.recv_loc_end[2] - sl.recv_loc_start[2];
+        for (int i = 0; i < ni; ++i) {
+            for (int j = 0; j < nj; ++j) {
+                for (int k = 0; k < nk; ++k) {
+                    const int si = i + sl.send_loc_start[0];
+                    const int sj = j + sl.send_loc_start[1];
+                    const int sk = k + sl.send_loc_start[2];
+                    const int dc = lidx(i + sl.recv_loc_start[0], j + sl.recv_loc_start[1], k + sl.recv_loc_start[2]);
+                    FxGop op;
+                    op.dst = FX_CELL_KEY(id, dc);
+                    op.aux = 0;
+                    op.type = FX_GOP_COPY;
+                    add_single(op, SPACE_CELL, cell_elem(b, lidx(si, sj, sk)), cell_elem(id, dc), r);
+                }
+            }
+        }
+    }
+
     /* prj_boundary_send (src/prj_boundary.c:190-399), cell part */
     bool send_cells(int b, int kind)
     {
@@ -558,6 +762,10 @@ private:
             }
             const int sk = sl.rel_level == 0 ? KIND_SAME : sl.rel_level < 0 ? KIND_RESTRICT : KIND_PROLONG;
             if (sk != kind) {
+                continue;
+            }
+            if (sk == KIND_SAME) {
+                cells_same_level(b, sl, nullptr);
                 continue;
             }
             const int ni = sl.recv_loc_end[0] - sl.recv_loc_start[0];
@@ -573,12 +781,7 @@ private:
                         FxGop op;
                         op.dst = FX_CELL_KEY(id, dc);
                         op.aux = 0;
-                        if (sl.rel_level == 0) {
-                            const int sc = lidx(i + sl.send_loc_start[0], j + sl.send_loc_start[1],
-                                k + sl.send_loc_start[2]);
-                            op.type = FX_GOP_COPY;
-                            add_single(op, SPACE_CELL, cell_elem(b, sc), cell_elem(id, dc));
-                        } else if (sl.rel_level == -1) {
+                        if (sl.rel_level == -1) {
                             const int si = 2 * i + sl.send_loc_start[0];
                             const int sj = 2 * j + sl.send_loc_start[1];
                             const int sk2 = 2 * k + sl.send_loc_start[2];
@@ -724,7 +927,7 @@ private:
      * reference buffers the source faces before writing; source and
      * destination are different blocks, so element operations are
      * equivalent. */
-    void copy_same_level(int src_b, int dst_b, const fx_slot &sl)
+    void copy_same_level(int src_b, int dst_b, const fx_slot &sl, Rec *r = nullptr)
     {
         for (int dir = 0; dir < 3; ++dir) {
             const int ni = sl.recv_loc_end[0] - sl.recv_loc_start[0] + (dir == 0 ? 1 : 0);
@@ -737,15 +940,17 @@ private:
                         const int rj = j + sl.recv_loc_start[1];
                         const int rk = k + sl.recv_loc_start[2];
                         if (face_active(dir, ri, rj, rk)) continue;
-                        const int sf = fidx(dir, i + sl.send_loc_start[0], j + sl.send_loc_start[1],
-                            k + sl.send_loc_start[2]);
+                        const int si = i + sl.send_loc_start[0];
+                        const int sj = j + sl.send_loc_start[1];
+                        const int sk = k + sl.send_loc_start[2];
+                        const int sf = fidx(dir, si, sj, sk);
                         const int df = fidx(dir, ri, rj, rk);
                         if (!lands(dst_b, dir, df, FID_SAME)) continue;
                         FxGop op;
                         op.dst = (dst_b << 15) | df;
                         op.aux = dir;
                         op.type = FX_FOP_COPY;
-                        add_single(op, SPACE_FACE, face_elem(src_b, dir, sf), face_elem(dst_b, dir, df));
+                        add_single(op, SPACE_FACE, face_elem(src_b, dir, sf), face_elem(dst_b, dir, df), r);
                     }
                 }
             }
@@ -1374,10 +1579,10 @@ private:
     int64_t nface_;
     std::vector<int8_t> fid_;
     std::vector<int> ver_;       /* element -> producer op (-1: initial value) */
-    std::vector<SeqOp> seq_;
-    std::vector<int> prod_;      /* producers of the values each op reads */
-    std::vector<Elem> rd_;       /* elements each op reads (parallel to prod_) */
-    std::vector<Elem> wr_;       /* elements each op writes */
+    Buf<SeqOp> seq_;
+    Buf<int> prod_;              /* producers of the values each op reads */
+    Buf<Elem> rd_;               /* elements each op reads (parallel to prod_) */
+    Buf<Elem> wr_;               /* elements each op writes */
     std::vector<FxPop> groups_;  /* face-prolongation groups (SPACE_GROUP ops) */
     ElemMap<ProlongSig> psig_;
     std::vector<int64_t> g_reads_, g_writes_;             /* prolong_group scratch */
