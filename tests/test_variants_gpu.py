@@ -45,9 +45,9 @@ def assert_state_equal(ctx, ref, mhd, active_only=False):
     if active_only:
         ints, _, _ = ref.mesh_arrays()
         sel = ints[:, 2] == 1
-    assert np.array_equal(W[sel], W_ref[sel])
+    assert H.same_values(W[sel], W_ref[sel])
     if mhd:
-        assert np.array_equal(Bf[sel], Bf_ref[sel])
+        assert H.same_values(Bf[sel], Bf_ref[sel])
 
 
 @pytest.mark.parametrize("variant", sorted(VARIANTS))
