@@ -145,6 +145,34 @@ def plan_export(cfg: FxConfig, desc, which: int):
     return ops[: nops.value], waves
 
 
+def shard_export(cfg: FxConfig, desc, owner, nranks: int, rank: int, which: int):
+    """Host-only dump of rank `rank`'s part of a sharded mesh
+    (fx_shard_export): which 0, 1, 4, 6 -> (ops, wave_begin) as plan_export
+    in the rank's local block numbering; 2 / 3 the correction records; 7 ->
+    (local-to-global block map, owned block count); 8 + k / 12 + k -> the send
+    / receive list of exchange k (0 cells, 1 faces, 2 flux, 3 EMF) as
+    ((local block, index) pairs [n, 2], per-peer offsets [nranks + 1])."""
+    L = library()
+    own = np.ascontiguousarray(owner, dtype=np.int32)
+    ip = C.POINTER(C.c_int32)
+    nops = C.c_int(0)
+    nwaves = C.c_int(0)
+    rc = L.fx_shard_export(C.byref(cfg), len(desc), desc, own.ctypes.data_as(ip), nranks, rank, which,
+                           None, C.byref(nops), None, C.byref(nwaves))
+    if rc != 0:
+        raise FxError(rc, "fx_shard_export failed")
+    width = 4 if which in (0, 1) else 1 if which == 7 else 2 if which >= 8 else 8
+    ops = np.zeros((max(nops.value, 1), width), dtype=np.int32)
+    waves = np.zeros(nwaves.value + 1, dtype=np.int32)
+    rc = L.fx_shard_export(C.byref(cfg), len(desc), desc, own.ctypes.data_as(ip), nranks, rank, which,
+                           ops.ctypes.data_as(ip), C.byref(nops), waves.ctypes.data_as(ip), C.byref(nwaves))
+    if rc != 0:
+        raise FxError(rc, "fx_shard_export failed")
+    if which == 7:
+        return ops[: nops.value, 0].copy(), nwaves.value
+    return ops[: nops.value], waves
+
+
 class Context:
     """One device context (fx_ctx) with a mesh mirror."""
 

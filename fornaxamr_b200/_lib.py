@@ -106,7 +106,7 @@ EXPORTS = [
     "fx_autotune", "fx_calc_dt_noalloc", "fx_face_eval_host", "fx_face_vjp_host",
     "fx_adjoint_forward", "fx_adjoint_backward", "fx_adjoint_time", "fx_set_flux_shape",
     "fx_amr_configure", "fx_amr_tag", "fx_amr_adapt", "fx_get_mesh", "fx_amr_energy_injected",
-    "fx_amr_remesh_host", "fx_amr_timings",
+    "fx_amr_remesh_host", "fx_amr_timings", "fx_shard_export",
 ]
 PHASE_FLUX, PHASE_EMF, PHASE_CT, PHASE_CELLS, PHASE_GHOST, PHASE_STEP = range(6)
 
@@ -150,6 +150,8 @@ def load() -> C.CDLL:
     L.fx_run.argtypes = [vp, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double, dp]
     L.fx_plan_export.argtypes = [C.POINTER(FxConfig), C.c_int, C.POINTER(FxBlockDesc), C.c_int,
                                  ip, C.POINTER(C.c_int), ip, C.POINTER(C.c_int)]
+    L.fx_shard_export.argtypes = [C.POINTER(FxConfig), C.c_int, C.POINTER(FxBlockDesc), ip, C.c_int,
+                                  C.c_int, C.c_int, ip, C.POINTER(C.c_int), ip, C.POINTER(C.c_int)]
     L.fx_time_phase.argtypes = [vp, C.c_int, C.c_int, C.c_double, dp]
     L.fx_info.argtypes = [vp, C.c_int, C.POINTER(C.c_longlong)]
     L.fx_autotune.argtypes = [vp, dp, C.c_int, C.POINTER(C.c_int)]

@@ -302,6 +302,15 @@ public:
         return true;
     }
 
+    /* sharded compile: owner[b] is the rank of block b; run() then keeps
+     * rank `rank`'s part of the plan */
+    void set_owners(const int *owner, int nranks, int rank)
+    {
+        owner_ = owner;
+        nranks_ = nranks;
+        rank_ = rank;
+    }
+
     bool run(FxPlan &plan, std::string *err)
     {
         err_ = err;
@@ -366,6 +375,11 @@ public:
         } else {
             plan.emf_corr_begin.assign(1, 0);
         }
+        if (owner_) {
+            shard_records(plan.flux_corr, plan.flux_corr_begin, 4, finit_);
+            shard_records(plan.emf_corr, plan.emf_corr_begin, 2, einit_);
+            localize(plan);
+        }
         return true;
     }
 
@@ -398,6 +412,12 @@ private:
 
     int64_t cell_elem(int b, int c) const { return (int64_t)b * FX_NCELLS + c; }
     int64_t face_elem(int b, int dir, int f) const { return 2 * ncell_ + ((int64_t)b * 3 + dir) * FX_NFACES + f; }
+    int block_of(int64_t e) const
+    {
+        if (e < ncell_) return (int)(e / FX_NCELLS);
+        if (e < 2 * ncell_) return (int)((e - ncell_) / FX_NCELLS);
+        return (int)((e - 2 * ncell_) / (3 * FX_NFACES));
+    }
 
     /* ---- recording -------------------------------------------------------- */
 
@@ -1396,6 +1416,18 @@ private:
                 if (prod_[p] >= 0) live[prod_[p]] = 1;
             }
         }
+        if (owner_) {
+            /* a live op belongs to the ranks owning the blocks it writes */
+            need_.assign(nseq, 0);
+            ginit_.assign(nranks_, {});
+            touched_.assign(n_, 0);
+            for (int x = 0; x < nseq; ++x) {
+                if (!live[x]) continue;
+                for (int q = seq_[x].w_begin; q < w_end(x); ++q) {
+                    need_[x] |= (uint16_t)(1u << owner_[block_of(wr_[q])]);
+                }
+            }
+        }
         /* 3. levelling over cell, cell-field and face elements: latest wave
          * that wrote / read each element (a fill has a handful of waves, far
          * below the int16 range) */
@@ -1441,14 +1473,22 @@ private:
             std::vector<std::vector<std::pair<int16_t, FxBop>>> part(nt);
             std::vector<std::vector<int>> cnt(nt);
             std::vector<long long> rew(nt, 0);
+            std::vector<std::vector<std::vector<Elem>>> tinit(nt, std::vector<std::vector<Elem>>(owner_ ? nranks_ : 0));
             parallel_for(nt, [&](int t) {
                 std::vector<std::pair<int16_t, FxBop>> &out = part[t];
                 /* per block: every face resolved once through its copy chain */
                 std::vector<int32_t> fkey(3 * FX_NFACES);
                 std::vector<int16_t> fwave(3 * FX_NFACES);
                 std::vector<char> ftouch(3 * FX_NFACES);
+                /* sharded: the producer and element of each resolved face,
+                 * and whether a cell-field op of the block read it yet */
+                std::vector<int> fver(owner_ ? 3 * FX_NFACES : 0);
+                std::vector<Elem> fel(owner_ ? 3 * FX_NFACES : 0);
+                std::vector<char> fmark(owner_ ? 3 * FX_NFACES : 0);
                 for (int ai = (int)((int64_t)na * t / nt); ai < (int)((int64_t)na * (t + 1) / nt); ++ai) {
                     const int b = plan.active[ai];
+                    const int ob = owner_ ? owner_[b] : 0;
+                    const bool emit = !owner_ || ob == rank_;
                     for (int d = 0; d < 3; ++d) {
                         for (int f = 0; f < FX_NFACES; ++f) {
                             int64_t e = face_elem(b, d, f);
@@ -1457,6 +1497,11 @@ private:
                             resolve(e, v, &rew[t]);
                             fkey[d * FX_NFACES + f] = face_key(e);
                             fwave[d * FX_NFACES + f] = (int16_t)(lw[(Elem)e] + 1);
+                            if (owner_) {
+                                fver[d * FX_NFACES + f] = v;
+                                fel[d * FX_NFACES + f] = (Elem)e;
+                                fmark[d * FX_NFACES + f] = 0;
+                            }
                         }
                     }
                     for (int i = -NG; i < BS + NG; ++i) {
@@ -1472,6 +1517,22 @@ private:
                                     if (ftouch[f[q]]) touched = true;
                                 }
                                 if (!ghost && !touched) continue;
+                                if (owner_) {
+                                    /* the block's owner reads these faces:
+                                     * their producers join its part, values
+                                     * at fill start come from their owner */
+                                    for (int q = 0; q < 6; ++q) {
+                                        const int fq = f[q];
+                                        if (fmark[fq]) continue;
+                                        fmark[fq] = 1;
+                                        if (fver[fq] >= 0) {
+                                            __atomic_fetch_or(&need_[fver[fq]], (uint16_t)(1u << ob), __ATOMIC_RELAXED);
+                                        } else if (owner_[block_of(fel[fq])] != ob) {
+                                            tinit[t][ob].push_back(fel[fq]);
+                                        }
+                                    }
+                                    if (!emit) continue;
+                                }
                                 FxBop bo;
                                 bo.dst = FX_CELL_KEY(b, lidx(i, j, k));
                                 bo.pad = 0;
@@ -1492,6 +1553,9 @@ private:
             for (int t = 0; t < nt; ++t) {
                 stats_.rewired += rew[t];
                 nbw = std::max(nbw, (int)cnt[t].size());
+                for (int r = 0; r < (int)tinit[t].size(); ++r) {
+                    ginit_[r].insert(ginit_[r].end(), tinit[t][r].begin(), tinit[t][r].end());
+                }
             }
             nwaves = std::max(nwaves, nbw);
             /* wave-major, thread-minor placement (block order within a wave) */
@@ -1514,6 +1578,11 @@ private:
         }
         std::vector<int16_t>().swap(lw);
         std::vector<int16_t>().swap(lr);
+        if (owner_) {
+            shard_closure();
+        }
+        const uint16_t rbit = (uint16_t)(1u << rank_);
+        auto keep = [&](int x) { return opwave[x] >= 0 && (!owner_ || (need_[x] & rbit)); };
         /* 5. per-wave arrays: a counting sort of the operations by (wave,
          * type), replay order kept within a bucket (the replay visits each
          * destination box in storage order) */
@@ -1521,7 +1590,7 @@ private:
         constexpr int NT = 16; /* op type values are below 16 */
         std::vector<int> nc((size_t)nwaves * NT + 1, 0), nf((size_t)nwaves * NT + 1, 0), np(nwaves + 1, 0);
         for (int x = 0; x < nseq; ++x) {
-            if (opwave[x] < 0) continue;
+            if (!keep(x)) continue;
             const SeqOp &o = seq_[x];
             if (o.space == SPACE_CELL) ++nc[(size_t)opwave[x] * NT + o.op.type + 1];
             else if (o.space == SPACE_FACE) ++nf[(size_t)opwave[x] * NT + o.op.type + 1];
@@ -1543,7 +1612,7 @@ private:
         }
         g.p_begin.assign(np.begin(), np.end());
         for (int x = 0; x < nseq; ++x) {
-            if (opwave[x] < 0) continue;
+            if (!keep(x)) continue;
             const SeqOp &o = seq_[x];
             if (o.space == SPACE_CELL) g.cell_ops[nc[(size_t)opwave[x] * NT + o.op.type]++] = o.op;
             else if (o.space == SPACE_FACE) g.face_ops[nf[(size_t)opwave[x] * NT + o.op.type]++] = o.op;
@@ -1572,6 +1641,192 @@ private:
         plan.stats = stats_;
     }
 
+    /* ---- sharding -------------------------------------------------------- */
+
+    /* reverse pass: an op joins the parts of the ranks that read its value;
+     * a read of a fill-start value from another rank's block is recorded
+     * for the reading rank */
+    void shard_closure()
+    {
+        const uint16_t rbit = (uint16_t)(1u << rank_);
+        for (int x = (int)seq_.size() - 1; x >= 0; --x) {
+            const uint16_t m = need_[x];
+            if (!m) continue;
+            const SeqOp &o = seq_[x];
+            const int pe = prod_end(x);
+            for (int p = o.prod_begin; p < pe; ++p) {
+                const int pr = prod_[p];
+                if (pr >= 0) {
+                    need_[pr] |= m;
+                } else {
+                    unsigned rest = m & ~(1u << owner_[block_of(rd_[p])]);
+                    while (rest) {
+                        const int r = __builtin_ctz(rest);
+                        rest &= rest - 1;
+                        ginit_[r].push_back(rd_[p]);
+                    }
+                }
+                if (m & rbit) touched_[block_of(rd_[p])] = 1;
+            }
+            if (m & rbit) {
+                for (int q = o.w_begin; q < w_end(x); ++q) touched_[block_of(wr_[q])] = 1;
+            }
+        }
+        for (auto &v : ginit_) {
+            std::sort(v.begin(), v.end());
+            v.erase(std::unique(v.begin(), v.end()), v.end());
+        }
+    }
+
+    static int64_t rec_key(int b, int idx) { return ((int64_t)b << 32) | (uint32_t)idx; }
+
+    /* the same for correction records (levelled, in wave order): a record
+     * reads nsrc entries of src_block, as the face / edge kernel left them
+     * or as an earlier record rewrote them; rank rank_ keeps the records
+     * into its blocks and their producers */
+    void shard_records(std::vector<FxCorr> &recs, std::vector<int> &begin, int nsrc,
+        std::vector<std::vector<int64_t>> &init)
+    {
+        const int n = (int)recs.size();
+        std::vector<int> prod((size_t)n * nsrc, -1);
+        std::unordered_map<int64_t, int> last;
+        last.reserve((size_t)n * 2 + 1);
+        for (int r = 0; r < n; ++r) {
+            for (int k = 0; k < nsrc; ++k) {
+                auto it = last.find(rec_key(recs[r].src_block, recs[r].src[k]));
+                if (it != last.end()) prod[(size_t)r * nsrc + k] = it->second;
+            }
+            last[rec_key(recs[r].dst_block, recs[r].dst)] = r;
+        }
+        std::vector<uint16_t> need(n);
+        for (int r = 0; r < n; ++r) need[r] = (uint16_t)(1u << owner_[recs[r].dst_block]);
+        init.assign(nranks_, {});
+        for (int r = n - 1; r >= 0; --r) {
+            for (int k = 0; k < nsrc; ++k) {
+                const int p = prod[(size_t)r * nsrc + k];
+                if (p >= 0) {
+                    need[p] |= need[r];
+                    continue;
+                }
+                unsigned rest = need[r] & ~(1u << owner_[recs[r].src_block]);
+                while (rest) {
+                    const int q = __builtin_ctz(rest);
+                    rest &= rest - 1;
+                    init[q].push_back(rec_key(recs[r].src_block, recs[r].src[k]));
+                }
+            }
+        }
+        std::vector<FxCorr> out;
+        std::vector<int> ob(1, 0);
+        for (size_t w = 0; w + 1 < begin.size(); ++w) {
+            for (int r = begin[w]; r < begin[w + 1]; ++r) {
+                if (!((need[r] >> rank_) & 1)) continue;
+                out.push_back(recs[r]);
+                touched_[recs[r].dst_block] = 1;
+                touched_[recs[r].src_block] = 1;
+            }
+            ob.push_back((int)out.size());
+        }
+        recs.swap(out);
+        begin.swap(ob);
+        for (auto &v : init) {
+            std::sort(v.begin(), v.end());
+            v.erase(std::unique(v.begin(), v.end()), v.end());
+        }
+    }
+
+    /* local numbering (owned active blocks, then the halo, each in mesh
+     * order), the renumbered programs and records, and the exchange lists */
+    void localize(FxPlan &plan)
+    {
+        FxShard &sh = plan.shard;
+        sh.nranks = nranks_;
+        sh.rank = rank_;
+        for (Elem e : ginit_[rank_]) touched_[block_of(e)] = 1;
+        for (int64_t k : finit_[rank_]) touched_[(int)(k >> 32)] = 1;
+        for (int64_t k : einit_[rank_]) touched_[(int)(k >> 32)] = 1;
+        std::vector<int> g2l(n_, -1);
+        std::vector<int> &l2g = sh.local_to_global;
+        for (int b : plan.active) {
+            if (owner_[b] == rank_) l2g.push_back(b);
+        }
+        sh.nowned = (int)l2g.size();
+        for (int b = 0; b < n_; ++b) {
+            if (touched_[b] && owner_[b] != rank_) l2g.push_back(b);
+        }
+        for (int l = 0; l < (int)l2g.size(); ++l) g2l[l2g[l]] = l;
+        auto ck = [&](int32_t key) { return (g2l[key >> 13] << 13) | (key & 8191); };
+        auto fk = [&](int32_t key) { return (g2l[key >> 15] << 15) | (key & 32767); };
+        FxProgram &g = plan.ghost;
+        for (FxGop &o : g.cell_ops) {
+            o.dst = ck(o.dst);
+            o.src = ck(o.src);
+        }
+        for (FxGop &o : g.face_ops) {
+            o.dst = fk(o.dst);
+            o.src = fk(o.src);
+        }
+        for (FxPop &o : g.p_ops) {
+            o.fine = g2l[o.fine];
+            o.coarse = g2l[o.coarse];
+        }
+        for (FxBop &o : g.b_ops) {
+            o.dst = ck(o.dst);
+            for (int q = 0; q < 6; ++q) o.f[q] = fk(o.f[q]);
+        }
+        for (std::vector<FxCorr> *recs : {&plan.flux_corr, &plan.emf_corr}) {
+            for (FxCorr &r : *recs) {
+                r.dst_block = g2l[r.dst_block];
+                r.src_block = g2l[r.src_block];
+            }
+        }
+        plan.active.clear();
+        for (int l = 0; l < sh.nowned; ++l) plan.active.push_back(l);
+        /* exchange lists: rank r receives init[r] from the owners; this rank
+         * sends the part of every init[r] it owns */
+        auto add_ghost = [&](FxXlist *lists, Elem e) {
+            const int b = block_of(e);
+            if (e < (Elem)ncell_) {
+                lists[FX_X_CELLS].el.push_back({g2l[b], (int32_t)(e % FX_NCELLS)});
+            } else {
+                lists[FX_X_FACES].el.push_back({g2l[b], (int32_t)((e - 2 * ncell_) % (3 * FX_NFACES))});
+            }
+        };
+        auto add_rec = [&](FxXlist &list, int64_t k) {
+            list.el.push_back({g2l[(int)(k >> 32)], (int32_t)(k & 0xffffffff)});
+        };
+        for (int k = 0; k < FX_X_KINDS; ++k) {
+            sh.send[k].begin.assign(1, 0);
+            sh.recv[k].begin.assign(1, 0);
+        }
+        for (int p = 0; p < nranks_; ++p) {
+            if (p != rank_) {
+                for (Elem e : ginit_[rank_]) {
+                    if (owner_[block_of(e)] == p) add_ghost(sh.recv, e);
+                }
+                for (Elem e : ginit_[p]) {
+                    if (owner_[block_of(e)] == rank_) add_ghost(sh.send, e);
+                }
+                for (int64_t k : finit_[rank_]) {
+                    if (owner_[(int)(k >> 32)] == p) add_rec(sh.recv[FX_X_FLUX], k);
+                }
+                for (int64_t k : finit_[p]) {
+                    if (owner_[(int)(k >> 32)] == rank_) add_rec(sh.send[FX_X_FLUX], k);
+                }
+                for (int64_t k : einit_[rank_]) {
+                    if (owner_[(int)(k >> 32)] == p) add_rec(sh.recv[FX_X_EMF], k);
+                }
+                for (int64_t k : einit_[p]) {
+                    if (owner_[(int)(k >> 32)] == rank_) add_rec(sh.send[FX_X_EMF], k);
+                }
+            }
+            for (int k = 0; k < FX_X_KINDS; ++k) {
+                sh.send[k].begin.push_back((int)sh.send[k].el.size());
+                sh.recv[k].begin.push_back((int)sh.recv[k].el.size());
+            }
+        }
+    }
+
     const fx_config &cfg_;
     int n_;
     const fx_block_desc *b_;
@@ -1590,6 +1845,15 @@ private:
     FxPlanStats stats_;
     std::string *err_ = nullptr;
     bool overflow_ = false;
+    /* sharding */
+    const int *owner_ = nullptr;
+    int nranks_ = 1;
+    int rank_ = 0;
+    std::vector<uint16_t> need_;               /* per op: ranks whose part holds it */
+    std::vector<std::vector<Elem>> ginit_;     /* per rank: elements read at their
+                                                  fill-start value from other ranks' blocks */
+    std::vector<std::vector<int64_t>> finit_, einit_; /* same for the correction records */
+    std::vector<char> touched_;                /* blocks this rank's part reads or writes */
 };
 
 } /* namespace */
@@ -1599,6 +1863,30 @@ bool fx_build_plan(const fx_config &cfg, int nblocks, const fx_block_desc *block
 {
     plan = FxPlan();
     Compiler c(cfg, nblocks, blocks);
+    return c.run(plan, err);
+}
+
+bool fx_build_shard_plan(const fx_config &cfg, int nblocks, const fx_block_desc *blocks,
+    const int *owner, int nranks, int rank, FxPlan &plan, std::string *err)
+{
+    plan = FxPlan();
+    if (nranks < 1 || nranks > FX_MAX_RANKS || rank < 0 || rank >= nranks || !owner) {
+        if (err) *err = "sharding: nranks outside [1, 16] or rank outside [0, nranks)";
+        return false;
+    }
+    /* the single-device sequence over all blocks: every block takes part */
+    std::vector<fx_block_desc> all(blocks, blocks + nblocks);
+    for (fx_block_desc &b : all) {
+        if (b.id >= 0 && b.active == 1) b.rank = 0;
+    }
+    for (int b = 0; b < nblocks; ++b) {
+        if (all[b].id >= 0 && all[b].active == 1 && (owner[b] < 0 || owner[b] >= nranks)) {
+            if (err) *err = "sharding: an active block has no rank in [0, nranks)";
+            return false;
+        }
+    }
+    Compiler c(cfg, nblocks, all.data());
+    c.set_owners(owner, nranks, rank);
     return c.run(plan, err);
 }
 

@@ -34,6 +34,39 @@ struct FxPlanStats {
     long long dead = 0;             /* overwritten before any read: dropped */
 };
 
+/* One element of a sharded exchange, in the receiving or sending rank's
+ * local block numbering.  idx: the cell (cells; the ghost-filled primitives
+ * move), dir * 8400 + face (faces), the component-0 entry of the block's
+ * stacked flux array (flux; every stored component moves) or the entry of
+ * its EMF array (emf). */
+struct FxXel {
+    int32_t block;
+    int32_t idx;
+};
+
+/* elements exchanged with each peer rank p: el[begin[p], begin[p + 1]) */
+struct FxXlist {
+    std::vector<FxXel> el;
+    std::vector<int> begin;
+};
+
+enum { FX_X_CELLS = 0, FX_X_FACES = 1, FX_X_FLUX = 2, FX_X_EMF = 3, FX_X_KINDS = 4 };
+
+/* A rank's part of a sharded mesh.  Local blocks are the owned active blocks
+ * (first, in mesh order) and then the halo: other ranks' blocks that the
+ * rank's programs read or write.  send[k] lists what this rank packs for
+ * each peer before exchange k, recv[k] what it unpacks into its halo; both
+ * sides of a pair order the elements by global block and index, so the
+ * lists match without being exchanged. */
+struct FxShard {
+    int nranks = 1;
+    int rank = 0;
+    int nowned = 0;
+    std::vector<int> local_to_global;
+    FxXlist send[FX_X_KINDS];
+    FxXlist recv[FX_X_KINDS];
+};
+
 struct FxPlan {
     FxProgram ghost;
     FxPlanStats stats;
@@ -42,13 +75,26 @@ struct FxPlan {
     std::vector<int> flux_corr_begin; /* per wave offsets (+1 closing entry) */
     std::vector<int> emf_corr_begin;
     std::vector<int> active;        /* active block indices in mesh order */
+    FxShard shard;                  /* sharded plans only */
 };
+
+#define FX_MAX_RANKS 16
 
 /* Builds the plan.  Returns false and sets *err for meshes the device path
  * does not handle (e.g. non-outflow field boundaries in an MHD run, which the
  * reference rejects too). */
 bool fx_build_plan(const fx_config &cfg, int nblocks, const fx_block_desc *blocks,
     FxPlan &plan, std::string *err);
+
+/* The part of the single-device plan that rank `rank` of `nranks` runs when
+ * owner[b] gives the rank of every block: the ghost-fill operations that
+ * write its blocks and, transitively, the operations on other ranks' blocks
+ * that produce what they read; the correction records likewise; renumbered
+ * to the rank's local blocks, with the exchange lists (plan.shard).  Running
+ * the parts on all ranks with the exchanges reproduces the single-device
+ * plan's values on every owned block. */
+bool fx_build_shard_plan(const fx_config &cfg, int nblocks, const fx_block_desc *blocks,
+    const int *owner, int nranks, int rank, FxPlan &plan, std::string *err);
 
 /* Only the coarse/fine flux and EMF correction records of the plan (fast:
  * no ghost-fill replay); the other members stay empty. */

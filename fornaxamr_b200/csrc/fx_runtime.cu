@@ -930,20 +930,32 @@ int fx_set_mesh(fx_ctx *c, int nblocks, const fx_block_desc *blocks)
     return FX_SUCCESS;
 }
 
-int fx_plan_export(const fx_config *cfg, int nblocks, const fx_block_desc *blocks, int which,
-    int32_t *ops, int *nops, int32_t *wave_begin, int *nwaves)
+namespace {
+
+/* fx_plan_export / fx_shard_export of a built plan */
+int export_plan(const FxPlan &plan, int which, int32_t *ops, int *nops, int32_t *wave_begin, int *nwaves)
 {
-    if (!cfg || nblocks <= 0 || !blocks || !nops || !nwaves || which < 0 || which > 6) {
-        return FX_EINVAL;
-    }
-    FxPlan plan;
-    std::string perr;
-    const bool corr_only = which == 2 || which == 3;
-    if (!(corr_only ? fx_build_corrections(*cfg, nblocks, blocks, plan, &perr) :
-                      fx_build_plan(*cfg, nblocks, blocks, plan, &perr))) {
-        return FX_EINVAL;
-    }
     const FxProgram &g = plan.ghost;
+    if (which >= 7) {
+        const FxShard &sh = plan.shard;
+        if (which == 7) {
+            const std::vector<int> &m = sh.local_to_global;
+            if (ops && (int)m.size() <= *nops && !m.empty()) std::memcpy(ops, m.data(), m.size() * sizeof(int));
+            *nops = (int)m.size();
+            *nwaves = sh.nowned;
+            return FX_SUCCESS;
+        }
+        const FxXlist &l = which < 12 ? sh.send[which - 8] : sh.recv[which - 12];
+        if (ops && (int)l.el.size() <= *nops && !l.el.empty()) {
+            std::memcpy(ops, l.el.data(), l.el.size() * sizeof(FxXel));
+        }
+        if (wave_begin && sh.nranks <= *nwaves) {
+            std::memcpy(wave_begin, l.begin.data(), l.begin.size() * sizeof(int));
+        }
+        *nops = (int)l.el.size();
+        *nwaves = sh.nranks;
+        return FX_SUCCESS;
+    }
     if (which <= 1 || which == 4 || which == 6) {
         const void *data = which == 0 ? (const void *)g.cell_ops.data() :
             which == 1 ? (const void *)g.face_ops.data() :
@@ -985,6 +997,39 @@ int fx_plan_export(const fx_config *cfg, int nblocks, const fx_block_desc *block
         *nwaves = nw;
     }
     return FX_SUCCESS;
+}
+
+} /* namespace */
+
+int fx_plan_export(const fx_config *cfg, int nblocks, const fx_block_desc *blocks, int which,
+    int32_t *ops, int *nops, int32_t *wave_begin, int *nwaves)
+{
+    if (!cfg || nblocks <= 0 || !blocks || !nops || !nwaves || which < 0 || which > 6) {
+        return FX_EINVAL;
+    }
+    FxPlan plan;
+    std::string perr;
+    const bool corr_only = which == 2 || which == 3;
+    if (!(corr_only ? fx_build_corrections(*cfg, nblocks, blocks, plan, &perr) :
+                      fx_build_plan(*cfg, nblocks, blocks, plan, &perr))) {
+        return FX_EINVAL;
+    }
+    return export_plan(plan, which, ops, nops, wave_begin, nwaves);
+}
+
+int fx_shard_export(const fx_config *cfg, int nblocks, const fx_block_desc *blocks, const int *owner,
+    int nranks, int rank, int which, int32_t *ops, int *nops, int32_t *wave_begin, int *nwaves)
+{
+    if (!cfg || nblocks <= 0 || !blocks || !owner || !nops || !nwaves || which < 0 || which > 15 ||
+        which == 5) {
+        return FX_EINVAL;
+    }
+    FxPlan plan;
+    std::string perr;
+    if (!fx_build_shard_plan(*cfg, nblocks, blocks, owner, nranks, rank, plan, &perr)) {
+        return FX_EINVAL;
+    }
+    return export_plan(plan, which, ops, nops, wave_begin, nwaves);
 }
 
 int fx_upload_block(fx_ctx *c, int b, const double *W, const double *const Bf[3],

@@ -157,6 +157,29 @@ int fx_set_mesh(fx_ctx *ctx, int nblocks, const fx_block_desc *blocks);
 int fx_plan_export(const fx_config *cfg, int nblocks, const fx_block_desc *blocks, int which,
     int32_t *ops, int *nops, int32_t *wave_begin, int *nwaves);
 
+/* ---- sharding over ranks (one GPU per rank) ---------------------------------
+ * The reference decomposes the block list over MPI ranks (block->rank,
+ * prj_mpi_decompose, src/prj_mpi.c:375-470) and exchanges ghost zones
+ * (prj_mpi_post/wait_ghosts_and_bf, src/prj_boundary.c:1184-1222), the
+ * coarse/fine flux and EMF records (prj_mpi_exchange_fluxes_and_emf,
+ * src/prj_mpi.c:4601) and the dt minimum (src/prj_mpi.c:4765-4778).  Here
+ * owner[b] assigns every active block to a rank; each rank runs its part of
+ * the single-device ghost-fill and correction programs (the operations into
+ * its blocks and, transitively, the operations on other ranks' blocks whose
+ * values they read) after receiving the values its part reads from other
+ * ranks' blocks.  Every rank then holds, for its blocks, exactly the values
+ * of the single-device step.
+ *
+ * Host-only inspection of rank `rank`'s part (no device needed): which 0-4,
+ * 6 as fx_plan_export (programs in the rank's local block numbering: owned
+ * blocks first, then the halo); 7: local -> global block map (*nops
+ * entries, *nwaves = owned blocks); 8 + k / 12 + k: the send / receive list
+ * of exchange k (0 cells, 1 faces, 2 flux entries, 3 EMF entries) as
+ * (local block, index) pairs with per-peer offsets in wave_begin (nranks + 1
+ * entries, *nwaves = nranks).  No counterpart in the reference. */
+int fx_shard_export(const fx_config *cfg, int nblocks, const fx_block_desc *blocks, const int *owner,
+    int nranks, int rank, int which, int32_t *ops, int *nops, int32_t *wave_begin, int *nwaves);
+
 /* Host <-> device copies of one block, in the reference's per-block layout:
  * W = block->W_mhd (NHYDRO * NS * 8000 doubles), Bf[d] = block->Bf[d]
  * (NS * 8400 doubles each, may be NULL for hydro), grav[d] = block->grav[d]

@@ -252,16 +252,23 @@ def apply_b_ops(W, Bf, bops, slot):
         W[db, 6 + d, slot, dc] = 0.5 * (Bf[k0 >> 15, d, slot, k0 & 32767] + Bf[k1 >> 15, d, slot, k1 & 32767])
 
 
-def apply_ghost_program(W, Bf, cfg, desc, slot):
-    """Runs the compiled ghost fill (fx_plan_export) in numpy, wave by wave."""
+def apply_ghost_program(W, Bf, cfg, desc, slot, export=None, blocks=None):
+    """Runs the compiled ghost fill (fx_plan_export, or `export(which)` for a
+    rank's part of a sharded mesh, whose local block l is desc[blocks[l]])
+    in numpy, wave by wave."""
     import fornaxamr_b200 as fx
-    cops, cw = fx.plan_export(cfg, desc, 0)
+    if export is None:
+        def export(which):
+            return fx.plan_export(cfg, desc, which)
+    if blocks is None:
+        blocks = range(len(desc))
+    cops, cw = export(0)
     nw = len(cw) - 1
     if Bf is not None:
-        fops, fw = fx.plan_export(cfg, desc, 1)
-        pops, pw = fx.plan_export(cfg, desc, 6)
-        bops, bw = fx.plan_export(cfg, desc, 4)
-        dx = np.array([[desc[b].dx[a] for a in range(3)] for b in range(len(desc))])
+        fops, fw = export(1)
+        pops, pw = export(6)
+        bops, bw = export(4)
+        dx = np.array([[desc[b].dx[a] for a in range(3)] for b in blocks])
     for w in range(nw):
         apply_cell_program(W, cops[cw[w]:cw[w + 1]], [0, cw[w + 1] - cw[w]], slot, 6)
         if Bf is not None:
