@@ -173,6 +173,52 @@ def shard_export(cfg: FxConfig, desc, owner, nranks: int, rank: int, which: int)
     return ops[: nops.value], waves
 
 
+class ShardGroup:
+    """Ranks of a sharded mesh emulated inside one process
+    (fx_shard_group_create): one context per rank, each driven from its own
+    host thread; every rank makes the same calls in the same order."""
+
+    def __init__(self, nranks: int):
+        self.L = library()
+        self._g = self.L.fx_shard_group_create(int(nranks))
+        if not self._g:
+            raise FxError(1, "fx_shard_group_create: nranks outside [1, 16]")
+        self.nranks = int(nranks)
+
+    def close(self) -> None:
+        if self._g:
+            self.L.fx_shard_group_destroy(self._g)
+            self._g = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def nccl_unique_id() -> bytes:
+    """fx_nccl_unique_id: the 128-byte id rank 0 shares with the other
+    ranks before fx_shard_attach_nccl."""
+    buf = (C.c_ubyte * 128)()
+    rc = library().fx_nccl_unique_id(buf)
+    if rc != 0:
+        raise FxError(rc, "fx_nccl_unique_id failed (libnccl.so.2 not loadable?)")
+    return bytes(buf)
+
+
+def morton_owner(desc, nranks: int) -> np.ndarray:
+    """owner[b] for fx_shard_set_mesh: the active blocks in mesh order (the
+    reference's Morton order) cut into nranks contiguous runs of equal size,
+    the unweighted form of prj_mpi_decompose (src/prj_mpi.c:375-470);
+    inactive entries get -1."""
+    active = [b for b in range(len(desc)) if desc[b].active == 1]
+    owner = np.full(len(desc), -1, np.int32)
+    for q, b in enumerate(active):
+        owner[b] = q * nranks // len(active)
+    return owner
+
+
 class Context:
     """One device context (fx_ctx) with a mesh mirror."""
 
@@ -221,6 +267,29 @@ class Context:
     def set_mesh(self, desc) -> None:
         self._check(self.L.fx_set_mesh(self._h, len(desc), desc))
         self.nblocks = len(desc)
+
+    def shard_set_mesh(self, desc, owner, nranks: int, rank: int) -> None:
+        """fx_shard_set_mesh: this context becomes rank `rank` of the mesh;
+        blocks are then addressed by their mesh index (owned ones only)."""
+        own = np.ascontiguousarray(owner, dtype=np.int32)
+        self._check(self.L.fx_shard_set_mesh(self._h, len(desc), desc, own.ctypes.data_as(C.POINTER(C.c_int32)),
+                                             int(nranks), int(rank)))
+        self.nblocks = len(desc)
+        self._group = None
+
+    def attach_group(self, group: "ShardGroup") -> None:
+        self._check(self.L.fx_shard_attach_group(self._h, group._g))
+        self._group = group  # the group outlives the context's use of it
+
+    def attach_nccl(self, uid: bytes) -> None:
+        buf = (C.c_ubyte * 128).from_buffer_copy(uid)
+        self._check(self.L.fx_shard_attach_nccl(self._h, buf))
+
+    def shard_info(self):
+        """(owned blocks, local blocks incl. halo, doubles sent per step)"""
+        a, b, n = C.c_int(0), C.c_int(0), C.c_longlong(0)
+        self._check(self.L.fx_shard_info(self._h, C.byref(a), C.byref(b), C.byref(n)))
+        return a.value, b.value, n.value
 
     def upload_block(self, b: int, W: np.ndarray, Bf=None, grav=None) -> None:
         W = np.ascontiguousarray(W, dtype=np.float64)

@@ -106,7 +106,9 @@ EXPORTS = [
     "fx_autotune", "fx_calc_dt_noalloc", "fx_face_eval_host", "fx_face_vjp_host",
     "fx_adjoint_forward", "fx_adjoint_backward", "fx_adjoint_time", "fx_set_flux_shape",
     "fx_amr_configure", "fx_amr_tag", "fx_amr_adapt", "fx_get_mesh", "fx_amr_energy_injected",
-    "fx_amr_remesh_host", "fx_amr_timings", "fx_shard_export",
+    "fx_amr_remesh_host", "fx_amr_timings", "fx_shard_export", "fx_shard_set_mesh",
+    "fx_shard_group_create", "fx_shard_group_destroy", "fx_shard_attach_group", "fx_nccl_unique_id",
+    "fx_shard_attach_nccl", "fx_shard_info",
 ]
 PHASE_FLUX, PHASE_EMF, PHASE_CT, PHASE_CELLS, PHASE_GHOST, PHASE_STEP = range(6)
 
@@ -152,6 +154,15 @@ def load() -> C.CDLL:
                                  ip, C.POINTER(C.c_int), ip, C.POINTER(C.c_int)]
     L.fx_shard_export.argtypes = [C.POINTER(FxConfig), C.c_int, C.POINTER(FxBlockDesc), ip, C.c_int,
                                   C.c_int, C.c_int, ip, C.POINTER(C.c_int), ip, C.POINTER(C.c_int)]
+    L.fx_shard_set_mesh.argtypes = [vp, C.c_int, C.POINTER(FxBlockDesc), ip, C.c_int, C.c_int]
+    L.fx_shard_group_create.argtypes = [C.c_int]
+    L.fx_shard_group_create.restype = vp
+    L.fx_shard_group_destroy.argtypes = [vp]
+    L.fx_shard_group_destroy.restype = None
+    L.fx_shard_attach_group.argtypes = [vp, vp]
+    L.fx_nccl_unique_id.argtypes = [C.POINTER(C.c_ubyte)]
+    L.fx_shard_attach_nccl.argtypes = [vp, C.POINTER(C.c_ubyte)]
+    L.fx_shard_info.argtypes = [vp, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_longlong)]
     L.fx_time_phase.argtypes = [vp, C.c_int, C.c_int, C.c_double, dp]
     L.fx_info.argtypes = [vp, C.c_int, C.POINTER(C.c_longlong)]
     L.fx_autotune.argtypes = [vp, dp, C.c_int, C.POINTER(C.c_int)]

@@ -23,7 +23,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-std=c++17", "--fmad=false", "-lineinfo", "-Xcompiler", "-fPIC",
               "-Xcompiler", "-O2", "--expt-relaxed-constexpr"]
 SOURCES = ["fx_kernels.cu", "fx_runtime.cu", "fx_plan.cpp", "fx_noalloc.cu", "fx_adjoint.cu", "fx_amr.cu",
-           "fx_amr_host.cpp"]
+           "fx_amr_host.cpp", "fx_transport.cpp"]
 
 
 def nvcc() -> str:
@@ -60,7 +60,7 @@ def build(verbose: bool = False, ptxas_info: bool = False) -> str:
             print(" ".join(cmd))
         subprocess.run(cmd, check=True)
     if _stale(LIB, objs):
-        cmd = [nvcc()] + ARCH + ["-shared", "-o", LIB] + objs + ["-lcudart"]
+        cmd = [nvcc()] + ARCH + ["-shared", "-o", LIB] + objs + ["-lcudart", "-ldl"]
         if verbose:
             print(" ".join(cmd))
         subprocess.run(cmd, check=True)

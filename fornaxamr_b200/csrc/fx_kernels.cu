@@ -946,6 +946,42 @@ __global__ void __launch_bounds__(256) k_ghost_wave(FxDev D, const FxGop *__rest
     if (t < nb) fx_ghost_b_op(D, bops[t], slot);
 }
 
+/* exchanges of a sharded mesh: one thread per listed element */
+__device__ __forceinline__ double *fx_xelem(const FxDev &D, const FxXent &x, int slot, int q)
+{
+    switch (x.kind) {
+    case 0:
+        return D.W + (size_t)x.block * FX_W_COUNT(D.nv) + (size_t)slot * FX_NCELLS + (size_t)q * kPlane + x.idx;
+    case 1: {
+        const int dir = x.idx / FX_NFACES;
+        return D.Bf + (size_t)x.block * FX_BF_COUNT + ((size_t)dir * FX_NSTAGES + slot) * FX_NFACES +
+            (x.idx - dir * FX_NFACES);
+    }
+    case 2:
+        return D.flux + (size_t)x.block * FX_FLUX_COUNT(D.nv) + x.idx + (size_t)q * FX_AOSOA_W;
+    default:
+        return D.emf + (size_t)x.block * FX_EMF_COUNT + x.idx;
+    }
+}
+
+__device__ __forceinline__ int fx_xwidth(int kind) { return kind == 0 || kind == 2 ? 6 : 1; }
+
+__global__ void k_xpack(FxDev D, const FxXent *__restrict__ ents, int n, double *__restrict__ buf, int slot)
+{
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    const FxXent x = ents[t];
+    for (int q = 0; q < fx_xwidth(x.kind); ++q) buf[x.off + q] = *fx_xelem(D, x, slot, q);
+}
+
+__global__ void k_xunpack(FxDev D, const FxXent *__restrict__ ents, int n, const double *__restrict__ buf, int slot)
+{
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    const FxXent x = ents[t];
+    for (int q = 0; q < fx_xwidth(x.kind); ++q) *fx_xelem(D, x, slot, q) = buf[x.off + q];
+}
+
 /* coarse/fine corrections */
 __global__ void k_flux_correct(FxDev D, const FxCorr *__restrict__ recs, int n, int ncomp)
 {
@@ -1220,6 +1256,16 @@ void fx_launch_ghost_wave(const FxDev &D, const FxGop *cops, int nc, const FxGop
     if (np > 0) {
         k_ghost_groups<<<fx_blocks(np, 128), 128, 0, s>>>(D, pops, np, slot);
     }
+}
+
+void fx_launch_xpack(const FxDev &D, const FxXent *ents, int n, double *buf, int slot, cudaStream_t s)
+{
+    if (n > 0) k_xpack<<<fx_blocks(n, 256), 256, 0, s>>>(D, ents, n, buf, slot);
+}
+
+void fx_launch_xunpack(const FxDev &D, const FxXent *ents, int n, const double *buf, int slot, cudaStream_t s)
+{
+    if (n > 0) k_xunpack<<<fx_blocks(n, 256), 256, 0, s>>>(D, ents, n, buf, slot);
 }
 
 void fx_launch_prolong_groups(const FxDev &D, const FxPop *pops, int np, int slot, cudaStream_t s)

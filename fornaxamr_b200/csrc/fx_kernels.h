@@ -132,6 +132,18 @@ struct FxCorr {
     int32_t pad;
 };
 
+/* one element of a packed exchange between ranks of a sharded mesh: kind 0
+ * a cell (the 6 ghost-filled primitives of W slot `slot`, idx the cell), 1 a
+ * face (Bf slot `slot`, idx = dir * 8400 + face), 2 a flux entry (the 6
+ * components the batched face kernel stores, idx their component-0 entry),
+ * 3 an EMF entry; off: its first double in the message buffer */
+struct FxXent {
+    int32_t block;
+    int32_t idx;
+    int32_t kind;
+    int32_t off;
+};
+
 #define FX_CELL_KEY(b, c) (((b) << 13) | (c))
 #define FX_CELL_BLOCK(key) ((key) >> 13)
 #define FX_CELL_IDX(key) ((key) & 8191)
@@ -164,6 +176,9 @@ void fx_launch_calc_dt(const FxDev &D, const int *blist, int nlist, int wslot, d
  * and cell-field ops) */
 void fx_launch_ghost_wave(const FxDev &D, const FxGop *cops, int nc, const FxGop *fops, int nf,
     const FxPop *pops, int np, const FxBop *bops, int nb, int slot, int nvg, cudaStream_t s);
+/* gather the listed elements into buf / scatter buf into them */
+void fx_launch_xpack(const FxDev &D, const FxXent *ents, int n, double *buf, int slot, cudaStream_t s);
+void fx_launch_xunpack(const FxDev &D, const FxXent *ents, int n, const double *buf, int slot, cudaStream_t s);
 /* one wave of correction records; ncomp flux components per record */
 void fx_launch_flux_correct(const FxDev &D, const FxCorr *recs, int n, int ncomp, cudaStream_t s);
 void fx_launch_emf_correct(const FxDev &D, const FxCorr *recs, int n, cudaStream_t s);

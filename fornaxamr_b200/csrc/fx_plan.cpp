@@ -1825,6 +1825,11 @@ private:
                 sh.recv[k].begin.push_back((int)sh.recv[k].el.size());
             }
         }
+        for (int r = 0; r < nranks_; ++r) {
+            for (Elem e : ginit_[r]) sh.any[e < (Elem)ncell_ ? FX_X_CELLS : FX_X_FACES] = true;
+            sh.any[FX_X_FLUX] = sh.any[FX_X_FLUX] || !finit_[r].empty();
+            sh.any[FX_X_EMF] = sh.any[FX_X_EMF] || !einit_[r].empty();
+        }
     }
 
     const fx_config &cfg_;

@@ -65,6 +65,7 @@ struct FxShard {
     std::vector<int> local_to_global;
     FxXlist send[FX_X_KINDS];
     FxXlist recv[FX_X_KINDS];
+    bool any[FX_X_KINDS] = {false, false, false, false}; /* some pair of ranks exchanges kind k */
 };
 
 struct FxPlan {

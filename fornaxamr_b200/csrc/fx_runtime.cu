@@ -28,6 +28,18 @@
 #include "fx_physics.cuh"
 #include "fx_amr.h"
 #include "fx_plan.h"
+#include "fx_transport.h"
+
+/* one exchange of a sharded step on the device: the packed elements of all
+ * peers (per-peer offsets in doubles) and the message buffers */
+struct FxXdev {
+    FxXent *d_send = nullptr, *d_recv = nullptr;
+    int nsend = 0, nrecv = 0;
+    double *sbuf = nullptr, *rbuf = nullptr;
+    std::vector<size_t> soff, roff;
+    bool any = false; /* some pair of ranks exchanges: every rank takes part */
+};
+enum { FX_XG = 0, FX_XF = 1, FX_XE = 2 }; /* ghost fill (cells + faces), flux, EMF */
 
 struct fx_ctx {
     int device = 0;
@@ -86,6 +98,16 @@ struct fx_ctx {
     fx_amr_config amr{};
     double E_injected = 0.0;          /* eos->E_injected of the remesh floors */
     double amr_ms[6] = {0, 0, 0, 0, 0, 0}; /* host wall time of the phases of the last adapt */
+
+    /* sharding: this context holds rank `rank`'s owned blocks (local ids
+     * [0, nowned)) and its halo; g2l maps the mesh's block ids */
+    int nranks = 1;
+    int rank = 0;
+    int nowned = 0;
+    std::vector<int> g2l;
+    FxXdev X[3];
+    FxTransport *transport = nullptr;
+    std::string xerr;                 /* first transport failure */
 };
 
 namespace {
@@ -153,6 +175,7 @@ int sync_and_check(fx_ctx *c)
 {
     FX_CUDA(c, cudaGetLastError()); /* launch failures (configuration, resources) */
     FX_CUDA(c, cudaStreamSynchronize(c->stream));
+    if (!c->xerr.empty()) return set_err(c, FX_ECOMM, "%s", c->xerr.c_str());
     return check_device_error(c);
 }
 
@@ -242,9 +265,35 @@ void free_mesh(fx_ctx *c)
     c->nblocks = 0;
     c->nactive = 0;
     c->cap = 0;
+    for (FxXdev &x : c->X) {
+        cudaFree(x.d_send);
+        cudaFree(x.d_recv);
+        cudaFree(x.sbuf);
+        cudaFree(x.rbuf);
+        x = FxXdev();
+    }
+    c->nranks = 1;
+    c->rank = 0;
+    c->nowned = 0;
+    c->g2l.clear();
 }
 
 bool has_mesh(const fx_ctx *c) { return c && c->nblocks > 0 && c->d_W; }
+
+/* a block index of the caller (the mesh's numbering) -> this context's;
+ * a sharded context serves the blocks its rank owns */
+int local_block(fx_ctx *c, int *b)
+{
+    if (c->nranks == 1) {
+        if (*b < 0 || *b >= c->nblocks) return set_err(c, FX_EINVAL, "block %d out of range", *b);
+        return FX_SUCCESS;
+    }
+    if (*b < 0 || *b >= (int)c->g2l.size() || c->g2l[*b] < 0 || c->g2l[*b] >= c->nowned) {
+        return set_err(c, FX_EINVAL, "block %d is not owned by rank %d", *b, c->rank);
+    }
+    *b = c->g2l[*b];
+    return FX_SUCCESS;
+}
 
 /* ---- phase sequencing ------------------------------------------------------ */
 
@@ -294,6 +343,35 @@ void emf_correct(fx_ctx *c, cudaStream_t s)
     }
 }
 
+/* exchange k of a sharded step: pack, move, unpack (slot: the W / Bf stage
+ * slot of a ghost-fill exchange) */
+void shard_exchange(fx_ctx *c, int k, int slot)
+{
+    FxXdev &x = c->X[k];
+    if (c->nranks == 1 || !x.any || !c->xerr.empty()) return;
+    if (!c->transport) {
+        c->xerr = "sharded mesh without a transport (fx_shard_attach_group / fx_shard_attach_nccl)";
+        return;
+    }
+    fx_launch_xpack(c->D, x.d_send, x.nsend, x.sbuf, slot, c->stream);
+    if (c->transport->exchange(k, x.sbuf, x.soff.data(), x.rbuf, x.roff.data(), c->stream)) {
+        c->xerr = c->transport->err;
+        return;
+    }
+    fx_launch_xunpack(c->D, x.d_recv, x.nrecv, x.rbuf, slot, c->stream);
+}
+
+/* minimum of the dt keys (first..first + count) over the ranks */
+void shard_min(fx_ctx *c, int first, int count)
+{
+    if (c->nranks == 1 || !c->xerr.empty()) return;
+    if (!c->transport) {
+        c->xerr = "sharded mesh without a transport (fx_shard_attach_group / fx_shard_attach_nccl)";
+        return;
+    }
+    if (c->transport->min_u64(c->d_red + first, count, c->stream)) c->xerr = c->transport->err;
+}
+
 /* one RK2 stage; dt is read from the control block */
 void stage_seq(fx_ctx *c, int form, int stage)
 {
@@ -302,9 +380,11 @@ void stage_seq(fx_ctx *c, int form, int stage)
     cudaStream_t s = c->stream;
     const int full = form == FX_FORM_PLAIN ? 1 : 0;
     per_block(c, form, [&](const int *l, int n) { fx_launch_flux(c->D, l, n, 3, src, src, full, s); });
+    shard_exchange(c, FX_XF, src);
     flux_correct(c, full ? c->nv : 6, s);
     if (c->cfg.mhd) {
         per_block(c, form, [&](const int *l, int n) { fx_launch_emf(c->D, l, n, src, src, s); });
+        shard_exchange(c, FX_XE, src);
         emf_correct(c, s);
         per_block(c, form, [&](const int *l, int n) { fx_launch_bf_update(c->D, l, n, stage, s); });
     }
@@ -314,6 +394,7 @@ void stage_seq(fx_ctx *c, int form, int stage)
     if (form == FX_FORM_PLAIN) {
         per_block(c, form, [&](const int *l, int n) { fx_launch_eos_fill(c->D, l, n, dst, 1, s); });
     }
+    shard_exchange(c, FX_XG, dst);
     ghost_fill(c, dst);
     if (form == FX_FORM_PLAIN) {
         per_block(c, form, [&](const int *l, int n) { fx_launch_eos_fill(c->D, l, n, dst, 0, s); });
@@ -407,6 +488,22 @@ int build_step_graph(fx_ctx *c)
     return FX_SUCCESS;
 }
 
+/* one batched driver step: calc_dt, dt selection, the step, dt_src clamp;
+ * sharded, the dt and dt_src keys are minimised over the ranks */
+void run_seq(fx_ctx *c, double cfl)
+{
+    fx_launch_reset_reductions(c->D, 1, c->stream);
+    fx_launch_calc_dt(c->D, c->d_active, c->nactive, 0, cfl, c->stream);
+    shard_min(c, 0, 1);
+    fx_launch_step_begin(c->D, c->stream);
+    step_seq(c, FX_FORM_BATCHED);
+    shard_min(c, 1, 1);
+    fx_launch_step_end(c->D, c->stream);
+}
+
+/* a sharded context whose transport cannot be captured runs eagerly */
+bool eager(const fx_ctx *c) { return c->nranks > 1 && (!c->transport || !c->transport->capturable()); }
+
 int build_run_graph(fx_ctx *c, double cfl)
 {
     if (c->g_run) {
@@ -414,11 +511,7 @@ int build_run_graph(fx_ctx *c, double cfl)
     }
     cudaGraph_t g;
     FX_CUDA(c, cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
-    fx_launch_reset_reductions(c->D, 1, c->stream);
-    fx_launch_calc_dt(c->D, c->d_active, c->nactive, 0, cfl, c->stream);
-    fx_launch_step_begin(c->D, c->stream);
-    step_seq(c, FX_FORM_BATCHED);
-    fx_launch_step_end(c->D, c->stream);
+    run_seq(c, cfl);
     FX_CUDA(c, cudaStreamEndCapture(c->stream, &g));
     cudaError_t e = cudaGraphInstantiate(&c->g_run, g, 0);
     cudaGraphDestroy(g);
@@ -869,6 +962,8 @@ void fx_destroy(fx_ctx *c)
         cudaStreamSynchronize(c->stream);
     }
     free_mesh(c);
+    delete c->transport;
+    c->transport = nullptr;
     cudaFree(c->d_err);
     cudaFree(c->d_red);
     cudaFree(c->d_ctl);
@@ -927,6 +1022,135 @@ int fx_set_mesh(fx_ctx *c, int nblocks, const fx_block_desc *blocks)
     if ((rc = alloc_block_arrays(c, nblocks, 0))) return rc;
     if ((rc = install_tables(c))) return rc;
     c->last_slot = 0;
+    return FX_SUCCESS;
+}
+
+int fx_shard_set_mesh(fx_ctx *c, int nblocks, const fx_block_desc *blocks, const int *owner, int nranks,
+    int rank)
+{
+    if (!c || nblocks <= 0 || !blocks || !owner) {
+        return c ? set_err(c, FX_EINVAL, "fx_shard_set_mesh: empty mesh") : FX_EINVAL;
+    }
+    if (c->cfg.integrator != FX_INT_RK2) {
+        return set_err(c, FX_EINVAL, "fx_shard_set_mesh: sharded meshes run the RK2 integrator");
+    }
+    FX_CUDA(c, cudaSetDevice(c->device));
+    FX_CUDA(c, cudaStreamSynchronize(c->stream));
+    free_mesh(c);
+    delete c->transport;
+    c->transport = nullptr;
+    c->xerr.clear();
+    std::string perr;
+    FxPlan plan;
+    if (!fx_build_shard_plan(c->cfg, nblocks, blocks, owner, nranks, rank, plan, &perr)) {
+        return set_err(c, FX_EINVAL, "fx_shard_set_mesh: %s", perr.c_str());
+    }
+    const FxShard &sh = plan.shard;
+    const int nl = (int)sh.local_to_global.size();
+    if (nl >= (1 << 16)) return set_err(c, FX_EINVAL, "fx_shard_set_mesh: at most 65535 blocks per device");
+    c->blocks.resize(nl);
+    for (int l = 0; l < nl; ++l) c->blocks[l] = blocks[sh.local_to_global[l]];
+    c->nblocks = nl;
+    c->nactive = (int)plan.active.size();
+    int rc;
+    if ((rc = alloc_block_arrays(c, nl, 0))) return rc;
+    c->plan = std::move(plan);
+    if ((rc = install_tables(c))) return rc;
+    c->last_slot = 0;
+    /* packed exchanges: ghost fill = cells (6 primitives) then faces, per
+     * peer; flux entries (6 components); EMF entries */
+    const FxShard &s2 = c->plan.shard;
+    const int kinds[3][2] = {{FX_X_CELLS, FX_X_FACES}, {FX_X_FLUX, -1}, {FX_X_EMF, -1}};
+    for (int x = 0; x < 3; ++x) {
+        FxXdev &X = c->X[x];
+        for (int dirn = 0; dirn < 2; ++dirn) {
+            const FxXlist *lists = dirn == 0 ? s2.send : s2.recv;
+            std::vector<FxXent> ents;
+            std::vector<size_t> off(1, 0);
+            size_t pos = 0;
+            for (int p = 0; p < nranks; ++p) {
+                for (int q = 0; q < 2; ++q) {
+                    const int k = kinds[x][q];
+                    if (k < 0) continue;
+                    const int width = (k == FX_X_CELLS || k == FX_X_FLUX) ? 6 : 1;
+                    const FxXlist &l = lists[k];
+                    for (int e = l.begin[p]; e < l.begin[p + 1]; ++e) {
+                        ents.push_back({l.el[e].block, l.el[e].idx, k, (int32_t)pos});
+                        pos += width;
+                    }
+                }
+                off.push_back(pos);
+            }
+            if (pos >= (size_t)1 << 31) return set_err(c, FX_ETOOBIG, "fx_shard_set_mesh: exchange too large");
+            FxXent **d = dirn == 0 ? &X.d_send : &X.d_recv;
+            double **buf = dirn == 0 ? &X.sbuf : &X.rbuf;
+            if ((rc = dev_alloc(c, d, ents.size()))) return rc;
+            if ((rc = dev_alloc(c, buf, pos))) return rc;
+            if (!ents.empty()) {
+                FX_CUDA(c, cudaMemcpy(*d, ents.data(), ents.size() * sizeof(FxXent), cudaMemcpyHostToDevice));
+            }
+            (dirn == 0 ? X.nsend : X.nrecv) = (int)ents.size();
+            (dirn == 0 ? X.soff : X.roff) = off;
+        }
+        X.any = s2.any[kinds[x][0]] || (kinds[x][1] >= 0 && s2.any[kinds[x][1]]);
+    }
+    c->nranks = nranks;
+    c->rank = rank;
+    c->nowned = s2.nowned;
+    c->g2l.assign(nblocks, -1);
+    for (int l = 0; l < nl; ++l) c->g2l[s2.local_to_global[l]] = l;
+    return FX_SUCCESS;
+}
+
+int fx_shard_attach_group(fx_ctx *c, fx_shard_group *g)
+{
+    if (!c || !g) return c ? set_err(c, FX_EINVAL, "fx_shard_attach_group: null group") : FX_EINVAL;
+    if (c->nranks == 1 || fx_group_size(g) != c->nranks) {
+        return set_err(c, FX_EINVAL, "fx_shard_attach_group: the group size must equal the mesh's rank count");
+    }
+    delete c->transport;
+    c->transport = fx_transport_group(g, c->rank);
+    free_graphs(c);
+    return FX_SUCCESS;
+}
+
+int fx_shard_attach_nccl(fx_ctx *c, const unsigned char id[128])
+{
+    if (!c || !id) return c ? set_err(c, FX_EINVAL, "fx_shard_attach_nccl: null id") : FX_EINVAL;
+    if (c->nranks == 1 && !c->nblocks) return set_err(c, FX_ENOMESH, "fx_shard_attach_nccl: no sharded mesh");
+    std::string err;
+    FxTransport *t = fx_transport_nccl(c->nranks, c->rank, id, c->device, &err);
+    if (!t) return set_err(c, FX_ECOMM, "fx_shard_attach_nccl: %s", err.c_str());
+    delete c->transport;
+    c->transport = t;
+    free_graphs(c);
+    return FX_SUCCESS;
+}
+
+int fx_nccl_unique_id(unsigned char id[128])
+{
+    if (!id) return FX_EINVAL;
+    std::string err;
+    return fx_transport_nccl_id(id, &err) ? FX_ECOMM : FX_SUCCESS;
+}
+
+fx_shard_group *fx_shard_group_create(int nranks) { return fx_group_new(nranks); }
+
+void fx_shard_group_destroy(fx_shard_group *g) { fx_group_delete(g); }
+
+int fx_shard_info(fx_ctx *c, int *nowned, int *nlocal, long long *doubles_per_step)
+{
+    if (!has_mesh(c)) return c ? set_err(c, FX_ENOMESH, "no mesh") : FX_EINVAL;
+    if (nowned) *nowned = c->nranks > 1 ? c->nowned : c->nactive;
+    if (nlocal) *nlocal = c->nblocks;
+    if (doubles_per_step) {
+        /* sent per RK2 step: two stages, each with every exchange */
+        long long n = 0;
+        for (const FxXdev &x : c->X) {
+            if (x.any && !x.soff.empty()) n += (long long)x.soff.back();
+        }
+        *doubles_per_step = 2 * n;
+    }
     return FX_SUCCESS;
 }
 
@@ -1036,8 +1260,8 @@ int fx_upload_block(fx_ctx *c, int b, const double *W, const double *const Bf[3]
     const double *const grav[3])
 {
     if (!has_mesh(c)) return c ? set_err(c, FX_ENOMESH, "no mesh") : FX_EINVAL;
-    if (b < 0 || b >= c->nblocks) return set_err(c, FX_EINVAL, "block %d out of range", b);
     int rc;
+    if ((rc = local_block(c, &b))) return rc;
     if (W && (rc = xfer_w(c, b, 1, const_cast<double *>(W), cudaMemcpyHostToDevice, false))) return rc;
     if (Bf && c->cfg.mhd) {
         for (int d = 0; d < 3; ++d) {
@@ -1059,8 +1283,8 @@ int fx_upload_block(fx_ctx *c, int b, const double *W, const double *const Bf[3]
 int fx_download_block(fx_ctx *c, int b, double *W, double *eosvar, double *const Bf[3])
 {
     if (!has_mesh(c)) return c ? set_err(c, FX_ENOMESH, "no mesh") : FX_EINVAL;
-    if (b < 0 || b >= c->nblocks) return set_err(c, FX_EINVAL, "block %d out of range", b);
     int rc;
+    if ((rc = local_block(c, &b))) return rc;
     if (W && (rc = xfer_w(c, b, 1, W, cudaMemcpyDeviceToHost, false))) return rc;
     if (eosvar) {
         fx_launch_eos_fill(c->D, c->d_ids + b, 1, c->last_slot, 0, c->stream);
@@ -1077,6 +1301,7 @@ int fx_download_block(fx_ctx *c, int b, double *W, double *eosvar, double *const
 
 int fx_upload_all(fx_ctx *c, const double *W_all, const double *Bf_all)
 {
+    if (c && c->nranks > 1) return set_err(c, FX_EINVAL, "%s: not available on a sharded mesh", __func__);
     if (!has_mesh(c)) return c ? set_err(c, FX_ENOMESH, "no mesh") : FX_EINVAL;
     int rc;
     if (W_all && (rc = xfer_w(c, 0, c->nblocks, const_cast<double *>(W_all), cudaMemcpyHostToDevice, false))) return rc;
@@ -1087,6 +1312,7 @@ int fx_upload_all(fx_ctx *c, const double *W_all, const double *Bf_all)
 
 int fx_download_all(fx_ctx *c, double *W_all, double *Bf_all)
 {
+    if (c && c->nranks > 1) return set_err(c, FX_EINVAL, "%s: not available on a sharded mesh", __func__);
     if (!has_mesh(c)) return c ? set_err(c, FX_ENOMESH, "no mesh") : FX_EINVAL;
     int rc;
     if (W_all && (rc = xfer_w(c, 0, c->nblocks, W_all, cudaMemcpyDeviceToHost, false))) return rc;
@@ -1096,6 +1322,7 @@ int fx_download_all(fx_ctx *c, double *W_all, double *Bf_all)
 
 int fx_upload_state(fx_ctx *c, const double *W_all, const double *Bf_all)
 {
+    if (c && c->nranks > 1) return set_err(c, FX_EINVAL, "%s: not available on a sharded mesh", __func__);
     if (!has_mesh(c)) return c ? set_err(c, FX_ENOMESH, "no mesh") : FX_EINVAL;
     int rc;
     if (W_all && (rc = xfer_w(c, 0, c->nblocks, const_cast<double *>(W_all), cudaMemcpyHostToDevice, true))) return rc;
@@ -1106,6 +1333,7 @@ int fx_upload_state(fx_ctx *c, const double *W_all, const double *Bf_all)
 
 int fx_download_state(fx_ctx *c, double *W_all, double *Bf_all)
 {
+    if (c && c->nranks > 1) return set_err(c, FX_EINVAL, "%s: not available on a sharded mesh", __func__);
     if (!has_mesh(c)) return c ? set_err(c, FX_ENOMESH, "no mesh") : FX_EINVAL;
     int rc;
     if (W_all && (rc = xfer_w(c, 0, c->nblocks, W_all, cudaMemcpyDeviceToHost, true))) return rc;
@@ -1115,6 +1343,7 @@ int fx_download_state(fx_ctx *c, double *W_all, double *Bf_all)
 
 int fx_download_array(fx_ctx *c, int b, int which, int dir, double *out)
 {
+    if (c && c->nranks > 1) return set_err(c, FX_EINVAL, "%s: not available on a sharded mesh", __func__);
     if (!has_mesh(c)) return c ? set_err(c, FX_ENOMESH, "no mesh") : FX_EINVAL;
     if (b < 0 || b >= c->nblocks || dir < 0 || dir > 2 || !out) {
         return set_err(c, FX_EINVAL, "fx_download_array: bad arguments");
@@ -1170,6 +1399,7 @@ static int check_block(fx_ctx *c, int b)
 
 int fx_flux_update(fx_ctx *c, int b, int w_slot, int use_bf1)
 {
+    if (c && c->nranks > 1) return set_err(c, FX_EINVAL, "%s: not available on a sharded mesh", __func__);
     int rc = check_block(c, b);
     if (rc) return rc;
     if (w_slot < 0 || w_slot > 1 || use_bf1 < 0 || use_bf1 > 1) return set_err(c, FX_EINVAL, "bad slot");
@@ -1180,6 +1410,7 @@ int fx_flux_update(fx_ctx *c, int b, int w_slot, int use_bf1)
 
 int fx_mhd_update_emf(fx_ctx *c, int b, int stage)
 {
+    if (c && c->nranks > 1) return set_err(c, FX_EINVAL, "%s: not available on a sharded mesh", __func__);
     int rc = check_block(c, b);
     if (rc) return rc;
     if (!c->cfg.mhd || stage < 0 || stage > 1) return set_err(c, FX_EINVAL, "bad emf call");
@@ -1190,6 +1421,7 @@ int fx_mhd_update_emf(fx_ctx *c, int b, int stage)
 
 int fx_mhd_update_bf(fx_ctx *c, int b, int stage, double dt)
 {
+    if (c && c->nranks > 1) return set_err(c, FX_EINVAL, "%s: not available on a sharded mesh", __func__);
     int rc = check_block(c, b);
     if (rc) return rc;
     if (!c->cfg.mhd || (stage != 1 && stage != 2)) return set_err(c, FX_EINVAL, "bad bf update call");
@@ -1200,6 +1432,7 @@ int fx_mhd_update_bf(fx_ctx *c, int b, int stage, double dt)
 
 int fx_update_cells(fx_ctx *c, int b, int stage, double dt, double *dt_src)
 {
+    if (c && c->nranks > 1) return set_err(c, FX_EINVAL, "%s: not available on a sharded mesh", __func__);
     int rc = check_block(c, b);
     if (rc) return rc;
     if (stage != 1 && stage != 2) return set_err(c, FX_EINVAL, "bad stage");
@@ -1218,6 +1451,7 @@ int fx_update_cells(fx_ctx *c, int b, int stage, double dt, double *dt_src)
 
 int fx_riemann_flux_send(fx_ctx *c)
 {
+    if (c && c->nranks > 1) return set_err(c, FX_EINVAL, "%s: not available on a sharded mesh", __func__);
     if (!has_mesh(c)) return c ? set_err(c, FX_ENOMESH, "no mesh") : FX_EINVAL;
     fx_launch_set_dt(c->D, 0.0, c->stream);
     flux_correct(c, c->nv, c->stream);
@@ -1226,6 +1460,7 @@ int fx_riemann_flux_send(fx_ctx *c)
 
 int fx_mhd_emf_send(fx_ctx *c)
 {
+    if (c && c->nranks > 1) return set_err(c, FX_EINVAL, "%s: not available on a sharded mesh", __func__);
     if (!has_mesh(c)) return c ? set_err(c, FX_ENOMESH, "no mesh") : FX_EINVAL;
     fx_launch_set_dt(c->D, 0.0, c->stream);
     emf_correct(c, c->stream);
@@ -1234,6 +1469,7 @@ int fx_mhd_emf_send(fx_ctx *c)
 
 int fx_eos_fill_active_cells(fx_ctx *c, int stage)
 {
+    if (c && c->nranks > 1) return set_err(c, FX_EINVAL, "%s: not available on a sharded mesh", __func__);
     if (!has_mesh(c)) return c ? set_err(c, FX_ENOMESH, "no mesh") : FX_EINVAL;
     const int slot = stage > 0 ? stage - 1 : 0;
     if (slot > 1) return set_err(c, FX_EINVAL, "bad stage");
@@ -1244,6 +1480,7 @@ int fx_eos_fill_active_cells(fx_ctx *c, int stage)
 
 int fx_eos_fill_mesh(fx_ctx *c, int stage)
 {
+    if (c && c->nranks > 1) return set_err(c, FX_EINVAL, "%s: not available on a sharded mesh", __func__);
     if (!has_mesh(c)) return c ? set_err(c, FX_ENOMESH, "no mesh") : FX_EINVAL;
     const int slot = stage > 0 ? stage - 1 : 0;
     if (slot > 1) return set_err(c, FX_EINVAL, "bad stage");
@@ -1254,6 +1491,7 @@ int fx_eos_fill_mesh(fx_ctx *c, int stage)
 
 int fx_boundary_fill_ghosts_and_bf(fx_ctx *c, int stage, int use_bf1)
 {
+    if (c && c->nranks > 1) return set_err(c, FX_EINVAL, "%s: not available on a sharded mesh", __func__);
     if (!has_mesh(c)) return c ? set_err(c, FX_ENOMESH, "no mesh") : FX_EINVAL;
     const int slot = stage > 0 ? stage - 1 : 0;
     if (slot > 1 || use_bf1 < 0 || use_bf1 > 1) return set_err(c, FX_EINVAL, "bad stage");
@@ -1273,6 +1511,7 @@ int fx_calc_dt(fx_ctx *c, double cfl, double *dt)
     if (!dt) return set_err(c, FX_EINVAL, "null dt");
     fx_launch_reset_reductions(c->D, 1, c->stream);
     fx_launch_calc_dt(c->D, c->d_active, c->nactive, 0, cfl, c->stream);
+    shard_min(c, 0, 1);
     FX_CUDA(c, cudaMemcpyAsync(c->h_red, c->d_red, 2 * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
         c->stream));
     int rc = sync_and_check(c);
@@ -1283,6 +1522,9 @@ int fx_calc_dt(fx_ctx *c, double cfl, double *dt)
 
 int fx_stage(fx_ctx *c, int form, int stage, double dt, double *dt_src)
 {
+    if (c && c->nranks > 1 && form != FX_FORM_BATCHED) {
+        return set_err(c, FX_EINVAL, "%s: a sharded mesh runs the batched form", __func__);
+    }
     if (!has_mesh(c)) return c ? set_err(c, FX_ENOMESH, "no mesh") : FX_EINVAL;
     if (c->cfg.integrator != FX_INT_RK2) return set_err(c, FX_EINVAL, "fx_stage: RK2 stages only");
     if ((form != FX_FORM_PLAIN && form != FX_FORM_BATCHED) || (stage != 1 && stage != 2)) {
@@ -1291,19 +1533,23 @@ int fx_stage(fx_ctx *c, int form, int stage, double dt, double *dt_src)
     fx_launch_set_dt(c->D, dt, c->stream);
     fx_launch_reset_reductions(c->D, 2, c->stream);
     stage_seq(c, form, stage);
+    shard_min(c, 1, 1);
     if (dt_src) return read_dt_src(c, dt_src);
-    return FX_SUCCESS;
+    return c->xerr.empty() ? FX_SUCCESS : set_err(c, FX_ECOMM, "%s", c->xerr.c_str());
 }
 
 int fx_step(fx_ctx *c, int form, double dt, double *dt_src)
 {
+    if (c && c->nranks > 1 && form != FX_FORM_BATCHED) {
+        return set_err(c, FX_EINVAL, "%s: a sharded mesh runs the batched form", __func__);
+    }
     if (!has_mesh(c)) return c ? set_err(c, FX_ENOMESH, "no mesh") : FX_EINVAL;
     if (form != FX_FORM_PLAIN && form != FX_FORM_BATCHED) {
         return set_err(c, FX_EINVAL, "fx_step: bad form");
     }
     if (c->sticky) return FX_EPHYSICS;
     fx_launch_set_dt(c->D, dt, c->stream);
-    if (form == FX_FORM_PLAIN) {
+    if (form == FX_FORM_PLAIN || eager(c)) {
         fx_launch_reset_reductions(c->D, 2, c->stream);
         step_seq(c, form);
     } else {
@@ -1312,12 +1558,16 @@ int fx_step(fx_ctx *c, int form, double dt, double *dt_src)
         FX_CUDA(c, cudaGraphLaunch(c->g_step, c->stream));
         c->last_slot = 0;
     }
+    shard_min(c, 1, 1);
     if (dt_src) return read_dt_src(c, dt_src);
-    return FX_SUCCESS;
+    return c->xerr.empty() ? FX_SUCCESS : set_err(c, FX_ECOMM, "%s", c->xerr.c_str());
 }
 
 int fx_run(fx_ctx *c, int form, int nsteps, double cfl, double dt_factor, double t_end, double *state)
 {
+    if (c && c->nranks > 1 && form != FX_FORM_BATCHED) {
+        return set_err(c, FX_EINVAL, "%s: a sharded mesh runs the batched form", __func__);
+    }
     if (!has_mesh(c)) return c ? set_err(c, FX_ENOMESH, "no mesh") : FX_EINVAL;
     if (!state || nsteps < 0) return set_err(c, FX_EINVAL, "fx_run: bad arguments");
     if (form == FX_FORM_PLAIN) {
@@ -1362,10 +1612,14 @@ int fx_run(fx_ctx *c, int form, int nsteps, double cfl, double dt_factor, double
     v.dt_mult = dt_mult(c);
     *c->h_ctl = v;
     fx_launch_set_ctl(c->D, v, c->stream);
-    int rc = build_run_graph(c, cfl);
-    if (rc) return rc;
-    for (int n = 0; n < nsteps; ++n) {
-        FX_CUDA(c, cudaGraphLaunch(c->g_run, c->stream));
+    int rc;
+    if (eager(c)) {
+        for (int n = 0; n < nsteps; ++n) run_seq(c, cfl);
+    } else {
+        if ((rc = build_run_graph(c, cfl))) return rc;
+        for (int n = 0; n < nsteps; ++n) {
+            FX_CUDA(c, cudaGraphLaunch(c->g_run, c->stream));
+        }
     }
     c->last_slot = 0;
     FX_CUDA(c, cudaMemcpyAsync(c->h_ctl, c->d_ctl, sizeof(FxCtl), cudaMemcpyDeviceToHost, c->stream));
@@ -1471,6 +1725,7 @@ int fx_set_flux_shape(fx_ctx *c, int variant)
 
 int fx_amr_configure(fx_ctx *c, const fx_amr_config *amr)
 {
+    if (c && c->nranks > 1) return set_err(c, FX_EINVAL, "%s: not available on a sharded mesh", __func__);
     if (!c || !amr) return c ? set_err(c, FX_EINVAL, "fx_amr_configure: null config") : FX_EINVAL;
     std::string why;
     if (!amr_config_ok(*amr, &why)) return set_err(c, FX_EINVAL, "fx_amr_configure: %s", why.c_str());
@@ -1481,6 +1736,7 @@ int fx_amr_configure(fx_ctx *c, const fx_amr_config *amr)
 
 int fx_amr_tag(fx_ctx *c, int32_t *refine_flag)
 {
+    if (c && c->nranks > 1) return set_err(c, FX_EINVAL, "%s: not available on a sharded mesh", __func__);
     if (!has_mesh(c)) return c ? set_err(c, FX_ENOMESH, "no mesh") : FX_EINVAL;
     if (!c->amr_set) return set_err(c, FX_EINVAL, "fx_amr_tag: fx_amr_configure first");
     if (!refine_flag) return set_err(c, FX_EINVAL, "fx_amr_tag: null output");
@@ -1494,6 +1750,7 @@ int fx_amr_tag(fx_ctx *c, int32_t *refine_flag)
 
 int fx_amr_adapt(fx_ctx *c, int *changed)
 {
+    if (c && c->nranks > 1) return set_err(c, FX_EINVAL, "%s: not available on a sharded mesh", __func__);
     if (!has_mesh(c)) return c ? set_err(c, FX_ENOMESH, "no mesh") : FX_EINVAL;
     if (!c->amr_set) return set_err(c, FX_EINVAL, "fx_amr_adapt: fx_amr_configure first");
     if (changed) *changed = 0;
@@ -1922,6 +2179,7 @@ int adjoint_reverse(fx_ctx *c)
 
 int fx_adjoint_forward(fx_ctx *c, int nsteps, double dt)
 {
+    if (c && c->nranks > 1) return set_err(c, FX_EINVAL, "%s: not available on a sharded mesh", __func__);
     if (!has_mesh(c)) return c ? set_err(c, FX_ENOMESH, "no mesh") : FX_EINVAL;
     if (nsteps < 1 || !(dt > 0.0)) return set_err(c, FX_EINVAL, "fx_adjoint_forward: nsteps >= 1 and dt > 0");
     int rc = adj_supported(c);
@@ -1961,6 +2219,7 @@ int fx_adjoint_forward(fx_ctx *c, int nsteps, double dt)
 int fx_adjoint_backward(fx_ctx *c, const double *W_bar, const double *Bf_bar, double *W_bar_out,
     double *Bf_bar_out, int initial_fill)
 {
+    if (c && c->nranks > 1) return set_err(c, FX_EINVAL, "%s: not available on a sharded mesh", __func__);
     if (!has_mesh(c)) return c ? set_err(c, FX_ENOMESH, "no mesh") : FX_EINVAL;
     if (c->adj_nsteps < 1 || !c->d_ckW) return set_err(c, FX_EINVAL, "fx_adjoint_backward: no stored forward pass");
     if (!W_bar || !W_bar_out || !Bf_bar_out) return set_err(c, FX_EINVAL, "fx_adjoint_backward: null array");

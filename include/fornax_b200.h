@@ -49,6 +49,7 @@ extern "C" {
 #define FX_EPHYSICS 4   /* device-side physics failure (reference exit path) */
 #define FX_ENOMEM 5     /* device allocation failed */
 #define FX_ETOOBIG 6    /* request exceeds a fixed capacity (FX_NOALLOC_MAX_BLOCKS) */
+#define FX_ECOMM 7      /* exchange between ranks of a sharded mesh failed */
 
 /* execution forms of a step */
 #define FX_FORM_PLAIN 0    /* per-block kernel launches in the reference's loop order */
@@ -179,6 +180,41 @@ int fx_plan_export(const fx_config *cfg, int nblocks, const fx_block_desc *block
  * entries, *nwaves = nranks).  No counterpart in the reference. */
 int fx_shard_export(const fx_config *cfg, int nblocks, const fx_block_desc *blocks, const int *owner,
     int nranks, int rank, int which, int32_t *ops, int *nops, int32_t *wave_begin, int *nwaves);
+
+/* Sets rank `rank`'s part of a mesh sharded over nranks ranks (owner[b]:
+ * the rank of active block b; contiguous runs of the reference's Morton
+ * order are the natural choice): device storage for the owned blocks and
+ * the halo, the rank's programs and exchange buffers.  Afterwards
+ * fx_upload_block / fx_download_block take the mesh's block indices of
+ * owned blocks, and fx_calc_dt, fx_step and fx_run (batched form, RK2) run
+ * the rank's part of every step, exchanging with the other ranks through
+ * the attached transport: every rank must make the same calls in the same
+ * order.  The per-block drop-in calls, whole-mesh copies, dynamic AMR and
+ * the adjoint are not available on a sharded mesh.  No counterpart in the
+ * reference (its ranks are MPI processes over one prj_mesh). */
+int fx_shard_set_mesh(fx_ctx *ctx, int nblocks, const fx_block_desc *blocks, const int *owner, int nranks,
+    int rank);
+
+/* Transports.  A group emulates nranks ranks inside one process (one host
+ * thread per rank, each driving its own context, possibly on one GPU):
+ * exchanges are device-to-device copies between the contexts' buffers with
+ * host barriers (a rank that does not arrive within 120 s fails the
+ * exchange with FX_ECOMM); steps run without graphs.  NCCL runs one process
+ * per GPU: rank 0 makes the unique id (fx_nccl_unique_id), the host shares
+ * it (e.g. torch.distributed), every rank attaches; exchanges are
+ * send/recv groups and dt minima all-reduces on the context's stream, and
+ * whole steps are captured as CUDA graphs.  libnccl.so.2 is loaded when
+ * first needed. */
+typedef struct fx_shard_group fx_shard_group;
+fx_shard_group *fx_shard_group_create(int nranks);
+void fx_shard_group_destroy(fx_shard_group *group);
+int fx_shard_attach_group(fx_ctx *ctx, fx_shard_group *group);
+int fx_nccl_unique_id(unsigned char id[128]);
+int fx_shard_attach_nccl(fx_ctx *ctx, const unsigned char id[128]);
+
+/* owned blocks, local blocks (owned + halo) and the doubles this rank sends
+ * per RK2 step over all exchanges */
+int fx_shard_info(fx_ctx *ctx, int *nowned, int *nlocal, long long *doubles_per_step);
 
 /* Host <-> device copies of one block, in the reference's per-block layout:
  * W = block->W_mhd (NHYDRO * NS * 8000 doubles), Bf[d] = block->Bf[d]

@@ -13,7 +13,7 @@ HEADER = os.path.join(ROOT, "include", "fornax_b200.h")
 
 def declared():
     text = open(HEADER).read()
-    return re.findall(r"^\s*(?:int|void)\s+(fx_\w+)\s*\(", text, re.M)
+    return re.findall(r"^\s*(?:int|void|fx_shard_group\s*\*)\s*(fx_\w+)\s*\(", text, re.M)
 
 
 def test_header_declares_entry_points():
