@@ -16,9 +16,11 @@ working set (~2.7 GB) is far larger than L2, so no explicit flush is needed.
 uploads the state (W and Bf, stage slot 0) from pinned host memory, steps,
 and downloads it again.
 
-Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
-For N > 1 (torchrun) every rank runs an independent replica (the path has no
-data exchange between GPUs in this build: replicas only); `value` is the sum.
+Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference] [--shard]
+For N > 1 (torchrun) every rank runs an independent replica by default
+(`value` is the sum); with --shard the ranks share one mesh of N x 512 blocks
+(a 128^3 cube per GPU), exchanging ghost zones and dt minima over NCCL inside
+each step's CUDA graph (weak scaling with the exchanges).
 """
 from __future__ import annotations
 
@@ -63,6 +65,9 @@ def parse():
                     help="batched steps of the static-AMR blast measurement (0: skip it)")
     ap.add_argument("--collapse", action="store_true",
                     help="also measure the 4-level gravity collapse (about 4600 blocks; slow set-up)")
+    ap.add_argument("--shard", action="store_true",
+                    help="N > 1: one mesh of N x 512 blocks sharded over the ranks (NCCL exchanges of ghost "
+                         "zones and dt minima) instead of N independent replicas")
     return ap.parse_args()
 
 
@@ -462,6 +467,86 @@ def run_adjoint(args, dev):
             "ms_per_step_forward": ms_fwd, "adjoint_over_forward": ms_adj / ms_fwd}
 
 
+def run_shard(args, rank, world, local_rank):
+    """Weak scaling with exchanges: one uniform mesh of (8 N) x 8 x 8 blocks
+    (N 128^3 cubes along x, outflow boundaries), the active blocks cut into
+    N contiguous runs of the mesh order, one rank per GPU over NCCL.  Every
+    stage exchanges the ghost zones at the rank boundaries and every step
+    takes the dt minima over the ranks, inside the step's CUDA graph."""
+    import numpy as np
+    import torch
+
+    import fornaxamr_b200 as fx
+    from fornaxamr_b200 import mesh, problems
+
+    dev = local_rank
+    torch.cuda.set_device(dev)
+    coord = (0.0, float(world), 0.0, 1.0, 0.0, 1.0)
+    blocks = mesh.uniform_mesh((ROOT * world, ROOT, ROOT), coord)
+    desc = mesh.to_desc(blocks)
+    owner = fx.morton_owner(desc, world)
+    mine = [int(b) for b in np.nonzero(owner == rank)[0]]
+    W0, Bf0 = problems.fourier_mhd([blocks[b] for b in mine])
+    ctx = fx.Context(True, 5.0 / 3.0, coord, device=dev)
+    ctx.shard_set_mesh(desc, owner, world, rank)
+    uid = torch.zeros(128, dtype=torch.uint8, device=f"cuda:{dev}")
+    if world > 1:
+        if rank == 0:
+            uid.copy_(torch.frombuffer(bytearray(fx.nccl_unique_id()), dtype=torch.uint8))
+        torch.distributed.broadcast(uid, 0)
+    else:
+        uid.copy_(torch.frombuffer(bytearray(fx.nccl_unique_id()), dtype=torch.uint8))
+    ctx.attach_nccl(bytes(uid.cpu().numpy().tobytes()))
+    for n, b in enumerate(mine):
+        ctx.upload_block(b, W0[n].ravel(), [Bf0[n, d].ravel() for d in range(3)])
+    ctx.boundary_fill(1, 0)
+    ctx.sync()
+    cfl, dt_factor, t_end = 0.4, 1.2, 1.0e30
+    stream = torch.cuda.ExternalStream(ctx.stream(), device=dev)
+
+    def max_over_ranks(x):
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{dev}")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        return float(t.item())
+
+    state = ctx.run(fx.FORM_BATCHED, args.warmup, cfl, dt_factor, t_end, (0.0, 0.0, 0))
+    ctx.sync()
+    torch.cuda.synchronize(dev)
+    if world > 1:
+        torch.distributed.barrier()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    with Clocks(dev) as clk:
+        torch.cuda.synchronize(dev)
+        e0.record(stream)
+        state = ctx.run(fx.FORM_BATCHED, args.steps, cfl, dt_factor, t_end, state)
+        e1.record(stream)
+        e1.synchronize()
+        torch.cuda.synchronize(dev)
+    if world > 1:
+        torch.distributed.barrier()
+    ms_total = max_over_ranks(e0.elapsed_time(e1))
+    nown, nlocal, doubles = ctx.shard_info()
+    zones = world * ZONES
+    line = {
+        "metric": METRIC, "value": zones * args.steps / (ms_total / 1000.0), "unit": UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_total / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded Fourier-mode MHD, host-generated per rank)",
+        "config": {"workload": f"3D ideal MHD, one mesh of {ROOT * world}x{ROOT}x{ROOT} blocks of 16^3 "
+                               "(128^3 zones per GPU), MC+HLLD+CT RK2, batched form",
+                   "blocks": len(desc), "zones": zones, "parallelism": f"shard x{world} (NCCL)",
+                   "l2": "working set > 2.7 GB per GPU >> 126 MB L2 (no flush)"},
+        "shard": {"owned_blocks": nown, "halo_blocks": nlocal - nown,
+                  "bytes_sent_per_step_rank0": 8 * doubles},
+        "clocks": clk.summary(),
+    }
+    ctx.close()
+    return line
+
+
 def run_fx(args, rank, world, local_rank):
     import numpy as np
     import torch
@@ -657,6 +742,16 @@ def main():
         import torch
         torch.cuda.set_device(local_rank)
         torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    if args.shard:
+        line = run_shard(args, rank, world, local_rank)
+        line["cpu_baseline"] = cb
+        if world > 1:
+            import torch
+            torch.distributed.barrier()
+            torch.distributed.destroy_process_group()
+        if rank == 0:
+            print(json.dumps(line))
+        return 0
     line = run_fx(args, rank, world, local_rank)
     line["cpu_baseline"] = cb
     if world == 1:

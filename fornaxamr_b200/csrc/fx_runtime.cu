@@ -1491,7 +1491,6 @@ int fx_eos_fill_mesh(fx_ctx *c, int stage)
 
 int fx_boundary_fill_ghosts_and_bf(fx_ctx *c, int stage, int use_bf1)
 {
-    if (c && c->nranks > 1) return set_err(c, FX_EINVAL, "%s: not available on a sharded mesh", __func__);
     if (!has_mesh(c)) return c ? set_err(c, FX_ENOMESH, "no mesh") : FX_EINVAL;
     const int slot = stage > 0 ? stage - 1 : 0;
     if (slot > 1 || use_bf1 < 0 || use_bf1 > 1) return set_err(c, FX_EINVAL, "bad stage");
@@ -1499,6 +1498,12 @@ int fx_boundary_fill_ghosts_and_bf(fx_ctx *c, int stage, int use_bf1)
         return set_err(c, FX_EINVAL, "fx_boundary_fill_ghosts_and_bf: W slot and Bf slot must agree");
     }
     fx_launch_set_dt(c->D, 0.0, c->stream);
+    if (c->nranks > 1) {
+        /* sharded: every rank takes part (the exchange before the fill) */
+        shard_exchange(c, FX_XG, slot);
+        ghost_fill(c, slot);
+        return sync_and_check(c);
+    }
     ghost_fill(c, slot);
     return FX_SUCCESS;
 }

@@ -189,8 +189,9 @@ int fx_shard_export(const fx_config *cfg, int nblocks, const fx_block_desc *bloc
  * owned blocks, and fx_calc_dt, fx_step and fx_run (batched form, RK2) run
  * the rank's part of every step, exchanging with the other ranks through
  * the attached transport: every rank must make the same calls in the same
- * order.  The per-block drop-in calls, whole-mesh copies, dynamic AMR and
- * the adjoint are not available on a sharded mesh.  No counterpart in the
+ * order; fx_boundary_fill_ghosts_and_bf fills the ghost zones of the owned
+ * blocks (with its exchange).  The other per-block drop-in calls, whole-mesh
+ * copies, dynamic AMR and the adjoint are not available on a sharded mesh.  No counterpart in the
  * reference (its ranks are MPI processes over one prj_mesh). */
 int fx_shard_set_mesh(fx_ctx *ctx, int nblocks, const fx_block_desc *blocks, const int *owner, int nranks,
     int rank);

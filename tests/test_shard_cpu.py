@@ -33,12 +33,7 @@ def build(levels, mhd):
 
 
 def morton_owner(desc, nranks):
-    """Equal contiguous chunks of the active blocks in mesh order."""
-    active = [b for b in range(len(desc)) if desc[b].active == 1]
-    owner = np.full(len(desc), -1, np.int32)
-    for q, b in enumerate(active):
-        owner[b] = q * nranks // len(active)
-    return owner
+    return fx.morton_owner(desc, nranks)
 
 
 def seeded_state(nb, mhd, seed=5):

@@ -165,3 +165,31 @@ def test_nccl_transport_attaches_on_one_rank(ref_mhd):
     assert state == (t_ref, dt_ref, st_ref)
     assert_owned_equal([ctx], owner, ref_mhd, True)
     ctx.close()
+
+
+def test_ghost_fill_on_ranks_matches_reference(ref_mhd):
+    """fx_boundary_fill_ghosts_and_bf on a sharded mesh, from ghost zones
+    scrambled on both sides (3-level blast, 3 ranks)"""
+    p = R.params_amr_blast(root=3, radii=(0.25, 0.1))
+    ref_mhd.setup(p)
+    W, Bf = H.ref_state(ref_mhd)
+    rng = np.random.default_rng(3)
+    ghost = np.ones(H.NCELLS, bool)
+    ghost[H.active_cells()] = False
+    active = ref_mhd.mesh_arrays()[0][:, 2] == 1
+    for b in np.nonzero(active)[0]:
+        W[b][:, :, ghost] = rng.uniform(0.5, 1.5, (W.shape[1], W.shape[2], int(ghost.sum())))
+        ref_mhd.set_W(int(b), W[b].ravel())
+    ctxs, owner, group = shard_contexts(ref_mhd, p, True, 3)
+    on_all_ranks(ctxs, lambda c: c.boundary_fill(1, 0))
+    ref_mhd.fill_ghosts(1, 0)
+    W_ref, Bf_ref = H.ref_state(ref_mhd)
+    for r, ctx in enumerate(ctxs):
+        for b in np.nonzero(owner == r)[0]:
+            Wd, _, Bd = ctx.download_block(int(b))
+            assert np.array_equal(Wd.reshape(W_ref[b].shape)[:, 0], W_ref[b][:, 0]), (r, b)
+            for d in range(3):
+                assert np.array_equal(Bd[d].reshape(2, -1)[0], Bf_ref[b, d, 0]), (r, b, d)
+    for c in ctxs:
+        c.close()
+    group.close()
