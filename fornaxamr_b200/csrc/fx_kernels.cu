@@ -200,114 +200,175 @@ __global__ void __launch_bounds__(TPB, MINB) k_flux(FxDev D, const int *__restri
 /* ------------------------------------------------------------------------ */
 /* Edge EMFs                                                                 */
 /* ------------------------------------------------------------------------ */
-__device__ __forceinline__ double fx_cell_emf(const double *Wb, int dir, int c)
-{
-    const int a = (dir + 1) % 3;
-    const int bb = (dir + 2) % 3;
-    const double bA = Wb[(size_t)(FX_B1 + a) * kPlane + c];
-    const double bB = Wb[(size_t)(FX_B1 + bb) * kPlane + c];
-    const double vA = Wb[(size_t)(FX_V1 + a) * kPlane + c];
-    const double vB = Wb[(size_t)(FX_V1 + bb) * kPlane + c];
-    return bA * vB - bB * vA;
-}
+/* One CTA per (block, chunk of edge layers along i).  For each layer i the
+ * CTA first evaluates, once per cell of plane i (j, k in [-1, 16]), the
+ * three cell-centred EMF components and the artificial eta (the reference
+ * precomputes the same per-cell grids, src/prj_timeint.c:313-338 and
+ * prj_timeint_mhd_fill_eta_mask), keeping planes i - 1 and i in shared
+ * memory; then its threads sweep the layer's edges of all three directions
+ * (an edge along x at layer i reads plane i only, edges along y and z read
+ * planes i - 1 and i).  The face EMFs and normal velocities of an edge come
+ * straight from global memory (each is read by two edges, coalesced along
+ * k).  Arithmetic of prj_timeint_mhd_update_emf (src/prj_timeint.c:292-413). */
+constexpr int kEmfChunk = 6;                        /* edge layers per CTA */
+constexpr int kEmfChunks = (FX_BS + 1 + kEmfChunk - 1) / kEmfChunk;
 
-__global__ void __launch_bounds__(128) k_emf(FxDev D, const int *__restrict__ blist, int wslot, int bfslot)
+__global__ void __launch_bounds__(256) k_emf(FxDev D, const int *__restrict__ blist, int wslot, int bfslot)
 {
     if (D.ctl->skip) {
         return;
     }
+    constexpr int P2 = FX_PBS * FX_PBS;          /* cells per plane */
+    /* [plane parity][E1, E2, E3, eta][in-plane cell] */
+    __shared__ double cq[2][4][P2];
     const int b = blist[blockIdx.y];
-    constexpr int NE = FX_BS * (FX_BS + 1) * (FX_BS + 1);
-    int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= 3 * NE) {
-        return;
-    }
-    const int dir = t / NE;
-    t -= dir * NE;
-    const int x2 = dir == 2 ? FX_BS : FX_BS + 1;
-    const int x1 = dir == 1 ? FX_BS : FX_BS + 1;
-    int e[3];
-    e[2] = t % x2;
-    t /= x2;
-    e[1] = t % x1;
-    e[0] = t / x1;
-    const int up = (dir + 1) % 3;
-    const int right = (dir + 2) % 3;
-    const int su = fx_axis_stride(up);
-    const int sr = fx_axis_stride(right);
-    const int c0 = fx_lidx(e[0], e[1], e[2]);   /* cell0 = e; face0 = face1 = e */
-    const int c1 = c0 - su;                      /* cell1 = e - up */
-    const int c2 = c0 - su - sr;                 /* cell2 = e - up - right */
-    const int c3 = c0 - sr;                      /* cell3 = e - right */
+    const int l0 = blockIdx.x * kEmfChunk;
+    const int l1 = min(l0 + kEmfChunk, FX_BS + 1);
     const double *Wb = D.W + (size_t)b * FX_W_COUNT(9) + (size_t)wslot * FX_NCELLS;
-    const double *bv1r = D.bv1 + (size_t)b * FX_BV_COUNT + (size_t)right * FX_NCELLS;
-    const double *bv2u = D.bv2 + (size_t)b * FX_BV_COUNT + (size_t)up * FX_NCELLS;
-    const double *vrr = D.vr + (size_t)b * FX_VR_COUNT + (size_t)right * 3 * FX_NCELLS;
-    const double *vru = D.vr + (size_t)b * FX_VR_COUNT + (size_t)up * 3 * FX_NCELLS;
-    double f[4], c[4], vn[4];
-    /* face0 = e (right-normal), face1 = e (up-normal), face2 = e - up
-     * (right-normal), face3 = e - right (up-normal) */
-    f[0] = bv1r[c0];
-    f[1] = bv2u[c0];
-    f[2] = bv1r[c1];
-    f[3] = bv2u[c3];
-    c[0] = fx_cell_emf(Wb, dir, c0);
-    c[1] = fx_cell_emf(Wb, dir, c1);
-    c[2] = fx_cell_emf(Wb, dir, c2);
-    c[3] = fx_cell_emf(Wb, dir, c3);
-    vn[0] = vrr[fx_bidx_cell(3, right, c0)];
-    vn[1] = vru[fx_bidx_cell(3, up, c0)];
-    vn[2] = vrr[fx_bidx_cell(3, right, c1)];
-    vn[3] = vru[fx_bidx_cell(3, up, c3)];
-    const int eidx = fx_edge_idx(dir, e[0], e[1], e[2]);
-    for (int n = 0; n < 4; ++n) {
-        if (!isfinite(f[n]) || !isfinite(c[n]) || !isfinite(vn[n])) {
-            fx_fail(D.err, FX_ERR_EMF_NONFINITE, b, eidx);
-        }
-    }
-    /* edge resistivity: run-time eta plus the maximum artificial eta of the
-     * four incident cells (src/prj_timeint.c:265-290) */
-    double eta_cells = 0.0;
-    {
-        const int cells[4] = {c0, c1, c2, c3};
-        for (int n = 0; n < 4; ++n) {
-            const double ce = fx_cell_eta(Wb[(size_t)FX_RHO * kPlane + cells[n]],
-                Wb[(size_t)FX_YE * kPlane + cells[n]]);
-            if (!isfinite(ce) || ce < 0.0) {
-                fx_fail(D.err, FX_ERR_ETA, b, eidx);
+
+    /* cell quantities of plane i into buffer (i + 2) & 1 */
+    auto cells = [&](int i) {
+        double (*q)[P2] = cq[(i + 2) & 1];
+        for (int t = threadIdx.x; t < (FX_BS + 2) * (FX_BS + 2); t += blockDim.x) {
+            const int jj = t / (FX_BS + 2);
+            const int kk = t - jj * (FX_BS + 2);
+            const int c = fx_lidx(i, jj - 1, kk - 1);
+            const double b1 = Wb[(size_t)FX_B1 * kPlane + c];
+            const double b2 = Wb[(size_t)FX_B2 * kPlane + c];
+            const double b3 = Wb[(size_t)FX_B3 * kPlane + c];
+            const double v1 = Wb[(size_t)FX_V1 * kPlane + c];
+            const double v2 = Wb[(size_t)FX_V2 * kPlane + c];
+            const double v3 = Wb[(size_t)FX_V3 * kPlane + c];
+            /* prj_timeint_mhd_cell_emf_all, src/prj_timeint.c:171-176 */
+            const double e1 = b2 * v3 - b3 * v2;
+            const double e2 = b3 * v1 - b1 * v3;
+            const double e3 = b1 * v2 - b2 * v1;
+            if (!isfinite(e1) || !isfinite(e2) || !isfinite(e3)) {
+                fx_fail(D.err, FX_ERR_EMF_NONFINITE, b, c);
             }
-            if (ce > eta_cells) {
-                eta_cells = ce;
+            const double eta = fx_cell_eta(Wb[(size_t)FX_RHO * kPlane + c], Wb[(size_t)FX_YE * kPlane + c]);
+            if (!isfinite(eta) || eta < 0.0) {
+                fx_fail(D.err, FX_ERR_ETA, b, c);
             }
+            const int pc = (jj + 1) * FX_PBS + (kk + 1);
+            q[0][pc] = e1;
+            q[1][pc] = e2;
+            q[2][pc] = e3;
+            q[3][pc] = eta;
         }
-    }
-    const double eta = D.mhd_eta + eta_cells;
-    double emf = fx_emf_upwind(f, c, vn);
-    if (eta != 0.0) {
-        /* resistive term, src/prj_mhd.c:682-709 */
-        const double *bf = D.Bf + (size_t)b * FX_BF_COUNT;
-        const double *b1 = bf + (size_t)(0 * FX_NSTAGES + bfslot) * FX_NFACES;
-        const double *b2 = bf + (size_t)(1 * FX_NSTAGES + bfslot) * FX_NFACES;
-        const double *b3 = bf + (size_t)(2 * FX_NSTAGES + bfslot) * FX_NFACES;
-        const FxBlockDev &B = D.blk[b];
-        const int i = e[0], j = e[1], k = e[2];
-        double curl_b;
-        if (dir == 0) {
-            curl_b = (b3[fx_face_idx(2, i, j, k)] - b3[fx_face_idx(2, i, j - 1, k)]) / B.dx[1] -
-                (b2[fx_face_idx(1, i, j, k)] - b2[fx_face_idx(1, i, j, k - 1)]) / B.dx[2];
-        } else if (dir == 1) {
-            curl_b = (b1[fx_face_idx(0, i, j, k)] - b1[fx_face_idx(0, i, j, k - 1)]) / B.dx[2] -
-                (b3[fx_face_idx(2, i, j, k)] - b3[fx_face_idx(2, i - 1, j, k)]) / B.dx[0];
-        } else {
-            curl_b = (b2[fx_face_idx(1, i, j, k)] - b2[fx_face_idx(1, i - 1, j, k)]) / B.dx[0] -
-                (b1[fx_face_idx(0, i, j, k)] - b1[fx_face_idx(0, i, j - 1, k)]) / B.dx[1];
+    };
+
+    constexpr int N0 = (FX_BS + 1) * (FX_BS + 1);   /* x edges of a layer (i < 16) */
+    constexpr int N1 = FX_BS * (FX_BS + 1);         /* y edges */
+    constexpr int N2 = (FX_BS + 1) * FX_BS;         /* z edges */
+    cells(l0 - 1);
+    for (int i0 = l0; i0 < l1; ++i0) {
+        cells(i0);
+        __syncthreads();
+        const int cur = (i0 + 2) & 1;   /* buffer of plane i0; plane i0 - 1 in 1 - cur */
+        const int n0 = i0 < FX_BS ? N0 : 0;
+        const int ntot = n0 + N1 + N2;
+        for (int t = threadIdx.x; t < ntot; t += blockDim.x) {
+            int dir, u = t, xk;
+            if (u < n0) {
+                dir = 0;
+                xk = FX_BS + 1;
+            } else if ((u -= n0) < N1) {
+                dir = 1;
+                xk = FX_BS + 1;
+            } else {
+                u -= N1;
+                dir = 2;
+                xk = FX_BS;
+            }
+            const int j = u / xk;
+            const int k = u - j * xk;
+            const int up = (dir + 1) % 3;
+            const int right = (dir + 2) % 3;
+            /* the four cells: c0 = e, c1 = e - up, c2 = e - up - right,
+             * c3 = e - right; buffer and in-plane index */
+            const int pc = (j + FX_NG) * FX_PBS + (k + FX_NG);
+            int cb[4], ci[4];
+            if (dir == 0) {
+                cb[0] = cur; ci[0] = pc;
+                cb[1] = cur; ci[1] = pc - FX_PBS;
+                cb[2] = cur; ci[2] = pc - FX_PBS - 1;
+                cb[3] = cur; ci[3] = pc - 1;
+            } else if (dir == 1) {
+                cb[0] = cur; ci[0] = pc;
+                cb[1] = cur; ci[1] = pc - 1;
+                cb[2] = 1 - cur; ci[2] = pc - 1;
+                cb[3] = 1 - cur; ci[3] = pc;
+            } else {
+                cb[0] = cur; ci[0] = pc;
+                cb[1] = 1 - cur; ci[1] = pc;
+                cb[2] = 1 - cur; ci[2] = pc - FX_PBS;
+                cb[3] = cur; ci[3] = pc - FX_PBS;
+            }
+            double c[4];
+            /* edge resistivity: run-time eta plus the maximum artificial eta
+             * of the four incident cells (src/prj_timeint.c:265-290) */
+            double eta_cells = 0.0;
+#pragma unroll
+            for (int n = 0; n < 4; ++n) {
+                c[n] = cq[cb[n]][dir][ci[n]];
+                const double ce = cq[cb[n]][3][ci[n]];
+                if (ce > eta_cells) {
+                    eta_cells = ce;
+                }
+            }
+            const int c0 = fx_lidx(i0, j, k);
+            const int c1 = c0 - fx_axis_stride(up);
+            const int c3 = c0 - fx_axis_stride(right);
+            const double *bv1r = D.bv1 + (size_t)b * FX_BV_COUNT + (size_t)right * FX_NCELLS;
+            const double *bv2u = D.bv2 + (size_t)b * FX_BV_COUNT + (size_t)up * FX_NCELLS;
+            const double *vrr = D.vr + (size_t)b * FX_VR_COUNT + (size_t)right * 3 * FX_NCELLS;
+            const double *vru = D.vr + (size_t)b * FX_VR_COUNT + (size_t)up * 3 * FX_NCELLS;
+            double f[4], vn[4];
+            f[0] = bv1r[c0];
+            f[1] = bv2u[c0];
+            f[2] = bv1r[c1];
+            f[3] = bv2u[c3];
+            vn[0] = vrr[fx_bidx_cell(3, right, c0)];
+            vn[1] = vru[fx_bidx_cell(3, up, c0)];
+            vn[2] = vrr[fx_bidx_cell(3, right, c1)];
+            vn[3] = vru[fx_bidx_cell(3, up, c3)];
+            const int eidx = fx_edge_idx(dir, i0, j, k);
+            for (int n = 0; n < 4; ++n) {
+                if (!isfinite(f[n]) || !isfinite(vn[n])) {
+                    fx_fail(D.err, FX_ERR_EMF_NONFINITE, b, eidx);
+                }
+            }
+            const double eta = D.mhd_eta + eta_cells;
+            double emf = fx_emf_upwind(f, c, vn);
+            if (eta != 0.0) {
+                /* resistive term, src/prj_mhd.c:682-709 */
+                const double *bf = D.Bf + (size_t)b * FX_BF_COUNT;
+                const double *b1 = bf + (size_t)(0 * FX_NSTAGES + bfslot) * FX_NFACES;
+                const double *b2 = bf + (size_t)(1 * FX_NSTAGES + bfslot) * FX_NFACES;
+                const double *b3 = bf + (size_t)(2 * FX_NSTAGES + bfslot) * FX_NFACES;
+                const FxBlockDev &B = D.blk[b];
+                const int i = i0;
+                double curl_b;
+                if (dir == 0) {
+                    curl_b = (b3[fx_face_idx(2, i, j, k)] - b3[fx_face_idx(2, i, j - 1, k)]) / B.dx[1] -
+                        (b2[fx_face_idx(1, i, j, k)] - b2[fx_face_idx(1, i, j, k - 1)]) / B.dx[2];
+                } else if (dir == 1) {
+                    curl_b = (b1[fx_face_idx(0, i, j, k)] - b1[fx_face_idx(0, i, j, k - 1)]) / B.dx[2] -
+                        (b3[fx_face_idx(2, i, j, k)] - b3[fx_face_idx(2, i - 1, j, k)]) / B.dx[0];
+                } else {
+                    curl_b = (b2[fx_face_idx(1, i, j, k)] - b2[fx_face_idx(1, i - 1, j, k)]) / B.dx[0] -
+                        (b1[fx_face_idx(0, i, j, k)] - b1[fx_face_idx(0, i, j - 1, k)]) / B.dx[1];
+                }
+                emf += eta * curl_b;
+            }
+            if (!isfinite(emf)) {
+                fx_fail(D.err, FX_ERR_EMF_NONFINITE, b, eidx);
+            }
+            D.emf[(size_t)b * FX_EMF_COUNT + (size_t)dir * FX_NEDGES + eidx] = emf;
         }
-        emf += eta * curl_b;
+        __syncthreads(); /* plane i0 - 1's buffer takes plane i0 + 1 next */
     }
-    if (!isfinite(emf)) {
-        fx_fail(D.err, FX_ERR_EMF_NONFINITE, b, eidx);
-    }
-    D.emf[(size_t)b * FX_EMF_COUNT + (size_t)dir * FX_NEDGES + eidx] = emf;
 }
 
 /* ------------------------------------------------------------------------ */
@@ -1202,8 +1263,7 @@ void fx_flux_shape(int variant, int *tpb, int *minb)
 void fx_launch_emf(const FxDev &D, const int *blist, int nlist, int wslot, int bfslot, cudaStream_t s)
 {
     if (nlist <= 0) return;
-    const int ne = 3 * FX_BS * (FX_BS + 1) * (FX_BS + 1);
-    k_emf<<<dim3(fx_blocks(ne, 128), nlist), 128, 0, s>>>(D, blist, wslot, bfslot);
+    k_emf<<<dim3(kEmfChunks, nlist), 256, 0, s>>>(D, blist, wslot, bfslot);
 }
 
 void fx_launch_bf_update(const FxDev &D, const int *blist, int nlist, int stage, cudaStream_t s)
