@@ -1632,6 +1632,21 @@ private:
             }
             const int nt = compile_threads();
             for (const auto &bk : buckets) sort_by_dst(bk.first, bk.second, nt);
+            /* face operations: direction-major (stable), so a warp's stores
+             * land in one direction's array and consecutive faces form runs */
+            std::vector<FxGop> tmp;
+            for (size_t q = 0; q + 1 < nf.size(); ++q) {
+                const int lo = q == 0 ? 0 : nf[q - 1];
+                const size_t n = (size_t)(nf[q] - lo);
+                if (n < 2) continue;
+                FxGop *ops = g.face_ops.data() + lo;
+                size_t cnt[4] = {0, 0, 0, 0};
+                for (size_t e = 0; e < n; ++e) ++cnt[(ops[e].aux & 3) + 1];
+                for (int d = 0; d < 3; ++d) cnt[d + 1] += cnt[d];
+                tmp.resize(n);
+                for (size_t e = 0; e < n; ++e) tmp[cnt[ops[e].aux & 3]++] = ops[e];
+                std::copy(tmp.begin(), tmp.end(), ops);
+            }
         }
         g.b_ops.swap(bops_all);
         g.b_begin.assign(1, 0);
