@@ -200,6 +200,119 @@ __global__ void __launch_bounds__(TPB, MINB) k_flux(FxDev D, const int *__restri
 /* ------------------------------------------------------------------------ */
 /* Edge EMFs                                                                 */
 /* ------------------------------------------------------------------------ */
+/* The per-block launches of the plain form: one thread per edge, so a
+ * single block still fills the device; the cell EMF components and eta of
+ * an edge's four cells are evaluated per edge (same arithmetic). */
+__device__ __forceinline__ double fx_cell_emf(const double *Wb, int dir, int c)
+{
+    const int a = (dir + 1) % 3;
+    const int bb = (dir + 2) % 3;
+    const double bA = Wb[(size_t)(FX_B1 + a) * kPlane + c];
+    const double bB = Wb[(size_t)(FX_B1 + bb) * kPlane + c];
+    const double vA = Wb[(size_t)(FX_V1 + a) * kPlane + c];
+    const double vB = Wb[(size_t)(FX_V1 + bb) * kPlane + c];
+    return bA * vB - bB * vA;
+}
+
+__global__ void __launch_bounds__(128) k_emf_edges(FxDev D, const int *__restrict__ blist, int wslot, int bfslot)
+{
+    if (D.ctl->skip) {
+        return;
+    }
+    const int b = blist[blockIdx.y];
+    constexpr int NE = FX_BS * (FX_BS + 1) * (FX_BS + 1);
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= 3 * NE) {
+        return;
+    }
+    const int dir = t / NE;
+    t -= dir * NE;
+    const int x2 = dir == 2 ? FX_BS : FX_BS + 1;
+    const int x1 = dir == 1 ? FX_BS : FX_BS + 1;
+    int e[3];
+    e[2] = t % x2;
+    t /= x2;
+    e[1] = t % x1;
+    e[0] = t / x1;
+    const int up = (dir + 1) % 3;
+    const int right = (dir + 2) % 3;
+    const int su = fx_axis_stride(up);
+    const int sr = fx_axis_stride(right);
+    const int c0 = fx_lidx(e[0], e[1], e[2]);   /* cell0 = e; face0 = face1 = e */
+    const int c1 = c0 - su;                      /* cell1 = e - up */
+    const int c2 = c0 - su - sr;                 /* cell2 = e - up - right */
+    const int c3 = c0 - sr;                      /* cell3 = e - right */
+    const double *Wb = D.W + (size_t)b * FX_W_COUNT(9) + (size_t)wslot * FX_NCELLS;
+    const double *bv1r = D.bv1 + (size_t)b * FX_BV_COUNT + (size_t)right * FX_NCELLS;
+    const double *bv2u = D.bv2 + (size_t)b * FX_BV_COUNT + (size_t)up * FX_NCELLS;
+    const double *vrr = D.vr + (size_t)b * FX_VR_COUNT + (size_t)right * 3 * FX_NCELLS;
+    const double *vru = D.vr + (size_t)b * FX_VR_COUNT + (size_t)up * 3 * FX_NCELLS;
+    double f[4], c[4], vn[4];
+    /* face0 = e (right-normal), face1 = e (up-normal), face2 = e - up
+     * (right-normal), face3 = e - right (up-normal) */
+    f[0] = bv1r[c0];
+    f[1] = bv2u[c0];
+    f[2] = bv1r[c1];
+    f[3] = bv2u[c3];
+    c[0] = fx_cell_emf(Wb, dir, c0);
+    c[1] = fx_cell_emf(Wb, dir, c1);
+    c[2] = fx_cell_emf(Wb, dir, c2);
+    c[3] = fx_cell_emf(Wb, dir, c3);
+    vn[0] = vrr[fx_bidx_cell(3, right, c0)];
+    vn[1] = vru[fx_bidx_cell(3, up, c0)];
+    vn[2] = vrr[fx_bidx_cell(3, right, c1)];
+    vn[3] = vru[fx_bidx_cell(3, up, c3)];
+    const int eidx = fx_edge_idx(dir, e[0], e[1], e[2]);
+    for (int n = 0; n < 4; ++n) {
+        if (!isfinite(f[n]) || !isfinite(c[n]) || !isfinite(vn[n])) {
+            fx_fail(D.err, FX_ERR_EMF_NONFINITE, b, eidx);
+        }
+    }
+    /* edge resistivity: run-time eta plus the maximum artificial eta of the
+     * four incident cells (src/prj_timeint.c:265-290) */
+    double eta_cells = 0.0;
+    {
+        const int cells[4] = {c0, c1, c2, c3};
+        for (int n = 0; n < 4; ++n) {
+            const double ce = fx_cell_eta(Wb[(size_t)FX_RHO * kPlane + cells[n]],
+                Wb[(size_t)FX_YE * kPlane + cells[n]]);
+            if (!isfinite(ce) || ce < 0.0) {
+                fx_fail(D.err, FX_ERR_ETA, b, eidx);
+            }
+            if (ce > eta_cells) {
+                eta_cells = ce;
+            }
+        }
+    }
+    const double eta = D.mhd_eta + eta_cells;
+    double emf = fx_emf_upwind(f, c, vn);
+    if (eta != 0.0) {
+        /* resistive term, src/prj_mhd.c:682-709 */
+        const double *bf = D.Bf + (size_t)b * FX_BF_COUNT;
+        const double *b1 = bf + (size_t)(0 * FX_NSTAGES + bfslot) * FX_NFACES;
+        const double *b2 = bf + (size_t)(1 * FX_NSTAGES + bfslot) * FX_NFACES;
+        const double *b3 = bf + (size_t)(2 * FX_NSTAGES + bfslot) * FX_NFACES;
+        const FxBlockDev &B = D.blk[b];
+        const int i = e[0], j = e[1], k = e[2];
+        double curl_b;
+        if (dir == 0) {
+            curl_b = (b3[fx_face_idx(2, i, j, k)] - b3[fx_face_idx(2, i, j - 1, k)]) / B.dx[1] -
+                (b2[fx_face_idx(1, i, j, k)] - b2[fx_face_idx(1, i, j, k - 1)]) / B.dx[2];
+        } else if (dir == 1) {
+            curl_b = (b1[fx_face_idx(0, i, j, k)] - b1[fx_face_idx(0, i, j, k - 1)]) / B.dx[2] -
+                (b3[fx_face_idx(2, i, j, k)] - b3[fx_face_idx(2, i - 1, j, k)]) / B.dx[0];
+        } else {
+            curl_b = (b2[fx_face_idx(1, i, j, k)] - b2[fx_face_idx(1, i - 1, j, k)]) / B.dx[0] -
+                (b1[fx_face_idx(0, i, j, k)] - b1[fx_face_idx(0, i, j - 1, k)]) / B.dx[1];
+        }
+        emf += eta * curl_b;
+    }
+    if (!isfinite(emf)) {
+        fx_fail(D.err, FX_ERR_EMF_NONFINITE, b, eidx);
+    }
+    D.emf[(size_t)b * FX_EMF_COUNT + (size_t)dir * FX_NEDGES + eidx] = emf;
+}
+
 /* One CTA per (block, chunk of edge layers along i).  For each layer i the
  * CTA first evaluates, once per cell of plane i (j, k in [-1, 16]), the
  * three cell-centred EMF components and the artificial eta (the reference
@@ -1265,6 +1378,11 @@ void fx_flux_shape(int variant, int *tpb, int *minb)
 void fx_launch_emf(const FxDev &D, const int *blist, int nlist, int wslot, int bfslot, cudaStream_t s)
 {
     if (nlist <= 0) return;
+    if (nlist < 16) {
+        const int ne = 3 * FX_BS * (FX_BS + 1) * (FX_BS + 1);
+        k_emf_edges<<<dim3(fx_blocks(ne, 128), nlist), 128, 0, s>>>(D, blist, wslot, bfslot);
+        return;
+    }
     k_emf<<<dim3(kEmfChunks, nlist), 256, 0, s>>>(D, blist, wslot, bfslot);
 }
 
