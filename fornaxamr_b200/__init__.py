@@ -19,14 +19,12 @@ from ._lib import (ARR_BF, ARR_BV1, ARR_BV2, ARR_EMF, ARR_EOSVAR, ARR_FLUX, ARR_
                    FORM_PLAIN, PHASE_CELLS, PHASE_CT, PHASE_EMF, PHASE_FLUX, PHASE_GHOST, PHASE_STEP,
                    AMR_FRACTIONAL_JUMP, AMR_LOEHNER, AMR_PRESSURE_SCALE_HEIGHT, AMR_VAR_DENSITY,
                    AMR_VAR_PRESSURE, AMR_VAR_TEMPERATURE, AMR_VELOCITY, INT_ESSPRK10_4, INT_RK2,
-                   RECON_MC, RECON_WENO3, FxAmrConfig, FxBlockDesc, FxConfig)
+                   RECON_MC, RECON_WENO3, RECON_WENO7, FxAmrConfig, FxBlockDesc, FxConfig)
 
 __all__ = ["Context", "FxError", "FORM_PLAIN", "FORM_BATCHED", "NCELLS", "NFACES", "NEDGES",
            "library", "plan_export", "amr_config", "amr_remesh_host"]
 
-NCELLS = 20 ** 3
-NFACES = 21 * 20 * 20
-NEDGES = 21 * 21 * 20
+from .layout import NCELLS, NEDGES, NFACES, NG  # noqa: E402  (sizes of the loaded build)
 NSTAGES = 2
 
 _L: Optional[C.CDLL] = None

@@ -8,10 +8,13 @@ from __future__ import annotations
 import ctypes as C
 import os
 
-HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "libfornax_b200.so")
+from .layout import NG
 
-FX_SUCCESS, FX_EINVAL, FX_ECUDA, FX_ENOMESH, FX_EPHYSICS, FX_ENOMEM, FX_ETOOBIG = range(7)
+HERE = os.path.dirname(os.path.abspath(__file__))
+# the build with the ghost layers of this process (FX_NGHOST)
+LIB_PATH = os.path.join(HERE, "libfornax_b200.so" if NG == 2 else f"libfornax_b200_ng{NG}.so")
+
+FX_SUCCESS, FX_EINVAL, FX_ECUDA, FX_ENOMESH, FX_EPHYSICS, FX_ENOMEM, FX_ETOOBIG, FX_ECOMM = range(8)
 NOALLOC_MAX_BLOCKS = 65536
 FORM_PLAIN, FORM_BATCHED = 0, 1
 BC_OUTFLOW, BC_REFLECT, BC_USER, BC_PERIODIC = 0, 1, 2, 3
@@ -62,7 +65,7 @@ class FxConfig(C.Structure):
     ]
 
 
-RECON_MC, RECON_WENO3 = 0, 1
+RECON_MC, RECON_WENO3, RECON_WENO7 = 0, 1, 2
 INT_RK2, INT_ESSPRK10_4 = 0, 1
 
 AMR_N = 4
@@ -108,7 +111,7 @@ EXPORTS = [
     "fx_amr_configure", "fx_amr_tag", "fx_amr_adapt", "fx_get_mesh", "fx_amr_energy_injected",
     "fx_amr_remesh_host", "fx_amr_timings", "fx_shard_export", "fx_shard_set_mesh",
     "fx_shard_group_create", "fx_shard_group_destroy", "fx_shard_attach_group", "fx_nccl_unique_id",
-    "fx_shard_attach_nccl", "fx_shard_info",
+    "fx_shard_attach_nccl", "fx_shard_info", "fx_ghost_layers",
 ]
 PHASE_FLUX, PHASE_EMF, PHASE_CT, PHASE_CELLS, PHASE_GHOST, PHASE_STEP = range(6)
 
@@ -119,6 +122,9 @@ def load() -> C.CDLL:
             f"{LIB_PATH} is missing: build it with `python -m fornaxamr_b200.build` "
             "(the package has no CPU fallback)")
     L = C.CDLL(LIB_PATH, mode=C.RTLD_LOCAL)
+    L.fx_ghost_layers.argtypes = []
+    if L.fx_ghost_layers() != NG:
+        raise ImportError(f"{LIB_PATH} was built with {L.fx_ghost_layers()} ghost layers, FX_NGHOST is {NG}")
     vp = C.c_void_p
     dp = C.POINTER(C.c_double)
     ip = C.POINTER(C.c_int32)

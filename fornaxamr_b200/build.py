@@ -3,7 +3,9 @@
     python -m fornaxamr_b200.build
 
 compiles fornaxamr_b200/csrc/*.cu and *.cpp with nvcc for sm_100a only and
-links them into fornaxamr_b200/libfornax_b200.so.  --fmad=false keeps every
+links them into fornaxamr_b200/libfornax_b200.so (2 ghost layers, 20^3 block
+arrays) and, with FX_NG=4, fornaxamr_b200/libfornax_b200_ng4.so (4 layers,
+24^3, the layout WENO-Z7 needs).  --fmad=false keeps every
 double multiply and add separately rounded, the arithmetic contract under
 which the kernels reproduce the reference CPU path bit for bit.
 """
@@ -13,6 +15,7 @@ import os
 import shutil
 import subprocess
 import sys
+from concurrent.futures import ThreadPoolExecutor
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
@@ -40,30 +43,48 @@ def _stale(obj: str, deps) -> bool:
     return any(os.path.getmtime(d) > t for d in deps)
 
 
-def build(verbose: bool = False, ptxas_info: bool = False) -> str:
-    os.makedirs(BUILD, exist_ok=True)
+# the 2-ghost-layer build (20^3 block arrays, the reference's default
+# PRJ_NGHOST) and the 4-layer build that WENO-Z7 needs (24^3)
+LIBS = {2: LIB, 4: os.path.join(HERE, "libfornax_b200_ng4.so")}
+
+
+def _build_one(ng: int, verbose: bool, ptxas_info: bool) -> str:
+    out_dir = BUILD if ng == 2 else os.path.join(BUILD, f"ng{ng}")
+    os.makedirs(out_dir, exist_ok=True)
     headers = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".h", ".cuh"))]
     headers.append(os.path.join(os.path.dirname(HERE), "include", "fornax_b200.h"))
-    objs = []
+    jobs, objs = [], []
     for src in SOURCES:
         path = os.path.join(CSRC, src)
-        obj = os.path.join(BUILD, src + ".o")
+        obj = os.path.join(out_dir, src + ".o")
         objs.append(obj)
         if not _stale(obj, [path] + headers + [__file__]):
             continue
-        cmd = [nvcc()] + ARCH + NVCC_FLAGS + ["-c", path, "-o", obj]
+        cmd = [nvcc()] + ARCH + NVCC_FLAGS + [f"-DFX_NG={ng}", "-c", path, "-o", obj]
         if ptxas_info and src.endswith(".cu"):
             cmd += ["-Xptxas", "-v"]
         if src.endswith(".cpp"):
             cmd += ["-x", "cu"]
+        jobs.append(cmd)
+    with ThreadPoolExecutor(max_workers=max(1, min(len(jobs), os.cpu_count() or 1))) as pool:
+        for cmd in jobs:
+            if verbose:
+                print(" ".join(cmd))
+        for r in pool.map(lambda c: subprocess.run(c, check=True), jobs):
+            pass
+    lib = LIBS[ng]
+    if _stale(lib, objs):
+        cmd = [nvcc()] + ARCH + ["-shared", "-o", lib] + objs + ["-lcudart", "-ldl"]
         if verbose:
             print(" ".join(cmd))
         subprocess.run(cmd, check=True)
-    if _stale(LIB, objs):
-        cmd = [nvcc()] + ARCH + ["-shared", "-o", LIB] + objs + ["-lcudart", "-ldl"]
-        if verbose:
-            print(" ".join(cmd))
-        subprocess.run(cmd, check=True)
+    return lib
+
+
+def build(verbose: bool = False, ptxas_info: bool = False) -> str:
+    """Builds both libraries; returns the 2-layer one's path."""
+    for ng in (2, 4):
+        _build_one(ng, verbose, ptxas_info)
     return LIB
 
 

@@ -62,15 +62,27 @@ __device__ __forceinline__ unsigned long long fx_double_key(double d)
  * q1, q2): MC slopes (the reference's fast path, prj_flux_recon_var_mc:
  * q +- 0.5 slope) or WENO-Z3 face values (its per-face path,
  * src/prj_flux.c:440-475) */
+/* cells of a face's stencil along the sweep: 4 (cL - 1 .. cR + 1) for MC
+ * and WENO-Z3, 8 (cL - 3 .. cR + 3) for WENO-Z7; q[n] is cell cL + n - NS/2 + 1 */
 template <int RECON>
-__device__ __forceinline__ void fx_recon_pair(double qm, double q0, double q1, double q2, double &wl, double &wr)
+struct FxStencil {
+    static constexpr int NS = RECON == FX_RECON_WENO7 ? 8 : 4;
+};
+
+template <int RECON>
+__device__ __forceinline__ void fx_recon_pair(const double (&q)[FxStencil<RECON>::NS], double &wl, double &wr)
 {
-    if (RECON == FX_RECON_WENO3) {
-        wl = fx_weno3_face(qm, q0, q1, 0.5);
-        wr = fx_weno3_face(q0, q1, q2, -0.5);
+    if constexpr (RECON == FX_RECON_WENO7) {
+        /* left state: cells cL-3 .. cL+3 at +1/2; right state: cells cR-3 ..
+         * cR+3 at -1/2, i.e. the mirrored stencil cR+3 .. cR-3 at +1/2 */
+        wl = fx_weno7_plus(q[0], q[1], q[2], q[3], q[4], q[5], q[6]);
+        wr = fx_weno7_plus(q[7], q[6], q[5], q[4], q[3], q[2], q[1]);
+    } else if constexpr (RECON == FX_RECON_WENO3) {
+        wl = fx_weno3_face(q[0], q[1], q[2], 0.5);
+        wr = fx_weno3_face(q[1], q[2], q[3], -0.5);
     } else {
-        wl = q0 + 0.5 * fx_mc_slope(qm, q0, q1);
-        wr = q1 - 0.5 * fx_mc_slope(q0, q1, q2);
+        wl = q[1] + 0.5 * fx_mc_slope(q[0], q[1], q[2]);
+        wr = q[2] - 0.5 * fx_mc_slope(q[1], q[2], q[3]);
     }
 }
 
@@ -109,45 +121,54 @@ __global__ void __launch_bounds__(TPB, MINB) k_flux(FxDev D, const int *__restri
 
     double WL[9];
     double WR[9];
-    /* density and internal energy at the four cells of the stencil also give
-     * the reconstructed pressure (eosvar p = (g-1) rho e of each cell). */
-    double rho4[4], eint4[4];
+    /* density and internal energy at the stencil cells also give the
+     * reconstructed pressure (eosvar p = (g-1) rho e of each cell). */
+    constexpr int NS = FxStencil<RECON>::NS;
+    const int c0 = cL - (NS / 2 - 1) * s;   /* first stencil cell */
+    double rhoS[NS], eintS[NS];
     {
-        const double *q = Wb + (size_t)FX_RHO * kPlane;
-        rho4[0] = q[cL - s]; rho4[1] = q[cL]; rho4[2] = q[cR]; rho4[3] = q[cR + s];
-        q = Wb + (size_t)FX_EINT * kPlane;
-        eint4[0] = q[cL - s]; eint4[1] = q[cL]; eint4[2] = q[cR]; eint4[3] = q[cR + s];
+        const double *qr = Wb + (size_t)FX_RHO * kPlane + c0;
+        const double *qe = Wb + (size_t)FX_EINT * kPlane + c0;
+#pragma unroll
+        for (int n = 0; n < NS; ++n) {
+            rhoS[n] = qr[n * s];
+            eintS[n] = qe[n * s];
+        }
     }
-    fx_recon_pair<RECON>(rho4[0], rho4[1], rho4[2], rho4[3], WL[FX_RHO], WR[FX_RHO]);
-    fx_recon_pair<RECON>(eint4[0], eint4[1], eint4[2], eint4[3], WL[FX_EINT], WR[FX_EINT]);
+    fx_recon_pair<RECON>(rhoS, WL[FX_RHO], WR[FX_RHO]);
+    fx_recon_pair<RECON>(eintS, WL[FX_EINT], WR[FX_EINT]);
 #pragma unroll
     for (int lv = 1; lv < nv; ++lv) {
         if (lv == FX_EINT || (MHD && lv == FX_B1)) {
             continue;
         }
-        const double *q = Wb + (size_t)fx_gmap(dir, lv) * kPlane;
-        const double qm = q[cL - s];
-        const double q0 = q[cL];
-        const double q1 = q[cR];
-        const double q2 = q[cR + s];
-        fx_recon_pair<RECON>(qm, q0, q1, q2, WL[lv], WR[lv]);
-    }
-    double p4[4];
+        const double *q = Wb + (size_t)fx_gmap(dir, lv) * kPlane + c0;
+        double qs[NS];
 #pragma unroll
-    for (int n = 0; n < 4; ++n) {
-        p4[n] = fx_pressure(g, rho4[n], eint4[n]);
+        for (int n = 0; n < NS; ++n) {
+            qs[n] = q[n * s];
+        }
+        fx_recon_pair<RECON>(qs, WL[lv], WR[lv]);
+    }
+    double pS[NS];
+#pragma unroll
+    for (int n = 0; n < NS; ++n) {
+        pS[n] = fx_pressure(g, rhoS[n], eintS[n]);
     }
     double pL, pR;
-    fx_recon_pair<RECON>(p4[0], p4[1], p4[2], p4[3], pL, pR);
+    fx_recon_pair<RECON>(pS, pL, pR);
     /* gamma is uniform for the ideal gas: its MC slope is exactly 0, so the
-     * MC face values equal g bit for bit; the WENO-Z3 weights of a constant
+     * MC face values equal g bit for bit; the WENO weights of a constant
      * stencil are evaluated as the reference does (their sum need not be 1) */
     double gL = g, gR = g;
-    if (RECON == FX_RECON_WENO3) {
-        gL = fx_weno3_face(g, g, g, 0.5);
-        gR = fx_weno3_face(g, g, g, -0.5);
+    if (RECON != FX_RECON_MC) {
+        double gS[NS];
+#pragma unroll
+        for (int n = 0; n < NS; ++n) {
+            gS[n] = g;
+        }
+        fx_recon_pair<RECON>(gS, gL, gR);
     }
-
     const size_t fbase = (size_t)b * FX_FLUX_COUNT(nv) + (size_t)dir * nv * FX_NCELLS;
     const size_t vbase = (size_t)b * FX_VR_COUNT + (size_t)dir * 3 * FX_NCELLS;
     if (MHD) {
@@ -365,7 +386,7 @@ __global__ void __launch_bounds__(256) k_emf(FxDev D, const int *__restrict__ bl
             if (!isfinite(eta) || eta < 0.0) {
                 fx_fail(D.err, FX_ERR_ETA, b, c);
             }
-            const int pc = (jj + 1) * FX_PBS + (kk + 1);
+            const int pc = (jj - 1 + FX_NG) * FX_PBS + (kk - 1 + FX_NG);
             q[0][pc] = e1;
             q[1][pc] = e2;
             q[2][pc] = e3;
@@ -943,8 +964,8 @@ __device__ __forceinline__ int fx_face_stride(int d, int a)
  * faces contribute their current fine value. */
 __device__ __forceinline__ void fx_ghost_prolong_group(const FxDev &D, const FxPop &op, int slot)
 {
-    const int f0[3] = {(op.pos & 31) - 2, ((op.pos >> 5) & 31) - 2, ((op.pos >> 10) & 31) - 2};
-    const int c0[3] = {((op.pos >> 15) & 31) - 2, ((op.pos >> 20) & 31) - 2, ((op.pos >> 25) & 31) - 2};
+    const int f0[3] = {(op.pos & 31) - FX_NG, ((op.pos >> 5) & 31) - FX_NG, ((op.pos >> 10) & 31) - FX_NG};
+    const int c0[3] = {((op.pos >> 15) & 31) - FX_NG, ((op.pos >> 20) & 31) - FX_NG, ((op.pos >> 25) & 31) - FX_NG};
     const FxBlockDev &fb = D.blk[op.fine];
     const double area[3] = {fb.dx[1] * fb.dx[2], fb.dx[0] * fb.dx[2], fb.dx[0] * fb.dx[1]};
     /* outer fluxes o[d][side][a][b] */
@@ -1334,8 +1355,10 @@ static void launch_flux_shape(const FxDev &D, const int *blist, int nlist, int n
     k_flux<MHD, FULL, TPB, MINB, RECON><<<g, TPB, 0, s>>>(D, blist, wslot, bfslot);
 }
 
-/* WENO-Z3 is compiled in one launch shape (the autotuner's variants all map
- * to it); MC in all of them */
+/* WENO-Z3 and WENO-Z7 are compiled in one launch shape (the autotuner's
+ * variants all map to it); MC in all of them.  WENO-Z7 reads three cells
+ * beyond each face's neighbours and exists in the four-ghost-layer build
+ * only (the context rejects it elsewhere). */
 template <bool MHD, bool FULL>
 static void launch_flux_variant(const FxDev &D, const int *blist, int nlist, int ndir, int wslot,
     int bfslot, int variant, cudaStream_t s)
@@ -1344,6 +1367,12 @@ static void launch_flux_variant(const FxDev &D, const int *blist, int nlist, int
         launch_flux_shape<MHD, FULL, 128, 4, FX_RECON_WENO3>(D, blist, nlist, ndir, wslot, bfslot, s);
         return;
     }
+#if FX_NG >= 4
+    if (D.recon == FX_RECON_WENO7) {
+        launch_flux_shape<MHD, FULL, 128, 2, FX_RECON_WENO7>(D, blist, nlist, ndir, wslot, bfslot, s);
+        return;
+    }
+#endif
     switch (variant) {
     case 1: launch_flux_shape<MHD, FULL, 128, 5>(D, blist, nlist, ndir, wslot, bfslot, s); break;
     case 2: launch_flux_shape<MHD, FULL, 128, 6>(D, blist, nlist, ndir, wslot, bfslot, s); break;

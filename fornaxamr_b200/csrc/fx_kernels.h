@@ -68,7 +68,7 @@ struct FxDev {
 void fx_flux_shape(int variant, int *tpb, int *minb);
 
 /* One element operation of a ghost-fill program.  dst/src pack
- * (block << 13) | cell for cell ops, or (block << 15) | face for face ops
+ * FX_CELL_KEY(block, cell) for cell ops, or (block << 15) | face for face ops
  * (with the face direction in `aux` bits 0-1). */
 enum FxGopType {
     FX_GOP_COPY = 0,        /* dst <- src (all ghost vars) */
@@ -90,7 +90,7 @@ struct FxGop {
 };
 
 /* cell-centred field of one cell from its six faces (bf2bc of one cell):
- * dst = (block << 13) | cell; f[2d], f[2d+1] = (block << 15) | face of the
+ * dst = FX_CELL_KEY(block, cell); f[2d], f[2d+1] = (block << 15) | face of the
  * lower and upper face along d (after copy propagation they may point at
  * the faces those were copied from) */
 struct FxBop {
@@ -102,7 +102,7 @@ struct FxBop {
 /* Divergence-preserving prolongation of the face field onto one 2x2x2 group
  * of fine cells (prj_mhd_prolong_bf_from_buffer, src/prj_mhd.c:374-512).
  * pos packs the fine corner (fi, fj, fk) and the coarse cell (ci, cj, ck),
- * each biased by 2, in 5 bits apiece: fi | fj << 5 | fk << 10 | ci << 15 |
+ * each biased by FX_NG, in 5 bits apiece: fi | fj << 5 | fk << 10 | ci << 15 |
  * cj << 20 | ck << 25.  Outer face q = 8 d + 4 s + 2 a + b is the face of
  * direction d on side s (s = 1: index +2 along d) at tangential offsets
  * (a, b) in increasing axis order; inner face q = 4 d + 2 a + b.  keep bit
@@ -144,9 +144,12 @@ struct FxXent {
     int32_t off;
 };
 
-#define FX_CELL_KEY(b, c) (((b) << 13) | (c))
-#define FX_CELL_BLOCK(key) ((key) >> 13)
-#define FX_CELL_IDX(key) ((key) & 8191)
+/* cell keys: (block << FX_CELL_BITS) | cell, with the cell index below
+ * 2^FX_CELL_BITS (8000 cells of a 20^3 block, 13824 of a 24^3 one) */
+#define FX_CELL_BITS (FX_NCELLS <= 8192 ? 13 : 14)
+#define FX_CELL_KEY(b, c) (((b) << FX_CELL_BITS) | (c))
+#define FX_CELL_BLOCK(key) ((key) >> FX_CELL_BITS)
+#define FX_CELL_IDX(key) ((key) & ((1 << FX_CELL_BITS) - 1))
 
 /* launchers (fx_kernels.cu); all asynchronous on `s` */
 void fx_launch_flux(const FxDev &D, const int *blist, int nlist, int ndir, int wslot, int bfslot,

@@ -26,7 +26,9 @@
 #endif
 
 #define FX_BS 16
-#define FX_NG 2
+#ifndef FX_NG
+#define FX_NG 2                              /* 4 for the WENO-Z7 build (PRJ_NGHOST) */
+#endif
 #define FX_PBS (FX_BS + 2 * FX_NG)          /* 20 */
 #define FX_NCELLS (FX_PBS * FX_PBS * FX_PBS) /* 8000 */
 #define FX_NFACES ((FX_PBS + 1) * FX_PBS * FX_PBS) /* 8400 */

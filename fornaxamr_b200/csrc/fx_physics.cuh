@@ -130,6 +130,66 @@ FX_HD double fx_weno3_face(double qm, double q0, double qp, double target)
     return (alpha0 * p0 + alpha1 * p1) / sum;
 }
 
+/* WENO-Z7 (src/prj_reconstruct.h:425-521): the i+1/2 face value of the cell
+ * at q[3] from q[0..6].  Smoothness indicators are quadratic forms over
+ * four consecutive cells, evaluated term by term in the order (0,0), (0,1),
+ * (0,2), (0,3), (1,1), (1,2), (1,3), (2,2), (2,3), (3,3) as ((c q_a) q_b),
+ * accumulated left to right and divided by 240; a term with a negative
+ * coefficient subtracts (|c| q_a) q_b, which is the same double.  The i-1/2
+ * face is the same formula on the mirrored stencil. */
+FX_HD double fx_weno7_beta(const double c[10], double q0, double q1, double q2, double q3)
+{
+    const double q[4] = {q0, q1, q2, q3};
+    double acc = c[0] * q[0] * q[0];
+    int t = 1;
+#pragma unroll
+    for (int a = 0; a < 4; ++a) {
+#pragma unroll
+        for (int b = a; b < 4; ++b) {
+            if (a == 0 && b == 0) continue;
+            acc = acc + c[t] * q[a] * q[b];
+            ++t;
+        }
+    }
+    return acc / 240.0;
+}
+
+FX_HD double fx_weno7_plus(double q0, double q1, double q2, double q3, double q4, double q5, double q6)
+{
+    /* Balsara-Shu seventh-order smoothness coefficients, one row per
+     * sub-stencil, terms in the order above */
+    const double C0[10] = {547.0, -3882.0, 4642.0, -1854.0, 7043.0, -17246.0, 7042.0, 11003.0, -9402.0, 2107.0};
+    const double C1[10] = {267.0, -1642.0, 1602.0, -494.0, 2843.0, -5966.0, 1922.0, 3443.0, -2522.0, 547.0};
+    const double C2[10] = {547.0, -2522.0, 1922.0, -494.0, 3443.0, -5966.0, 1602.0, 2843.0, -1642.0, 267.0};
+    const double C3[10] = {2107.0, -9402.0, 7042.0, -1854.0, 11003.0, -17246.0, 4642.0, 7043.0, -3882.0, 547.0};
+    const double eps = 1.0e-40;
+    /* third-order candidates of the four sub-stencils */
+    const double p0 = (-3.0 * q0 + 13.0 * q1 - 23.0 * q2 + 25.0 * q3) / 12.0;
+    const double p1 = (q1 - 5.0 * q2 + 13.0 * q3 + 3.0 * q4) / 12.0;
+    const double p2 = (-q2 + 7.0 * q3 + 7.0 * q4 - q5) / 12.0;
+    const double p3 = (3.0 * q3 + 13.0 * q4 - 5.0 * q5 + q6) / 12.0;
+    const double b0 = fx_weno7_beta(C0, q0, q1, q2, q3);
+    const double b1 = fx_weno7_beta(C1, q1, q2, q3, q4);
+    const double b2 = fx_weno7_beta(C2, q2, q3, q4, q5);
+    const double b3 = fx_weno7_beta(C3, q3, q4, q5, q6);
+    /* global indicator tau7 and Z weights with the linear weights 1/35,
+     * 12/35, 18/35, 4/35 */
+    double tau7 = b0 - b3 + 3.0 * (b1 - b2);
+    if (tau7 < 0.0) {
+        tau7 = -tau7;
+    }
+    const double r0 = tau7 / (eps + b0);
+    const double r1 = tau7 / (eps + b1);
+    const double r2 = tau7 / (eps + b2);
+    const double r3 = tau7 / (eps + b3);
+    const double a0 = (1.0 / 35.0) * (1.0 + r0 * r0);
+    const double a1 = (12.0 / 35.0) * (1.0 + r1 * r1);
+    const double a2 = (18.0 / 35.0) * (1.0 + r2 * r2);
+    const double a3 = (4.0 / 35.0) * (1.0 + r3 * r3);
+    const double sum = a0 + a1 + a2 + a3;
+    return (a0 * p0 + a1 * p1 + a2 * p2 + a3 * p3) / sum;
+}
+
 /* minmod slope of prj_reconstruct_minmod_slope (src/prj_reconstruct.h:46-62) */
 FX_HD double fx_minmod_slope(double qm, double q0, double qp)
 {

@@ -465,7 +465,7 @@ private:
         }
     }
 
-    static int32_t cell_key(int64_t e) { return (int32_t)(((e / FX_NCELLS) << 13) | (e % FX_NCELLS)); }
+    static int32_t cell_key(int64_t e) { return (int32_t)FX_CELL_KEY(e / FX_NCELLS, e % FX_NCELLS); }
 
     int32_t face_key(int64_t e) const
     {
@@ -1053,8 +1053,8 @@ private:
         std::memset(&p, 0, sizeof(p));
         p.fine = fine;
         p.coarse = coarse;
-        p.pos = (f[0] + 2) | ((f[1] + 2) << 5) | ((f[2] + 2) << 10) | ((c[0] + 2) << 15) |
-            ((c[1] + 2) << 20) | ((c[2] + 2) << 25);
+        p.pos = (f[0] + FX_NG) | ((f[1] + FX_NG) << 5) | ((f[2] + FX_NG) << 10) | ((c[0] + FX_NG) << 15) |
+            ((c[1] + FX_NG) << 20) | ((c[2] + FX_NG) << 25);
         std::vector<int64_t> &reads = g_reads_;
         std::vector<int64_t> &writes = g_writes_;
         std::vector<std::pair<int64_t, ProlongSig>> &sigs = g_sigs_;
@@ -1770,7 +1770,7 @@ private:
             if (touched_[b] && owner_[b] != rank_) l2g.push_back(b);
         }
         for (int l = 0; l < (int)l2g.size(); ++l) g2l[l2g[l]] = l;
-        auto ck = [&](int32_t key) { return (g2l[key >> 13] << 13) | (key & 8191); };
+        auto ck = [&](int32_t key) { return FX_CELL_KEY(g2l[FX_CELL_BLOCK(key)], FX_CELL_IDX(key)); };
         auto fk = [&](int32_t key) { return (g2l[key >> 15] << 15) | (key & 32767); };
         FxProgram &g = plan.ghost;
         for (FxGop &o : g.cell_ops) {

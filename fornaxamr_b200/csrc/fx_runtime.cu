@@ -841,8 +841,8 @@ void child_groups(const FxAmrRefine &r, std::vector<FxPop> &out)
                 std::memset(&p, 0, sizeof(p));
                 p.fine = r.child;
                 p.coarse = r.parent;
-                p.pos = (f[0] + 2) | ((f[1] + 2) << 5) | ((f[2] + 2) << 10) | ((ci + 2) << 15) |
-                    ((cj + 2) << 20) | ((ck + 2) << 25);
+                p.pos = (f[0] + FX_NG) | ((f[1] + FX_NG) << 5) | ((f[2] + FX_NG) << 10) | ((ci + FX_NG) << 15) |
+                    ((cj + FX_NG) << 20) | ((ck + FX_NG) << 25);
                 for (int d = 0; d < 3; ++d) {
                     for (int side = 0; side < 2; ++side) {
                         const int x = f[d] + 2 * side;
@@ -893,6 +893,8 @@ void drop_adjoint(fx_ctx *c)
 
 extern "C" {
 
+int fx_ghost_layers(void) { return FX_NG; }
+
 int fx_create(int device, const fx_config *cfg, fx_ctx **out)
 {
     if (!cfg || !out) {
@@ -905,9 +907,12 @@ int fx_create(int device, const fx_config *cfg, fx_ctx **out)
     if (!(cfg->gamma > 0.0)) {
         return FX_EINVAL;
     }
-    if ((cfg->recon != FX_RECON_MC && cfg->recon != FX_RECON_WENO3) ||
+    if ((cfg->recon != FX_RECON_MC && cfg->recon != FX_RECON_WENO3 && cfg->recon != FX_RECON_WENO7) ||
         (cfg->integrator != FX_INT_RK2 && cfg->integrator != FX_INT_ESSPRK10_4)) {
         return FX_EINVAL;
+    }
+    if (cfg->recon == FX_RECON_WENO7 && FX_NG < 4) {
+        return FX_EINVAL; /* PRJ_RECON_WENO7 requires PRJ_NGHOST >= 4 (src/prj_defs.h:349-351) */
     }
     fx_ctx *c = new fx_ctx();
     c->device = device;

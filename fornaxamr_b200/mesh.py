@@ -19,8 +19,7 @@ import numpy as np
 
 from ._lib import FxBlockDesc
 
-BS = 16
-NG = 2
+from .layout import BS, NG  # noqa: E402  (block size, ghost layers of the loaded build)
 
 NEIGHBOR_NONE, NEIGHBOR_FACE, NEIGHBOR_EDGE, NEIGHBOR_CORNER = 0, 1, 2, 3
 

@@ -108,6 +108,9 @@ typedef struct fx_block_desc {
 /* reconstruction (PRJ_RECON_HYDRO, src/prj_defs.h:299-301) */
 #define FX_RECON_MC 0      /* PRJ_RECON_MC: monotonised-central slopes */
 #define FX_RECON_WENO3 1   /* PRJ_RECON_WENO3: WENO-Z3 face values (src/prj_reconstruct.h:383-423) */
+#define FX_RECON_WENO7 2   /* PRJ_RECON_WENO7: WENO-Z7 face values (src/prj_reconstruct.h:425-521);
+                              needs four ghost layers: the library built with FX_NG=4
+                              (libfornax_b200_ng4.so, 24^3 block arrays) */
 /* time integration (TIME_INTEGRATION, src/prj_defs.h:135-150) */
 #define FX_INT_RK2 0           /* RK2: two stages, block arrays with 2 stage slots */
 #define FX_INT_ESSPRK10_4 1    /* eSSPRK10_4 (the reference's default): ten forward-Euler
@@ -122,14 +125,22 @@ typedef struct fx_config {
     double coord[6];    /* domain: x1min, x1max, x2min, x2max, x3min, x3max (prj_coord) */
     int32_t bc[6];      /* x1 inner, x1 outer, x2 inner, x2 outer, x3 inner, x3 outer */
     double mhd_eta;     /* prj_mesh.mhd_eta */
-    int32_t recon;      /* FX_RECON_MC or FX_RECON_WENO3 */
+    int32_t recon;      /* FX_RECON_MC, FX_RECON_WENO3 or FX_RECON_WENO7 */
     int32_t integrator; /* FX_INT_RK2 or FX_INT_ESSPRK10_4 */
 } fx_config;
 
 /* ---- context -------------------------------------------------------------- */
 
+/* Ghost layers of this build (the reference's compile-time PRJ_NGHOST):
+ * 2 for libfornax_b200.so (20^3 block arrays), 4 for libfornax_b200_ng4.so
+ * (24^3, needed by FX_RECON_WENO7).  Every per-block size in this header
+ * (8000 cells, 8400 faces, 8820 edges) is that of the 2-layer build; the
+ * 4-layer build uses 13824, 14400 and 15000. */
+int fx_ghost_layers(void);
+
 /* Creates a context on `device`.  Replaces nothing: the reference has no
- * device; this owns the stream, the device mirror and the step graphs. */
+ * device; this owns the stream, the device mirror and the step graphs.
+ * FX_EINVAL for FX_RECON_WENO7 in the 2-layer build. */
 int fx_create(int device, const fx_config *cfg, fx_ctx **out);
 void fx_destroy(fx_ctx *ctx);
 int fx_last_error(const fx_ctx *ctx, char *buf, size_t len);

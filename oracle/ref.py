@@ -20,8 +20,10 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 REF_DIR = os.path.join(HERE, "_ref")
 
+# the process's ghost layers (FX_NGHOST, 2 or 4) select the reference builds
+# with the same PRJ_NGHOST
+NG = int(os.environ.get("FX_NGHOST", "2"))
 BS = 16
-NG = 2
 PBS = BS + 2 * NG
 NCELLS = PBS ** 3
 NFACES = (PBS + 1) * PBS * PBS
@@ -120,7 +122,14 @@ def amr_params(max_level: int, criteria, min_dx: float = 0.0, reach_density: flo
 
 
 def lib_path(mhd: bool, variant: str = "") -> str:
-    """variant: "" (RK2, MC), "weno3", "ess" (eSSPRK10_4), "ess_weno3"."""
+    """variant: "" (RK2, MC), "weno3", "ess" (eSSPRK10_4), "ess_weno3"; with
+    four ghost layers "" (MC, PRJ_NGHOST=4) or "weno7" (WENO-Z7)."""
+    if NG == 4 and variant not in ("", "weno7"):
+        raise ValueError(f"no four-ghost-layer reference build for variant {variant!r}")
+    if NG == 2 and variant == "weno7":
+        raise ValueError("WENO-Z7 needs four ghost layers (FX_NGHOST=4)")
+    if NG == 4 and not variant:
+        variant = "ng4"
     name = ("mhd" if mhd else "hydro") + ("_" + variant if variant else "")
     return os.path.join(REF_DIR, f"libprjref_{name}.so")
 
@@ -179,6 +188,8 @@ class Reference:
             L.rh_emf_upwind.restype = C.c_double
         self.nhydro = L.rh_nhydro()
         self.nstages = L.rh_nstages()
+        if L.rh_nghost() != NG:
+            raise RuntimeError(f"{path}: PRJ_NGHOST {L.rh_nghost()}, FX_NGHOST {NG}")
 
     # -- set-up and stepping ------------------------------------------------
     def setup(self, params: RhParams) -> None:

@@ -5,10 +5,11 @@ from __future__ import annotations
 
 import numpy as np
 
-BS, NG, PBS = 16, 2, 20
-NCELLS = PBS ** 3
-NFACES = 21 * 20 * 20
-NEDGES = 21 * 21 * 20
+from fornaxamr_b200.layout import BS, NCELLS, NEDGES, NFACES, NG, PBS  # noqa: E402
+
+# cell keys of the compiled programs: (block << CELL_BITS) | cell
+CELL_BITS = 13 if NCELLS <= 8192 else 14
+CELL_MASK = (1 << CELL_BITS) - 1
 
 GOP_COPY, GOP_COPY_NEG, GOP_COPY_USER, GOP_RESTRICT, GOP_PROLONG = 0, 1, 2, 3, 4
 FOP_COPY, FOP_RESTRICT, FOP_PROLONG = 8, 9, 10
@@ -97,8 +98,8 @@ def apply_cell_program(W, ops, waves, slot, nvg):
         o = ops[waves[w]:waves[w + 1]]
         for t in np.unique(o[:, 3]):
             s = o[o[:, 3] == t]
-            db, dc = s[:, 0] >> 13, s[:, 0] & 8191
-            sb, sc = s[:, 1] >> 13, s[:, 1] & 8191
+            db, dc = s[:, 0] >> CELL_BITS, s[:, 0] & CELL_MASK
+            sb, sc = s[:, 1] >> CELL_BITS, s[:, 1] & CELL_MASK
             if t in (GOP_COPY, GOP_COPY_NEG, GOP_COPY_USER):
                 vals = W[sb, :nvg, slot, sc].copy()
                 if t == GOP_COPY_NEG:
@@ -115,13 +116,13 @@ def apply_cell_program(W, ops, waves, slot, nvg):
                 def q(off):
                     return W[sb[:, None], np.arange(nvg)[None, :], slot, (sc + off)[:, None]]
                 base = q(0)
-                vx = base + minmod(q(-400), base, q(400)) * tx
-                vy = base + minmod(q(-20), base, q(20)) * ty
+                vx = base + minmod(q(-PBS * PBS), base, q(PBS * PBS)) * tx
+                vy = base + minmod(q(-PBS), base, q(PBS)) * ty
                 vz = base + minmod(q(-1), base, q(1)) * tz
                 W[db[:, None], np.arange(nvg)[None, :], slot, dc[:, None]] = vx + vy + vz - 2.0 * base
             elif t == GOP_RESTRICT:
                 acc = None
-                for off in (0, 1, 20, 21, 400, 401, 420, 421):
+                for off in (0, 1, PBS, PBS + 1, PBS * PBS, PBS * PBS + 1, PBS * PBS + PBS, PBS * PBS + PBS + 1):
                     v = W[sb, :nvg, slot, sc + off]
                     acc = v if acc is None else acc + v
                 W[db, :nvg, slot, dc] = 0.125 * acc
@@ -170,8 +171,8 @@ def apply_prolong_groups(Bf, pops, slot, dx):
     fine, coarse, pos = pops[:, 0], pops[:, 1], pops[:, 2].astype(np.int64)
     keep, ow, iw = pops[:, 3].astype(np.int64), pops[:, 4].astype(np.int64), pops[:, 5].astype(np.int64)
     f0 = [(pos >> (5 * a)) & 31 for a in range(3)]
-    f0 = [x - 2 for x in f0]
-    c0 = [((pos >> (15 + 5 * a)) & 31) - 2 for a in range(3)]
+    f0 = [x - NG for x in f0]
+    c0 = [((pos >> (15 + 5 * a)) & 31) - NG for a in range(3)]
     fdx = dx[fine]
     area = [fdx[:, 1] * fdx[:, 2], fdx[:, 0] * fdx[:, 2], fdx[:, 0] * fdx[:, 1]]
     o = {}
@@ -246,7 +247,7 @@ def apply_b_ops(W, Bf, bops, slot):
     """cell-field operations: W[6+d] of dst = 0.5 (f[2d] + f[2d+1])."""
     if len(bops) == 0:
         return
-    db, dc = bops[:, 0] >> 13, bops[:, 0] & 8191
+    db, dc = bops[:, 0] >> CELL_BITS, bops[:, 0] & CELL_MASK
     for d in range(3):
         k0, k1 = bops[:, 1 + 2 * d], bops[:, 2 + 2 * d]
         W[db, 6 + d, slot, dc] = 0.5 * (Bf[k0 >> 15, d, slot, k0 & 32767] + Bf[k1 >> 15, d, slot, k1 & 32767])
@@ -307,7 +308,7 @@ def bf2bc(W, Bf, slot):
 
 
 def ref_state(ref):
-    """W [nb, nv, 2, 8000] and Bf [nb, 3, 2, 8400] of every block entry;
+    """W [nb, nv, ns, NCELLS] and Bf [nb, 3, ns, NFACES] of every block entry;
     entries without storage (freed by a coarsening) read as zeros."""
     nb = ref.nblocks()
     ns = ref.nstages

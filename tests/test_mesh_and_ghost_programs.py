@@ -118,9 +118,9 @@ def test_ghost_compiler_statistics(ref_mhd):
     bops, _ = fx.plan_export(cfg, desc, 4)
     assert rewired > 0 and dead > 0
     assert len(cops) + len(fops) == emitted_cells + emitted_faces - dead
-    # every ghost cell of every block written once (8 blocks x (20^3 - 16^3))
-    assert len(np.unique(cops[:, 0])) == len(cops) == 8 * (20 ** 3 - 16 ** 3)
-    assert len(bops) == 8 * (20 ** 3 - 16 ** 3)
+    # every ghost cell of every block written once (8 blocks x (PBS^3 - 16^3))
+    assert len(np.unique(cops[:, 0])) == len(cops) == 8 * (H.PBS ** 3 - 16 ** 3)
+    assert len(bops) == 8 * (H.PBS ** 3 - 16 ** 3)
 
 
 # static AMR hierarchies of the magnetised blast: (root, radii) -> per-level
