@@ -65,6 +65,8 @@ def parse():
                     help="batched steps of the static-AMR blast measurement (0: skip it)")
     ap.add_argument("--collapse", action="store_true",
                     help="also measure the 4-level gravity collapse (about 4600 blocks; slow set-up)")
+    ap.add_argument("--weno7-child", action="store_true",
+                    help="internal: the WENO-Z7 measurement, run in a child process with FX_NGHOST=4")
     ap.add_argument("--shard", action="store_true",
                     help="N > 1: one mesh of N x 512 blocks sharded over the ranks (NCCL exchanges of ghost "
                          "zones and dt minima) instead of N independent replicas")
@@ -402,8 +404,11 @@ def run_variants(args, dev, cpu):
     blocks = mesh.uniform_mesh((ROOT, ROOT, ROOT), coord)
     W0, Bf0 = problems.fourier_mhd(blocks)
     out = {}
-    for name, recon, integ in (("weno3", fx.RECON_WENO3, fx.INT_RK2), ("ess", fx.RECON_MC, fx.INT_ESSPRK10_4),
-                               ("ess_weno3", fx.RECON_WENO3, fx.INT_ESSPRK10_4)):
+    variants = (("weno3", fx.RECON_WENO3, fx.INT_RK2), ("ess", fx.RECON_MC, fx.INT_ESSPRK10_4),
+                ("ess_weno3", fx.RECON_WENO3, fx.INT_ESSPRK10_4))
+    if fx.NG == 4:
+        variants = (("mc_4ghost", fx.RECON_MC, fx.INT_RK2), ("weno7", fx.RECON_WENO7, fx.INT_RK2))
+    for name, recon, integ in variants:
         ctx = fx.Context(True, 5.0 / 3.0, coord, device=dev, recon=recon, integrator=integ)
         ctx.set_mesh(mesh.to_desc(blocks))
         ns = ctx.ns
@@ -432,6 +437,31 @@ def run_variants(args, dev, cpu):
             out[name]["cpu_reference_1core"] = cpu[name]
         ctx.close()
     return out
+
+
+def run_weno7(args):
+    """WENO-Z7 needs the four-ghost-layer build, which a process selects at
+    start (FX_NGHOST=4): a child process measures it (and MC on the same
+    24^3 layout) on the headline workload, plus one core of the reference
+    built with WENO-Z7 on a 2^3-block instance."""
+    env = dict(os.environ, FX_NGHOST="4")
+    cmd = [sys.executable, os.path.abspath(__file__), "--weno7-child", "--warmup", str(args.warmup)]
+    if args.no_cpu_baseline:
+        cmd.append("--no-cpu-baseline")
+    r = subprocess.run(cmd, env=env, capture_output=True, text=True, timeout=1200)
+    if r.returncode != 0:
+        return {"unavailable": (r.stderr or r.stdout).strip().splitlines()[-1:]}
+    return json.loads(r.stdout.strip().splitlines()[-1])
+
+
+def weno7_child(args):
+    cpu = None
+    if not args.no_cpu_baseline:
+        ctx = mp.get_context("spawn")
+        with ctx.Pool(1) as pool:
+            res = pool.map(_cpu_variant_worker, ["weno7"])
+        cpu = {v: {"value": x, "unit": UNIT, "cores": 1} for v, x in res}
+    return run_variants(args, 0, cpu)
 
 
 def run_adjoint(args, dev):
@@ -698,6 +728,10 @@ def main():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
 
+    if args.weno7_child:
+        print(json.dumps(weno7_child(args)))
+        return 0
+
     if args.impl == "reference":
         if rank != 0:
             return 0
@@ -758,6 +792,7 @@ def main():
         line["adjoint"] = run_adjoint(args, local_rank)
     if world == 1 and args.variants:
         line["variants"] = run_variants(args, local_rank, cv)
+        line["variants"].update(run_weno7(args))
     if world == 1 and args.amr_steps > 0:
         line["amr_blast"] = run_amr(args, local_rank, "blast")
         if args.collapse:

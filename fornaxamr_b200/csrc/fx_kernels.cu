@@ -1355,10 +1355,26 @@ static void launch_flux_shape(const FxDev &D, const int *blist, int nlist, int n
     k_flux<MHD, FULL, TPB, MINB, RECON><<<g, TPB, 0, s>>>(D, blist, wslot, bfslot);
 }
 
-/* WENO-Z3 and WENO-Z7 are compiled in one launch shape (the autotuner's
- * variants all map to it); MC in all of them.  WENO-Z7 reads three cells
- * beyond each face's neighbours and exists in the four-ghost-layer build
- * only (the context rejects it elsewhere). */
+/* the autotuner's launch shapes (threads per CTA, minimum CTAs per SM) */
+template <bool MHD, bool FULL, int RECON>
+static void launch_flux_shapes(const FxDev &D, const int *blist, int nlist, int ndir, int wslot,
+    int bfslot, int variant, cudaStream_t s)
+{
+    switch (variant) {
+    case 1: launch_flux_shape<MHD, FULL, 128, 5, RECON>(D, blist, nlist, ndir, wslot, bfslot, s); break;
+    case 2: launch_flux_shape<MHD, FULL, 128, 6, RECON>(D, blist, nlist, ndir, wslot, bfslot, s); break;
+    case 3: launch_flux_shape<MHD, FULL, 256, 2, RECON>(D, blist, nlist, ndir, wslot, bfslot, s); break;
+    case 4: launch_flux_shape<MHD, FULL, 256, 3, RECON>(D, blist, nlist, ndir, wslot, bfslot, s); break;
+    case 5: launch_flux_shape<MHD, FULL, 64, 8, RECON>(D, blist, nlist, ndir, wslot, bfslot, s); break;
+    default: launch_flux_shape<MHD, FULL, 128, 4, RECON>(D, blist, nlist, ndir, wslot, bfslot, s); break;
+    }
+}
+
+/* MC and WENO-Z7 are compiled in every launch shape; WENO-Z3 in one (the
+ * autotuner's variants all map to it).  WENO-Z7 reads three cells beyond
+ * each face's neighbours and exists in the four-ghost-layer build only (the
+ * context rejects it elsewhere); its register demand (about 180 per thread
+ * unbounded) makes the shape matter. */
 template <bool MHD, bool FULL>
 static void launch_flux_variant(const FxDev &D, const int *blist, int nlist, int ndir, int wslot,
     int bfslot, int variant, cudaStream_t s)
@@ -1369,18 +1385,11 @@ static void launch_flux_variant(const FxDev &D, const int *blist, int nlist, int
     }
 #if FX_NG >= 4
     if (D.recon == FX_RECON_WENO7) {
-        launch_flux_shape<MHD, FULL, 128, 2, FX_RECON_WENO7>(D, blist, nlist, ndir, wslot, bfslot, s);
+        launch_flux_shapes<MHD, FULL, FX_RECON_WENO7>(D, blist, nlist, ndir, wslot, bfslot, variant, s);
         return;
     }
 #endif
-    switch (variant) {
-    case 1: launch_flux_shape<MHD, FULL, 128, 5>(D, blist, nlist, ndir, wslot, bfslot, s); break;
-    case 2: launch_flux_shape<MHD, FULL, 128, 6>(D, blist, nlist, ndir, wslot, bfslot, s); break;
-    case 3: launch_flux_shape<MHD, FULL, 256, 2>(D, blist, nlist, ndir, wslot, bfslot, s); break;
-    case 4: launch_flux_shape<MHD, FULL, 256, 3>(D, blist, nlist, ndir, wslot, bfslot, s); break;
-    case 5: launch_flux_shape<MHD, FULL, 64, 8>(D, blist, nlist, ndir, wslot, bfslot, s); break;
-    default: launch_flux_shape<MHD, FULL, 128, 4>(D, blist, nlist, ndir, wslot, bfslot, s); break;
-    }
+    launch_flux_shapes<MHD, FULL, FX_RECON_MC>(D, blist, nlist, ndir, wslot, bfslot, variant, s);
 }
 
 void fx_launch_flux(const FxDev &D, const int *blist, int nlist, int ndir, int wslot, int bfslot,

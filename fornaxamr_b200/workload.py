@@ -3,7 +3,7 @@ cases the kernel profiles are taken on).
 
     python -m fornaxamr_b200.workload [--problem fourier|blast|collapse]
         [--root R] [--steps N] [--form batched|plain] [--adjoint N] [--shape S]
-        [--amr-interval K [--max-level L]] [--variant rk2|weno3|ess|ess_weno3]
+        [--amr-interval K [--max-level L]] [--variant rk2|weno3|ess|ess_weno3|weno7]
 
 fourier: uniform root^3 mesh of 16^3 blocks on [0,1]^3 with the seeded
 Fourier-mode MHD state (fornaxamr_b200.problems.fourier_mhd).
@@ -17,7 +17,8 @@ and prints the time per step.  With --amr-interval K the mesh adapts every K
 steps (prj_amr_adapt with a Loehner pressure criterion, refine 0.3 /
 derefine 0.1, up to level L, default 3) and the adapt phases are printed.
 --variant selects the reference build variant: WENO-Z3 reconstruction
-(weno3), the eSSPRK10_4 integrator (ess) or both (ess_weno3).  With --adjoint N (fourier only, amplitude
+(weno3), the eSSPRK10_4 integrator (ess) or both (ess_weno3), or WENO-Z7
+(weno7; run the process with FX_NGHOST=4, the four-ghost-layer build).  With --adjoint N (fourier only, amplitude
 0.01, |k| <= 3) it runs N fixed-dt steps storing every stage, then one
 reverse sweep, and prints the reverse sweep's device time per step.
 """
@@ -39,7 +40,7 @@ def main():
     ap.add_argument("--adjoint", type=int, default=0)
     ap.add_argument("--shape", type=int, default=-1, help="force a face-kernel launch shape (fx_set_flux_shape)")
     ap.add_argument("--amr-interval", type=int, default=0)
-    ap.add_argument("--variant", default="rk2", choices=["rk2", "weno3", "ess", "ess_weno3"])
+    ap.add_argument("--variant", default="rk2", choices=["rk2", "weno3", "ess", "ess_weno3", "weno7"])
     ap.add_argument("--max-level", type=int, default=3)
     args = ap.parse_args()
     if args.variant != "rk2" and args.problem == "collapse":
@@ -74,7 +75,8 @@ def main():
             gamma = 4.0 / 3.0
             gravity = True
             W, Bf, grav = problems.collapse(blocks, recs, half_width=hw)
-    recon = fx.RECON_WENO3 if "weno3" in args.variant else fx.RECON_MC
+    recon = fx.RECON_WENO3 if "weno3" in args.variant else fx.RECON_WENO7 if args.variant == "weno7" \
+        else fx.RECON_MC
     integ = fx.INT_ESSPRK10_4 if args.variant.startswith("ess") else fx.INT_RK2
     ctx = fx.Context(True, gamma, coord, gravity=gravity, recon=recon, integrator=integ)
     ctx.set_mesh(mesh.to_desc(blocks))

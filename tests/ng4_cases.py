@@ -109,3 +109,23 @@ def test_weno7_face_value_matches_reference_on_random_stencils():
 def test_weno7_context_needs_four_ghosts_build():
     cfg = fx.make_config(True, 5.0 / 3.0, (0, 1, 0, 1, 0, 1), recon=fx.RECON_WENO7)
     assert cfg.recon == fx.RECON_WENO7
+
+
+@pytest.mark.gpu
+def test_weno7_every_launch_shape_matches_reference():
+    """the autotuner's six launch shapes of the WENO-Z7 face kernel (register
+    caps from 80 to 128, some with spills) give the same bits"""
+    ref = R.Reference(True, "weno7")
+    p = R.params_fourier(root=2, nmodes=16, kmax=3, amp_rho=0.3)
+    ref.setup(p)
+    ctxs = []
+    for v in range(6):
+        ctx = make_ctx(ref, p, True, fx.RECON_WENO7)
+        ctx.set_flux_shape(v)
+        ctxs.append(ctx)
+    n, t_ref, dt_ref, st_ref = ref.run(2)
+    for ctx in ctxs:
+        t, dt, st = ctx.run(fx.FORM_BATCHED, 2, p.cfl, p.dt_factor, p.t_end, (0.0, 0.0, 0.0))
+        assert (t, dt, st) == (t_ref, dt_ref, st_ref)
+        assert_state_equal(ctx, ref, True)
+        ctx.close()
