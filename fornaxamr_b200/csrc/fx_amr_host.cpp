@@ -6,6 +6,7 @@
  * moved by the device kernels of fx_amr.cu from the job lists built here.
  */
 #include "fx_amr.h"
+#include "fx_layout.h"
 
 #include <algorithm>
 #include <cmath>
@@ -15,8 +16,8 @@
 
 namespace {
 
-constexpr int kBS = 16;
-constexpr int kNG = 2;
+constexpr int kBS = FX_BS;
+constexpr int kNG = FX_NG; /* PRJ_NGHOST of the build: the slots' send / recv boxes depend on it */
 constexpr double kTol = 1.0e-12;
 
 enum { NB_NONE = 0, NB_FACE = 1, NB_EDGE = 2, NB_CORNER = 3 };

@@ -129,3 +129,43 @@ def test_weno7_every_launch_shape_matches_reference():
         assert (t, dt, st) == (t_ref, dt_ref, st_ref)
         assert_state_equal(ctx, ref, True)
         ctx.close()
+
+
+def _amr(ctx, ref, p, crit, max_level):
+    ctx.amr_configure(fx.amr_config(tuple(p.root), max_level, [crit]))
+    ref.amr_configure(R.amr_params(max_level, [dict(estimator=crit["estimator"], refine=crit["refine"],
+                                                    derefine=crit["derefine"], lohner_var=crit.get("var", 1),
+                                                    jump_var=min(crit.get("var", 1), 1),
+                                                    eps=crit.get("eps", 0.1))]))
+
+
+def _mesh_equal(ctx, ref):
+    from fornaxamr_b200 import mesh
+    i2, g2, s2 = ref.mesh_arrays()
+    mi, mg, ms = mesh.desc_to_arrays(ctx.get_mesh())
+    assert np.array_equal(i2, mi) and np.array_equal(g2, mg) and np.array_equal(s2, ms)
+
+
+@pytest.mark.gpu
+def test_dynamic_amr_weno7_matches_reference():
+    """prj_amr_adapt on the four-ghost layout: device tag votes, host remesh
+    (slot boxes of four ghost layers), prolongation and restriction of cells
+    and faces, recompiled fill; refine, step, then coarsen"""
+    ref = R.Reference(True, "weno7")
+    p = R.params_amr_blast(root=2, max_level=1, radii=(0.4,))
+    ref.setup(p)
+    _, t0, dt0, st0 = ref.run(2)
+    ctx = make_ctx(ref, p, True, fx.RECON_WENO7)
+    _amr(ctx, ref, p, dict(estimator=fx.AMR_LOEHNER, refine=0.3, derefine=0.1, var=1), 2)
+    assert np.array_equal(ctx.amr_tag(), ref.amr_tag())
+    assert ctx.amr_adapt() == bool(ref.amr_adapt()) is True
+    _mesh_equal(ctx, ref)
+    assert_state_equal(ctx, ref, True, active_only=True)
+    n, t_ref, dt_ref, st_ref = ref.run(1)
+    t, dt, st = ctx.run(fx.FORM_BATCHED, 1, p.cfl, p.dt_factor, p.t_end, (t0, dt0, st0))
+    assert (t, dt, st) == (t_ref, dt_ref, st_ref)
+    _amr(ctx, ref, p, dict(estimator=fx.AMR_LOEHNER, refine=100.0, derefine=100.0, var=1), 2)
+    assert ctx.amr_adapt() == bool(ref.amr_adapt()) is True
+    _mesh_equal(ctx, ref)
+    assert_state_equal(ctx, ref, True, active_only=True)
+    ctx.close()
