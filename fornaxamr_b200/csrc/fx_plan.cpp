@@ -1584,69 +1584,82 @@ private:
         const uint16_t rbit = (uint16_t)(1u << rank_);
         auto keep = [&](int x) { return opwave[x] >= 0 && (!owner_ || (need_[x] & rbit)); };
         /* 5. per-wave arrays: a counting sort of the operations by (wave,
-         * type), replay order kept within a bucket (the replay visits each
-         * destination box in storage order) */
+         * type) -- faces by (wave, type, direction), so a warp's stores land
+         * in one direction's array -- replay order kept within a bucket (the
+         * replay visits each destination box in storage order).  Threads
+         * count and place contiguous ranges of the sequence; bucket-major,
+         * thread-minor offsets keep the serial order. */
         FxProgram &g = plan.ghost;
-        constexpr int NT = 16; /* op type values are below 16 */
-        std::vector<int> nc((size_t)nwaves * NT + 1, 0), nf((size_t)nwaves * NT + 1, 0), np(nwaves + 1, 0);
-        for (int x = 0; x < nseq; ++x) {
-            if (!keep(x)) continue;
-            const SeqOp &o = seq_[x];
-            if (o.space == SPACE_CELL) ++nc[(size_t)opwave[x] * NT + o.op.type + 1];
-            else if (o.space == SPACE_FACE) ++nf[(size_t)opwave[x] * NT + o.op.type + 1];
-            else ++np[opwave[x] + 1];
-        }
-        for (size_t q = 0; q + 1 < nc.size(); ++q) {
-            nc[q + 1] += nc[q];
-            nf[q + 1] += nf[q];
-        }
-        for (int w = 0; w < nwaves; ++w) np[w + 1] += np[w];
-        g.cell_ops.resize(nc.back());
-        g.face_ops.resize(nf.back());
-        g.p_ops.resize(np[nwaves]);
+        constexpr int NT = 16;      /* op type values are below 16 */
+        constexpr int NTF = 3 * NT; /* faces: (type, direction) */
+        const size_t KC = (size_t)nwaves * NT, KF = (size_t)nwaves * NTF, KP = (size_t)nwaves;
+        const int nts = compile_threads();
+        auto seq_lo = [&](int t) { return (int)((int64_t)nseq * t / nts); };
+        auto ckey = [&](const SeqOp &o, int x) { return (size_t)opwave[x] * NT + o.op.type; };
+        auto fkey = [&](const SeqOp &o, int x) {
+            return (size_t)opwave[x] * NTF + (size_t)o.op.type * 3 + (o.op.aux & 3);
+        };
+        std::vector<std::vector<int>> tcnt_c(nts, std::vector<int>(KC, 0));
+        std::vector<std::vector<int>> tcnt_f(nts, std::vector<int>(KF, 0));
+        std::vector<std::vector<int>> tcnt_p(nts, std::vector<int>(KP, 0));
+        parallel_for(nts, [&](int t) {
+            for (int x = seq_lo(t); x < seq_lo(t + 1); ++x) {
+                if (!keep(x)) continue;
+                const SeqOp &o = seq_[x];
+                if (o.space == SPACE_CELL) ++tcnt_c[t][ckey(o, x)];
+                else if (o.space == SPACE_FACE) ++tcnt_f[t][fkey(o, x)];
+                else ++tcnt_p[t][opwave[x]];
+            }
+        });
+        /* bucket starts; per-thread counts become per-thread write cursors */
+        auto offsets = [&](std::vector<std::vector<int>> &tc, size_t K) {
+            std::vector<int> start(K + 1);
+            int run = 0;
+            for (size_t k = 0; k < K; ++k) {
+                start[k] = run;
+                for (int t = 0; t < nts; ++t) {
+                    const int n = tc[t][k];
+                    tc[t][k] = run;
+                    run += n;
+                }
+            }
+            start[K] = run;
+            return start;
+        };
+        const std::vector<int> bc = offsets(tcnt_c, KC);
+        const std::vector<int> bf = offsets(tcnt_f, KF);
+        const std::vector<int> bp = offsets(tcnt_p, KP);
+        g.cell_ops.resize(bc[KC]);
+        g.face_ops.resize(bf[KF]);
+        g.p_ops.resize(bp[KP]);
         g.cell_begin.resize(nwaves + 1);
         g.face_begin.resize(nwaves + 1);
+        g.p_begin.resize(nwaves + 1);
         for (int w = 0; w <= nwaves; ++w) {
-            g.cell_begin[w] = nc[(size_t)w * NT];
-            g.face_begin[w] = nf[(size_t)w * NT];
+            g.cell_begin[w] = bc[(size_t)w * NT];
+            g.face_begin[w] = bf[(size_t)w * NTF];
+            g.p_begin[w] = bp[(size_t)w];
         }
-        g.p_begin.assign(np.begin(), np.end());
-        for (int x = 0; x < nseq; ++x) {
-            if (!keep(x)) continue;
-            const SeqOp &o = seq_[x];
-            if (o.space == SPACE_CELL) g.cell_ops[nc[(size_t)opwave[x] * NT + o.op.type]++] = o.op;
-            else if (o.space == SPACE_FACE) g.face_ops[nf[(size_t)opwave[x] * NT + o.op.type]++] = o.op;
-            else g.p_ops[np[opwave[x]]++] = groups_[o.op.dst];
-        }
-        /* within a (wave, type) bucket, destination order: neighbouring
-         * threads of the fill kernel then store to neighbouring addresses */
+        parallel_for(nts, [&](int t) {
+            for (int x = seq_lo(t); x < seq_lo(t + 1); ++x) {
+                if (!keep(x)) continue;
+                const SeqOp &o = seq_[x];
+                if (o.space == SPACE_CELL) g.cell_ops[tcnt_c[t][ckey(o, x)]++] = o.op;
+                else if (o.space == SPACE_FACE) g.face_ops[tcnt_f[t][fkey(o, x)]++] = o.op;
+                else g.p_ops[tcnt_p[t][opwave[x]]++] = groups_[o.op.dst];
+            }
+        });
+        /* within a bucket, destination order: neighbouring threads of the
+         * fill kernel then store to neighbouring addresses */
         {
             std::vector<std::pair<FxGop *, size_t>> buckets;
-            for (size_t q = 0; q + 1 < nc.size(); ++q) {
-                const int lo = q == 0 ? 0 : nc[q - 1];
-                if (nc[q] > lo) buckets.emplace_back(g.cell_ops.data() + lo, (size_t)(nc[q] - lo));
+            for (size_t k = 0; k < KC; ++k) {
+                if (bc[k + 1] > bc[k]) buckets.emplace_back(g.cell_ops.data() + bc[k], (size_t)(bc[k + 1] - bc[k]));
             }
-            for (size_t q = 0; q + 1 < nf.size(); ++q) {
-                const int lo = q == 0 ? 0 : nf[q - 1];
-                if (nf[q] > lo) buckets.emplace_back(g.face_ops.data() + lo, (size_t)(nf[q] - lo));
+            for (size_t k = 0; k < KF; ++k) {
+                if (bf[k + 1] > bf[k]) buckets.emplace_back(g.face_ops.data() + bf[k], (size_t)(bf[k + 1] - bf[k]));
             }
-            const int nt = compile_threads();
-            for (const auto &bk : buckets) sort_by_dst(bk.first, bk.second, nt);
-            /* face operations: direction-major (stable), so a warp's stores
-             * land in one direction's array and consecutive faces form runs */
-            std::vector<FxGop> tmp;
-            for (size_t q = 0; q + 1 < nf.size(); ++q) {
-                const int lo = q == 0 ? 0 : nf[q - 1];
-                const size_t n = (size_t)(nf[q] - lo);
-                if (n < 2) continue;
-                FxGop *ops = g.face_ops.data() + lo;
-                size_t cnt[4] = {0, 0, 0, 0};
-                for (size_t e = 0; e < n; ++e) ++cnt[(ops[e].aux & 3) + 1];
-                for (int d = 0; d < 3; ++d) cnt[d + 1] += cnt[d];
-                tmp.resize(n);
-                for (size_t e = 0; e < n; ++e) tmp[cnt[ops[e].aux & 3]++] = ops[e];
-                std::copy(tmp.begin(), tmp.end(), ops);
-            }
+            for (const auto &bk : buckets) sort_by_dst(bk.first, bk.second, nts);
         }
         g.b_ops.swap(bops_all);
         g.b_begin.assign(1, 0);
