@@ -123,10 +123,10 @@ def amr_params(max_level: int, criteria, min_dx: float = 0.0, reach_density: flo
 
 def lib_path(mhd: bool, variant: str = "") -> str:
     """variant: "" (RK2, MC), "weno3", "ess" (eSSPRK10_4), "ess_weno3"; with
-    four ghost layers "" (MC, PRJ_NGHOST=4) or "weno7" (WENO-Z7)."""
-    if NG == 4 and variant not in ("", "weno7"):
+    four ghost layers "" (MC, PRJ_NGHOST=4), "weno7" (WENO-Z7) or "ess_weno7"."""
+    if NG == 4 and variant not in ("", "weno7", "ess_weno7"):
         raise ValueError(f"no four-ghost-layer reference build for variant {variant!r}")
-    if NG == 2 and variant == "weno7":
+    if NG == 2 and variant.endswith("weno7"):
         raise ValueError("WENO-Z7 needs four ghost layers (FX_NGHOST=4)")
     if NG == 4 and not variant:
         variant = "ng4"

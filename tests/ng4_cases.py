@@ -169,3 +169,25 @@ def test_dynamic_amr_weno7_matches_reference():
     _mesh_equal(ctx, ref)
     assert_state_equal(ctx, ref, True, active_only=True)
     ctx.close()
+
+
+@pytest.mark.gpu
+def test_essprk_weno7_matches_reference():
+    """the reference's default integrator (eSSPRK10_4, three stage slots)
+    with WENO-Z7, both forms' batched path on the Fourier workload"""
+    ref = R.Reference(True, "ess_weno7")
+    p = R.params_fourier(root=2)
+    ref.setup(p)
+    desc = H.ref_desc(ref)
+    coord = [p.xmin[0], p.xmax[0], p.xmin[1], p.xmax[1], p.xmin[2], p.xmax[2]]
+    ctx = fx.Context(True, p.gamma, coord, bc=tuple(p.bc), recon=fx.RECON_WENO7, integrator=fx.INT_ESSPRK10_4)
+    ctx.set_mesh(desc)
+    W, Bf = H.ref_state(ref)
+    for b in range(W.shape[0]):
+        ctx.upload_block(b, W[b].ravel(), [Bf[b, d].ravel() for d in range(3)])
+    assert ctx.calc_dt(p.cfl) == ref.calc_dt()
+    n, t_ref, dt_ref, st_ref = ref.run(2)
+    t, dt, st = ctx.run(fx.FORM_BATCHED, 2, p.cfl, p.dt_factor, p.t_end, (0.0, 0.0, 0.0))
+    assert (t, dt, st) == (t_ref, dt_ref, st_ref)
+    assert_state_equal(ctx, ref, True)
+    ctx.close()
