@@ -1370,17 +1370,16 @@ static void launch_flux_shapes(const FxDev &D, const int *blist, int nlist, int 
     }
 }
 
-/* MC and WENO-Z7 are compiled in every launch shape; WENO-Z3 in one (the
- * autotuner's variants all map to it).  WENO-Z7 reads three cells beyond
- * each face's neighbours and exists in the four-ghost-layer build only (the
- * context rejects it elsewhere); its register demand (about 180 per thread
- * unbounded) makes the shape matter. */
+/* Every reconstruction is compiled in every launch shape.  WENO-Z7 reads
+ * three cells beyond each face's neighbours and exists in the
+ * four-ghost-layer build only (the context rejects it elsewhere); its
+ * register demand (about 180 per thread unbounded) makes the shape matter. */
 template <bool MHD, bool FULL>
 static void launch_flux_variant(const FxDev &D, const int *blist, int nlist, int ndir, int wslot,
     int bfslot, int variant, cudaStream_t s)
 {
     if (D.recon == FX_RECON_WENO3) {
-        launch_flux_shape<MHD, FULL, 128, 4, FX_RECON_WENO3>(D, blist, nlist, ndir, wslot, bfslot, s);
+        launch_flux_shapes<MHD, FULL, FX_RECON_WENO3>(D, blist, nlist, ndir, wslot, bfslot, variant, s);
         return;
     }
 #if FX_NG >= 4

@@ -107,3 +107,22 @@ def test_dynamic_amr_with_ess_matches_reference():
     assert state == (t_ref, dt_ref, st_ref)
     assert_state_equal(ctx, ref, True, active_only=True)
     ctx.close()
+
+
+def test_weno3_every_launch_shape_matches_reference():
+    """the autotuner's six launch shapes of the WENO-Z3 face kernel give the
+    same bits"""
+    ref = R.Reference(True, "weno3")
+    p = R.params_fourier(root=2, nmodes=16, kmax=3, amp_rho=0.3)
+    ref.setup(p)
+    ctxs = []
+    for v in range(6):
+        ctx = make_ctx(ref, p, True, "weno3")
+        ctx.set_flux_shape(v)
+        ctxs.append(ctx)
+    n, t_ref, dt_ref, st_ref = ref.run(2)
+    for ctx in ctxs:
+        t, dt, st = ctx.run(fx.FORM_BATCHED, 2, p.cfl, p.dt_factor, p.t_end, (0.0, 0.0, 0.0))
+        assert (t, dt, st) == (t_ref, dt_ref, st_ref)
+        assert_state_equal(ctx, ref, True)
+        ctx.close()
