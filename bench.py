@@ -710,7 +710,7 @@ def run_fx(args, rank, world, local_rank):
             "kernel": "k_flux (face fluxes, three directions, all blocks)",
             "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
             "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
-            "note": "FP64 HLLD issue rate bounds this kernel before HBM (see DESIGN.md)",
+            "note": "FP64 HLLD issue rate bounds this kernel before HBM (FP64 pipe 53 % busy, profiles/k_flux_fourier216.md)",
         },
         "e2e": None if e2e_ms is None else {
             "value": world * ZONES / (e2e_ms * 1e-3), "unit": UNIT,

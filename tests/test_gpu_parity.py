@@ -5,7 +5,7 @@ with the same dt sequence, and every block array is compared.
 
 Tolerance: the kernels evaluate the reference's double operations in the
 same order with no contraction, so agreement is expected to be bit for bit;
-the asserted bound is the north-star 1e-12 relative (per array, relative to
+the asserted bound is the required 1e-12 relative (per array, relative to
 its max magnitude), and bit equality is asserted where it holds by design.
 """
 import numpy as np
