@@ -191,3 +191,52 @@ def test_essprk_weno7_matches_reference():
     assert (t, dt, st) == (t_ref, dt_ref, st_ref)
     assert_state_equal(ctx, ref, True)
     ctx.close()
+
+
+@pytest.mark.gpu
+def test_sharded_weno7_on_emulated_ranks_matches_reference():
+    """a mesh sharded over three ranks (contexts of one process on one GPU)
+    on the four-ghost layout with WENO-Z7: halo exchanges of four ghost
+    layers and the wider stencil"""
+    import threading
+    ref = R.Reference(True, "weno7")
+    p = R.params_amr_blast(root=3, radii=(0.25, 0.1))
+    ref.setup(p)
+    desc = H.ref_desc(ref)
+    nranks = 3
+    owner = fx.morton_owner(desc, nranks)
+    coord = [p.xmin[0], p.xmax[0], p.xmin[1], p.xmax[1], p.xmin[2], p.xmax[2]]
+    W, Bf = H.ref_state(ref)
+    group = fx.ShardGroup(nranks)
+    ctxs = []
+    for r in range(nranks):
+        ctx = fx.Context(True, p.gamma, coord, bc=tuple(p.bc), recon=fx.RECON_WENO7)
+        ctx.shard_set_mesh(desc, owner, nranks, r)
+        ctx.attach_group(group)
+        for b in np.nonzero(owner == r)[0]:
+            ctx.upload_block(int(b), W[b].ravel(), [Bf[b, d].ravel() for d in range(3)])
+        ctxs.append(ctx)
+    out, err = [None] * nranks, []
+
+    def work(r):
+        try:
+            out[r] = ctxs[r].run(fx.FORM_BATCHED, 2, p.cfl, p.dt_factor, p.t_end, (0.0, 0.0, 0.0))
+        except Exception as e:
+            err.append(e)
+    threads = [threading.Thread(target=work, args=(r,)) for r in range(nranks)]
+    for t in threads:
+        t.start()
+    for t in threads:
+        t.join(timeout=600)
+    assert not err, err
+    n, t_ref, dt_ref, st_ref = ref.run(2)
+    assert out == [(t_ref, dt_ref, st_ref)] * nranks
+    W_ref, Bf_ref = H.ref_state(ref)
+    for r, ctx in enumerate(ctxs):
+        for b in np.nonzero(owner == r)[0]:
+            Wd, _, Bd = ctx.download_block(int(b))
+            assert np.array_equal(Wd, W_ref[b].ravel()), (r, b)
+            for d in range(3):
+                assert np.array_equal(Bd[d], Bf_ref[b, d].ravel()), (r, b, d)
+        ctx.close()
+    group.close()
