@@ -66,6 +66,10 @@ struct fx_ctx {
     FxPop *d_pops = nullptr;
     FxBop *d_bops = nullptr;
     FxCorr *d_fcorr = nullptr, *d_ecorr = nullptr;
+    /* element capacities of the seven program tables above (active list,
+     * cell / face / group / cell-field ops, flux / EMF records): an adapt
+     * reuses them when the new programs fit */
+    size_t tab_cap[7] = {0, 0, 0, 0, 0, 0, 0};
 
     FxErr *d_err = nullptr;
     unsigned long long *d_red = nullptr;
@@ -237,6 +241,7 @@ void free_mesh(fx_ctx *c)
     c->d_bops = nullptr;
     cudaFree(c->d_fcorr);
     cudaFree(c->d_ecorr);
+    for (size_t &cap : c->tab_cap) cap = 0;
     c->d_blk = nullptr;
     c->d_W = c->d_Bf = c->d_flux = c->d_vr = c->d_bv1 = c->d_bv2 = nullptr;
     c->d_emf = c->d_eos = c->d_rhs = c->d_grav = nullptr;
@@ -279,6 +284,20 @@ void free_mesh(fx_ctx *c)
 }
 
 bool has_mesh(const fx_ctx *c) { return c && c->nblocks > 0 && c->d_W; }
+
+/* device array of at least `count` elements, reusing the current one when it
+ * is large enough (a grown one gets 1/8 headroom) */
+template <typename T>
+int dev_reserve(fx_ctx *c, T **p, size_t *cap, size_t count)
+{
+    if (*p && count <= *cap) {
+        return FX_SUCCESS;
+    }
+    const size_t n = count + count / 8;
+    int rc = dev_alloc(c, p, n);
+    *cap = rc == FX_SUCCESS && *p ? n : 0;
+    return rc;
+}
 
 /* a block index of the caller (the mesh's numbering) -> this context's;
  * a sharded context serves the blocks its rank owns */
@@ -686,13 +705,14 @@ int install_tables(fx_ctx *c)
     std::vector<int> ids(nblocks);
     for (int b = 0; b < nblocks; ++b) ids[b] = b;
     int rc;
-    if ((rc = dev_alloc(c, &c->d_active, (size_t)c->nactive))) return rc;
-    if ((rc = dev_alloc(c, &c->d_cops, c->plan.ghost.cell_ops.size()))) return rc;
-    if ((rc = dev_alloc(c, &c->d_fops, c->plan.ghost.face_ops.size()))) return rc;
-    if ((rc = dev_alloc(c, &c->d_pops, c->plan.ghost.p_ops.size()))) return rc;
-    if ((rc = dev_alloc(c, &c->d_bops, c->plan.ghost.b_ops.size()))) return rc;
-    if ((rc = dev_alloc(c, &c->d_fcorr, c->plan.flux_corr.size()))) return rc;
-    if ((rc = dev_alloc(c, &c->d_ecorr, c->plan.emf_corr.size()))) return rc;
+    size_t *cap = c->tab_cap;
+    if ((rc = dev_reserve(c, &c->d_active, &cap[0], (size_t)c->nactive))) return rc;
+    if ((rc = dev_reserve(c, &c->d_cops, &cap[1], c->plan.ghost.cell_ops.size()))) return rc;
+    if ((rc = dev_reserve(c, &c->d_fops, &cap[2], c->plan.ghost.face_ops.size()))) return rc;
+    if ((rc = dev_reserve(c, &c->d_pops, &cap[3], c->plan.ghost.p_ops.size()))) return rc;
+    if ((rc = dev_reserve(c, &c->d_bops, &cap[4], c->plan.ghost.b_ops.size()))) return rc;
+    if ((rc = dev_reserve(c, &c->d_fcorr, &cap[5], c->plan.flux_corr.size()))) return rc;
+    if ((rc = dev_reserve(c, &c->d_ecorr, &cap[6], c->plan.emf_corr.size()))) return rc;
     cudaStream_t s = c->stream;
     const cudaMemcpyKind h2d = cudaMemcpyHostToDevice;
     FX_CUDA(c, cudaMemcpyAsync(c->d_blk, hb.data(), (size_t)nblocks * sizeof(FxBlockDev), h2d, s));
