@@ -237,3 +237,18 @@ def test_two_gloo_ranks_exchange_and_fill():
         p.join(timeout=60)
     assert [r[1] for r in res] == [True, True], res
     assert all(r[2] > 0 for r in res)
+
+
+def test_weak_scaling_mesh_gives_each_rank_one_cube():
+    """bench.py --shard: a (8 N) x 8 x 8 root mesh over [0, N] x [0, 1]^2 cut
+    into N runs of the mesh order gives every rank the 512 blocks of one
+    unit cube, so each GPU holds a 128^3 sub-domain"""
+    for nranks in (2, 3):
+        coord = (0.0, float(nranks), 0.0, 1.0, 0.0, 1.0)
+        desc = mesh.to_desc(mesh.uniform_mesh((8 * nranks, 8, 8), coord))
+        owner = fx.morton_owner(desc, nranks)
+        for r in range(nranks):
+            mine = np.nonzero(owner == r)[0]
+            assert len(mine) == 512
+            xs = np.array([desc[b].xmin[0] for b in mine])
+            assert xs.min() >= r - 1e-12 and xs.max() < r + 1 - 1e-12
