@@ -510,22 +510,13 @@ __global__ void __launch_bounds__(256) k_emf(FxDev D, const int *__restrict__ bl
 /* ------------------------------------------------------------------------ */
 /* CT face update                                                            */
 /* ------------------------------------------------------------------------ */
-__global__ void __launch_bounds__(128) k_bf_update(FxDev D, const int *__restrict__ blist, int stage)
+/* one face of direction DIR (compile-time, so the index arithmetic divides
+ * by constants); grid (face chunk, direction, block) */
+template <int DIR>
+__device__ __forceinline__ void fx_bf_face(const FxDev &D, int b, int t, int stage, double dt)
 {
-    if (D.ctl->skip) {
-        return;
-    }
-    const double dt = D.ctl->dt_stage;
-    const int b = blist[blockIdx.y];
-    constexpr int NF = (FX_BS + 1) * FX_BS * FX_BS;
-    int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= 3 * NF) {
-        return;
-    }
-    const int dir = t / NF;
-    t -= dir * NF;
-    const int x2 = dir == 2 ? FX_BS + 1 : FX_BS;
-    const int x1 = dir == 1 ? FX_BS + 1 : FX_BS;
+    constexpr int x2 = DIR == 2 ? FX_BS + 1 : FX_BS;
+    constexpr int x1 = DIR == 1 ? FX_BS + 1 : FX_BS;
     const int k = t % x2;
     t /= x2;
     const int j = t % x1;
@@ -538,12 +529,12 @@ __global__ void __launch_bounds__(128) k_bf_update(FxDev D, const int *__restric
     const double *e2 = e + FX_NEDGES;
     const double *e3 = e + 2 * FX_NEDGES;
     const FxBlockDev &B = D.blk[b];
-    const int f = fx_face_idx(dir, i, j, k);
-    double value = bf[((size_t)dir * FX_NSTAGES + src_slot) * FX_NFACES + f];
-    if (dir == 0) {
+    const int f = fx_face_idx(DIR, i, j, k);
+    double value = bf[((size_t)DIR * FX_NSTAGES + src_slot) * FX_NFACES + f];
+    if (DIR == 0) {
         value += -dt * (e3[fx_edge_idx(2, i, j + 1, k)] - e3[fx_edge_idx(2, i, j, k)]) / B.dx[1];
         value += dt * (e2[fx_edge_idx(1, i, j, k + 1)] - e2[fx_edge_idx(1, i, j, k)]) / B.dx[2];
-    } else if (dir == 1) {
+    } else if (DIR == 1) {
         value += -dt * (e1[fx_edge_idx(0, i, j, k + 1)] - e1[fx_edge_idx(0, i, j, k)]) / B.dx[2];
         value += dt * (e3[fx_edge_idx(2, i + 1, j, k)] - e3[fx_edge_idx(2, i, j, k)]) / B.dx[0];
     } else {
@@ -554,9 +545,28 @@ __global__ void __launch_bounds__(128) k_bf_update(FxDev D, const int *__restric
         fx_fail(D.err, FX_ERR_BF_NONFINITE, b, f);
     }
     if (stage == 2) {
-        value = 0.5 * bf[((size_t)dir * FX_NSTAGES + 0) * FX_NFACES + f] + 0.5 * value;
+        value = 0.5 * bf[((size_t)DIR * FX_NSTAGES + 0) * FX_NFACES + f] + 0.5 * value;
     }
-    bf[((size_t)dir * FX_NSTAGES + dst_slot) * FX_NFACES + f] = value;
+    bf[((size_t)DIR * FX_NSTAGES + dst_slot) * FX_NFACES + f] = value;
+}
+
+__global__ void __launch_bounds__(128) k_bf_update(FxDev D, const int *__restrict__ blist, int stage)
+{
+    if (D.ctl->skip) {
+        return;
+    }
+    constexpr int NF = (FX_BS + 1) * FX_BS * FX_BS;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= NF) {
+        return;
+    }
+    const double dt = D.ctl->dt_stage;
+    const int b = blist[blockIdx.z];
+    switch (blockIdx.y) {
+    case 0: fx_bf_face<0>(D, b, t, stage, dt); break;
+    case 1: fx_bf_face<1>(D, b, t, stage, dt); break;
+    default: fx_bf_face<2>(D, b, t, stage, dt); break;
+    }
 }
 
 /* ------------------------------------------------------------------------ */
@@ -1426,8 +1436,8 @@ void fx_launch_emf(const FxDev &D, const int *blist, int nlist, int wslot, int b
 void fx_launch_bf_update(const FxDev &D, const int *blist, int nlist, int stage, cudaStream_t s)
 {
     if (nlist <= 0) return;
-    const int nf = 3 * (FX_BS + 1) * FX_BS * FX_BS;
-    k_bf_update<<<dim3(fx_blocks(nf, 128), nlist), 128, 0, s>>>(D, blist, stage);
+    const int nf = (FX_BS + 1) * FX_BS * FX_BS;
+    k_bf_update<<<dim3(fx_blocks(nf, 128), 3, nlist), 128, 0, s>>>(D, blist, stage);
 }
 
 void fx_launch_cell_update(const FxDev &D, const int *blist, int nlist, int stage,
