@@ -405,20 +405,25 @@ __global__ void __launch_bounds__(256) k_emf(FxDev D, const int *__restrict__ bl
         const int n0 = i0 < FX_BS ? N0 : 0;
         const int ntot = n0 + N1 + N2;
         for (int t = threadIdx.x; t < ntot; t += blockDim.x) {
-            int dir, u = t, xk;
+            int dir, u = t;
             if (u < n0) {
                 dir = 0;
-                xk = FX_BS + 1;
             } else if ((u -= n0) < N1) {
                 dir = 1;
-                xk = FX_BS + 1;
             } else {
                 u -= N1;
                 dir = 2;
-                xk = FX_BS;
             }
-            const int j = u / xk;
-            const int k = u - j * xk;
+            /* k runs over 17 edges for x and y edges, 16 for z edges:
+             * constant divisors */
+            int j, k;
+            if (dir == 2) {
+                j = u / FX_BS;
+                k = u - j * FX_BS;
+            } else {
+                j = u / (FX_BS + 1);
+                k = u - j * (FX_BS + 1);
+            }
             const int up = (dir + 1) % 3;
             const int right = (dir + 2) % 3;
             /* the four cells: c0 = e, c1 = e - up, c2 = e - up - right,
