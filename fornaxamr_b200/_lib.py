@@ -174,7 +174,7 @@ def load() -> C.CDLL:
     L.fx_autotune.argtypes = [vp, dp, C.c_int, C.POINTER(C.c_int)]
     L.fx_set_flux_shape.argtypes = [vp, C.c_int]
     # device pointers (W, dx, blocks, dt) and the stream pass as plain addresses
-    L.fx_calc_dt_noalloc.argtypes = [vp, C.c_int, vp, vp, C.c_int, C.c_double, C.c_double, vp, vp]
+    L.fx_calc_dt_noalloc.argtypes = [vp, C.c_int, C.c_int, vp, C.c_int, vp, C.c_int, C.c_double, C.c_double, vp, vp]
     L.fx_adjoint_forward.argtypes = [vp, C.c_int, C.c_double]
     L.fx_adjoint_backward.argtypes = [vp, dp, dp, dp, dp, C.c_int]
     L.fx_adjoint_time.argtypes = [vp, dp]

@@ -66,7 +66,10 @@ def _build_one(ng: int, verbose: bool, ptxas_info: bool) -> str:
         if src.endswith(".cpp"):
             cmd += ["-x", "cu"]
         jobs.append(cmd)
-    with ThreadPoolExecutor(max_workers=max(1, min(len(jobs), os.cpu_count() or 1))) as pool:
+    # FX_BUILD_JOBS bounds the parallel compiles (each nvcc of the kernel
+    # sources takes a few GB of host memory)
+    workers = int(os.environ.get("FX_BUILD_JOBS", "0")) or (os.cpu_count() or 1)
+    with ThreadPoolExecutor(max_workers=max(1, min(len(jobs), workers))) as pool:
         for cmd in jobs:
             if verbose:
                 print(" ".join(cmd))

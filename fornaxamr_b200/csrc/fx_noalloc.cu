@@ -6,10 +6,14 @@
  * Two launches on the caller's stream:
  *   k_dt_partial   one CTA per listed block: min over the block's 16^3 active
  *                  cells of cfl / sum_d (|v_d| + c_s) / dx_d, as an ordered
- *                  integer key, into g_dt_partial[list position];
+ *                  integer key, into g_dt_partial[list position]; a listed
+ *                  index outside [0, nblocks) reads nothing and stores the
+ *                  smallest key, which decodes to NaN;
  *   k_dt_finish    one CTA: min of the nlist keys and the reference's initial
- *                  dt_min = 1e99 (src/prj_timeint.c:2147), stored as a double
- *                  at the caller's output pointer.
+ *                  dt_min = 1e99 (src/prj_timeint.c:2147), times the
+ *                  integrator's factor (6 for eSSPRK10_4,
+ *                  src/prj_timeint.c:2250-2251), stored as a double at the
+ *                  caller's output pointer.
  * Every scratch word k_dt_finish reads was written by k_dt_partial of the
  * same call, so the scratch needs no clearing and nothing carries over from
  * one call to the next.  The per-cell arithmetic is the one the context's
@@ -70,12 +74,20 @@ __device__ __forceinline__ unsigned long long cta_min(unsigned long long key)
     return key;
 }
 
-__global__ void __launch_bounds__(kPartialThreads) k_dt_partial(const double *__restrict__ W, int nv,
-    const double *__restrict__ dx, const int *__restrict__ blist, double gamma, double cfl,
+__global__ void __launch_bounds__(kPartialThreads) k_dt_partial(const double *__restrict__ W, int nv, int ns,
+    const double *__restrict__ dx, int nblocks, const int *__restrict__ blist, double gamma, double cfl,
     unsigned long long *__restrict__ partial)
 {
     const int b = blist ? blist[blockIdx.x] : (int)blockIdx.x;
-    const double *w = W + (size_t)b * FX_W_COUNT(nv); /* stage slot 0 */
+    if (b < 0 || b >= nblocks) {
+        if (threadIdx.x == 0) {
+            partial[blockIdx.x] = 0ULL; /* decodes to NaN and wins the min */
+        }
+        return;
+    }
+    /* stage slot 0 of block b: W + b * nv * ns * NCELLS, variables ns * NCELLS apart */
+    const size_t vs = (size_t)ns * FX_NCELLS;
+    const double *w = W + (size_t)b * nv * vs;
     const double dx0 = dx[3 * (size_t)b + 0];
     const double dx1 = dx[3 * (size_t)b + 1];
     const double dx2 = dx[3 * (size_t)b + 2];
@@ -85,12 +97,12 @@ __global__ void __launch_bounds__(kPartialThreads) k_dt_partial(const double *__
         const int j = (t / FX_BS) % FX_BS;
         const int i = t / (FX_BS * FX_BS);
         const int c = fx_lidx(i, j, k);
-        const double rho = w[(size_t)FX_RHO * 2 * FX_NCELLS + c];
-        const double p = fx_pressure(gamma, rho, w[(size_t)FX_EINT * 2 * FX_NCELLS + c]);
+        const double rho = w[FX_RHO * vs + c];
+        const double p = fx_pressure(gamma, rho, w[FX_EINT * vs + c]);
         const double cs = sqrt(gamma * p / rho);
-        const double denom = (fabs(w[(size_t)FX_V1 * 2 * FX_NCELLS + c]) + cs) / dx0 +
-            (fabs(w[(size_t)FX_V2 * 2 * FX_NCELLS + c]) + cs) / dx1 +
-            (fabs(w[(size_t)FX_V3 * 2 * FX_NCELLS + c]) + cs) / dx2;
+        const double denom = (fabs(w[FX_V1 * vs + c]) + cs) / dx0 +
+            (fabs(w[FX_V2 * vs + c]) + cs) / dx1 +
+            (fabs(w[FX_V3 * vs + c]) + cs) / dx2;
         const double dt_cell = cfl / denom;
         if (dt_cell == dt_cell) {
             const unsigned long long kc = dt_key(dt_cell);
@@ -104,7 +116,7 @@ __global__ void __launch_bounds__(kPartialThreads) k_dt_partial(const double *__
 }
 
 __global__ void __launch_bounds__(kFinishThreads) k_dt_finish(const unsigned long long *__restrict__ partial,
-    int nlist, double *__restrict__ dt)
+    int nlist, double mult, double *__restrict__ dt)
 {
     unsigned long long key = threadIdx.x == 0 ? dt_key(1.0e99) : ~0ULL;
     for (int q = threadIdx.x; q < nlist; q += kFinishThreads) {
@@ -112,7 +124,7 @@ __global__ void __launch_bounds__(kFinishThreads) k_dt_finish(const unsigned lon
     }
     key = cta_min<kFinishThreads>(key);
     if (threadIdx.x == 0) {
-        *dt = dt_from_key(key);
+        *dt = dt_from_key(key) * mult;
     }
 }
 
@@ -139,14 +151,19 @@ int partial_scratch(unsigned long long **out)
 
 } // namespace
 
-extern "C" int fx_calc_dt_noalloc(const double *W, int mhd, const double *dx, const int *blocks, int nlist,
-    double gamma, double cfl, void *stream, double *dt)
+extern "C" int fx_calc_dt_noalloc(const double *W, int mhd, int integrator, const double *dx, int nblocks,
+    const int *blocks, int nlist, double gamma, double cfl, void *stream, double *dt)
 {
-    if (!W || !dx || !dt || nlist <= 0 || (mhd != 0 && mhd != 1) || !(gamma > 1.0) || !(cfl > 0.0)) {
+    if (!W || !dx || !dt || nblocks <= 0 || nlist <= 0 || (mhd != 0 && mhd != 1) ||
+        (integrator != FX_INT_RK2 && integrator != FX_INT_ESSPRK10_4) || !(gamma > 1.0) || !(cfl > 0.0)) {
         return FX_EINVAL;
     }
     if (nlist > FX_NOALLOC_MAX_BLOCKS) {
         return FX_ETOOBIG;
+    }
+    /* an error the caller left pending is reported, not consumed */
+    if (cudaPeekAtLastError() != cudaSuccess) {
+        return FX_ECUDA;
     }
     unsigned long long *partial = nullptr;
     const int rc = partial_scratch(&partial);
@@ -154,9 +171,14 @@ extern "C" int fx_calc_dt_noalloc(const double *W, int mhd, const double *dx, co
         return rc;
     }
     const int nv = mhd ? FX_MAXVAR : FX_MAXVAR - 3;
+    const int ns = integrator == FX_INT_ESSPRK10_4 ? 3 : 2;
+    const double mult = integrator == FX_INT_ESSPRK10_4 ? 6.0 : 1.0;
     cudaStream_t s = static_cast<cudaStream_t>(stream);
-    k_dt_partial<<<nlist, kPartialThreads, 0, s>>>(W, nv, dx, blocks, gamma, cfl, partial);
-    k_dt_finish<<<1, kFinishThreads, 0, s>>>(partial, nlist, dt);
+    k_dt_partial<<<nlist, kPartialThreads, 0, s>>>(W, nv, ns, dx, nblocks, blocks, gamma, cfl, partial);
+    if (cudaGetLastError() != cudaSuccess) {
+        return FX_ECUDA;
+    }
+    k_dt_finish<<<1, kFinishThreads, 0, s>>>(partial, nlist, mult, dt);
     if (cudaGetLastError() != cudaSuccess) {
         return FX_ECUDA;
     }

@@ -305,27 +305,43 @@ int fx_run(fx_ctx *ctx, int form, int nsteps, double cfl, double dt_factor, doub
  * reference, which has no device; nothing is allocated, here or by the
  * library calls it makes.
  *
- *   W       device; block b's W_mhd (2 stages, src/prj_defs.h WIDX layout,
- *           NHYDRO = 9 if mhd else 6) at W + b * NHYDRO * 2 * 8000; stage 0
- *           is read
- *   dx      device; dx[3b + d] = cell width of block b along d
- *   blocks  device; nlist block indices to reduce over (the active blocks),
- *           or NULL for blocks 0 .. nlist-1
- *   stream  cudaStream_t the two kernels are queued on (NULL: default stream)
- *   dt      device; receives the minimum (1e99 if no cell gives a finite
- *           value), stream-ordered: the call does not synchronise
+ *   W           device; block b's W_mhd in the reference layout (src/prj_defs.h
+ *               WIDX): NHYDRO variables (9 if mhd else 6) x NS stage slots x
+ *               NCELLS cells, block b at W + b * NHYDRO * NS * NCELLS, where
+ *               NS = 2 for FX_INT_RK2 and 3 for FX_INT_ESSPRK10_4 (the
+ *               reference's PRJ_BLOCK_NSTAGES) and NCELLS = (16 + 2 NG)^3 with
+ *               NG = fx_ghost_layers() of the loaded library (8000 cells in
+ *               libfornax_b200.so, 13824 in libfornax_b200_ng4.so); stage
+ *               slot 0 is read
+ *   integrator  FX_INT_RK2 or FX_INT_ESSPRK10_4: the stage slots of W and the
+ *               factor the minimum is multiplied by (1, or 6 as the
+ *               reference does for eSSPRK10_4, src/prj_timeint.c:2250-2251)
+ *   dx          device; dx[3b + d] = cell width of block b along d
+ *   nblocks     the number of blocks present in W and dx
+ *   blocks      device; nlist block indices to reduce over (the active
+ *               blocks), or NULL for blocks 0 .. nlist-1; an index outside
+ *               [0, nblocks) is not read and makes the result NaN
+ *   stream      cudaStream_t the two kernels are queued on (NULL: default stream)
+ *   dt          device; receives the minimum (1e99 if no cell gives a finite
+ *               value) times the integrator's factor, stream-ordered: the
+ *               call does not synchronise
  *
  * Returns FX_ETOOBIG, before any device work, when nlist exceeds
- * FX_NOALLOC_MAX_BLOCKS, and FX_EINVAL for null pointers, nlist <= 0, mhd not
- * 0/1, gamma <= 1 or cfl <= 0.  The scratch is one fixed 512 KiB device
- * array per device, written in full by each call before it is read, so it
- * needs no clearing.  The first call on a device resolves its address with
- * cudaGetSymbolAddress (with that device current); make that first call
- * before any stream capture.  Calls on one device share the scratch: two
- * calls whose kernels overlap (different streams or host threads) race and
- * give wrong results, so order them on one stream or serialise them. */
-int fx_calc_dt_noalloc(const double *W, int mhd, const double *dx, const int *blocks, int nlist,
-    double gamma, double cfl, void *stream, double *dt);
+ * FX_NOALLOC_MAX_BLOCKS, and FX_EINVAL for null pointers, nblocks <= 0,
+ * nlist <= 0, mhd not 0/1, an unknown integrator, gamma <= 1 or cfl <= 0.
+ * A CUDA error already pending in the calling thread is left in place and
+ * reported as FX_ECUDA without queueing anything; a failed launch returns
+ * FX_ECUDA.  The scratch is one fixed 512 KiB device array per device,
+ * written in full by each call before it is read, so it needs no clearing.
+ * The first call on a device resolves its address with cudaGetSymbolAddress
+ * (with that device current) and keeps it for the life of the process; make
+ * that first call before any stream capture, and do not call the function
+ * after a cudaDeviceReset of that device (the array's address may change).
+ * Calls on one device share the scratch: two calls whose kernels overlap
+ * (different streams or host threads) race and give wrong results, so order
+ * them on one stream or serialise them. */
+int fx_calc_dt_noalloc(const double *W, int mhd, int integrator, const double *dx, int nblocks,
+    const int *blocks, int nlist, double gamma, double cfl, void *stream, double *dt);
 
 /* ---- dynamic AMR ---------------------------------------------------------------- */
 
