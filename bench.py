@@ -219,17 +219,21 @@ def measured_peak_hbm():
         return 6650.0, "fallback"
 
 
-def flux_traffic_per_launch():
-    """DRAM bytes of one face-flux launch from the committed ncu summary, or None."""
+def flux_profile_figures():
+    """Figures of one face-flux launch of the 512-block step from the committed
+    ncu summary: DRAM bytes (read + write) per launch and the FP64-pipe
+    fraction; None where absent."""
     path = os.path.join(HERE, "profiles", "k_flux_traffic_fourier128.txt")
+    out = {"dram_bytes_per_launch": None, "fp64_pipe_frac": None}
     try:
         with open(path) as f:
             for line in f:
-                if line.startswith("dram_bytes_per_launch:"):
-                    return float(line.split(":", 1)[1])
+                key, _, val = line.partition(":")
+                if key.strip() in out:
+                    out[key.strip()] = float(val)
     except (OSError, ValueError):
         pass
-    return None
+    return out
 
 
 def run_amr(args, dev, kind):
@@ -671,15 +675,20 @@ def run_fx(args, rank, world, local_rank):
         e2e_ms = max_over_ranks(e0.elapsed_time(e1)) / args.e2e_steps
 
     peak, peak_kind = measured_peak_hbm()
-    # algorithmic bytes of one face-flux launch (all three directions, all
-    # blocks): per direction and block the 8 primitive inputs of the
-    # 20 x 18 x 18 stencil cells, and per face the face field (8 B) plus the
-    # outputs later phases read: 6 hydro fluxes, the normal velocity,
-    # Bv1, Bv2 (9 doubles)
+    # roofline of the face-flux launch (one RK stage's face sweep over all
+    # blocks, three directions): algorithmic bytes = half of the step's
+    # compulsory state traffic, 180 B per zone (9 FP64 variables x 8 B x 5
+    # passes per RK2 step / 2 stages)
+    alg_bytes = ZONES * BYTES_PER_ZONE_STEP / 2.0
+    achieved = alg_bytes / (ms_flux * 1e-3) / 1e9
+    # the kernel's own input and output bytes: per direction and block the 8
+    # primitive inputs of the 20 x 18 x 18 stencil cells, and per face the
+    # face field (8 B) plus the outputs later phases read (6 hydro fluxes, the
+    # normal velocity, Bv1, Bv2: 9 doubles)
     faces = nb * 3 * 17 * 18 * 18
-    flux_bytes = nb * 3 * 20 * 18 * 18 * 8 * 8 + faces * 8 + faces * 9 * 8
-    achieved = flux_bytes / (ms_flux * 1e-3) / 1e9
-    traffic = flux_traffic_per_launch()
+    kernel_bytes = nb * 3 * 20 * 18 * 18 * 8 * 8 + faces * 8 + faces * 9 * 8
+    prof = flux_profile_figures()
+    traffic = prof["dram_bytes_per_launch"]
     launches_per_step = ctx.info(0) + 4
     line = {
         "metric": METRIC,
@@ -701,16 +710,24 @@ def run_fx(args, rank, world, local_rank):
             "parallelism": f"replicas x{world}",
         },
         "hbm_gbs_step": ZONES * BYTES_PER_ZONE_STEP / (ms_step * 1e-3) / 1e9,
+        "hbm_frac_step": ZONES * BYTES_PER_ZONE_STEP / (ms_step * 1e-3) / 1e9 / peak,
         "plain": None if ms_plain is None else {
             "ms_per_step": ms_plain, "value": world * ZONES / (ms_plain * 1e-3),
             "batched_over_plain": ms_plain / ms_step},
         "phases_ms": phases,
         "autotune": {"flux_shape": tuned, "flux_ms_per_shape": [round(x, 4) for x in tune_ms[:6]]},
         "roofline": {
-            "kernel": "k_flux (face fluxes, three directions, all blocks)",
+            "kernel": "k_flux (face fluxes, three directions, all blocks; one launch per RK stage)",
             "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
             "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
-            "note": "FP64 HLLD issue rate bounds this kernel before HBM (FP64 pipe 53 % busy, profiles/k_flux_fourier216.md)",
+            "algorithmic_bytes_per_launch": alg_bytes,
+            "traffic_over_algorithmic": None if traffic is None else traffic / alg_bytes,
+            "kernel_bytes_per_launch": kernel_bytes,
+            "kernel_bytes_gbs": kernel_bytes / (ms_flux * 1e-3) / 1e9,
+            "ms_per_launch": ms_flux,
+            "fp64": {"pipe_frac": prof["fp64_pipe_frac"],
+                     "note": "the FP64 issue rate of the HLLD solver bounds this kernel before HBM; "
+                             "pipe fraction from an ncu capture of one launch"},
         },
         "e2e": None if e2e_ms is None else {
             "value": world * ZONES / (e2e_ms * 1e-3), "unit": UNIT,

@@ -44,6 +44,11 @@ int fx_amr_remesh(const fx_config &cfg, const fx_amr_config &amr, int nblocks,
     const fx_block_desc *blocks, const int32_t *votes, int capacity, FxAmrResult &res,
     std::string *err);
 
+/* prj_neighbor_compute_geometry (src/prj_mesh.c:46-243): type, relative
+ * level and send/recv boxes of neighbour b in slot s of block a; false when
+ * the levels differ by more than one. */
+bool fx_neighbor_geometry(const fx_block_desc &a, const fx_block_desc &b, fx_slot &s);
+
 /* prj_amr_tag passes 2-4 (src/prj_amr.c:1707-1774) alone: refine_flag per
  * block from the pass-1 votes. */
 void fx_amr_flags(const fx_amr_config &amr, int nblocks, const fx_block_desc *blocks,

@@ -22,43 +22,11 @@ constexpr double kTol = 1.0e-12;
 
 enum { NB_NONE = 0, NB_FACE = 1, NB_EDGE = 2, NB_CORNER = 3 };
 
-bool is_active(const fx_block_desc &b) { return b.id >= 0 && b.active == 1; }
-
-void clear_slots(fx_block_desc &b)
-{
-    for (int n = 0; n < 56; ++n) {
-        fx_slot &s = b.slot[n];
-        std::memset(&s, 0, sizeof(s));
-        s.id = -1;
-    }
-}
-
-void reset_children(fx_block_desc &b)
-{
-    for (int n = 0; n < 8; ++n) b.children[n] = -1;
-}
-
-/* prj_block_setup_geometry (src/prj_mesh.c:675-687) */
-void setup_geometry(fx_block_desc &b)
-{
-    b.vol = b.dx[0] * b.dx[1] * b.dx[2];
-    b.area[0] = b.dx[1] * b.dx[2];
-    b.area[1] = b.dx[0] * b.dx[2];
-    b.area[2] = b.dx[0] * b.dx[1];
-}
-
-/* prj_block_cell_size (src/prj_amr.c:42-57) */
-double cell_size(const fx_block_desc &b)
-{
-    double c = b.dx[0];
-    if (b.dx[1] > c) c = b.dx[1];
-    if (b.dx[2] > c) c = b.dx[2];
-    return c;
-}
+} /* namespace */
 
 /* send/recv boxes of neighbour b as seen from a: prj_neighbor_compute_geometry
  * (src/prj_mesh.c:46-243) */
-bool compute_geometry(const fx_block_desc &a, const fx_block_desc &b, fx_slot &s)
+bool fx_neighbor_geometry(const fx_block_desc &a, const fx_block_desc &b, fx_slot &s)
 {
     int axisrel[3] = {0, 0, 0};
     int touching = 0;
@@ -109,6 +77,42 @@ bool compute_geometry(const fx_block_desc &a, const fx_block_desc &b, fx_slot &s
         s.send_loc_end[d] = (int8_t)se;
     }
     return true;
+}
+
+namespace {
+
+bool is_active(const fx_block_desc &b) { return b.id >= 0 && b.active == 1; }
+
+void clear_slots(fx_block_desc &b)
+{
+    for (int n = 0; n < 56; ++n) {
+        fx_slot &s = b.slot[n];
+        std::memset(&s, 0, sizeof(s));
+        s.id = -1;
+    }
+}
+
+void reset_children(fx_block_desc &b)
+{
+    for (int n = 0; n < 8; ++n) b.children[n] = -1;
+}
+
+/* prj_block_setup_geometry (src/prj_mesh.c:675-687) */
+void setup_geometry(fx_block_desc &b)
+{
+    b.vol = b.dx[0] * b.dx[1] * b.dx[2];
+    b.area[0] = b.dx[1] * b.dx[2];
+    b.area[1] = b.dx[0] * b.dx[2];
+    b.area[2] = b.dx[0] * b.dx[1];
+}
+
+/* prj_block_cell_size (src/prj_amr.c:42-57) */
+double cell_size(const fx_block_desc &b)
+{
+    double c = b.dx[0];
+    if (b.dx[1] > c) c = b.dx[1];
+    if (b.dx[2] > c) c = b.dx[2];
+    return c;
 }
 
 /* prj_boxes_touch_face_edge_corner (src/prj_amr.c:398-425) */
@@ -164,7 +168,7 @@ struct Mesh {
         for (int n = 0; n < 56; ++n) {
             if (a.slot[n].id < 0) {
                 a.slot[n].id = nb.id;
-                if (!compute_geometry(a, nb, a.slot[n])) geom_error = true;
+                if (!fx_neighbor_geometry(a, nb, a.slot[n])) geom_error = true;
                 return;
             }
         }

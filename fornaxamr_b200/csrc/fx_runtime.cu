@@ -1976,6 +1976,24 @@ int fx_amr_energy_injected(fx_ctx *c, double *e)
     return FX_SUCCESS;
 }
 
+int fx_mesh_slot_geometry(int nblocks, fx_block_desc *blocks)
+{
+    if (nblocks < 0 || (nblocks > 0 && !blocks)) return FX_EINVAL;
+    for (int i = 0; i < nblocks; ++i) {
+        for (int s = 0; s < 56; ++s) {
+            fx_slot &sl = blocks[i].slot[s];
+            if (sl.id < 0) {
+                const int32_t id = sl.id;
+                std::memset(&sl, 0, sizeof(sl));
+                sl.id = id;
+                continue;
+            }
+            if (sl.id >= nblocks || !fx_neighbor_geometry(blocks[i], blocks[sl.id], sl)) return FX_EINVAL;
+        }
+    }
+    return FX_SUCCESS;
+}
+
 int fx_amr_remesh_host(const fx_config *cfg, const fx_amr_config *amr, int nblocks, const fx_block_desc *in,
     const int32_t *votes, int32_t *flags, int capacity, fx_block_desc *out, int *nout)
 {

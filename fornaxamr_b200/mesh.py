@@ -4,10 +4,12 @@ A FornaxAMR mesh is a list of blocks (geometry, level, 56 neighbour slots).
 This module builds that description for uniform root grids the way
 prj_mesh_init does (reference src/prj_mesh.c:1438-1686): blocks ordered
 i-major over the root grid, 16^3 cells each, and neighbour slots from the
-26 adjacent root blocks with the send/recv boxes of
-prj_neighbor_compute_geometry (src/prj_mesh.c:46-243).  The slot table is an
-interface the drop-in must reproduce exactly, so the box rules are restated
-here with the same meaning.
+26 adjacent root blocks.  The builders here decide which block sits in which
+slot (the reference's probe and first-free-slot order); the slot's type,
+relative level and send/recv boxes (prj_neighbor_compute_geometry,
+src/prj_mesh.c:46-243) are filled by the native library
+(fx_mesh_slot_geometry) when the description is made, so the box rules exist
+once, in the library the dynamic-AMR remesh uses too.
 """
 from __future__ import annotations
 
@@ -26,13 +28,7 @@ NEIGHBOR_NONE, NEIGHBOR_FACE, NEIGHBOR_EDGE, NEIGHBOR_CORNER = 0, 1, 2, 3
 
 @dataclass
 class Slot:
-    id: int = -1
-    rel_level: int = 0
-    type: int = NEIGHBOR_NONE
-    send_start: List[int] = field(default_factory=lambda: [0, 0, 0])
-    send_end: List[int] = field(default_factory=lambda: [0, 0, 0])
-    recv_start: List[int] = field(default_factory=lambda: [0, 0, 0])
-    recv_end: List[int] = field(default_factory=lambda: [0, 0, 0])
+    id: int = -1   # neighbour block index, -1 if the slot is free
 
 
 @dataclass
@@ -66,56 +62,6 @@ def slot_index(ox: int, oy: int, oz: int) -> int:
     return index - 1 if index > 13 else index
 
 
-def compute_geometry(a: Block, b: Block, slot: Slot) -> None:
-    """Send/recv boxes of neighbour b as seen from block a (the slot lives in
-    a; send boxes are in a's cells, recv boxes in b's cells)."""
-    axisrel = [0, 0, 0]
-    touching = 0
-    for d in range(3):
-        tol = 1.0e-2 * min(a.dx[d], b.dx[d])
-        if abs(a.xmax[d] - b.xmin[d]) < tol:
-            axisrel[d] = 1
-            touching += 1
-        elif abs(b.xmax[d] - a.xmin[d]) < tol:
-            axisrel[d] = -1
-            touching += 1
-    slot.type = [NEIGHBOR_NONE, NEIGHBOR_FACE, NEIGHBOR_EDGE, NEIGHBOR_CORNER][touching]
-    slot.rel_level = b.level - a.level
-    for d in range(3):
-        if slot.rel_level == 0:
-            if axisrel[d] == 1:
-                rs, re, ss, se = -NG, 0, BS - NG, BS
-            elif axisrel[d] == -1:
-                rs, re, ss, se = BS, BS + NG, 0, NG
-            else:
-                rs, re, ss, se = 0, BS, 0, BS
-        elif slot.rel_level == -1:
-            if axisrel[d] == 1:
-                rs, re, ss, se = -NG, 0, BS - 2 * NG, BS
-            elif axisrel[d] == -1:
-                rs, re, ss, se = BS, BS + NG, 0, 2 * NG
-            else:
-                if (b.xmin[d] + b.xmax[d]) > (a.xmin[d] + a.xmax[d]):
-                    rs, re = 0, BS // 2
-                else:
-                    rs, re = BS // 2, BS
-                ss, se = 0, BS
-        elif slot.rel_level == 1:
-            if axisrel[d] == 1:
-                rs, re, ss, se = -NG, 0, BS - NG // 2, BS
-            elif axisrel[d] == -1:
-                rs, re, ss, se = BS, BS + NG, 0, NG // 2
-            else:
-                if (b.xmin[d] + b.xmax[d]) > (a.xmin[d] + a.xmax[d]):
-                    rs, re, ss, se = -NG, BS, BS // 2 - NG // 2, BS
-                else:
-                    rs, re, ss, se = 0, BS + NG, 0, BS // 2 + NG // 2
-        else:
-            raise ValueError("neighbour geometry error: level jump larger than one")
-        slot.recv_start[d], slot.recv_end[d] = rs, re
-        slot.send_start[d], slot.send_end[d] = ss, se
-
-
 def uniform_mesh(root: Sequence[int], coord: Sequence[float]) -> List[Block]:
     """Root grid of root[0] x root[1] x root[2] blocks on the box
     coord = (x1min, x1max, x2min, x2max, x3min, x3max), non-periodic."""
@@ -146,7 +92,6 @@ def uniform_mesh(root: Sequence[int], coord: Sequence[float]) -> List[Block]:
                                 continue
                             nid = (n[0] * ny + n[1]) * nz + n[2]
                             b.slots[s].id = nid
-                            compute_geometry(b, blocks[nid], b.slots[s])
     return blocks
 
 
@@ -176,7 +121,6 @@ def _add_neighbor(a: Block, b: Block) -> None:
     for sl in a.slots:
         if sl.id < 0:
             sl.id = b.id
-            compute_geometry(a, b, sl)
             return
     raise ValueError("more than 56 neighbours")
 
@@ -343,15 +287,11 @@ def to_desc(blocks: Sequence[Block]) -> "C.Array":
             d.children[o] = b.children[o]
         d.can_refine = 1
         for s, sl in enumerate(b.slots):
-            ds = d.slot[s]
-            ds.id = sl.id
-            ds.rel_level = sl.rel_level
-            ds.type = sl.type
-            for a in range(3):
-                ds.send_loc_start[a] = sl.send_start[a]
-                ds.send_loc_end[a] = sl.send_end[a]
-                ds.recv_loc_start[a] = sl.recv_start[a]
-                ds.recv_loc_end[a] = sl.recv_end[a]
+            d.slot[s].id = sl.id
+    from . import library
+    rc = library().fx_mesh_slot_geometry(len(blocks), arr)
+    if rc != 0:
+        raise ValueError(f"fx_mesh_slot_geometry failed ({rc}): a slot id outside the mesh or a level jump > 1")
     return arr
 
 

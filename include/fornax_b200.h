@@ -13,9 +13,13 @@
  * Build variants of the reference map onto run-time settings:
  *   PRJ_MHD=1 -> fx_config.mhd = 1 (NHYDRO = 9, HLLD, constrained transport)
  *   PRJ_MHD=0 -> fx_config.mhd = 0 (NHYDRO = 6, HLLC)
- *   PRJ_RECON_HYDRO -> fx_config.recon (MC or WENO-Z3)
+ *   PRJ_RECON_HYDRO -> fx_config.recon (MC, WENO-Z3, or WENO-Z7 in the
+ *                      four-ghost-layer library)
  *   TIME_INTEGRATION -> fx_config.integrator (RK2 or eSSPRK10_4)
- * Fixed: PRJ_BLOCK_SIZE = 16, PRJ_NGHOST = 2, ideal-gas EOS with a run-time
+ *   PRJ_NGHOST -> the library: libfornax_b200.so (2 layers, 20^3 block
+ *                 arrays) or libfornax_b200_ng4.so (4 layers, 24^3);
+ *                 fx_ghost_layers() reports which one is loaded
+ * Fixed: PRJ_BLOCK_SIZE = 16, ideal-gas EOS with a run-time
  * adiabatic index, no radiation, no GR.  The number of stage slots of the
  * block W and Bf arrays (NS below) is 2 for RK2 and 3 for eSSPRK10_4.
  *
@@ -414,6 +418,14 @@ int fx_amr_timings(fx_ctx *ctx, double *ms);
 int fx_amr_remesh_host(const fx_config *cfg, const fx_amr_config *amr, int nblocks,
     const fx_block_desc *in, const int32_t *votes, int32_t *flags, int capacity, fx_block_desc *out,
     int *nout);
+
+/* Neighbour-slot geometry of a mesh whose slot ids are set: for every slot
+ * with id >= 0, its type, relative level and send/recv boxes
+ * (prj_neighbor_compute_geometry, src/prj_mesh.c:46-243); slots with id < 0
+ * are reset to the empty slot (type 0, level 0, zero boxes).  Returns
+ * FX_EINVAL for an id outside [0, nblocks) or neighbours more than one
+ * level apart.  The product's mesh builders use this one restatement. */
+int fx_mesh_slot_geometry(int nblocks, fx_block_desc *blocks);
 
 /* ---- measurement --------------------------------------------------------------- */
 
