@@ -182,6 +182,7 @@ class Reference:
         L.rh_weno3_face.argtypes = [C.c_double] * 4
         L.rh_weno3_face.restype = C.c_double
         L.rh_sim_dt.restype = C.c_double
+        L.rh_set_mhd_eta.argtypes = [C.c_double]
         if mhd:
             L.rh_hlld.argtypes = [dp, dp] + [C.c_double] * 5 + [dp]
             L.rh_emf_upwind.argtypes = [dp, dp, dp]
@@ -217,6 +218,15 @@ class Reference:
 
     def time_steps(self, nsteps: int, dt: float) -> float:
         return self.lib.rh_time_steps(nsteps, dt)
+
+    def set_mhd_eta(self, eta: float) -> None:
+        """Run-time resistivity (prj_mesh.mhd_eta)."""
+        self.lib.rh_set_mhd_eta(eta)
+
+    def refill(self) -> None:
+        """The driver's set-up refill (eos, ghost fill, eos) after stage-0
+        cells or faces were rewritten with set_W / set_Bf."""
+        self.lib.rh_refill()
 
     # -- dynamic AMR ------------------------------------------------------------
     def amr_configure(self, a: RhAmr) -> None:

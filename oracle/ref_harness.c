@@ -927,6 +927,25 @@ void rh_fill_ghosts(int stage, int use_bf1)
     prj_eos_fill_mesh(&g_sim.mesh, &g_sim.eos, &g_mpi, stage, PRJ_EOS_CTX_MAIN);
 }
 
+/* Run-time resistivity of the mesh (prj_mesh.mhd_eta, src/prj_types.h:497),
+ * which the EMF update adds to the artificial eta of each edge
+ * (src/prj_timeint.c:404-408, 525). */
+void rh_set_mhd_eta(double eta)
+{
+    g_sim.mesh.mhd_eta = eta;
+}
+
+/* The driver's set-up refill (src/main.c:437-448) after the caller has
+ * rewritten stage-0 cells or faces: eos of the active cells, ghost fill
+ * with the cell field from the faces, eos of the whole mesh. */
+void rh_refill(void)
+{
+    prj_eos_fill_active_cells(&g_sim.mesh, &g_sim.eos, &g_mpi, 1, PRJ_EOS_CTX_MAIN);
+    prj_boundary_fill_ghosts_and_bf(&g_sim.mesh, &g_mpi, &g_sim.bc, 1, 0, &g_sim.eos, 0,
+        &g_sim.rad, PRJ_BOUNDARY_TIMER_SCOPE_NONE);
+    prj_eos_fill_mesh(&g_sim.mesh, &g_sim.eos, &g_mpi, 1, PRJ_EOS_CTX_MAIN);
+}
+
 /* The coarse/fine corrections of a stage (src/prj_timeint.c:2750, 528). */
 void rh_flux_send(void)
 {
