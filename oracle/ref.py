@@ -123,7 +123,12 @@ def amr_params(max_level: int, criteria, min_dx: float = 0.0, reach_density: flo
 
 def lib_path(mhd: bool, variant: str = "") -> str:
     """variant: "" (RK2, MC), "weno3", "ess" (eSSPRK10_4), "ess_weno3"; with
-    four ghost layers "" (MC, PRJ_NGHOST=4), "weno7" (WENO-Z7) or "ess_weno7"."""
+    four ghost layers "" (MC, PRJ_NGHOST=4), "weno7" (WENO-Z7) or "ess_weno7".
+    "fx": the RK2 / MC build with the drop-in binding linked in its place
+    (prj_timeint_step and prj_timeint_calc_dt reach the device through
+    fornaxamr_b200/dropin/prj_fx.c)."""
+    if NG == 4 and variant == "fx":
+        raise ValueError("the drop-in build links the two-ghost-layer library")
     if NG == 4 and variant not in ("", "weno7", "ess_weno7"):
         raise ValueError(f"no four-ghost-layer reference build for variant {variant!r}")
     if NG == 2 and variant.endswith("weno7"):
@@ -187,6 +192,10 @@ class Reference:
             L.rh_hlld.argtypes = [dp, dp] + [C.c_double] * 5 + [dp]
             L.rh_emf_upwind.argtypes = [dp, dp, dp]
             L.rh_emf_upwind.restype = C.c_double
+        if variant == "fx":
+            L.prj_fx_configure.argtypes = [C.c_int, C.c_int]
+            L.prj_fx_active.restype = C.c_int
+        self.variant = variant
         self.nhydro = L.rh_nhydro()
         self.nstages = L.rh_nstages()
         if L.rh_nghost() != NG:
@@ -218,6 +227,23 @@ class Reference:
 
     def time_steps(self, nsteps: int, dt: float) -> float:
         return self.lib.rh_time_steps(nsteps, dt)
+
+    # -- the drop-in build ("fx") ----------------------------------------------
+    DROPIN_MIRROR, DROPIN_RESIDENT = 0, 1
+
+    def dropin_configure(self, form: int, mode: int) -> None:
+        """prj_fx_configure: the device form and where the state lives."""
+        self.lib.prj_fx_configure(form, mode)
+
+    def dropin_release(self) -> None:
+        self.lib.prj_fx_release()
+
+    def dropin_active(self) -> bool:
+        return bool(self.lib.prj_fx_active())
+
+    def dropin_to_host(self) -> None:
+        """prj_fx_to_host on the harness's mesh (resident mode)."""
+        self.lib.rh_dropin_to_host()
 
     def set_mhd_eta(self, eta: float) -> None:
         """Run-time resistivity (prj_mesh.mhd_eta)."""

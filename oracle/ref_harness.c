@@ -946,6 +946,15 @@ void rh_refill(void)
     prj_eos_fill_mesh(&g_sim.mesh, &g_sim.eos, &g_mpi, 1, PRJ_EOS_CTX_MAIN);
 }
 
+#ifdef PRJ_FX_WRAP
+/* The drop-in build: refresh the host arrays from the device (resident mode). */
+#include "prj_fx.h"
+void rh_dropin_to_host(void)
+{
+    prj_fx_to_host(&g_sim.mesh);
+}
+#endif
+
 /* The coarse/fine corrections of a stage (src/prj_timeint.c:2750, 528). */
 void rh_flux_send(void)
 {
