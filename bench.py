@@ -61,10 +61,10 @@ def parse():
                     help="skip the WENO-Z3 / eSSPRK10_4 variant measurements")
     ap.add_argument("--ref-adapt", action="store_true",
                     help="also time the reference's adapt on the dynamic-AMR mesh (about a minute of CPU)")
-    ap.add_argument("--amr-steps", type=int, default=10,
-                    help="batched steps of the static-AMR blast measurement (0: skip it)")
-    ap.add_argument("--collapse", action="store_true",
-                    help="also measure the 4-level gravity collapse (about 4600 blocks; slow set-up)")
+    ap.add_argument("--amr-steps", type=int, default=50,
+                    help="batched steps of the static-AMR measurements (0: skip them)")
+    ap.add_argument("--no-collapse", dest="collapse", action="store_false",
+                    help="skip the 4-level gravity collapse (about 4600 blocks; a minute of set-up)")
     ap.add_argument("--weno7-child", action="store_true",
                     help="internal: the WENO-Z7 measurement, run in a child process with FX_NGHOST=4")
     ap.add_argument("--shard", action="store_true",
@@ -77,17 +77,46 @@ def parse():
 # CPU reference (oracle/_ref: the reference's own C core), one process per core
 # ---------------------------------------------------------------------------
 
-def _cpu_worker(args):
-    nsteps, warm, root = args
+def _avx512() -> bool:
+    try:
+        with open("/proc/cpuinfo") as f:
+            return "avx512f" in f.read()
+    except OSError:
+        return False
+
+
+def _timing_variant() -> str:
+    """The reference build the CPU baseline times: the AVX-512 build
+    (x86-64-v4, same doubles as the parity build) where the host has it."""
     from oracle import ref as R
-    r = R.Reference(True)
-    p = R.params_fourier(root=root)
+    return "v4" if _avx512() and R.available(True, "v4") else ""
+
+
+# CPU-baseline samples: (reference preset, its arguments).  The reference has
+# no threads and this host has no MPI, so the baseline runs one independent
+# instance per core; each instance is a scaled-down case of the measured
+# workload (same recipe, same levels), small enough to time in seconds.
+CPU_SAMPLES = {
+    "fourier": ("params_fourier", dict(root=4)),
+    "blast": ("params_amr_blast", dict(root=4, max_level=2, radii=(0.4, 0.2))),
+    "collapse": ("params_collapse", dict(root=5)),
+}
+
+
+def _cpu_worker(args):
+    kind, nsteps, warm, variant = args
+    from oracle import ref as R
+    r = R.Reference(True, variant)
+    fn, kw = CPU_SAMPLES[kind]
+    p = getattr(R, fn)(**kw)
     r.setup(p)
+    ints, _, _ = r.mesh_arrays()
+    active = int((ints[:, 2] == 1).sum())
     dt = r.calc_dt()
     if warm:
         r.time_steps(warm, dt)
     secs = r.time_steps(nsteps, dt)
-    return nsteps * (root ** 3) * 4096, secs
+    return nsteps * active * 4096, secs, active
 
 
 def _cpu_variant_worker(variant):
@@ -135,22 +164,28 @@ def ref_adapt_sample():
                       "Loehner pressure 0.3 / 0.1 up to level 3, initial state"}
 
 
-def cpu_reference(steps: int, warmup: int, seconds: float):
-    """Reference CPU path on all host cores: one independent 2x2x2-block
-    (32^3-zone) instance of the workload per core, timed over `steps` steps.
-    The step count is bounded so the whole run takes about `seconds`."""
+def cpu_reference(steps: int, warmup: int, seconds: float, kind: str = "fourier"):
+    """Reference CPU path on all host cores: one independent instance of a
+    scaled-down case of the workload per core (CPU_SAMPLES), timed over a
+    bounded number of RK2 steps, then zone-updates/s summed over the cores
+    (zones of every instance / the slowest instance's time).  The step count
+    is bounded so the timed part takes about `seconds`."""
     cores = min(len(os.sched_getaffinity(0)), 128)
+    variant = _timing_variant()
     ctx = mp.get_context("spawn")
-    # ~0.14 s per step per 2^3-block instance on one core: bound the sample
-    steps = max(1, min(steps, int(seconds / 0.15)))
+    # seconds per RK2 step of one instance on one core (AVX-512 build)
+    per_step = {"fourier": 0.9, "blast": 6.0, "collapse": 8.0}[kind]
+    steps = max(1, min(steps, int(seconds / per_step)))
     with ctx.Pool(cores) as pool:
-        res = pool.map(_cpu_worker, [(steps, warmup, 2)] * cores)
-    zones = sum(z for z, _ in res)
-    wall = max(s for _, s in res)
+        res = pool.map(_cpu_worker, [(kind, steps, warmup, variant)] * cores)
+    zones = sum(z for z, _, _ in res)
+    wall = max(t for _, t, _ in res)
+    fn, kw = CPU_SAMPLES[kind]
+    build = "-O3 -march=x86-64-v4 -ffp-contract=off (AVX-512)" if variant == "v4" else "-O3 -march=x86-64-v3 -ffp-contract=off"
     return {"value": zones / wall, "unit": UNIT, "cores": cores, "kind": "reference",
-            "sample": f"{cores} independent instances of the workload recipe on 2^3 blocks of 16^3 "
-                      f"(32^3 zones each), {steps} RK2 steps each, serial reference C core "
-                      f"(-O3 -ffp-contract=off), one process per core"}
+            "sample": f"{cores} independent instances of {fn}({', '.join(f'{k}={v}' for k, v in kw.items())}) "
+                      f"({res[0][2]} active blocks of 16^3 each), {steps} RK2 step(s) each after {warmup} untimed, "
+                      f"serial reference C core ({build}), one process per core; no MPI on this host"}
 
 
 # ---------------------------------------------------------------------------
@@ -781,6 +816,14 @@ def main():
             cv = cpu_variants()
         except Exception as exc:
             cv = {"unavailable": str(exc)}
+    cb_amr = {}
+    if rank == 0 and world == 1 and not args.no_cpu_baseline and args.amr_steps > 0:
+        for kind in ("blast",) + (("collapse",) if args.collapse else ()):
+            try:
+                cb_amr[kind] = cpu_reference(1, 0, 1.0, kind)
+            except Exception as exc:
+                cb_amr[kind] = {"value": None, "unit": UNIT, "cores": 0, "kind": "reference",
+                                "sample": f"unavailable: {exc}"}
     ra = None
     if rank == 0 and world == 1 and args.ref_adapt:
         try:
@@ -812,8 +855,10 @@ def main():
         line["variants"].update(run_weno7(args))
     if world == 1 and args.amr_steps > 0:
         line["amr_blast"] = run_amr(args, local_rank, "blast")
+        line["amr_blast"]["cpu_reference"] = cb_amr.get("blast")
         if args.collapse:
             line["amr_collapse"] = run_amr(args, local_rank, "collapse")
+            line["amr_collapse"]["cpu_reference"] = cb_amr.get("collapse")
     if world == 1 and args.amr_dynamic_adapts > 0:
         line["amr_dynamic"] = run_amr_dynamic(args, local_rank)
         if ra is not None:

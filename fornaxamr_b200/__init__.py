@@ -414,6 +414,15 @@ class Context:
         self._check(self.L.fx_autotune(self._h, _dp(times), 16, C.byref(choice)))
         return choice.value, times
 
+    def branch_signature_start(self) -> None:
+        """Starts the plain form's branch signature (fx_branch_signature)."""
+        self._check(self.L.fx_branch_signature(self._h, 1, None))
+
+    def branch_signature_stop(self) -> int:
+        v = C.c_ulonglong(0)
+        self._check(self.L.fx_branch_signature(self._h, 0, C.byref(v)))
+        return v.value
+
     def set_flux_shape(self, variant: int) -> None:
         """Force a face-kernel launch shape (see fx_set_flux_shape)."""
         self._check(self.L.fx_set_flux_shape(self._h, variant))

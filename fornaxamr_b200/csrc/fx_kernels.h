@@ -59,6 +59,10 @@ struct FxDev {
     FxCtl *ctl;
     int flux_variant;         /* launch shape of the face kernel (autotuned) */
     int recon;                /* FX_RECON_MC or FX_RECON_WENO3 */
+    /* branch signature of the plain form (null unless requested): the
+     * per-block face and edge kernels add a hash of every face's MC limiter
+     * regimes and HLLD decisions and every edge's upwind directions */
+    unsigned long long *bsig;
     double *W2;   /* eSSPRK10_4 stage slot 2 of W: [b][v][cell] (null for RK2) */
     double *Bf2;  /* eSSPRK10_4 stage slot 2 of Bf: [b][dir][face] (null for RK2 or hydro) */
 };

@@ -941,17 +941,17 @@ int fx_create(int device, const fx_config *cfg, fx_ctx **out)
     if (cudaSetDevice(device) != cudaSuccess ||
         cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess ||
         cudaMalloc((void **)&c->d_err, sizeof(FxErr)) != cudaSuccess ||
-        cudaMalloc((void **)&c->d_red, 2 * sizeof(unsigned long long)) != cudaSuccess ||
+        cudaMalloc((void **)&c->d_red, 3 * sizeof(unsigned long long)) != cudaSuccess ||
         cudaMalloc((void **)&c->d_ctl, sizeof(FxCtl)) != cudaSuccess ||
         cudaMallocHost((void **)&c->h_err, sizeof(FxErr)) != cudaSuccess ||
-        cudaMallocHost((void **)&c->h_red, 2 * sizeof(unsigned long long)) != cudaSuccess ||
+        cudaMallocHost((void **)&c->h_red, 3 * sizeof(unsigned long long)) != cudaSuccess ||
         cudaMallocHost((void **)&c->h_ctl, sizeof(FxCtl)) != cudaSuccess) {
         fx_destroy(c);
         return FX_ECUDA;
     }
     cudaMemsetAsync(c->d_err, 0, sizeof(FxErr), c->stream);
     cudaMemsetAsync(c->d_ctl, 0, sizeof(FxCtl), c->stream);
-    cudaMemsetAsync(c->d_red, 0, 2 * sizeof(unsigned long long), c->stream);
+    cudaMemsetAsync(c->d_red, 0, 3 * sizeof(unsigned long long), c->stream);
     if (cudaStreamSynchronize(c->stream) != cudaSuccess) {
         fx_destroy(c);
         return FX_ECUDA;
@@ -1738,6 +1738,27 @@ int fx_autotune(fx_ctx *c, double *times_ms, int n, int *choice)
     free_graphs(c); /* captured graphs hold the previous launch shape */
     *choice = best;
     return check_device_error(c);
+}
+
+int fx_branch_signature(fx_ctx *c, int enable, unsigned long long *value)
+{
+    if (!c) return FX_EINVAL;
+    if (enable) {
+        FX_CUDA(c, cudaMemsetAsync(c->d_red + 2, 0, sizeof(unsigned long long), c->stream));
+        c->D.bsig = c->d_red + 2;
+        free_graphs(c); /* captured graphs hold the previous device view */
+        return FX_SUCCESS;
+    }
+    if (!value) return set_err(c, FX_EINVAL, "fx_branch_signature: null value");
+    if (!c->D.bsig) return set_err(c, FX_EINVAL, "fx_branch_signature: not enabled");
+    FX_CUDA(c, cudaMemcpyAsync(c->h_red + 2, c->d_red + 2, sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+        c->stream));
+    const int rc = sync_and_check(c);
+    c->D.bsig = nullptr;
+    free_graphs(c);
+    if (rc) return rc;
+    *value = c->h_red[2];
+    return FX_SUCCESS;
 }
 
 int fx_set_flux_shape(fx_ctx *c, int variant)

@@ -427,6 +427,20 @@ int fx_amr_remesh_host(const fx_config *cfg, const fx_amr_config *amr, int nbloc
  * level apart.  The product's mesh builders use this one restatement. */
 int fx_mesh_slot_geometry(int nblocks, fx_block_desc *blocks);
 
+/* Branch signature of the plain form (no reference counterpart; for checks
+ * of the discrete adjoint against finite differences).  enable = 1 zeroes
+ * a device sum and makes every following per-block face and edge launch add
+ * a hash of each face's decisions (the MC limiter's selected candidate for
+ * every reconstructed quantity, the HLLD wave-speed arguments, clamped
+ * discriminants, fan region, bn_small, contact side, sign of bn, single or
+ * double star, degenerate outer-star denominators) and each edge's upwind
+ * directions (src/prj_reconstruct.h:355-375, src/prj_riemann.c:117-440,
+ * src/prj_mhd.c:627-680); enable = 0 returns the sum in *value and stops.
+ * Two runs with equal sums took the same branches everywhere (up to hash
+ * collisions, about 2^-64).  MHD with MC reconstruction; the batched form
+ * does not add to it. */
+int fx_branch_signature(fx_ctx *ctx, int enable, unsigned long long *value);
+
 /* ---- measurement --------------------------------------------------------------- */
 
 /* phases for fx_time_phase: the batched sweep of one phase over all blocks */
