@@ -339,6 +339,16 @@ class Context:
         self._check(self.L.fx_download_state(self._h, w, f))
         self.sync()
 
+    def upload_state_active(self, W_all: np.ndarray, Bf_all: Optional[np.ndarray]) -> None:
+        """fx_upload_state_active: slot 0 of the active cells and faces from
+        page-locked host arrays (e.g. torch pin_memory), then the ghost fill."""
+        self._check(self.L.fx_upload_state_active(self._h, W_all.ctypes.data,
+                                                  None if Bf_all is None else Bf_all.ctypes.data))
+
+    def download_state_active(self, W_all: np.ndarray, Bf_all: Optional[np.ndarray]) -> None:
+        self._check(self.L.fx_download_state_active(self._h, W_all.ctypes.data,
+                                                    None if Bf_all is None else Bf_all.ctypes.data))
+
     def download_array(self, b: int, which: int, dir_: int = 0) -> np.ndarray:
         sizes = {ARR_W: self.nv * self.ns * NCELLS, ARR_EOSVAR: 3 * NCELLS, ARR_RHS: self.nv * NCELLS,
                  ARR_FLUX: self.nv * NCELLS, ARR_VRIEMANN: 3 * NCELLS, ARR_GRAV: NCELLS,

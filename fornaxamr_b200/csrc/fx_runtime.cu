@@ -1366,6 +1366,49 @@ int fx_download_state(fx_ctx *c, double *W_all, double *Bf_all)
     return FX_SUCCESS;
 }
 
+/* device-mapped alias of a page-locked host buffer, or null */
+double *mapped_host(const void *p)
+{
+    if (!p) return nullptr;
+    cudaPointerAttributes a{};
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return nullptr;
+    }
+    if (a.type != cudaMemoryTypeHost || !a.devicePointer) return nullptr;
+    return static_cast<double *>(a.devicePointer);
+}
+
+int active_state(fx_ctx *c, double *W_all, double *Bf_all, bool to_device, const char *fn)
+{
+    if (c && c->nranks > 1) return set_err(c, FX_EINVAL, "%s: not available on a sharded mesh", fn);
+    if (!has_mesh(c)) return c ? set_err(c, FX_ENOMESH, "no mesh") : FX_EINVAL;
+    if (!W_all) return set_err(c, FX_EINVAL, "%s: W_all is required", fn);
+    double *hW = mapped_host(W_all);
+    double *hB = c->cfg.mhd ? mapped_host(Bf_all) : nullptr;
+    if (!hW || (c->cfg.mhd && Bf_all && !hB)) {
+        return set_err(c, FX_EINVAL, "%s: the host arrays must be page-locked (cudaHostAlloc / cudaHostRegister)", fn);
+    }
+    fx_launch_active_state(c->D, c->d_active, c->nactive, hW, hB, host_ns(c), to_device, c->stream);
+    FX_CUDA(c, cudaGetLastError());
+    return FX_SUCCESS;
+}
+
+int fx_upload_state_active(fx_ctx *c, const double *W_all, const double *Bf_all)
+{
+    int rc = active_state(c, const_cast<double *>(W_all), const_cast<double *>(Bf_all), true, __func__);
+    if (rc) return rc;
+    /* the ghost cells and faces of slot 0 from the active ones: the fill
+     * that produced the host's ghost zones (src/main.c:446) */
+    return fx_boundary_fill_ghosts_and_bf(c, 1, 0);
+}
+
+int fx_download_state_active(fx_ctx *c, double *W_all, double *Bf_all)
+{
+    const int rc = active_state(c, W_all, Bf_all, false, __func__);
+    return rc ? rc : sync_and_check(c);
+}
+
 int fx_download_array(fx_ctx *c, int b, int which, int dir, double *out)
 {
     if (c && c->nranks > 1) return set_err(c, FX_EINVAL, "%s: not available on a sharded mesh", __func__);
