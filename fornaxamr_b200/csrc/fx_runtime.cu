@@ -1394,9 +1394,58 @@ int active_state(fx_ctx *c, double *W_all, double *Bf_all, bool to_device, const
     return FX_SUCCESS;
 }
 
+/* Host -> device copy of slot 0's active region by the copy engines: one
+ * 3-D copy for W over (block, variable) planes, one per Bf direction over
+ * blocks; every copied row is the whole span of one i-plane's active rows
+ * (ghost columns along k included), 2.5-2.7 KB, so the engines run at full
+ * rate.  Every block entry (active or not) is covered. */
+int dma_active_h2d(fx_ctx *c, const double *W_all, const double *Bf_all)
+{
+    constexpr size_t P = FX_PBS;
+    constexpr size_t G = FX_NG;
+    constexpr size_t B = FX_BS;
+    const size_t hs = (size_t)host_ns(c);
+    const size_t nb = (size_t)c->nblocks;
+    auto copy3d = [&](const double *src, size_t src_ysize, double *dst, size_t dst_ysize, size_t pitch_el,
+                      size_t width_el, size_t height, size_t depth) -> cudaError_t {
+        cudaMemcpy3DParms p{};
+        p.srcPtr = make_cudaPitchedPtr(const_cast<double *>(src), pitch_el * sizeof(double), width_el * sizeof(double),
+            src_ysize);
+        p.dstPtr = make_cudaPitchedPtr(dst, pitch_el * sizeof(double), width_el * sizeof(double), dst_ysize);
+        p.extent = make_cudaExtent(width_el * sizeof(double), height, depth);
+        p.kind = cudaMemcpyHostToDevice;
+        return cudaMemcpy3DAsync(&p, c->stream);
+    };
+    if (W_all) {
+        /* cell (i, j, k) = (i + G) P^2 + (j + G) P + (k + G); rows: i-planes of
+         * the active j range, z: (block, variable) with hs (2) slots apart */
+        const size_t off = G * P * P + G * P;
+        FX_CUDA(c, copy3d(W_all + off, hs * P, c->d_W + off, (size_t)FX_NSTAGES * P, P * P, B * P, B,
+            nb * (size_t)c->nv));
+    }
+    if (Bf_all && c->cfg.mhd) {
+        for (int d = 0; d < 3; ++d) {
+            /* face strides: i-planes P^2 (d = 0) or P (P + 1); rows P (d = 0, 1) or P + 1 */
+            const size_t plane = d == 0 ? P * P : P * (P + 1);
+            const size_t row = d == 2 ? P + 1 : P;
+            const size_t nplanes = d == 0 ? B + 1 : B;
+            const size_t nrows = d == 1 ? B + 1 : B;
+            const size_t off = G * plane + G * row;
+            const size_t hoff = (size_t)d * hs * FX_NFACES + off;
+            const size_t doff = (size_t)d * FX_NSTAGES * FX_NFACES + off;
+            FX_CUDA(c, copy3d(Bf_all + hoff, 3 * hs * FX_NFACES / plane, c->d_Bf + doff,
+                3 * (size_t)FX_NSTAGES * FX_NFACES / plane, plane, nrows * row, nplanes, nb));
+        }
+    }
+    return FX_SUCCESS;
+}
+
 int fx_upload_state_active(fx_ctx *c, const double *W_all, const double *Bf_all)
 {
-    int rc = active_state(c, const_cast<double *>(W_all), const_cast<double *>(Bf_all), true, __func__);
+    if (c && c->nranks > 1) return set_err(c, FX_EINVAL, "%s: not available on a sharded mesh", __func__);
+    if (!has_mesh(c)) return c ? set_err(c, FX_ENOMESH, "no mesh") : FX_EINVAL;
+    if (!W_all) return set_err(c, FX_EINVAL, "%s: W_all is required", __func__);
+    int rc = dma_active_h2d(c, W_all, Bf_all);
     if (rc) return rc;
     /* the ghost cells and faces of slot 0 from the active ones: the fill
      * that produced the host's ghost zones (src/main.c:446) */

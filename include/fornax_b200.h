@@ -250,18 +250,24 @@ int fx_download_all(fx_ctx *ctx, double *W_all, double *Bf_all);
  * prj_timeint_step (slot 1 is the step's scratch). */
 int fx_upload_state(fx_ctx *ctx, const double *W_all, const double *Bf_all);
 int fx_download_state(fx_ctx *ctx, double *W_all, double *Bf_all);
-/* The state through its active region only: stage slot 0 of the active
- * blocks' 16^3 active cells (every variable) and their active faces (17 x 16
- * x 16 per direction), in the host layout of fx_upload_state, moved by
- * kernels that read and write the host arrays directly over the bus -- about
- * half the bytes of fx_upload_state for 16^3 blocks with two ghost layers.
- * The host arrays must be page-locked (cudaHostAlloc, cudaMallocHost or
- * cudaHostRegister), else FX_EINVAL.  fx_upload_state_active then runs the
- * ghost fill of slot 0 (prj_boundary_fill_ghosts_and_bf with stage 1 and
- * the stage-0 field), so the device state equals the one fx_upload_state
- * gives when the host's ghost zones come from that fill, as they do after
- * every reference step; fx_download_state_active synchronises and leaves
- * the host's ghost entries, other slots and inactive blocks untouched. */
+/* The state through its active region: stage slot 0 of the 16^3 active
+ * cells (every variable) and the active faces (17 x 16 x 16 per direction),
+ * in the host layout of fx_upload_state -- about two thirds (upload) and one
+ * half (download) of fx_upload_state's bytes for 16^3 blocks with two ghost
+ * layers.  fx_upload_state_active moves, per block, the rows of the active
+ * (i, j) range whole (ghost columns along k included) with the copy engines,
+ * then runs the ghost fill of slot 0 (prj_boundary_fill_ghosts_and_bf with
+ * stage 1 and the stage-0 field).  fx_download_state_active writes only the
+ * active entries of slot 0 of the active blocks, with kernels that store
+ * straight into the host arrays, and synchronises; its host arrays must be
+ * page-locked (cudaHostAlloc, cudaMallocHost or cudaHostRegister), else
+ * FX_EINVAL.  The ghost fill does not write every ghost entry: a few of the
+ * outermost ghost faces and corner cells keep the values the set-up gave
+ * them, in the reference as here.  Make one full transfer (fx_upload_state
+ * or fx_upload_all) first; from then on the device state after
+ * fx_upload_state_active equals the one fx_upload_state gives whenever the
+ * host's ghost zones come from that fill, as they do after every reference
+ * step. */
 int fx_upload_state_active(fx_ctx *ctx, const double *W_all, const double *Bf_all);
 int fx_download_state_active(fx_ctx *ctx, double *W_all, double *Bf_all);
 /* Any block array, including the step's scratch, for inspection. */

