@@ -424,13 +424,18 @@ class Context:
         self._check(self.L.fx_autotune(self._h, _dp(times), 16, C.byref(choice)))
         return choice.value, times
 
-    def branch_signature_start(self) -> None:
-        """Starts the plain form's branch signature (fx_branch_signature)."""
-        self._check(self.L.fx_branch_signature(self._h, 1, None))
+    def branch_record(self, max_stages: int) -> None:
+        """fx_branch_trace(RECORD): the next plain-form stages record their decisions."""
+        self._check(self.L.fx_branch_trace(self._h, _lib.BRANCH_RECORD, int(max_stages), None))
 
-    def branch_signature_stop(self) -> int:
+    def branch_replay(self) -> None:
+        """fx_branch_trace(REPLAY): the next plain-form stages replay them."""
+        self._check(self.L.fx_branch_trace(self._h, _lib.BRANCH_REPLAY, 0, None))
+
+    def branch_off(self) -> int:
+        """fx_branch_trace(OFF); returns the decisions the last replay overrode."""
         v = C.c_ulonglong(0)
-        self._check(self.L.fx_branch_signature(self._h, 0, C.byref(v)))
+        self._check(self.L.fx_branch_trace(self._h, _lib.BRANCH_OFF, 0, C.byref(v)))
         return v.value
 
     def set_flux_shape(self, variant: int) -> None:

@@ -17,6 +17,8 @@
  */
 #include <cuda_runtime.h>
 
+#include <type_traits>
+
 #include "../../include/fornax_b200.h"
 #include "fx_kernels.h"
 #include "fx_physics.cuh"
@@ -86,139 +88,26 @@ __device__ __forceinline__ void fx_recon_pair(const double (&q)[FxStencil<RECON>
     }
 }
 
-/* ---- branch signature (a diagnostic of the plain form) ------------------ */
-/* The map from initial data to a later state is smooth except where a
- * branch of the arithmetic switches (the limiter's selection, the Riemann
- * fan, the upwind direction).  With FxDev::bsig set, the per-block kernels
- * add a hash of every such decision to one 64-bit sum, so two runs that
- * took the same branches everywhere give the same sum; finite-difference
- * checks of the adjoint use it to keep only probes that cross no switch. */
-__device__ __forceinline__ unsigned long long fx_sig_hash(unsigned long long key, unsigned long long code)
+/* MC face values of a 4-cell stencil with the limiter's selections through
+ * a branch policy: bits 4 q + 0 and 4 q + 2 of the face's word */
+template <class BR>
+__device__ __forceinline__ void fx_recon_pair_br(const double (&q)[4], double &wl, double &wr, BR &br, int q4)
 {
-    unsigned long long z = key * 0x9E3779B97F4A7C15ULL ^ (code + 0x632BE59BD9B4E019ULL);
-    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
-    z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
-    return z ^ (z >> 31);
+    wl = q[1] + 0.5 * fx_mc_slope_br(q[0], q[1], q[2], br, q4);
+    wr = q[2] - 0.5 * fx_mc_slope_br(q[1], q[2], q[3], br, q4 + 2);
 }
 
-/* which candidate fx_mc_slope selects: 0, 1, 2 (c0, c1, c2), 3 for zero */
-__device__ __forceinline__ unsigned fx_mc_regime(double qm, double q0, double qp)
-{
-    const double sl = q0 - qm;
-    const double sr = qp - q0;
-    if (!(sl * sr > 0.0)) {
-        return 3u;
-    }
-    const double c0 = 2.0 * sl;
-    const double c1 = sl + 0.5 * (sr - sl);
-    const double c2 = 2.0 * sr;
-    if (sl > 0.0) {
-        const double m = c0 < c1 ? c0 : c1;
-        return m < c2 ? (c0 < c1 ? 0u : 1u) : 2u;
-    }
-    const double m = c0 > c1 ? c0 : c1;
-    return m > c2 ? (c0 > c1 ? 0u : 1u) : 2u;
-}
-
-/* the decisions of fx_riemann_hlld_folded for one face, same arithmetic:
- * bits 0-1 which side gives SL / SR, 2-3 clamped fast-speed discriminants,
- * 4-6 fan region (0 left supersonic, 1 right supersonic, 2 HLL fallback,
- * 3 star), 7 bn_small, 8 contact side, 9 sign of bn, 10 single star,
- * 11-12 degenerate outer-star denominators (near, far) */
-__device__ unsigned fx_hlld_regime(const double *WL, const double *WR, double pL, double pR,
-    double gL, double gR, double bn)
-{
-    FxHlldState L, R;
-    fx_hlld_state(WL, pL, gL, bn, L, nullptr, 0, 0);
-    fx_hlld_state(WR, pR, gR, bn, R, nullptr, 0, 0);
-    unsigned code = 0;
-    const FxHlldState *S[2] = {&L, &R};
-    for (int n = 0; n < 2; ++n) {
-        const FxHlldState &s = *S[n];
-        const double a2 = s.gamma * s.p / s.rho;
-        const double bx2_rho = s.bx * s.bx / s.rho;
-        const double b2_rho = (s.bx * s.bx + s.by * s.by + s.bz * s.bz) / s.rho;
-        const double disc = (a2 + b2_rho) * (a2 + b2_rho) - 4.0 * a2 * bx2_rho;
-        code |= (disc < 0.0 ? 1u : 0u) << (2 + n);
-    }
-    const double cfL = fx_hlld_fast_speed(L, nullptr, 0, 0);
-    const double cfR = fx_hlld_fast_speed(R, nullptr, 0, 0);
-    const double aL = L.vx - cfL, aR = R.vx - cfR;
-    const double bL = L.vx + cfL, bR = R.vx + cfR;
-    code |= (aL < aR ? 0u : 1u) | ((bL > bR ? 0u : 1u) << 1);
-    const double SL = fx_min(aL, aR);
-    const double SR = fx_max(bL, bR);
-    if (0.0 <= SL) return code;
-    if (SR <= 0.0) return code | (1u << 4);
-    const double denom = R.rho * (SR - R.vx) - L.rho * (SL - L.vx);
-    const double SM = (R.rho * R.vx * (SR - R.vx) -
-        L.rho * L.vx * (SL - L.vx) + (L.pt - R.pt)) / denom;
-    const double pt_star_l = L.pt + L.rho * (SL - L.vx) * (SM - L.vx);
-    const double pt_star_r = R.pt + R.rho * (SR - R.vx) * (SM - R.vx);
-    const double pt_star = 0.5 * (pt_star_l + pt_star_r);
-    if (pt_star <= 0.0 || !isfinite(pt_star)) return code | (2u << 4);
-    code |= 3u << 4;
-    const bool left = (0.0 <= SM);
-    code |= (0.5 * bn * bn < FX_HLLD_SMALL * pt_star ? 1u : 0u) << 7;
-    code |= (left ? 1u : 0u) << 8;
-    code |= (bn < 0.0 ? 1u : 0u) << 9;
-    const FxHlldState &N = left ? L : R;
-    const FxHlldState &F = left ? R : L;
-    const double SN = left ? SL : SR;
-    const double SF = left ? SR : SL;
-    FxHlldStar Ns;
-    fx_hlld_outer_star(N, SN, SM, pt_star, Ns, nullptr, 0, 0);
-    {
-        const double alpha = SN - N.vx;
-        const double dn = N.rho * alpha * (SN - SM) - N.bx * N.bx;
-        code |= (fabs(dn) < FX_HLLD_SMALL * pt_star ? 1u : 0u) << 11;
-    }
-    const double a = fabs(bn) / sqrt(Ns.rho);
-    const double SNs = left ? SM - a : SM + a;
-    const bool single = (left ? (0.0 <= SNs) : (SNs <= 0.0)) || (code >> 7 & 1u);
-    code |= (single ? 1u : 0u) << 10;
-    if (!single) {
-        const double alpha = SF - F.vx;
-        const double df = F.rho * alpha * (SF - SM) - F.bx * F.bx;
-        code |= (fabs(df) < FX_HLLD_SMALL * pt_star ? 1u : 0u) << 12;
-    }
-    return code;
-}
-
-/* the face's MC regimes (9 reconstructed quantities incl. pressure, two
- * slopes each) and HLLD decisions, hashed into D.bsig */
-__device__ void fx_sig_face(const FxDev &D, const double *Wb, int b, int dir, int cR, int s,
-    const double *WL, const double *WR, double pL, double pR, double g, double bn)
-{
-    constexpr int kPlaneS = FX_NSTAGES * FX_NCELLS;
-    const int c0 = cR - 2 * s;
-    unsigned long long mc = 0;
-    double rho[4], eint[4];
-    for (int n = 0; n < 4; ++n) {
-        rho[n] = Wb[(size_t)FX_RHO * kPlaneS + c0 + n * s];
-        eint[n] = Wb[(size_t)FX_EINT * kPlaneS + c0 + n * s];
-    }
-    /* the 9 variables (the normal field comes from the face, not
-     * reconstructed) and, as v = 9, the pressure */
-    for (int v = 0; v < 10; ++v) {
-        if (v == FX_B1 + dir) {
-            continue;
-        }
-        double q[4];
-        for (int n = 0; n < 4; ++n) {
-            q[n] = v == 9 ? fx_pressure(g, rho[n], eint[n]) : Wb[(size_t)v * kPlaneS + c0 + n * s];
-        }
-        mc = mc << 4 | fx_mc_regime(q[0], q[1], q[2]) << 2 | fx_mc_regime(q[1], q[2], q[3]);
-    }
-    const unsigned hl = fx_hlld_regime(WL, WR, pL, pR, g, g, bn);
-    const unsigned long long key = ((unsigned long long)(b * 3 + dir) << 32) | (unsigned)cR;
-    atomicAdd(D.bsig, fx_sig_hash(key, mc ^ ((unsigned long long)hl << 40)));
-}
-
-template <bool MHD, bool FULL, int TPB, int MINB, int RECON>
+/* BRM: 0 the solver as it stands; 1 record / 2 replay every face's
+ * decisions in D.br_words (FxBrRecord / FxBrReplay; MHD, MC and the plain
+ * form only), the branch-frozen map the adjoint checks use */
+template <bool MHD, bool FULL, int TPB, int MINB, int RECON, int BRM = 0>
 __global__ void __launch_bounds__(TPB, MINB) k_flux(FxDev D, const int *__restrict__ blist,
     int wslot, int bfslot)
 {
+    static_assert(BRM == 0 || (MHD && FULL && RECON == FX_RECON_MC), "decision record / replay: MHD, MC, plain");
+    using Br = typename std::conditional<BRM == 1, FxBrRecord,
+        typename std::conditional<BRM == 2, FxBrReplay, FxBrFree>::type>::type;
+    Br br;
     if (D.ctl->skip) {
         return;
     }
@@ -234,6 +123,11 @@ __global__ void __launch_bounds__(TPB, MINB) k_flux(FxDev D, const int *__restri
     int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= NF) {
         return;
+    }
+    /* this face's decision word (record / replay) */
+    const size_t bri = D.br_off + ((size_t)b * 3 + dir) * NF + t;
+    if constexpr (BRM == 2) {
+        br.w = D.br_words[bri];
     }
     const int e2 = dir == 2 ? FX_BS + 1 : T;
     const int e1 = dir == 1 ? FX_BS + 1 : T;
@@ -264,8 +158,13 @@ __global__ void __launch_bounds__(TPB, MINB) k_flux(FxDev D, const int *__restri
             eintS[n] = qe[n * s];
         }
     }
-    fx_recon_pair<RECON>(rhoS, WL[FX_RHO], WR[FX_RHO]);
-    fx_recon_pair<RECON>(eintS, WL[FX_EINT], WR[FX_EINT]);
+    if constexpr (BRM == 0) {
+        fx_recon_pair<RECON>(rhoS, WL[FX_RHO], WR[FX_RHO]);
+        fx_recon_pair<RECON>(eintS, WL[FX_EINT], WR[FX_EINT]);
+    } else {
+        fx_recon_pair_br(rhoS, WL[FX_RHO], WR[FX_RHO], br, 4 * FX_RHO);
+        fx_recon_pair_br(eintS, WL[FX_EINT], WR[FX_EINT], br, 4 * FX_EINT);
+    }
 #pragma unroll
     for (int lv = 1; lv < nv; ++lv) {
         if (lv == FX_EINT || (MHD && lv == FX_B1)) {
@@ -277,7 +176,11 @@ __global__ void __launch_bounds__(TPB, MINB) k_flux(FxDev D, const int *__restri
         for (int n = 0; n < NS; ++n) {
             qs[n] = q[n * s];
         }
-        fx_recon_pair<RECON>(qs, WL[lv], WR[lv]);
+        if constexpr (BRM == 0) {
+            fx_recon_pair<RECON>(qs, WL[lv], WR[lv]);
+        } else {
+            fx_recon_pair_br(qs, WL[lv], WR[lv], br, 4 * lv);
+        }
     }
     double pS[NS];
 #pragma unroll
@@ -285,7 +188,12 @@ __global__ void __launch_bounds__(TPB, MINB) k_flux(FxDev D, const int *__restri
         pS[n] = fx_pressure(g, rhoS[n], eintS[n]);
     }
     double pL, pR;
-    fx_recon_pair<RECON>(pS, pL, pR);
+    if constexpr (BRM == 0) {
+        fx_recon_pair<RECON>(pS, pL, pR);
+    } else {
+        /* the pressure takes the normal field's (unreconstructed) bits */
+        fx_recon_pair_br(pS, pL, pR, br, 4 * FX_B1);
+    }
     /* gamma is uniform for the ideal gas: its MC slope is exactly 0, so the
      * MC face values equal g bit for bit; the WENO weights of a constant
      * stencil are evaluated as the reference does (their sum need not be 1) */
@@ -306,10 +214,14 @@ __global__ void __launch_bounds__(TPB, MINB) k_flux(FxDev D, const int *__restri
         WL[FX_B1] = bn;
         WR[FX_B1] = bn;
         FxFaceOut o;
-        fx_riemann_hlld_folded(WL, WR, pL, pR, gL, gR, bn, o, D.err, b, cR);
-        if constexpr (FULL && RECON == FX_RECON_MC) {
-            if (D.bsig != nullptr) {
-                fx_sig_face(D, Wb, b, dir, cR, s, WL, WR, pL, pR, g, bn);
+        if constexpr (BRM == 0) {
+            fx_riemann_hlld_folded(WL, WR, pL, pR, gL, gR, bn, o, D.err, b, cR);
+        } else {
+            fx_riemann_hlld_folded_br(WL, WR, pL, pR, gL, gR, bn, o, D.err, b, cR, br);
+            if constexpr (BRM == 1) {
+                D.br_words[bri] = br.w;
+            } else if (br.flips) {
+                atomicAdd(D.br_flips, (unsigned long long)br.flips);
             }
         }
 #pragma unroll
@@ -382,6 +294,7 @@ __global__ void __launch_bounds__(128) k_emf_edges(FxDev D, const int *__restric
     }
     const int dir = t / NE;
     t -= dir * NE;
+    const int te = t; /* edge index within the direction */
     const int x2 = dir == 2 ? FX_BS : FX_BS + 1;
     const int x1 = dir == 1 ? FX_BS : FX_BS + 1;
     int e[3];
@@ -418,14 +331,6 @@ __global__ void __launch_bounds__(128) k_emf_edges(FxDev D, const int *__restric
     vn[2] = vrr[fx_bidx_cell(3, right, c1)];
     vn[3] = vru[fx_bidx_cell(3, up, c3)];
     const int eidx = fx_edge_idx(dir, e[0], e[1], e[2]);
-    if (D.bsig != nullptr) {
-        unsigned code = 0;
-        for (int n = 0; n < 4; ++n) {
-            code = code * 3u + (vn[n] > 0.0 ? 0u : vn[n] < 0.0 ? 1u : 2u);
-        }
-        const unsigned long long key = (1ULL << 62) | ((unsigned long long)(b * 3 + dir) << 32) | (unsigned)eidx;
-        atomicAdd(D.bsig, fx_sig_hash(key, code));
-    }
     for (int n = 0; n < 4; ++n) {
         if (!isfinite(f[n]) || !isfinite(c[n]) || !isfinite(vn[n])) {
             fx_fail(D.err, FX_ERR_EMF_NONFINITE, b, eidx);
@@ -448,7 +353,25 @@ __global__ void __launch_bounds__(128) k_emf_edges(FxDev D, const int *__restric
         }
     }
     const double eta = D.mhd_eta + eta_cells;
-    double emf = fx_emf_upwind(f, c, vn);
+    double emf;
+    if (D.br_mode == 0) {
+        emf = fx_emf_upwind(f, c, vn);
+    } else {
+        /* this edge's decision word (record / replay) */
+        const size_t bri = D.br_eoff + ((size_t)b * 3 + dir) * NE + te;
+        if (D.br_mode == 1) {
+            FxBrRecord br;
+            emf = fx_emf_upwind_br(f, c, vn, br);
+            D.br_edges[bri] = br.w;
+        } else {
+            FxBrReplay br;
+            br.w = D.br_edges[bri];
+            emf = fx_emf_upwind_br(f, c, vn, br);
+            if (br.flips) {
+                atomicAdd(D.br_flips, (unsigned long long)br.flips);
+            }
+        }
+    }
     if (eta != 0.0) {
         /* resistive term, src/prj_mhd.c:682-709 */
         const double *bf = D.Bf + (size_t)b * FX_BF_COUNT;
@@ -1552,6 +1475,17 @@ void fx_launch_flux(const FxDev &D, const int *blist, int nlist, int ndir, int w
     int full, cudaStream_t s)
 {
     if (nlist <= 0) return;
+    if (D.br_mode != 0 && full && D.nv == 9 && D.recon == FX_RECON_MC) {
+        /* the plain form recording or replaying its decisions */
+        constexpr int nf = (FX_BS + 1) * (FX_BS + 2) * (FX_BS + 2);
+        const dim3 g(fx_blocks(nf, 128), ndir, nlist);
+        if (D.br_mode == 1) {
+            k_flux<true, true, 128, 4, FX_RECON_MC, 1><<<g, 128, 0, s>>>(D, blist, wslot, bfslot);
+        } else {
+            k_flux<true, true, 128, 4, FX_RECON_MC, 2><<<g, 128, 0, s>>>(D, blist, wslot, bfslot);
+        }
+        return;
+    }
     const int v = D.flux_variant;
     if (D.nv == 9) {
         if (full) launch_flux_variant<true, true>(D, blist, nlist, ndir, wslot, bfslot, v, s);

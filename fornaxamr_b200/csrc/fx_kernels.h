@@ -59,10 +59,14 @@ struct FxDev {
     FxCtl *ctl;
     int flux_variant;         /* launch shape of the face kernel (autotuned) */
     int recon;                /* FX_RECON_MC or FX_RECON_WENO3 */
-    /* branch signature of the plain form (null unless requested): the
-     * per-block face and edge kernels add a hash of every face's MC limiter
-     * regimes and HLLD decisions and every edge's upwind directions */
-    unsigned long long *bsig;
+    /* decisions of the plain form's face and edge kernels (MHD, MC):
+     * br_mode 0 none, 1 record into / 2 replay from br_words (one word per
+     * face, at br_off + (b * 3 + dir) * faces per direction + face) and
+     * br_edges (likewise per edge, br_eoff); replays count the decisions
+     * whose comparison differs from the recorded one in br_flips */
+    int br_mode;
+    size_t br_off, br_eoff;
+    unsigned long long *br_words, *br_edges, *br_flips;
     double *W2;   /* eSSPRK10_4 stage slot 2 of W: [b][v][cell] (null for RK2) */
     double *Bf2;  /* eSSPRK10_4 stage slot 2 of Bf: [b][dir][face] (null for RK2 or hydro) */
 };

@@ -75,6 +75,61 @@ FX_HD double fx_min(double a, double b) { return a < b ? a : b; }
 FX_HD double fx_max(double a, double b) { return a > b ? a : b; }
 
 /* ------------------------------------------------------------------------ */
+/* Branch policies.  The solvers below take their data-dependent decisions  */
+/* (limiter candidate, wave-speed argument, fan region, upwind direction)   */
+/* through a policy: FxBrFree evaluates each comparison (the solver as the   */
+/* reference runs it), FxBrRecord evaluates and records them in one 64-bit   */
+/* word per face or edge, and FxBrReplay takes them from such a word -- the */
+/* discrete map with its branches frozen at the recorded state, the map the */
+/* discrete adjoint differentiates -- counting the decisions whose           */
+/* comparison now comes out otherwise.                                       */
+/* ------------------------------------------------------------------------ */
+struct FxBrFree {
+    FX_HD bool bit(int, bool c) { return c; }
+    FX_HD unsigned field(int, unsigned c) { return c; }
+};
+
+struct FxBrRecord {
+    unsigned long long w = 0;
+    FX_HD bool bit(int k, bool c)
+    {
+        if (c) w |= 1ULL << k;
+        return c;
+    }
+    FX_HD unsigned field(int k, unsigned c)
+    {
+        w |= (unsigned long long)c << k;
+        return c;
+    }
+};
+
+struct FxBrReplay {
+    unsigned long long w = 0;
+    unsigned flips = 0;
+    FX_HD bool bit(int k, bool c)
+    {
+        const bool f = ((w >> k) & 1ULL) != 0;
+        flips += f != c ? 1u : 0u;
+        return f;
+    }
+    FX_HD unsigned field(int k, unsigned c)
+    {
+        const unsigned f = (unsigned)(w >> k) & 3u;
+        flips += f != c ? 1u : 0u;
+        return f;
+    }
+};
+
+/* bit positions of a face's word: MC candidates 2 bits per slope at
+ * 4 q + 2 s (q: the reconstructed quantity, 0-8; s: 0 the left cell's
+ * slope, 1 the right cell's), then the HLLD decisions */
+enum FxBrBit {
+    FX_BR_DISC_L = 36, FX_BR_DISC_R = 37, FX_BR_SL = 38, FX_BR_SR = 39, FX_BR_SUPER_L = 40,
+    FX_BR_SUPER_R = 41, FX_BR_HLL = 42, FX_BR_BNSMALL = 43, FX_BR_LEFT = 44, FX_BR_DEGEN_N = 45,
+    FX_BR_SINGLE = 46, FX_BR_DEGEN_F = 47, FX_BR_BNEG = 48
+};
+
+/* ------------------------------------------------------------------------ */
 /* MC limited slope, src/prj_reconstruct.h:355-375 (branchless form).        */
 /* ------------------------------------------------------------------------ */
 FX_HD double fx_mc_slope(double qm, double q0, double qp)
@@ -90,6 +145,31 @@ FX_HD double fx_mc_slope(double qm, double q0, double qp)
     mx = mx > c2 ? mx : c2;
     const double slope = sl > 0.0 ? mn : mx;
     return (sl * sr > 0.0) ? slope : 0.0;
+}
+
+/* fx_mc_slope with its selection through a policy: candidate 0, 1, 2 (c0,
+ * c1, c2) or 3 (zero slope) in the 2-bit field at bit k; the selected
+ * candidate is the same double fx_mc_slope returns */
+template <class BR>
+FX_HD double fx_mc_slope_br(double qm, double q0, double qp, BR &br, int k)
+{
+    const double sl = q0 - qm;
+    const double sr = qp - q0;
+    const double c0 = 2.0 * sl;
+    const double c1 = sl + 0.5 * (sr - sl);
+    const double c2 = 2.0 * sr;
+    unsigned reg = 3u;
+    if (sl * sr > 0.0) {
+        if (sl > 0.0) {
+            const double m = c0 < c1 ? c0 : c1;
+            reg = m < c2 ? (c0 < c1 ? 0u : 1u) : 2u;
+        } else {
+            const double m = c0 > c1 ? c0 : c1;
+            reg = m > c2 ? (c0 > c1 ? 0u : 1u) : 2u;
+        }
+    }
+    reg = br.field(k, reg);
+    return reg == 0u ? c0 : reg == 1u ? c1 : reg == 2u ? c2 : 0.0;
 }
 
 /* ------------------------------------------------------------------------ */
@@ -352,14 +432,16 @@ FX_HD void fx_hlld_state(const double *w, double p, double gamma, double bn,
     s.pt = s.p + magnetic;
 }
 
-/* prj_hlld_fast_speed, src/prj_riemann.c:117-140 */
-FX_HD double fx_hlld_fast_speed(const FxHlldState &s, FxErr *err, int blk, int idx)
+/* prj_hlld_fast_speed, src/prj_riemann.c:117-140; the clamp of a negative
+ * discriminant is decision bit k */
+template <class BR>
+FX_HD double fx_hlld_fast_speed_br(const FxHlldState &s, FxErr *err, int blk, int idx, BR &br, int k)
 {
     const double a2 = s.gamma * s.p / s.rho;
     const double bx2_rho = s.bx * s.bx / s.rho;
     const double b2_rho = (s.bx * s.bx + s.by * s.by + s.bz * s.bz) / s.rho;
     double disc = (a2 + b2_rho) * (a2 + b2_rho) - 4.0 * a2 * bx2_rho;
-    if (disc < 0.0) {
+    if (br.bit(k, disc < 0.0)) {
         if (disc < -1.0e-12 * (a2 + b2_rho) * (a2 + b2_rho)) {
             fx_fail(err, FX_ERR_HLLD_DISC, blk, idx);
         }
@@ -372,9 +454,17 @@ FX_HD double fx_hlld_fast_speed(const FxHlldState &s, FxErr *err, int blk, int i
     return sqrt(cf2);
 }
 
-/* prj_hlld_outer_star, src/prj_riemann.c:185-232 */
-FX_HD void fx_hlld_outer_star(const FxHlldState &s, double S, double SM,
-    double pt_star, FxHlldStar &st, FxErr *err, int blk, int idx)
+FX_HD double fx_hlld_fast_speed(const FxHlldState &s, FxErr *err, int blk, int idx)
+{
+    FxBrFree br;
+    return fx_hlld_fast_speed_br(s, err, blk, idx, br, 0);
+}
+
+/* prj_hlld_outer_star, src/prj_riemann.c:185-232; the degenerate-denominator
+ * branch is decision bit k */
+template <class BR>
+FX_HD void fx_hlld_outer_star_br(const FxHlldState &s, double S, double SM,
+    double pt_star, FxHlldStar &st, FxErr *err, int blk, int idx, BR &br, int k)
 {
     const double alpha = S - s.vx;
     const double smdiff = S - SM;
@@ -389,7 +479,7 @@ FX_HD void fx_hlld_outer_star(const FxHlldState &s, double S, double SM,
     st.bx = s.bx;
     st.ye = s.ye;
     const double denom = s.rho * alpha * smdiff - s.bx * s.bx;
-    if (fabs(denom) < FX_HLLD_SMALL * pt_star) {
+    if (br.bit(k, fabs(denom) < FX_HLLD_SMALL * pt_star)) {
         st.vy = s.vy;
         st.vz = s.vz;
         st.by = s.by;
@@ -405,6 +495,13 @@ FX_HD void fx_hlld_outer_star(const FxHlldState &s, double S, double SM,
     const double vdotb = s.vx * s.bx + s.vy * s.by + s.vz * s.bz;
     const double vstar_dotbstar = st.vx * st.bx + st.vy * st.by + st.vz * st.bz;
     st.e = (alpha * s.e - s.pt * s.vx + pt_star * SM + s.bx * (vdotb - vstar_dotbstar)) / smdiff;
+}
+
+FX_HD void fx_hlld_outer_star(const FxHlldState &s, double S, double SM,
+    double pt_star, FxHlldStar &st, FxErr *err, int blk, int idx)
+{
+    FxBrFree br;
+    fx_hlld_outer_star_br(s, S, SM, pt_star, st, err, blk, idx, br, 0);
 }
 
 /* prj_hlld_double_star_one, src/prj_riemann.c:234-282 */
@@ -566,22 +663,26 @@ static __device__ __noinline__ void fx_riemann_hlld(const double *WL, const doub
  * Selecting operands and choosing between x - t and x + t are exact, so the
  * result is bit-identical to fx_riemann_hlld; warps whose faces straddle
  * SM = 0 no longer execute both branches. */
-FX_HD void fx_riemann_hlld_folded(const double *WL, const double *WR,
+template <class BR>
+FX_HD void fx_riemann_hlld_folded_br(const double *WL, const double *WR,
     double pL, double pR, double gL, double gR, double bn, FxFaceOut &o,
-    FxErr *err, int blk, int idx)
+    FxErr *err, int blk, int idx, BR &br)
 {
     FxHlldState L, R;
     fx_hlld_state(WL, pL, gL, bn, L, err, blk, idx);
     fx_hlld_state(WR, pR, gR, bn, R, err, blk, idx);
-    const double cfL = fx_hlld_fast_speed(L, err, blk, idx);
-    const double cfR = fx_hlld_fast_speed(R, err, blk, idx);
-    const double SL = fx_min(L.vx - cfL, R.vx - cfR);
-    const double SR = fx_max(L.vx + cfL, R.vx + cfR);
+    const double cfL = fx_hlld_fast_speed_br(L, err, blk, idx, br, FX_BR_DISC_L);
+    const double cfR = fx_hlld_fast_speed_br(R, err, blk, idx, br, FX_BR_DISC_R);
+    const double aL = L.vx - cfL, aR = R.vx - cfR;
+    const double bL = L.vx + cfL, bR = R.vx + cfR;
+    const double SL = br.bit(FX_BR_SL, aL < aR) ? aL : aR;   /* fx_min */
+    const double SR = br.bit(FX_BR_SR, bL > bR) ? bL : bR;   /* fx_max */
     if (!(SL < SR)) {
         fx_fail(err, FX_ERR_HLLD_ORDER, blk, idx);
     }
-    if (0.0 <= SL || SR <= 0.0) {
-        const FxHlldState &X = (0.0 <= SL) ? L : R;
+    const bool super_l = br.bit(FX_BR_SUPER_L, 0.0 <= SL);
+    if (super_l || br.bit(FX_BR_SUPER_R, SR <= 0.0)) {
+        const FxHlldState &X = super_l ? L : R;
 #pragma unroll
         for (int v = 0; v < 9; ++v) o.F[v] = fx_hlld_state_f(X, v);
         fx_face_outputs(X.vx, X.vy, X.vz, X.bx, X.by, X.bz, o);
@@ -597,7 +698,7 @@ FX_HD void fx_riemann_hlld_folded(const double *WL, const double *WR,
     const double pt_star_l = L.pt + L.rho * (SL - L.vx) * (SM - L.vx);
     const double pt_star_r = R.pt + R.rho * (SR - R.vx) * (SM - R.vx);
     const double pt_star = 0.5 * (pt_star_l + pt_star_r);
-    if (pt_star <= 0.0 || !isfinite(pt_star)) {
+    if (br.bit(FX_BR_HLL, pt_star <= 0.0 || !isfinite(pt_star))) {
         const double inv = 1.0 / (SR - SL);
         double Uh[9];
 #pragma unroll
@@ -613,15 +714,15 @@ FX_HD void fx_riemann_hlld_folded(const double *WL, const double *WR,
         fx_face_outputs(Uh[1] / rho, Uh[2] / rho, Uh[3] / rho, Uh[6], Uh[7], Uh[8], o);
         return;
     }
-    const bool bn_small = (0.5 * bn * bn < FX_HLLD_SMALL * pt_star);
-    const bool left = (0.0 <= SM);
+    const bool bn_small = br.bit(FX_BR_BNSMALL, 0.5 * bn * bn < FX_HLLD_SMALL * pt_star);
+    const bool left = br.bit(FX_BR_LEFT, 0.0 <= SM);
     const FxHlldState N = left ? L : R;
     const double SN = left ? SL : SR;
     FxHlldStar Ns;
-    fx_hlld_outer_star(N, SN, SM, pt_star, Ns, err, blk, idx);
+    fx_hlld_outer_star_br(N, SN, SM, pt_star, Ns, err, blk, idx, br, FX_BR_DEGEN_N);
     const double a = fabs(bn) / sqrt(Ns.rho);
     const double SNs = left ? SM - a : SM + a;
-    const bool single = (left ? (0.0 <= SNs) : (SNs <= 0.0)) || bn_small;
+    const bool single = br.bit(FX_BR_SINGLE, (left ? (0.0 <= SNs) : (SNs <= 0.0)) || bn_small);
     if (single) {
 #pragma unroll
         for (int v = 0; v < 9; ++v) {
@@ -633,7 +734,7 @@ FX_HD void fx_riemann_hlld_folded(const double *WL, const double *WR,
     const FxHlldState Fr = left ? R : L;
     const double SF = left ? SR : SL;
     FxHlldStar Fs;
-    fx_hlld_outer_star(Fr, SF, SM, pt_star, Fs, err, blk, idx);
+    fx_hlld_outer_star_br(Fr, SF, SM, pt_star, Fs, err, blk, idx, br, FX_BR_DEGEN_F);
     const FxHlldStar Ls = left ? Ns : Fs;
     const FxHlldStar Rs = left ? Fs : Ns;
     /* prj_hlld_double_star_one, src/prj_riemann.c:234-282 */
@@ -643,7 +744,7 @@ FX_HD void fx_riemann_hlld_folded(const double *WL, const double *WR,
         fx_fail(err, FX_ERR_HLLD_DSTAR, blk, idx);
     }
     const double inv_sum = 1.0 / (sqrt_l + sqrt_r);
-    const double sign_bx = bn < 0.0 ? -1.0 : 1.0;
+    const double sign_bx = br.bit(FX_BR_BNEG, bn < 0.0) ? -1.0 : 1.0;
     FxHlldStar ss = Ns;
     ss.vy = (sqrt_l * Ls.vy + sqrt_r * Rs.vy + (Rs.by - Ls.by) * sign_bx) * inv_sum;
     ss.vz = (sqrt_l * Ls.vz + sqrt_r * Rs.vz + (Rs.bz - Ls.bz) * sign_bx) * inv_sum;
@@ -660,6 +761,14 @@ FX_HD void fx_riemann_hlld_folded(const double *WL, const double *WR,
             SNs * (fx_hlld_u(ss, v) - us);
     }
     fx_face_outputs(ss.vx, ss.vy, ss.vz, ss.bx, ss.by, ss.bz, o);
+}
+
+FX_HD void fx_riemann_hlld_folded(const double *WL, const double *WR,
+    double pL, double pR, double gL, double gR, double bn, FxFaceOut &o,
+    FxErr *err, int blk, int idx)
+{
+    FxBrFree br;
+    fx_riemann_hlld_folded_br(WL, WR, pL, pR, gL, gR, bn, o, err, blk, idx, br);
 }
 
 /* ------------------------------------------------------------------------ */
@@ -765,38 +874,52 @@ static __device__ __noinline__ void fx_riemann_hllc(const double *WL, const doub
 /* ------------------------------------------------------------------------ */
 /* Upwind corner EMF, src/prj_mhd.c:627-718 (eta term separate).            */
 /* ------------------------------------------------------------------------ */
-FX_HD double fx_emf_upwind(const double f[4], const double c[4], const double vn[4])
+/* the upwind direction of face n (0: vn > 0, 1: vn < 0, 2: vn == 0) is the
+ * 2-bit decision field at bit 2 n of an edge's word */
+template <class BR>
+FX_HD double fx_emf_upwind_br(const double f[4], const double c[4], const double vn[4], BR &br)
 {
+    unsigned u[4];
+#pragma unroll
+    for (int n = 0; n < 4; ++n) {
+        u[n] = br.field(2 * n, vn[n] > 0.0 ? 0u : vn[n] < 0.0 ? 1u : 2u);
+    }
     double emf = 0.25 * (f[0] + f[1] + f[2] + f[3]);
-    if (vn[0] > 0.0) {
+    if (u[0] == 0u) {
         emf += 0.25 * (f[3] - c[3]);
-    } else if (vn[0] < 0.0) {
+    } else if (u[0] == 1u) {
         emf += 0.25 * (f[1] - c[0]);
     } else {
         emf += 0.125 * (f[3] - c[3] + f[1] - c[0]);
     }
-    if (vn[1] > 0.0) {
+    if (u[1] == 0u) {
         emf += 0.25 * (f[2] - c[1]);
-    } else if (vn[1] < 0.0) {
+    } else if (u[1] == 1u) {
         emf += 0.25 * (f[0] - c[0]);
     } else {
         emf += 0.125 * (f[2] - c[1] + f[0] - c[0]);
     }
-    if (vn[2] > 0.0) {
+    if (u[2] == 0u) {
         emf += 0.25 * (f[3] - c[2]);
-    } else if (vn[2] < 0.0) {
+    } else if (u[2] == 1u) {
         emf += 0.25 * (f[1] - c[1]);
     } else {
         emf += 0.125 * (f[3] - c[2] + f[1] - c[1]);
     }
-    if (vn[3] > 0.0) {
+    if (u[3] == 0u) {
         emf += 0.25 * (f[2] - c[2]);
-    } else if (vn[3] < 0.0) {
+    } else if (u[3] == 1u) {
         emf += 0.25 * (f[0] - c[3]);
     } else {
         emf += 0.125 * (f[2] - c[2] + f[0] - c[3]);
     }
     return emf;
+}
+
+FX_HD double fx_emf_upwind(const double f[4], const double c[4], const double vn[4])
+{
+    FxBrFree br;
+    return fx_emf_upwind_br(f, c, vn, br);
 }
 
 /* artificial CT resistivity of one cell, src/prj_timeint.c:222-262 */

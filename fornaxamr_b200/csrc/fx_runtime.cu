@@ -96,6 +96,14 @@ struct fx_ctx {
     FxAdjSrc *d_adj_csrc = nullptr, *d_adj_fsrc = nullptr;
     FxAdjEnt *d_adj_ents = nullptr;
 
+    /* decision record / replay of the plain form (fx_branch_trace) */
+    unsigned long long *d_br_words = nullptr, *d_br_edges = nullptr;
+    int br_cap = 0;        /* stages the buffers hold */
+    int br_nblocks = 0;    /* blocks they were sized for */
+    int br_stage = 0;      /* next stage's slot */
+    int br_recorded = 0;   /* stages of the last record */
+    bool br_overflow = false;
+
     int cap = 0;                      /* blocks the per-block device arrays hold */
     /* dynamic AMR */
     bool amr_set = false;
@@ -398,6 +406,22 @@ void stage_seq(fx_ctx *c, int form, int stage)
     const int dst = stage == 1 ? 1 : 0; /* W slot the update writes */
     cudaStream_t s = c->stream;
     const int full = form == FX_FORM_PLAIN ? 1 : 0;
+    /* decisions are recorded / replayed by the plain form only, one slot
+     * of the buffers per stage */
+    const int br_mode = c->D.br_mode;
+    if (br_mode && form != FX_FORM_PLAIN) {
+        c->D.br_mode = 0;
+    } else if (br_mode) {
+        if (c->br_stage >= c->br_cap) {
+            c->br_overflow = true;
+            c->D.br_mode = 0;
+        } else {
+            c->D.br_off = (size_t)c->br_stage * c->nblocks * 3 * (FX_BS + 1) * (FX_BS + 2) * (FX_BS + 2);
+            c->D.br_eoff = (size_t)c->br_stage * c->nblocks * 3 * FX_BS * (FX_BS + 1) * (FX_BS + 1);
+            ++c->br_stage;
+            if (br_mode == FX_BRANCH_RECORD) c->br_recorded = c->br_stage;
+        }
+    }
     per_block(c, form, [&](const int *l, int n) { fx_launch_flux(c->D, l, n, 3, src, src, full, s); });
     shard_exchange(c, FX_XF, src);
     flux_correct(c, full ? c->nv : 6, s);
@@ -419,6 +443,7 @@ void stage_seq(fx_ctx *c, int form, int stage)
         per_block(c, form, [&](const int *l, int n) { fx_launch_eos_fill(c->D, l, n, dst, 0, s); });
     }
     c->last_slot = dst;
+    if (!c->br_overflow) c->D.br_mode = br_mode;
 }
 
 /* the refill after a substep or a blend: eos (active) -> ghost fill -> eos
@@ -989,6 +1014,8 @@ void fx_destroy(fx_ctx *c)
     free_mesh(c);
     delete c->transport;
     c->transport = nullptr;
+    cudaFree(c->d_br_words);
+    cudaFree(c->d_br_edges);
     cudaFree(c->d_err);
     cudaFree(c->d_red);
     cudaFree(c->d_ctl);
@@ -1832,24 +1859,69 @@ int fx_autotune(fx_ctx *c, double *times_ms, int n, int *choice)
     return check_device_error(c);
 }
 
-int fx_branch_signature(fx_ctx *c, int enable, unsigned long long *value)
+int fx_branch_trace(fx_ctx *c, int mode, int max_stages, unsigned long long *flips)
 {
     if (!c) return FX_EINVAL;
-    if (enable) {
-        FX_CUDA(c, cudaMemsetAsync(c->d_red + 2, 0, sizeof(unsigned long long), c->stream));
-        c->D.bsig = c->d_red + 2;
-        free_graphs(c); /* captured graphs hold the previous device view */
+    if (!has_mesh(c)) return set_err(c, FX_ENOMESH, "no mesh");
+    if (!c->cfg.mhd || c->cfg.recon != FX_RECON_MC || c->cfg.integrator != FX_INT_RK2 || c->nranks > 1) {
+        return set_err(c, FX_EINVAL, "fx_branch_trace: MHD, MC, RK2, one rank only");
+    }
+    if (mode == FX_BRANCH_OFF) {
+        const int was = c->D.br_mode;
+        c->D.br_mode = 0;
+        free_graphs(c);
+        if (c->br_overflow) {
+            c->br_overflow = false;
+            return set_err(c, FX_ETOOBIG, "fx_branch_trace: more stages than the %d recorded", c->br_cap);
+        }
+        if (flips) {
+            *flips = 0;
+            if (was == FX_BRANCH_REPLAY) {
+                FX_CUDA(c, cudaMemcpyAsync(c->h_red + 2, c->d_red + 2, sizeof(unsigned long long),
+                    cudaMemcpyDeviceToHost, c->stream));
+                const int rc = sync_and_check(c);
+                if (rc) return rc;
+                *flips = c->h_red[2];
+            }
+        }
         return FX_SUCCESS;
     }
-    if (!value) return set_err(c, FX_EINVAL, "fx_branch_signature: null value");
-    if (!c->D.bsig) return set_err(c, FX_EINVAL, "fx_branch_signature: not enabled");
-    FX_CUDA(c, cudaMemcpyAsync(c->h_red + 2, c->d_red + 2, sizeof(unsigned long long), cudaMemcpyDeviceToHost,
-        c->stream));
-    const int rc = sync_and_check(c);
-    c->D.bsig = nullptr;
-    free_graphs(c);
-    if (rc) return rc;
-    *value = c->h_red[2];
+    const size_t faces = (size_t)c->nblocks * 3 * (FX_BS + 1) * (FX_BS + 2) * (FX_BS + 2);
+    const size_t edges = (size_t)c->nblocks * 3 * FX_BS * (FX_BS + 1) * (FX_BS + 1);
+    if (mode == FX_BRANCH_RECORD) {
+        if (max_stages <= 0) return set_err(c, FX_EINVAL, "fx_branch_trace: max_stages must be positive");
+        if (c->br_cap != max_stages || c->br_nblocks != c->nblocks) {
+            cudaFree(c->d_br_words);
+            cudaFree(c->d_br_edges);
+            c->d_br_words = c->d_br_edges = nullptr;
+            c->br_cap = 0;
+            if (cudaMalloc((void **)&c->d_br_words, faces * max_stages * sizeof(unsigned long long)) != cudaSuccess ||
+                cudaMalloc((void **)&c->d_br_edges, edges * max_stages * sizeof(unsigned long long)) != cudaSuccess) {
+                cudaGetLastError();
+                cudaFree(c->d_br_words);
+                cudaFree(c->d_br_edges);
+                c->d_br_words = c->d_br_edges = nullptr;
+                return set_err(c, FX_ENOMEM, "fx_branch_trace: no room for %d stages of decisions", max_stages);
+            }
+            c->br_cap = max_stages;
+            c->br_nblocks = c->nblocks;
+        }
+        c->br_recorded = 0;
+    } else if (mode == FX_BRANCH_REPLAY) {
+        if (!c->d_br_words || c->br_nblocks != c->nblocks || c->br_recorded == 0) {
+            return set_err(c, FX_EINVAL, "fx_branch_trace: nothing recorded to replay");
+        }
+        FX_CUDA(c, cudaMemsetAsync(c->d_red + 2, 0, sizeof(unsigned long long), c->stream));
+    } else {
+        return set_err(c, FX_EINVAL, "fx_branch_trace: unknown mode %d", mode);
+    }
+    c->br_stage = 0;
+    c->br_overflow = false;
+    c->D.br_mode = mode;
+    c->D.br_words = c->d_br_words;
+    c->D.br_edges = c->d_br_edges;
+    c->D.br_flips = c->d_red + 2;
+    free_graphs(c); /* captured graphs hold the previous device view */
     return FX_SUCCESS;
 }
 

@@ -447,19 +447,29 @@ int fx_amr_remesh_host(const fx_config *cfg, const fx_amr_config *amr, int nbloc
  * level apart.  The product's mesh builders use this one restatement. */
 int fx_mesh_slot_geometry(int nblocks, fx_block_desc *blocks);
 
-/* Branch signature of the plain form (no reference counterpart; for checks
- * of the discrete adjoint against finite differences).  enable = 1 zeroes
- * a device sum and makes every following per-block face and edge launch add
- * a hash of each face's decisions (the MC limiter's selected candidate for
- * every reconstructed quantity, the HLLD wave-speed arguments, clamped
- * discriminants, fan region, bn_small, contact side, sign of bn, single or
- * double star, degenerate outer-star denominators) and each edge's upwind
- * directions (src/prj_reconstruct.h:355-375, src/prj_riemann.c:117-440,
- * src/prj_mhd.c:627-680); enable = 0 returns the sum in *value and stops.
- * Two runs with equal sums took the same branches everywhere (up to hash
- * collisions, about 2^-64).  MHD with MC reconstruction; the batched form
- * does not add to it. */
-int fx_branch_signature(fx_ctx *ctx, int enable, unsigned long long *value);
+/* Decision record and replay of the plain form (no reference counterpart;
+ * for checking the discrete adjoint against finite differences).  The
+ * update is smooth in the state except where a decision switches: the MC
+ * limiter's candidate for each reconstructed quantity, the HLLD
+ * wave-speed arguments, clamped discriminants, fan region, bn_small,
+ * contact side, single or double star, degenerate outer-star denominators
+ * and the sign of bn (src/prj_reconstruct.h:355-375,
+ * src/prj_riemann.c:117-440), and each edge's upwind directions
+ * (src/prj_mhd.c:627-680).
+ *   FX_BRANCH_RECORD: the following plain-form RK2 stages (at most
+ *     max_stages) record every face's and edge's decisions;
+ *   FX_BRANCH_REPLAY: the following plain-form stages take those decisions
+ *     instead of evaluating them -- the map with its branches frozen at the
+ *     recorded state, whose derivative the adjoint computes -- and count the
+ *     decisions that would have come out otherwise;
+ *   FX_BRANCH_OFF: back to the solver as it stands; after a replay *flips
+ *     (may be NULL) receives that count.  FX_ETOOBIG if more stages ran
+ *     than were recorded.
+ * MHD, MC, RK2, one rank; the batched form is not affected. */
+#define FX_BRANCH_OFF 0
+#define FX_BRANCH_RECORD 1
+#define FX_BRANCH_REPLAY 2
+int fx_branch_trace(fx_ctx *ctx, int mode, int max_stages, unsigned long long *flips);
 
 /* ---- measurement --------------------------------------------------------------- */
 
