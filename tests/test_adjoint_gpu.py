@@ -10,7 +10,9 @@ Objective J = sum over cells with |x - (0.5, 0.5, 0.5)| < 0.25 of
 The discrete map is piecewise smooth: the MC limiter's candidate, the HLLD
 fan and the upwind direction switch at kinks, and with 2.5e5 cells every
 probe direction crosses some of them even at eps = 1e-8 (the decision
-replay below counts them).  So the adjoint is checked two ways:
+replay below counts them; most are ties at round-off, such as the limiter
+choices on the initially uniform pressure, whose noise-level differences
+the perturbation reshuffles).  So the adjoint is checked two ways:
 
 * against the branch-frozen map, the map the discrete adjoint
   differentiates: the forward at the unperturbed state records every face's

@@ -74,6 +74,7 @@ def test_active_state_transfers_match_full_transfers(ref_mhd, ref_hydro, mhd):
         if mhd:
             Bp[...] = np.nan
         b.download_state_active(Wp, Bp)
+        act = H.active_cells()
         assert np.array_equal(Wp[:, :, 0][..., act], Wa[:, :, 0][..., act])
         rest = np.ones(H.NCELLS, bool)
         rest[act] = False
