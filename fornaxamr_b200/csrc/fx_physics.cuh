@@ -74,6 +74,9 @@ FX_HD void fx_fail(FxErr *err, int code, int block, int index)
 FX_HD double fx_min(double a, double b) { return a < b ? a : b; }
 FX_HD double fx_max(double a, double b) { return a > b ? a : b; }
 
+/* the face solver's divisions (correctly rounded, as in the reference) */
+FX_HD double fx_div(double a, double b) { return a / b; }
+
 /* ------------------------------------------------------------------------ */
 /* Branch policies.  The solvers below take their data-dependent decisions  */
 /* (limiter candidate, wave-speed argument, fan region, upwind direction)   */
@@ -437,9 +440,9 @@ FX_HD void fx_hlld_state(const double *w, double p, double gamma, double bn,
 template <class BR>
 FX_HD double fx_hlld_fast_speed_br(const FxHlldState &s, FxErr *err, int blk, int idx, BR &br, int k)
 {
-    const double a2 = s.gamma * s.p / s.rho;
-    const double bx2_rho = s.bx * s.bx / s.rho;
-    const double b2_rho = (s.bx * s.bx + s.by * s.by + s.bz * s.bz) / s.rho;
+    const double a2 = fx_div(s.gamma * s.p, s.rho);
+    const double bx2_rho = fx_div(s.bx * s.bx, s.rho);
+    const double b2_rho = fx_div(s.bx * s.bx + s.by * s.by + s.bz * s.bz, s.rho);
     double disc = (a2 + b2_rho) * (a2 + b2_rho) - 4.0 * a2 * bx2_rho;
     if (br.bit(k, disc < 0.0)) {
         if (disc < -1.0e-12 * (a2 + b2_rho) * (a2 + b2_rho)) {
@@ -471,7 +474,7 @@ FX_HD void fx_hlld_outer_star_br(const FxHlldState &s, double S, double SM,
     if (fabs(smdiff) <= 1.0e-14 * (fabs(S) + fabs(SM) + 1.0)) {
         fx_fail(err, FX_ERR_HLLD_OUTER, blk, idx);
     }
-    st.rho = s.rho * alpha / smdiff;
+    st.rho = fx_div(s.rho * alpha, smdiff);
     if (st.rho <= 0.0 || !isfinite(st.rho)) {
         fx_fail(err, FX_ERR_HLLD_STARRHO, blk, idx);
     }
@@ -485,8 +488,8 @@ FX_HD void fx_hlld_outer_star_br(const FxHlldState &s, double S, double SM,
         st.by = s.by;
         st.bz = s.bz;
     } else {
-        const double sm_diff_vx_over_denom = (SM - s.vx) / denom;
-        const double mag_factor = (s.rho * alpha * alpha - s.bx * s.bx) / denom;
+        const double sm_diff_vx_over_denom = fx_div(SM - s.vx, denom);
+        const double mag_factor = fx_div(s.rho * alpha * alpha - s.bx * s.bx, denom);
         st.vy = s.vy - s.bx * s.by * sm_diff_vx_over_denom;
         st.vz = s.vz - s.bx * s.bz * sm_diff_vx_over_denom;
         st.by = s.by * mag_factor;
@@ -494,7 +497,7 @@ FX_HD void fx_hlld_outer_star_br(const FxHlldState &s, double S, double SM,
     }
     const double vdotb = s.vx * s.bx + s.vy * s.by + s.vz * s.bz;
     const double vstar_dotbstar = st.vx * st.bx + st.vy * st.by + st.vz * st.bz;
-    st.e = (alpha * s.e - s.pt * s.vx + pt_star * SM + s.bx * (vdotb - vstar_dotbstar)) / smdiff;
+    st.e = fx_div(alpha * s.e - s.pt * s.vx + pt_star * SM + s.bx * (vdotb - vstar_dotbstar), smdiff);
 }
 
 FX_HD void fx_hlld_outer_star(const FxHlldState &s, double S, double SM,
@@ -693,13 +696,13 @@ FX_HD void fx_riemann_hlld_folded_br(const double *WL, const double *WR,
         (fabs(R.rho * (SR - R.vx)) + fabs(L.rho * (SL - L.vx)) + 1.0)) {
         fx_fail(err, FX_ERR_HLLD_DENOM, blk, idx);
     }
-    const double SM = (R.rho * R.vx * (SR - R.vx) -
-        L.rho * L.vx * (SL - L.vx) + (L.pt - R.pt)) / denom;
+    const double SM = fx_div(R.rho * R.vx * (SR - R.vx) -
+        L.rho * L.vx * (SL - L.vx) + (L.pt - R.pt), denom);
     const double pt_star_l = L.pt + L.rho * (SL - L.vx) * (SM - L.vx);
     const double pt_star_r = R.pt + R.rho * (SR - R.vx) * (SM - R.vx);
     const double pt_star = 0.5 * (pt_star_l + pt_star_r);
     if (br.bit(FX_BR_HLL, pt_star <= 0.0 || !isfinite(pt_star))) {
-        const double inv = 1.0 / (SR - SL);
+        const double inv = fx_div(1.0, SR - SL);
         double Uh[9];
 #pragma unroll
         for (int v = 0; v < 9; ++v) {
@@ -711,7 +714,7 @@ FX_HD void fx_riemann_hlld_folded_br(const double *WL, const double *WR,
             Uh[v] = (SR * ru - SL * lu + lf - rf) * inv;
         }
         const double rho = Uh[0];
-        fx_face_outputs(Uh[1] / rho, Uh[2] / rho, Uh[3] / rho, Uh[6], Uh[7], Uh[8], o);
+        fx_face_outputs(fx_div(Uh[1], rho), fx_div(Uh[2], rho), fx_div(Uh[3], rho), Uh[6], Uh[7], Uh[8], o);
         return;
     }
     const bool bn_small = br.bit(FX_BR_BNSMALL, 0.5 * bn * bn < FX_HLLD_SMALL * pt_star);
@@ -720,7 +723,7 @@ FX_HD void fx_riemann_hlld_folded_br(const double *WL, const double *WR,
     const double SN = left ? SL : SR;
     FxHlldStar Ns;
     fx_hlld_outer_star_br(N, SN, SM, pt_star, Ns, err, blk, idx, br, FX_BR_DEGEN_N);
-    const double a = fabs(bn) / sqrt(Ns.rho);
+    const double a = fx_div(fabs(bn), sqrt(Ns.rho));
     const double SNs = left ? SM - a : SM + a;
     const bool single = br.bit(FX_BR_SINGLE, (left ? (0.0 <= SNs) : (SNs <= 0.0)) || bn_small);
     if (single) {
@@ -743,7 +746,7 @@ FX_HD void fx_riemann_hlld_folded_br(const double *WL, const double *WR,
     if (sqrt_l + sqrt_r <= 0.0) {
         fx_fail(err, FX_ERR_HLLD_DSTAR, blk, idx);
     }
-    const double inv_sum = 1.0 / (sqrt_l + sqrt_r);
+    const double inv_sum = fx_div(1.0, sqrt_l + sqrt_r);
     const double sign_bx = br.bit(FX_BR_BNEG, bn < 0.0) ? -1.0 : 1.0;
     FxHlldStar ss = Ns;
     ss.vy = (sqrt_l * Ls.vy + sqrt_r * Rs.vy + (Rs.by - Ls.by) * sign_bx) * inv_sum;
