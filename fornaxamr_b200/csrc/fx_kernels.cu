@@ -215,19 +215,7 @@ __global__ void __launch_bounds__(TPB, MINB) k_flux(FxDev D, const int *__restri
         WR[FX_B1] = bn;
         FxFaceOut o;
         if constexpr (BRM == 0) {
-            /* divisions by fused multiply-adds (FxDivFma: the correctly
-             * rounded quotient, branch-free); a face whose operands leave
-             * that method's range is redone with native division, and the
-             * first pass's error reports are kept back until it is accepted */
-            FxErrLocal le;
-            FxDivFma dv;
-            FxBrFree bf;
-            fx_riemann_hlld_folded_br(WL, WR, pL, pR, gL, gR, bn, o, &le, b, cR, bf, dv);
-            if (!dv.ok) {
-                fx_riemann_hlld_folded(WL, WR, pL, pR, gL, gR, bn, o, D.err, b, cR);
-            } else if (le.code != 0) {
-                fx_fail(D.err, le.code, le.block, le.index);
-            }
+            fx_riemann_hlld_folded(WL, WR, pL, pR, gL, gR, bn, o, D.err, b, cR);
         } else {
             fx_riemann_hlld_folded_br(WL, WR, pL, pR, gL, gR, bn, o, D.err, b, cR, br);
             if constexpr (BRM == 1) {
@@ -1513,67 +1501,6 @@ void fx_flux_shape(int variant, int *tpb, int *minb)
     const int v = variant >= 0 && variant < FX_FLUX_VARIANTS ? variant : 0;
     *tpb = kFluxShapes[v][0];
     *minb = kFluxShapes[v][1];
-}
-
-/* ------------------------------------------------------------------------ */
-/* Self-test of FxDivFma against native division                            */
-/* ------------------------------------------------------------------------ */
-__device__ __forceinline__ unsigned long long fx_mix64(unsigned long long z)
-{
-    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
-    z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
-    return z ^ (z >> 31);
-}
-
-/* a random double: random sign and significand, exponent uniform in
- * [-emax, emax]; every 8th draw takes one of the significands where
- * reciprocal refinement is delicate (all ones, one, one plus an ulp, all
- * ones but the last bit) */
-__device__ __forceinline__ double fx_test_double(unsigned long long r, int emax)
-{
-    unsigned long long m = r & 0x000FFFFFFFFFFFFFULL;
-    const unsigned kind = (unsigned)(r >> 61);
-    const unsigned sel = (unsigned)(r >> 52) & 7u;
-    if (sel == 0) {
-        const unsigned long long special[4] = {0x000FFFFFFFFFFFFFULL, 0ULL, 1ULL, 0x000FFFFFFFFFFFFEULL};
-        m = special[kind & 3u];
-    }
-    const long long e = (long long)(fx_mix64(r + 0x9E3779B97F4A7C15ULL) % (unsigned long long)(2 * emax + 1)) - emax;
-    const unsigned long long sign = (r >> 55 & 1ULL) << 63;
-    return __longlong_as_double((long long)(sign | ((unsigned long long)(e + 1023) << 52) | m));
-}
-
-__global__ void __launch_bounds__(256) k_selftest_div(long long n, unsigned long long seed, int emax,
-    unsigned long long *counts)
-{
-    unsigned long long bad = 0, out = 0;
-    const long long stride = (long long)gridDim.x * blockDim.x;
-    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += stride) {
-        const unsigned long long r = fx_mix64(seed + 2 * (unsigned long long)t);
-        const unsigned long long r2 = fx_mix64(seed + 2 * (unsigned long long)t + 1);
-        double a = fx_test_double(r, emax);
-        const double b = fx_test_double(r2, emax);
-        if ((r2 >> 60) == 0) {
-            a = (r >> 59 & 1ULL) ? -0.0 : 0.0;
-        }
-        bool ok = true;
-        const double q = fx_div_fma(a, b, ok);
-        const double qn = a / b;
-        if (!ok) {
-            ++out;
-        } else if (__double_as_longlong(q) != __double_as_longlong(qn)) {
-            ++bad;
-        }
-    }
-    atomicAdd(&counts[0], bad);
-    atomicAdd(&counts[1], out);
-}
-
-int fx_launch_selftest_div(long long n, unsigned long long seed, int emax, unsigned long long *d_counts,
-    cudaStream_t s)
-{
-    k_selftest_div<<<148 * 8, 256, 0, s>>>(n, seed, emax, d_counts);
-    return cudaGetLastError() == cudaSuccess ? 0 : 1;
 }
 
 /* ------------------------------------------------------------------------ */

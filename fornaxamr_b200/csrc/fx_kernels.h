@@ -195,11 +195,6 @@ void fx_launch_xunpack(const FxDev &D, const FxXent *ents, int n, const double *
  * arrays and device-mapped page-locked host arrays (hs host stage slots) */
 void fx_launch_active_state(const FxDev &D, const int *blist, int nlist, double *hW, double *hBf, int hs,
     bool to_device, cudaStream_t s);
-/* FxDivFma against native division on n random operand pairs (exponents in
- * [-emax, emax]); d_counts[0] += differing quotients inside the method's
- * range, d_counts[1] += pairs outside it */
-int fx_launch_selftest_div(long long n, unsigned long long seed, int emax, unsigned long long *d_counts,
-    cudaStream_t s);
 void fx_launch_flux_correct(const FxDev &D, const FxCorr *recs, int n, int ncomp, cudaStream_t s);
 void fx_launch_emf_correct(const FxDev &D, const FxCorr *recs, int n, cudaStream_t s);
 void fx_launch_reset_reductions(const FxDev &D, int which, cudaStream_t s);

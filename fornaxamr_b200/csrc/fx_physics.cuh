@@ -74,91 +74,8 @@ FX_HD void fx_fail(FxErr *err, int code, int block, int index)
 FX_HD double fx_min(double a, double b) { return a < b ? a : b; }
 FX_HD double fx_max(double a, double b) { return a > b ? a : b; }
 
-/* A thread-local error record with fx_fail's first-error-wins rule, for a
- * solver pass whose reports are kept back until its result is accepted. */
-struct FxErrLocal {
-    int code = 0;
-    int block = 0;
-    int index = 0;
-};
-
-FX_HD void fx_fail(FxErrLocal *err, int code, int block, int index)
-{
-    if (err != nullptr && err->code == 0) {
-        err->code = code;
-        err->block = block;
-        err->index = index;
-    }
-}
-
-/* Division policies of the face solver.  FxDivNative is the language's
- * correctly rounded division.  FxDivFma computes the same correctly rounded
- * quotient from fused multiply-adds and a reciprocal seed, without the
- * general path's branches for operands near the ends of the exponent range
- * (Markstein's method, as in P. Markstein, "IA-64 and Elementary Functions",
- * 2000, and J.-M. Muller et al., "Handbook of Floating-Point Arithmetic",
- * ch. 4-5):
- *   - the hardware seed y0 ~ 1/b is refined by Newton-Raphson steps
- *     y <- y + y (1 - b y) until y is within one ulp of 1/b; then
- *     e = 1 - b y is exact, and one more step gives the correctly rounded
- *     reciprocal RN(1/b), except for the significand 1.11...1, whose
- *     reciprocal 2^-(k+1) (1 + 2^-52) is set directly;
- *   - q = RN(a y) is within 1.5 ulp of a/b; one correction
- *     q <- q + (a - b q) y brings it within one ulp, and with y = RN(1/b)
- *     the next correction (exact residual a - b q by the FMA) gives RN(a/b)
- *     (Markstein's theorem).
- * The argument holds while no step overflows or underflows: b and the
- * quotient normal with magnitudes in [2^-400, 2^401), or a = 0.  Outside
- * that range `ok` turns false and the caller redoes the face with
- * FxDivNative; inside it the quotient equals a / b bit for bit (checked on
- * the device against native division by fx_selftest_div). */
-struct FxDivNative {
-    FX_HD double operator()(double a, double b) { return a / b; }
-};
-
-__device__ __forceinline__ double fx_rcp_seed(double b)
-{
-    double y;
-    asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(b));
-    return y;
-}
-
-__device__ __forceinline__ double fx_div_fma(double a, double b, bool &ok)
-{
-    double y = fx_rcp_seed(b);
-    double e = fma(-b, y, 1.0);
-    y = fma(y, e, y);
-    e = fma(-b, y, 1.0);
-    y = fma(y, e, y);
-    e = fma(-b, y, 1.0);
-    y = fma(y, e, y);            /* within one ulp of 1/b */
-    e = fma(-b, y, 1.0);         /* exact */
-    y = fma(y, e, y);            /* RN(1/b) unless b's significand is all ones */
-    const long long bb = __double_as_longlong(b);
-    const long long eb = (bb >> 52) & 0x7FF;
-    if ((bb & 0x000FFFFFFFFFFFFFLL) == 0x000FFFFFFFFFFFFFLL) {
-        y = __longlong_as_double((bb & (long long)0x8000000000000000ULL) | ((2045 - eb) << 52) | 1LL);
-    }
-    const double q0 = a * y;
-    double q = fma(fma(-b, q0, a), y, q0);
-    q = fma(fma(-b, q, a), y, q);
-    const long long eq = (__double_as_longlong(q) >> 52) & 0x7FF;
-    ok = ok && (unsigned long long)(eb - 623) <= 801ULL &&
-        ((unsigned long long)(eq - 623) <= 801ULL || a == 0.0);
-    return a == 0.0 ? q0 : q;
-}
-
-struct FxDivFma {
-    bool ok = true;
-    FX_HD double operator()(double a, double b)
-    {
-#ifdef __CUDA_ARCH__
-        return fx_div_fma(a, b, ok);
-#else
-        return a / b;
-#endif
-    }
-};
+/* the face solver's divisions (correctly rounded, as in the reference) */
+FX_HD double fx_div(double a, double b) { return a / b; }
 
 /* ------------------------------------------------------------------------ */
 /* Branch policies.  The solvers below take their data-dependent decisions  */
@@ -496,9 +413,8 @@ FX_HD double fx_hlld_state_f(const FxHlldState &s, int v)
 
 /* prj_hlld_state_from_prim, src/prj_riemann.c:142-178; w is the local
  * (direction-rotated) primitive vector, the normal field is bn. */
-template <class E>
-FX_HD void fx_hlld_state_e(const double *w, double p, double gamma, double bn,
-    FxHlldState &s, E *err, int blk, int idx)
+FX_HD void fx_hlld_state(const double *w, double p, double gamma, double bn,
+    FxHlldState &s, FxErr *err, int blk, int idx)
 {
     s.rho = w[FX_RHO];
     s.vx = w[FX_V1];
@@ -519,20 +435,14 @@ FX_HD void fx_hlld_state_e(const double *w, double p, double gamma, double bn,
     s.pt = s.p + magnetic;
 }
 
-FX_HD void fx_hlld_state(const double *w, double p, double gamma, double bn,
-    FxHlldState &s, FxErr *err, int blk, int idx)
-{
-    fx_hlld_state_e(w, p, gamma, bn, s, err, blk, idx);
-}
-
 /* prj_hlld_fast_speed, src/prj_riemann.c:117-140; the clamp of a negative
  * discriminant is decision bit k */
-template <class BR, class DV = FxDivNative, class E = FxErr>
-FX_HD double fx_hlld_fast_speed_br(const FxHlldState &s, E *err, int blk, int idx, BR &br, int k, DV &&dv = DV())
+template <class BR>
+FX_HD double fx_hlld_fast_speed_br(const FxHlldState &s, FxErr *err, int blk, int idx, BR &br, int k)
 {
-    const double a2 = dv(s.gamma * s.p, s.rho);
-    const double bx2_rho = dv(s.bx * s.bx, s.rho);
-    const double b2_rho = dv(s.bx * s.bx + s.by * s.by + s.bz * s.bz, s.rho);
+    const double a2 = fx_div(s.gamma * s.p, s.rho);
+    const double bx2_rho = fx_div(s.bx * s.bx, s.rho);
+    const double b2_rho = fx_div(s.bx * s.bx + s.by * s.by + s.bz * s.bz, s.rho);
     double disc = (a2 + b2_rho) * (a2 + b2_rho) - 4.0 * a2 * bx2_rho;
     if (br.bit(k, disc < 0.0)) {
         if (disc < -1.0e-12 * (a2 + b2_rho) * (a2 + b2_rho)) {
@@ -555,16 +465,16 @@ FX_HD double fx_hlld_fast_speed(const FxHlldState &s, FxErr *err, int blk, int i
 
 /* prj_hlld_outer_star, src/prj_riemann.c:185-232; the degenerate-denominator
  * branch is decision bit k */
-template <class BR, class DV = FxDivNative, class E = FxErr>
+template <class BR>
 FX_HD void fx_hlld_outer_star_br(const FxHlldState &s, double S, double SM,
-    double pt_star, FxHlldStar &st, E *err, int blk, int idx, BR &br, int k, DV &&dv = DV())
+    double pt_star, FxHlldStar &st, FxErr *err, int blk, int idx, BR &br, int k)
 {
     const double alpha = S - s.vx;
     const double smdiff = S - SM;
     if (fabs(smdiff) <= 1.0e-14 * (fabs(S) + fabs(SM) + 1.0)) {
         fx_fail(err, FX_ERR_HLLD_OUTER, blk, idx);
     }
-    st.rho = dv(s.rho * alpha, smdiff);
+    st.rho = fx_div(s.rho * alpha, smdiff);
     if (st.rho <= 0.0 || !isfinite(st.rho)) {
         fx_fail(err, FX_ERR_HLLD_STARRHO, blk, idx);
     }
@@ -578,8 +488,8 @@ FX_HD void fx_hlld_outer_star_br(const FxHlldState &s, double S, double SM,
         st.by = s.by;
         st.bz = s.bz;
     } else {
-        const double sm_diff_vx_over_denom = dv(SM - s.vx, denom);
-        const double mag_factor = dv(s.rho * alpha * alpha - s.bx * s.bx, denom);
+        const double sm_diff_vx_over_denom = fx_div(SM - s.vx, denom);
+        const double mag_factor = fx_div(s.rho * alpha * alpha - s.bx * s.bx, denom);
         st.vy = s.vy - s.bx * s.by * sm_diff_vx_over_denom;
         st.vz = s.vz - s.bx * s.bz * sm_diff_vx_over_denom;
         st.by = s.by * mag_factor;
@@ -587,7 +497,7 @@ FX_HD void fx_hlld_outer_star_br(const FxHlldState &s, double S, double SM,
     }
     const double vdotb = s.vx * s.bx + s.vy * s.by + s.vz * s.bz;
     const double vstar_dotbstar = st.vx * st.bx + st.vy * st.by + st.vz * st.bz;
-    st.e = dv(alpha * s.e - s.pt * s.vx + pt_star * SM + s.bx * (vdotb - vstar_dotbstar), smdiff);
+    st.e = fx_div(alpha * s.e - s.pt * s.vx + pt_star * SM + s.bx * (vdotb - vstar_dotbstar), smdiff);
 }
 
 FX_HD void fx_hlld_outer_star(const FxHlldState &s, double S, double SM,
@@ -756,16 +666,16 @@ static __device__ __noinline__ void fx_riemann_hlld(const double *WL, const doub
  * Selecting operands and choosing between x - t and x + t are exact, so the
  * result is bit-identical to fx_riemann_hlld; warps whose faces straddle
  * SM = 0 no longer execute both branches. */
-template <class BR, class DV = FxDivNative, class E = FxErr>
+template <class BR>
 FX_HD void fx_riemann_hlld_folded_br(const double *WL, const double *WR,
     double pL, double pR, double gL, double gR, double bn, FxFaceOut &o,
-    E *err, int blk, int idx, BR &br, DV &&dv = DV())
+    FxErr *err, int blk, int idx, BR &br)
 {
     FxHlldState L, R;
-    fx_hlld_state_e(WL, pL, gL, bn, L, err, blk, idx);
-    fx_hlld_state_e(WR, pR, gR, bn, R, err, blk, idx);
-    const double cfL = fx_hlld_fast_speed_br(L, err, blk, idx, br, FX_BR_DISC_L, dv);
-    const double cfR = fx_hlld_fast_speed_br(R, err, blk, idx, br, FX_BR_DISC_R, dv);
+    fx_hlld_state(WL, pL, gL, bn, L, err, blk, idx);
+    fx_hlld_state(WR, pR, gR, bn, R, err, blk, idx);
+    const double cfL = fx_hlld_fast_speed_br(L, err, blk, idx, br, FX_BR_DISC_L);
+    const double cfR = fx_hlld_fast_speed_br(R, err, blk, idx, br, FX_BR_DISC_R);
     const double aL = L.vx - cfL, aR = R.vx - cfR;
     const double bL = L.vx + cfL, bR = R.vx + cfR;
     const double SL = br.bit(FX_BR_SL, aL < aR) ? aL : aR;   /* fx_min */
@@ -786,13 +696,13 @@ FX_HD void fx_riemann_hlld_folded_br(const double *WL, const double *WR,
         (fabs(R.rho * (SR - R.vx)) + fabs(L.rho * (SL - L.vx)) + 1.0)) {
         fx_fail(err, FX_ERR_HLLD_DENOM, blk, idx);
     }
-    const double SM = dv(R.rho * R.vx * (SR - R.vx) -
+    const double SM = fx_div(R.rho * R.vx * (SR - R.vx) -
         L.rho * L.vx * (SL - L.vx) + (L.pt - R.pt), denom);
     const double pt_star_l = L.pt + L.rho * (SL - L.vx) * (SM - L.vx);
     const double pt_star_r = R.pt + R.rho * (SR - R.vx) * (SM - R.vx);
     const double pt_star = 0.5 * (pt_star_l + pt_star_r);
     if (br.bit(FX_BR_HLL, pt_star <= 0.0 || !isfinite(pt_star))) {
-        const double inv = dv(1.0, SR - SL);
+        const double inv = fx_div(1.0, SR - SL);
         double Uh[9];
 #pragma unroll
         for (int v = 0; v < 9; ++v) {
@@ -804,7 +714,7 @@ FX_HD void fx_riemann_hlld_folded_br(const double *WL, const double *WR,
             Uh[v] = (SR * ru - SL * lu + lf - rf) * inv;
         }
         const double rho = Uh[0];
-        fx_face_outputs(dv(Uh[1], rho), dv(Uh[2], rho), dv(Uh[3], rho), Uh[6], Uh[7], Uh[8], o);
+        fx_face_outputs(fx_div(Uh[1], rho), fx_div(Uh[2], rho), fx_div(Uh[3], rho), Uh[6], Uh[7], Uh[8], o);
         return;
     }
     const bool bn_small = br.bit(FX_BR_BNSMALL, 0.5 * bn * bn < FX_HLLD_SMALL * pt_star);
@@ -812,8 +722,8 @@ FX_HD void fx_riemann_hlld_folded_br(const double *WL, const double *WR,
     const FxHlldState N = left ? L : R;
     const double SN = left ? SL : SR;
     FxHlldStar Ns;
-    fx_hlld_outer_star_br(N, SN, SM, pt_star, Ns, err, blk, idx, br, FX_BR_DEGEN_N, dv);
-    const double a = dv(fabs(bn), sqrt(Ns.rho));
+    fx_hlld_outer_star_br(N, SN, SM, pt_star, Ns, err, blk, idx, br, FX_BR_DEGEN_N);
+    const double a = fx_div(fabs(bn), sqrt(Ns.rho));
     const double SNs = left ? SM - a : SM + a;
     const bool single = br.bit(FX_BR_SINGLE, (left ? (0.0 <= SNs) : (SNs <= 0.0)) || bn_small);
     if (single) {
@@ -827,7 +737,7 @@ FX_HD void fx_riemann_hlld_folded_br(const double *WL, const double *WR,
     const FxHlldState Fr = left ? R : L;
     const double SF = left ? SR : SL;
     FxHlldStar Fs;
-    fx_hlld_outer_star_br(Fr, SF, SM, pt_star, Fs, err, blk, idx, br, FX_BR_DEGEN_F, dv);
+    fx_hlld_outer_star_br(Fr, SF, SM, pt_star, Fs, err, blk, idx, br, FX_BR_DEGEN_F);
     const FxHlldStar Ls = left ? Ns : Fs;
     const FxHlldStar Rs = left ? Fs : Ns;
     /* prj_hlld_double_star_one, src/prj_riemann.c:234-282 */
@@ -836,7 +746,7 @@ FX_HD void fx_riemann_hlld_folded_br(const double *WL, const double *WR,
     if (sqrt_l + sqrt_r <= 0.0) {
         fx_fail(err, FX_ERR_HLLD_DSTAR, blk, idx);
     }
-    const double inv_sum = dv(1.0, sqrt_l + sqrt_r);
+    const double inv_sum = fx_div(1.0, sqrt_l + sqrt_r);
     const double sign_bx = br.bit(FX_BR_BNEG, bn < 0.0) ? -1.0 : 1.0;
     FxHlldStar ss = Ns;
     ss.vy = (sqrt_l * Ls.vy + sqrt_r * Rs.vy + (Rs.by - Ls.by) * sign_bx) * inv_sum;

@@ -1859,34 +1859,6 @@ int fx_autotune(fx_ctx *c, double *times_ms, int n, int *choice)
     return check_device_error(c);
 }
 
-int fx_selftest_div(int device, long long n, unsigned long long seed, int emax, unsigned long long *mismatches,
-    unsigned long long *out_of_range)
-{
-    if (n <= 0 || emax <= 0 || emax > 1022 || !mismatches || !out_of_range) return FX_EINVAL;
-    if (cudaSetDevice(device) != cudaSuccess) {
-        cudaGetLastError();
-        return FX_ECUDA;
-    }
-    unsigned long long *d = nullptr;
-    unsigned long long h[2] = {0, 0};
-    cudaStream_t s = nullptr;
-    int rc = FX_SUCCESS;
-    if (cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess ||
-        cudaMalloc((void **)&d, 2 * sizeof(unsigned long long)) != cudaSuccess ||
-        cudaMemsetAsync(d, 0, 2 * sizeof(unsigned long long), s) != cudaSuccess ||
-        fx_launch_selftest_div(n, seed, emax, d, s) != 0 ||
-        cudaMemcpyAsync(h, d, sizeof h, cudaMemcpyDeviceToHost, s) != cudaSuccess ||
-        cudaStreamSynchronize(s) != cudaSuccess) {
-        cudaGetLastError();
-        rc = FX_ECUDA;
-    }
-    cudaFree(d);
-    if (s) cudaStreamDestroy(s);
-    *mismatches = h[0];
-    *out_of_range = h[1];
-    return rc;
-}
-
 int fx_branch_trace(fx_ctx *c, int mode, int max_stages, unsigned long long *flips)
 {
     if (!c) return FX_EINVAL;

@@ -447,17 +447,6 @@ int fx_amr_remesh_host(const fx_config *cfg, const fx_amr_config *amr, int nbloc
  * level apart.  The product's mesh builders use this one restatement. */
 int fx_mesh_slot_geometry(int nblocks, fx_block_desc *blocks);
 
-/* Self-test of the face solver's division (no reference counterpart): the
- * fused-multiply-add division the batched face kernel uses inside its
- * proven range against the device's native division, on n seeded random
- * operand pairs (random signs and significands, the delicate significands
- * 1.11...1, 1, 1 + ulp among them, zero dividends, exponents uniform in
- * [-emax, emax]).  *mismatches receives the quotients inside the range
- * that differ in any bit, *out_of_range the pairs the method hands back to
- * native division. */
-int fx_selftest_div(int device, long long n, unsigned long long seed, int emax, unsigned long long *mismatches,
-    unsigned long long *out_of_range);
-
 /* Decision record and replay of the plain form (no reference counterpart;
  * for checking the discrete adjoint against finite differences).  The
  * update is smooth in the state except where a decision switches: the MC
