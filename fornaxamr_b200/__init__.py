@@ -120,6 +120,15 @@ def amr_remesh_host(cfg: FxConfig, amr: FxAmrConfig, desc, votes: np.ndarray, ca
     return flags, res
 
 
+def dump_metadata(desc) -> np.ndarray:
+    """fx_dump_metadata: the MetaData rows of prj_io_write_dump."""
+    out = np.zeros((len(desc), _lib.DUMP_METADATA_SIZE))
+    rc = library().fx_dump_metadata(len(desc), desc, out.ctypes.data)
+    if rc != 0:
+        raise FxError(rc, "fx_dump_metadata failed")
+    return out
+
+
 def plan_export(cfg: FxConfig, desc, which: int):
     """Host-only dump of the compiled ghost fill: which = 0 cell ops, 1 face
     ops, 4 cell-field ops, 6 face-prolongation groups -> (ops [n, 4 or 8]
@@ -348,6 +357,17 @@ class Context:
     def download_state_active(self, W_all: np.ndarray, Bf_all: Optional[np.ndarray]) -> None:
         self._check(self.L.fx_download_state_active(self._h, W_all.ctypes.data,
                                                     None if Bf_all is None else Bf_all.ctypes.data))
+
+    def dump_gather(self, bf: bool = False):
+        """fx_dump_gather: the Data, Eos (and Bf) dataset contents of
+        prj_io_write_dump; rows of non-active entries stay zero."""
+        nb = self.nblocks
+        data = np.zeros((nb, self.nv, 16 ** 3))
+        eos = np.zeros((nb, 3, 16 ** 3))
+        bfa = np.zeros((nb, 3, NFACES)) if (bf and self.mhd) else None
+        self._check(self.L.fx_dump_gather(self._h, data.ctypes.data, eos.ctypes.data,
+                                          None if bfa is None else bfa.ctypes.data))
+        return data, eos, bfa
 
     def download_array(self, b: int, which: int, dir_: int = 0) -> np.ndarray:
         sizes = {ARR_W: self.nv * self.ns * NCELLS, ARR_EOSVAR: 3 * NCELLS, ARR_RHS: self.nv * NCELLS,

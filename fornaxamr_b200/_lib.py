@@ -16,6 +16,7 @@ LIB_PATH = os.path.join(HERE, "libfornax_b200.so" if NG == 2 else f"libfornax_b2
 
 FX_SUCCESS, FX_EINVAL, FX_ECUDA, FX_ENOMESH, FX_EPHYSICS, FX_ENOMEM, FX_ETOOBIG, FX_ECOMM = range(8)
 NOALLOC_MAX_BLOCKS = 65536
+DUMP_METADATA_SIZE = 639
 BRANCH_OFF, BRANCH_RECORD, BRANCH_REPLAY = 0, 1, 2
 FORM_PLAIN, FORM_BATCHED = 0, 1
 BC_OUTFLOW, BC_REFLECT, BC_USER, BC_PERIODIC = 0, 1, 2, 3
@@ -107,7 +108,7 @@ EXPORTS = [
     "fx_update_cells", "fx_riemann_flux_send", "fx_mhd_emf_send", "fx_eos_fill_active_cells",
     "fx_eos_fill_mesh", "fx_boundary_fill_ghosts_and_bf", "fx_calc_dt", "fx_stage", "fx_step",
     "fx_run", "fx_plan_export", "fx_time_phase", "fx_info", "fx_upload_state", "fx_download_state",
-    "fx_autotune", "fx_calc_dt_noalloc", "fx_mesh_slot_geometry", "fx_branch_trace",
+    "fx_autotune", "fx_calc_dt_noalloc", "fx_mesh_slot_geometry", "fx_branch_trace", "fx_dump_gather", "fx_dump_metadata",
     "fx_upload_state_active", "fx_download_state_active", "fx_face_eval_host", "fx_face_vjp_host",
     "fx_adjoint_forward", "fx_adjoint_backward", "fx_adjoint_time", "fx_set_flux_shape",
     "fx_amr_configure", "fx_amr_tag", "fx_amr_adapt", "fx_get_mesh", "fx_amr_energy_injected",
@@ -179,6 +180,8 @@ def load() -> C.CDLL:
     L.fx_branch_trace.argtypes = [vp, C.c_int, C.c_int, C.POINTER(C.c_ulonglong)]
     L.fx_upload_state_active.argtypes = [vp, vp, vp]
     L.fx_download_state_active.argtypes = [vp, vp, vp]
+    L.fx_dump_gather.argtypes = [vp, vp, vp, vp]
+    L.fx_dump_metadata.argtypes = [C.c_int, C.POINTER(FxBlockDesc), vp]
     L.fx_mesh_slot_geometry.argtypes = [C.c_int, C.POINTER(FxBlockDesc)]
     L.fx_calc_dt_noalloc.argtypes = [vp, C.c_int, C.c_int, vp, C.c_int, vp, C.c_int, C.c_double, C.c_double, vp, vp]
     L.fx_adjoint_forward.argtypes = [vp, C.c_int, C.c_double]

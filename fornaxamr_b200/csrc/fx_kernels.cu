@@ -1504,6 +1504,47 @@ void fx_flux_shape(int variant, int *tpb, int *minb)
 }
 
 /* ------------------------------------------------------------------------ */
+/* Dump payloads (prj_io_write_dump, src/prj_io.c:1994-2330)                */
+/* ------------------------------------------------------------------------ */
+/* The rows of the dump's Data, Eos and Bf datasets for the listed blocks,
+ * packed per list position q at out + q * row: Data [v][cell] (stage slot 0
+ * of W, cell = (i * 16 + j) * 16 + k over the active cells), Eos [v][cell]
+ * (p, T, gamma from eosvar), then, when faces is set, Bf [d][face] (stage
+ * slot 0, all faces). */
+__global__ void __launch_bounds__(256) k_dump_pack(FxDev D, const int *__restrict__ blist, int faces,
+    double *__restrict__ out)
+{
+    constexpr int NC = FX_BS * FX_BS * FX_BS;
+    const int nv = D.nv;
+    const size_t row = (size_t)(nv + 3) * NC + (faces ? (size_t)3 * FX_NFACES : 0);
+    const int b = blist[blockIdx.y];
+    double *o = out + (size_t)blockIdx.y * row;
+    for (size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x; t < row; t += (size_t)gridDim.x * blockDim.x) {
+        if (t < (size_t)(nv + 3) * NC) {
+            const int v = (int)(t / NC);
+            const int r = (int)(t - (size_t)v * NC);
+            const int i = r / (FX_BS * FX_BS), j = (r / FX_BS) % FX_BS, k = r % FX_BS;
+            if (v < nv) {
+                o[t] = D.W[(size_t)b * FX_W_COUNT(nv) + (size_t)v * FX_NSTAGES * FX_NCELLS + fx_lidx(i, j, k)];
+            } else {
+                o[t] = D.eos[(size_t)b * FX_EOS_COUNT + fx_bidx(3, v - nv, i, j, k)];
+            }
+        } else {
+            const size_t u = t - (size_t)(nv + 3) * NC;
+            const int d = (int)(u / FX_NFACES);
+            const int n = (int)(u - (size_t)d * FX_NFACES);
+            o[t] = D.Bf[(size_t)b * FX_BF_COUNT + (size_t)d * FX_NSTAGES * FX_NFACES + n];
+        }
+    }
+}
+
+void fx_launch_dump_pack(const FxDev &D, const int *blist, int nlist, int faces, double *out, cudaStream_t s)
+{
+    if (nlist <= 0) return;
+    k_dump_pack<<<dim3(64, nlist), 256, 0, s>>>(D, blist, faces, out);
+}
+
+/* ------------------------------------------------------------------------ */
 /* Active-region state transfer with page-locked host memory                 */
 /* ------------------------------------------------------------------------ */
 /* Stage slot 0 of the listed blocks' active cells (every variable) and

@@ -195,6 +195,9 @@ void fx_launch_xunpack(const FxDev &D, const FxXent *ents, int n, const double *
  * arrays and device-mapped page-locked host arrays (hs host stage slots) */
 void fx_launch_active_state(const FxDev &D, const int *blist, int nlist, double *hW, double *hBf, int hs,
     bool to_device, cudaStream_t s);
+/* the dump rows (Data, Eos, optionally Bf) of the listed blocks, packed
+ * contiguously per list position */
+void fx_launch_dump_pack(const FxDev &D, const int *blist, int nlist, int faces, double *out, cudaStream_t s);
 void fx_launch_flux_correct(const FxDev &D, const FxCorr *recs, int n, int ncomp, cudaStream_t s);
 void fx_launch_emf_correct(const FxDev &D, const FxCorr *recs, int n, cudaStream_t s);
 void fx_launch_reset_reductions(const FxDev &D, int which, cudaStream_t s);

@@ -1485,6 +1485,77 @@ int fx_download_state_active(fx_ctx *c, double *W_all, double *Bf_all)
     return rc ? rc : sync_and_check(c);
 }
 
+int fx_dump_gather(fx_ctx *c, double *data, double *eos, double *bf)
+{
+    if (c && c->nranks > 1) return set_err(c, FX_EINVAL, "%s: not available on a sharded mesh", __func__);
+    if (!has_mesh(c)) return c ? set_err(c, FX_ENOMESH, "no mesh") : FX_EINVAL;
+    if (!data && !eos && !bf) return set_err(c, FX_EINVAL, "%s: no output", __func__);
+    const int faces = (bf && c->cfg.mhd) ? 1 : 0;
+    const size_t nc = (size_t)FX_BS * FX_BS * FX_BS;
+    const size_t nw = (size_t)c->nv * nc;
+    const size_t row = nw + 3 * nc + (faces ? (size_t)3 * FX_NFACES : 0);
+    const size_t n = (size_t)c->nactive;
+    if (n == 0) return FX_SUCCESS;
+    /* eosvar of the stored state (the batched form does not keep it) */
+    fx_launch_eos_fill(c->D, c->d_active, c->nactive, 0, 1, c->stream);
+    double *d = nullptr;
+    cudaError_t e = cudaMalloc((void **)&d, n * row * sizeof(double));
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return set_err(c, FX_ENOMEM, "%s: no room for the %zu-byte staging buffer", __func__, n * row * sizeof(double));
+    }
+    std::vector<double> h(n * row);
+    fx_launch_dump_pack(c->D, c->d_active, c->nactive, faces, d, c->stream);
+    e = cudaMemcpyAsync(h.data(), d, n * row * sizeof(double), cudaMemcpyDeviceToHost, c->stream);
+    const cudaError_t e2 = cudaStreamSynchronize(c->stream);
+    cudaFree(d);
+    if (e != cudaSuccess || e2 != cudaSuccess) {
+        cudaGetLastError();
+        return set_err(c, FX_ECUDA, "%s: %s", __func__, cudaGetErrorString(e != cudaSuccess ? e : e2));
+    }
+    std::vector<int> act(n);
+    FX_CUDA(c, cudaMemcpy(act.data(), c->d_active, n * sizeof(int), cudaMemcpyDeviceToHost));
+    for (size_t q = 0; q < n; ++q) {
+        const size_t b = (size_t)act[q];
+        const double *r = h.data() + q * row;
+        if (data) std::memcpy(data + b * nw, r, nw * sizeof(double));
+        if (eos) std::memcpy(eos + b * 3 * nc, r + nw, 3 * nc * sizeof(double));
+        if (faces) std::memcpy(bf + b * 3 * FX_NFACES, r + nw + 3 * nc, 3 * (size_t)FX_NFACES * sizeof(double));
+    }
+    return sync_and_check(c);
+}
+
+int fx_dump_metadata(int nblocks, const fx_block_desc *blocks, double *meta)
+{
+    if (nblocks < 0 || (nblocks > 0 && (!blocks || !meta))) return FX_EINVAL;
+    for (int b = 0; b < nblocks; ++b) {
+        const fx_block_desc &k = blocks[b];
+        double *m = meta + (size_t)b * FX_DUMP_METADATA_SIZE;
+        std::fill(m, m + FX_DUMP_METADATA_SIZE, 0.0);
+        m[0] = (double)k.id;
+        m[2] = (double)k.level;
+        m[3] = (double)k.active;
+        for (int a = 0; a < 3; ++a) {
+            m[4 + a] = k.xmin[a];
+            m[7 + a] = k.xmax[a];
+            m[10 + a] = k.dx[a];
+        }
+        m[13] = (double)k.parent;
+        for (int o = 0; o < 8; ++o) m[15 + o] = (double)k.children[o];
+        int idx = 23;
+        for (int n = 0; n < 56; ++n) {
+            const int id = k.slot[n].id;
+            m[idx++] = (double)id;
+            ++idx; /* the slot's rank: 0 */
+            const bool nb = id >= 0 && id < nblocks;
+            for (int a = 0; a < 3; ++a) m[idx++] = nb ? blocks[id].xmin[a] : 0.0;
+            for (int a = 0; a < 3; ++a) m[idx++] = nb ? blocks[id].xmax[a] : 0.0;
+            for (int a = 0; a < 3; ++a) m[idx++] = nb ? blocks[id].dx[a] : 0.0;
+        }
+    }
+    return FX_SUCCESS;
+}
+
 int fx_download_array(fx_ctx *c, int b, int which, int dir, double *out)
 {
     if (c && c->nranks > 1) return set_err(c, FX_EINVAL, "%s: not available on a sharded mesh", __func__);

@@ -250,6 +250,32 @@ int fx_download_all(fx_ctx *ctx, double *W_all, double *Bf_all);
  * prj_timeint_step (slot 1 is the step's scratch). */
 int fx_upload_state(fx_ctx *ctx, const double *W_all, const double *Bf_all);
 int fx_download_state(fx_ctx *ctx, double *W_all, double *Bf_all);
+/* ---- dump payloads ------------------------------------------------------------ */
+
+/* Values per block of the dump's MetaData dataset (src/prj_io.c:19). */
+#define FX_DUMP_METADATA_SIZE 639
+
+/* The contents of prj_io_write_dump's datasets (src/prj_io.c:1994-2330,
+ * dump_format_version 4), gathered from the device state for a host that
+ * writes them into its own container (the HDF5 library is not linked here):
+ *   data  [nblocks][NHYDRO][16^3]: Data, stage slot 0 of W at the active
+ *         cells, cell = (i 16 + j) 16 + k;
+ *   eos   [nblocks][3][16^3]: Eos, pressure, temperature and adiabatic index
+ *         (eosvar) at the active cells, from that state;
+ *   bf    [nblocks][3][NFACES]: Bf (the reference writes it in its
+ *         PRJ_MHD_DEBUG builds), stage slot 0 of every face.
+ * Rows of entries that are not active blocks are left untouched (the
+ * reference never writes them: zero-fill the arrays first for its file
+ * contents).  Any argument may be NULL; bf is ignored without MHD. */
+int fx_dump_gather(fx_ctx *ctx, double *data, double *eos, double *bf);
+
+/* The MetaData rows of prj_io_fill_metadata (src/prj_io.c:1133-1165) for a
+ * mesh description (e.g. from fx_get_mesh): id, rank 0, level, active,
+ * xmin[3], xmax[3], dx[3], parent, 0, children[8], then per slot the
+ * neighbour id, rank 0 and the neighbour's xmin[3], xmax[3], dx[3] (zeros
+ * for a free slot).  Host only. */
+int fx_dump_metadata(int nblocks, const fx_block_desc *blocks, double *meta);
+
 /* The state through its active region: stage slot 0 of the 16^3 active
  * cells (every variable) and the active faces (17 x 16 x 16 per direction),
  * in the host layout of fx_upload_state -- about two thirds (upload) and one
