@@ -13,7 +13,8 @@
  * eos fill (k_eos_fill)       prj_eos_fill_block/_active_cells, src/prj_eos.c:1087-1162
  * dt (k_calc_dt)              prj_timeint_calc_dt, src/prj_timeint.c:2144-2256
  * ghost programs              prj_boundary_fill_ghosts_and_bf, src/prj_boundary.c:1150-1241
- * bf2bc (k_bf2bc)             prj_mhd_bf2bc_impl, src/prj_mhd.c:555-603
+ * bf2bc                       prj_mhd_bf2bc_impl, src/prj_mhd.c:555-603: ghost cells in
+ *                             the ghost programs, active cells in k_cell_field_active
  */
 #include <cuda_runtime.h>
 
@@ -1595,6 +1596,41 @@ __global__ void __launch_bounds__(256) k_active_state(FxDev D, const int *__rest
     } else {
         *h = *d;
     }
+}
+
+/* The cell-centred field of the listed blocks' active cells from their
+ * faces, stage slot 0: prj_mhd_bf2bc_impl's arithmetic (src/prj_mhd.c:
+ * 585-590; the metric factor is 1 outside dynamical GR) */
+__global__ void __launch_bounds__(256) k_cell_field_active(FxDev D, const int *__restrict__ blist)
+{
+    constexpr int NC = FX_BS * FX_BS * FX_BS;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= NC) {
+        return;
+    }
+    const int b = blist[blockIdx.y];
+    const int i = t / (FX_BS * FX_BS), j = (t / FX_BS) % FX_BS, k = t % FX_BS;
+    const double *bf = D.Bf + (size_t)b * FX_BF_COUNT;
+    const double *f1 = bf;
+    const double *f2 = bf + (size_t)FX_NSTAGES * FX_NFACES;
+    const double *f3 = bf + (size_t)2 * FX_NSTAGES * FX_NFACES;
+    const double b1 = 0.5 * (f1[fx_face_idx(0, i, j, k)] + f1[fx_face_idx(0, i + 1, j, k)]);
+    const double b2 = 0.5 * (f2[fx_face_idx(1, i, j, k)] + f2[fx_face_idx(1, i, j + 1, k)]);
+    const double b3 = 0.5 * (f3[fx_face_idx(2, i, j, k)] + f3[fx_face_idx(2, i, j, k + 1)]);
+    if (!isfinite(b1) || !isfinite(b2) || !isfinite(b3)) {
+        fx_fail(D.err, FX_ERR_B_NONFINITE, b, fx_lidx(i, j, k));
+    }
+    double *w = D.W + (size_t)b * FX_W_COUNT(9) + fx_lidx(i, j, k);
+    w[(size_t)FX_B1 * FX_NSTAGES * FX_NCELLS] = b1;
+    w[(size_t)FX_B2 * FX_NSTAGES * FX_NCELLS] = b2;
+    w[(size_t)FX_B3 * FX_NSTAGES * FX_NCELLS] = b3;
+}
+
+void fx_launch_cell_field_active(const FxDev &D, const int *blist, int nlist, cudaStream_t s)
+{
+    if (nlist <= 0) return;
+    constexpr int NC = FX_BS * FX_BS * FX_BS;
+    k_cell_field_active<<<dim3(fx_blocks(NC, 256), nlist), 256, 0, s>>>(D, blist);
 }
 
 void fx_launch_active_state(const FxDev &D, const int *blist, int nlist, double *hW, double *hBf, int hs,

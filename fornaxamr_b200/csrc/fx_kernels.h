@@ -198,6 +198,8 @@ void fx_launch_active_state(const FxDev &D, const int *blist, int nlist, double 
 /* the dump rows (Data, Eos, optionally Bf) of the listed blocks, packed
  * contiguously per list position */
 void fx_launch_dump_pack(const FxDev &D, const int *blist, int nlist, int faces, double *out, cudaStream_t s);
+/* cell-centred field of the listed blocks' active cells from the faces (slot 0) */
+void fx_launch_cell_field_active(const FxDev &D, const int *blist, int nlist, cudaStream_t s);
 void fx_launch_flux_correct(const FxDev &D, const FxCorr *recs, int n, int ncomp, cudaStream_t s);
 void fx_launch_emf_correct(const FxDev &D, const FxCorr *recs, int n, cudaStream_t s);
 void fx_launch_reset_reductions(const FxDev &D, int which, cudaStream_t s);

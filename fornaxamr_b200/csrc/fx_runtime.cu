@@ -1445,10 +1445,17 @@ int dma_active_h2d(fx_ctx *c, const double *W_all, const double *Bf_all)
     };
     if (W_all) {
         /* cell (i, j, k) = (i + G) P^2 + (j + G) P + (k + G); rows: i-planes of
-         * the active j range, z: (block, variable) with hs (2) slots apart */
+         * the active j range, z: blocks, one copy per variable.  The cell
+         * field (MHD) is not copied: it is the face average, recomputed on
+         * the device from the faces */
         const size_t off = G * P * P + G * P;
-        FX_CUDA(c, copy3d(W_all + off, hs * P, c->d_W + off, (size_t)FX_NSTAGES * P, P * P, B * P, B,
-            nb * (size_t)c->nv));
+        const size_t nvar = c->cfg.mhd ? (size_t)FX_B1 : (size_t)c->nv;
+        for (size_t v = 0; v < nvar; ++v) {
+            const size_t hoff = v * hs * FX_NCELLS + off;
+            const size_t doff = v * FX_NSTAGES * FX_NCELLS + off;
+            FX_CUDA(c, copy3d(W_all + hoff, (size_t)c->nv * hs * P, c->d_W + doff, (size_t)c->nv * FX_NSTAGES * P,
+                P * P, B * P, B, nb));
+        }
     }
     if (Bf_all && c->cfg.mhd) {
         for (int d = 0; d < 3; ++d) {
@@ -1474,6 +1481,10 @@ int fx_upload_state_active(fx_ctx *c, const double *W_all, const double *Bf_all)
     if (!W_all) return set_err(c, FX_EINVAL, "%s: W_all is required", __func__);
     int rc = dma_active_h2d(c, W_all, Bf_all);
     if (rc) return rc;
+    if (c->cfg.mhd) {
+        if (!Bf_all) return set_err(c, FX_EINVAL, "%s: Bf_all is required in MHD runs", __func__);
+        fx_launch_cell_field_active(c->D, c->d_active, c->nactive, c->stream);
+    }
     /* the ghost cells and faces of slot 0 from the active ones: the fill
      * that produced the host's ghost zones (src/main.c:446) */
     return fx_boundary_fill_ghosts_and_bf(c, 1, 0);

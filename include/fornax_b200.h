@@ -278,11 +278,12 @@ int fx_dump_metadata(int nblocks, const fx_block_desc *blocks, double *meta);
 
 /* The state through its active region: stage slot 0 of the 16^3 active
  * cells (every variable) and the active faces (17 x 16 x 16 per direction),
- * in the host layout of fx_upload_state -- about two thirds (upload) and one
- * half (download) of fx_upload_state's bytes for 16^3 blocks with two ghost
- * layers.  fx_upload_state_active moves, per block, the rows of the active
- * (i, j) range whole (ghost columns along k included) with the copy engines,
- * then runs the ghost fill of slot 0 (prj_boundary_fill_ghosts_and_bf with
+ * in the host layout of fx_upload_state -- about half of fx_upload_state's
+ * bytes each way for 16^3 blocks with two ghost layers.  fx_upload_state_active moves, per block, the rows of the active
+ * (i, j) range whole (ghost columns along k included) with the copy engines
+ * -- in MHD runs all variables but the cell-centred field, which it sets
+ * from the faces as prj_mhd_bf2bc does (Bf_all is then required) -- and
+ * runs the ghost fill of slot 0 (prj_boundary_fill_ghosts_and_bf with
  * stage 1 and the stage-0 field).  fx_download_state_active writes only the
  * active entries of slot 0 of the active blocks, with kernels that store
  * straight into the host arrays, and synchronises; its host arrays must be
