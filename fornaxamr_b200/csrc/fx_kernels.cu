@@ -216,7 +216,12 @@ __global__ void __launch_bounds__(TPB, MINB) k_flux(FxDev D, const int *__restri
         WR[FX_B1] = bn;
         FxFaceOut o;
         if constexpr (BRM == 0) {
-            fx_riemann_hlld_folded(WL, WR, pL, pR, gL, gR, bn, o, D.err, b, cR);
+            FxErrLocal le;
+            FxBrFree bf;
+            fx_riemann_hlld_folded_br(WL, WR, pL, pR, gL, gR, bn, o, &le, b, cR, bf);
+            if (le.code != 0) {
+                fx_fail(D.err, le.code, le.block, le.index);
+            }
         } else {
             fx_riemann_hlld_folded_br(WL, WR, pL, pR, gL, gR, bn, o, D.err, b, cR, br);
             if constexpr (BRM == 1) {

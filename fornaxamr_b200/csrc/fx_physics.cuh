@@ -77,6 +77,24 @@ FX_HD double fx_max(double a, double b) { return a > b ? a : b; }
 /* the face solver's divisions (correctly rounded, as in the reference) */
 FX_HD double fx_div(double a, double b) { return a / b; }
 
+/* A thread-local record of the first failure, with fx_fail's
+ * first-error-wins rule: the face kernel collects a face's checks here (a
+ * predicated store each, so the checks do not split the solver into short
+ * basic blocks) and reports the record once the face is done. */
+struct FxErrLocal {
+    int code = 0;
+    int block = 0;
+    int index = 0;
+};
+
+FX_HD void fx_fail(FxErrLocal *err, int code, int block, int index)
+{
+    const bool first = err->code == 0;
+    err->code = first ? code : err->code;
+    err->block = first ? block : err->block;
+    err->index = first ? index : err->index;
+}
+
 /* ------------------------------------------------------------------------ */
 /* Branch policies.  The solvers below take their data-dependent decisions  */
 /* (limiter candidate, wave-speed argument, fan region, upwind direction)   */
@@ -413,8 +431,9 @@ FX_HD double fx_hlld_state_f(const FxHlldState &s, int v)
 
 /* prj_hlld_state_from_prim, src/prj_riemann.c:142-178; w is the local
  * (direction-rotated) primitive vector, the normal field is bn. */
-FX_HD void fx_hlld_state(const double *w, double p, double gamma, double bn,
-    FxHlldState &s, FxErr *err, int blk, int idx)
+template <class E>
+FX_HD void fx_hlld_state_e(const double *w, double p, double gamma, double bn,
+    FxHlldState &s, E *err, int blk, int idx)
 {
     s.rho = w[FX_RHO];
     s.vx = w[FX_V1];
@@ -435,10 +454,16 @@ FX_HD void fx_hlld_state(const double *w, double p, double gamma, double bn,
     s.pt = s.p + magnetic;
 }
 
+FX_HD void fx_hlld_state(const double *w, double p, double gamma, double bn,
+    FxHlldState &s, FxErr *err, int blk, int idx)
+{
+    fx_hlld_state_e(w, p, gamma, bn, s, err, blk, idx);
+}
+
 /* prj_hlld_fast_speed, src/prj_riemann.c:117-140; the clamp of a negative
  * discriminant is decision bit k */
-template <class BR>
-FX_HD double fx_hlld_fast_speed_br(const FxHlldState &s, FxErr *err, int blk, int idx, BR &br, int k)
+template <class BR, class E = FxErr>
+FX_HD double fx_hlld_fast_speed_br(const FxHlldState &s, E *err, int blk, int idx, BR &br, int k)
 {
     const double a2 = fx_div(s.gamma * s.p, s.rho);
     const double bx2_rho = fx_div(s.bx * s.bx, s.rho);
@@ -465,9 +490,9 @@ FX_HD double fx_hlld_fast_speed(const FxHlldState &s, FxErr *err, int blk, int i
 
 /* prj_hlld_outer_star, src/prj_riemann.c:185-232; the degenerate-denominator
  * branch is decision bit k */
-template <class BR>
+template <class BR, class E = FxErr>
 FX_HD void fx_hlld_outer_star_br(const FxHlldState &s, double S, double SM,
-    double pt_star, FxHlldStar &st, FxErr *err, int blk, int idx, BR &br, int k)
+    double pt_star, FxHlldStar &st, E *err, int blk, int idx, BR &br, int k)
 {
     const double alpha = S - s.vx;
     const double smdiff = S - SM;
@@ -666,14 +691,14 @@ static __device__ __noinline__ void fx_riemann_hlld(const double *WL, const doub
  * Selecting operands and choosing between x - t and x + t are exact, so the
  * result is bit-identical to fx_riemann_hlld; warps whose faces straddle
  * SM = 0 no longer execute both branches. */
-template <class BR>
+template <class BR, class E = FxErr>
 FX_HD void fx_riemann_hlld_folded_br(const double *WL, const double *WR,
     double pL, double pR, double gL, double gR, double bn, FxFaceOut &o,
-    FxErr *err, int blk, int idx, BR &br)
+    E *err, int blk, int idx, BR &br)
 {
     FxHlldState L, R;
-    fx_hlld_state(WL, pL, gL, bn, L, err, blk, idx);
-    fx_hlld_state(WR, pR, gR, bn, R, err, blk, idx);
+    fx_hlld_state_e(WL, pL, gL, bn, L, err, blk, idx);
+    fx_hlld_state_e(WR, pR, gR, bn, R, err, blk, idx);
     const double cfL = fx_hlld_fast_speed_br(L, err, blk, idx, br, FX_BR_DISC_L);
     const double cfR = fx_hlld_fast_speed_br(R, err, blk, idx, br, FX_BR_DISC_R);
     const double aL = L.vx - cfL, aR = R.vx - cfR;
@@ -723,7 +748,8 @@ FX_HD void fx_riemann_hlld_folded_br(const double *WL, const double *WR,
     const double SN = left ? SL : SR;
     FxHlldStar Ns;
     fx_hlld_outer_star_br(N, SN, SM, pt_star, Ns, err, blk, idx, br, FX_BR_DEGEN_N);
-    const double a = fx_div(fabs(bn), sqrt(Ns.rho));
+    const double sqN = sqrt(Ns.rho);
+    const double a = fx_div(fabs(bn), sqN);
     const double SNs = left ? SM - a : SM + a;
     const bool single = br.bit(FX_BR_SINGLE, (left ? (0.0 <= SNs) : (SNs <= 0.0)) || bn_small);
     if (single) {
@@ -741,8 +767,10 @@ FX_HD void fx_riemann_hlld_folded_br(const double *WL, const double *WR,
     const FxHlldStar Ls = left ? Ns : Fs;
     const FxHlldStar Rs = left ? Fs : Ns;
     /* prj_hlld_double_star_one, src/prj_riemann.c:234-282 */
-    const double sqrt_l = sqrt(Ls.rho);
-    const double sqrt_r = sqrt(Rs.rho);
+    /* sqrt(Ls.rho), sqrt(Rs.rho): the near star's was taken above */
+    const double sqF = sqrt(Fs.rho);
+    const double sqrt_l = left ? sqN : sqF;
+    const double sqrt_r = left ? sqF : sqN;
     if (sqrt_l + sqrt_r <= 0.0) {
         fx_fail(err, FX_ERR_HLLD_DSTAR, blk, idx);
     }
