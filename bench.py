@@ -700,13 +700,14 @@ def run_fx(args, rank, world, local_rank):
     L = ctx.L
     dp = fx._dp
     h2d_full = nb * (9 * fx.NCELLS + 3 * fx.NFACES) * 8
-    # active upload: per block the rows of the active (i, j) range, ghost
-    # columns along k included, of the 6 non-field variables and of the
-    # three face directions (the cell field is recomputed from the faces);
-    # active download: the active cells (9 variables) and faces only
+    # active transfers: per block the rows of the active (i, j) range, ghost
+    # columns along k included, of the three face directions and of the 6
+    # non-field variables up (the cell field is recomputed from the faces),
+    # all 9 variables down
     P = 16 + 2 * fx.NG
-    h2d_active = nb * (6 * 16 * 16 * P + 17 * 16 * P + 16 * 17 * P + 16 * 16 * (P + 1)) * 8
-    d2h_active = nb * (9 * 16 ** 3 + 3 * 17 * 16 * 16) * 8
+    faces_span = 17 * 16 * P + 16 * 17 * P + 16 * 16 * (P + 1)
+    h2d_active = nb * (6 * 16 * 16 * P + faces_span) * 8
+    d2h_active = nb * (9 * 16 * 16 * P + faces_span) * 8
     e2e_ms = e2e_full_ms = None
     if args.e2e_steps > 0:
         for kind in ("active", "full"):
@@ -789,9 +790,9 @@ def run_fx(args, rank, world, local_rank):
         "e2e": None if e2e_ms is None else {
             "value": world * ZONES / (e2e_ms * 1e-3), "unit": UNIT, "ms_per_step": e2e_ms,
             "h2d_bytes_per_step": h2d_active, "d2h_bytes_per_step": d2h_active,
-            "copies": "fx_upload_state_active (copy engines: active-row spans of slot 0, cell field recomputed "
-                      "from the faces, ghost fill on the device) / fx_download_state_active (active cells and "
-                      "faces written into page-locked host arrays by the device)"},
+            "copies": "fx_upload_state_active / fx_download_state_active: copy-engine row copies of slot 0's "
+                      "active region (cell field recomputed from the faces and ghost zones refilled on the "
+                      "device after the upload)"},
         "e2e_full": None if e2e_full_ms is None else {
             "value": world * ZONES / (e2e_full_ms * 1e-3), "unit": UNIT, "ms_per_step": e2e_full_ms,
             "h2d_bytes_per_step": h2d_full, "d2h_bytes_per_step": h2d_full,

@@ -1551,58 +1551,8 @@ void fx_launch_dump_pack(const FxDev &D, const int *blist, int nlist, int faces,
 }
 
 /* ------------------------------------------------------------------------ */
-/* Active-region state transfer with page-locked host memory                 */
+/* Active-region state transfers: the cell-centred field after an upload    */
 /* ------------------------------------------------------------------------ */
-/* Stage slot 0 of the listed blocks' active cells (every variable) and
- * active faces (three directions) between the device arrays and host arrays
- * in the per-block reference layout (W: nv x hs slots x NCELLS, Bf: 3 x hs x
- * NFACES), the host side addressed through its device-mapped alias.  One
- * thread per double: a warp moves two 16-double rows of cells, so each host
- * access is a contiguous 128-byte run. */
-template <bool TO_DEVICE>
-__global__ void __launch_bounds__(256) k_active_state(FxDev D, const int *__restrict__ blist,
-    double *__restrict__ hW, double *__restrict__ hBf, int hs)
-{
-    constexpr int NC = FX_BS * FX_BS * FX_BS;
-    constexpr int NFA = (FX_BS + 1) * FX_BS * FX_BS;
-    const int nv = D.nv;
-    const int nw = nv * NC;
-    const int ntot = nw + (hBf != nullptr ? 3 * NFA : 0);
-    const int b = blist[blockIdx.y];
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= ntot) {
-        return;
-    }
-    if (t < nw) {
-        const int v = t / NC;
-        const int r = t - v * NC;
-        const int c = fx_lidx(r / (FX_BS * FX_BS), (r / FX_BS) % FX_BS, r % FX_BS);
-        double *h = hW + ((size_t)b * nv + v) * hs * FX_NCELLS + c;
-        double *d = D.W + (size_t)b * FX_W_COUNT(nv) + (size_t)v * FX_NSTAGES * FX_NCELLS + c;
-        if (TO_DEVICE) {
-            *d = *h;
-        } else {
-            *h = *d;
-        }
-        return;
-    }
-    int u = t - nw;
-    const int dir = u / NFA;
-    u -= dir * NFA;
-    const int e2 = dir == 2 ? FX_BS + 1 : FX_BS;
-    const int e1 = dir == 1 ? FX_BS + 1 : FX_BS;
-    const int k = u % e2;
-    u /= e2;
-    const int f = fx_face_idx(dir, u / e1, u % e1, k);
-    double *h = hBf + ((size_t)b * 3 + dir) * hs * FX_NFACES + f;
-    double *d = D.Bf + (size_t)b * FX_BF_COUNT + (size_t)dir * FX_NSTAGES * FX_NFACES + f;
-    if (TO_DEVICE) {
-        *d = *h;
-    } else {
-        *h = *d;
-    }
-}
-
 /* The cell-centred field of the listed blocks' active cells from their
  * faces, stage slot 0: prj_mhd_bf2bc_impl's arithmetic (src/prj_mhd.c:
  * 585-590; the metric factor is 1 outside dynamical GR) */
@@ -1636,21 +1586,6 @@ void fx_launch_cell_field_active(const FxDev &D, const int *blist, int nlist, cu
     if (nlist <= 0) return;
     constexpr int NC = FX_BS * FX_BS * FX_BS;
     k_cell_field_active<<<dim3(fx_blocks(NC, 256), nlist), 256, 0, s>>>(D, blist);
-}
-
-void fx_launch_active_state(const FxDev &D, const int *blist, int nlist, double *hW, double *hBf, int hs,
-    bool to_device, cudaStream_t s)
-{
-    if (nlist <= 0) return;
-    constexpr int NC = FX_BS * FX_BS * FX_BS;
-    constexpr int NFA = (FX_BS + 1) * FX_BS * FX_BS;
-    const int ntot = D.nv * NC + (hBf != nullptr ? 3 * NFA : 0);
-    const dim3 g(fx_blocks(ntot, 256), nlist);
-    if (to_device) {
-        k_active_state<true><<<g, 256, 0, s>>>(D, blist, hW, hBf, hs);
-    } else {
-        k_active_state<false><<<g, 256, 0, s>>>(D, blist, hW, hBf, hs);
-    }
 }
 
 void fx_launch_emf(const FxDev &D, const int *blist, int nlist, int wslot, int bfslot, cudaStream_t s)

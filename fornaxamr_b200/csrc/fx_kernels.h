@@ -191,10 +191,6 @@ void fx_launch_ghost_wave(const FxDev &D, const FxGop *cops, int nc, const FxGop
 void fx_launch_xpack(const FxDev &D, const FxXent *ents, int n, double *buf, int slot, cudaStream_t s);
 void fx_launch_xunpack(const FxDev &D, const FxXent *ents, int n, const double *buf, int slot, cudaStream_t s);
 /* one wave of correction records; ncomp flux components per record */
-/* slot 0 of the listed blocks' active cells and faces between the device
- * arrays and device-mapped page-locked host arrays (hs host stage slots) */
-void fx_launch_active_state(const FxDev &D, const int *blist, int nlist, double *hW, double *hBf, int hs,
-    bool to_device, cudaStream_t s);
 /* the dump rows (Data, Eos, optionally Bf) of the listed blocks, packed
  * contiguously per list position */
 void fx_launch_dump_pack(const FxDev &D, const int *blist, int nlist, int faces, double *out, cudaStream_t s);

@@ -1393,63 +1393,37 @@ int fx_download_state(fx_ctx *c, double *W_all, double *Bf_all)
     return FX_SUCCESS;
 }
 
-/* device-mapped alias of a page-locked host buffer, or null */
-double *mapped_host(const void *p)
-{
-    if (!p) return nullptr;
-    cudaPointerAttributes a{};
-    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
-        cudaGetLastError();
-        return nullptr;
-    }
-    if (a.type != cudaMemoryTypeHost || !a.devicePointer) return nullptr;
-    return static_cast<double *>(a.devicePointer);
-}
-
-int active_state(fx_ctx *c, double *W_all, double *Bf_all, bool to_device, const char *fn)
-{
-    if (c && c->nranks > 1) return set_err(c, FX_EINVAL, "%s: not available on a sharded mesh", fn);
-    if (!has_mesh(c)) return c ? set_err(c, FX_ENOMESH, "no mesh") : FX_EINVAL;
-    if (!W_all) return set_err(c, FX_EINVAL, "%s: W_all is required", fn);
-    double *hW = mapped_host(W_all);
-    double *hB = c->cfg.mhd ? mapped_host(Bf_all) : nullptr;
-    if (!hW || (c->cfg.mhd && Bf_all && !hB)) {
-        return set_err(c, FX_EINVAL, "%s: the host arrays must be page-locked (cudaHostAlloc / cudaHostRegister)", fn);
-    }
-    fx_launch_active_state(c->D, c->d_active, c->nactive, hW, hB, host_ns(c), to_device, c->stream);
-    FX_CUDA(c, cudaGetLastError());
-    return FX_SUCCESS;
-}
-
-/* Host -> device copy of slot 0's active region by the copy engines: one
- * 3-D copy for W over (block, variable) planes, one per Bf direction over
- * blocks; every copied row is the whole span of one i-plane's active rows
- * (ghost columns along k included), 2.5-2.7 KB, so the engines run at full
- * rate.  Every block entry (active or not) is covered. */
-int dma_active_h2d(fx_ctx *c, const double *W_all, const double *Bf_all)
+/* Copies of slot 0's active region by the copy engines: for W one 3-D copy
+ * per variable over blocks, for Bf one per direction over blocks; every
+ * copied row is the whole span of one i-plane's active rows (ghost columns
+ * along k included), 2.5-2.7 KB, so the engines run at full rate.  Every
+ * block entry (active or not) is covered.  Host -> device leaves out the
+ * cell-centred field (MHD; recomputed from the faces), device -> host
+ * copies every variable. */
+int dma_active(fx_ctx *c, double *W_all, double *Bf_all, cudaMemcpyKind kind)
 {
     constexpr size_t P = FX_PBS;
     constexpr size_t G = FX_NG;
     constexpr size_t B = FX_BS;
     const size_t hs = (size_t)host_ns(c);
     const size_t nb = (size_t)c->nblocks;
-    auto copy3d = [&](const double *src, size_t src_ysize, double *dst, size_t dst_ysize, size_t pitch_el,
+    const bool up = kind == cudaMemcpyHostToDevice;
+    auto copy3d = [&](double *host, size_t host_ysize, double *dev, size_t dev_ysize, size_t pitch_el,
                       size_t width_el, size_t height, size_t depth) -> cudaError_t {
         cudaMemcpy3DParms p{};
-        p.srcPtr = make_cudaPitchedPtr(const_cast<double *>(src), pitch_el * sizeof(double), width_el * sizeof(double),
-            src_ysize);
-        p.dstPtr = make_cudaPitchedPtr(dst, pitch_el * sizeof(double), width_el * sizeof(double), dst_ysize);
+        cudaPitchedPtr h = make_cudaPitchedPtr(host, pitch_el * sizeof(double), width_el * sizeof(double), host_ysize);
+        cudaPitchedPtr d = make_cudaPitchedPtr(dev, pitch_el * sizeof(double), width_el * sizeof(double), dev_ysize);
+        p.srcPtr = up ? h : d;
+        p.dstPtr = up ? d : h;
         p.extent = make_cudaExtent(width_el * sizeof(double), height, depth);
-        p.kind = cudaMemcpyHostToDevice;
+        p.kind = kind;
         return cudaMemcpy3DAsync(&p, c->stream);
     };
     if (W_all) {
         /* cell (i, j, k) = (i + G) P^2 + (j + G) P + (k + G); rows: i-planes of
-         * the active j range, z: blocks, one copy per variable.  The cell
-         * field (MHD) is not copied: it is the face average, recomputed on
-         * the device from the faces */
+         * the active j range, z: blocks, one copy per variable */
         const size_t off = G * P * P + G * P;
-        const size_t nvar = c->cfg.mhd ? (size_t)FX_B1 : (size_t)c->nv;
+        const size_t nvar = (up && c->cfg.mhd) ? (size_t)FX_B1 : (size_t)c->nv;
         for (size_t v = 0; v < nvar; ++v) {
             const size_t hoff = v * hs * FX_NCELLS + off;
             const size_t doff = v * FX_NSTAGES * FX_NCELLS + off;
@@ -1479,7 +1453,7 @@ int fx_upload_state_active(fx_ctx *c, const double *W_all, const double *Bf_all)
     if (c && c->nranks > 1) return set_err(c, FX_EINVAL, "%s: not available on a sharded mesh", __func__);
     if (!has_mesh(c)) return c ? set_err(c, FX_ENOMESH, "no mesh") : FX_EINVAL;
     if (!W_all) return set_err(c, FX_EINVAL, "%s: W_all is required", __func__);
-    int rc = dma_active_h2d(c, W_all, Bf_all);
+    int rc = dma_active(c, const_cast<double *>(W_all), const_cast<double *>(Bf_all), cudaMemcpyHostToDevice);
     if (rc) return rc;
     if (c->cfg.mhd) {
         if (!Bf_all) return set_err(c, FX_EINVAL, "%s: Bf_all is required in MHD runs", __func__);
@@ -1492,7 +1466,10 @@ int fx_upload_state_active(fx_ctx *c, const double *W_all, const double *Bf_all)
 
 int fx_download_state_active(fx_ctx *c, double *W_all, double *Bf_all)
 {
-    const int rc = active_state(c, W_all, Bf_all, false, __func__);
+    if (c && c->nranks > 1) return set_err(c, FX_EINVAL, "%s: not available on a sharded mesh", __func__);
+    if (!has_mesh(c)) return c ? set_err(c, FX_ENOMESH, "no mesh") : FX_EINVAL;
+    if (!W_all) return set_err(c, FX_EINVAL, "%s: W_all is required", __func__);
+    const int rc = dma_active(c, W_all, Bf_all, cudaMemcpyDeviceToHost);
     return rc ? rc : sync_and_check(c);
 }
 

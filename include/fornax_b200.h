@@ -277,24 +277,24 @@ int fx_dump_gather(fx_ctx *ctx, double *data, double *eos, double *bf);
 int fx_dump_metadata(int nblocks, const fx_block_desc *blocks, double *meta);
 
 /* The state through its active region: stage slot 0 of the 16^3 active
- * cells (every variable) and the active faces (17 x 16 x 16 per direction),
- * in the host layout of fx_upload_state -- about half of fx_upload_state's
- * bytes each way for 16^3 blocks with two ghost layers.  fx_upload_state_active moves, per block, the rows of the active
- * (i, j) range whole (ghost columns along k included) with the copy engines
- * -- in MHD runs all variables but the cell-centred field, which it sets
- * from the faces as prj_mhd_bf2bc does (Bf_all is then required) -- and
- * runs the ghost fill of slot 0 (prj_boundary_fill_ghosts_and_bf with
- * stage 1 and the stage-0 field).  fx_download_state_active writes only the
- * active entries of slot 0 of the active blocks, with kernels that store
- * straight into the host arrays, and synchronises; its host arrays must be
- * page-locked (cudaHostAlloc, cudaMallocHost or cudaHostRegister), else
- * FX_EINVAL.  The ghost fill does not write every ghost entry: a few of the
+ * cells and of the active faces (17 x 16 x 16 per direction), in the host
+ * layout of fx_upload_state, moved by the copy engines as whole rows of the
+ * active (i, j) range (the ghost columns along k of those rows included) --
+ * about half of fx_upload_state's bytes each way for 16^3 blocks with two
+ * ghost layers.  fx_upload_state_active leaves out the cell-centred field
+ * in MHD runs and sets it from the faces as prj_mhd_bf2bc does (Bf_all is
+ * then required), then runs the ghost fill of slot 0
+ * (prj_boundary_fill_ghosts_and_bf with stage 1 and the stage-0 field).
+ * fx_download_state_active copies every variable and synchronises; the
+ * rest of the host arrays (the other ghost entries, other slots) is left
+ * untouched.  The ghost fill does not write every ghost entry: a few of the
  * outermost ghost faces and corner cells keep the values the set-up gave
  * them, in the reference as here.  Make one full transfer (fx_upload_state
  * or fx_upload_all) first; from then on the device state after
  * fx_upload_state_active equals the one fx_upload_state gives whenever the
  * host's ghost zones come from that fill, as they do after every reference
- * step. */
+ * step.  Page-locked host arrays make the copies asynchronous and fast;
+ * pageable ones work at the copy engines' staged rate. */
 int fx_upload_state_active(fx_ctx *ctx, const double *W_all, const double *Bf_all);
 int fx_download_state_active(fx_ctx *ctx, double *W_all, double *Bf_all);
 /* Any block array, including the step's scratch, for inspection. */

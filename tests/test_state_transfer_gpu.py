@@ -1,14 +1,14 @@
 """fx_upload_state_active / fx_download_state_active: the state through its
 active region, against the full-array transfers.
 
-The upload copies the rows of the active region with the copy engines and
-then runs the slot-0 ghost fill, so after one full upload (the contract: a
+Both copy the rows of the active region (the active (i, j) range, every k)
+with the copy engines.  The upload then sets the cell field from the faces
+and runs the slot-0 ghost fill, so after one full upload (the contract: a
 few outermost ghost entries are written by no fill and keep their set-up
 values) the device state must return to the host's state bit for bit even
 after the device has stepped away from it, and stay equal to a fresh full
-upload through a step.  The download must reproduce the active entries of a
-full download and leave every other host entry untouched; it needs
-page-locked host memory and rejects pageable arrays.
+upload through a step.  The download must reproduce those rows of a full
+download and leave every other host entry untouched.
 """
 import numpy as np
 import pytest
@@ -74,21 +74,25 @@ def test_active_state_transfers_match_full_transfers(ref_mhd, ref_hydro, mhd):
         if mhd:
             Bp[...] = np.nan
         b.download_state_active(Wp, Bp)
-        act = H.active_cells()
-        assert np.array_equal(Wp[:, :, 0][..., act], Wa[:, :, 0][..., act])
-        rest = np.ones(H.NCELLS, bool)
-        rest[act] = False
-        assert np.isnan(Wp[:, :, 0][..., rest]).all() and np.isnan(Wp[:, :, 1]).all()
+        r = np.arange(-H.NG, 16 + H.NG)
+        i, j, k = np.meshgrid(r, r, r, indexing="ij")
+        rows = ((i >= 0) & (i < 16) & (j >= 0) & (j < 16)).ravel()
+        cells = H.lidx(i, j, k).ravel()
+        span = np.zeros(H.NCELLS, bool)
+        span[cells[rows]] = True
+        assert np.array_equal(Wp[:, :, 0][..., span], Wa[:, :, 0][..., span])
+        assert np.isnan(Wp[:, :, 0][..., ~span]).all() and np.isnan(Wp[:, :, 1]).all()
         if mhd:
             for d in range(3):
-                fa = H.active_faces(d)
-                assert np.array_equal(Bp[:, d, 0][:, fa], Ba[:, d, 0][:, fa])
-                rest = np.ones(H.NFACES, bool)
-                rest[fa] = False
-                assert np.isnan(Bp[:, d, 0][:, rest]).all()
-
-        with pytest.raises(fx.FxError):
-            b.download_state_active(np.ascontiguousarray(W), None if Bf is None else np.ascontiguousarray(Bf))
+                e = [np.arange(-H.NG, 16 + H.NG + (1 if a == d else 0)) for a in range(3)]
+                fi, fj, fk = np.meshgrid(*e, indexing="ij")
+                top = [16 if d == 0 else 15, 16 if d == 1 else 15]
+                sel = ((fi >= 0) & (fi <= top[0]) & (fj >= 0) & (fj <= top[1])).ravel()
+                faces = H.face_idx(d, fi, fj, fk).ravel()
+                fspan = np.zeros(H.NFACES, bool)
+                fspan[faces[sel]] = True
+                assert np.array_equal(Bp[:, d, 0][:, fspan], Ba[:, d, 0][:, fspan])
+                assert np.isnan(Bp[:, d, 0][:, ~fspan]).all()
     finally:
         a.close()
         b.close()
