@@ -420,7 +420,7 @@ __global__ void __launch_bounds__(128) k_emf_edges(FxDev D, const int *__restric
 constexpr int kEmfChunk = 2;
 constexpr int kEmfChunks = (FX_BS + 1 + kEmfChunk - 1) / kEmfChunk;
 
-__global__ void __launch_bounds__(256) k_emf(FxDev D, const int *__restrict__ blist, int wslot, int bfslot)
+__global__ void __launch_bounds__(256, 5) k_emf(FxDev D, const int *__restrict__ blist, int wslot, int bfslot)
 {
     if (D.ctl->skip) {
         return;
