@@ -49,8 +49,9 @@ def _dp(a: np.ndarray):
 
 def make_config(mhd: bool, gamma: float, coord: Sequence[float], bc: Sequence[int] = (0,) * 6,
                 gravity: bool = False, mhd_eta: float = 0.0, recon: int = RECON_MC,
-                integrator: int = INT_RK2) -> FxConfig:
+                integrator: int = INT_RK2, use_bj: bool = False) -> FxConfig:
     cfg = FxConfig()
+    cfg.use_bj = 1 if use_bj else 0
     cfg.recon = int(recon)
     cfg.integrator = int(integrator)
     cfg.mhd = 1 if mhd else 0
@@ -231,13 +232,13 @@ class Context:
 
     def __init__(self, mhd: bool, gamma: float, coord: Sequence[float], bc: Sequence[int] = (0,) * 6,
                  gravity: bool = False, mhd_eta: float = 0.0, device: int = 0, recon: int = RECON_MC,
-                 integrator: int = INT_RK2):
+                 integrator: int = INT_RK2, use_bj: bool = False):
         self.L = library()
         self.mhd = bool(mhd)
         self.nv = 9 if mhd else 6
         # stage slots of the block W / Bf arrays: 2 (RK2) or 3 (eSSPRK10_4)
         self.ns = 3 if integrator == INT_ESSPRK10_4 else 2
-        self.cfg = make_config(mhd, gamma, coord, bc, gravity, mhd_eta, recon, integrator)
+        self.cfg = make_config(mhd, gamma, coord, bc, gravity, mhd_eta, recon, integrator, use_bj)
         self._h = C.c_void_p()
         rc = self.L.fx_create(device, C.byref(self.cfg), C.byref(self._h))
         if rc != 0:

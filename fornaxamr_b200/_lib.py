@@ -64,6 +64,8 @@ class FxConfig(C.Structure):
         ("mhd_eta", C.c_double),
         ("recon", C.c_int32),
         ("integrator", C.c_int32),
+        ("use_bj", C.c_int32),
+        ("pad", C.c_int32),
     ]
 
 

@@ -392,8 +392,9 @@ __device__ __forceinline__ void store_cell(const FxDev &D, int b, int i, int j, 
 /* conserved prolongation: the parent's octant plus one halo cell (10^3) as
  * conserved variables in shared memory, then per child cell the minmod
  * prolongation of prj_reconstruct_cell_for_prolongate_minmod
- * (src/prj_reconstruct.h:111-143), the density guard, the face-average field
- * and the primitive sync */
+ * (src/prj_reconstruct.h:111-143), or with use_BJ the Barth-Jespersen one
+ * (:145-195) on the 27-cell stencil, the density guard, the face-average
+ * field and the primitive sync */
 template <bool MHD>
 __global__ void __launch_bounds__(256) k_amr_prolong_cells(FxDev D, const FxAmrChildJob *__restrict__ jobs,
     double E_floor, double *inj)
@@ -425,6 +426,11 @@ __global__ void __launch_bounds__(256) k_amr_prolong_cells(FxDev D, const FxAmrC
         double u[FX_MAXVAR];
         for (int v = 0; v < NV; ++v) {
             const double *q = sU + v * R * R * R;
+            if (D.use_bj) {
+                const double *qr = q + r;
+                u[v] = fx_bj_cell([qr](int di, int dj, int dk) { return qr[(di * R + dj) * R + dk]; }, tx, ty, tz);
+                continue;
+            }
             const double base = q[r];
             const double vx = base + fx_minmod_slope(q[r - R * R], base, q[r + R * R]) * tx;
             const double vy = base + fx_minmod_slope(q[r - R], base, q[r + R]) * ty;

@@ -941,8 +941,8 @@ __global__ void k_step_end(FxDev D)
 
 /* prj_reconstruct_cell_for_prolongate_minmod (src/prj_reconstruct.h:111-143):
  * per axis base + slope * target, combined as vx + vy + vz - 2 base; target
- * offsets are +-1/4 of a coarse cell.  (The use_BJ = 1 limiter of the
- * reference is not selected by any configuration of this path.) */
+ * offsets are +-1/4 of a coarse cell.  use_BJ = 1 takes fx_bj_cell /
+ * fx_bj_face on the full 27-cell (3x3-face) stencil instead. */
 __device__ __forceinline__ double fx_prolong_cell(const double *q, int c, double tx, double ty, double tz)
 {
     const double base = q[c];
@@ -963,6 +963,10 @@ __device__ __forceinline__ double fx_prolong_face(const double *q, int f, int s0
     return vx + vy - base;
 }
 
+/* BJ: the program may hold Barth-Jespersen prolongations (use_BJ); the
+ * other instance keeps the copy-dominated wave kernel at its small register
+ * count */
+template <bool BJ>
 __device__ __forceinline__ void fx_ghost_cell_op(const FxDev &D, const FxGop op, int wslot, int nvg)
 {
     const int db = FX_CELL_BLOCK(op.dst);
@@ -1008,6 +1012,21 @@ __device__ __forceinline__ void fx_ghost_cell_op(const FxDev &D, const FxGop op,
         const double tz = (op.aux & 1) ? 0.25 : -0.25;
         for (int v = 0; v < nvg; ++v) {
             Wd[(size_t)v * kPlane + dc] = fx_prolong_cell(Ws + (size_t)v * kPlane, sc, tx, ty, tz);
+        }
+        break;
+    }
+    case FX_GOP_PROLONG_BJ: {
+        if constexpr (!BJ) {
+            break;
+        }
+        const double tx = (op.aux & 4) ? 0.25 : -0.25;
+        const double ty = (op.aux & 2) ? 0.25 : -0.25;
+        const double tz = (op.aux & 1) ? 0.25 : -0.25;
+#pragma unroll 1
+        for (int v = 0; v < nvg; ++v) {
+            const double *q = Ws + (size_t)v * kPlane + sc;
+            Wd[(size_t)v * kPlane + dc] = fx_bj_cell(
+                [q](int di, int dj, int dk) { return q[(di * FX_PBS + dj) * FX_PBS + dk]; }, tx, ty, tz);
         }
         break;
     }
@@ -1083,7 +1102,12 @@ __device__ __forceinline__ void fx_ghost_prolong_group(const FxDev &D, const FxP
                     if ((op.keep >> q) & 1) {
                         flux = Bfine[xf] * area[d];
                     } else {
-                        const double value = fx_prolong_face(Bc, cf, s0, s1, a ? 0.25 : -0.25, b ? 0.25 : -0.25);
+                        const double ta = a ? 0.25 : -0.25;
+                        const double tb = b ? 0.25 : -0.25;
+                        const double *qc = Bc + cf;
+                        const double value = (op.flags & 1)
+                            ? fx_bj_face([qc, s0, s1](int d0, int d1) { return qc[d0 * s0 + d1 * s1]; }, ta, tb)
+                            : fx_prolong_face(Bc, cf, s0, s1, ta, tb);
                         flux = value * area[d];
                         if ((op.owrite >> q) & 1) {
                             Bfine[xf] = flux / area[d];
@@ -1204,6 +1228,7 @@ __global__ void __launch_bounds__(128) k_ghost_groups(FxDev D, const FxPop *__re
 
 /* one conflict-free wave of the ghost fill: CTAs [0, nbc) run cell ops,
  * then face ops and cell-field ops */
+template <bool BJ>
 __global__ void __launch_bounds__(256) k_ghost_wave(FxDev D, const FxGop *__restrict__ cops, int nc,
     const FxGop *__restrict__ fops, int nf, const FxBop *__restrict__ bops, int nb, int slot, int nvg)
 {
@@ -1215,7 +1240,7 @@ __global__ void __launch_bounds__(256) k_ghost_wave(FxDev D, const FxGop *__rest
     int blk = blockIdx.x;
     if (blk < nbc) {
         const int t = blk * 256 + threadIdx.x;
-        if (t < nc) fx_ghost_cell_op(D, cops[t], slot, nvg);
+        if (t < nc) fx_ghost_cell_op<BJ>(D, cops[t], slot, nvg);
         return;
     }
     blk -= nbc;
@@ -1644,7 +1669,11 @@ void fx_launch_ghost_wave(const FxDev &D, const FxGop *cops, int nc, const FxGop
      * in either order */
     const unsigned grid = fx_blocks(nc, 256) + fx_blocks(nf, 256) + fx_blocks(nb, 256);
     if (grid > 0) {
-        k_ghost_wave<<<grid, 256, 0, s>>>(D, cops, nc, fops, nf, bops, nb, slot, nvg);
+        if (D.use_bj) {
+            k_ghost_wave<true><<<grid, 256, 0, s>>>(D, cops, nc, fops, nf, bops, nb, slot, nvg);
+        } else {
+            k_ghost_wave<false><<<grid, 256, 0, s>>>(D, cops, nc, fops, nf, bops, nb, slot, nvg);
+        }
     }
     if (np > 0) {
         k_ghost_groups<<<fx_blocks(np, 128), 128, 0, s>>>(D, pops, np, slot);

@@ -59,6 +59,7 @@ struct FxDev {
     FxCtl *ctl;
     int flux_variant;         /* launch shape of the face kernel (autotuned) */
     int recon;                /* FX_RECON_MC or FX_RECON_WENO3 */
+    int use_bj;               /* Barth-Jespersen prolongation limiter (refinement) */
     /* decisions of the plain form's face and edge kernels (MHD, MC):
      * br_mode 0 none, 1 record into / 2 replay from br_words (one word per
      * face, at br_off + (b * 3 + dir) * faces per direction + face) and
@@ -85,6 +86,8 @@ enum FxGopType {
     FX_GOP_RESTRICT = 3,    /* dst <- 1/8 sum of the 2x2x2 cells at src */
     FX_GOP_PROLONG = 4,     /* dst <- minmod-limited linear from src and its 6 axis neighbours,
                                target offsets +-1/4 from aux bits 2, 1, 0 (set: +) */
+    FX_GOP_PROLONG_BJ = 5,  /* dst <- Barth-Jespersen-limited linear from src and its 26
+                               neighbours, target offsets as FX_GOP_PROLONG */
     FX_FOP_COPY = 8,        /* face: dst <- src */
     FX_FOP_RESTRICT = 9,    /* face: dst <- 1/4 sum of 4 fine faces */
     FX_FOP_PROLONG = 10     /* face: divergence-free prolongation value */
@@ -116,7 +119,9 @@ struct FxBop {
  * (a, b) in increasing axis order; inner face q = 4 d + 2 a + b.  keep bit
  * q: outer face q keeps the fine block's value (its fidelity is above
  * COARSER); owrite bit q: outer face q is stored; iwrite bit q: inner face q
- * is stored.  The masks come from the data-independent fidelity replay. */
+ * is stored.  The masks come from the data-independent fidelity replay.
+ * flags bit 0: the outer faces take the Barth-Jespersen limiter on the 3x3
+ * tangential stencil (use_BJ), else minmod on the 5-point cross. */
 struct FxPop {
     int32_t fine;
     int32_t coarse;
@@ -124,7 +129,8 @@ struct FxPop {
     int32_t keep;
     int32_t owrite;
     int32_t iwrite;
-    int32_t pad[2];
+    int32_t flags;
+    int32_t pad;
 };
 
 /* coarse/fine correction records: entry dst of block dst_block <- 0.25 *

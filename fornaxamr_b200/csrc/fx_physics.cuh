@@ -302,6 +302,88 @@ FX_HD double fx_minmod_slope(double qm, double q0, double qp)
     return fabs(sl) < fabs(sr) ? sl : sr;
 }
 
+/* Barth-Jespersen limited prolongation (use_BJ), the stencil read through
+ * q(di, dj, dk) / q(di, dj) with offsets in {-1, 0, 1}:
+ * prj_reconstruct_cell_for_prolongate_bj and _face_for_prolongate_bj
+ * (src/prj_reconstruct.h:145-195, 248-290).  The central-difference
+ * gradient is scaled by the largest alpha in [0, 1] that keeps the eight
+ * fine sub-cell (four sub-face) values at offsets +-1/4 inside the range of
+ * the stencil's neighbours; the minimum / maximum and the alpha reduction run
+ * in the reference's loop order (a < b ? a : b, so the order decides which
+ * of +0.0 and -0.0 survives a tie). */
+FX_HD double fx_bj_min(double a, double b) { return a < b ? a : b; }
+FX_HD double fx_bj_max(double a, double b) { return a > b ? a : b; }
+FX_HD double fx_bj_clamp01(double x) { return x < 0.0 ? 0.0 : (x > 1.0 ? 1.0 : x); }
+
+/* alpha update of one sub-cell value base + delta */
+FX_HD double fx_bj_alpha(double alpha, double base, double delta, double qmin, double qmax)
+{
+    const double q = base + delta;
+    if (q > qmax) {
+        const double a = delta != 0.0 ? (qmax - base) / delta : 0.0;
+        return fx_bj_min(alpha, fx_bj_clamp01(a));
+    }
+    if (q < qmin) {
+        const double a = delta != 0.0 ? (qmin - base) / delta : 0.0;
+        return fx_bj_min(alpha, fx_bj_clamp01(a));
+    }
+    return alpha;
+}
+
+template <class Q>
+FX_HD double fx_bj_cell(const Q &q, double tx, double ty, double tz)
+{
+    const double base = q(0, 0, 0);
+    const double g0 = 0.5 * (q(1, 0, 0) - q(-1, 0, 0));
+    const double g1 = 0.5 * (q(0, 1, 0) - q(0, -1, 0));
+    const double g2 = 0.5 * (q(0, 0, 1) - q(0, 0, -1));
+    double qmin = q(-1, -1, -1);
+    double qmax = qmin;
+#pragma unroll 1
+    for (int n = 0; n < 27; ++n) {
+        if (n == 13) continue;
+        const double v = q(n / 9 - 1, (n / 3) % 3 - 1, n % 3 - 1);
+        qmin = fx_bj_min(qmin, v);
+        qmax = fx_bj_max(qmax, v);
+    }
+    double alpha = 1.0;
+#pragma unroll
+    for (int s = 0; s < 8; ++s) {
+        const double o0 = (s & 4) ? 0.25 : -0.25;
+        const double o1 = (s & 2) ? 0.25 : -0.25;
+        const double o2 = (s & 1) ? 0.25 : -0.25;
+        const double delta = g0 * o0 + g1 * o1 + g2 * o2;
+        alpha = fx_bj_alpha(alpha, base, delta, qmin, qmax);
+    }
+    return base + alpha * (g0 * tx + g1 * ty + g2 * tz);
+}
+
+template <class Q>
+FX_HD double fx_bj_face(const Q &q, double t0, double t1)
+{
+    const double base = q(0, 0);
+    const double g0 = 0.5 * (q(1, 0) - q(-1, 0));
+    const double g1 = 0.5 * (q(0, 1) - q(0, -1));
+    double qmin = q(-1, -1);
+    double qmax = qmin;
+#pragma unroll
+    for (int n = 0; n < 9; ++n) {
+        if (n == 4) continue;
+        const double v = q(n / 3 - 1, n % 3 - 1);
+        qmin = fx_bj_min(qmin, v);
+        qmax = fx_bj_max(qmax, v);
+    }
+    double alpha = 1.0;
+#pragma unroll
+    for (int s = 0; s < 4; ++s) {
+        const double o0 = (s & 2) ? 0.25 : -0.25;
+        const double o1 = (s & 1) ? 0.25 : -0.25;
+        const double delta = g0 * o0 + g1 * o1;
+        alpha = fx_bj_alpha(alpha, base, delta, qmin, qmax);
+    }
+    return base + alpha * (g0 * t0 + g1 * t1);
+}
+
 /* prj_eos_prim2cons, src/prj_eos.c:2112-2151 */
 template <bool MHD>
 FX_HD void fx_prim2cons(const double *w, double *u)

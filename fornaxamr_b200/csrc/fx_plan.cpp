@@ -269,7 +269,7 @@ struct ProlongSig {
     int op;            /* the group that stored it */
     int64_t coarse_face;
     int target;
-    int ver[5];
+    int ver[9];        /* stencil versions: 5 (minmod cross) or 9 (Barth-Jespersen 3x3) */
 };
 
 class Compiler {
@@ -819,15 +819,26 @@ private:
                             const int cj = j / 2 + sl.send_loc_start[1];
                             const int ck = k / 2 + sl.send_loc_start[2];
                             op.src = FX_CELL_KEY(b, lidx(ci, cj, ck));
-                            op.type = FX_GOP_PROLONG;
+                            op.type = cfg_.use_bj ? FX_GOP_PROLONG_BJ : FX_GOP_PROLONG;
                             /* target offsets: (index % 2 == 0) ? -0.25 : +0.25 in C
                              * semantics (src/prj_boundary.c:318-320) */
                             op.aux = ((ai % 2 == 0) ? 0 : 4) | ((aj % 2 == 0) ? 0 : 2) | ((ak % 2 == 0) ? 0 : 1);
                             /* the 27-cell stencil is range checked
                              * (src/prj_boundary.c:60-72); the minmod limiter
-                             * reads the centre and its six axis neighbours */
+                             * reads the centre and its six axis neighbours,
+                             * Barth-Jespersen all 27 cells */
                             if (!cell_in_storage(ci - 1, cj - 1, ck - 1) || !cell_in_storage(ci + 1, cj + 1, ck + 1)) {
                                 return fail("prj_boundary_read_value: out-of-range access");
+                            }
+                            if (cfg_.use_bj) {
+                                int64_t r[27];
+                                int q = 0;
+                                for (int di = -1; di <= 1; ++di)
+                                    for (int dj = -1; dj <= 1; ++dj)
+                                        for (int dk = -1; dk <= 1; ++dk)
+                                            r[q++] = cell_elem(b, lidx(ci + di, cj + dj, ck + dk));
+                                add_multi(op, SPACE_CELL, r, 27, cell_elem(id, dc));
+                                continue;
                             }
                             const int64_t r[7] = {cell_elem(b, lidx(ci, cj, ck)),
                                 cell_elem(b, lidx(ci - 1, cj, ck)), cell_elem(b, lidx(ci + 1, cj, ck)),
@@ -1055,6 +1066,7 @@ private:
         p.coarse = coarse;
         p.pos = (f[0] + FX_NG) | ((f[1] + FX_NG) << 5) | ((f[2] + FX_NG) << 10) | ((c[0] + FX_NG) << 15) |
             ((c[1] + FX_NG) << 20) | ((c[2] + FX_NG) << 25);
+        p.flags = cfg_.use_bj ? 1 : 0;
         std::vector<int64_t> &reads = g_reads_;
         std::vector<int64_t> &writes = g_writes_;
         std::vector<std::pair<int64_t, ProlongSig>> &sigs = g_sigs_;
@@ -1066,16 +1078,21 @@ private:
             const int t0 = d == 0 ? 1 : 0;
             const int t1 = d == 2 ? 1 : 2;
             for (int side = 0; side < 2; ++side) {
-                /* the coarse face and its four tangential neighbours are the
-                 * stencil of all four outer faces of this side */
+                /* the coarse face and its four tangential neighbours (minmod),
+                 * or the 3x3 tangential block about it (Barth-Jespersen), are
+                 * the stencil of all four outer faces of this side */
                 int y[3] = {c[0], c[1], c[2]};
                 y[d] += side;
                 const int64_t cf = face_elem(coarse, d, fidx(d, y[0], y[1], y[2]));
-                int64_t ze[5];
-                int zv[5];
+                int64_t ze[9];
+                int zv[9];
                 bool stencil_read = false;
-                const int off[5][2] = {{0, 0}, {-1, 0}, {1, 0}, {0, -1}, {0, 1}};
-                for (int n = 0; n < 5; ++n) {
+                static const int cross[5][2] = {{0, 0}, {-1, 0}, {1, 0}, {0, -1}, {0, 1}};
+                static const int box[9][2] = {{-1, -1}, {-1, 0}, {-1, 1}, {0, -1}, {0, 0}, {0, 1},
+                    {1, -1}, {1, 0}, {1, 1}};
+                const int nst = cfg_.use_bj ? 9 : 5;
+                const int (*off)[2] = cfg_.use_bj ? box : cross;
+                for (int n = 0; n < nst; ++n) {
                     int z[3] = {y[0], y[1], y[2]};
                     z[t0] += off[n][0];
                     z[t1] += off[n][1];
@@ -1097,14 +1114,14 @@ private:
                             continue;
                         }
                         if (!stencil_read) {
-                            for (int n = 0; n < 5; ++n) reads.push_back(ze[n]);
+                            for (int n = 0; n < nst; ++n) reads.push_back(ze[n]);
                             stencil_read = true;
                         }
                         ProlongSig sg;
                         sg.op = op_index;
                         sg.coarse_face = cf;
                         sg.target = 2 * a + bb;
-                        for (int n = 0; n < 5; ++n) sg.ver[n] = zv[n];
+                        for (int n = 0; n < 9; ++n) sg.ver[n] = n < nst ? zv[n] : -2;
                         fid(fine, d, xf) = FID_COARSER;
                         const ProlongSig *prev = psig_.find((uint64_t)xe);
                         if (prev != nullptr && same_sig(*prev, sg) && ver_[xe] == prev->op) {
@@ -1145,7 +1162,7 @@ private:
     static bool same_sig(const ProlongSig &a, const ProlongSig &b)
     {
         if (a.coarse_face != b.coarse_face || a.target != b.target) return false;
-        for (int n = 0; n < 5; ++n) {
+        for (int n = 0; n < 9; ++n) {
             if (a.ver[n] != b.ver[n]) return false;
         }
         return true;

@@ -875,7 +875,7 @@ int amr_votes(fx_ctx *c, std::vector<int32_t> &votes)
 /* Toth-Roe groups that prolong a new child's faces from its parent: 8^3
  * coarse cells of the child's octant, outer faces kept where the child
  * copied a finer neighbour's layer, every face stored once */
-void child_groups(const FxAmrRefine &r, std::vector<FxPop> &out)
+void child_groups(const FxAmrRefine &r, bool use_bj, std::vector<FxPop> &out)
 {
     const int o[3] = {(r.oct & 1) * 8, ((r.oct >> 1) & 1) * 8, ((r.oct >> 2) & 1) * 8};
     for (int ci = o[0]; ci < o[0] + 8; ++ci) {
@@ -902,6 +902,7 @@ void child_groups(const FxAmrRefine &r, std::vector<FxPop> &out)
                     }
                 }
                 p.iwrite = 0xFFF;
+                p.flags = use_bj ? 1 : 0;
                 out.push_back(p);
             }
         }
@@ -988,6 +989,7 @@ int fx_create(int device, const fx_config *cfg, fx_ctx **out)
     c->D.red = c->d_red;
     c->D.ctl = c->d_ctl;
     c->D.recon = cfg->recon;
+    c->D.use_bj = cfg->use_bj != 0;
     {
         FxCtl v{};
         v.dt_mult = dt_mult(c);
@@ -2105,7 +2107,7 @@ int fx_amr_adapt(fx_ctx *c, int *changed)
                 cp.side = q % 2;
                 copies.push_back(cp);
             }
-            child_groups(r, pops);
+            child_groups(r, c->cfg.use_bj != 0, pops);
         }
     }
     std::vector<FxAmrParentJob> pjobs;

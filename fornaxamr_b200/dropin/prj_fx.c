@@ -190,6 +190,7 @@ static void prj_fx_create(const prj_mesh *mesh, const prj_bc *bc, prj_eos *eos)
     cfg.bc[4] = bc->bc_x3_inner;
     cfg.bc[5] = bc->bc_x3_outer;
     cfg.mhd_eta = mesh->mhd_eta;
+    cfg.use_bj = mesh->use_BJ != 0;
 #if PRJ_RECON_HYDRO == PRJ_RECON_WENO7
     cfg.recon = FX_RECON_WENO7;
 #elif PRJ_RECON_HYDRO == PRJ_RECON_WENO3

@@ -16,6 +16,8 @@
  *   PRJ_RECON_HYDRO -> fx_config.recon (MC, WENO-Z3, or WENO-Z7 in the
  *                      four-ghost-layer library)
  *   TIME_INTEGRATION -> fx_config.integrator (RK2 or eSSPRK10_4)
+ *   prj_mesh.use_BJ -> fx_config.use_bj (Barth-Jespersen instead of minmod
+ *                      in the coarse-to-fine prolongation of cells and faces)
  *   PRJ_NGHOST -> the library: libfornax_b200.so (2 layers, 20^3 block
  *                 arrays) or libfornax_b200_ng4.so (4 layers, 24^3);
  *                 fx_ghost_layers() reports which one is loaded
@@ -131,6 +133,11 @@ typedef struct fx_config {
     double mhd_eta;     /* prj_mesh.mhd_eta */
     int32_t recon;      /* FX_RECON_MC, FX_RECON_WENO3 or FX_RECON_WENO7 */
     int32_t integrator; /* FX_INT_RK2 or FX_INT_ESSPRK10_4 */
+    int32_t use_bj;     /* prj_mesh.use_BJ: 1 selects the Barth-Jespersen limiter of
+                         * prj_reconstruct_{cell,face}_for_prolongate_bj
+                         * (src/prj_reconstruct.h:145-313) in the ghost fill's and the
+                         * refinement's prolongation, 0 the minmod limiter */
+    int32_t pad;
 } fx_config;
 
 /* ---- context -------------------------------------------------------------- */
@@ -430,8 +437,8 @@ typedef struct fx_amr_config {
 
 /* Sets the refinement parameters and the refinement tree of the mirrored
  * mesh (the parent/children/can_refine of the last fx_set_mesh).  The
- * Barth-Jespersen prolongation limiter (use_BJ), the angular-resolution cap
- * and the Z4c estimator are not supported. */
+ * prolongation limiter is fx_config.use_bj; the angular-resolution cap and
+ * the Z4c estimator are not supported. */
 int fx_amr_configure(fx_ctx *ctx, const fx_amr_config *amr);
 /* prj_amr_tag (src/prj_amr.c:1581-1782) on the device state (W slot 0 after a
  * step or a fill): refine_flag[b] for every block entry (+1 refine, -1

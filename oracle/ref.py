@@ -188,6 +188,7 @@ class Reference:
         L.rh_weno3_face.restype = C.c_double
         L.rh_sim_dt.restype = C.c_double
         L.rh_set_mhd_eta.argtypes = [C.c_double]
+        L.rh_set_use_bj.argtypes = [C.c_int]
         if mhd:
             L.rh_hlld.argtypes = [dp, dp] + [C.c_double] * 5 + [dp]
             L.rh_emf_upwind.argtypes = [dp, dp, dp]
@@ -248,6 +249,11 @@ class Reference:
     def set_mhd_eta(self, eta: float) -> None:
         """Run-time resistivity (prj_mesh.mhd_eta)."""
         self.lib.rh_set_mhd_eta(eta)
+
+    def set_use_bj(self, on: bool) -> None:
+        """Barth-Jespersen prolongation limiter (prj_mesh.use_BJ); rh_setup
+        resets it to off."""
+        self.lib.rh_set_use_bj(1 if on else 0)
 
     def refill(self) -> None:
         """The driver's set-up refill (eos, ghost fill, eos) after stage-0

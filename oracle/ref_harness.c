@@ -935,6 +935,13 @@ void rh_set_mhd_eta(double eta)
     g_sim.mesh.mhd_eta = eta;
 }
 
+/* prj_mesh.use_BJ (the prolongation limiter of the ghost fill and of
+ * prj_amr_adapt); kept by rh_amr_configure, reset by rh_setup */
+void rh_set_use_bj(int on)
+{
+    g_sim.mesh.use_BJ = on != 0;
+}
+
 /* The driver's set-up refill (src/main.c:437-448) after the caller has
  * rewritten stage-0 cells or faces: eos of the active cells, ghost fill
  * with the cell field from the faces, eos of the whole mesh. */
@@ -1081,7 +1088,6 @@ void rh_amr_configure(const rh_amr *a)
     g_sim.mesh.min_dx = a->min_dx;
     g_sim.mesh.amr_reach_highest_level_at_density = a->reach_density;
     g_sim.mesh.E_floor = a->E_floor;
-    g_sim.mesh.use_BJ = 0;
     g_sim.mesh.use_amr_angular_resolution_limit = 0;
     g_sim.mesh.amr_init_refine_fn = 0;
     for (n = 0; n < PRJ_AMR_N; ++n) {

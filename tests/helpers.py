@@ -11,7 +11,7 @@ from fornaxamr_b200.layout import BS, NCELLS, NEDGES, NFACES, NG, PBS  # noqa: E
 CELL_BITS = 13 if NCELLS <= 8192 else 14
 CELL_MASK = (1 << CELL_BITS) - 1
 
-GOP_COPY, GOP_COPY_NEG, GOP_COPY_USER, GOP_RESTRICT, GOP_PROLONG = 0, 1, 2, 3, 4
+GOP_COPY, GOP_COPY_NEG, GOP_COPY_USER, GOP_RESTRICT, GOP_PROLONG, GOP_PROLONG_BJ = 0, 1, 2, 3, 4, 5
 FOP_COPY, FOP_RESTRICT, FOP_PROLONG = 8, 9, 10
 
 
@@ -120,6 +120,15 @@ def apply_cell_program(W, ops, waves, slot, nvg):
                 vy = base + minmod(q(-PBS), base, q(PBS)) * ty
                 vz = base + minmod(q(-1), base, q(1)) * tz
                 W[db[:, None], np.arange(nvg)[None, :], slot, dc[:, None]] = vx + vy + vz - 2.0 * base
+            elif t == GOP_PROLONG_BJ:
+                tx = np.where(s[:, 2] & 4, 0.25, -0.25)[:, None]
+                ty = np.where(s[:, 2] & 2, 0.25, -0.25)[:, None]
+                tz = np.where(s[:, 2] & 1, 0.25, -0.25)[:, None]
+
+                def q3(di, dj, dk):
+                    off = (di * PBS + dj) * PBS + dk
+                    return W[sb[:, None], np.arange(nvg)[None, :], slot, (sc + off)[:, None]]
+                W[db[:, None], np.arange(nvg)[None, :], slot, dc[:, None]] = bj_cell(q3, tx, ty, tz)
             elif t == GOP_RESTRICT:
                 acc = None
                 for off in (0, 1, PBS, PBS + 1, PBS * PBS, PBS * PBS + 1, PBS * PBS + PBS, PBS * PBS + PBS + 1):
@@ -157,6 +166,64 @@ def minmod(qm, q0, qp):
     return np.where(sl * sr <= 0.0, 0.0, np.where(np.abs(sl) < np.abs(sr), sl, sr))
 
 
+def _bj_alpha(alpha, base, delta, qmin, qmax):
+    """one sub-cell of the Barth-Jespersen alpha loop (src/prj_reconstruct.h:178-190)"""
+    q = base + delta
+    with np.errstate(divide="ignore", invalid="ignore"):
+        a_hi = np.where(delta != 0.0, (qmax - base) / np.where(delta != 0.0, delta, 1.0), 0.0)
+        a_lo = np.where(delta != 0.0, (qmin - base) / np.where(delta != 0.0, delta, 1.0), 0.0)
+    a = np.where(q > qmax, a_hi, a_lo)
+    a = np.where(a < 0.0, 0.0, np.where(a > 1.0, 1.0, a))
+    upd = np.where(alpha < a, alpha, a)
+    return np.where((q > qmax) | (q < qmin), upd, alpha)
+
+
+def bj_cell(q, tx, ty, tz):
+    """prj_reconstruct_cell_for_prolongate_bj (src/prj_reconstruct.h:145-195),
+    vectorised: q(di, dj, dk) returns the stencil values at that offset."""
+    base = q(0, 0, 0)
+    g0 = 0.5 * (q(1, 0, 0) - q(-1, 0, 0))
+    g1 = 0.5 * (q(0, 1, 0) - q(0, -1, 0))
+    g2 = 0.5 * (q(0, 0, 1) - q(0, 0, -1))
+    qmin = q(-1, -1, -1)
+    qmax = qmin
+    for di in (-1, 0, 1):
+        for dj in (-1, 0, 1):
+            for dk in (-1, 0, 1):
+                if di == 0 and dj == 0 and dk == 0:
+                    continue
+                v = q(di, dj, dk)
+                qmin = np.where(qmin < v, qmin, v)
+                qmax = np.where(qmax > v, qmax, v)
+    alpha = np.ones_like(base)
+    for o0 in (-0.25, 0.25):
+        for o1 in (-0.25, 0.25):
+            for o2 in (-0.25, 0.25):
+                alpha = _bj_alpha(alpha, base, g0 * o0 + g1 * o1 + g2 * o2, qmin, qmax)
+    return base + alpha * (g0 * tx + g1 * ty + g2 * tz)
+
+
+def bj_face(q, t0, t1):
+    """prj_reconstruct_face_for_prolongate_bj (src/prj_reconstruct.h:248-290)."""
+    base = q(0, 0)
+    g0 = 0.5 * (q(1, 0) - q(-1, 0))
+    g1 = 0.5 * (q(0, 1) - q(0, -1))
+    qmin = q(-1, -1)
+    qmax = qmin
+    for di in (-1, 0, 1):
+        for dj in (-1, 0, 1):
+            if di == 0 and dj == 0:
+                continue
+            v = q(di, dj)
+            qmin = np.where(qmin < v, qmin, v)
+            qmax = np.where(qmax > v, qmax, v)
+    alpha = np.ones_like(base)
+    for o0 in (-0.25, 0.25):
+        for o1 in (-0.25, 0.25):
+            alpha = _bj_alpha(alpha, base, g0 * o0 + g1 * o1, qmin, qmax)
+    return base + alpha * (g0 * t0 + g1 * t1)
+
+
 def face_stride(d, a):
     u = [0, 0, 0]
     u[a] = 1
@@ -170,6 +237,7 @@ def apply_prolong_groups(Bf, pops, slot, dx):
         return
     fine, coarse, pos = pops[:, 0], pops[:, 1], pops[:, 2].astype(np.int64)
     keep, ow, iw = pops[:, 3].astype(np.int64), pops[:, 4].astype(np.int64), pops[:, 5].astype(np.int64)
+    bj = (pops[:, 6] & 1).astype(bool)
     f0 = [(pos >> (5 * a)) & 31 for a in range(3)]
     f0 = [x - NG for x in f0]
     c0 = [((pos >> (15 + 5 * a)) & 31) - NG for a in range(3)]
@@ -197,7 +265,12 @@ def apply_prolong_groups(Bf, pops, slot, dx):
                     base = Bf[coarse, d, slot, cf]
                     vx = base + minmod(Bf[coarse, d, slot, cf - s0], base, Bf[coarse, d, slot, cf + s0]) * (0.25 if a else -0.25)
                     vy = base + minmod(Bf[coarse, d, slot, cf - s1], base, Bf[coarse, d, slot, cf + s1]) * (0.25 if b else -0.25)
-                    flux = (vx + vy - base) * area[d]
+                    value = vx + vy - base
+                    if bj.any():
+                        vb = bj_face(lambda d0, d1: Bf[coarse, d, slot, cf + d0 * s0 + d1 * s1],
+                                     0.25 if a else -0.25, 0.25 if b else -0.25)
+                        value = np.where(bj, vb, value)
+                    flux = value * area[d]
                     o[d, side, a, b] = np.where(kept, Bf[fine, d, slot, xf] * area[d], flux)
                     m = (~kept) & ((ow >> q) & 1).astype(bool)
                     writes.append((d, fine[m], xf[m], flux[m] / area[d][m]))

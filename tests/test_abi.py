@@ -34,7 +34,7 @@ def test_struct_layout_matches_header():
     from fornaxamr_b200._lib import FxBlockDesc, FxConfig, FxSlot
     assert ctypes.sizeof(FxSlot) == 24
     assert ctypes.sizeof(FxBlockDesc) == 16 + 13 * 8 + 56 * 24 + 10 * 4
-    assert ctypes.sizeof(FxConfig) == 8 + 8 + 48 + 24 + 8 + 8
+    assert ctypes.sizeof(FxConfig) == 8 + 8 + 48 + 24 + 8 + 8 + 8
     from fornaxamr_b200._lib import FxAmrConfig, FxAmrCriterion
     assert ctypes.sizeof(FxAmrCriterion) == 16 + 24
     assert ctypes.sizeof(FxAmrConfig) == 24 + 24 + 4 * 40

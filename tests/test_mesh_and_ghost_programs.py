@@ -12,11 +12,11 @@ from oracle import ref as R
 from tests import helpers as H
 
 
-def _desc_and_cfg(ref, p, mhd):
+def _desc_and_cfg(ref, p, mhd, use_bj=False):
     import fornaxamr_b200 as fx
     desc = H.ref_desc(ref)
     coord = [p.xmin[0], p.xmax[0], p.xmin[1], p.xmax[1], p.xmin[2], p.xmax[2]]
-    return desc, fx.make_config(mhd, p.gamma, coord, bc=tuple(p.bc))
+    return desc, fx.make_config(mhd, p.gamma, coord, bc=tuple(p.bc), use_bj=use_bj)
 
 
 @pytest.mark.parametrize("root", [(2, 2, 2), (3, 2, 1), (1, 1, 1)])
@@ -35,10 +35,10 @@ def test_uniform_mesh_matches_reference(ref_mhd, root):
     assert np.array_equal(ms, slots)
 
 
-def _scrambled_fill_check(ref, p, mhd, seed):
-    import fornaxamr_b200 as fx
+def _scrambled_fill_check(ref, p, mhd, seed, use_bj=False):
     ref.setup(p)
-    desc, cfg = _desc_and_cfg(ref, p, mhd)
+    ref.set_use_bj(use_bj)
+    desc, cfg = _desc_and_cfg(ref, p, mhd, use_bj)
     W, Bf = H.ref_state(ref)
     nb = W.shape[0]
     rng = np.random.default_rng(seed)
@@ -55,6 +55,7 @@ def _scrambled_fill_check(ref, p, mhd, seed):
                 ref.set_Bf(b, d, Bf[b, d].ravel())
     ref.fill_ghosts(1, 0)
     W_ref, Bf_ref = H.ref_state(ref)
+    ref.set_use_bj(False)
 
     Wm = W.copy()
     Bm = Bf.copy() if mhd else None
@@ -139,6 +140,27 @@ def test_amr_ghost_program_matches_reference(ref_mhd, root, radii):
 def test_amr_hydro_ghost_program_matches_reference(ref_hydro):
     p = R.params_amr_blast(root=2, radii=(0.3, 0.1))
     _scrambled_fill_check(ref_hydro, p, False, seed=11)
+
+
+@pytest.mark.parametrize("root,radii", AMR_CASES)
+def test_amr_ghost_program_with_barth_jespersen_matches_reference(ref_mhd, root, radii):
+    """use_BJ = 1: the cell prolongations read all 27 coarse cells and the
+    outer faces of the Toth-Roe groups the 3x3 tangential face stencil
+    (src/prj_reconstruct.h:145-195, 248-290)."""
+    import fornaxamr_b200 as fx
+    p = R.params_amr_blast(root=root, radii=radii)
+    nw = _scrambled_fill_check(ref_mhd, p, True, seed=root + 5, use_bj=True)
+    assert nw >= 2
+    desc, cfg = _desc_and_cfg(ref_mhd, p, True, use_bj=True)
+    cops, _ = fx.plan_export(cfg, desc, 0)
+    pops, _ = fx.plan_export(cfg, desc, 6)
+    assert (cops[:, 3] == H.GOP_PROLONG_BJ).sum() > 0 and (cops[:, 3] == H.GOP_PROLONG).sum() == 0
+    assert len(pops) > 0 and np.all(pops[:, 6] & 1)
+
+
+def test_amr_hydro_ghost_program_with_barth_jespersen_matches_reference(ref_hydro):
+    p = R.params_amr_blast(root=2, radii=(0.3, 0.1))
+    _scrambled_fill_check(ref_hydro, p, False, seed=13, use_bj=True)
 
 
 @pytest.mark.parametrize("root,radii", AMR_CASES)

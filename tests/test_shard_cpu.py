@@ -23,13 +23,13 @@ from tests import helpers as H
 COORD = (-0.7, 0.7, -0.7, 0.7, -0.7, 0.7)
 
 
-def build(levels, mhd):
+def build(levels, mhd, use_bj=False):
     if levels == 0:
         blocks = mesh.uniform_mesh((2, 2, 2), COORD)
     else:
         blocks = mesh.static_amr_mesh((2, 2, 2), COORD, levels,
                                       mesh.ball_refiner((0.1, 0.05, 0.0), (0.4, 0.2)[:levels]))
-    return fx.make_config(mhd, 5.0 / 3.0, COORD), mesh.to_desc(blocks)
+    return fx.make_config(mhd, 5.0 / 3.0, COORD, use_bj=use_bj), mesh.to_desc(blocks)
 
 
 def morton_owner(desc, nranks):
@@ -96,9 +96,12 @@ class Part:
         return ok
 
 
-@pytest.mark.parametrize("levels,mhd,nranks", [(0, True, 2), (1, True, 3), (1, False, 4), (2, True, 3)])
-def test_rank_parts_reproduce_the_single_device_fill(levels, mhd, nranks):
-    cfg, desc = build(levels, mhd)
+@pytest.mark.parametrize("levels,mhd,nranks,use_bj", [(0, True, 2, False), (1, True, 3, False), (1, False, 4, False),
+                                                     (2, True, 3, False), (2, True, 3, True), (1, False, 4, True)])
+def test_rank_parts_reproduce_the_single_device_fill(levels, mhd, nranks, use_bj):
+    """use_bj: the Barth-Jespersen prolongations read the coarse cells' edge
+    and corner neighbours too, so the halo exchange must carry them."""
+    cfg, desc = build(levels, mhd, use_bj)
     owner = morton_owner(desc, nranks)
     W0, Bf0 = seeded_state(len(desc), mhd)
     slot = 1
