@@ -31,6 +31,7 @@ import os
 import statistics
 import subprocess
 import sys
+import threading
 import time
 
 HERE = os.path.dirname(os.path.abspath(__file__))
@@ -193,15 +194,58 @@ def cpu_reference(steps: int, warmup: int, seconds: float, kind: str = "fourier"
 # ---------------------------------------------------------------------------
 
 class Clocks:
+    """SM clock and clock-event reasons of the benchmark's GPU while the timed
+    region runs.  NVML (read-only queries) is polled every 2 ms on a thread,
+    so even a 50 ms timed region gets a few dozen samples; `mark()` brackets
+    the timed region and only samples inside it count.  Without NVML the
+    recipe's nvidia-smi line (-lms 200) is used instead."""
     QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    REASONS = {0x8: "hw_slowdown", 0x40: "hw_thermal_slowdown", 0x20: "sw_thermal_slowdown",
+               0x4: "sw_power_cap", 0x80: "hw_power_brake_slowdown"}
 
     def __init__(self, device: int):
         self.device = device
         self.proc = None
+        self.nvml = None
+        self.samples = []          # (time, sm MHz, reason bits)
+        self.window = None
+        self.smax = None
+        self.lines = []
+
+    def _handle(self):
+        import pynvml
+        pynvml.nvmlInit()
+        try:
+            import torch
+            uuid = str(torch.cuda.get_device_properties(self.device).uuid)
+            return pynvml, pynvml.nvmlDeviceGetHandleByUUID(uuid if uuid.startswith("GPU-") else "GPU-" + uuid)
+        except Exception:
+            return pynvml, pynvml.nvmlDeviceGetHandleByIndex(self.device)
+
+    def _poll(self):
+        nv, h = self.nvml
+        while not self.stop:
+            try:
+                sm = nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)
+                bits = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+                self.samples.append((time.perf_counter(), float(sm), int(bits)))
+            except Exception:
+                return
+            time.sleep(0.002)
 
     def __enter__(self):
+        try:
+            self.nvml = self._handle()
+            nv, h = self.nvml
+            self.smax = float(nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM))
+            self.stop = False
+            self.thread = threading.Thread(target=self._poll, daemon=True)
+            self.thread.start()
+            return self
+        except Exception:
+            self.nvml = None
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits", "-lms", "200",
@@ -210,8 +254,19 @@ class Clocks:
             self.proc = None
         return self
 
+    def mark(self, t0, t1):
+        """host times bracketing the timed region"""
+        self.window = (t0, t1)
+
     def __exit__(self, *exc):
-        self.lines = []
+        if self.nvml is not None:
+            self.stop = True
+            self.thread.join(timeout=1.0)
+            try:
+                self.nvml[0].nvmlShutdown()
+            except Exception:
+                pass
+            return
         if self.proc is not None:
             time.sleep(0.3)
             self.proc.terminate()
@@ -223,6 +278,14 @@ class Clocks:
             self.lines = [l for l in out.splitlines() if l.strip()]
 
     def summary(self):
+        if self.nvml is not None:
+            sel = [x for x in self.samples if self.window is None or self.window[0] <= x[0] <= self.window[1]]
+            if not sel:
+                return {"sm_mhz": None, "sm_max_mhz": self.smax, "reasons": [], "samples": 0, "source": "nvml"}
+            reasons = sorted({n for _, _, b in sel for bit, n in self.REASONS.items() if b & bit})
+            return {"sm_mhz": statistics.median(x[1] for x in sel), "sm_max_mhz": self.smax,
+                    "sm_min_mhz": min(x[1] for x in sel), "reasons": reasons, "samples": len(sel),
+                    "source": "nvml, 2 ms polling inside the timed region"}
         sm, smax, reasons = [], None, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         for l in self.lines:
@@ -238,9 +301,9 @@ class Clocks:
                 if v.lower().startswith("active"):
                     reasons.add(n)
         if not sm:
-            return {"sm_mhz": None, "sm_max_mhz": smax, "reasons": [], "samples": 0}
+            return {"sm_mhz": None, "sm_max_mhz": smax, "reasons": [], "samples": 0, "source": "nvidia-smi"}
         return {"sm_mhz": statistics.median(sm), "sm_max_mhz": smax, "reasons": sorted(reasons),
-                "samples": len(sm)}
+                "samples": len(sm), "source": "nvidia-smi -lms 200"}
 
 
 # ---------------------------------------------------------------------------
@@ -589,11 +652,13 @@ def run_shard(args, rank, world, local_rank):
     e1 = torch.cuda.Event(enable_timing=True)
     with Clocks(dev) as clk:
         torch.cuda.synchronize(dev)
+        h0 = time.perf_counter()
         e0.record(stream)
         state = ctx.run(fx.FORM_BATCHED, args.steps, cfl, dt_factor, t_end, state)
         e1.record(stream)
         e1.synchronize()
         torch.cuda.synchronize(dev)
+        clk.mark(h0, time.perf_counter())
     if world > 1:
         torch.distributed.barrier()
     ms_total = max_over_ranks(e0.elapsed_time(e1))
@@ -660,11 +725,13 @@ def run_fx(args, rank, world, local_rank):
     e1 = torch.cuda.Event(enable_timing=True)
     with Clocks(dev) as clk:
         torch.cuda.synchronize(dev)
+        h0 = time.perf_counter()
         e0.record(stream)
         state = ctx.run(fx.FORM_BATCHED, args.steps, cfl, dt_factor, t_end, state)
         e1.record(stream)
         e1.synchronize()
         torch.cuda.synchronize(dev)
+        clk.mark(h0, time.perf_counter())
     barrier()
     ms_total = max_over_ranks(e0.elapsed_time(e1))
     ms_step = ms_total / args.steps
