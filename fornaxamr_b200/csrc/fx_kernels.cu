@@ -975,31 +975,48 @@ __device__ __forceinline__ void fx_ghost_cell_op(const FxDev &D, const FxGop op,
     const int sc = FX_CELL_IDX(op.src);
     double *Wd = D.W + (size_t)db * FX_W_COUNT(D.nv) + (size_t)wslot * FX_NCELLS;
     const double *Ws = D.W + (size_t)sb * FX_W_COUNT(D.nv) + (size_t)wslot * FX_NCELLS;
+    if constexpr (BJ) {
+        if (op.type == FX_GOP_PROLONG_BJ) {
+            const double tx = (op.aux & 4) ? 0.25 : -0.25;
+            const double ty = (op.aux & 2) ? 0.25 : -0.25;
+            const double tz = (op.aux & 1) ? 0.25 : -0.25;
+#pragma unroll 1
+            for (int v = 0; v < nvg; ++v) {
+                const double *q = Ws + (size_t)v * kPlane + sc;
+                Wd[(size_t)v * kPlane + dc] = fx_bj_cell(
+                    [q](int di, int dj, int dk) { return q[(di * FX_PBS + dj) * FX_PBS + dk]; }, tx, ty, tz);
+            }
+            return;
+        }
+    }
+    /* every variable's value first, then the stores: the loads of all
+     * variables are in flight together (the wave's operations are conflict
+     * free, so no store of the wave feeds a load of it) */
+    double val[FX_MAXVAR];
     switch (op.type) {
     case FX_GOP_COPY:
-        for (int v = 0; v < nvg; ++v) {
-            Wd[(size_t)v * kPlane + dc] = Ws[(size_t)v * kPlane + sc];
-        }
-        break;
     case FX_GOP_COPY_NEG:
-        for (int v = 0; v < nvg; ++v) {
-            Wd[(size_t)v * kPlane + dc] = Ws[(size_t)v * kPlane + sc];
-        }
-        Wd[(size_t)op.aux * kPlane + dc] = -Ws[(size_t)op.aux * kPlane + sc];
-        break;
     case FX_GOP_COPY_USER:
-        for (int v = 0; v < nvg; ++v) {
-            Wd[(size_t)v * kPlane + dc] = Ws[(size_t)v * kPlane + sc];
+#pragma unroll
+        for (int v = 0; v < FX_MAXVAR; ++v) {
+            if (v < nvg) val[v] = Ws[(size_t)v * kPlane + sc];
         }
-        if (op.aux) {
-            Wd[(size_t)FX_V1 * kPlane + dc] = 5.0;
+        if (op.type == FX_GOP_COPY_NEG) {
+#pragma unroll
+            for (int v = 0; v < FX_MAXVAR; ++v) {
+                if (v == op.aux) val[v] = -val[v];
+            }
+        } else if (op.type == FX_GOP_COPY_USER && op.aux) {
+            val[FX_V1] = 5.0;
         }
         break;
     case FX_GOP_RESTRICT:
-        for (int v = 0; v < nvg; ++v) {
+#pragma unroll
+        for (int v = 0; v < FX_MAXVAR; ++v) {
+            if (v >= nvg) continue;
             const double *q = Ws + (size_t)v * kPlane + sc;
             /* order of src/prj_boundary.c:238-261 */
-            Wd[(size_t)v * kPlane + dc] = 0.125 *
+            val[v] = 0.125 *
                 (q[0] + q[1] + q[FX_PBS] + q[FX_PBS + 1] +
                  q[FX_PBS * FX_PBS] + q[FX_PBS * FX_PBS + 1] +
                  q[FX_PBS * FX_PBS + FX_PBS] + q[FX_PBS * FX_PBS + FX_PBS + 1]);
@@ -1010,35 +1027,29 @@ __device__ __forceinline__ void fx_ghost_cell_op(const FxDev &D, const FxGop op,
         const double tx = (op.aux & 4) ? 0.25 : -0.25;
         const double ty = (op.aux & 2) ? 0.25 : -0.25;
         const double tz = (op.aux & 1) ? 0.25 : -0.25;
-        for (int v = 0; v < nvg; ++v) {
-            Wd[(size_t)v * kPlane + dc] = fx_prolong_cell(Ws + (size_t)v * kPlane, sc, tx, ty, tz);
-        }
-        break;
-    }
-    case FX_GOP_PROLONG_BJ: {
-        if constexpr (!BJ) {
-            break;
-        }
-        const double tx = (op.aux & 4) ? 0.25 : -0.25;
-        const double ty = (op.aux & 2) ? 0.25 : -0.25;
-        const double tz = (op.aux & 1) ? 0.25 : -0.25;
-#pragma unroll 1
-        for (int v = 0; v < nvg; ++v) {
-            const double *q = Ws + (size_t)v * kPlane + sc;
-            Wd[(size_t)v * kPlane + dc] = fx_bj_cell(
-                [q](int di, int dj, int dk) { return q[(di * FX_PBS + dj) * FX_PBS + dk]; }, tx, ty, tz);
+#pragma unroll
+        for (int v = 0; v < FX_MAXVAR; ++v) {
+            if (v < nvg) val[v] = fx_prolong_cell(Ws + (size_t)v * kPlane, sc, tx, ty, tz);
         }
         break;
     }
     default:
-        break;
+        return;
+    }
+#pragma unroll
+    for (int v = 0; v < FX_MAXVAR; ++v) {
+        if (v < nvg) Wd[(size_t)v * kPlane + dc] = val[v];
     }
 }
 
 __device__ __forceinline__ int fx_face_key_block(int key) { return key >> 15; }
 __device__ __forceinline__ int fx_face_key_idx(int key) { return key & 32767; }
 
-__device__ __forceinline__ void fx_ghost_face_op(const FxDev &D, const FxGop op, int bfslot)
+/* the value of one face operation (its loads) and where it goes; the store
+ * is left to the caller, so that a thread can issue the loads of several
+ * operations before their stores (the operations of a wave are conflict
+ * free).  Null for an unknown type. */
+__device__ __forceinline__ double *fx_ghost_face_value(const FxDev &D, const FxGop op, int bfslot, double &v)
 {
     const int dir = op.aux & 3;
     const int db = fx_face_key_block(op.dst);
@@ -1048,14 +1059,23 @@ __device__ __forceinline__ void fx_ghost_face_op(const FxDev &D, const FxGop op,
     double *Bd = D.Bf + (size_t)db * FX_BF_COUNT + ((size_t)dir * FX_NSTAGES + bfslot) * FX_NFACES;
     const double *Bs = D.Bf + (size_t)sb * FX_BF_COUNT + ((size_t)dir * FX_NSTAGES + bfslot) * FX_NFACES;
     if (op.type == FX_FOP_COPY) {
-        Bd[df] = Bs[sf];
-    } else if (op.type == FX_FOP_RESTRICT) {
+        v = Bs[sf];
+        return Bd + df;
+    }
+    if (op.type == FX_FOP_RESTRICT) {
         /* 0.25*(s0 + s0+t1 + s0+t0 + s0+t0+t1), src/prj_boundary.c:738-764 */
         const int o1 = (op.aux >> 2) & 1023;   /* stride of tan1 */
         const int o0 = (op.aux >> 12) & 1023;  /* stride of tan0 */
-        Bd[df] = 0.25 * (Bs[sf] + Bs[sf + o1] + Bs[sf + o0] + Bs[sf + o0 + o1]);
+        v = 0.25 * (Bs[sf] + Bs[sf + o1] + Bs[sf + o0] + Bs[sf + o0 + o1]);
+        return Bd + df;
     }
+    return nullptr;
 }
+
+/* face operations per thread of the wave kernel: a face copy moves one
+ * double, so one operation per thread leaves too few loads in flight to
+ * keep HBM busy */
+constexpr int FX_GW_FACE_OPS = 4;
 
 /* face-index offset of a unit step along axis a for faces of direction d */
 __device__ __forceinline__ int fx_face_stride(int d, int a)
@@ -1227,16 +1247,19 @@ __global__ void __launch_bounds__(128) k_ghost_groups(FxDev D, const FxPop *__re
 }
 
 /* one conflict-free wave of the ghost fill: CTAs [0, nbc) run cell ops,
- * then face ops and cell-field ops */
+ * then face ops (FX_GW_FACE_OPS per thread) and cell-field ops.  At 6 CTAs
+ * of 256 per SM the kernel keeps 40 registers without spills; on the 512-block
+ * uniform fill this took 0.165 ms down to 0.148 ms. */
 template <bool BJ>
-__global__ void __launch_bounds__(256) k_ghost_wave(FxDev D, const FxGop *__restrict__ cops, int nc,
+__global__ void __launch_bounds__(256, 6) k_ghost_wave(FxDev D, const FxGop *__restrict__ cops, int nc,
     const FxGop *__restrict__ fops, int nf, const FxBop *__restrict__ bops, int nb, int slot, int nvg)
 {
     if (D.ctl->skip) {
         return;
     }
+    constexpr int UF = FX_GW_FACE_OPS;
     const int nbc = (nc + 255) / 256;
-    const int nbf = (nf + 255) / 256;
+    const int nbf = (nf + 256 * UF - 1) / (256 * UF);
     int blk = blockIdx.x;
     if (blk < nbc) {
         const int t = blk * 256 + threadIdx.x;
@@ -1245,8 +1268,19 @@ __global__ void __launch_bounds__(256) k_ghost_wave(FxDev D, const FxGop *__rest
     }
     blk -= nbc;
     if (blk < nbf) {
-        const int t = blk * 256 + threadIdx.x;
-        if (t < nf) fx_ghost_face_op(D, fops[t], slot);
+        /* operations t0 + 256 u, u < UF: every load first, then the stores */
+        const int t0 = blk * 256 * UF + threadIdx.x;
+        double v[UF];
+        double *dst[UF];
+#pragma unroll
+        for (int u = 0; u < UF; ++u) {
+            const int t = t0 + 256 * u;
+            dst[u] = t < nf ? fx_ghost_face_value(D, fops[t], slot, v[u]) : nullptr;
+        }
+#pragma unroll
+        for (int u = 0; u < UF; ++u) {
+            if (dst[u]) *dst[u] = v[u];
+        }
         return;
     }
     blk -= nbf;
@@ -1667,7 +1701,7 @@ void fx_launch_ghost_wave(const FxDev &D, const FxGop *cops, int nc, const FxGop
 {
     /* the operations of a wave are conflict free: the two launches may run
      * in either order */
-    const unsigned grid = fx_blocks(nc, 256) + fx_blocks(nf, 256) + fx_blocks(nb, 256);
+    const unsigned grid = fx_blocks(nc, 256) + fx_blocks(nf, 256 * FX_GW_FACE_OPS) + fx_blocks(nb, 256);
     if (grid > 0) {
         if (D.use_bj) {
             k_ghost_wave<true><<<grid, 256, 0, s>>>(D, cops, nc, fops, nf, bops, nb, slot, nvg);
