@@ -112,6 +112,23 @@ __global__ void __launch_bounds__(TPB, MINB) k_flux(FxDev D, const int *__restri
     if (D.ctl->skip) {
         return;
     }
+    /* gamma is uniform for the ideal gas: its MC slope is exactly 0, so the
+     * MC face values equal g bit for bit; the WENO weights of a constant
+     * stencil are evaluated as the reference does (their sum need not be 1).
+     * Those face values depend on g alone, so one thread of the CTA
+     * evaluates them for all (before any thread leaves). */
+    __shared__ double s_gface[2];
+    if constexpr (RECON != FX_RECON_MC) {
+        if (threadIdx.x == 0) {
+            double gS[FxStencil<RECON>::NS];
+#pragma unroll
+            for (int n = 0; n < FxStencil<RECON>::NS; ++n) {
+                gS[n] = D.gamma;
+            }
+            fx_recon_pair<RECON>(gS, s_gface[0], s_gface[1]);
+        }
+        __syncthreads();
+    }
     /* grid (face chunk, direction, block): the three sweeps of a block are
      * scheduled back to back, so its stencil cells are re-read from L2 */
     const int dir = blockIdx.y;
@@ -195,17 +212,10 @@ __global__ void __launch_bounds__(TPB, MINB) k_flux(FxDev D, const int *__restri
         /* the pressure takes the normal field's (unreconstructed) bits */
         fx_recon_pair_br(pS, pL, pR, br, 4 * FX_B1);
     }
-    /* gamma is uniform for the ideal gas: its MC slope is exactly 0, so the
-     * MC face values equal g bit for bit; the WENO weights of a constant
-     * stencil are evaluated as the reference does (their sum need not be 1) */
     double gL = g, gR = g;
-    if (RECON != FX_RECON_MC) {
-        double gS[NS];
-#pragma unroll
-        for (int n = 0; n < NS; ++n) {
-            gS[n] = g;
-        }
-        fx_recon_pair<RECON>(gS, gL, gR);
+    if constexpr (RECON != FX_RECON_MC) {
+        gL = s_gface[0];
+        gR = s_gface[1];
     }
     const size_t fbase = (size_t)b * FX_FLUX_COUNT(nv) + (size_t)dir * nv * FX_NCELLS;
     const size_t vbase = (size_t)b * FX_VR_COUNT + (size_t)dir * 3 * FX_NCELLS;
