@@ -163,7 +163,11 @@ __global__ void __launch_bounds__(TPB, MINB) k_flux(FxDev D, const int *__restri
     double WL[9];
     double WR[9];
     /* density and internal energy at the stencil cells also give the
-     * reconstructed pressure (eosvar p = (g-1) rho e of each cell). */
+     * reconstructed pressure (eosvar p = (g-1) rho e of each cell).  The
+     * stencil comes through the read-only data path: this launch does not
+     * write W (on the 128^3 state 0.628 -> 0.623 ms at 64 x 8, 0.699 ->
+     * 0.665 ms at 256 x 3; the normal field that way, and the EMF, CT,
+     * fill and cell kernels, measured no faster). */
     constexpr int NS = FxStencil<RECON>::NS;
     const int c0 = cL - (NS / 2 - 1) * s;   /* first stencil cell */
     double rhoS[NS], eintS[NS];
@@ -172,8 +176,8 @@ __global__ void __launch_bounds__(TPB, MINB) k_flux(FxDev D, const int *__restri
         const double *qe = Wb + (size_t)FX_EINT * kPlane + c0;
 #pragma unroll
         for (int n = 0; n < NS; ++n) {
-            rhoS[n] = qr[n * s];
-            eintS[n] = qe[n * s];
+            rhoS[n] = __ldg(qr + n * s);
+            eintS[n] = __ldg(qe + n * s);
         }
     }
     if constexpr (BRM == 0) {
@@ -192,7 +196,7 @@ __global__ void __launch_bounds__(TPB, MINB) k_flux(FxDev D, const int *__restri
         double qs[NS];
 #pragma unroll
         for (int n = 0; n < NS; ++n) {
-            qs[n] = q[n * s];
+            qs[n] = __ldg(q + n * s);
         }
         if constexpr (BRM == 0) {
             fx_recon_pair<RECON>(qs, WL[lv], WR[lv]);
