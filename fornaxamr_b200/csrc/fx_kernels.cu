@@ -98,6 +98,18 @@ __device__ __forceinline__ void fx_recon_pair_br(const double (&q)[4], double &w
     wr = q[2] - 0.5 * fx_mc_slope_br(q[1], q[2], q[3], br, q4 + 2);
 }
 
+/* a stencil value of the face kernel: through the read-only data path for
+ * the 4-cell stencils (MC, WENO-Z3), a plain load for WENO-Z7's 8 cells */
+template <int RECON>
+__device__ __forceinline__ double fx_stencil_load(const double *p)
+{
+    if constexpr (RECON == FX_RECON_WENO7) {
+        return *p;
+    } else {
+        return __ldg(p);
+    }
+}
+
 /* BRM: 0 the solver as it stands; 1 record / 2 replay every face's
  * decisions in D.br_words (FxBrRecord / FxBrReplay; MHD, MC and the plain
  * form only), the branch-frozen map the adjoint checks use */
@@ -164,10 +176,12 @@ __global__ void __launch_bounds__(TPB, MINB) k_flux(FxDev D, const int *__restri
     double WR[9];
     /* density and internal energy at the stencil cells also give the
      * reconstructed pressure (eosvar p = (g-1) rho e of each cell).  The
-     * stencil comes through the read-only data path: this launch does not
-     * write W (on the 128^3 state 0.628 -> 0.623 ms at 64 x 8, 0.699 ->
-     * 0.665 ms at 256 x 3; the normal field that way, and the EMF, CT,
-     * fill and cell kernels, measured no faster). */
+     * MC and WENO-Z3 stencils come through the read-only data path
+     * (fx_stencil_load): this launch does not write W (on the 128^3 state
+     * 0.628 -> 0.623 ms at 64 x 8, 0.699 -> 0.665 ms at 256 x 3; the normal
+     * field that way, and the EMF, CT, fill and cell kernels, measured no
+     * faster; WENO-Z7's 8-cell stencils 4.60 ms with plain loads against
+     * 4.75 ms). */
     constexpr int NS = FxStencil<RECON>::NS;
     const int c0 = cL - (NS / 2 - 1) * s;   /* first stencil cell */
     double rhoS[NS], eintS[NS];
@@ -176,8 +190,8 @@ __global__ void __launch_bounds__(TPB, MINB) k_flux(FxDev D, const int *__restri
         const double *qe = Wb + (size_t)FX_EINT * kPlane + c0;
 #pragma unroll
         for (int n = 0; n < NS; ++n) {
-            rhoS[n] = __ldg(qr + n * s);
-            eintS[n] = __ldg(qe + n * s);
+            rhoS[n] = fx_stencil_load<RECON>(qr + n * s);
+            eintS[n] = fx_stencil_load<RECON>(qe + n * s);
         }
     }
     if constexpr (BRM == 0) {
@@ -196,7 +210,7 @@ __global__ void __launch_bounds__(TPB, MINB) k_flux(FxDev D, const int *__restri
         double qs[NS];
 #pragma unroll
         for (int n = 0; n < NS; ++n) {
-            qs[n] = __ldg(q + n * s);
+            qs[n] = fx_stencil_load<RECON>(q + n * s);
         }
         if constexpr (BRM == 0) {
             fx_recon_pair<RECON>(qs, WL[lv], WR[lv]);
