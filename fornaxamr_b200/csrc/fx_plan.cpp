@@ -39,6 +39,7 @@
 #include <array>
 #include <cmath>
 #include <cstdint>
+#include <cstdlib>
 #include <cstring>
 #include <memory>
 #include <thread>
@@ -210,57 +211,46 @@ struct Rec {
     long long rewired = 0;
 };
 
-/* open-addressing map from a face element to the signature of the value
- * a face-prolongation group stored there (linear probing, grows at half
- * load; keys are element ids, never ~0) */
+/* map from a face element (ids in [base, base + n)) to the signature of the
+ * value a face-prolongation group stored there: a direct index per element
+ * into the list of signatures.  The index array comes from calloc, so only
+ * the pages of elements that groups write are ever touched (a 2864-block
+ * mesh has 72 M face elements, of which about 1.5 M get a signature). */
 template <typename V>
-class ElemMap {
+class FaceIndexMap {
 public:
-    V *find(uint64_t key)
+    void init(int64_t base, int64_t n)
     {
-        if (keys_.empty()) return nullptr;
-        for (size_t i = slot(key);; i = (i + 1) & (keys_.size() - 1)) {
-            if (keys_[i] == key) return &vals_[i];
-            if (keys_[i] == kEmpty) return nullptr;
-        }
+        base_ = base;
+        n_ = n;
+        idx_.reset(static_cast<int32_t *>(std::calloc((size_t)std::max<int64_t>(n, 1), sizeof(int32_t))));
+        vals_.clear();
     }
-    void put(uint64_t key, const V &v)
+    bool ok() const { return (bool)idx_; }
+    V *find(int64_t key)
     {
-        if (2 * (n_ + 1) > keys_.size()) grow();
-        for (size_t i = slot(key);; i = (i + 1) & (keys_.size() - 1)) {
-            if (keys_[i] == key) {
-                vals_[i] = v;
-                return;
-            }
-            if (keys_[i] == kEmpty) {
-                keys_[i] = key;
-                vals_[i] = v;
-                ++n_;
-                return;
-            }
+        const int32_t q = idx_.get()[key - base_];
+        return q ? &vals_[(size_t)q - 1] : nullptr;
+    }
+    void put(int64_t key, const V &v)
+    {
+        int32_t &q = idx_.get()[key - base_];
+        if (q) {
+            vals_[(size_t)q - 1] = v;
+            return;
         }
+        vals_.push_back(v);
+        q = (int32_t)vals_.size();
     }
 
 private:
-    static constexpr uint64_t kEmpty = ~0ULL;
-    size_t slot(uint64_t key) const { return (size_t)((key * 0x9E3779B97F4A7C15ULL) >> 20) & (keys_.size() - 1); }
-    void grow()
-    {
-        std::vector<uint64_t> ok;
-        std::vector<V> ov;
-        ok.swap(keys_);
-        ov.swap(vals_);
-        const size_t cap = ok.empty() ? 1024 : 2 * ok.size();
-        keys_.assign(cap, kEmpty);
-        vals_.resize(cap);
-        n_ = 0;
-        for (size_t i = 0; i < ok.size(); ++i) {
-            if (ok[i] != kEmpty) put(ok[i], ov[i]);
-        }
-    }
-    std::vector<uint64_t> keys_;
+    struct Free {
+        void operator()(int32_t *p) const { std::free(p); }
+    };
+    int64_t base_ = 0;
+    int64_t n_ = 0;
+    std::unique_ptr<int32_t, Free> idx_;
     std::vector<V> vals_;
-    size_t n_ = 0;
 };
 
 /* what a prolonged outer face was computed from: a recomputation with the
@@ -323,6 +313,12 @@ public:
             return false;
         }
         fid_.assign((size_t)nface_, 0);
+        if (cfg_.mhd) {
+            psig_.init(2 * ncell_, nface_);
+            if (!psig_.ok()) {
+                return fail("ghost-fill compiler: no host memory for the face-prolongation signatures");
+            }
+        }
         ver_.assign((size_t)(2 * ncell_ + nface_), -1);
         /* the replay records about 36000 operations per block with a field
          * (ghost cells, ghost faces, groups, and the writes later found
@@ -1123,7 +1119,7 @@ private:
                         sg.target = 2 * a + bb;
                         for (int n = 0; n < 9; ++n) sg.ver[n] = n < nst ? zv[n] : -2;
                         fid(fine, d, xf) = FID_COARSER;
-                        const ProlongSig *prev = psig_.find((uint64_t)xe);
+                        const ProlongSig *prev = psig_.find(xe);
                         if (prev != nullptr && same_sig(*prev, sg) && ver_[xe] == prev->op) {
                             continue; /* recomputes the value the face already holds */
                         }
@@ -1154,7 +1150,7 @@ private:
         reads.erase(std::unique(reads.begin(), reads.end()), reads.end());
         add_group(p, reads, writes);
         for (auto &e : sigs) {
-            psig_.put((uint64_t)e.first, e.second);
+            psig_.put(e.first, e.second);
         }
         return true;
     }
@@ -1889,7 +1885,7 @@ private:
     Buf<Elem> rd_;               /* elements each op reads (parallel to prod_) */
     Buf<Elem> wr_;               /* elements each op writes */
     std::vector<FxPop> groups_;  /* face-prolongation groups (SPACE_GROUP ops) */
-    ElemMap<ProlongSig> psig_;
+    FaceIndexMap<ProlongSig> psig_;
     std::vector<int64_t> g_reads_, g_writes_;             /* prolong_group scratch */
     std::vector<std::pair<int64_t, ProlongSig>> g_sigs_;
     FxPlanStats stats_;
