@@ -262,14 +262,40 @@ struct ProlongSig {
     int ver[9];        /* stencil versions: 5 (minmod cross) or 9 (Barth-Jespersen 3x3) */
 };
 
+} /* namespace */
+
+struct FxPlanWorkspace {
+    std::vector<int8_t> fid;
+    std::vector<int> ver;
+    Buf<SeqOp> seq;
+    Buf<int> prod;
+    Buf<Elem> rd, wr;
+    std::vector<int16_t> lw, lr;
+};
+
+namespace {
+
 class Compiler {
 public:
-    Compiler(const fx_config &cfg, int nblocks, const fx_block_desc *blocks)
+    Compiler(const fx_config &cfg, int nblocks, const fx_block_desc *blocks, FxPlanWorkspace *ws = nullptr)
         : cfg_(cfg), n_(nblocks), b_(blocks),
           ncell_((int64_t)nblocks * FX_NCELLS),
-          nface_((int64_t)(cfg.mhd ? nblocks : 0) * 3 * FX_NFACES)
+          nface_((int64_t)(cfg.mhd ? nblocks : 0) * 3 * FX_NFACES), ws_(ws)
     {
+        if (ws_) {
+            borrow();
+            seq_.clear();
+            prod_.clear();
+            rd_.clear();
+            wr_.clear();
+        }
     }
+    ~Compiler()
+    {
+        if (ws_) borrow();  /* the buffers go back, their memory kept */
+    }
+    Compiler(const Compiler &) = delete;
+    Compiler &operator=(const Compiler &) = delete;
 
     /* the coarse/fine correction records only (no ghost-fill replay) */
     bool run_corrections(FxPlan &plan, std::string *err)
@@ -380,6 +406,18 @@ public:
     }
 
 private:
+    void borrow()
+    {
+        fid_.swap(ws_->fid);
+        ver_.swap(ws_->ver);
+        seq_.swap(ws_->seq);
+        prod_.swap(ws_->prod);
+        rd_.swap(ws_->rd);
+        wr_.swap(ws_->wr);
+        lw_.swap(ws_->lw);
+        lr_.swap(ws_->lr);
+    }
+
     bool fail(const char *msg)
     {
         if (err_) *err_ = msg;
@@ -1444,8 +1482,10 @@ private:
         /* 3. levelling over cell, cell-field and face elements: latest wave
          * that wrote / read each element (a fill has a handful of waves, far
          * below the int16 range) */
-        std::vector<int16_t> lw((size_t)(2 * ncell_ + nface_), -1);
-        std::vector<int16_t> lr((size_t)(2 * ncell_ + nface_), -1);
+        std::vector<int16_t> &lw = lw_;
+        std::vector<int16_t> &lr = lr_;
+        lw.assign((size_t)(2 * ncell_ + nface_), -1);
+        lr.assign((size_t)(2 * ncell_ + nface_), -1);
         int nwaves = 0;
         auto place = [&](const Elem *reads, int nr, const Elem *writes, int nw) {
             int wave = 0;
@@ -1589,8 +1629,10 @@ private:
                 std::vector<std::pair<int16_t, FxBop>>().swap(part[t]);
             });
         }
-        std::vector<int16_t>().swap(lw);
-        std::vector<int16_t>().swap(lr);
+        if (!ws_) {
+            std::vector<int16_t>().swap(lw);
+            std::vector<int16_t>().swap(lr);
+        }
         if (owner_) {
             shard_closure();
         }
@@ -1884,6 +1926,8 @@ private:
     Buf<int> prod_;              /* producers of the values each op reads */
     Buf<Elem> rd_;               /* elements each op reads (parallel to prod_) */
     Buf<Elem> wr_;               /* elements each op writes */
+    std::vector<int16_t> lw_, lr_; /* levelling: latest wave that wrote / read each element */
+    FxPlanWorkspace *ws_ = nullptr;
     std::vector<FxPop> groups_;  /* face-prolongation groups (SPACE_GROUP ops) */
     FaceIndexMap<ProlongSig> psig_;
     std::vector<int64_t> g_reads_, g_writes_;             /* prolong_group scratch */
@@ -1904,11 +1948,21 @@ private:
 
 } /* namespace */
 
+FxPlanWorkspace *fx_plan_workspace_new()
+{
+    return new FxPlanWorkspace();
+}
+
+void fx_plan_workspace_free(FxPlanWorkspace *ws)
+{
+    delete ws;
+}
+
 bool fx_build_plan(const fx_config &cfg, int nblocks, const fx_block_desc *blocks,
-    FxPlan &plan, std::string *err)
+    FxPlan &plan, std::string *err, FxPlanWorkspace *ws)
 {
     plan = FxPlan();
-    Compiler c(cfg, nblocks, blocks);
+    Compiler c(cfg, nblocks, blocks, ws);
     return c.run(plan, err);
 }
 

@@ -46,6 +46,9 @@ struct fx_ctx {
     fx_config cfg{};
     int nv = 9;
     cudaStream_t stream = nullptr;
+    /* the ghost-fill compiler's working buffers, kept from one adapt to the
+     * next (created by the first fx_amr_adapt) */
+    FxPlanWorkspace *plan_ws = nullptr;
     std::string err;
     int sticky = 0; /* a device-side physics failure was seen */
 
@@ -1009,6 +1012,8 @@ void fx_destroy(fx_ctx *c)
     if (!c) {
         return;
     }
+    fx_plan_workspace_free(c->plan_ws);
+    c->plan_ws = nullptr;
     cudaSetDevice(c->device);
     if (c->stream) {
         cudaStreamSynchronize(c->stream);
@@ -2149,7 +2154,8 @@ int fx_amr_adapt(fx_ctx *c, int *changed)
     /* the ghost fill of the new mesh compiles while the device moves data */
     t = clk::now();
     FxPlan plan;
-    if (!fx_build_plan(c->cfg, nb, res.blocks.data(), plan, &err)) {
+    if (!c->plan_ws) c->plan_ws = fx_plan_workspace_new();
+    if (!fx_build_plan(c->cfg, nb, res.blocks.data(), plan, &err, c->plan_ws)) {
         cudaFree(d_inj);
         return set_err(c, FX_EINVAL, "fx_amr_adapt: %s", err.c_str());
     }
