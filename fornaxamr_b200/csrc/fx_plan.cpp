@@ -62,8 +62,8 @@ void parallel_for(int n, F fn);
 /* stable sort of ops by destination key (keys are below 2^31; face keys
  * repeat across the three face directions): a parallel stable
  * most-significant pass on key >> 13 (the block, with two face bits), then
- * each bin stable-sorted on its own */
-void sort_by_dst(FxGop *a, size_t n, int nt)
+ * each bin stable-sorted on its own; tmp: room for n operations */
+void sort_by_dst(FxGop *a, size_t n, int nt, FxGop *tmp)
 {
     if (n < 2) return;
     uint32_t top = 0;
@@ -93,7 +93,6 @@ void sort_by_dst(FxGop *a, size_t n, int nt)
         }
     }
     bin_begin[nbins] = run;
-    std::vector<FxGop> tmp(n);
     parallel_for(nt, [&](int t) {
         size_t lo, hi;
         chunk(t, lo, hi);
@@ -102,7 +101,7 @@ void sort_by_dst(FxGop *a, size_t n, int nt)
     });
     parallel_for(nt, [&](int t) {
         for (size_t bin = (size_t)t; bin < nbins; bin += (size_t)nt) {
-            FxGop *x = tmp.data() + bin_begin[bin];
+            FxGop *x = tmp + bin_begin[bin];
             const size_t m = bin_begin[bin + 1] - bin_begin[bin];
             std::stable_sort(x, x + m, [](const FxGop &u, const FxGop &v) { return u.dst < v.dst; });
             std::memcpy(a + bin_begin[bin], x, m * sizeof(FxGop));
@@ -271,6 +270,9 @@ struct FxPlanWorkspace {
     Buf<int> prod;
     Buf<Elem> rd, wr;
     std::vector<int16_t> lw, lr;
+    std::vector<Rec> recs;                                   /* parallel replay passes */
+    std::vector<Buf<std::pair<int16_t, FxBop>>> bparts;      /* cell-field operations per thread */
+    Buf<FxGop> sort_tmp;                                     /* sort_by_dst scratch */
 };
 
 namespace {
@@ -565,7 +567,15 @@ private:
                 seq_[sb[t] + q] = x;
                 ver_[wr_[x.w_begin]] = (int)(sb[t] + q);
             }
-            r = Rec();
+            if (ws_) {
+                r.seq.clear();
+                r.prod.clear();
+                r.rd.clear();
+                r.wr.clear();
+                r.rewired = 0;
+            } else {
+                r = Rec();
+            }
         });
     }
 
@@ -648,7 +658,16 @@ private:
                 if (acc * nt >= work * t) cut[t++] = q + 1;
             }
         }
-        std::vector<Rec> recs(nt);
+        std::vector<Rec> own;
+        std::vector<Rec> &recs = ws_ ? ws_->recs : own;
+        if ((int)recs.size() < nt) recs.resize(nt);
+        for (Rec &r : recs) {
+            r.seq.clear();
+            r.prod.clear();
+            r.rd.clear();
+            r.wr.clear();
+            r.rewired = 0;
+        }
         parallel_for(nt, [&](int t) {
             Rec &r = recs[t];
             for (size_t q = cut[t]; q < cut[t + 1]; ++q) {
@@ -1523,12 +1542,15 @@ private:
         if (cfg_.mhd) {
             const int nt = compile_threads();
             const int na = (int)plan.active.size();
-            std::vector<std::vector<std::pair<int16_t, FxBop>>> part(nt);
+            std::vector<Buf<std::pair<int16_t, FxBop>>> own_parts;
+            std::vector<Buf<std::pair<int16_t, FxBop>>> &part = ws_ ? ws_->bparts : own_parts;
+            if ((int)part.size() < nt) part.resize(nt);
+            for (auto &v : part) v.clear();
             std::vector<std::vector<int>> cnt(nt);
             std::vector<long long> rew(nt, 0);
             std::vector<std::vector<std::vector<Elem>>> tinit(nt, std::vector<std::vector<Elem>>(owner_ ? nranks_ : 0));
             parallel_for(nt, [&](int t) {
-                std::vector<std::pair<int16_t, FxBop>> &out = part[t];
+                Buf<std::pair<int16_t, FxBop>> &out = part[t];
                 /* per block: every face resolved once through its copy chain */
                 std::vector<int32_t> fkey(3 * FX_NFACES);
                 std::vector<int16_t> fwave(3 * FX_NFACES);
@@ -1626,7 +1648,11 @@ private:
             bops_all.resize(run);
             parallel_for(nt, [&](int t) {
                 for (const auto &e : part[t]) bops_all[at[t][e.first]++] = e.second;
-                std::vector<std::pair<int16_t, FxBop>>().swap(part[t]);
+                if (ws_) {
+                    part[t].clear();
+                } else {
+                    Buf<std::pair<int16_t, FxBop>>().swap(part[t]);
+                }
             });
         }
         if (!ws_) {
@@ -1714,7 +1740,12 @@ private:
             for (size_t k = 0; k < KF; ++k) {
                 if (bf[k + 1] > bf[k]) buckets.emplace_back(g.face_ops.data() + bf[k], (size_t)(bf[k + 1] - bf[k]));
             }
-            for (const auto &bk : buckets) sort_by_dst(bk.first, bk.second, nts);
+            size_t most = 0;
+            for (const auto &bk : buckets) most = std::max(most, bk.second);
+            Buf<FxGop> own_tmp;
+            Buf<FxGop> &tmp = ws_ ? ws_->sort_tmp : own_tmp;
+            if (tmp.size() < most) tmp.resize(most);
+            for (const auto &bk : buckets) sort_by_dst(bk.first, bk.second, nts, tmp.data());
         }
         g.b_ops.swap(bops_all);
         g.b_begin.assign(1, 0);

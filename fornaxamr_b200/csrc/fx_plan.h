@@ -82,11 +82,12 @@ struct FxPlan {
 #define FX_MAX_RANKS 16
 
 /* The ghost-fill compiler's large working buffers (element versions and
- * fidelities, the recorded sequence, the wave arrays), kept between
+ * fidelities, the recorded sequence and its per-thread parts, the wave
+ * arrays, the cell-field operations per thread, the sort scratch), kept between
  * compiles: a later compile reuses their memory instead of faulting in
- * fresh pages, which is about a sixth of a compile of a few thousand
- * blocks.  Holds about 1.1 MB of host memory per MHD block entry of the
- * largest mesh compiled with it (2.7 GB for 2352 entries). */
+ * fresh pages, which is about a fifth of a compile of a few thousand
+ * blocks.  Holds about 1.7 MB of host memory per MHD block entry of the
+ * largest mesh compiled with it (4.1 GB for 2352 entries). */
 struct FxPlanWorkspace;
 FxPlanWorkspace *fx_plan_workspace_new();
 void fx_plan_workspace_free(FxPlanWorkspace *ws);
