@@ -273,6 +273,7 @@ struct FxPlanWorkspace {
     std::vector<Rec> recs;                                   /* parallel replay passes */
     std::vector<Buf<std::pair<int16_t, FxBop>>> bparts;      /* cell-field operations per thread */
     Buf<FxGop> sort_tmp;                                     /* sort_by_dst scratch */
+    FxProgram spare;                                         /* arrays of a retired plan */
 };
 
 namespace {
@@ -1538,6 +1539,7 @@ private:
          * blocks are independent: they run on worker threads and are merged
          * in block order. */
         std::vector<FxBop> bops_all;
+        if (ws_ && cfg_.mhd) bops_all.swap(ws_->spare.b_ops);   /* every entry is written below */
         std::vector<int> bops_begin;
         if (cfg_.mhd) {
             const int nt = compile_threads();
@@ -1710,6 +1712,13 @@ private:
         const std::vector<int> bc = offsets(tcnt_c, KC);
         const std::vector<int> bf = offsets(tcnt_f, KF);
         const std::vector<int> bp = offsets(tcnt_p, KP);
+        if (ws_) {
+            /* every entry is written below: a retired plan's arrays serve
+             * (resize keeps what they hold, so no new pages are touched) */
+            g.cell_ops.swap(ws_->spare.cell_ops);
+            g.face_ops.swap(ws_->spare.face_ops);
+            g.p_ops.swap(ws_->spare.p_ops);
+        }
         g.cell_ops.resize(bc[KC]);
         g.face_ops.resize(bf[KF]);
         g.p_ops.resize(bp[KP]);
@@ -1987,6 +1996,15 @@ FxPlanWorkspace *fx_plan_workspace_new()
 void fx_plan_workspace_free(FxPlanWorkspace *ws)
 {
     delete ws;
+}
+
+void fx_plan_workspace_recycle(FxPlanWorkspace *ws, FxPlan &&old)
+{
+    if (!ws) return;
+    ws->spare.cell_ops.swap(old.ghost.cell_ops);
+    ws->spare.face_ops.swap(old.ghost.face_ops);
+    ws->spare.p_ops.swap(old.ghost.p_ops);
+    ws->spare.b_ops.swap(old.ghost.b_ops);
 }
 
 bool fx_build_plan(const fx_config &cfg, int nblocks, const fx_block_desc *blocks,

@@ -91,6 +91,9 @@ struct FxPlan {
 struct FxPlanWorkspace;
 FxPlanWorkspace *fx_plan_workspace_new();
 void fx_plan_workspace_free(FxPlanWorkspace *ws);
+/* hands a plan that is no longer used to the workspace: the next compile
+ * writes its ghost-fill program into that plan's arrays */
+void fx_plan_workspace_recycle(FxPlanWorkspace *ws, FxPlan &&old);
 
 /* Builds the plan.  Returns false and sets *err for meshes the device path
  * does not handle (e.g. non-outflow field boundaries in an MHD run, which the

@@ -2161,7 +2161,12 @@ int fx_amr_adapt(fx_ctx *c, int *changed)
     }
     free_graphs(c);
     drop_adjoint(c);
-    c->plan = std::move(plan);
+    {
+        /* the retired plan's program arrays take the next adapt's program */
+        FxPlan old = std::move(c->plan);
+        c->plan = std::move(plan);
+        fx_plan_workspace_recycle(c->plan_ws, std::move(old));
+    }
     c->blocks = std::move(res.blocks);
     c->nblocks = nb;
     c->nactive = (int)c->plan.active.size();

@@ -451,8 +451,9 @@ int fx_amr_tag(fx_ctx *ctx, int32_t *refine_flag);
  * and fills the ghosts of slot 0.  *changed = 1 if the mesh changed.  From
  * the first call on, the context keeps the ghost-fill compiler's working
  * buffers in host memory (about 1.7 MB per MHD block entry of the largest
- * adapted mesh: 4.1 GB for 2352 entries) so that later adapts reuse them
- * instead of faulting in fresh pages; fx_destroy releases them. */
+ * adapted mesh: 4.1 GB for 2352 entries, plus the program arrays of the
+ * previous mesh's ghost fill) so that later adapts reuse them instead of
+ * faulting in fresh pages; fx_destroy releases them. */
 int fx_amr_adapt(fx_ctx *ctx, int *changed);
 /* The mirrored mesh: *nblocks entries (unused ones have id < 0) are written
  * to out if capacity allows; *nblocks is always set. */
